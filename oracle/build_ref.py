@@ -1,0 +1,136 @@
+"""Build recipe for oracle/_ref: the reference's own WGSL compute shaders,
+translated to C++ (oracle/wgsl2cpp.py) and compiled with g++ for the host.
+
+TEST INFRASTRUCTURE ONLY.  Reads the reference checkout (default
+/root/reference, override with NPRUSH_REFERENCE) at build time; outputs go only
+to oracle/_ref/ (git-ignored).  Sizes are baked into the shaders exactly as the
+reference bakes them at pipeline creation (`{@NUM_SPLATS}` etc.), so one shared
+object is built per (shader, size) and cached by content hash.
+
+Each shared object exports:
+  wg_bind(group, binding, void*)          storage / uniform buffer binding
+  wg_bind_tex(group, binding, rgba*, w, h) texture_2d<f32> binding (fp32 RGBA)
+  wg_size(unsigned[3])                    @workgroup_size
+  wg_run_one(x, y, z, gx, gy, gz)         run one workgroup to completion
+  wg_dispatch(gx, gy, gz)                 run all workgroups in x-fastest order
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+import re
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF_OUT = HERE / "_ref"
+SHADERS = ("splat_backward", "splat_step", "splat_adc", "bezier_backward", "bezier_step", "bezier_adc")
+
+
+def reference_root() -> Path:
+    return Path(os.environ.get("NPRUSH_REFERENCE", "/root/reference"))
+
+
+def reference_available() -> bool:
+    return (reference_root() / "src/lib/gpu/splat_backward.wgsl").is_file()
+
+
+def gpu_constants() -> dict:
+    """GPU_CONSTANTS parsed from the reference's src/lib/gpu/constants.ts:5-42."""
+    text = (reference_root() / "src/lib/gpu/constants.ts").read_text()
+    body = text[text.index("GPU_CONSTANTS = {"):]
+    body = body[: body.index("};")]
+    out = {}
+    for m in re.finditer(r"^\s*([A-Z0-9_]+)\s*:\s*([^,/\n]+),", body, re.M):
+        expr = m.group(2).strip()
+        if not re.fullmatch(r"[0-9eE.+\-*/ ()]+", expr):
+            raise ValueError(f"unexpected constant expression {expr!r}")
+        out[m.group(1)] = eval(expr, {"__builtins__": {}})  # numeric literal arithmetic only
+    return out
+
+
+def splat_consts(n: int) -> dict:
+    # GpuSplatOptimizerManager.ts:127-136
+    c = dict(gpu_constants())
+    c.update(NUM_SPLATS=n, NUM_SPLATS_PLUS_ONE=n + 1, NUM_SPLATS_MINUS_ONE=n - 1,
+             NUM_SPLATS_DIV_32=-(-n // 32), NUM_PARAMS=n * 16)
+    return c
+
+
+def bezier_consts(n: int) -> dict:
+    # GpuBezierOptimizerManager.ts:146-158 (OPTIM_WIDTH/HEIGHT are baked as 256)
+    c = dict(gpu_constants())
+    c.update(NUM_BEZIERS=n, NUM_BEZIERS_PLUS_ONE=n + 1, NUM_BEZIERS_MINUS_ONE=n - 1,
+             NUM_BEZIERS_DIV_32=-(-n // 32), NUM_BEZIER_PARAMS=n * 18,
+             PIXEL_LOSS_SIZE=c["PIXEL_LOSS_MAX"], OPTIM_WIDTH=256, OPTIM_HEIGHT=256)
+    return c
+
+
+def build(shader: str, n: int) -> Path:
+    """Translate + compile `shader` with N baked in; returns the .so path."""
+    from wgsl2cpp import TRANSLATOR_VERSION, translate  # noqa: local import (sys.path set by caller)
+
+    if shader not in SHADERS:
+        raise ValueError(shader)
+    src_path = reference_root() / "src/lib/gpu" / f"{shader}.wgsl"
+    src = src_path.read_text()
+    consts = splat_consts(n) if shader.startswith("splat") else bezier_consts(n)
+    rt = (HERE / "wgsl_rt.h").read_text()
+    key = hashlib.sha256(
+        (src + repr(sorted(consts.items())) + TRANSLATOR_VERSION + rt + (HERE / "wgsl2cpp.py").read_text()).encode()
+    ).hexdigest()[:16]
+    REF_OUT.mkdir(exist_ok=True)
+    so = REF_OUT / f"{shader}_n{n}_{key}.so"
+    if so.exists():
+        return so
+    cpp = REF_OUT / f"{shader}_n{n}_{key}.cpp"
+    cpp.write_text(translate(src, consts, f"src/lib/gpu/{shader}.wgsl"))
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+           "-w", f"-I{HERE}", "-o", str(so) + ".tmp", str(cpp)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed for {shader}:\n{r.stderr[-4000:]}")
+    os.replace(str(so) + ".tmp", so)
+    return so
+
+
+class RefModule:
+    """ctypes handle on one compiled reference shader."""
+
+    def __init__(self, shader: str, n: int):
+        import sys
+        if str(HERE) not in sys.path:
+            sys.path.insert(0, str(HERE))
+        self.path = build(shader, n)
+        self.lib = ctypes.CDLL(str(self.path))
+        self.lib.wg_bind.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        self.lib.wg_bind_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint]
+        self.lib.wg_run_one.argtypes = [ctypes.c_uint] * 6
+        self.lib.wg_dispatch.argtypes = [ctypes.c_uint] * 3
+        ws = (ctypes.c_uint * 3)()
+        self.lib.wg_size(ws)
+        self.wgsize = tuple(ws)
+        self._keep = []
+
+    def bind(self, binding: int, arr, group: int = 0):
+        self._keep.append(arr)
+        self.lib.wg_bind(group, binding, arr.ctypes.data)
+
+    def bind_tex(self, binding: int, rgba, group: int = 0):
+        assert rgba.dtype.name == "float32" and rgba.ndim == 3 and rgba.shape[2] == 4 and rgba.flags.c_contiguous
+        self._keep.append(rgba)
+        self.lib.wg_bind_tex(group, binding, rgba.ctypes.data, rgba.shape[1], rgba.shape[0])
+
+    def dispatch(self, gx: int, gy: int = 1, gz: int = 1):
+        self.lib.wg_dispatch(gx, gy, gz)
+
+    def run_one(self, x, y, z, gx, gy, gz):
+        self.lib.wg_run_one(x, y, z, gx, gy, gz)
+
+
+if __name__ == "__main__":
+    import sys
+    sys.path.insert(0, str(HERE))
+    for sh in SHADERS:
+        print(build(sh, 64))

@@ -1,0 +1,118 @@
+"""ctypes front end of the CPU oracle (oracle/nps_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, always as the checker.  The product library
+(nprush_b200) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "libnps_oracle.so"
+SOURCES = [HERE / "nps_oracle.cpp", HERE / "nps_oracle_gs.cpp"]
+
+
+def build(force: bool = False) -> Path:
+    newest = max(s.stat().st_mtime for s in SOURCES if s.exists())
+    if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
+        return LIB
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+           "-shared", "-o", str(LIB) + ".tmp"] + [str(s) for s in SOURCES if s.exists()]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stderr[-4000:])
+    os.replace(str(LIB) + ".tmp", LIB)
+    return LIB
+
+
+_lib = None
+F = ctypes.POINTER(ctypes.c_float)
+I = ctypes.POINTER(ctypes.c_int32)
+U = ctypes.POINTER(ctypes.c_uint32)
+D = ctypes.POINTER(ctypes.c_double)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB))
+    return _lib
+
+
+def _p(a, t):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ------------------------------------------------------------- compat splats
+def splat_backward(splats, vp, vpinv, tgt_rgba, tgt_depth, grads_q=None, want_float=True, want_image=True):
+    """One view of splat_backward.wgsl. Returns dict(grads_q, grads_f, image, tile_count)."""
+    splats = _f32(splats)
+    n = splats.shape[0]
+    h, w = tgt_depth.shape
+    gq = np.zeros((n, 16), np.int32) if grads_q is None else grads_q
+    gf = np.zeros((n, 16), np.float32) if want_float else None
+    img = np.zeros((h, w, 4), np.float32) if want_image else None
+    tc = np.zeros(((h + 15) // 16, (w + 15) // 16), np.uint32)
+    lib().orc_splat_backward(_p(splats, F), n, _p(_f32(vp), F), _p(_f32(vpinv), F), _p(_f32(tgt_rgba), F),
+                             _p(_f32(tgt_depth), F), w, h, _p(gq, I), _p(gf, F), _p(img, F), _p(tc, U))
+    return dict(grads_q=gq, grads_f=gf, image=img, tile_count=tc)
+
+
+def splat_step(splats, grads, m, v, adam_t, grad_accum):
+    """In place: splats, grads (zeroed), m, v, grad_accum. Returns new t."""
+    t = np.array([adam_t], np.float32)
+    lib().orc_splat_step(_p(splats, F), _p(grads, I), _p(m, F), _p(v, F), _p(t, F), _p(grad_accum, F),
+                         splats.shape[0])
+    return float(t[0])
+
+
+def splat_adc(splats, m, v, adam_t, grad_accum):
+    lib().orc_splat_adc(_p(splats, F), _p(m, F), _p(v, F), ctypes.c_float(adam_t), _p(grad_accum, F),
+                        splats.shape[0])
+
+
+# ------------------------------------------------------------ compat beziers
+def bezier_backward(beziers, vp, uni, tgt_rgba, tgt_depth, bg_rgba, bg_depth, normal_rgba,
+                    grads_q=None, loss_accum=None, pixel_loss=None, want_float=True, want_image=True):
+    beziers = _f32(beziers)
+    n = beziers.shape[0]
+    h, w = tgt_depth.shape
+    gq = np.zeros((n, 18), np.int32) if grads_q is None else grads_q
+    gf = np.zeros((n, 18), np.float32) if want_float else None
+    la = np.zeros(n, np.float32) if loss_accum is None else loss_accum
+    pl = np.zeros(512 * 512, np.int32) if pixel_loss is None else pixel_loss
+    img = np.zeros((h, w, 4), np.float32) if want_image else None
+    tc = np.zeros(((h + 15) // 16, (w + 15) // 16), np.uint32)
+    lib().orc_bezier_backward(_p(beziers, F), n, _p(_f32(vp), F), _p(_f32(uni), F), _p(_f32(tgt_rgba), F),
+                              _p(_f32(tgt_depth), F), _p(_f32(bg_rgba), F), _p(_f32(bg_depth), F),
+                              _p(_f32(normal_rgba), F), w, h, _p(gq, I), _p(gf, F), _p(la, F), _p(pl, I),
+                              _p(img, F), _p(tc, U))
+    return dict(grads_q=gq, grads_f=gf, loss_accum=la, pixel_loss=pl, image=img, tile_count=tc)
+
+
+def bezier_step(beziers, grads, m, v, adam_t, pixel_count, no_kill, grad_accum, vp, uni):
+    t = np.array([adam_t], np.float32)
+    lib().orc_bezier_step(_p(beziers, F), _p(grads, I), _p(m, F), _p(v, F), _p(t, F), ctypes.c_float(pixel_count),
+                          ctypes.c_float(no_kill), _p(grad_accum, F), _p(_f32(vp), F), _p(_f32(uni), F),
+                          beziers.shape[0])
+    return float(t[0])
+
+
+def bezier_adc(beziers, m, v, adam_t, no_kill, grad_accum, loss_accum, pixel_loss, vp, vpinv):
+    lib().orc_bezier_adc(_p(beziers, F), _p(m, F), _p(v, F), ctypes.c_float(adam_t), ctypes.c_float(no_kill),
+                         _p(grad_accum, F), _p(loss_accum, F), _p(pixel_loss, I), _p(_f32(vp), F),
+                         _p(_f32(vpinv), F), beziers.shape[0])
