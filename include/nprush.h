@@ -1,0 +1,123 @@
+/* nprush.h — C ABI of libnprush_cuda.so, the B200 (sm_100a) implementation of
+ * nprush's differentiable splat / Bezier rasterisation hot path.
+ *
+ * The reference (wooningeire/nprush) exposes this path through TypeScript
+ * manager classes over WebGPU.  Each entry point below names the reference
+ * method it replaces (file:line in src/lib/gpu/).  All functions:
+ *   - are extern "C", take plain pointers and sizes, and return int status
+ *     (NPS_OK = 0, negative on error); nps_last_error() gives a thread-local
+ *     message for the last failure on the calling thread;
+ *   - enqueue work on the context's CUDA stream and return without waiting,
+ *     except the read_* functions, which wait for the copy to finish;
+ *   - are not thread-safe per context: one host thread drives one context,
+ *     as one JS thread drives one GPUDevice queue in the reference.
+ * Matrices are 16 floats, column-major (WGSL mat4x4f as uploaded by
+ * Float32Array from wgpu-matrix).  Images are row-major, y = 0 at the top.
+ */
+#ifndef NPRUSH_H
+#define NPRUSH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  NPS_OK = 0,
+  NPS_ERR_INVALID = -1,   /* bad argument (null handle, size 0, size mismatch) */
+  NPS_ERR_CUDA = -2,      /* CUDA runtime error (message in nps_last_error) */
+  NPS_ERR_NOMEM = -3,     /* device allocation failed */
+  NPS_ERR_CAPACITY = -4,  /* a work buffer was too small; sizes were grown, retry */
+  NPS_ERR_TIMEOUT = -5,   /* a bounded device-side wait gave up */
+  NPS_ERR_STATE = -6      /* call order violated (e.g. dispatch before set_target) */
+};
+
+/* Where a pointer argument lives. */
+enum {
+  NPS_MEM_HOST = 0,          /* host memory: copied before the call returns */
+  NPS_MEM_DEVICE = 1,        /* device memory: copied on the context stream */
+  NPS_MEM_DEVICE_BORROW = 2  /* device memory kept by reference until replaced
+                                (like a texture view bound into a bind group) */
+};
+
+typedef struct nps_ctx nps_ctx;
+typedef struct nps_splat_opt nps_splat_opt;
+typedef struct nps_bezier_opt nps_bezier_opt;
+typedef struct nps_gs nps_gs;
+
+/* ---------------------------------------------------------------- context */
+/* Replaces requestGpu() (requestGpu.ts:16-64): binds a CUDA device and stream. */
+int nps_create(int device, nps_ctx** out);
+int nps_destroy(nps_ctx* ctx);
+/* Waits for all work queued on the context stream (the reference never waits). */
+int nps_sync(nps_ctx* ctx);
+/* Uses an external CUDA stream (cudaStream_t) instead of the context's own. */
+int nps_set_stream(nps_ctx* ctx, void* cuda_stream);
+const char* nps_last_error(void);
+const char* nps_version(void);
+
+/* ============================================= splats, reference semantics
+ * Parameter record: 16 floats per splat, the reference's AoS layout
+ * (splat_forward.wgsl:1-6): pos.xyz, sx | r, g, b, opacity | qw, qx, qy, qz |
+ * sy, shape_a, shape_b, sz.  Gradients are the reference's fixed-point i32
+ * sums (splat_backward.wgsl:436-455); Adam state m, v is 16 floats per splat.
+ */
+/* new GpuSplatOptimizerManager({numSplats}) (GpuSplatOptimizerManager.ts:43-125).
+ * Parameters start zeroed (all splats dead); upload them with write_params. */
+int nps_splat_opt_create(nps_ctx* ctx, uint32_t num_splats, nps_splat_opt** out);
+int nps_splat_opt_destroy(nps_splat_opt* opt);
+/* queue.writeBuffer(splatBuffer, first*64, ...) (GpuSplatOptimizerManager.ts:93). */
+int nps_splat_opt_write_params(nps_splat_opt* opt, const float* splats, uint32_t first, uint32_t count, int mem);
+/* Optimizer state for tests and checkpoints: the i32 gradient accumulators
+ * (N*16), Adam m, v (N*16 f32 each), the step counter t and grad_accum (N f32).
+ * Null pointers are skipped. */
+int nps_splat_opt_write_state(nps_splat_opt* opt, const int32_t* grads, const float* adam_m, const float* adam_v,
+                              float adam_t, const float* grad_accum, int mem);
+int nps_splat_opt_read_state(nps_splat_opt* opt, float* splats, int32_t* grads, float* adam_m, float* adam_v,
+                             float* adam_t, float* grad_accum);
+/* writeSplatVPMatrix(vp, vpInv, blur) (GpuSplatOptimizerManager.ts:281-301),
+ * for num_views views (16 floats each).  blur_enabled is stored, unused, as in
+ * the reference backward. */
+int nps_splat_opt_write_vp(nps_splat_opt* opt, const float* vp, const float* vp_inv, uint32_t num_views,
+                           int blur_enabled);
+/* setBackwardTarget(colour, depth, w, h) (GpuSplatOptimizerManager.ts:303-317):
+ * rgba num_views*h*w*4 floats (.rgb used), depth num_views*h*w floats
+ * (reciprocal encoding 1 - 0.1/w, 1.0 = background). */
+int nps_splat_opt_set_target(nps_splat_opt* opt, const float* rgba, const float* depth, uint32_t width,
+                             uint32_t height, uint32_t num_views, int mem);
+/* dispatch(encoder) (GpuSplatOptimizerManager.ts:365-388): backward over all
+ * views, Adam step, and ADC on every 25th call. */
+int nps_splat_opt_dispatch(nps_splat_opt* opt);
+/* The three stages of dispatch, separately (splat_backward / splat_step /
+ * splat_adc).  backward optionally writes the fp32 composite the backward
+ * computes (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device). */
+int nps_splat_opt_backward(nps_splat_opt* opt, float* out_rgbd_device);
+int nps_splat_opt_step(nps_splat_opt* opt);
+int nps_splat_opt_adc(nps_splat_opt* opt);
+/* Headless GpuSplatForwardPipelineManager.dispatch(enc, clear=true)
+ * (GpuSplatForwardPipelineManager.ts:114-137, splat_forward.wgsl:42-156):
+ * fp32 composite of all splats (index 0 in front), w < 0.1 culled, alpha
+ * < 0.001 discarded, cleared to colour 0.05 / depth 1.  out_rgba and out_depth
+ * are device buffers of h*w*4 floats each (depth replicated in rgb, alpha in a). */
+int nps_splat_opt_render(nps_splat_opt* opt, const float* vp, uint32_t width, uint32_t height, float* out_rgba,
+                         float* out_depth);
+/* Device pointers of the library-owned buffers (splatBuffer, gradBuffer,
+ * Adam m / v, grad_accum), for zero-copy access; valid until destroy. */
+int nps_splat_opt_buffers(nps_splat_opt* opt, float** splats, int32_t** grads, float** adam_m, float** adam_v,
+                          float** grad_accum);
+
+typedef struct nps_stats {
+  uint64_t pairs;          /* (tile, primitive) pairs emitted by the last backward, all views */
+  uint64_t pairs_capped;   /* pairs composited after the per-tile cap */
+  uint32_t max_tile_len;   /* longest tile list before the cap */
+  uint32_t adc_clones;     /* clones + splits performed by the last ADC */
+  uint32_t step_count;     /* dispatch() calls so far */
+  uint32_t reserved[3];
+} nps_stats;
+int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NPRUSH_H */

@@ -1,0 +1,1012 @@
+// compat_splat.cu — splat training step with the reference's semantics.
+//
+// Implements GpuSplatOptimizerManager.dispatch() (GpuSplatOptimizerManager.ts:
+// 365-388) as B200 kernels instead of the reference's per-tile all-N scan:
+//   k_project      per (view, splat): the pixel-independent part of eval_splat
+//                  (splat_backward.wgsl:92-126) + the binning AABB
+//                  (:155-195) turned into a tile rectangle (exact predicate,
+//                  binary search over per-axis tile bounds)
+//   scan + k_emit  one (view*tiles + tile, splat) pair per overlapped tile
+//   radix sort     stable by key, so every tile list is in ascending splat
+//                  index order, as the reference's bitmask compaction
+//                  (:199-210) produces
+//   k_raster       one CTA per (tile, view): first 1024 entries only (the cap
+//                  at :205), fp32 front-to-back composite (:216-248), L2 +
+//                  depth loss (:250-257), reverse backward (:259-456) with
+//                  transmittance replayed exactly from per-32-splat
+//                  checkpoints, per-pair i32 truncation, warp __reduce_add_sync
+//                  and CTA shared-memory sums before one global atomic per
+//                  (splat, param) per tile
+//   k_step         splat_step.wgsl:32-106
+//   k_adc          splat_adc.wgsl:28-87, same serial result, computed a
+//                  1024-splat window at a time
+// This file is compiled with --fmad=false: every float operation is rounded
+// separately, in the reference's order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+
+namespace nps {
+namespace compat {
+
+constexpr int kFwd = 16;        // floats per forward record
+constexpr int kBwd = 32;        // floats per backward record
+constexpr uint32_t kCap = 1024; // SPLAT_MAX_TILE_SPLATS, constants.ts:35
+constexpr int kChunk = 32;
+constexpr int kThreads = 256;
+constexpr float kFpPos = 10000.0f, kFpCol = 100000.0f;  // constants.ts:36-37
+constexpr float kOpacityKill = 0.05f, kVolumeKill = 1e-7f, kGradThresh = 0.00005f, kAdcPeriod = 25.0f;
+
+__constant__ float c_lr[16] = {0.0005f, 0.0005f, 0.0005f, 0.01f, 0.02f, 0.02f, 0.02f, 0.01f,
+                               0.005f, 0.005f, 0.005f, 0.005f, 0.01f, 0.01f, 0.01f, 0.01f};
+__constant__ float c_mu[16] = {0.005f, 0.005f, 0.005f, 0.005f, 0.001f, 0.001f, 0.001f, 0.0005f,
+                               0.005f, 0.005f, 0.005f, 0.005f, 0.005f, 0.05f, 0.05f, 0.005f};
+__constant__ float c_lo[16] = {-1e9f, -1e9f, -1e9f, 0.001f, 0.05f, 0.05f, 0.05f, 0.01f,
+                               -1e9f, -1e9f, -1e9f, -1e9f, 0.001f, 0.1f, 0.01f, 0.001f};
+__constant__ float c_hi[16] = {1e9f, 1e9f, 1e9f, 2.0f, 1.0f, 1.0f, 1.0f, 0.99f,
+                               1e9f, 1e9f, 1e9f, 1e9f, 2.0f, 10.0f, 5.0f, 2.0f};
+
+__device__ __forceinline__ float clampf(float e, float lo, float hi) { return fminf(fmaxf(e, lo), hi); }
+
+// WGSL i32(f32): truncate toward zero, saturate.
+__device__ __forceinline__ int32_t to_i32(float a) {
+  if (a != a) return 0;
+  if (a >= 2147483520.0f) return 2147483520;
+  if (a <= -2147483648.0f) return INT32_MIN;
+  return (int32_t)a;
+}
+
+// WGSL M * vec4 with a column-major matrix, summed left to right.
+__device__ __forceinline__ float4 mulv(const float* m, float x, float y, float z, float w) {
+  float4 o;
+  o.x = m[0] * x + m[4] * y + m[8] * z + m[12] * w;
+  o.y = m[1] * x + m[5] * y + m[9] * z + m[13] * w;
+  o.z = m[2] * x + m[6] * y + m[10] * z + m[14] * w;
+  o.w = m[3] * x + m[7] * y + m[11] * z + m[15] * w;
+  return o;
+}
+
+struct f3 { float x, y, z; };
+__device__ __forceinline__ f3 cross3(f3 a, f3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+// splat_backward.wgsl:42-45
+__device__ __forceinline__ f3 quat_rotate(float qw, float qx, float qy, float qz, f3 v) {
+  f3 u{qx, qy, qz};
+  f3 c = cross3(u, v);
+  f3 t{2.0f * c.x, 2.0f * c.y, 2.0f * c.z};
+  f3 c2 = cross3(u, t);
+  return {v.x + qw * t.x + c2.x, v.y + qw * t.y + c2.y, v.z + qw * t.z + c2.z};
+}
+// splat_backward.wgsl:52-58
+__device__ __forceinline__ float2 project_axis(const float* vp, f3 ax, float cx, float cy, float w, float aspect) {
+  float4 ac = mulv(vp, ax.x, ax.y, ax.z, 0.0f);
+  return make_float2((ac.x * w - cx * ac.w) / (w * w) * aspect, (ac.y * w - cy * ac.w) / (w * w));
+}
+// splat_backward.wgsl:34-40, one axis at a time
+__device__ __forceinline__ float pixel_px(uint32_t px, uint32_t w, float aspect) {
+  float u = ((float)px + 0.5f) / (float)w;
+  return (u * 2.0f - 1.0f) * aspect;
+}
+__device__ __forceinline__ float pixel_py(uint32_t py, uint32_t h) {
+  float u = ((float)py + 0.5f) / (float)h;
+  return -(u * 2.0f - 1.0f);
+}
+
+// Tile bounds per axis, splat_backward.wgsl:148-153.
+__global__ void k_tile_tables(float* tabs, uint32_t tiles_x, uint32_t tiles_y, uint32_t w, uint32_t h) {
+  const float aspect = (float)w / (float)h;
+  for (uint32_t t = threadIdx.x; t < tiles_x; t += blockDim.x) {
+    tabs[t] = pixel_px(t * 16u, w, aspect);                            // tile_min_p.x
+    tabs[tiles_x + t] = pixel_px(min(t * 16u + 16u, w), w, aspect);    // tile_max_p.x
+  }
+  for (uint32_t t = threadIdx.x; t < tiles_y; t += blockDim.x) {
+    tabs[2 * tiles_x + t] = pixel_py(min(t * 16u + 16u, h), h);        // tile_min_p.y
+    tabs[2 * tiles_x + tiles_y + t] = pixel_py(t * 16u, h);            // tile_max_p.y
+  }
+}
+
+__global__ void __launch_bounds__(256) k_project(const float* __restrict__ splats, uint32_t n,
+                                                 const float* __restrict__ views, uint32_t nv, uint32_t w, uint32_t h,
+                                                 const float* __restrict__ tabs, uint32_t tiles_x, uint32_t tiles_y,
+                                                 float* __restrict__ fwd, float* __restrict__ bwd,
+                                                 uint32_t* __restrict__ counts, uint2* __restrict__ rects) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * n) return;
+  const uint32_t v = g / n, i = g - v * n;
+  const float* vp = views + 32 * (size_t)v;
+  float s[16];
+  const float4* sp4 = reinterpret_cast<const float4*>(splats + 16 * (size_t)i);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 t = sp4[q];
+    s[4 * q] = t.x; s[4 * q + 1] = t.y; s[4 * q + 2] = t.z; s[4 * q + 3] = t.w;
+  }
+  const float aspect = (float)w / (float)h;
+  // eval_splat, pixel-independent part (splat_backward.wgsl:94-126)
+  float4 clip = mulv(vp, s[0], s[1], s[2], 1.0f);
+  const float W = clip.w;
+  const float scx = clip.x / clip.w * aspect, scy = clip.y / clip.w;
+  const float sx = fmaxf(s[3], 0.0001f), sy = fmaxf(s[12], 0.0001f), sz = fmaxf(s[15], 0.0001f);
+  f3 axw = quat_rotate(s[8], s[9], s[10], s[11], {1.0f, 0.0f, 0.0f});
+  f3 ayw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 1.0f, 0.0f});
+  f3 azw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 0.0f, 1.0f});
+  float2 ax = project_axis(vp, axw, clip.x, clip.y, W, aspect);
+  float2 ay = project_axis(vp, ayw, clip.x, clip.y, W, aspect);
+  float2 az = project_axis(vp, azw, clip.x, clip.y, W, aspect);
+  const float m0x = ax.x * sx, m0y = ax.y * sx, m1x = ay.x * sy, m1y = ay.y * sy, m2x = az.x * sz, m2y = az.y * sz;
+  float cov00 = m0x * m0x + m1x * m1x + m2x * m2x;
+  float cov01 = m0x * m0y + m1x * m1y + m2x * m2y;
+  float cov11 = m0y * m0y + m1y * m1y + m2y * m2y;
+  const float filter_std = 0.3f * (2.0f / (float)h);
+  const float filter2 = filter_std * filter_std;
+  cov00 += filter2;
+  cov11 += filter2;
+  const float det = cov00 * cov11 - cov01 * cov01;
+  const float inv_det = fabsf(det) < 1e-10f ? 0.0f : 1.0f / det;
+  const float A = cov11 * inv_det, B = -cov01 * inv_det, C = cov00 * inv_det;
+  const float ld = fmaxf(W, 0.1f);
+  const float depth = clampf(1.0f - 0.1f / ld, 0.0f, 1.0f);
+
+  float4* f4 = reinterpret_cast<float4*>(fwd + (size_t)g * kFwd);
+  f4[0] = make_float4(scx, scy, A, B);
+  f4[1] = make_float4(C, s[13], s[14], s[7]);
+  f4[2] = make_float4(s[4], s[5], s[6], depth);
+  f4[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float4* b4 = reinterpret_cast<float4*>(bwd + (size_t)g * kBwd);
+  b4[0] = make_float4(W, clip.x, clip.y, sx);
+  b4[1] = make_float4(sy, sz, m0x, m0y);
+  b4[2] = make_float4(m1x, m1y, m2x, m2y);
+  b4[3] = make_float4(ax.x, ax.y, ay.x, ay.y);
+  b4[4] = make_float4(az.x, az.y, s[0], s[1]);
+  b4[5] = make_float4(s[2], s[8], s[9], s[10]);
+  b4[6] = make_float4(s[11], 0.0f, 0.0f, 0.0f);
+  b4[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+
+  // binning AABB, splat_backward.wgsl:157-190 (same arithmetic, cov00/cov11
+  // recomputed there without cov01: identical values)
+  uint32_t cnt = 0;
+  uint2 rect = make_uint2(0u, 0u);
+  if (!(s[7] < 0.005f) && !(W < 0.0f)) {
+    const float safe_sb = fmaxf(s[14], 0.0001f);
+    const float R = powf(15.0f / safe_sb, 1.0f / s[13]);
+    const float max_r = R * sqrtf(fmaxf(fmaxf(cov00, cov11), 1e-9f));
+    const float smin_x = scx - max_r, smin_y = scy - max_r, smax_x = scx + max_r, smax_y = scy + max_r;
+    const float* tminx = tabs;
+    const float* tmaxx = tabs + tiles_x;
+    const float* tminy = tabs + 2 * tiles_x;
+    const float* tmaxy = tabs + 2 * tiles_x + tiles_y;
+    // first tx with !(smin.x > tile_max.x)
+    uint32_t lo = 0, hi = tiles_x;
+    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (!(smin_x > tmaxx[m])) hi = m; else lo = m + 1; }
+    const uint32_t x0 = lo;
+    // first tx with (smax.x < tile_min.x) -> last overlapping = that - 1
+    lo = 0; hi = tiles_x;
+    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (smax_x < tminx[m]) hi = m; else lo = m + 1; }
+    const uint32_t x1 = lo;  // exclusive
+    // rows: tile_max.y / tile_min.y decrease with ty
+    lo = 0; hi = tiles_y;
+    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (!(smax_y < tminy[m])) hi = m; else lo = m + 1; }
+    const uint32_t y0 = lo;
+    lo = 0; hi = tiles_y;
+    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (smin_y > tmaxy[m]) hi = m; else lo = m + 1; }
+    const uint32_t y1 = lo;  // exclusive
+    if (x1 > x0 && y1 > y0) {
+      cnt = (x1 - x0) * (y1 - y0);
+      rect = make_uint2(x0 | (x1 << 16), y0 | (y1 << 16));
+    }
+  }
+  counts[g] = cnt;
+  rects[g] = rect;
+}
+
+__global__ void k_emit(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                       const uint2* __restrict__ rects, uint32_t n, uint32_t nv, uint32_t tiles_x, uint32_t num_tiles,
+                       uint32_t cap, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * n) return;
+  const uint32_t c = counts[g];
+  if (c == 0) return;
+  const uint32_t v = g / n, i = g - v * n;
+  uint32_t pos = offsets[g];
+  const uint2 r = rects[g];
+  const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
+  for (uint32_t ty = y0; ty < y1; ++ty)
+    for (uint32_t tx = x0; tx < x1; ++tx) {
+      if (pos < cap) {
+        keys[pos] = v * num_tiles + ty * tiles_x + tx;
+        vals[pos] = i;
+      }
+      ++pos;
+    }
+}
+
+// Tile list bounds in the sorted key array.
+__global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
+                         uint32_t* __restrict__ rstart, uint32_t* __restrict__ rend) {
+  const uint32_t K = min(*total, cap);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < K; p += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[p];
+    if (p == 0 || keys[p - 1] != k) rstart[k] = p;
+    if (p == K - 1 || keys[p + 1] != k) rend[k] = p + 1;
+  }
+}
+
+struct RasterArgs {
+  const float* fwd;
+  const float* bwd;
+  const uint32_t* vals;
+  const uint32_t* rstart;
+  const uint32_t* rend;
+  const float* views;
+  const float* tgt_rgba;
+  const float* tgt_depth;
+  int32_t* grads;
+  float* out_rgbd;
+  uint32_t n, w, h, tiles_x, num_tiles;
+};
+
+constexpr size_t kRasterSmem = sizeof(uint32_t) * kChunk + sizeof(float) * kChunk * (kFwd + kBwd) +
+                               sizeof(float) * 3 * kChunk * kThreads + sizeof(int32_t) * kChunk * 16;
+
+__device__ __forceinline__ float splat_alpha(const float* f, float px, float py) {
+  const float dx = px - f[0], dy = py - f[1];
+  const float spx = f[2] * dx + f[3] * dy;
+  const float spy = f[3] * dx + f[4] * dy;
+  const float r2 = dx * spx + dy * spy;
+  const float r = sqrtf(fmaxf(r2, 0.0001f));
+  const float power = -f[6] * powf(r, f[5]);
+  return clampf(power > -15.0f ? expf(power) * f[7] : 0.0f, 0.0f, 0.999f);
+}
+
+__global__ void __launch_bounds__(kThreads) k_raster(RasterArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* ids = reinterpret_cast<uint32_t*>(smem);
+  float* sf = reinterpret_cast<float*>(smem + sizeof(uint32_t) * kChunk);  // [kChunk][kFwd]
+  float* sb = sf + kChunk * kFwd;                                          // [kChunk][kBwd]
+  float* ckpt = sb + kChunk * kBwd;                                        // [kChunk][kThreads]
+  float* sA = ckpt + kChunk * kThreads;                                    // [kChunk][kThreads]
+  float* sT = sA + kChunk * kThreads;                                      // [kChunk][kThreads]
+  int32_t* gacc = reinterpret_cast<int32_t*>(sT + kChunk * kThreads);      // [kChunk][16]
+  __shared__ float vpm[16];
+
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z;
+  const uint32_t tid = threadIdx.x, lane = tid & 31;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const bool inside = px < a.w && py < a.h;
+  const float aspect = (float)a.w / (float)a.h;
+  const float ppx = pixel_px(px, a.w, aspect), ppy = pixel_py(py, a.h);
+  if (tid < 16) vpm[tid] = a.views[32 * (size_t)v + tid];
+  const uint32_t key = v * a.num_tiles + ty * a.tiles_x + tx;
+  const uint32_t start = a.rstart[key];
+  const uint32_t len = min(a.rend[key] - start, kCap);
+  const uint32_t nch = (len + kChunk - 1) / kChunk;
+  const float* fwd_v = a.fwd + (size_t)v * a.n * kFwd;
+  const float* bwd_v = a.bwd + (size_t)v * a.n * kBwd;
+
+  float T = 1.0f, Cr = 0.0f, Cg = 0.0f, Cb = 0.0f, D = 0.0f;
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t cnt = min((uint32_t)kChunk, len - c * kChunk);
+    __syncthreads();
+    if (tid < cnt) ids[tid] = a.vals[start + c * kChunk + tid];
+    __syncthreads();
+    if (tid < cnt * 4) {
+      const uint32_t k = tid >> 2, q = tid & 3;
+      reinterpret_cast<float4*>(sf)[k * 4 + q] =
+          reinterpret_cast<const float4*>(fwd_v + (size_t)ids[k] * kFwd)[q];
+    }
+    ckpt[c * kThreads + tid] = T;
+    __syncthreads();
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const float* f = sf + k * kFwd;
+      const float al = splat_alpha(f, ppx, ppy);
+      Cr += T * al * f[8];
+      Cg += T * al * f[9];
+      Cb += T * al * f[10];
+      D += T * al * f[11];
+      T = T * (1.0f - al);
+    }
+  }
+  const float bg = 0.05f;
+  Cr += T * bg; Cg += T * bg; Cb += T * bg;
+  D += T * 1.0f;
+  const size_t pix = ((size_t)v * a.h + (inside ? py : 0)) * a.w + (inside ? px : 0);
+  if (inside && a.out_rgbd) reinterpret_cast<float4*>(a.out_rgbd)[pix] = make_float4(Cr, Cg, Cb, D);
+  // loss, splat_backward.wgsl:250-257
+  float4 tc = inside ? reinterpret_cast<const float4*>(a.tgt_rgba)[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float td = inside ? a.tgt_depth[pix] : 1.0f;
+  const float dCr = 2.0f * (Cr - tc.x), dCg = 2.0f * (Cg - tc.y), dCb = 2.0f * (Cb - tc.z);
+  const bool fg = td < 0.99f;
+  const float dD = fg ? 2.0f * (D - td) : 0.0f;
+  float dT_C = dCr * bg + dCg * bg + dCb * bg;
+  float dT_D = dD * 1.0f;
+  // reconstruct_world_pos (splat_backward.wgsl:64-75): pair-independent
+  float surf_x = 0.0f, surf_y = 0.0f, surf_z = 0.0f;
+  if (fg) {
+    const float* vpi = a.views + 32 * (size_t)v + 16;
+    const float wr = 0.1f / fmaxf(1.0f - td, 1e-5f);
+    const float ndx = ppx / aspect, ndy = ppy;
+    float4 wp = mulv(vpi, ndx * wr, ndy * wr, wr, wr);
+    surf_x = wp.x / wp.w; surf_y = wp.y / wp.w; surf_z = wp.z / wp.w;
+  }
+  const float DEPTH_NEAR = 0.1f;
+
+  for (int c = (int)nch - 1; c >= 0; --c) {
+    const uint32_t cnt = min((uint32_t)kChunk, len - (uint32_t)c * kChunk);
+    __syncthreads();
+    if (tid < cnt) ids[tid] = a.vals[start + c * kChunk + tid];
+    gacc[tid] = 0;
+    gacc[tid + kThreads] = 0;
+    __syncthreads();
+    if (tid < cnt * 4) {
+      const uint32_t k = tid >> 2, q = tid & 3;
+      reinterpret_cast<float4*>(sf)[k * 4 + q] =
+          reinterpret_cast<const float4*>(fwd_v + (size_t)ids[k] * kFwd)[q];
+    }
+    for (uint32_t e = tid; e < cnt * 8; e += kThreads) {
+      const uint32_t k = e >> 3, q = e & 7;
+      reinterpret_cast<float4*>(sb)[k * 8 + q] = reinterpret_cast<const float4*>(bwd_v + (size_t)ids[k] * kBwd)[q];
+    }
+    __syncthreads();
+    // replay the chunk forward from its checkpoint: bit-identical alphas / Ts
+    float Tc = ckpt[c * kThreads + tid];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const float al = splat_alpha(sf + k * kFwd, ppx, ppy);
+      sA[k * kThreads + tid] = al;
+      sT[k * kThreads + tid] = Tc;
+      Tc = Tc * (1.0f - al);
+    }
+    for (int k = (int)cnt - 1; k >= 0; --k) {
+      const float al = sA[k * kThreads + tid];
+      const bool valid = inside && !(al < 0.001f);
+      if (!__any_sync(0xffffffffu, valid)) continue;
+      int32_t q[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) q[j] = 0;
+      if (valid) {
+        const float* f = sf + k * kFwd;
+        const float* b = sb + k * kBwd;
+        const float T_prev = sT[k * kThreads + tid];
+        const float cr = f[8], cg = f[9], cb = f[10], opacity = f[7], depth = f[11];
+        const float shape_a = f[5], shape_b = f[6];
+        const float Wc = b[0], clip_x = b[1], clip_y = b[2], sx = b[3], sy = b[4], sz = b[5];
+        const float m0x = b[6], m0y = b[7], m1x = b[8], m1y = b[9], m2x = b[10], m2y = b[11];
+        const float axx = b[12], axy = b[13], ayx = b[14], ayy = b[15], azx = b[16], azy = b[17];
+        const float pos0 = b[18], pos1 = b[19], pos2 = b[20];
+        const float qw = b[21], qx = b[22], qy = b[23], qz = b[24];
+        // eval_splat per-pixel part
+        const float ddx0 = ppx - f[0], ddy0 = ppy - f[1];
+        const float spx = f[2] * ddx0 + f[3] * ddy0;
+        const float spy = f[3] * ddx0 + f[4] * ddy0;
+        const float r2 = ddx0 * spx + ddy0 * spy;
+        const float r = sqrtf(fmaxf(r2, 0.0001f));
+        const float TA = T_prev * al;
+        const float dColr = dCr * TA, dColg = dCg * TA, dColb = dCb * TA;
+        const float tcr = T_prev * cr, tcg = T_prev * cg, tcb = T_prev * cb;
+        const float da_C = dT_C * (-T_prev) + (dCr * tcr + dCg * tcg + dCb * tcb);
+        const float da_D = dT_D * (-T_prev) + dD * T_prev * depth;
+        const float da = da_C + da_D;
+        const float acr = al * cr, acg = al * cg, acb = al * cb;
+        dT_C = dT_C * (1.0f - al) + (dCr * acr + dCg * acg + dCb * acb);
+        dT_D = dT_D * (1.0f - al) + dD * al * depth;
+        const float d_depth = dD * T_prev * al;
+        const float power = -shape_b * powf(r, shape_a);
+        const bool above = power > -15.0f;
+        const float a_un = above ? expf(power) : 0.0f;
+        const float d_opacity = above ? da * a_un : 0.0f;
+        const float d_power = above ? da * opacity * a_un : 0.0f;
+        const float r_pow_a = powf(r, shape_a);
+        const float r_pow_a_m2 = powf(r, shape_a - 2.0f);
+        float d_shape_a = above ? d_power * (-shape_b * r_pow_a * logf(r)) : 0.0f;
+        float d_shape_b = above ? d_power * (-r_pow_a) : 0.0f;
+        const float kk = d_power * (-shape_b * shape_a * r_pow_a_m2);
+        const float ddx = above ? kk * spx : 0.0f, ddy = above ? kk * spy : 0.0f;
+        const float dsx_ = -ddx, dsy_ = -ddy;
+        const float sp0 = spx * m0x + spy * m0y;
+        const float sp1 = spx * m1x + spy * m1y;
+        const float sp2 = spx * m2x + spy * m2y;
+        const float dm0x = -sp0 * ddx, dm0y = -sp0 * ddy;
+        const float dm1x = -sp1 * ddx, dm1y = -sp1 * ddy;
+        const float dm2x = -sp2 * ddx, dm2y = -sp2 * ddy;
+        const float daxx = dm0x * sx, daxy = dm0y * sx, dayx = dm1x * sy, dayy = dm1y * sy, dazx = dm2x * sz,
+                    dazy = dm2y * sz;
+        const float d_sx = dm0x * axx + dm0y * axy;
+        const float d_sy = dm1x * ayx + dm1y * ayy;
+        const float d_sz = dm2x * azx + dm2y * azy;
+        const float w2 = Wc * Wc;
+        float dpos[3], daw[3], dbw[3], dcw[3];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          const float vp0 = vpm[ax * 4 + 0], vp1 = vpm[ax * 4 + 1], vp3 = vpm[ax * 4 + 3];
+          const float ds_dx = aspect * (vp0 * Wc - clip_x * vp3) / w2;
+          const float ds_dy = (vp1 * Wc - clip_y * vp3) / w2;
+          dpos[ax] = dsx_ * ds_dx + dsy_ * ds_dy;
+          const float d_depth_d_w = DEPTH_NEAR / (Wc * Wc);
+          dpos[ax] += (Wc > DEPTH_NEAR) ? vp3 * d_depth_d_w * d_depth : 0.0f;
+          daw[ax] = daxx * ds_dx + daxy * ds_dy;
+          dbw[ax] = dayx * ds_dx + dayy * ds_dy;
+          dcw[ax] = dazx * ds_dx + dazy * ds_dy;
+        }
+        if (fg) {
+          dpos[0] += 0.3f * 2.0f * (pos0 - surf_x) * (T_prev * al);
+          dpos[1] += 0.3f * 2.0f * (pos1 - surf_y) * (T_prev * al);
+          dpos[2] += 0.3f * 2.0f * (pos2 - surf_z) * (T_prev * al);
+        }
+        // splat_backward.wgsl:410-426
+        const float d_qw = (daw[1] * 2.0f * qz - daw[2] * 2.0f * qy) + (-dbw[0] * 2.0f * qz + dbw[2] * 2.0f * qx) +
+                           (dcw[0] * 2.0f * qy - dcw[1] * 2.0f * qx);
+        const float d_qx = (daw[1] * 2.0f * qy + daw[2] * 2.0f * qz) +
+                           (dbw[0] * 2.0f * qy - dbw[1] * 4.0f * qx + dbw[2] * 2.0f * qw) +
+                           (dcw[0] * 2.0f * qz - dcw[1] * 2.0f * qw - dcw[2] * 4.0f * qx);
+        const float d_qy = (-daw[0] * 4.0f * qy + daw[1] * 2.0f * qx + daw[2] * (-2.0f * qw)) +
+                           (dbw[0] * 2.0f * qx + dbw[2] * 2.0f * qz) +
+                           (dcw[0] * 2.0f * qw + dcw[1] * 2.0f * qz - dcw[2] * 4.0f * qy);
+        const float d_qz = (-daw[0] * 4.0f * qz + daw[1] * 2.0f * qw + daw[2] * 2.0f * qx) +
+                           (-dbw[0] * 2.0f * qw - dbw[1] * 4.0f * qz + dbw[2] * 2.0f * qy) +
+                           (dcw[0] * 2.0f * qx + dcw[1] * 2.0f * qy);
+        d_shape_a += 0.005f * 2.0f * (shape_a - 6.0f);
+        d_shape_b += 0.005f * 2.0f * (shape_b - 0.3f);
+        q[0] = to_i32(dpos[0] * kFpPos);
+        q[1] = to_i32(dpos[1] * kFpPos);
+        q[2] = to_i32(dpos[2] * kFpPos);
+        q[3] = to_i32(d_sx * kFpPos);
+        q[4] = to_i32(dColr * kFpCol);
+        q[5] = to_i32(dColg * kFpCol);
+        q[6] = to_i32(dColb * kFpCol);
+        q[7] = to_i32(d_opacity * kFpCol);
+        q[8] = to_i32(d_qw * kFpPos);
+        q[9] = to_i32(d_qx * kFpPos);
+        q[10] = to_i32(d_qy * kFpPos);
+        q[11] = to_i32(d_qz * kFpPos);
+        q[12] = to_i32(d_sy * kFpPos);
+        q[13] = to_i32(d_shape_a * kFpPos);
+        q[14] = to_i32(d_shape_b * kFpPos);
+        q[15] = to_i32(d_sz * kFpPos);
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int32_t r = __reduce_add_sync(0xffffffffu, q[j]);
+        if (lane == 0 && r != 0) atomicAdd(&gacc[k * 16 + j], r);
+      }
+    }
+    __syncthreads();
+    for (uint32_t e = tid; e < cnt * 16; e += kThreads) {
+      const int32_t val = gacc[e];
+      if (val != 0) atomicAdd(&a.grads[16 * (size_t)ids[e >> 4] + (e & 15)], val);
+    }
+  }
+}
+
+// splat_step.wgsl:32-106, one thread per splat.
+__global__ void __launch_bounds__(256) k_step(float* __restrict__ splats, int32_t* __restrict__ grads,
+                                              float* __restrict__ am, float* __restrict__ av,
+                                              float* __restrict__ gacc, uint32_t n, float bc1, float bc2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s[16], m[16], v[16];
+  int32_t g[16];
+  float4* s4 = reinterpret_cast<float4*>(splats + 16 * (size_t)i);
+  float4* m4 = reinterpret_cast<float4*>(am + 16 * (size_t)i);
+  float4* v4 = reinterpret_cast<float4*>(av + 16 * (size_t)i);
+  int4* g4 = reinterpret_cast<int4*>(grads + 16 * (size_t)i);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 a = s4[q], b = m4[q], c = v4[q];
+    int4 d = g4[q];
+    s[4 * q] = a.x; s[4 * q + 1] = a.y; s[4 * q + 2] = a.z; s[4 * q + 3] = a.w;
+    m[4 * q] = b.x; m[4 * q + 1] = b.y; m[4 * q + 2] = b.z; m[4 * q + 3] = b.w;
+    v[4 * q] = c.x; v[4 * q + 1] = c.y; v[4 * q + 2] = c.z; v[4 * q + 3] = c.w;
+    g[4 * q] = d.x; g[4 * q + 1] = d.y; g[4 * q + 2] = d.z; g[4 * q + 3] = d.w;
+  }
+  const float B1 = 0.9f, B2 = 0.999f, EPS = 1e-8f;
+  float pos_g2 = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const float fps = (k >= 4 && k <= 7) ? kFpCol : kFpPos;
+    const float gr = (float)g[k] / fps / 16384.0f;
+    const float mm = B1 * m[k] + (1.0f - B1) * gr;
+    const float vv = B2 * v[k] + (1.0f - B2) * gr * gr;
+    m[k] = mm;
+    v[k] = vv;
+    const float m_hat = mm / bc1, v_hat = vv / bc2;
+    const float raw_u = c_lr[k] * m_hat / (sqrtf(v_hat) + EPS);
+    const float u = clampf(raw_u, -c_mu[k], c_mu[k]);
+    s[k] = clampf(s[k] - u, c_lo[k], c_hi[k]);
+    if (k <= 2) pos_g2 += gr * gr;
+  }
+  float ql = sqrtf(s[8] * s[8] + s[9] * s[9] + s[10] * s[10] + s[11] * s[11]);
+  ql = fmaxf(ql, 1e-8f);
+  s[8] = s[8] / ql; s[9] = s[9] / ql; s[10] = s[10] / ql; s[11] = s[11] / ql;
+  gacc[i] = gacc[i] + sqrtf(pos_g2);
+  const float vol = s[3] * s[12] * s[15];
+  if (s[7] < kOpacityKill || vol < kVolumeKill) s[7] = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    s4[q] = make_float4(s[4 * q], s[4 * q + 1], s[4 * q + 2], s[4 * q + 3]);
+    m4[q] = make_float4(m[4 * q], m[4 * q + 1], m[4 * q + 2], m[4 * q + 3]);
+    v4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    g4[q] = make_int4(0, 0, 0, 0);
+  }
+}
+
+constexpr int kAdcThreads = 1024;
+
+// Exclusive scan of one value per thread over a 1024-thread block.
+__device__ __forceinline__ uint32_t block_exclusive_scan_adc(uint32_t x, uint32_t* total) {
+  __shared__ uint32_t warp_sums[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_sums[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = warp_sums[lane];
+    uint32_t si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, si, o);
+      if (lane >= o) si += y;
+    }
+    warp_sums[lane] = si - s;
+    if (lane == 31) *total = si;
+  }
+  __syncthreads();
+  uint32_t r = warp_sums[wid] + inc - x;
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ float fractf(float x) { return x - floorf(x); }
+
+// splat_adc.wgsl:28-87.  One CTA.  The serial loop is reproduced window by
+// window: every splat of a 1024-wide window is classified in parallel, the
+// k-th clone candidate takes the k-th unused dead slot, and the window is
+// committed up to the first slot that a candidate fills AHEAD of itself inside
+// the window (that slot is alive, with its stale accumulator, when the serial
+// loop reaches it) — the window then restarts there.
+__global__ void __launch_bounds__(kAdcThreads) k_adc(float* __restrict__ splats, float* __restrict__ am,
+                                                     float* __restrict__ av, float* __restrict__ gacc,
+                                                     uint32_t* __restrict__ dead, uint32_t n, float adam_t,
+                                                     uint32_t* __restrict__ stats) {
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_min;
+  const uint32_t tid = threadIdx.x;
+  // dead slots at entry, ascending (the serial search order)
+  uint32_t nd = 0;
+  for (uint32_t base = 0; base < n; base += kAdcThreads) {
+    const uint32_t i = base + tid;
+    const uint32_t f = (i < n && splats[16 * (size_t)i + 7] < kOpacityKill) ? 1u : 0u;
+    const uint32_t r = block_exclusive_scan_adc(f, &s_total);
+    if (f) dead[nd + r] = i;
+    nd += s_total;
+    __syncthreads();
+  }
+  uint32_t cursor = 0, clones = 0;
+  uint32_t base = 0;
+  while (base < n) {
+    const uint32_t i = base + tid;
+    const bool inwin = i < n;
+    bool alive = false, cand = false;
+    if (inwin) {
+      const float op = splats[16 * (size_t)i + 7];
+      alive = !(op < kOpacityKill);
+      cand = alive && (gacc[i] / kAdcPeriod > kGradThresh);
+    }
+    const uint32_t r = block_exclusive_scan_adc(cand ? 1u : 0u, &s_total);
+    const bool has_slot = cand && (cursor + r < nd);
+    const uint32_t d = has_slot ? dead[cursor + r] : 0u;
+    if (tid == 0) s_min = 0xffffffffu;
+    __syncthreads();
+    if (has_slot && d > i && d < base + kAdcThreads) atomicMin(&s_min, d);
+    __syncthreads();
+    const uint32_t commit_end = s_min == 0xffffffffu ? base + kAdcThreads : s_min;
+    const bool commit = inwin && i < commit_end;
+    if (commit && alive) gacc[i] = 0.0f;
+    if (commit && has_slot) {
+      float s[16], ns[16];
+      float4* s4 = reinterpret_cast<float4*>(splats + 16 * (size_t)i);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 t = s4[q];
+        s[4 * q] = t.x; s[4 * q + 1] = t.y; s[4 * q + 2] = t.z; s[4 * q + 3] = t.w;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) ns[k] = s[k];
+      const float scale_norm = sqrtf(s[3] * s[3] + s[12] * s[12] + s[15] * s[15]);
+      if (scale_norm > 0.01f) {
+        const float fct = 0.625f;
+        s[3] *= fct; s[12] *= fct; s[15] *= fct;
+        ns[3] *= fct; ns[12] *= fct; ns[15] *= fct;
+        s[0] -= s[3] * 0.05f;
+        ns[0] += s[3] * 0.05f;
+      } else {
+        const float seed = (float)i * 3.14159f + adam_t;
+        ns[0] += (fractf(sinf(seed * 12.9898f) * 43758.5453f) - 0.5f) * 0.002f;
+        ns[1] += (fractf(sinf(seed * 78.233f) * 43758.5453f) - 0.5f) * 0.002f;
+      }
+      float4* d4 = reinterpret_cast<float4*>(splats + 16 * (size_t)d);
+      float4* mi = reinterpret_cast<float4*>(am + 16 * (size_t)i);
+      float4* vi = reinterpret_cast<float4*>(av + 16 * (size_t)i);
+      float4* md = reinterpret_cast<float4*>(am + 16 * (size_t)d);
+      float4* vd = reinterpret_cast<float4*>(av + 16 * (size_t)d);
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        s4[q] = make_float4(s[4 * q], s[4 * q + 1], s[4 * q + 2], s[4 * q + 3]);
+        d4[q] = make_float4(ns[4 * q], ns[4 * q + 1], ns[4 * q + 2], ns[4 * q + 3]);
+        mi[q] = z; vi[q] = z; md[q] = z; vd[q] = z;
+      }
+    }
+    const uint32_t used = __syncthreads_count(commit && has_slot);
+    cursor += used;
+    clones += used;
+    __threadfence_block();
+    __syncthreads();
+    base = commit_end;
+  }
+  if (tid == 0 && stats) stats[0] = clones;
+}
+
+}  // namespace compat
+}  // namespace nps
+
+// =================================================================== host side
+using namespace nps;
+
+struct nps_splat_opt {
+  nps_ctx* ctx = nullptr;
+  uint32_t n = 0;
+  DevBuf params, grads, am, av, gacc;
+  float adam_t = 0.0f;
+  uint32_t step_count = 0;
+  // cameras
+  uint32_t nv = 0;
+  DevBuf views;  // nv * 32 floats: vp, vp_inv
+  // targets
+  uint32_t w = 0, h = 0, tv = 0;
+  DevBuf tgt_rgba_own, tgt_depth_own;
+  const float* tgt_rgba = nullptr;
+  const float* tgt_depth = nullptr;
+  // work
+  DevBuf fwd, bwd, counts, offsets, rects, total, keys, vals, ranges, tabs, dead, stat;
+  SortWork sw;
+  uint32_t pair_cap = 0;
+  nps_stats stats{};
+};
+
+namespace {
+
+int copy_in(void* dst, const void* src, size_t bytes, int mem, cudaStream_t s) {
+  if (bytes == 0) return NPS_OK;
+  if (!src) {
+    set_error("null source pointer");
+    return NPS_ERR_INVALID;
+  }
+  if (mem == NPS_MEM_HOST) {
+    NPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaStreamSynchronize(s));  // host buffer may be reused on return
+  } else {
+    NPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  return NPS_OK;
+}
+
+int check_opt(nps_splat_opt* o) {
+  if (!o) {
+    set_error("null splat optimizer");
+    return NPS_ERR_INVALID;
+  }
+  return bind_device(o->ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int nps_splat_opt_create(nps_ctx* ctx, uint32_t num_splats, nps_splat_opt** out) {
+  if (!out || num_splats == 0 || num_splats > (1u << 26)) {
+    set_error("nps_splat_opt_create: bad arguments (num_splats=%u)", num_splats);
+    return NPS_ERR_INVALID;
+  }
+  *out = nullptr;
+  NPS_TRY(bind_device(ctx));
+  nps_splat_opt* o = new nps_splat_opt();
+  o->ctx = ctx;
+  o->n = num_splats;
+  const size_t p16 = sizeof(float) * 16 * (size_t)num_splats;
+  int rc = NPS_OK;
+  if ((rc = o->params.ensure(p16)) || (rc = o->grads.ensure(p16)) || (rc = o->am.ensure(p16)) ||
+      (rc = o->av.ensure(p16)) || (rc = o->gacc.ensure(sizeof(float) * num_splats)) ||
+      (rc = o->dead.ensure(sizeof(uint32_t) * num_splats)) || (rc = o->stat.ensure(64)) ||
+      (rc = o->total.ensure(sizeof(uint32_t) * 4))) {
+    delete o;
+    return rc;
+  }
+  cudaStream_t s = ctx->stream;
+  cudaMemsetAsync(o->params.p, 0, p16, s);
+  cudaMemsetAsync(o->grads.p, 0, p16, s);
+  cudaMemsetAsync(o->am.p, 0, p16, s);
+  cudaMemsetAsync(o->av.p, 0, p16, s);
+  cudaMemsetAsync(o->gacc.p, 0, sizeof(float) * num_splats, s);
+  cudaMemsetAsync(o->stat.p, 0, 64, s);
+  NPS_CUDA(cudaGetLastError());
+  *out = o;
+  return NPS_OK;
+}
+
+int nps_splat_opt_destroy(nps_splat_opt* o) {
+  if (!o) return NPS_OK;
+  cudaSetDevice(o->ctx->device);
+  cudaStreamSynchronize(o->ctx->stream);
+  for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->views, &o->tgt_rgba_own,
+                    &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->offsets, &o->rects, &o->total,
+                    &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->sw.hist, &o->sw.partial,
+                    &o->sw.keys_alt, &o->sw.vals_alt})
+    b->release();
+  delete o;
+  return NPS_OK;
+}
+
+int nps_splat_opt_write_params(nps_splat_opt* o, const float* splats, uint32_t first, uint32_t count, int mem) {
+  NPS_TRY(check_opt(o));
+  if ((uint64_t)first + count > o->n) {
+    set_error("write_params: range [%u, %u) beyond %u splats", first, first + count, o->n);
+    return NPS_ERR_INVALID;
+  }
+  return copy_in(o->params.as<float>() + 16 * (size_t)first, splats, sizeof(float) * 16 * (size_t)count, mem,
+                 o->ctx->stream);
+}
+
+int nps_splat_opt_write_state(nps_splat_opt* o, const int32_t* grads, const float* m, const float* v, float t,
+                              const float* gacc, int mem) {
+  NPS_TRY(check_opt(o));
+  const size_t p16 = sizeof(float) * 16 * (size_t)o->n;
+  if (grads) NPS_TRY(copy_in(o->grads.p, grads, p16, mem, o->ctx->stream));
+  if (m) NPS_TRY(copy_in(o->am.p, m, p16, mem, o->ctx->stream));
+  if (v) NPS_TRY(copy_in(o->av.p, v, p16, mem, o->ctx->stream));
+  if (gacc) NPS_TRY(copy_in(o->gacc.p, gacc, sizeof(float) * o->n, mem, o->ctx->stream));
+  o->adam_t = t;
+  return NPS_OK;
+}
+
+int nps_splat_opt_read_state(nps_splat_opt* o, float* splats, int32_t* grads, float* m, float* v, float* t,
+                             float* gacc) {
+  NPS_TRY(check_opt(o));
+  cudaStream_t s = o->ctx->stream;
+  const size_t p16 = sizeof(float) * 16 * (size_t)o->n;
+  if (splats) NPS_CUDA(cudaMemcpyAsync(splats, o->params.p, p16, cudaMemcpyDeviceToHost, s));
+  if (grads) NPS_CUDA(cudaMemcpyAsync(grads, o->grads.p, p16, cudaMemcpyDeviceToHost, s));
+  if (m) NPS_CUDA(cudaMemcpyAsync(m, o->am.p, p16, cudaMemcpyDeviceToHost, s));
+  if (v) NPS_CUDA(cudaMemcpyAsync(v, o->av.p, p16, cudaMemcpyDeviceToHost, s));
+  if (gacc) NPS_CUDA(cudaMemcpyAsync(gacc, o->gacc.p, sizeof(float) * o->n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  if (t) *t = o->adam_t;
+  return NPS_OK;
+}
+
+int nps_splat_opt_write_vp(nps_splat_opt* o, const float* vp, const float* vp_inv, uint32_t num_views, int blur) {
+  (void)blur;
+  NPS_TRY(check_opt(o));
+  if (!vp || !vp_inv || num_views == 0 || num_views > 4096) {
+    set_error("write_vp: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  std::vector<float> host(32 * (size_t)num_views);
+  for (uint32_t v = 0; v < num_views; ++v) {
+    std::memcpy(&host[32 * v], vp + 16 * v, 64);
+    std::memcpy(&host[32 * v + 16], vp_inv + 16 * v, 64);
+  }
+  NPS_TRY(o->views.ensure(sizeof(float) * host.size()));
+  o->nv = num_views;
+  return copy_in(o->views.p, host.data(), sizeof(float) * host.size(), NPS_MEM_HOST, o->ctx->stream);
+}
+
+int nps_splat_opt_set_target(nps_splat_opt* o, const float* rgba, const float* depth, uint32_t w, uint32_t h,
+                             uint32_t nv, int mem) {
+  NPS_TRY(check_opt(o));
+  if (!rgba || !depth || w == 0 || h == 0 || nv == 0 || w > 16 * 65535 || h > 16 * 65535) {
+    set_error("set_target: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  const size_t px = (size_t)w * h * nv;
+  if (mem == NPS_MEM_DEVICE_BORROW) {
+    if (((uintptr_t)rgba & 15) != 0) {
+      set_error("set_target: borrowed rgba must be 16-byte aligned");
+      return NPS_ERR_INVALID;
+    }
+    o->tgt_rgba = rgba;
+    o->tgt_depth = depth;
+  } else {
+    NPS_TRY(o->tgt_rgba_own.ensure(sizeof(float) * 4 * px));
+    NPS_TRY(o->tgt_depth_own.ensure(sizeof(float) * px));
+    NPS_TRY(copy_in(o->tgt_rgba_own.p, rgba, sizeof(float) * 4 * px, mem, o->ctx->stream));
+    NPS_TRY(copy_in(o->tgt_depth_own.p, depth, sizeof(float) * px, mem, o->ctx->stream));
+    o->tgt_rgba = o->tgt_rgba_own.as<float>();
+    o->tgt_depth = o->tgt_depth_own.as<float>();
+  }
+  o->w = w;
+  o->h = h;
+  o->tv = nv;
+  const uint32_t tx = div_up(w, 16), ty = div_up(h, 16);
+  NPS_TRY(o->tabs.ensure(sizeof(float) * 2 * (tx + ty)));
+  compat::k_tile_tables<<<1, 256, 0, o->ctx->stream>>>(o->tabs.as<float>(), tx, ty, w, h);
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
+int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
+  NPS_TRY(check_opt(o));
+  if (!o->tgt_rgba || o->nv == 0) {
+    set_error("backward: set_target and write_vp first");
+    return NPS_ERR_STATE;
+  }
+  if (o->tv != o->nv) {
+    set_error("backward: %u target views but %u cameras", o->tv, o->nv);
+    return NPS_ERR_STATE;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n, nv = o->nv;
+  const uint32_t tiles_x = div_up(o->w, 16), tiles_y = div_up(o->h, 16), num_tiles = tiles_x * tiles_y;
+  const size_t g = (size_t)n * nv;
+  if (g >= (1ull << 31) || (uint64_t)num_tiles * nv >= (1ull << 31)) {
+    set_error("backward: problem too large");
+    return NPS_ERR_INVALID;
+  }
+  NPS_TRY(o->fwd.ensure(sizeof(float) * compat::kFwd * g));
+  NPS_TRY(o->bwd.ensure(sizeof(float) * compat::kBwd * g));
+  NPS_TRY(o->counts.ensure(sizeof(uint32_t) * g));
+  NPS_TRY(o->offsets.ensure(sizeof(uint32_t) * g));
+  NPS_TRY(o->rects.ensure(sizeof(uint2) * g));
+  NPS_TRY(o->ranges.ensure(sizeof(uint32_t) * 2 * (size_t)num_tiles * nv));
+  compat::k_project<<<div_up(g, 256), 256, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, o->w, o->h,
+                                                    o->tabs.as<float>(), tiles_x, tiles_y, o->fwd.as<float>(),
+                                                    o->bwd.as<float>(), o->counts.as<uint32_t>(),
+                                                    o->rects.as<uint2>());
+  NPS_CHECK_LAUNCH();
+  uint32_t* total = o->total.as<uint32_t>();
+  NPS_TRY(exclusive_scan_u32(o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)g, total, o->sw, s));
+  uint32_t K = 0;
+  NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  if (K > o->pair_cap) {
+    uint32_t cap = K + K / 4 + 4096;
+    NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
+    NPS_TRY(o->vals.ensure(sizeof(uint32_t) * (size_t)cap));
+    o->pair_cap = cap;
+  }
+  NPS_CUDA(cudaMemsetAsync(o->ranges.p, 0, sizeof(uint32_t) * 2 * (size_t)num_tiles * nv, s));
+  uint32_t* rstart = o->ranges.as<uint32_t>();
+  uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  if (K > 0) {
+    compat::k_emit<<<div_up(g, 256), 256, 0, s>>>(o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(),
+                                                   o->rects.as<uint2>(), n, nv, tiles_x, num_tiles, o->pair_cap,
+                                                   o->keys.as<uint32_t>(), o->vals.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+    int bits = 1;
+    while ((1ull << bits) < (uint64_t)num_tiles * nv) ++bits;
+    uint32_t *ks = nullptr, *vs = nullptr;
+    NPS_TRY(radix_sort_u32(o->keys.as<uint32_t>(), o->vals.as<uint32_t>(), total, o->pair_cap, bits, o->sw, s, &ks,
+                           &vs));
+    compat::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, o->pair_cap, rstart, rend);
+    NPS_CHECK_LAUNCH();
+    compat::RasterArgs ra;
+    ra.fwd = o->fwd.as<float>();
+    ra.bwd = o->bwd.as<float>();
+    ra.vals = vs;
+    ra.rstart = rstart;
+    ra.rend = rend;
+    ra.views = o->views.as<float>();
+    ra.tgt_rgba = o->tgt_rgba;
+    ra.tgt_depth = o->tgt_depth;
+    ra.grads = o->grads.as<int32_t>();
+    ra.out_rgbd = out_rgbd;
+    ra.n = n;
+    ra.w = o->w;
+    ra.h = o->h;
+    ra.tiles_x = tiles_x;
+    ra.num_tiles = num_tiles;
+    static bool attr_set = false;
+    if (!attr_set) {
+      NPS_CUDA(cudaFuncSetAttribute(compat::k_raster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)compat::kRasterSmem));
+      attr_set = true;
+    }
+    compat::k_raster<<<dim3(tiles_x, tiles_y, nv), compat::kThreads, compat::kRasterSmem, s>>>(ra);
+    NPS_CHECK_LAUNCH();
+  } else {
+    // no pairs: every pixel is background; the backward still writes the image
+    compat::RasterArgs ra{};
+    ra.fwd = o->fwd.as<float>();
+    ra.bwd = o->bwd.as<float>();
+    ra.vals = o->counts.as<uint32_t>();
+    ra.rstart = rstart;
+    ra.rend = rend;
+    ra.views = o->views.as<float>();
+    ra.tgt_rgba = o->tgt_rgba;
+    ra.tgt_depth = o->tgt_depth;
+    ra.grads = o->grads.as<int32_t>();
+    ra.out_rgbd = out_rgbd;
+    ra.n = n;
+    ra.w = o->w;
+    ra.h = o->h;
+    ra.tiles_x = tiles_x;
+    ra.num_tiles = num_tiles;
+    NPS_CUDA(cudaFuncSetAttribute(compat::k_raster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)compat::kRasterSmem));
+    compat::k_raster<<<dim3(tiles_x, tiles_y, nv), compat::kThreads, compat::kRasterSmem, s>>>(ra);
+    NPS_CHECK_LAUNCH();
+  }
+  o->stats.pairs = K;
+  return NPS_OK;
+}
+
+int nps_splat_opt_step(nps_splat_opt* o) {
+  NPS_TRY(check_opt(o));
+  const float t = o->adam_t + 1.0f;
+  // 1 - pow(beta, t) in f32, as splat_step.wgsl:71-72 evaluates it
+  const float bc1 = 1.0f - std::pow(0.9f, t), bc2 = 1.0f - std::pow(0.999f, t);
+  compat::k_step<<<div_up(o->n, 256), 256, 0, o->ctx->stream>>>(o->params.as<float>(), o->grads.as<int32_t>(),
+                                                                 o->am.as<float>(), o->av.as<float>(),
+                                                                 o->gacc.as<float>(), o->n, bc1, bc2);
+  NPS_CHECK_LAUNCH();
+  o->adam_t = t;
+  return NPS_OK;
+}
+
+int nps_splat_opt_adc(nps_splat_opt* o) {
+  NPS_TRY(check_opt(o));
+  compat::k_adc<<<1, compat::kAdcThreads, 0, o->ctx->stream>>>(o->params.as<float>(), o->am.as<float>(),
+                                                                o->av.as<float>(), o->gacc.as<float>(),
+                                                                o->dead.as<uint32_t>(), o->n, o->adam_t,
+                                                                o->stat.as<uint32_t>());
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
+int nps_splat_opt_dispatch(nps_splat_opt* o) {
+  NPS_TRY(nps_splat_opt_backward(o, nullptr));
+  NPS_TRY(nps_splat_opt_step(o));
+  o->step_count++;
+  if (o->step_count % 25 == 0) NPS_TRY(nps_splat_opt_adc(o));  // GpuSplatOptimizerManager.ts:380-385
+  return NPS_OK;
+}
+
+int nps_splat_opt_buffers(nps_splat_opt* o, float** splats, int32_t** grads, float** m, float** v, float** gacc) {
+  NPS_TRY(check_opt(o));
+  if (splats) *splats = o->params.as<float>();
+  if (grads) *grads = o->grads.as<int32_t>();
+  if (m) *m = o->am.as<float>();
+  if (v) *v = o->av.as<float>();
+  if (gacc) *gacc = o->gacc.as<float>();
+  return NPS_OK;
+}
+
+int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
+  NPS_TRY(check_opt(o));
+  if (!out) return NPS_ERR_INVALID;
+  uint32_t clones = 0;
+  NPS_CUDA(cudaMemcpyAsync(&clones, o->stat.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, o->ctx->stream));
+  NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  o->stats.adc_clones = clones;
+  o->stats.step_count = o->step_count;
+  *out = o->stats;
+  return NPS_OK;
+}
+
+int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
+                         float* out_depth) {
+  (void)vp; (void)w; (void)h; (void)out_rgba; (void)out_depth;
+  NPS_TRY(check_opt(o));
+  set_error("render: not implemented yet");
+  return NPS_ERR_STATE;
+}
+
+}  // extern "C"
