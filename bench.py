@@ -1,11 +1,18 @@
-"""Benchmark: train steps/s of the splat trainer on B200.
+"""Benchmark: train steps/s (fwd + bwd + Adam, 200k Gaussians SH3, 800x800,
+8 views per step) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path compat]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path gs|compat]
 
-Prints ONE JSON line (rank 0).  A step is one full training iteration over
-the step's views (forward + loss + backward + Adam) on synthetic, seeded
-inputs of the workload's shapes.  See DESIGN.md for the workload, the
-algorithmic-byte model behind `roofline` and the CPU baseline.
+Prints ONE JSON line (rank 0).  A step is one full training iteration over 8
+of 32 sphere cameras (forward + L1/D-SSIM loss + backward + Adam) on seeded
+synthetic inputs: a 200k-Gaussian student fitted to images rendered from a
+250k-Gaussian teacher.  `value` is timed with CUDA events on the library's
+stream with everything resident in HBM; `e2e` goes through the public API with
+the step's target images copied from pinned host memory and the loss read
+back every step.  `--impl reference` times the reference's own shader code
+for this path (translated to C++, oracle/_ref) on the host, on a bounded
+sample of the same shape.  Multi-GPU runs are independent replicas (weak
+scaling, no collective).
 """
 from __future__ import annotations
 
@@ -23,28 +30,27 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 800, 8, 32, 3
+P_USED = 59          # floats per Gaussian used by the model
+S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, opacity)
 
 
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return d, "measured"
-    return PEAKS_FALLBACK, "fallback"
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-# ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
-        self.index = index
-        self.proc = None
+        self.index, self.proc, self.lines = index, None, []
 
     def __enter__(self):
         try:
@@ -53,12 +59,12 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
-        self.lines = []
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.2)
             self.proc.terminate()
             try:
                 out, _ = self.proc.communicate(timeout=5)
@@ -86,17 +92,164 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ----------------------------------------------------------- workloads
-def config2_cameras(n_cams=32, w=800, h=800, fov_deg=50.0, radius=4.0):
-    from nprush_b200.camera import sphere_cameras
-    return sphere_cameras(n_cams, radius, math.radians(fov_deg), w / h)
+def stage_bytes(stage: str, V: int, N: int, K: int, npx: int, tile_passes: int) -> float:
+    """Algorithmic (compulsory) bytes of one launch of a stage of the step."""
+    return {
+        "preprocess": V * N * (P_USED * 4 + S_REC + 20),
+        "depth_sort": 4 * 16 * V * N,
+        "emit": V * N * 16 + K * 8,
+        "tile_sort": tile_passes * 16 * K,
+        "ranges": K * 4 + 8 * V * npx / 256,
+        "raster_fwd": K * (4 + S_REC) + V * npx * (12 + 8),
+        "loss": V * npx * (12 + 12 + 12),
+        "raster_bwd": K * (4 + S_REC) + V * npx * (12 + 8 + 12) + V * N * 40,
+        "project_bwd": V * N * (40 + S_REC) + 2 * N * P_USED * 4,
+        "adam": N * P_USED * 4 * 7,
+    }[stage]
 
 
-def compat_scene(n, seed):
-    """Config-2 distribution in the reference's 16-float record: means U[-1,1]^3,
-    scales exp(N(-4, 0.5)), random unit quaternions, opacity sigmoid(N(0,1)),
-    RGB U[0,1], Gaussian shape (a=2, b=0.5)."""
-    rng = np.random.default_rng(seed)
+def step_bytes(V, N, K, npx):
+    """Whole-step compulsory bytes (forward + backward + Adam)."""
+    fwd = V * N * P_USED * 4 + V * N * S_REC + K * 8 + K * (8 + S_REC) + V * npx * 12
+    bwd = K * (8 + S_REC) + V * npx * (12 + 8) + V * N * S_REC + V * N * (S_REC + P_USED * 4) + N * P_USED * 4
+    return fwd + bwd + N * P_USED * 4 * 7
+
+
+# ----------------------------------------------------------------- our arm
+def build_scene(dev):
+    import torch
+
+    from nprush_b200.gaussians import GaussianTrainer, config2_cameras, random_gaussians
+    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    teacher = GaussianTrainer(N_TEACHER, sh_degree=SH_DEG, device=dev, params=random_gaussians(N_TEACHER, 11))
+    tg = torch.zeros((CAMS, HEIGHT, WIDTH, 4), device=f"cuda:{dev}")
+    for c0 in range(0, CAMS, VIEWS):
+        teacher.set_views(vp[c0:c0 + VIEWS], vpi[c0:c0 + VIEWS])
+        teacher.forward(out=tg[c0:c0 + VIEWS])
+    teacher.close()
+    tg[..., 3] = 1.0
+    student = GaussianTrainer(N_GAUSS, sh_degree=SH_DEG, device=dev, params=random_gaussians(N_GAUSS, 10))
+    return vp, vpi, tg, student
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    from nprush_b200 import _lib
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = _lib.context(dev)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        vp, vpi, tg, st = build_scene(dev)
+        torch.cuda.synchronize()
+        st.set_targets(tg, borrow=True)
+        rng = np.random.default_rng(1234)
+        sched = [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(args.warmup + args.steps + 4)]
+        flush = torch.empty(64 * 1024 * 1024, device=f"cuda:{dev}")  # 256 MB > L2
+
+        def step(k):
+            sel = sched[k]
+            st.set_views(vp[sel], vpi[sel], sel)
+            st.train_step()
+
+        for k in range(args.warmup):
+            step(k)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        st.set_timing(True)
+        st.stage_times(reset=True)
+        times, pairs = [], []
+        with ClockSampler(dev) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step(args.warmup + k)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                pairs.append(st.stats()["pairs"])
+        stages = st.stage_times(reset=True)
+        st.set_timing(False)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        # ---- end to end through the public API with host buffers
+        pinned = torch.empty((VIEWS, HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
+        host_all = tg.cpu()
+        e2e_times = []
+        loss_last = None
+        for k in range(args.steps + 1):
+            sel = sched[k]
+            pinned.copy_(host_all[torch.as_tensor(sel)])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st.set_targets(pinned.numpy())                  # H2D of the step's inputs
+            st.set_views(vp[sel], vpi[sel], np.arange(VIEWS))
+            loss_last = st.train_step(read_loss=True)        # D2H of the loss
+            dt = time.perf_counter() - t0
+            if k > 0:
+                e2e_times.append(dt * 1000.0)
+        h2d = VIEWS * HEIGHT * WIDTH * 4 * 4 + VIEWS * (32 * 4 + 4)
+        d2h = 3 * 4
+    return dict(ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
+                clocks=clk.summary(), e2e_ms=float(np.mean(e2e_times)), h2d=h2d, d2h=d2h, loss=loss_last)
+
+
+def cpu_baseline_port():
+    """The oracle port of the same step on the host: one view of the workload
+    (forward + loss + backward), plus Adam over all Gaussians, extrapolated to
+    the 8-view step."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc  # checker / baseline only
+
+    from nprush_b200.gaussians import config2_cameras, random_gaussians, view_records
+    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    views = view_records(vp[:1], vpi[:1])
+    teacher = random_gaussians(N_TEACHER, 11)
+    timg, _ = orc.gs_forward(teacher, SH_DEG, views, WIDTH, HEIGHT)
+    tg = timg.copy()
+    tg[..., 3] = 1.0
+    p = random_gaussians(N_GAUSS, 10)
+    t0 = time.perf_counter()
+    img, nc = orc.gs_forward(p, SH_DEG, views, WIDTH, HEIGHT)
+    l3, dimg = orc.gs_loss(img, tg, np.zeros(1, np.uint32))
+    g = orc.gs_backward(p, SH_DEG, views, WIDTH, HEIGHT, img, nc, dimg)
+    t_view = time.perf_counter() - t0
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    t0 = time.perf_counter()
+    orc.gs_adam(p, g, m, v, 1, (1.6e-4, 5e-3, 1e-3, 5e-2, 2.5e-3, 1.25e-4))
+    t_adam = time.perf_counter() - t0
+    step_s = VIEWS * t_view + t_adam
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 of 8 views of one step (fwd+loss+bwd {t_view:.2f} s) + Adam over all {N_GAUSS} "
+                      f"Gaussians ({t_adam:.2f} s), extrapolated x8 views; fp32 C++ oracle, OpenMP"}
+
+
+# ----------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's own splat_backward.wgsl + splat_step.wgsl (translated to
+    C++ and compiled for the host, oracle/_ref) at this workload's shape:
+    200k splats, 800x800, 8 views per step.  Each timed sample runs a few
+    16x16 workgroups (tiles) of one view; the step time is extrapolated by the
+    tile count and view count, plus one full splat_step dispatch."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import build_ref
+
+    from nprush_b200.gaussians import config2_cameras
+    n = N_GAUSS
+    so = sorted((ROOT / "oracle" / "_ref").glob(f"splat_backward_n{n}_*.so"))
+    so_step = sorted((ROOT / "oracle" / "_ref").glob(f"splat_step_n{n}_*.so"))
+    if not so or not so_step:
+        if not build_ref.reference_available():
+            return {"impl": "reference", "unavailable": "oracle/_ref for 200k splats was not built (no reference checkout)"}
+    mod_b = build_ref.RefModule.from_path(so[-1]) if so else build_ref.RefModule("splat_backward", n)
+    mod_s = build_ref.RefModule.from_path(so_step[-1]) if so_step else build_ref.RefModule("splat_step", n)
+    rng = np.random.default_rng(10)
     s = np.zeros((n, 16), np.float32)
     s[:, 0:3] = rng.uniform(-1, 1, (n, 3))
     sc = np.exp(rng.normal(-4.0, 0.5, (n, 3)))
@@ -106,76 +259,60 @@ def compat_scene(n, seed):
     q = rng.normal(size=(n, 4))
     s[:, 8:12] = q / np.linalg.norm(q, axis=1, keepdims=True)
     s[:, 13], s[:, 14] = 2.0, 0.5
-    return s
+    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    tgt = np.zeros((HEIGHT, WIDTH, 4), np.float32)
+    tgt[..., :3] = rng.random((HEIGHT, WIDTH, 3))
+    dep = np.zeros((HEIGHT, WIDTH, 4), np.float32)
+    dep[..., 0] = np.where(rng.random((HEIGHT, WIDTH)) < 0.5, 0.97, 1.0)
+    grads = np.zeros(n * 16, np.int32)
+    uni = np.zeros(40, np.float32)
+    uni[0:16], uni[16:32] = vp[0], vpi[0]
+    mod_b.bind(0, s)
+    mod_b.bind(1, grads)
+    mod_b.bind_tex(2, tgt)
+    mod_b.bind_tex(3, dep)
+    mod_b.bind(4, uni)
+    gx, gy = (WIDTH + 15) // 16, (HEIGHT + 15) // 16
+    # tiles spread over the image (the centre tiles are the busiest)
+    tiles = [(gx // 2 + dx, gy // 2 + dy) for dx, dy in ((0, 0), (-8, 3), (9, -6), (-17, -14), (15, 16), (-3, 20))]
+    per_step = []
+    for k in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        for (tx, ty) in tiles:
+            mod_b.run_one(tx, ty, 0, gx, gy, 1)
+        t_tiles = (time.perf_counter() - t0) / len(tiles)
+        per_step.append(t_tiles)
+    adam = np.zeros(32 * n + 8, np.float32)
+    acc = np.zeros(n, np.float32)
+    mod_s.bind(0, s)
+    mod_s.bind(1, grads)
+    mod_s.bind(2, adam)
+    mod_s.bind(3, acc)
+    t0 = time.perf_counter()
+    mod_s.dispatch((n + 63) // 64, 1, 1)
+    t_step = time.perf_counter() - t0
+    t_tile = float(np.median(per_step))
+    step_s = t_tile * gx * gy * VIEWS + t_step
+    v = 1.0 / step_s
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "higher_is_better": True,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "reference splat_backward + splat_step (its own WGSL, translated to C++) at the "
+                                   "config-2 shape: 200k splats, 800x800, 8 views per step"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "reference",
+                             "sample": f"{len(tiles)} of {gx * gy} tiles of one view per timed sample "
+                                       f"({t_tile * 1000:.0f} ms per tile), extrapolated x{gx * gy} tiles x{VIEWS} "
+                                       f"views + one full splat_step ({t_step:.2f} s); single host thread"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def run_compat(args, rank, world):
-    """Reference-semantics trainer at the config-2 shape (200k splats, 800^2,
-    8 of 32 views per step)."""
-    import torch
+METRIC = "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)"
 
-    from nprush_b200 import _lib
-    from nprush_b200.splat import GpuSplatOptimizerManager
 
-    dev = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(dev)
-    n, w, h, vps = 200_000, 800, 800, 8
-    vp, vpi = config2_cameras()
-    stream = torch.cuda.Stream(dev)
-    ctx = _lib.context(dev)
-    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
-    # teacher renders the targets for all 32 cameras
-    teacher = GpuSplatOptimizerManager(250_000, device=dev, init=compat_scene(250_000, 11 + 1000 * rank))
-    tg = torch.zeros((32, h, w, 4), device=f"cuda:{dev}")
-    zero_t = torch.zeros((32, h, w, 4), device=f"cuda:{dev}")
-    zero_d = torch.ones((32, h, w), device=f"cuda:{dev}")
-    for c0 in range(0, 32, 8):
-        teacher.write_splat_vp_matrix(vp[c0:c0 + 8], vpi[c0:c0 + 8])
-        teacher.set_backward_target(zero_t[c0:c0 + 8], zero_d[c0:c0 + 8], w, h)
-        teacher.backward(out_rgbd=tg[c0:c0 + 8])
-    teacher.close()
-    del zero_t, zero_d
-    tgt_rgba = tg.clone()
-    tgt_rgba[..., 3] = 1.0
-    tgt_depth = tg[..., 3].contiguous()
-    del tg
-    student = GpuSplatOptimizerManager(n, device=dev, init=compat_scene(n, 10 + 1000 * rank))
-    perm_rng = np.random.default_rng(1234 + rank)
-
-    def views_for(step):
-        perm = perm_rng.permutation(32)
-        return np.sort(perm[:vps])
-
-    flush = torch.empty(256 * 1024 * 1024 // 4, device=f"cuda:{dev}")
-
-    def one_step(step):
-        sel = views_for(step)
-        student.write_splat_vp_matrix(vp[sel], vpi[sel])
-        idx = torch.as_tensor(sel, device=f"cuda:{dev}")
-        student.set_backward_target(tgt_rgba.index_select(0, idx), tgt_depth.index_select(0, idx), w, h)
-        student.dispatch()
-
-    with torch.cuda.stream(stream):
-        for s in range(args.warmup):
-            one_step(s)
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
-        times = []
-        with ClockSampler(dev) as clk:
-            for s in range(args.steps):
-                flush.zero_()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                one_step(args.warmup + s)
-                e1.record(stream)
-                e1.synchronize()
-                times.append(e0.elapsed_time(e1))
-        torch.cuda.synchronize()
-    ms = float(np.sum(times))
-    st = student.stats()
-    return dict(ms_total=ms, times=times, clocks=clk.summary(), pairs=st["pairs"], n=n, w=w, h=h, views=vps)
+def launches_per_step(tile_passes: int) -> int:
+    # preprocess, set count, depth sort (4 passes x 3), gather, scan (3), emit,
+    # tile sort (passes x 3), ranges, forward, ssim fwd / bwd / reduce,
+    # backward, projection backward, Adam
+    return 1 + 1 + 12 + 1 + 3 + 1 + 3 * tile_passes + 1 + 1 + 3 + 1 + 1 + 1
 
 
 def main():
@@ -184,22 +321,21 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--path", default="compat", choices=["compat"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
     if world > 1:
         import datetime
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.impl == "reference":
-        if rank == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "CPU reference leg not wired yet"}))
-        return
-    res = run_compat(args, rank, world)
+    res = run_ours(args, rank, world)
     ms = res["ms_total"]
     if world > 1:
         import torch
@@ -207,20 +343,43 @@ def main():
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     ms_per_step = ms / args.steps
     value = world * 1000.0 / ms_per_step
-    if rank == 0:
-        line = {
-            "metric": "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)",
-            "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded, teacher-rendered targets)",
-            "config": {"workload": "reference-semantics splat trainer at the config-2 shape", "splats": res["n"],
-                       "resolution": [res["w"], res["h"]], "views_per_step": res["views"],
-                       "l2": "flushed between steps", "pairs_last_step": res["pairs"]},
-            "clocks": res["clocks"],
-        }
-        print(json.dumps(line))
+    pk, pk_kind = peaks()
+    npx = WIDTH * HEIGHT
+    K = res["pairs"]
+    tile_passes = int(math.ceil(math.ceil(math.log2(VIEWS * ((WIDTH + 15) // 16) * ((HEIGHT + 15) // 16))) / 8))
+    st = res["stages"]
+    dom = max(st, key=lambda k: st[k][0])
+    dom_ms = st[dom][0] / max(st[dom][1], 1)
+    achieved = stage_bytes(dom, VIEWS, N_GAUSS, K, npx, tile_passes) / (dom_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded 200k-Gaussian student, targets rendered from a seeded 250k-Gaussian teacher",
+        "config": {"workload": "config 2: 200k Gaussians SH3, 800x800, 8 of 32 sphere cameras per step, "
+                               "L1 + 0.2 D-SSIM, Adam", "gaussians": N_GAUSS, "resolution": [WIDTH, HEIGHT],
+                   "views_per_step": VIEWS, "l2": "flushed between timed steps (256 MB write)",
+                   "pairs_per_step": K, "parallelism": "replicas" if world > 1 else "single GPU"},
+        "clocks": res["clocks"],
+        "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
+                "d2h_bytes_per_step": res["d2h"]},
+        "gpu_launches": launches_per_step(tile_passes) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_kind": pk_kind,
+                     "step_algorithmic_bytes": step_bytes(VIEWS, N_GAUSS, K, npx),
+                     "step_frac": step_bytes(VIEWS, N_GAUSS, K, npx) / (ms_per_step * 1e-3) / 1e9 / pk["hbm_gbs"]},
+        "stages_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in st.items()},
+        "final_loss": res["loss"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port()
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

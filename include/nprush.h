@@ -117,6 +117,57 @@ typedef struct nps_stats {
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
 
+/* ====================================== 3D Gaussians (north-star trainer)
+ * No counterpart in the reference, which fits linear-parameter generalised
+ * splats; this trainer keeps the reference's fit-a-scene call pattern
+ * (GpuSplatOptimizerManager: write params, write camera(s), set target(s),
+ * dispatch) for standard 3D Gaussians.  Parameter record: 64 floats per
+ * Gaussian (256 B): mean xyz | log-scale xyz | quaternion wxyz | opacity logit |
+ * pad | SH coefficients 16 x rgb (coefficient-major) | pad.  Loss: 0.8 L1 +
+ * 0.2 (1 - SSIM).  All views of a step are processed by every launch. */
+int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** out);
+int nps_gs_destroy(nps_gs* gs);
+/* Upload records [first, first+count); the active count grows to cover them. */
+int nps_gs_write_params(nps_gs* gs, const float* params, uint32_t first, uint32_t count, int mem);
+int nps_gs_set_count(nps_gs* gs, uint32_t count);
+int nps_gs_write_state(nps_gs* gs, const float* adam_m, const float* adam_v, uint32_t step, int mem);
+/* Host copies of the active records (null pointers skipped); adc_grad / adc_denom
+ * are the accumulated view-space gradient norms and visibility counts. */
+int nps_gs_read_state(nps_gs* gs, float* params, float* grads, float* adam_m, float* adam_v, float* adc_grad,
+                      float* adc_denom);
+/* Learning rates: mean, log-scale, quaternion, opacity logit, SH DC, SH rest. */
+int nps_gs_set_lr(nps_gs* gs, const float* lr6);
+int nps_gs_set_background(nps_gs* gs, float r, float g, float b);
+/* Target images: num_targets x h x w x 4 floats (rgb used), resident on the device. */
+int nps_gs_set_targets(nps_gs* gs, const float* rgba, uint32_t width, uint32_t height, uint32_t num_targets, int mem);
+/* Cameras of the next step: num_views view-projection matrices (+ inverses),
+ * and for each the index of its target image (null = 0, 1, 2, ...). */
+int nps_gs_set_views(nps_gs* gs, const float* vp, const float* vp_inv, const uint32_t* target_ids, uint32_t num_views);
+/* Paired differentiable rendering: forward keeps only per-record and per-pixel
+ * state (final transmittance + last contributor); backward replays. */
+int nps_gs_forward(nps_gs* gs, float* out_rgba_device);
+/* Fused loss of the last forward against the targets; loss3 (host, may be
+ * null) = {loss, mean L1, mean SSIM}.  Also stores dL/dimage for backward. */
+int nps_gs_loss(nps_gs* gs, float* loss3);
+/* dl_dimage: device num_views*h*w*4 floats, or null for the fused loss gradient. */
+int nps_gs_backward(nps_gs* gs, const float* dl_dimage_device);
+int nps_gs_adam(nps_gs* gs);
+/* forward + loss + backward + Adam. */
+int nps_gs_train_step(nps_gs* gs, float* loss3);
+/* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
+ * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
+int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
+int nps_gs_buffers(nps_gs* gs, float** params, float** grads, float** adam_m, float** adam_v, float** image,
+                   float** dl_dimage);
+int nps_gs_stats(nps_gs* gs, nps_stats* out);
+/* Per-stage device timing with CUDA events on the context stream (off by
+ * default).  Stages: 0 preprocess, 1 depth sort, 2 pair emit, 3 tile sort,
+ * 4 tile ranges, 5 forward raster, 6 loss, 7 backward raster, 8 projection
+ * backward, 9 Adam.  stage_times waits for the stream, adds the recorded
+ * intervals to the totals, and returns totals (ms) and counts per stage. */
+int nps_gs_set_timing(nps_gs* gs, int enable);
+int nps_gs_stage_times(nps_gs* gs, double* ms, uint64_t* calls, uint32_t n, int reset);
+
 #ifdef __cplusplus
 }
 #endif

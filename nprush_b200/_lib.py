@@ -55,6 +55,26 @@ SIGNATURES = {
     "nps_splat_opt_render": [P, P, U32, U32, P, P],
     "nps_splat_opt_buffers": [P, PP, PP, PP, PP, PP],
     "nps_splat_opt_stats": [P, ctypes.POINTER(nps_stats)],
+    "nps_gs_create": [P, U32, U32, PP],
+    "nps_gs_destroy": [P],
+    "nps_gs_write_params": [P, P, U32, U32, I32],
+    "nps_gs_set_count": [P, U32],
+    "nps_gs_write_state": [P, P, P, U32, I32],
+    "nps_gs_read_state": [P, P, P, P, P, P, P],
+    "nps_gs_set_lr": [P, P],
+    "nps_gs_set_background": [P, F32, F32, F32],
+    "nps_gs_set_targets": [P, P, U32, U32, U32, I32],
+    "nps_gs_set_views": [P, P, P, P, U32],
+    "nps_gs_forward": [P, P],
+    "nps_gs_loss": [P, P],
+    "nps_gs_backward": [P, P],
+    "nps_gs_adam": [P],
+    "nps_gs_train_step": [P, P],
+    "nps_gs_read_image": [P, P, P],
+    "nps_gs_buffers": [P, PP, PP, PP, PP, PP, PP],
+    "nps_gs_stats": [P, ctypes.POINTER(nps_stats)],
+    "nps_gs_set_timing": [P, I32],
+    "nps_gs_stage_times": [P, P, P, U32, I32],
 }
 _RET = {"nps_last_error": ctypes.c_char_p, "nps_version": ctypes.c_char_p}
 

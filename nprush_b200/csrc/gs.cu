@@ -1,0 +1,1244 @@
+// gs.cu — batched multi-view 3D Gaussian trainer (forward, L1 + D-SSIM loss,
+// backward, Adam) for sm_100a.
+//
+// One train step over V views is a fixed sequence of launches, each covering
+// all views at once:
+//   k_preprocess   (view, Gaussian): projection, EWA 2D covariance, conic,
+//                  3-sigma tile rectangle, SH colour, depth key
+//   radix sort     32-bit depth keys of all (view, Gaussian) records
+//   k_gather_counts + scan + k_emit: (view * tiles + tile, record) pairs
+//                  written in depth order
+//   radix sort     stable by tile key -> every tile list is depth ordered
+//   k_ranges       tile list bounds
+//   k_fwd          one CTA per (tile, view): records staged in shared memory
+//                  256 at a time, front-to-back compositing with alpha
+//                  clamp 0.99, 1/255 skip and early termination at T < 1e-4
+//                  (block-wide vote ends the tile), final T and last
+//                  contributor stored per pixel (O(pixels) state, no
+//                  per-pair state)
+//   k_ssim_fwd / k_ssim_bwd / k_loss_reduce: (1 - l) L1 + l (1 - SSIM), 11x11
+//                  Gaussian window (sigma 1.5), l = 0.2, and dL/dimage
+//   k_bwd          reverse traversal replaying transmittance from the final
+//                  T, per-Gaussian gradients summed over the warp with
+//                  shuffles, then over the CTA in shared memory, then one
+//                  global atomic per (tile, Gaussian, value)
+//   k_project_bwd  one thread per Gaussian looping over the views:
+//                  screen-space gradients -> parameter gradients (no
+//                  atomics: deterministic), ADC statistics
+//   k_adam         fused Adam over the 59 parameters of every Gaussian
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+#include "gs_math.cuh"
+
+namespace nps {
+namespace gs {
+
+using namespace gsm;
+
+constexpr int kThreads = 256;
+constexpr float kLowpass = 0.3f;       // px^2 added to the 2D covariance diagonal
+constexpr float kNear = 0.2f;          // cull Gaussians closer than this (view depth)
+constexpr float kAlphaMin = 1.0f / 255.0f;
+constexpr float kAlphaMax = 0.99f;
+constexpr float kTMin = 1e-4f;
+constexpr int kG2 = 12;                // floats per screen-space gradient record
+constexpr int kSsimWin = 11;
+constexpr float kSsimC1 = 0.01f * 0.01f, kSsimC2 = 0.03f * 0.03f;
+
+__constant__ float c_ssim_w[kSsimWin];
+
+struct Rec {  // projected record, 3 x float4 = 48 B
+  float4 a;   // u, v, conic a, conic b
+  float4 b;   // conic c, opacity, r, g
+  float4 c;   // b, depth, radius, 0
+};
+
+__device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+// ------------------------------------------------------------ preprocess
+__global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ params, uint32_t n, int sh_deg,
+                                                    const float* __restrict__ views, uint32_t nv, uint32_t W,
+                                                    uint32_t H, uint32_t tiles_x, uint32_t tiles_y,
+                                                    Rec* __restrict__ recs, uint32_t* __restrict__ counts,
+                                                    uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
+                                                    uint32_t* __restrict__ dvals) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nv * n) return;
+  const uint32_t v = g / n, i = g - v * n;
+  const float* p = params + (size_t)i * kP;
+  const float* view = views + (size_t)v * kViewRec;
+  float mean[3] = {p[0], p[1], p[2]};
+  float ls[3] = {p[3], p[4], p[5]};
+  float q[4] = {p[6], p[7], p[8], p[9]};
+  Proj<float> P;
+  project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
+  uint32_t cnt = 0;
+  uint2 rect = make_uint2(0, 0);
+  uint32_t key = 0xffffffffu;
+  Rec r;
+  r.a = make_float4(0, 0, 0, 0);
+  r.b = make_float4(0, 0, 0, 0);
+  r.c = make_float4(0, 0, 0, 0);
+  if (P.cw > kNear && P.det > 0.0f) {
+    const float mid = 0.5f * (P.A + P.C);
+    const float lam = mid + sqrtf(fmaxf(0.1f, mid * mid - P.det));
+    const float radius = ceilf(3.0f * sqrtf(lam));
+    const int x0 = max(0, min((int)tiles_x, (int)floorf((P.u - radius) / 16.0f)));
+    const int x1 = max(0, min((int)tiles_x, (int)floorf((P.u + radius) / 16.0f) + 1));
+    const int y0 = max(0, min((int)tiles_y, (int)floorf((P.v - radius) / 16.0f)));
+    const int y1 = max(0, min((int)tiles_y, (int)floorf((P.v + radius) / 16.0f) + 1));
+    if (x1 > x0 && y1 > y0) {
+      cnt = (uint32_t)((x1 - x0) * (y1 - y0));
+      rect = make_uint2((uint32_t)x0 | ((uint32_t)x1 << 16), (uint32_t)y0 | ((uint32_t)y1 << 16));
+      key = __float_as_uint(P.cw);  // positive floats order like their bit patterns
+      // SH colour for the view direction
+      const float dx = mean[0] - view[32], dy = mean[1] - view[33], dz = mean[2] - view[34];
+      const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-20f));
+      float basis[16];
+      sh_basis<float>(sh_deg, dx * il, dy * il, dz * il, basis);
+      const int nb = (sh_deg + 1) * (sh_deg + 1);
+      float col[3] = {0.5f, 0.5f, 0.5f};
+      for (int k = 0; k < nb; ++k) {
+        col[0] += basis[k] * p[kSH + 3 * k + 0];
+        col[1] += basis[k] * p[kSH + 3 * k + 1];
+        col[2] += basis[k] * p[kSH + 3 * k + 2];
+      }
+      const float op = sigmoidf(p[kOpacity]);
+      r.a = make_float4(P.u, P.v, P.ca, P.cb);
+      r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
+      r.c = make_float4(fmaxf(col[2], 0.0f), P.cw, radius, 0.0f);
+    }
+  }
+  recs[g] = r;
+  counts[g] = cnt;
+  rects[g] = rect;
+  dkeys[g] = key;
+  dvals[g] = g;
+}
+
+__global__ void k_gather_counts(const uint32_t* __restrict__ sorted_g, const uint32_t* __restrict__ counts,
+                                uint32_t m, uint32_t* __restrict__ out) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) out[j] = counts[sorted_g[j]];
+}
+
+__global__ void k_emit(const uint32_t* __restrict__ sorted_g, const uint32_t* __restrict__ counts,
+                       const uint32_t* __restrict__ offsets, const uint2* __restrict__ rects, uint32_t m, uint32_t n,
+                       uint32_t tiles_x, uint32_t num_tiles, uint32_t cap, uint32_t* __restrict__ keys,
+                       uint32_t* __restrict__ vals) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t g = sorted_g[j];
+  const uint32_t c = counts[g];
+  if (c == 0) return;
+  const uint32_t v = g / n;
+  uint32_t pos = offsets[j];
+  const uint2 r = rects[g];
+  const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
+  for (uint32_t ty = y0; ty < y1; ++ty)
+    for (uint32_t tx = x0; tx < x1; ++tx) {
+      if (pos < cap) {
+        keys[pos] = v * num_tiles + ty * tiles_x + tx;
+        vals[pos] = g;
+      }
+      ++pos;
+    }
+}
+
+__global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
+                         uint32_t* __restrict__ rstart, uint32_t* __restrict__ rend) {
+  const uint32_t K = min(*total, cap);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < K; p += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[p];
+    if (p == 0 || keys[p - 1] != k) rstart[k] = p;
+    if (p == K - 1 || keys[p + 1] != k) rend[k] = p + 1;
+  }
+}
+
+// ------------------------------------------------------------ forward raster
+__global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                                  const uint32_t* __restrict__ rstart,
+                                                  const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
+                                                  uint32_t tiles_x, uint32_t num_tiles, float3 bg,
+                                                  float4* __restrict__ img, uint32_t* __restrict__ ncontrib) {
+  __shared__ float4 s_a[kThreads];
+  __shared__ float4 s_b[kThreads];
+  __shared__ float s_c[kThreads];
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const bool inside = px < W && py < H;
+  const float fx = (float)px, fy = (float)py;
+  const uint32_t key = v * num_tiles + ty * tiles_x + tx;
+  const uint32_t start = rstart[key], end = rend[key];
+  float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
+  uint32_t last = 0;
+  bool done = !inside;
+  for (uint32_t base = start; base < end; base += kThreads) {
+    if (__syncthreads_count(done) == kThreads) break;
+    const uint32_t idx = base + tid;
+    if (idx < end) {
+      const Rec r = recs[vals[idx]];
+      s_a[tid] = r.a;
+      s_b[tid] = r.b;
+      s_c[tid] = r.c.x;
+    }
+    __syncthreads();
+    const uint32_t nb = min((uint32_t)kThreads, end - base);
+    for (uint32_t j = 0; j < nb && !done; ++j) {
+      const float4 a = s_a[j];
+      const float4 b = s_b[j];
+      const float dx = a.x - fx, dy = a.y - fy;
+      const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+      if (power > 0.0f) continue;
+      const float alpha = fminf(kAlphaMax, b.y * __expf(power));
+      if (alpha < kAlphaMin) continue;
+      const float test_T = T * (1.0f - alpha);
+      if (test_T < kTMin) {
+        done = true;
+        break;
+      }
+      const float w = alpha * T;
+      C0 += b.z * w;
+      C1 += b.w * w;
+      C2 += s_c[j] * w;
+      T = test_T;
+      last = base - start + j + 1;
+    }
+  }
+  if (inside) {
+    const size_t pix = ((size_t)v * H + py) * W + px;
+    img[pix] = make_float4(C0 + T * bg.x, C1 + T * bg.y, C2 + T * bg.z, T);
+    ncontrib[pix] = last;
+  }
+}
+
+// ------------------------------------------------------------ loss
+// (1 - l) * mean|x - y| + l * (1 - mean SSIM), averaged over views.
+// k_ssim_fwd writes, per pixel and channel, the three maps whose Gaussian
+// correlation gives dL/dx; plus per-block partial sums of |x - y| and SSIM.
+constexpr int kHalo = kSsimWin / 2;
+constexpr int kTileP = 16 + 2 * kHalo;  // 26
+
+__global__ void __launch_bounds__(kThreads) k_ssim_fwd(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                                                       const uint32_t* __restrict__ tgt_ids, uint32_t W, uint32_t H,
+                                                       float lambda, float inv_norm, float* __restrict__ maps,
+                                                       float* __restrict__ partial) {
+  __shared__ float sx[3][kTileP][kTileP];
+  __shared__ float sy[3][kTileP][kTileP];
+  __shared__ float hm[15][kTileP][16];  // horizontal pass: 5 moments x 3 channels
+  __shared__ float red[2][kThreads / 32];
+  const uint32_t v = blockIdx.z, tid = threadIdx.x;
+  const int ox = blockIdx.x * 16 - kHalo, oy = blockIdx.y * 16 - kHalo;
+  const float4* im = img + (size_t)v * W * H;
+  const float4* tg = tgt + (size_t)tgt_ids[v] * W * H;
+  for (int e = tid; e < kTileP * kTileP; e += kThreads) {
+    const int ly = e / kTileP, lx = e - ly * kTileP;
+    const int gx = ox + lx, gy = oy + ly;
+    float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0);
+    if (gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H) {
+      a = im[(size_t)gy * W + gx];
+      b = tg[(size_t)gy * W + gx];
+    }
+    sx[0][ly][lx] = a.x; sx[1][ly][lx] = a.y; sx[2][ly][lx] = a.z;
+    sy[0][ly][lx] = b.x; sy[1][ly][lx] = b.y; sy[2][ly][lx] = b.z;
+  }
+  __syncthreads();
+  for (int e = tid; e < kTileP * 16; e += kThreads) {
+    const int ly = e / 16, lx = e - ly * 16;
+    for (int c = 0; c < 3; ++c) {
+      float m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0;
+#pragma unroll
+      for (int k = 0; k < kSsimWin; ++k) {
+        const float w = c_ssim_w[k];
+        const float x = sx[c][ly][lx + k], y = sy[c][ly][lx + k];
+        m0 += w * x; m1 += w * y; m2 += w * x * x; m3 += w * y * y; m4 += w * x * y;
+      }
+      hm[5 * c + 0][ly][lx] = m0; hm[5 * c + 1][ly][lx] = m1; hm[5 * c + 2][ly][lx] = m2;
+      hm[5 * c + 3][ly][lx] = m3; hm[5 * c + 4][ly][lx] = m4;
+    }
+  }
+  __syncthreads();
+  const int lx = tid & 15, ly = tid >> 4;
+  const int px = blockIdx.x * 16 + lx, py = blockIdx.y * 16 + ly;
+  const bool inside = px < (int)W && py < (int)H;
+  float l1 = 0.0f, ss = 0.0f;
+  if (inside) {
+    float* mp = maps + (((size_t)v * H + py) * W + px) * 9;
+    for (int c = 0; c < 3; ++c) {
+      float mo[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < kSsimWin; ++k) {
+        const float w = c_ssim_w[k];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) mo[q] += w * hm[5 * c + q][ly + k][lx];
+      }
+      const float mx = mo[0], my = mo[1];
+      const float sxx = mo[2] - mx * mx, syy = mo[3] - my * my, sxy = mo[4] - mx * my;
+      const float A1 = 2.0f * mx * my + kSsimC1, A2 = 2.0f * sxy + kSsimC2;
+      const float B1 = mx * mx + my * my + kSsimC1, B2 = sxx + syy + kSsimC2;
+      const float s = (A1 * A2) / (B1 * B2);
+      ss += s;
+      const float dLds = -lambda * inv_norm;
+      const float ds_dmx = (2.0f * my * A2) / (B1 * B2) - s * 2.0f * mx / B1;
+      const float ds_dsxx = -s / B2;
+      const float ds_dsxy = 2.0f * A1 / (B1 * B2);
+      const float dm = dLds * ds_dmx, d2 = dLds * ds_dsxx, dxy = dLds * ds_dsxy;
+      mp[3 * c + 0] = dm - 2.0f * mx * d2 - my * dxy;
+      mp[3 * c + 1] = d2;
+      mp[3 * c + 2] = dxy;
+      l1 += fabsf(sx[c][ly + kHalo][lx + kHalo] - sy[c][ly + kHalo][lx + kHalo]);
+    }
+  }
+  // block partial sums (deterministic order)
+  for (int o = 16; o > 0; o >>= 1) {
+    l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+    ss += __shfl_xor_sync(0xffffffffu, ss, o);
+  }
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = l1;
+    red[1][tid >> 5] = ss;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float a = 0, b = 0;
+    for (int w = 0; w < kThreads / 32; ++w) { a += red[0][w]; b += red[1][w]; }
+    const size_t bi = ((size_t)v * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    partial[2 * bi] = a;
+    partial[2 * bi + 1] = b;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ssim_bwd(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                                                       const uint32_t* __restrict__ tgt_ids, const float* __restrict__ maps,
+                                                       uint32_t W, uint32_t H, float lambda, float inv_norm,
+                                                       float4* __restrict__ dimg) {
+  __shared__ float sm[9][kTileP][kTileP];
+  __shared__ float hm[9][kTileP][16];
+  const uint32_t v = blockIdx.z, tid = threadIdx.x;
+  const int ox = blockIdx.x * 16 - kHalo, oy = blockIdx.y * 16 - kHalo;
+  const float* mv = maps + (size_t)v * W * H * 9;
+  for (int e = tid; e < kTileP * kTileP; e += kThreads) {
+    const int ly = e / kTileP, lx = e - ly * kTileP;
+    const int gx = ox + lx, gy = oy + ly;
+    const bool ok = gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H;
+    const float* src = mv + ((size_t)(ok ? gy : 0) * W + (ok ? gx : 0)) * 9;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) sm[q][ly][lx] = ok ? src[q] : 0.0f;
+  }
+  __syncthreads();
+  for (int e = tid; e < kTileP * 16; e += kThreads) {
+    const int ly = e / 16, lx = e - ly * 16;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * sm[q][ly][lx + k];
+      hm[q][ly][lx] = acc;
+    }
+  }
+  __syncthreads();
+  const int lx = tid & 15, ly = tid >> 4;
+  const int px = blockIdx.x * 16 + lx, py = blockIdx.y * 16 + ly;
+  if (px >= (int)W || py >= (int)H) return;
+  float cv[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * hm[q][ly + k][lx];
+    cv[q] = acc;
+  }
+  const size_t pix = ((size_t)v * H + py) * W + px;
+  const float4 x = img[pix];
+  const float4 y = tgt[(size_t)tgt_ids[v] * W * H + (size_t)py * W + px];
+  const float l1w = (1.0f - lambda) * inv_norm;
+  const float xs[3] = {x.x, x.y, x.z}, ys[3] = {y.x, y.y, y.z};
+  float d[3];
+  for (int c = 0; c < 3; ++c) {
+    const float diff = xs[c] - ys[c];
+    const float sgn = diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f);
+    d[c] = cv[3 * c] + 2.0f * xs[c] * cv[3 * c + 1] + ys[c] * cv[3 * c + 2] + l1w * sgn;
+  }
+  dimg[pix] = make_float4(d[0], d[1], d[2], 0.0f);
+}
+
+__global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblocks, float lambda, float inv_norm,
+                              float* __restrict__ loss) {
+  __shared__ float r0[kThreads], r1[kThreads];
+  float a = 0, b = 0;
+  for (uint32_t i = threadIdx.x; i < nblocks; i += kThreads) {
+    a += partial[2 * i];
+    b += partial[2 * i + 1];
+  }
+  r0[threadIdx.x] = a;
+  r1[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      r0[threadIdx.x] += r0[threadIdx.x + s];
+      r1[threadIdx.x] += r1[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    // inv_norm = 1 / (3 H W V)
+    loss[0] = (1.0f - lambda) * r0[0] * inv_norm + lambda * (1.0f - r1[0] * inv_norm);
+    loss[1] = r0[0] * inv_norm;  // mean L1
+    loss[2] = r1[0] * inv_norm;  // mean SSIM
+  }
+}
+
+// ------------------------------------------------------------ backward raster
+__global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                                  const uint32_t* __restrict__ rstart,
+                                                  const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
+                                                  uint32_t tiles_x, uint32_t num_tiles, float3 bg,
+                                                  const float4* __restrict__ img, const uint32_t* __restrict__ ncontrib,
+                                                  const float4* __restrict__ dimg, float* __restrict__ g2) {
+  __shared__ float4 s_a[kThreads];
+  __shared__ float4 s_b[kThreads];
+  __shared__ float s_c[kThreads];
+  __shared__ uint32_t s_g[kThreads];
+  __shared__ float s_acc[kThreads][10];
+  __shared__ uint32_t s_max;
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const bool inside = px < W && py < H;
+  const float fx = (float)px, fy = (float)py;
+  const uint32_t key = v * num_tiles + ty * tiles_x + tx;
+  const uint32_t start = rstart[key], end = rend[key];
+  float T = 1.0f, T_final = 1.0f;
+  uint32_t last = 0;
+  float dC[3] = {0, 0, 0};
+  if (inside) {
+    const size_t pix = ((size_t)v * H + py) * W + px;
+    const float4 o = img[pix];
+    T = o.w;
+    T_final = o.w;
+    last = ncontrib[pix];
+    const float4 d = dimg[pix];
+    dC[0] = d.x; dC[1] = d.y; dC[2] = d.z;
+  }
+  if (tid == 0) s_max = 0;
+  __syncthreads();
+  atomicMax(&s_max, last);
+  __syncthreads();
+  const uint32_t maxlast = s_max;
+  const float bg_dot = bg.x * dC[0] + bg.y * dC[1] + bg.z * dC[2];
+  float accum[3] = {0, 0, 0}, last_col[3] = {0, 0, 0};
+  float last_alpha = 0.0f;
+  for (uint32_t bend = start + maxlast; bend > start;) {
+    const uint32_t bstart = bend > start + kThreads ? bend - kThreads : start;
+    const uint32_t nb = bend - bstart;
+    __syncthreads();
+    if (tid < nb) {
+      const uint32_t gg = vals[bstart + tid];
+      const Rec r = recs[gg];
+      s_a[tid] = r.a;
+      s_b[tid] = r.b;
+      s_c[tid] = r.c.x;
+      s_g[tid] = gg;
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
+    __syncthreads();
+    for (int j = (int)nb - 1; j >= 0; --j) {
+      const uint32_t cur = bstart + (uint32_t)j - start;
+      float gv[10];
+#pragma unroll
+      for (int k = 0; k < 10; ++k) gv[k] = 0.0f;
+      bool contrib = false;
+      if (inside && cur < last) {
+        const float4 a = s_a[j];
+        const float4 b = s_b[j];
+        const float col[3] = {b.z, b.w, s_c[j]};
+        const float dx = a.x - fx, dy = a.y - fy;
+        const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+        if (power <= 0.0f) {
+          const float G = __expf(power);
+          const float araw = b.y * G;
+          const float alpha = fminf(kAlphaMax, araw);
+          if (alpha >= kAlphaMin) {
+            contrib = true;
+            T = T / (1.0f - alpha);
+            const float wgt = alpha * T;
+            float dL_dalpha = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              accum[c] = last_alpha * last_col[c] + (1.0f - last_alpha) * accum[c];
+              last_col[c] = col[c];
+              dL_dalpha += (col[c] - accum[c]) * dC[c];
+              gv[6 + c] = wgt * dC[c];
+            }
+            dL_dalpha *= T;
+            last_alpha = alpha;
+            dL_dalpha += (-T_final / (1.0f - alpha)) * bg_dot;
+            if (araw <= kAlphaMax) {
+              const float dL_dG = b.y * dL_dalpha;
+              const float gdx = G * dx, gdy = G * dy;
+              gv[0] = dL_dG * (-gdx * a.z - gdy * a.w);   // d/du
+              gv[1] = dL_dG * (-gdy * b.x - gdx * a.w);   // d/dv
+              gv[2] = -0.5f * gdx * dx * dL_dG;           // d/d conic a
+              gv[3] = -gdx * dy * dL_dG;                  // d/d conic b
+              gv[4] = -0.5f * gdy * dy * dL_dG;           // d/d conic c
+              gv[5] = G * dL_dalpha;                      // d/d opacity
+            }
+          }
+        }
+      }
+      if (__any_sync(0xffffffffu, contrib)) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+          float x = gv[k];
+          x += __shfl_xor_sync(0xffffffffu, x, 16);
+          x += __shfl_xor_sync(0xffffffffu, x, 8);
+          x += __shfl_xor_sync(0xffffffffu, x, 4);
+          x += __shfl_xor_sync(0xffffffffu, x, 2);
+          x += __shfl_xor_sync(0xffffffffu, x, 1);
+          gv[k] = x;
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int k = 0; k < 10; ++k) atomicAdd(&s_acc[j][k], gv[k]);
+        }
+      }
+    }
+    __syncthreads();
+    if (tid < nb) {
+      float* dst = g2 + (size_t)s_g[tid] * kG2;
+#pragma unroll
+      for (int k = 0; k < 10; ++k) {
+        const float x = s_acc[tid][k];
+        if (x != 0.0f) atomicAdd(dst + k, x);
+      }
+    }
+    bend = bstart;
+  }
+}
+
+// ------------------------------------------------------------ projection backward
+__global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ params, uint32_t n, int sh_deg,
+                                                     const float* __restrict__ views, uint32_t nv, uint32_t W,
+                                                     uint32_t H, const Rec* __restrict__ recs,
+                                                     const uint32_t* __restrict__ counts,
+                                                     const float* __restrict__ g2, float* __restrict__ grads,
+                                                     float* __restrict__ adc_grad, float* __restrict__ adc_denom) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* p = params + (size_t)i * kP;
+  float mean[3] = {p[0], p[1], p[2]};
+  float ls[3] = {p[3], p[4], p[5]};
+  float q[4] = {p[6], p[7], p[8], p[9]};
+  float gmean[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, gop = 0.0f;
+  float gsh[48];
+  const int nb = (sh_deg + 1) * (sh_deg + 1);
+  for (int k = 0; k < 48; ++k) gsh[k] = 0.0f;
+  float adc_g = 0.0f, adc_n = 0.0f;
+  const float op = sigmoidf(p[kOpacity]);
+  for (uint32_t v = 0; v < nv; ++v) {
+    const size_t g = (size_t)v * n + i;
+    if (counts[g] == 0) continue;
+    const float* gr = g2 + g * kG2;
+    const float du = gr[0], dv = gr[1], dca = gr[2], dcb = gr[3], dcc = gr[4], dop = gr[5];
+    const float dcol[3] = {gr[6], gr[7], gr[8]};
+    const float* view = views + (size_t)v * kViewRec;
+    Proj<float> P;
+    project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
+    adc_g += sqrtf((du * 0.5f * W) * (du * 0.5f * W) + (dv * 0.5f * H) * (dv * 0.5f * H));
+    adc_n += 1.0f;
+    gop += dop;
+    // colour: clamp at 0 blocks the gradient
+    const Rec rc = recs[g];
+    const float colv[3] = {rc.b.z, rc.b.w, rc.c.x};
+    const float ddx = mean[0] - view[32], ddy = mean[1] - view[33], ddz = mean[2] - view[34];
+    const float l2 = fmaxf(ddx * ddx + ddy * ddy + ddz * ddz, 1e-20f);
+    const float il = rsqrtf(l2);
+    const float dir[3] = {ddx * il, ddy * il, ddz * il};
+    float basis[16];
+    sh_basis<float>(sh_deg, dir[0], dir[1], dir[2], basis);
+    // the stored colour is clamped; recompute the unclamped value to test the clamp
+    float dc[3];
+    for (int c = 0; c < 3; ++c) {
+      float raw = 0.5f;
+      for (int k = 0; k < nb; ++k) raw += basis[k] * p[kSH + 3 * k + c];
+      dc[c] = raw < 0.0f ? 0.0f : dcol[c];
+      (void)colv;
+    }
+    float ddir[3] = {0, 0, 0};
+    if (sh_deg > 0) {
+      float bx[16], by[16], bz[16];
+      sh_basis_grad<float>(sh_deg, dir[0], dir[1], dir[2], bx, by, bz);
+      for (int k = 1; k < nb; ++k) {
+        const float s = p[kSH + 3 * k] * dc[0] + p[kSH + 3 * k + 1] * dc[1] + p[kSH + 3 * k + 2] * dc[2];
+        ddir[0] += s * bx[k];
+        ddir[1] += s * by[k];
+        ddir[2] += s * bz[k];
+      }
+      const float dd = dir[0] * ddir[0] + dir[1] * ddir[1] + dir[2] * ddir[2];
+      for (int c = 0; c < 3; ++c) gmean[c] += (ddir[c] - dir[c] * dd) * il;
+    }
+    for (int k = 0; k < nb; ++k)
+      for (int c = 0; c < 3; ++c) gsh[3 * k + c] += basis[k] * dc[c];
+    // conic -> covariance: dL/dCov = -Inv H Inv, H = [[ga, gb/2], [gb/2, gc]]
+    const float ia = P.ca, ib = P.cb, ic = P.cc;
+    const float h00 = dca, h01 = 0.5f * dcb, h11 = dcc;
+    // X = H Inv
+    const float x00 = h00 * ia + h01 * ib, x01 = h00 * ib + h01 * ic;
+    const float x10 = h01 * ia + h11 * ib, x11 = h01 * ib + h11 * ic;
+    // Gc = -Inv X
+    const float G00 = -(ia * x00 + ib * x10);
+    const float G01 = -(ia * x01 + ib * x11);
+    const float G10 = -(ib * x00 + ic * x10);
+    const float G11 = -(ib * x01 + ic * x11);
+    const float Gs[2][2] = {{G00, 0.5f * (G01 + G10)}, {0.5f * (G01 + G10), G11}};
+    // dL/dSigma = J^T Gs J ; dL/dJ = 2 Gs J Sigma
+    float GJ[2][3];
+    for (int r = 0; r < 2; ++r)
+      for (int c = 0; c < 3; ++c) GJ[r][c] = Gs[r][0] * P.J[0][c] + Gs[r][1] * P.J[1][c];
+    float dS[3][3];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) dS[r][c] = P.J[0][r] * GJ[0][c] + P.J[1][r] * GJ[1][c];
+    float dJ[2][3];
+    for (int r = 0; r < 2; ++r)
+      for (int c = 0; c < 3; ++c)
+        dJ[r][c] = 2.0f * (GJ[r][0] * P.S[0][c] + GJ[r][1] * P.S[1][c] + GJ[r][2] * P.S[2][c]);
+    // J depends on the mean through clip (x, y, w)
+    {
+      const float r0[3] = {view[0], view[4], view[8]};
+      const float r1[3] = {view[1], view[5], view[9]};
+      const float r3[3] = {view[3], view[7], view[11]};
+      const float a = 0.5f * W, b = 0.5f * H;
+      const float iw = 1.0f / P.cw, iw2 = iw * iw, iw3 = iw2 * iw;
+      const float d0r0 = dJ[0][0] * r0[0] + dJ[0][1] * r0[1] + dJ[0][2] * r0[2];
+      const float d0r3 = dJ[0][0] * r3[0] + dJ[0][1] * r3[1] + dJ[0][2] * r3[2];
+      const float d1r1 = dJ[1][0] * r1[0] + dJ[1][1] * r1[1] + dJ[1][2] * r1[2];
+      const float d1r3 = dJ[1][0] * r3[0] + dJ[1][1] * r3[1] + dJ[1][2] * r3[2];
+      for (int l = 0; l < 3; ++l) {
+        gmean[l] += a * (-d0r0 * r3[l] * iw2 - d0r3 * r0[l] * iw2 + 2.0f * P.cx * d0r3 * r3[l] * iw3);
+        gmean[l] += -b * (-d1r1 * r3[l] * iw2 - d1r3 * r1[l] * iw2 + 2.0f * P.cy * d1r3 * r3[l] * iw3);
+        gmean[l] += P.J[0][l] * du + P.J[1][l] * dv;
+      }
+    }
+    // Sigma = M M^T, M = R diag(s)
+    float dM[3][3];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        dM[r][c] = 2.0f * (dS[r][0] * P.M[0][c] + dS[r][1] * P.M[1][c] + dS[r][2] * P.M[2][c]);
+    float dR[3][3];
+    for (int c = 0; c < 3; ++c) {
+      float ds = 0.0f;
+      for (int r = 0; r < 3; ++r) {
+        ds += dM[r][c] * P.R[r][c];
+        dR[r][c] = dM[r][c] * P.sc[c];
+      }
+      gls[c] += ds * P.sc[c];
+    }
+    float dqn[4];
+    rot_grad_to_quat<float>(P.qn[0], P.qn[1], P.qn[2], P.qn[3], dR, dqn);
+    const float qd = P.qn[0] * dqn[0] + P.qn[1] * dqn[1] + P.qn[2] * dqn[2] + P.qn[3] * dqn[3];
+    for (int k = 0; k < 4; ++k) gq[k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
+  }
+  float* out = grads + (size_t)i * kP;
+  out[0] = gmean[0]; out[1] = gmean[1]; out[2] = gmean[2];
+  out[3] = gls[0]; out[4] = gls[1]; out[5] = gls[2];
+  out[6] = gq[0]; out[7] = gq[1]; out[8] = gq[2]; out[9] = gq[3];
+  out[10] = gop * op * (1.0f - op);
+  out[11] = 0.0f;
+  for (int k = 0; k < 48; ++k) out[kSH + k] = gsh[k];
+  out[60] = out[61] = out[62] = out[63] = 0.0f;
+  adc_grad[i] += adc_g;
+  adc_denom[i] += adc_n;
+}
+
+// ------------------------------------------------------------ Adam
+struct AdamArgs {
+  float lr[6];  // mean, log-scale, quat, opacity, SH DC, SH rest
+  float b1, b2, eps, bc1, bc2;
+};
+
+__device__ __forceinline__ float lr_of(const AdamArgs& a, int k) {
+  return k < 3 ? a.lr[0] : k < 6 ? a.lr[1] : k < 10 ? a.lr[2] : k < 12 ? a.lr[3] : k < 15 ? a.lr[4] : a.lr[5];
+}
+
+// one thread per float4 of the parameter record (16 per Gaussian)
+__global__ void __launch_bounds__(256) k_adam(float4* __restrict__ p, const float4* __restrict__ g,
+                                              float4* __restrict__ m, float4* __restrict__ v, uint32_t n4,
+                                              AdamArgs a) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n4) return;
+  const int k0 = (int)(t & 15u) * 4;
+  float4 pp = p[t], gg = g[t], mm = m[t], vv = v[t];
+  float* pf = &pp.x;
+  const float* gf = &gg.x;
+  float* mf = &mm.x;
+  float* vf = &vv.x;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int k = k0 + c;
+    if (k == 11 || k >= kUsed) continue;
+    const float gr = gf[c];
+    mf[c] = a.b1 * mf[c] + (1.0f - a.b1) * gr;
+    vf[c] = a.b2 * vf[c] + (1.0f - a.b2) * gr * gr;
+    const float mh = mf[c] / a.bc1, vh = vf[c] / a.bc2;
+    pf[c] -= lr_of(a, k) * mh / (sqrtf(vh) + a.eps);
+  }
+  p[t] = pp;
+  m[t] = mm;
+  v[t] = vv;
+}
+
+}  // namespace gs
+}  // namespace nps
+
+// =================================================================== host side
+using namespace nps;
+
+namespace {
+__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
+}  // namespace
+
+struct nps_gs {
+  nps_ctx* ctx = nullptr;
+  uint32_t cap = 0, n = 0;
+  int sh_deg = 3;
+  DevBuf params, grads, am, av, adc_grad, adc_denom;
+  uint32_t step = 0;
+  float lr[6] = {1.6e-4f, 5e-3f, 1e-3f, 5e-2f, 2.5e-3f, 2.5e-3f / 20.0f};
+  float lambda = 0.2f;
+  float bg[3] = {0.0f, 0.0f, 0.0f};
+  // targets
+  uint32_t w = 0, h = 0, nt = 0;
+  DevBuf tgt_own;
+  const float4* tgt = nullptr;
+  // views of the current step
+  uint32_t nv = 0;
+  DevBuf views, tids;
+  // forward state
+  DevBuf recs, counts, rects, dkeys, dvals, cnt_sorted, offsets, total, mcount, keys, vals, ranges, img, ncontrib;
+  DevBuf maps, partial, loss, dimg, g2;
+  SortWork sw_depth, sw_tile;
+  uint32_t pair_cap = 0;
+  uint32_t K = 0;
+  const uint32_t* sorted_vals = nullptr;
+  bool fwd_valid = false, loss_valid = false;
+  nps_stats stats{};
+  // optional per-stage timing with CUDA events on the context stream
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+  double stage_ms[16] = {0};
+  uint64_t stage_calls[16] = {0};
+};
+
+namespace {
+// stage ids reported by nps_gs_stage_times
+enum { ST_PRE = 0, ST_DSORT, ST_EMIT, ST_TSORT, ST_RANGES, ST_FWD, ST_LOSS, ST_BWD, ST_PBWD, ST_ADAM, ST_COUNT };
+cudaEvent_t ev_get(nps_gs* o) {
+  if (o->ev_pool.empty()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  cudaEvent_t e = o->ev_pool.back();
+  o->ev_pool.pop_back();
+  return e;
+}
+struct StageTimer {
+  nps_gs* o;
+  int id;
+  cudaEvent_t e0 = nullptr;
+  StageTimer(nps_gs* oo, int i) : o(oo), id(i) {
+    if (o->timing) {
+      e0 = ev_get(o);
+      cudaEventRecord(e0, o->ctx->stream);
+    }
+  }
+  ~StageTimer() {
+    if (o->timing) {
+      cudaEvent_t e1 = ev_get(o);
+      cudaEventRecord(e1, o->ctx->stream);
+      o->ev_used.push_back({id, {e0, e1}});
+    }
+  }
+};
+}  // namespace
+
+namespace {
+int check_gs(nps_gs* o) {
+  if (!o) {
+    set_error("null Gaussian trainer");
+    return NPS_ERR_INVALID;
+  }
+  return bind_device(o->ctx);
+}
+int copy_in_gs(void* dst, const void* src, size_t bytes, int mem, cudaStream_t s) {
+  if (bytes == 0) return NPS_OK;
+  if (!src) {
+    set_error("null source pointer");
+    return NPS_ERR_INVALID;
+  }
+  if (mem == NPS_MEM_HOST) {
+    NPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaStreamSynchronize(s));
+  } else {
+    NPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  return NPS_OK;
+}
+bool g_ssim_w_set = false;
+int ensure_ssim_weights() {
+  if (g_ssim_w_set) return NPS_OK;
+  float w[gs::kSsimWin];
+  double s = 0;
+  for (int k = 0; k < gs::kSsimWin; ++k) {
+    double d = k - gs::kSsimWin / 2;
+    w[k] = (float)std::exp(-d * d / (2.0 * 1.5 * 1.5));
+    s += w[k];
+  }
+  for (int k = 0; k < gs::kSsimWin; ++k) w[k] = (float)(w[k] / s);
+  NPS_CUDA(cudaMemcpyToSymbol(gs::c_ssim_w, w, sizeof(w)));
+  g_ssim_w_set = true;
+  return NPS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** out) {
+  if (!out || capacity == 0 || capacity > (1u << 26) || sh_degree > 3) {
+    set_error("nps_gs_create: bad arguments (capacity=%u, sh_degree=%u)", capacity, sh_degree);
+    return NPS_ERR_INVALID;
+  }
+  *out = nullptr;
+  NPS_TRY(bind_device(ctx));
+  NPS_TRY(ensure_ssim_weights());
+  nps_gs* o = new nps_gs();
+  o->ctx = ctx;
+  o->cap = capacity;
+  o->n = 0;
+  o->sh_deg = (int)sh_degree;
+  const size_t pb = sizeof(float) * gsm::kP * (size_t)capacity;
+  int rc = NPS_OK;
+  if ((rc = o->params.ensure(pb)) || (rc = o->grads.ensure(pb)) || (rc = o->am.ensure(pb)) ||
+      (rc = o->av.ensure(pb)) || (rc = o->adc_grad.ensure(sizeof(float) * capacity)) ||
+      (rc = o->adc_denom.ensure(sizeof(float) * capacity)) || (rc = o->total.ensure(16)) ||
+      (rc = o->mcount.ensure(16)) || (rc = o->loss.ensure(64))) {
+    delete o;
+    return rc;
+  }
+  cudaStream_t s = ctx->stream;
+  for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av}) cudaMemsetAsync(b->p, 0, pb, s);
+  cudaMemsetAsync(o->adc_grad.p, 0, sizeof(float) * capacity, s);
+  cudaMemsetAsync(o->adc_denom.p, 0, sizeof(float) * capacity, s);
+  cudaMemsetAsync(o->loss.p, 0, 64, s);
+  NPS_CUDA(cudaGetLastError());
+  *out = o;
+  return NPS_OK;
+}
+
+int nps_gs_destroy(nps_gs* o) {
+  if (!o) return NPS_OK;
+  cudaSetDevice(o->ctx->device);
+  cudaStreamSynchronize(o->ctx->stream);
+  for (auto& u : o->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
+  for (cudaEvent_t e : o->ev_pool) cudaEventDestroy(e);
+  for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
+                    &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
+                    &o->total, &o->mcount, &o->keys, &o->vals, &o->ranges, &o->img, &o->ncontrib, &o->maps,
+                    &o->partial, &o->loss, &o->dimg, &o->g2, &o->sw_depth.hist, &o->sw_depth.partial,
+                    &o->sw_depth.keys_alt, &o->sw_depth.vals_alt, &o->sw_tile.hist, &o->sw_tile.partial,
+                    &o->sw_tile.keys_alt, &o->sw_tile.vals_alt})
+    b->release();
+  delete o;
+  return NPS_OK;
+}
+
+int nps_gs_write_params(nps_gs* o, const float* params, uint32_t first, uint32_t count, int mem) {
+  NPS_TRY(check_gs(o));
+  if ((uint64_t)first + count > o->cap) {
+    set_error("gs_write_params: range [%u, %u) beyond capacity %u", first, first + count, o->cap);
+    return NPS_ERR_INVALID;
+  }
+  NPS_TRY(copy_in_gs(o->params.as<float>() + (size_t)gsm::kP * first, params, sizeof(float) * gsm::kP * count, mem,
+                     o->ctx->stream));
+  if (first + count > o->n) o->n = first + count;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_set_count(nps_gs* o, uint32_t n) {
+  NPS_TRY(check_gs(o));
+  if (n > o->cap) {
+    set_error("gs_set_count: %u beyond capacity %u", n, o->cap);
+    return NPS_ERR_INVALID;
+  }
+  o->n = n;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_write_state(nps_gs* o, const float* adam_m, const float* adam_v, uint32_t step, int mem) {
+  NPS_TRY(check_gs(o));
+  const size_t pb = sizeof(float) * gsm::kP * (size_t)o->n;
+  if (adam_m) NPS_TRY(copy_in_gs(o->am.p, adam_m, pb, mem, o->ctx->stream));
+  if (adam_v) NPS_TRY(copy_in_gs(o->av.p, adam_v, pb, mem, o->ctx->stream));
+  o->step = step;
+  return NPS_OK;
+}
+
+int nps_gs_read_state(nps_gs* o, float* params, float* grads, float* adam_m, float* adam_v, float* adc_grad,
+                      float* adc_denom) {
+  NPS_TRY(check_gs(o));
+  cudaStream_t s = o->ctx->stream;
+  const size_t pb = sizeof(float) * gsm::kP * (size_t)o->n;
+  if (params) NPS_CUDA(cudaMemcpyAsync(params, o->params.p, pb, cudaMemcpyDeviceToHost, s));
+  if (grads) NPS_CUDA(cudaMemcpyAsync(grads, o->grads.p, pb, cudaMemcpyDeviceToHost, s));
+  if (adam_m) NPS_CUDA(cudaMemcpyAsync(adam_m, o->am.p, pb, cudaMemcpyDeviceToHost, s));
+  if (adam_v) NPS_CUDA(cudaMemcpyAsync(adam_v, o->av.p, pb, cudaMemcpyDeviceToHost, s));
+  if (adc_grad) NPS_CUDA(cudaMemcpyAsync(adc_grad, o->adc_grad.p, sizeof(float) * o->n, cudaMemcpyDeviceToHost, s));
+  if (adc_denom)
+    NPS_CUDA(cudaMemcpyAsync(adc_denom, o->adc_denom.p, sizeof(float) * o->n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  return NPS_OK;
+}
+
+int nps_gs_set_lr(nps_gs* o, const float* lr6) {
+  NPS_TRY(check_gs(o));
+  if (!lr6) return NPS_ERR_INVALID;
+  for (int k = 0; k < 6; ++k) o->lr[k] = lr6[k];
+  return NPS_OK;
+}
+
+int nps_gs_set_background(nps_gs* o, float r, float g, float b) {
+  NPS_TRY(check_gs(o));
+  o->bg[0] = r; o->bg[1] = g; o->bg[2] = b;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_set_targets(nps_gs* o, const float* rgba, uint32_t w, uint32_t h, uint32_t num_targets, int mem) {
+  NPS_TRY(check_gs(o));
+  if (!rgba || w == 0 || h == 0 || num_targets == 0 || w > 16 * 4096 || h > 16 * 4096) {
+    set_error("gs_set_targets: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  if (((uintptr_t)rgba & 15) != 0 && mem != NPS_MEM_HOST) {
+    set_error("gs_set_targets: device targets must be 16-byte aligned");
+    return NPS_ERR_INVALID;
+  }
+  const size_t bytes = sizeof(float) * 4 * (size_t)w * h * num_targets;
+  if (mem == NPS_MEM_DEVICE_BORROW) {
+    o->tgt = (const float4*)rgba;
+  } else {
+    NPS_TRY(o->tgt_own.ensure(bytes));
+    NPS_TRY(copy_in_gs(o->tgt_own.p, rgba, bytes, mem, o->ctx->stream));
+    o->tgt = o->tgt_own.as<float4>();
+  }
+  o->w = w;
+  o->h = h;
+  o->nt = num_targets;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint32_t* target_ids, uint32_t nv) {
+  NPS_TRY(check_gs(o));
+  if (!vp || !vp_inv || nv == 0 || nv > 1024) {
+    set_error("gs_set_views: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  std::vector<float> host((size_t)gsm::kViewRec * nv, 0.0f);
+  std::vector<uint32_t> ids(nv, 0);
+  for (uint32_t v = 0; v < nv; ++v) {
+    float* r = &host[(size_t)gsm::kViewRec * v];
+    std::memcpy(r, vp + 16 * v, 64);
+    std::memcpy(r + 16, vp_inv + 16 * v, 64);
+    // camera centre: VP^-1 (0, 0, 1, 0), dehomogenised
+    const float* iv = vp_inv + 16 * v;
+    const double cw = iv[11];
+    if (std::fabs(cw) < 1e-30) {
+      set_error("gs_set_views: view %u has no finite camera centre", v);
+      return NPS_ERR_INVALID;
+    }
+    r[32] = (float)(iv[8] / cw);
+    r[33] = (float)(iv[9] / cw);
+    r[34] = (float)(iv[10] / cw);
+    ids[v] = target_ids ? target_ids[v] : v;
+    if (o->nt && ids[v] >= o->nt) {
+      set_error("gs_set_views: target id %u out of range (%u targets)", ids[v], o->nt);
+      return NPS_ERR_INVALID;
+    }
+  }
+  NPS_TRY(o->views.ensure(sizeof(float) * host.size()));
+  NPS_TRY(o->tids.ensure(sizeof(uint32_t) * nv));
+  cudaStream_t s = o->ctx->stream;
+  NPS_CUDA(cudaMemcpyAsync(o->views.p, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice, s));
+  NPS_CUDA(cudaMemcpyAsync(o->tids.p, ids.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  o->nv = nv;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_forward(nps_gs* o, float* out_rgba) {
+  NPS_TRY(check_gs(o));
+  if (o->nv == 0 || o->w == 0) {
+    set_error("gs_forward: set_targets and set_views first");
+    return NPS_ERR_STATE;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n, nv = o->nv, W = o->w, H = o->h;
+  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const size_t M = (size_t)n * nv;
+  const size_t npix = (size_t)W * H * nv;
+  if (M >= (1ull << 31) || (uint64_t)num_tiles * nv >= (1ull << 31)) {
+    set_error("gs_forward: problem too large");
+    return NPS_ERR_INVALID;
+  }
+  NPS_TRY(o->recs.ensure(sizeof(gs::Rec) * (M + 1)));
+  NPS_TRY(o->counts.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->rects.ensure(sizeof(uint2) * (M + 1)));
+  NPS_TRY(o->dkeys.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->dvals.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->cnt_sorted.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->offsets.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->ranges.ensure(sizeof(uint32_t) * 2 * (size_t)num_tiles * nv));
+  NPS_TRY(o->img.ensure(sizeof(float4) * npix));
+  NPS_TRY(o->ncontrib.ensure(sizeof(uint32_t) * npix));
+  uint32_t* rstart = o->ranges.as<uint32_t>();
+  uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  NPS_CUDA(cudaMemsetAsync(o->ranges.p, 0, sizeof(uint32_t) * 2 * (size_t)num_tiles * nv, s));
+  uint32_t K = 0;
+  const uint32_t* vs = o->counts.as<uint32_t>();
+  if (M > 0) {
+    { StageTimer t_pre(o, ST_PRE);
+    gs::k_preprocess<<<div_up(M, 256), 256, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
+                                                     H, tiles_x, tiles_y, o->recs.as<gs::Rec>(),
+                                                     o->counts.as<uint32_t>(), o->rects.as<uint2>(),
+                                                     o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>());
+    NPS_CHECK_LAUNCH(); }
+    k_set_u32<<<1, 1, 0, s>>>(o->mcount.as<uint32_t>(), (uint32_t)M);
+    uint32_t *dk = nullptr, *dv = nullptr;
+    { StageTimer t(o, ST_DSORT);
+    NPS_TRY(radix_sort_u32(o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>(), o->mcount.as<uint32_t>(), (uint32_t)M, 32,
+                           o->sw_depth, s, &dk, &dv)); }
+    o->sorted_vals = dv;
+    gs::k_gather_counts<<<div_up(M, 256), 256, 0, s>>>(dv, o->counts.as<uint32_t>(), (uint32_t)M,
+                                                        o->cnt_sorted.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+    uint32_t* total = o->total.as<uint32_t>();
+    NPS_TRY(exclusive_scan_u32(o->cnt_sorted.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)M, total, o->sw_tile,
+                               s));
+    NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaStreamSynchronize(s));
+    if (K > o->pair_cap) {
+      const uint32_t cap = K + K / 4 + 4096;
+      NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
+      NPS_TRY(o->vals.ensure(sizeof(uint32_t) * (size_t)cap));
+      o->pair_cap = cap;
+    }
+    if (K > 0) {
+      { StageTimer t(o, ST_EMIT);
+      gs::k_emit<<<div_up(M, 256), 256, 0, s>>>(dv, o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(),
+                                                 o->rects.as<uint2>(), (uint32_t)M, n, tiles_x, num_tiles, o->pair_cap,
+                                                 o->keys.as<uint32_t>(), o->vals.as<uint32_t>());
+      NPS_CHECK_LAUNCH(); }
+      int bits = 1;
+      while ((1ull << bits) < (uint64_t)num_tiles * nv) ++bits;
+      uint32_t *ks = nullptr, *vv = nullptr;
+      { StageTimer t(o, ST_TSORT);
+      NPS_TRY(radix_sort_u32(o->keys.as<uint32_t>(), o->vals.as<uint32_t>(), total, o->pair_cap, bits, o->sw_tile, s,
+                             &ks, &vv)); }
+      { StageTimer t(o, ST_RANGES);
+      gs::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, o->pair_cap, rstart, rend);
+      NPS_CHECK_LAUNCH(); }
+      vs = vv;
+    }
+  }
+  o->K = K;
+  o->sorted_vals = vs;
+  const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  StageTimer t_fwd(o, ST_FWD);
+  gs::k_fwd<<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(o->recs.as<gs::Rec>(), vs, rstart, rend, W, H,
+                                                                 tiles_x, num_tiles, bg, o->img.as<float4>(),
+                                                                 o->ncontrib.as<uint32_t>());
+  NPS_CHECK_LAUNCH();
+  if (out_rgba) NPS_CUDA(cudaMemcpyAsync(out_rgba, o->img.p, sizeof(float4) * npix, cudaMemcpyDeviceToDevice, s));
+  o->fwd_valid = true;
+  o->loss_valid = false;
+  o->stats.pairs = K;
+  return NPS_OK;
+}
+
+int nps_gs_loss(nps_gs* o, float* loss3_host) {
+  NPS_TRY(check_gs(o));
+  if (!o->fwd_valid || !o->tgt) {
+    set_error("gs_loss: forward (and set_targets) first");
+    return NPS_ERR_STATE;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t W = o->w, H = o->h, nv = o->nv;
+  const size_t npix = (size_t)W * H * nv;
+  const dim3 grid(div_up(W, 16), div_up(H, 16), nv);
+  const uint32_t nblocks = grid.x * grid.y * grid.z;
+  NPS_TRY(o->maps.ensure(sizeof(float) * 9 * npix));
+  NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
+  NPS_TRY(o->dimg.ensure(sizeof(float4) * npix));
+  const float inv_norm = (float)(1.0 / (3.0 * (double)W * H * nv));
+  { StageTimer t(o, ST_LOSS);
+  gs::k_ssim_fwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H, o->lambda,
+                                               inv_norm, o->maps.as<float>(), o->partial.as<float>());
+  gs::k_ssim_bwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
+                                               o->maps.as<float>(), W, H, o->lambda, inv_norm, o->dimg.as<float4>());
+  gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->lambda, inv_norm,
+                                               o->loss.as<float>());
+  NPS_CHECK_LAUNCH(); }
+  if (loss3_host) {
+    NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaStreamSynchronize(s));
+  }
+  o->loss_valid = true;
+  return NPS_OK;
+}
+
+int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
+  NPS_TRY(check_gs(o));
+  if (!o->fwd_valid) {
+    set_error("gs_backward: forward first");
+    return NPS_ERR_STATE;
+  }
+  if (!dl_dimg && !o->loss_valid) {
+    set_error("gs_backward: no image gradient given and no fused loss computed");
+    return NPS_ERR_STATE;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n, nv = o->nv, W = o->w, H = o->h;
+  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const size_t M = (size_t)n * nv;
+  NPS_TRY(o->g2.ensure(sizeof(float) * gs::kG2 * (M + 1)));
+  NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
+  const uint32_t* rstart = o->ranges.as<uint32_t>();
+  const uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
+  { StageTimer t(o, ST_BWD);
+  gs::k_bwd<<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend,
+                                                                 W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
+                                                                 o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>());
+  NPS_CHECK_LAUNCH(); }
+  if (n > 0) {
+    StageTimer t(o, ST_PBWD);
+    gs::k_project_bwd<<<div_up(n, 128), 128, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
+                                                     H, o->recs.as<gs::Rec>(), o->counts.as<uint32_t>(),
+                                                     o->g2.as<float>(), o->grads.as<float>(), o->adc_grad.as<float>(),
+                                                     o->adc_denom.as<float>());
+    NPS_CHECK_LAUNCH();
+  }
+  return NPS_OK;
+}
+
+int nps_gs_adam(nps_gs* o) {
+  NPS_TRY(check_gs(o));
+  if (o->n == 0) return NPS_OK;
+  o->step += 1;
+  gs::AdamArgs a;
+  for (int k = 0; k < 6; ++k) a.lr[k] = o->lr[k];
+  a.b1 = 0.9f;
+  a.b2 = 0.999f;
+  a.eps = 1e-15f;
+  a.bc1 = (float)(1.0 - std::pow(0.9, (double)o->step));
+  a.bc2 = (float)(1.0 - std::pow(0.999, (double)o->step));
+  const uint32_t n4 = o->n * 16;
+  StageTimer t_adam(o, ST_ADAM);
+  gs::k_adam<<<div_up(n4, 256), 256, 0, o->ctx->stream>>>(o->params.as<float4>(), o->grads.as<float4>(),
+                                                           o->am.as<float4>(), o->av.as<float4>(), n4, a);
+  NPS_CHECK_LAUNCH();
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_train_step(nps_gs* o, float* loss3_host) {
+  NPS_TRY(nps_gs_forward(o, nullptr));
+  NPS_TRY(nps_gs_loss(o, loss3_host));
+  NPS_TRY(nps_gs_backward(o, nullptr));
+  NPS_TRY(nps_gs_adam(o));
+  return NPS_OK;
+}
+
+int nps_gs_read_image(nps_gs* o, float* rgba, float* dl_dimage) {
+  NPS_TRY(check_gs(o));
+  const size_t bytes = sizeof(float4) * (size_t)o->w * o->h * o->nv;
+  cudaStream_t s = o->ctx->stream;
+  if (rgba) {
+    if (!o->fwd_valid) {
+      set_error("gs_read_image: no forward state");
+      return NPS_ERR_STATE;
+    }
+    NPS_CUDA(cudaMemcpyAsync(rgba, o->img.p, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if (dl_dimage) {
+    if (!o->loss_valid) {
+      set_error("gs_read_image: no loss gradient");
+      return NPS_ERR_STATE;
+    }
+    NPS_CUDA(cudaMemcpyAsync(dl_dimage, o->dimg.p, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  NPS_CUDA(cudaStreamSynchronize(s));
+  return NPS_OK;
+}
+
+int nps_gs_buffers(nps_gs* o, float** params, float** grads, float** adam_m, float** adam_v, float** image,
+                   float** dl_dimage) {
+  NPS_TRY(check_gs(o));
+  if (params) *params = o->params.as<float>();
+  if (grads) *grads = o->grads.as<float>();
+  if (adam_m) *adam_m = o->am.as<float>();
+  if (adam_v) *adam_v = o->av.as<float>();
+  if (image) *image = o->img.as<float>();
+  if (dl_dimage) *dl_dimage = o->dimg.as<float>();
+  return NPS_OK;
+}
+
+int nps_gs_set_timing(nps_gs* o, int enable) {
+  NPS_TRY(check_gs(o));
+  o->timing = enable != 0;
+  return NPS_OK;
+}
+
+int nps_gs_stage_times(nps_gs* o, double* ms, uint64_t* calls, uint32_t n, int reset) {
+  NPS_TRY(check_gs(o));
+  if (!o->ev_used.empty()) NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  for (auto& u : o->ev_used) {
+    float t = 0.0f;
+    NPS_CUDA(cudaEventElapsedTime(&t, u.second.first, u.second.second));
+    o->stage_ms[u.first] += t;
+    o->stage_calls[u.first] += 1;
+    o->ev_pool.push_back(u.second.first);
+    o->ev_pool.push_back(u.second.second);
+  }
+  o->ev_used.clear();
+  for (uint32_t k = 0; k < n && k < ST_COUNT; ++k) {
+    if (ms) ms[k] = o->stage_ms[k];
+    if (calls) calls[k] = o->stage_calls[k];
+  }
+  if (reset)
+    for (int k = 0; k < 16; ++k) { o->stage_ms[k] = 0; o->stage_calls[k] = 0; }
+  return NPS_OK;
+}
+
+int nps_gs_stats(nps_gs* o, nps_stats* out) {
+  NPS_TRY(check_gs(o));
+  if (!out) return NPS_ERR_INVALID;
+  o->stats.step_count = o->step;
+  *out = o->stats;
+  return NPS_OK;
+}
+
+}  // extern "C"

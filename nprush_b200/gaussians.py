@@ -1,0 +1,200 @@
+"""3D Gaussian trainer over libnprush_cuda (the north-star model).
+
+Keeps the reference's fit-a-scene call pattern (GpuSplatOptimizerManager:
+write params -> write camera(s) -> set target(s) -> dispatch), for standard
+3D Gaussians with SH colour, batched over many views per call, plus the paired
+forward / backward entry points.
+
+Parameter record (64 floats): mean xyz, log-scale xyz, quaternion wxyz,
+opacity logit, pad, 16 x rgb SH coefficients (coefficient-major), pad.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import NPS_MEM_HOST, call
+from .splat import _ptr
+
+P = 64
+SH_C0 = 0.28209479177387814
+PARAM_FIELDS = {"mean": slice(0, 3), "log_scale": slice(3, 6), "quat": slice(6, 10), "opacity": slice(10, 11),
+                "sh": slice(12, 60)}
+
+
+def random_gaussians(n: int, seed: int, sh_degree: int = 3, sh_rest_std: float = 0.1) -> np.ndarray:
+    """Seeded scene: means U[-1,1]^3, log-scales N(-4, 0.5), random unit
+    quaternions, opacity logits N(0,1), RGB U[0,1] as SH DC, higher SH N(0, std)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros((n, P), np.float32)
+    p[:, 0:3] = rng.uniform(-1, 1, (n, 3))
+    p[:, 3:6] = rng.normal(-4.0, 0.5, (n, 3))
+    q = rng.normal(size=(n, 4))
+    p[:, 6:10] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    p[:, 10] = rng.normal(0, 1, n)
+    rgb = rng.random((n, 3))
+    p[:, 12:15] = (rgb - 0.5) / SH_C0
+    nb = (sh_degree + 1) ** 2
+    if nb > 1:
+        p[:, 15:12 + 3 * nb] = rng.normal(0, sh_rest_std, (n, 3 * (nb - 1)))
+    return p
+
+
+def view_records(vp, vp_inv) -> np.ndarray:
+    """The 48-float per-view record the kernels use: vp, vp_inv, camera centre."""
+    vp = np.asarray(vp, np.float32).reshape(-1, 16)
+    vpi = np.asarray(vp_inv, np.float32).reshape(-1, 16)
+    out = np.zeros((vp.shape[0], 48), np.float32)
+    out[:, :16] = vp
+    out[:, 16:32] = vpi
+    c = vpi[:, 8:12].astype(np.float64)
+    out[:, 32:35] = (c[:, :3] / c[:, 3:4]).astype(np.float32)
+    return out
+
+
+class GaussianTrainer:
+    LR_DEFAULT = (1.6e-4, 5e-3, 1e-3, 5e-2, 2.5e-3, 2.5e-3 / 20)
+
+    def __init__(self, capacity: int, sh_degree: int = 3, device: int = 0, params=None, lr=None):
+        self.capacity = int(capacity)
+        self.sh_degree = int(sh_degree)
+        self.device = device
+        self._ctx = _lib.context(device)
+        h = ctypes.c_void_p()
+        call("nps_gs_create", self._ctx, self.capacity, self.sh_degree, ctypes.byref(h))
+        self._h = h.value
+        self.count = 0
+        self._keep = []
+        if params is not None:
+            self.write_params(params)
+        self.set_lr(lr or self.LR_DEFAULT)
+
+    def write_params(self, params, first: int = 0):
+        p, mem, keep = _ptr(params)
+        n = (keep.numel() if mem != NPS_MEM_HOST else keep.size) // P
+        call("nps_gs_write_params", self._h, p, first, n, mem)
+        self.count = max(self.count, first + n)
+
+    def set_count(self, n: int):
+        call("nps_gs_set_count", self._h, n)
+        self.count = n
+
+    def set_lr(self, lr6):
+        a = np.ascontiguousarray(lr6, np.float32)
+        call("nps_gs_set_lr", self._h, a.ctypes.data)
+
+    def set_background(self, rgb):
+        call("nps_gs_set_background", self._h, float(rgb[0]), float(rgb[1]), float(rgb[2]))
+
+    def set_targets(self, rgba, borrow: bool = False):
+        """rgba: T x H x W x 4 float images (numpy or torch CUDA)."""
+        t, h, w = rgba.shape[0], rgba.shape[1], rgba.shape[2]
+        p, mem, keep = _ptr(rgba, borrow=borrow)
+        call("nps_gs_set_targets", self._h, p, w, h, t, mem)
+        self._keep = [keep] if borrow else []
+        self.width, self.height = w, h
+
+    def set_views(self, vp, vp_inv, target_ids=None):
+        vp = np.ascontiguousarray(vp, np.float32).reshape(-1, 16)
+        vpi = np.ascontiguousarray(vp_inv, np.float32).reshape(-1, 16)
+        ids = None
+        if target_ids is not None:
+            ids = np.ascontiguousarray(target_ids, np.uint32)
+        call("nps_gs_set_views", self._h, vp.ctypes.data, vpi.ctypes.data, None if ids is None else ids.ctypes.data,
+             vp.shape[0])
+        self.num_views = vp.shape[0]
+
+    def forward(self, out=None):
+        """Renders all views; out: optional torch CUDA tensor [V,H,W,4] (rgb, T)."""
+        p = None
+        if out is not None:
+            import torch
+            torch.cuda.current_stream(out.device).synchronize()
+            p = out.data_ptr()
+        call("nps_gs_forward", self._h, p)
+        if out is not None:
+            self.sync()
+
+    def loss(self, read_back: bool = True):
+        l3 = np.zeros(3, np.float32)
+        call("nps_gs_loss", self._h, l3.ctypes.data if read_back else None)
+        return tuple(float(x) for x in l3) if read_back else None
+
+    def backward(self, dl_dimage=None):
+        p = None
+        if dl_dimage is not None:
+            import torch
+            torch.cuda.current_stream(dl_dimage.device).synchronize()
+            p = dl_dimage.data_ptr()
+        call("nps_gs_backward", self._h, p)
+
+    def adam(self):
+        call("nps_gs_adam", self._h)
+
+    def train_step(self, read_loss: bool = False):
+        l3 = np.zeros(3, np.float32)
+        call("nps_gs_train_step", self._h, l3.ctypes.data if read_loss else None)
+        return tuple(float(x) for x in l3) if read_loss else None
+
+    def read_state(self):
+        n = self.count
+        out = {k: np.empty((n, P), np.float32) for k in ("params", "grads", "adam_m", "adam_v")}
+        ag = np.empty(n, np.float32)
+        ad = np.empty(n, np.float32)
+        call("nps_gs_read_state", self._h, out["params"].ctypes.data, out["grads"].ctypes.data,
+             out["adam_m"].ctypes.data, out["adam_v"].ctypes.data, ag.ctypes.data, ad.ctypes.data)
+        out["adc_grad"], out["adc_denom"] = ag, ad
+        return out
+
+    def read_image(self):
+        """(image [V,H,W,4], dL/dimage [V,H,W,4]) of the last forward / loss."""
+        shape = (self.num_views, self.height, self.width, 4)
+        img = np.empty(shape, np.float32)
+        dimg = np.empty(shape, np.float32)
+        call("nps_gs_read_image", self._h, img.ctypes.data, dimg.ctypes.data)
+        return img, dimg
+
+    def buffers(self) -> dict:
+        ptrs = [ctypes.c_void_p() for _ in range(6)]
+        call("nps_gs_buffers", self._h, *[ctypes.byref(p) for p in ptrs])
+        return dict(zip(("params", "grads", "adam_m", "adam_v", "image", "dl_dimage"), [p.value for p in ptrs]))
+
+    def stats(self) -> dict:
+        st = _lib.nps_stats()
+        call("nps_gs_stats", self._h, ctypes.byref(st))
+        return dict(pairs=st.pairs, step_count=st.step_count)
+
+    STAGES = ("preprocess", "depth_sort", "emit", "tile_sort", "ranges", "raster_fwd", "loss", "raster_bwd",
+              "project_bwd", "adam")
+
+    def set_timing(self, enable: bool):
+        call("nps_gs_set_timing", self._h, int(bool(enable)))
+
+    def stage_times(self, reset: bool = True) -> dict:
+        """{stage: (total ms, launches)} since the last reset."""
+        ms = np.zeros(len(self.STAGES), np.float64)
+        calls = np.zeros(len(self.STAGES), np.uint64)
+        call("nps_gs_stage_times", self._h, ms.ctypes.data, calls.ctypes.data, len(self.STAGES), int(reset))
+        return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(self.STAGES)}
+
+    def sync(self):
+        call("nps_sync", self._ctx)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            call("nps_gs_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def config2_cameras(n: int = 32, width: int = 800, height: int = 800, fov_deg: float = 50.0, radius: float = 4.0):
+    from .camera import sphere_cameras
+    return sphere_cameras(n, radius, math.radians(fov_deg), width / height)

@@ -98,11 +98,11 @@ def build(shader: str, n: int) -> Path:
 class RefModule:
     """ctypes handle on one compiled reference shader."""
 
-    def __init__(self, shader: str, n: int):
+    def __init__(self, shader: str, n: int, path=None):
         import sys
         if str(HERE) not in sys.path:
             sys.path.insert(0, str(HERE))
-        self.path = build(shader, n)
+        self.path = Path(path) if path is not None else build(shader, n)
         self.lib = ctypes.CDLL(str(self.path))
         self.lib.wg_bind.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         self.lib.wg_bind_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint]
@@ -112,6 +112,11 @@ class RefModule:
         self.lib.wg_size(ws)
         self.wgsize = tuple(ws)
         self._keep = []
+
+    @classmethod
+    def from_path(cls, path):
+        """Loads an already built module (no reference checkout needed)."""
+        return cls("", 0, path=path)
 
     def bind(self, binding: int, arr, group: int = 0):
         self._keep.append(arr)

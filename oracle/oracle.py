@@ -116,3 +116,71 @@ def bezier_adc(beziers, m, v, adam_t, no_kill, grad_accum, loss_accum, pixel_los
     lib().orc_bezier_adc(_p(beziers, F), _p(m, F), _p(v, F), ctypes.c_float(adam_t), ctypes.c_float(no_kill),
                          _p(grad_accum, F), _p(loss_accum, F), _p(pixel_loss, I), _p(_f32(vp), F),
                          _p(_f32(vpinv), F), beziers.shape[0])
+
+
+# ------------------------------------------------------------- Gaussians
+def _setup_gs():
+    L = lib()
+    L.orc_gs_loss_f64.restype = ctypes.c_double
+    return L
+
+
+def gs_forward(params, deg, views48, w, h, bg=(0.0, 0.0, 0.0)):
+    params = _f32(params)
+    views48 = _f32(views48)
+    nv = views48.shape[0]
+    img = np.zeros((nv, h, w, 4), np.float32)
+    nc = np.zeros((nv, h, w), np.uint32)
+    bgv = _f32(bg)
+    lib().orc_gs_forward(_p(params, F), params.shape[0], deg, _p(views48, F), nv, w, h, _p(bgv, F), _p(img, F),
+                         _p(nc, U))
+    return img, nc
+
+
+def gs_loss(img, targets, tids, lam=0.2):
+    img = _f32(img)
+    nv, h, w, _ = img.shape
+    targets = _f32(targets)
+    tids = np.ascontiguousarray(tids, np.uint32)
+    l3 = np.zeros(3, np.float32)
+    dimg = np.zeros_like(img)
+    lib().orc_gs_loss(_p(img, F), _p(targets, F), _p(tids, U), nv, w, h, ctypes.c_float(lam), _p(l3, F), _p(dimg, F))
+    return l3, dimg
+
+
+def gs_backward(params, deg, views48, w, h, img, ncontrib, dimg, bg=(0.0, 0.0, 0.0)):
+    params = _f32(params)
+    views48 = _f32(views48)
+    grads = np.zeros_like(params)
+    bgv = _f32(bg)
+    lib().orc_gs_backward(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h, _p(bgv, F),
+                          _p(_f32(img), F), _p(np.ascontiguousarray(ncontrib, np.uint32), U), _p(_f32(dimg), F),
+                          _p(grads, F))
+    return grads
+
+
+def gs_adam(params, grads, m, v, step, lr6):
+    lr = _f32(lr6)
+    lib().orc_gs_adam(_p(params, F), _p(_f32(grads), F), _p(m, F), _p(v, F), params.shape[0], step, _p(lr, F))
+
+
+def gs_loss_f64(params, deg, views48, w, h, targets, tids, lam=0.2, bg=(0.0, 0.0, 0.0)):
+    L = _setup_gs()
+    params = _f32(params)
+    views48 = _f32(views48)
+    tids = np.ascontiguousarray(tids, np.uint32)
+    return L.orc_gs_loss_f64(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h,
+                             _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam))
+
+
+def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=0.2, bg=(0.0, 0.0, 0.0)):
+    """FP64 central differences of the loss w.r.t. flat parameter indices."""
+    params = _f32(params)
+    views48 = _f32(views48)
+    tids = np.ascontiguousarray(tids, np.uint32)
+    pidx = np.ascontiguousarray(pidx, np.uint32)
+    out = np.zeros(len(pidx), np.float64)
+    lib().orc_gs_loss_cd(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h,
+                         _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam), _p(pidx, U),
+                         len(pidx), ctypes.c_double(h_rel), _p(out, D))
+    return out

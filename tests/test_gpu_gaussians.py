@@ -1,0 +1,141 @@
+"""GPU parity of the Gaussian trainer against the CPU oracle
+(oracle/nps_oracle_gs.cpp), whose analytic backward is itself checked against
+FP64 central differences (test_oracle_gs.py).
+
+Tolerances: rendered images 1e-5 absolute per channel; loss 1e-5 relative;
+dL/dimage 1e-6 absolute (its entries are ~1/(3HW)); parameter gradients 1e-4
+relative (relative L2 over all gradients, and per value against
+max(|ref|, 1e-3 * max|ref|) at the 99th percentile, since float atomics sum
+the per-pixel terms in another order); Adam 1e-6 relative.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+import oracle as orc  # noqa: E402
+from gs_scenes import gs_scene, gs_targets, gs_views  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def trainer_cls():
+    from nprush_b200 import build
+    build.build()
+    from nprush_b200.gaussians import GaussianTrainer
+    return GaussianTrainer
+
+
+def run_gpu(cls, p, deg, vp, vpi, tg, tids):
+    nv = vp.shape[0]
+    h, w = tg.shape[1], tg.shape[2]
+    t = cls(p.shape[0], sh_degree=deg, params=p)
+    t.set_targets(tg)
+    t.set_views(vp, vpi, tids)
+    img = torch.zeros((nv, h, w, 4), device="cuda")
+    t.forward(out=img)
+    l3 = t.loss()
+    t.backward()
+    st = t.read_state()
+    return t, img.cpu().numpy(), l3, st
+
+
+CASES = [
+    (1024, 64, 64, 0, ((0.0, 0.0, 4.0),), -4.0),
+    (3000, 96, 80, 3, ((0.0, 0.0, 4.0), (3.0, 1.0, 2.5)), -3.5),
+    (20000, 256, 256, 0, ((0.0, 0.0, 4.0),), -4.0),
+]
+
+
+@pytest.mark.parametrize("n,w,h,deg,eyes,lsm", CASES)
+def test_forward_loss_backward_match_oracle(trainer_cls, n, w, h, deg, eyes, lsm):
+    p = gs_scene(n, 11 + deg, deg=deg, log_scale_mean=lsm)
+    vp, vpi, views = gs_views(w, h, eyes)
+    nv = len(eyes)
+    tg = gs_targets(nv + 1, w, h, 5)
+    tids = np.arange(nv, dtype=np.uint32)[::-1].copy()  # views map to targets out of order
+    t, img, l3, st = run_gpu(trainer_cls, p, deg, vp, vpi, tg, tids)
+    rimg, rnc = orc.gs_forward(p, deg, views, w, h)
+    np.testing.assert_allclose(img, rimg, atol=1e-5, rtol=0)
+    rl3, rdimg = orc.gs_loss(rimg, tg, tids)
+    np.testing.assert_allclose(l3, rl3, rtol=1e-5, atol=1e-7)
+    img2, dimg = t.read_image()
+    np.testing.assert_array_equal(img2, img)
+    np.testing.assert_allclose(dimg[..., :3], rdimg[..., :3], atol=1e-6, rtol=1e-4)
+    rg = orc.gs_backward(p, deg, views, w, h, rimg, rnc, rdimg)
+    g = st["grads"]
+    used = np.r_[0:11, 12:12 + 3 * (deg + 1) ** 2]
+    a, b = g[:, used].astype(np.float64), rg[:, used].astype(np.float64)
+    rel_l2 = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel_l2 < 1e-4, rel_l2
+    scale = np.abs(b).max(axis=0, keepdims=True)
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * scale)
+    assert np.quantile(rel, 0.99) < 1e-3, np.quantile(rel, 0.99)
+    assert t.stats()["pairs"] > 0
+
+
+def test_gradients_match_fp64_central_differences(trainer_cls):
+    """Config-1 style check: 1024 Gaussians, 64x64, L1 + D-SSIM loss, CUDA
+    gradients against FP64 central differences (h = 1e-4 relative)."""
+    n, w, h, deg = 1024, 64, 64, 0
+    p = gs_scene(n, 2, deg=deg, log_scale_mean=-3.5)
+    vp, vpi, views = gs_views(w, h)
+    tg = gs_targets(1, w, h, 3)
+    tids = np.zeros(1, np.uint32)
+    t, img, l3, st = run_gpu(trainer_cls, p, deg, vp, vpi, tg, tids)
+    g = st["grads"]
+    rng = np.random.default_rng(1)
+    touched = np.nonzero(np.abs(g[:, 0]) > 0)[0]
+    gi = rng.choice(touched, min(40, len(touched)), replace=False)
+    fields = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 13, 14]
+    pidx = np.array([i * 64 + f for i in gi for f in fields], np.uint32)
+    cd = orc.gs_loss_cd(p, deg, views, w, h, tg, tids, pidx)
+    an = g.reshape(-1)[pidx].astype(np.float64)
+    rel = np.abs(an - cd) / np.maximum(np.abs(cd), 1e-3 * np.abs(cd).max())
+    assert np.median(rel) < 1e-4, np.median(rel)
+    assert np.quantile(rel, 0.95) < 1e-3, np.quantile(rel, 0.95)
+
+
+def test_adam_matches_oracle(trainer_cls):
+    n, w, h, deg = 2000, 64, 48, 3
+    p = gs_scene(n, 4, deg=deg, log_scale_mean=-3.5)
+    vp, vpi, views = gs_views(w, h, ((0.0, 0.0, 4.0), (0.0, 3.0, 2.5)))
+    tg = gs_targets(2, w, h, 9)
+    tids = np.arange(2, dtype=np.uint32)
+    t = trainer_cls(n, sh_degree=deg, params=p)
+    t.set_targets(tg)
+    t.set_views(vp, vpi, tids)
+    for _ in range(3):
+        t.train_step()
+    s0 = t.read_state()
+    t.forward()
+    t.loss()
+    t.backward()
+    g = t.read_state()["grads"]
+    t.adam()
+    s1 = t.read_state()
+    pp, mm, vv = s0["params"].copy(), s0["adam_m"].copy(), s0["adam_v"].copy()
+    orc.gs_adam(pp, g, mm, vv, 4, t.LR_DEFAULT)
+    np.testing.assert_allclose(s1["adam_m"], mm, rtol=1e-6, atol=1e-12)
+    np.testing.assert_allclose(s1["adam_v"], vv, rtol=1e-6, atol=1e-18)
+    np.testing.assert_allclose(s1["params"], pp, rtol=1e-6, atol=1e-7)
+
+
+def test_training_reduces_loss(trainer_cls):
+    """Fit a student to a teacher's renders: the loss must drop."""
+    n, w, h, deg = 4000, 96, 96, 1
+    teacher = gs_scene(n, 21, deg=deg, log_scale_mean=-3.2)
+    eyes = ((0.0, 0.0, 4.0), (4.0, 0.0, 0.5), (0.0, 4.0, 0.5), (-3.0, -1.0, 2.5))
+    vp, vpi, views = gs_views(w, h, eyes)
+    tgt_img, _ = orc.gs_forward(teacher, deg, views, w, h)
+    tg = tgt_img.copy()
+    tg[..., 3] = 1.0
+    student = gs_scene(n, 22, deg=deg, log_scale_mean=-3.2)
+    t = trainer_cls(n, sh_degree=deg, params=student)
+    t.set_targets(tg)
+    t.set_views(vp, vpi, np.arange(4, dtype=np.uint32))
+    first = t.train_step(read_loss=True)[0]
+    for _ in range(150):
+        last = t.train_step(read_loss=True)[0]
+    assert last < 0.7 * first, (first, last)
