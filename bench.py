@@ -123,6 +123,7 @@ def build_scene(dev):
     vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
     teacher = GaussianTrainer(N_TEACHER, sh_degree=SH_DEG, device=dev, params=random_gaussians(N_TEACHER, 11))
     tg = torch.zeros((CAMS, HEIGHT, WIDTH, 4), device=f"cuda:{dev}")
+    teacher.set_image_size(WIDTH, HEIGHT)
     for c0 in range(0, CAMS, VIEWS):
         teacher.set_views(vp[c0:c0 + VIEWS], vpi[c0:c0 + VIEWS])
         teacher.forward(out=tg[c0:c0 + VIEWS])

@@ -140,6 +140,8 @@ int nps_gs_set_lr(nps_gs* gs, const float* lr6);
 int nps_gs_set_background(nps_gs* gs, float r, float g, float b);
 /* Target images: num_targets x h x w x 4 floats (rgb used), resident on the device. */
 int nps_gs_set_targets(nps_gs* gs, const float* rgba, uint32_t width, uint32_t height, uint32_t num_targets, int mem);
+/* Image size for rendering without targets (set_targets sets it too). */
+int nps_gs_set_image_size(nps_gs* gs, uint32_t width, uint32_t height);
 /* Cameras of the next step: num_views view-projection matrices (+ inverses),
  * and for each the index of its target image (null = 0, 1, 2, ...). */
 int nps_gs_set_views(nps_gs* gs, const float* vp, const float* vp_inv, const uint32_t* target_ids, uint32_t num_views);

@@ -65,6 +65,7 @@ SIGNATURES = {
     "nps_gs_set_background": [P, F32, F32, F32],
     "nps_gs_set_targets": [P, P, U32, U32, U32, I32],
     "nps_gs_set_views": [P, P, P, P, U32],
+    "nps_gs_set_image_size": [P, U32, U32],
     "nps_gs_forward": [P, P],
     "nps_gs_loss": [P, P],
     "nps_gs_backward": [P, P],

