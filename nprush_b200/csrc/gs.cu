@@ -1182,9 +1182,14 @@ int nps_gs_adam(nps_gs* o) {
 
 int nps_gs_train_step(nps_gs* o, float* loss3_host) {
   NPS_TRY(nps_gs_forward(o, nullptr));
-  NPS_TRY(nps_gs_loss(o, loss3_host));
+  NPS_TRY(nps_gs_loss(o, nullptr));
   NPS_TRY(nps_gs_backward(o, nullptr));
   NPS_TRY(nps_gs_adam(o));
+  if (loss3_host) {
+    // the step's loss, read once the whole step (Adam included) has finished
+    NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, o->ctx->stream));
+    NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  }
   return NPS_OK;
 }
 
