@@ -4,14 +4,16 @@
 // One train step over V views is a fixed sequence of launches, each covering
 // all views at once:
 //   k_preprocess   (view, Gaussian): projection, EWA 2D covariance, conic,
-//                  3-sigma tile rectangle, SH colour, depth key
+//                  tile rectangle of the alpha >= 1/255 ellipse, SH colour,
+//                  depth key
 //   radix sort     32-bit depth keys of all (view, Gaussian) records
 //   k_gather_counts + scan + k_emit: (view * tiles + tile, record) pairs
 //                  written in depth order
 //   radix sort     stable by tile key -> every tile list is depth ordered
 //   k_ranges       tile list bounds
 //   k_fwd          one CTA per (tile, view): records staged in shared memory
-//                  256 at a time, front-to-back compositing with alpha
+//                  256 at a time, warps skip records whose footprint misses
+//                  their two pixel rows, front-to-back compositing with alpha
 //                  clamp 0.99, 1/255 skip and early termination at T < 1e-4
 //                  (block-wide vote ends the tile), final T and last
 //                  contributor stored per pixel (O(pixels) state, no
@@ -19,8 +21,8 @@
 //   k_ssim_fwd / k_ssim_bwd / k_loss_reduce: (1 - l) L1 + l (1 - SSIM), 11x11
 //                  Gaussian window (sigma 1.5), l = 0.2, and dL/dimage
 //   k_bwd          reverse traversal replaying transmittance from the final
-//                  T, per-Gaussian gradients summed over the warp with
-//                  shuffles, then over the CTA in shared memory, then one
+//                  T, per-Gaussian gradients summed over the warp by a
+//                  16-shuffle reduce-scatter, then over the CTA in shared memory, then one
 //                  global atomic per (tile, Gaussian, value)
 //   k_project_bwd  one thread per Gaussian looping over the views:
 //                  screen-space gradients -> parameter gradients (no
@@ -57,8 +59,41 @@ __constant__ float c_ssim_w[kSsimWin];
 struct Rec {  // projected record, 3 x float4 = 48 B
   float4 a;   // u, v, conic a, conic b
   float4 b;   // conic c, opacity, r, g
-  float4 c;   // b, depth, radius, 0
+  float4 c;   // b, depth, half-extents (x, y) of the alpha >= 1/255 ellipse box
 };
+
+// true if the Gaussian's alpha >= 1/255 box misses the warp's pixels
+// (rows y0, y0 + 1 and columns x0 .. x0 + 15)
+__device__ __forceinline__ bool warp_misses(float u, float v, float ex, float ey, float x0, float y0) {
+  return (u + ex < x0) || (u - ex > x0 + 15.0f) || (v + ey < y0) || (v - ey > y0 + 1.0f);
+}
+
+// Sum of 16 values over the warp by recursive halving (reduce-scatter): 16
+// shuffles instead of 5 per value.  On return, lanes 2k and 2k+1 hold the
+// warp total of value k.
+__device__ __forceinline__ float warp_sum16(float (&v)[16], uint32_t lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float send = b4 ? v[j] : v[j + 8], keep = b4 ? v[j + 8] : v[j];
+    v[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float send = b3 ? v[j] : v[j + 4], keep = b3 ? v[j + 4] : v[j];
+    v[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const float send = b2 ? v[j] : v[j + 2], keep = b2 ? v[j + 2] : v[j];
+    v[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  {
+    const float send = b1 ? v[0] : v[1], keep = b1 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
 
 __device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(-x)); }
 
@@ -86,14 +121,18 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
   r.a = make_float4(0, 0, 0, 0);
   r.b = make_float4(0, 0, 0, 0);
   r.c = make_float4(0, 0, 0, 0);
-  if (P.cw > kNear && P.det > 0.0f) {
-    const float mid = 0.5f * (P.A + P.C);
-    const float lam = mid + sqrtf(fmaxf(0.1f, mid * mid - P.det));
-    const float radius = ceilf(3.0f * sqrtf(lam));
-    const int x0 = max(0, min((int)tiles_x, (int)floorf((P.u - radius) / 16.0f)));
-    const int x1 = max(0, min((int)tiles_x, (int)floorf((P.u + radius) / 16.0f) + 1));
-    const int y0 = max(0, min((int)tiles_y, (int)floorf((P.v - radius) / 16.0f)));
-    const int y1 = max(0, min((int)tiles_y, (int)floorf((P.v + radius) / 16.0f) + 1));
+  const float op = sigmoidf(p[kOpacity]);
+  // A pixel contributes only where o * G >= 1/255, i.e. inside the ellipse
+  // d^T Sigma^-1 d <= t2 = 2 ln(255 o).  Its axis-aligned box, centre +-
+  // sqrt(t2 * Sigma_xx), +- sqrt(t2 * Sigma_yy), bounds the tile rectangle and
+  // the per-warp culling (1% margin on t2 for rounding).
+  if (P.cw > kNear && P.det > 0.0f && op * 255.0f > 1.0f) {
+    const float t2 = 2.0f * logf(255.0f * op) * 1.01f;
+    const float ex = sqrtf(t2 * P.A), ey = sqrtf(t2 * P.C);
+    const int x0 = max(0, min((int)tiles_x, (int)floorf((P.u - ex) / 16.0f)));
+    const int x1 = max(0, min((int)tiles_x, (int)floorf((P.u + ex) / 16.0f) + 1));
+    const int y0 = max(0, min((int)tiles_y, (int)floorf((P.v - ey) / 16.0f)));
+    const int y1 = max(0, min((int)tiles_y, (int)floorf((P.v + ey) / 16.0f) + 1));
     if (x1 > x0 && y1 > y0) {
       cnt = (uint32_t)((x1 - x0) * (y1 - y0));
       rect = make_uint2((uint32_t)x0 | ((uint32_t)x1 << 16), (uint32_t)y0 | ((uint32_t)y1 << 16));
@@ -110,10 +149,9 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
         col[1] += basis[k] * p[kSH + 3 * k + 1];
         col[2] += basis[k] * p[kSH + 3 * k + 2];
       }
-      const float op = sigmoidf(p[kOpacity]);
       r.a = make_float4(P.u, P.v, P.ca, P.cb);
       r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
-      r.c = make_float4(fmaxf(col[2], 0.0f), P.cw, radius, 0.0f);
+      r.c = make_float4(fmaxf(col[2], 0.0f), P.cw, ex, ey);
     }
   }
   recs[g] = r;
@@ -170,11 +208,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
                                                   float4* __restrict__ img, uint32_t* __restrict__ ncontrib) {
   __shared__ float4 s_a[kThreads];
   __shared__ float4 s_b[kThreads];
-  __shared__ float s_c[kThreads];
+  __shared__ float4 s_c[kThreads];
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
   const bool inside = px < W && py < H;
   const float fx = (float)px, fy = (float)py;
+  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * (tid >> 5));
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key], end = rend[key];
   float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
@@ -187,12 +226,14 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
       const Rec r = recs[vals[idx]];
       s_a[tid] = r.a;
       s_b[tid] = r.b;
-      s_c[tid] = r.c.x;
+      s_c[tid] = r.c;
     }
     __syncthreads();
     const uint32_t nb = min((uint32_t)kThreads, end - base);
     for (uint32_t j = 0; j < nb && !done; ++j) {
       const float4 a = s_a[j];
+      const float4 c4 = s_c[j];
+      if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
       const float4 b = s_b[j];
       const float dx = a.x - fx, dy = a.y - fy;
       const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
@@ -207,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
       const float w = alpha * T;
       C0 += b.z * w;
       C1 += b.w * w;
-      C2 += s_c[j] * w;
+      C2 += c4.x * w;
       T = test_T;
       last = base - start + j + 1;
     }
@@ -404,7 +445,7 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
                                                   const float4* __restrict__ dimg, float* __restrict__ g2) {
   __shared__ float4 s_a[kThreads];
   __shared__ float4 s_b[kThreads];
-  __shared__ float s_c[kThreads];
+  __shared__ float4 s_c[kThreads];
   __shared__ uint32_t s_g[kThreads];
   __shared__ float s_acc[kThreads][10];
   __shared__ uint32_t s_max;
@@ -412,6 +453,7 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
   const bool inside = px < W && py < H;
   const float fx = (float)px, fy = (float)py;
+  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * (tid >> 5));
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key], end = rend[key];
   float T = 1.0f, T_final = 1.0f;
@@ -443,7 +485,7 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
       const Rec r = recs[gg];
       s_a[tid] = r.a;
       s_b[tid] = r.b;
-      s_c[tid] = r.c.x;
+      s_c[tid] = r.c;
       s_g[tid] = gg;
     }
 #pragma unroll
@@ -451,14 +493,16 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
     __syncthreads();
     for (int j = (int)nb - 1; j >= 0; --j) {
       const uint32_t cur = bstart + (uint32_t)j - start;
-      float gv[10];
+      const float4 a = s_a[j];
+      const float4 c4 = s_c[j];
+      if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
+      float gv[16];
 #pragma unroll
-      for (int k = 0; k < 10; ++k) gv[k] = 0.0f;
+      for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
       bool contrib = false;
       if (inside && cur < last) {
-        const float4 a = s_a[j];
         const float4 b = s_b[j];
-        const float col[3] = {b.z, b.w, s_c[j]};
+        const float col[3] = {b.z, b.w, c4.x};
         const float dx = a.x - fx, dy = a.y - fy;
         const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
         if (power <= 0.0f) {
@@ -494,20 +538,9 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
         }
       }
       if (__any_sync(0xffffffffu, contrib)) {
-#pragma unroll
-        for (int k = 0; k < 10; ++k) {
-          float x = gv[k];
-          x += __shfl_xor_sync(0xffffffffu, x, 16);
-          x += __shfl_xor_sync(0xffffffffu, x, 8);
-          x += __shfl_xor_sync(0xffffffffu, x, 4);
-          x += __shfl_xor_sync(0xffffffffu, x, 2);
-          x += __shfl_xor_sync(0xffffffffu, x, 1);
-          gv[k] = x;
-        }
-        if (lane == 0) {
-#pragma unroll
-          for (int k = 0; k < 10; ++k) atomicAdd(&s_acc[j][k], gv[k]);
-        }
+        const float tot = warp_sum16(gv, lane);
+        const uint32_t k = lane >> 1;
+        if ((lane & 1) == 0 && k < 10) atomicAdd(&s_acc[j][k], tot);
       }
     }
     __syncthreads();

@@ -7,7 +7,8 @@
 // code:
 //   * standard 3D Gaussians: mean, log-scales, quaternion, opacity logit,
 //     real SH up to degree 3 (colour = SH + 0.5, clamped at 0);
-//   * EWA projection with +0.3 px^2 low-pass, 3-sigma tile rectangle, tiles of
+//   * EWA projection with +0.3 px^2 low-pass; tile rectangle from the box of
+//     the alpha >= 1/255 ellipse (Gaussians with 255 o <= 1 culled); tiles of
 //     16x16, per-tile lists ordered by (f32 view depth, index);
 //   * compositing with alpha = min(0.99, o * G), skip alpha < 1/255, stop
 //     before T would fall below 1e-4;
@@ -72,14 +73,15 @@ void preprocess(const T* params, uint32_t n, int deg, const float* view, uint32_
       g.col[c] = col < 0 ? (T)0 : col;
     }
     g.x0 = g.x1 = g.y0 = g.y1 = 0;
-    if (!(P.cw > (T)kNear && P.det > 0)) continue;
-    const T mid = (T)0.5 * (P.A + P.C);
-    const T lam = mid + std::sqrt(std::max((T)0.1, mid * mid - P.det));
-    const T radius = std::ceil((T)3 * std::sqrt(lam));
-    const int x0 = std::max(0, std::min((int)tx, (int)std::floor((P.u - radius) / (T)16)));
-    const int x1 = std::max(0, std::min((int)tx, (int)std::floor((P.u + radius) / (T)16) + 1));
-    const int y0 = std::max(0, std::min((int)ty, (int)std::floor((P.v - radius) / (T)16)));
-    const int y1 = std::max(0, std::min((int)ty, (int)std::floor((P.v + radius) / (T)16) + 1));
+    // footprint: the alpha >= 1/255 ellipse d^T Sigma^-1 d <= 2 ln(255 o)
+    // (1% margin), bounded by centre +- sqrt(t2 Sigma_xx), +- sqrt(t2 Sigma_yy)
+    if (!(P.cw > (T)kNear && P.det > 0 && g.op * (T)255 > (T)1)) continue;
+    const T t2 = (T)2 * std::log((T)255 * g.op) * (T)1.01;
+    const T ex = std::sqrt(t2 * P.A), ey = std::sqrt(t2 * P.C);
+    const int x0 = std::max(0, std::min((int)tx, (int)std::floor((P.u - ex) / (T)16)));
+    const int x1 = std::max(0, std::min((int)tx, (int)std::floor((P.u + ex) / (T)16) + 1));
+    const int y0 = std::max(0, std::min((int)ty, (int)std::floor((P.v - ey) / (T)16)));
+    const int y1 = std::max(0, std::min((int)ty, (int)std::floor((P.v + ey) / (T)16) + 1));
     if (!(x1 > x0 && y1 > y0)) continue;
     g.vis = true;
     g.x0 = x0; g.x1 = x1; g.y0 = y0; g.y1 = y1;
