@@ -117,6 +117,51 @@ typedef struct nps_stats {
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
 
+/* ========================================== Bezier strokes, reference semantics
+ * Record: 20 floats per curve (bezier_forward.wgsl:1-7): p0.xyz, width |
+ * p1.xyz, softness | p2.xyz, _ | p3.xyz, _ | r, g, b, a.  18 optimised
+ * parameters, fixed-point i32 gradients (bezier_backward.wgsl:536-558), Adam m,
+ * v 18 floats per curve, ADC accumulators grad_accum / loss_accum (1 float per
+ * curve each) and the 512 x 512 i32 pixel_loss map. */
+/* new GpuBezierOptimizerManager({numBeziers}) (GpuBezierOptimizerManager.ts:46-267). */
+int nps_bezier_opt_create(nps_ctx* ctx, uint32_t num_beziers, nps_bezier_opt** out);
+int nps_bezier_opt_destroy(nps_bezier_opt* opt);
+/* queue.writeBuffer(bezierBuffer, first*80, ...) (GpuBezierOptimizerManager.ts:102). */
+int nps_bezier_opt_write_params(nps_bezier_opt* opt, const float* beziers, uint32_t first, uint32_t count, int mem);
+int nps_bezier_opt_write_state(nps_bezier_opt* opt, const int32_t* grads, const float* adam_m, const float* adam_v,
+                               float adam_t, const float* grad_accum, const float* loss_accum,
+                               const int32_t* pixel_loss, int mem);
+int nps_bezier_opt_read_state(nps_bezier_opt* opt, float* beziers, int32_t* grads, float* adam_m, float* adam_v,
+                              float* adam_t, float* grad_accum, float* loss_accum, int32_t* pixel_loss);
+/* writeVPMatrix + writeVPInvMatrix (GpuBezierOptimizerManager.ts:269-288) for
+ * num_views views; the Adam step's offscreen kill and the ADC use the first. */
+int nps_bezier_opt_write_vp(nps_bezier_opt* opt, const float* vp, const float* vp_inv, uint32_t num_views);
+/* writeMode (:290), writeBgPenalty (:298), writeMaxWidth (:309),
+ * writeKillThresholds (:318), setAdcPeriod (:328), writeNoKill (:332). */
+int nps_bezier_opt_write_mode(nps_bezier_opt* opt, float mode);
+int nps_bezier_opt_write_bg_penalty(nps_bezier_opt* opt, float weight);
+int nps_bezier_opt_write_max_width(nps_bezier_opt* opt, float max_width);
+int nps_bezier_opt_write_kill_thresholds(nps_bezier_opt* opt, float alpha_thresh, float width_thresh);
+int nps_bezier_opt_set_adc_period(nps_bezier_opt* opt, uint32_t period);
+int nps_bezier_opt_write_no_kill(nps_bezier_opt* opt, int no_kill);
+/* setBackwardTarget(target, targetDepth, bg, bgDepth, normal, w, h)
+ * (GpuBezierOptimizerManager.ts:341-368): RGBA textures num_views*h*w*4
+ * floats, depth textures num_views*h*w floats. */
+int nps_bezier_opt_set_target(nps_bezier_opt* opt, const float* target_rgba, const float* target_depth,
+                              const float* bg_rgba, const float* bg_depth, const float* normal_rgba, uint32_t width,
+                              uint32_t height, uint32_t num_views, int mem);
+/* dispatch(encoder) (GpuBezierOptimizerManager.ts:370-406): backward over all
+ * views, Adam step (gradients / (w*h)), ADC every adc_period calls. */
+int nps_bezier_opt_dispatch(nps_bezier_opt* opt);
+/* The stages of dispatch separately; backward optionally writes the composite
+ * (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device). */
+int nps_bezier_opt_backward(nps_bezier_opt* opt, float* out_rgbd_device);
+int nps_bezier_opt_step(nps_bezier_opt* opt);
+int nps_bezier_opt_adc(nps_bezier_opt* opt);
+int nps_bezier_opt_buffers(nps_bezier_opt* opt, float** beziers, int32_t** grads, float** adam_m, float** adam_v,
+                           float** grad_accum, float** loss_accum, int32_t** pixel_loss);
+int nps_bezier_opt_stats(nps_bezier_opt* opt, nps_stats* out);
+
 /* ====================================== 3D Gaussians (north-star trainer)
  * No counterpart in the reference, which fits linear-parameter generalised
  * splats; this trainer keeps the reference's fit-a-scene call pattern

@@ -55,6 +55,25 @@ SIGNATURES = {
     "nps_splat_opt_render": [P, P, U32, U32, P, P],
     "nps_splat_opt_buffers": [P, PP, PP, PP, PP, PP],
     "nps_splat_opt_stats": [P, ctypes.POINTER(nps_stats)],
+    "nps_bezier_opt_create": [P, U32, PP],
+    "nps_bezier_opt_destroy": [P],
+    "nps_bezier_opt_write_params": [P, P, U32, U32, I32],
+    "nps_bezier_opt_write_state": [P, P, P, P, F32, P, P, P, I32],
+    "nps_bezier_opt_read_state": [P, P, P, P, P, P, P, P, P],
+    "nps_bezier_opt_write_vp": [P, P, P, U32],
+    "nps_bezier_opt_write_mode": [P, F32],
+    "nps_bezier_opt_write_bg_penalty": [P, F32],
+    "nps_bezier_opt_write_max_width": [P, F32],
+    "nps_bezier_opt_write_kill_thresholds": [P, F32, F32],
+    "nps_bezier_opt_set_adc_period": [P, U32],
+    "nps_bezier_opt_write_no_kill": [P, I32],
+    "nps_bezier_opt_set_target": [P, P, P, P, P, P, U32, U32, U32, I32],
+    "nps_bezier_opt_dispatch": [P],
+    "nps_bezier_opt_backward": [P, P],
+    "nps_bezier_opt_step": [P],
+    "nps_bezier_opt_adc": [P],
+    "nps_bezier_opt_buffers": [P, PP, PP, PP, PP, PP, PP, PP],
+    "nps_bezier_opt_stats": [P, ctypes.POINTER(nps_stats)],
     "nps_gs_create": [P, U32, U32, PP],
     "nps_gs_destroy": [P],
     "nps_gs_write_params": [P, P, U32, U32, I32],

@@ -1,0 +1,173 @@
+"""Python mirror of the reference's Bezier optimiser over libnprush_cuda.
+
+GpuBezierOptimizerManager  <->  src/lib/gpu/GpuBezierOptimizerManager.ts
+    constructor({numBeziers})            -> GpuBezierOptimizerManager(num_beziers=...)
+    writeVPMatrix / writeVPInvMatrix     -> write_vp_matrix / write_vp_inv_matrix
+    writeMode, writeBgPenalty, writeMaxWidth, writeKillThresholds,
+    setAdcPeriod, writeNoKill            -> same names in snake_case
+    setBackwardTarget(t, td, bg, bgd, n, w, h) -> set_backward_target(...)
+    dispatch(encoder)                    -> dispatch()
+Errors raise NpsError (the reference reports them asynchronously).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import NPS_MEM_DEVICE_BORROW, NPS_MEM_HOST, call
+from .splat import _ptr
+
+FLOATS_PER_BEZIER = 20
+PARAMS_PER_BEZIER = 18
+PIXEL_LOSS_SIZE = 512 * 512
+
+
+def reference_init(num_beziers: int, seed: int = 0) -> np.ndarray:
+    """Seeded version of the reference's initial curves
+    (GpuBezierOptimizerManager.ts:60-95): short random squiggles near the origin."""
+    rng = np.random.default_rng(seed)
+    n = num_beziers
+    b = np.zeros((n, 20), np.float32)
+    cx, cy = rng.random(n) * 2 - 1, rng.random(n) * 2 - 1
+    ln = 0.2 + rng.random(n) * 0.2
+    ang = rng.random(n) * math.pi * 2
+    dx, dy = np.cos(ang) * ln, np.sin(ang) * ln
+    jit = lambda: (rng.random(n) - 0.5) * 0.08  # noqa: E731
+    b[:, 0], b[:, 1], b[:, 2], b[:, 3] = cx - dx * 0.5, cy - dy * 0.5, (rng.random(n) * 2 - 1) * 0.3, 0.02
+    b[:, 4], b[:, 5], b[:, 6], b[:, 7] = cx - dx * 0.15 + jit(), cy - dy * 0.15 + jit(), (rng.random(n) * 2 - 1) * 0.3, 0.005
+    b[:, 8], b[:, 9], b[:, 10] = cx + dx * 0.15 + jit(), cy + dy * 0.15 + jit(), (rng.random(n) * 2 - 1) * 0.3
+    b[:, 12], b[:, 13], b[:, 14] = cx + dx * 0.5, cy + dy * 0.5, (rng.random(n) * 2 - 1) * 0.3
+    b[:, 16:19] = rng.random((n, 3))
+    b[:, 19] = 0.5
+    return b
+
+
+class GpuBezierOptimizerManager:
+    def __init__(self, num_beziers: int = 16, device: int = 0, init=None, seed: int = 0):
+        self.num_beziers = int(num_beziers)
+        self.num_params = self.num_beziers * PARAMS_PER_BEZIER
+        self._ctx = _lib.context(device)
+        h = ctypes.c_void_p()
+        call("nps_bezier_opt_create", self._ctx, self.num_beziers, ctypes.byref(h))
+        self._h = h.value
+        self._keep = []
+        self._vp = None
+        if init is None:
+            init = reference_init(self.num_beziers, seed)
+        if init is not False:
+            self.write_params(init)
+
+    def write_params(self, beziers, first: int = 0):
+        p, mem, keep = _ptr(beziers)
+        count = (keep.numel() if mem != NPS_MEM_HOST else keep.size) // FLOATS_PER_BEZIER
+        call("nps_bezier_opt_write_params", self._h, p, first, count, mem)
+
+    def write_state(self, grads=None, adam_m=None, adam_v=None, adam_t=0.0, grad_accum=None, loss_accum=None,
+                    pixel_loss=None):
+        ptrs = []
+        keep = []
+        for a, dt in ((grads, np.int32), (adam_m, np.float32), (adam_v, np.float32), (grad_accum, np.float32),
+                      (loss_accum, np.float32), (pixel_loss, np.int32)):
+            p, _, k = _ptr(a, dt)
+            ptrs.append(p)
+            keep.append(k)
+        call("nps_bezier_opt_write_state", self._h, ptrs[0], ptrs[1], ptrs[2], ctypes.c_float(adam_t), ptrs[3],
+             ptrs[4], ptrs[5], NPS_MEM_HOST)
+
+    def read_state(self):
+        n = self.num_beziers
+        out = dict(beziers=np.empty((n, 20), np.float32), grads=np.empty((n, 18), np.int32),
+                   adam_m=np.empty((n, 18), np.float32), adam_v=np.empty((n, 18), np.float32),
+                   grad_accum=np.empty(n, np.float32), loss_accum=np.empty(n, np.float32),
+                   pixel_loss=np.empty(PIXEL_LOSS_SIZE, np.int32))
+        t = ctypes.c_float()
+        call("nps_bezier_opt_read_state", self._h, out["beziers"].ctypes.data, out["grads"].ctypes.data,
+             out["adam_m"].ctypes.data, out["adam_v"].ctypes.data, ctypes.byref(t), out["grad_accum"].ctypes.data,
+             out["loss_accum"].ctypes.data, out["pixel_loss"].ctypes.data)
+        out["adam_t"] = t.value
+        return out
+
+    # ---- reference API
+    def write_vp(self, vp, vp_inv):
+        vp = np.ascontiguousarray(vp, np.float32).reshape(-1, 16)
+        vpi = np.ascontiguousarray(vp_inv, np.float32).reshape(-1, 16)
+        call("nps_bezier_opt_write_vp", self._h, vp.ctypes.data, vpi.ctypes.data, vp.shape[0])
+
+    def write_mode(self, mode: float = 0.0):
+        call("nps_bezier_opt_write_mode", self._h, float(mode))
+
+    def write_bg_penalty(self, weight: float = 0.0):
+        call("nps_bezier_opt_write_bg_penalty", self._h, float(weight))
+
+    def write_max_width(self, max_width: float = 0.0):
+        call("nps_bezier_opt_write_max_width", self._h, float(max_width))
+
+    def write_kill_thresholds(self, alpha_thresh: float = 0.0, width_thresh: float = 0.0):
+        call("nps_bezier_opt_write_kill_thresholds", self._h, float(alpha_thresh), float(width_thresh))
+
+    def set_adc_period(self, period: int):
+        call("nps_bezier_opt_set_adc_period", self._h, int(period))
+
+    def write_no_kill(self, no_kill: bool):
+        call("nps_bezier_opt_write_no_kill", self._h, int(bool(no_kill)))
+
+    def set_backward_target(self, target, target_depth, bg, bg_depth, normal, width: int, height: int,
+                            borrow: bool = False):
+        shape = tuple(target.shape)
+        views = 1 if len(shape) == 3 else shape[0]
+        ps, keep = [], []
+        mem = NPS_MEM_HOST
+        for a in (target, target_depth, bg, bg_depth, normal):
+            p, m, k = _ptr(a, borrow=borrow)
+            ps.append(p)
+            keep.append(k)
+            mem = m
+        call("nps_bezier_opt_set_target", self._h, *ps, width, height, views, mem)
+        self._keep = keep if borrow else []
+
+    def dispatch(self):
+        call("nps_bezier_opt_dispatch", self._h)
+
+    def backward(self, out_rgbd=None):
+        p = None
+        if out_rgbd is not None:
+            import torch
+            torch.cuda.current_stream(out_rgbd.device).synchronize()
+            p = out_rgbd.data_ptr()
+        call("nps_bezier_opt_backward", self._h, p)
+        if out_rgbd is not None:
+            call("nps_sync", self._ctx)
+
+    def step(self):
+        call("nps_bezier_opt_step", self._h)
+
+    def adc(self):
+        call("nps_bezier_opt_adc", self._h)
+
+    def stats(self) -> dict:
+        st = _lib.nps_stats()
+        call("nps_bezier_opt_stats", self._h, ctypes.byref(st))
+        return dict(pairs=st.pairs, adc_clones=st.adc_clones, spawns=st.reserved[0], step_count=st.step_count)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            call("nps_bezier_opt_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # camelCase aliases (the reference's method names)
+    writeMode = write_mode
+    writeBgPenalty = write_bg_penalty
+    writeMaxWidth = write_max_width
+    writeKillThresholds = write_kill_thresholds
+    setAdcPeriod = set_adc_period
+    writeNoKill = write_no_kill
+    setBackwardTarget = set_backward_target
