@@ -107,6 +107,26 @@ int nps_splat_opt_render(nps_splat_opt* opt, const float* vp, uint32_t width, ui
 int nps_splat_opt_buffers(nps_splat_opt* opt, float** splats, int32_t** grads, float** adam_m, float** adam_v,
                           float** grad_accum);
 
+/* ADC without device allocation.  No counterpart in the reference.  For
+ * callers that cannot let the library allocate device memory: applications
+ * that give their whole device-memory budget to their own arena or pool, and
+ * ones that share the GPU with latency-critical work (a render loop), where
+ * cudaMalloc / cudaFree may synchronise the device.  Runs the splat ADC
+ * (splat_adc.wgsl:28-87, same kernel as nps_splat_opt_adc) on caller-owned
+ * device buffers: splats N*16, adam_m / adam_v N*16, grad_accum N floats.
+ * Its scratch (dead-slot list + result word) is a fixed array compiled into
+ * the library: at most 262144 splats (larger N returns NPS_ERR_CAPACITY), and
+ * every GPU that loads the library holds that 1 MiB until exit.  Allocates
+ * nothing.  The first call on a device looks up the array's device address
+ * (with that device current), so make the first call before any stream
+ * capture.  Calls share the array, which keeps the last call's contents;
+ * calls that overlap on the GPU (different streams, or different host
+ * threads) race on it.  Runs on cuda_stream (null = legacy default stream) of
+ * the current device; clones_host (may be null) receives the number of clones
+ * and splits, which makes the call wait for the stream. */
+int nps_splat_adc_noalloc(float* splats, float* adam_m, float* adam_v, float* grad_accum, uint32_t num_splats,
+                          float adam_t, void* cuda_stream, uint32_t* clones_host);
+
 typedef struct nps_stats {
   uint64_t pairs;          /* (tile, primitive) pairs emitted by the last backward, all views */
   uint64_t pairs_capped;   /* pairs composited after the per-tile cap */

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1010,3 +1011,75 @@ int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t
 }
 
 }  // extern "C"
+
+// ============================================ ADC without device allocation
+// Some callers cannot let a library allocate device memory: an application
+// that hands its whole device-memory budget to its own arena or pool (a
+// cudaMalloc from the library would fail or break its accounting), or one that
+// shares the GPU with latency-critical work such as a render loop, where
+// cudaMalloc / cudaFree may synchronise the device and stall that work.
+// nps_splat_adc_noalloc runs the splat ADC (splat_adc.wgsl:28-87) on buffers
+// the caller owns, with the kernel's scratch (the dead-slot list and a result
+// word) in a fixed array compiled into the library.
+
+namespace {
+constexpr uint32_t kNoAllocMaxSplats = 262144;  // 1 MiB of dead-slot list
+// Scratch for nps_splat_adc_noalloc: [0, kNoAllocMaxSplats) dead-slot list,
+// then 64 words of results.  Every GPU that loads the library holds it until
+// exit.  Host code must not use this name as a device address (it is a host
+// stand-in); the address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) uint32_t g_adc_scratch[kNoAllocMaxSplats + 64];
+
+constexpr int kMaxDevices = 64;
+uint32_t* g_adc_scratch_dev[kMaxDevices] = {nullptr};
+std::mutex g_adc_scratch_mu;
+
+// The scratch array's device address on the current device (looked up once
+// per device, with that device current).
+int adc_scratch_address(uint32_t** out) {
+  int dev = 0;
+  NPS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("splat_adc_noalloc: device %d beyond %d supported", dev, kMaxDevices);
+    return NPS_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_adc_scratch_mu);
+  if (!g_adc_scratch_dev[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_adc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("splat_adc_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
+      return NPS_ERR_CUDA;
+    }
+    g_adc_scratch_dev[dev] = (uint32_t*)p;
+  }
+  *out = g_adc_scratch_dev[dev];
+  return NPS_OK;
+}
+}  // namespace
+
+extern "C" int nps_splat_adc_noalloc(float* splats, float* adam_m, float* adam_v, float* grad_accum, uint32_t n,
+                                     float adam_t, void* cuda_stream, uint32_t* clones_host) {
+  if (!splats || !adam_m || !adam_v || !grad_accum || n == 0) {
+    set_error("splat_adc_noalloc: null buffer or zero splats");
+    return NPS_ERR_INVALID;
+  }
+  if (n > kNoAllocMaxSplats) {
+    set_error("splat_adc_noalloc: %u splats exceed the fixed scratch of %u (use nps_splat_opt_adc)", n,
+              kNoAllocMaxSplats);
+    return NPS_ERR_CAPACITY;
+  }
+  uint32_t* scratch = nullptr;
+  NPS_TRY(adc_scratch_address(&scratch));
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  uint32_t* stats = scratch + kNoAllocMaxSplats;
+  // the dead-slot list is written before it is read; the result word is cleared
+  NPS_CUDA(cudaMemsetAsync(stats, 0, sizeof(uint32_t), s));
+  compat::k_adc<<<1, compat::kAdcThreads, 0, s>>>(splats, adam_m, adam_v, grad_accum, scratch, n, adam_t, stats);
+  NPS_CHECK_LAUNCH();
+  if (clones_host) {
+    NPS_CUDA(cudaMemcpyAsync(clones_host, stats, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaStreamSynchronize(s));
+  }
+  return NPS_OK;
+}
