@@ -178,6 +178,14 @@ int nps_bezier_opt_dispatch(nps_bezier_opt* opt);
 int nps_bezier_opt_backward(nps_bezier_opt* opt, float* out_rgbd_device);
 int nps_bezier_opt_step(nps_bezier_opt* opt);
 int nps_bezier_opt_adc(nps_bezier_opt* opt);
+/* Headless GpuBezierForwardPipelineManager.dispatch (GpuBezierForwardPipelineManager.ts:131-148,
+ * bezier_forward.wgsl:48-182): fp32 premultiplied composite of all curves
+ * (curve 0 in front) over bg_rgba (device h*w*4, null = cleared to 0), with
+ * an optional single-channel brush texture (device brush_h*brush_w, sampled
+ * bilinearly at level 0, u repeat / v clamp; null = analytic coverage only).
+ * out_rgba: device h*w*4. */
+int nps_bezier_opt_render(nps_bezier_opt* opt, const float* vp, uint32_t width, uint32_t height, const float* bg_rgba,
+                          const float* brush, uint32_t brush_w, uint32_t brush_h, float* out_rgba);
 int nps_bezier_opt_buffers(nps_bezier_opt* opt, float** beziers, int32_t** grads, float** adam_m, float** adam_v,
                            float** grad_accum, float** loss_accum, int32_t** pixel_loss);
 int nps_bezier_opt_stats(nps_bezier_opt* opt, nps_stats* out);

@@ -73,6 +73,7 @@ SIGNATURES = {
     "nps_bezier_opt_backward": [P, P],
     "nps_bezier_opt_step": [P],
     "nps_bezier_opt_adc": [P],
+    "nps_bezier_opt_render": [P, P, U32, U32, P, P, U32, U32, P],
     "nps_bezier_opt_buffers": [P, PP, PP, PP, PP, PP, PP, PP],
     "nps_bezier_opt_stats": [P, ctypes.POINTER(nps_stats)],
     "nps_gs_create": [P, U32, U32, PP],

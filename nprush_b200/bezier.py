@@ -141,6 +141,18 @@ class GpuBezierOptimizerManager:
         if out_rgbd is not None:
             call("nps_sync", self._ctx)
 
+    def render(self, vp, width: int, height: int, out, background=None, brush=None):
+        """Headless GpuBezierForwardPipelineManager.dispatch: out (torch CUDA
+        [H,W,4]) receives the premultiplied composite over `background`
+        (torch CUDA [H,W,4] or None = cleared); brush: torch CUDA [bh,bw]."""
+        import torch
+        torch.cuda.current_stream(out.device).synchronize()
+        vp = np.ascontiguousarray(vp, np.float32).reshape(16)
+        bgp = background.data_ptr() if background is not None else None
+        brp, bw, bh = (None, 0, 0) if brush is None else (brush.data_ptr(), brush.shape[1], brush.shape[0])
+        call("nps_bezier_opt_render", self._h, vp.ctypes.data, width, height, bgp, brp, bw, bh, out.data_ptr())
+        call("nps_sync", self._ctx)
+
     def step(self):
         call("nps_bezier_opt_step", self._h)
 

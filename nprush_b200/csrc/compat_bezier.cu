@@ -830,6 +830,143 @@ __global__ void __launch_bounds__(kAdcThreads) k_bz_adc(float* __restrict__ bz, 
   if (tid == 0 && stats) { stats[0] = clones; stats[1] = spawns; }
 }
 
+
+// ------------------------------------------------------------- display forward
+// bezier_forward.wgsl:48-182 headless: each curve covers its hull box +-
+// (width + softness), clamped to +-4 (SCREEN_BOUND) and culled if any control
+// point has w <= 0; the fragment walks the 16 segments, applies pressure,
+// coverage and (optionally) the brush alpha, and composites premultiplied,
+// front to back with curve 0 in front (reverse instance order in the
+// reference), over the given background.
+constexpr int kBRend = 20;
+
+__global__ void __launch_bounds__(256) k_bz_render_project(const float* __restrict__ bz, uint32_t n,
+                                                           const float* __restrict__ vp, uint32_t w, uint32_t h,
+                                                           const float* __restrict__ tabs, uint32_t tiles_x,
+                                                           uint32_t tiles_y, float* __restrict__ rec,
+                                                           uint32_t* __restrict__ counts, uint2* __restrict__ rects) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float b[20];
+  const float4* b4 = reinterpret_cast<const float4*>(bz + 20 * (size_t)i);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const float4 t = b4[q];
+    b[4 * q] = t.x; b[4 * q + 1] = t.y; b[4 * q + 2] = t.z; b[4 * q + 3] = t.w;
+  }
+  const float aspect = (float)w / (float)h;
+  float px[4], py[4];
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float4 cl = mulv(vp, b[4 * c], b[4 * c + 1], b[4 * c + 2], 1.0f);
+    px[c] = cl.x / cl.w * aspect;
+    py[c] = cl.y / cl.w;
+    ok = ok && !(cl.w <= 0.0f);
+  }
+  uint32_t cnt = 0;
+  uint2 rect = make_uint2(0u, 0u);
+  if (ok) {
+    const float width = fmaxf(b[3], 0.0001f), soft = fmaxf(b[7], 0.0001f), pad = width + soft;
+    const float SB = 4.0f;
+    const float x0 = fmaxf(fminf(fminf(px[0], px[1]), fminf(px[2], px[3])) - pad, -SB);
+    const float y0 = fmaxf(fminf(fminf(py[0], py[1]), fminf(py[2], py[3])) - pad, -SB);
+    const float x1 = fminf(fmaxf(fmaxf(px[0], px[1]), fmaxf(px[2], px[3])) + pad, SB);
+    const float y1 = fminf(fmaxf(fmaxf(py[0], py[1]), fmaxf(py[2], py[3])) + pad, SB);
+    float4* r4 = reinterpret_cast<float4*>(rec + (size_t)i * kBRend);
+    r4[0] = make_float4(px[0], py[0], px[1], py[1]);
+    r4[1] = make_float4(px[2], py[2], px[3], py[3]);
+    r4[2] = make_float4(x0, x1, y0, y1);
+    r4[3] = make_float4(width, soft, b[19], b[16]);
+    r4[4] = make_float4(b[17], b[18], 0.0f, 0.0f);
+    if (bin::tile_rect(tabs, tiles_x, tiles_y, x0, y0, x1, y1, &rect))
+      cnt = ((rect.x >> 16) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.y & 0xffffu));
+  }
+  counts[i] = cnt;
+  rects[i] = rect;
+}
+
+__device__ __forceinline__ float brush_sample(const float* brush, uint32_t bw, uint32_t bh, float u, float v) {
+  if (!brush) return 1.0f;
+  const float x = u * (float)bw - 0.5f, y = v * (float)bh - 0.5f;
+  const float fx = floorf(x), fy = floorf(y);
+  const float ax = x - fx, ay = y - fy;
+  const int ix = (int)fx, iy = (int)fy;
+  auto at = [&](int xx, int yy) {
+    xx = ((xx % (int)bw) + (int)bw) % (int)bw;
+    yy = min(max(yy, 0), (int)bh - 1);
+    return brush[(size_t)yy * bw + xx];
+  };
+  return (1 - ay) * ((1 - ax) * at(ix, iy) + ax * at(ix + 1, iy)) + ay * ((1 - ax) * at(ix, iy + 1) + ax * at(ix + 1, iy + 1));
+}
+
+__global__ void __launch_bounds__(256) k_bz_render_raster(const float* __restrict__ rec,
+                                                          const uint32_t* __restrict__ vals,
+                                                          const uint32_t* __restrict__ rstart,
+                                                          const uint32_t* __restrict__ rend, uint32_t w, uint32_t h,
+                                                          uint32_t tiles_x, const float4* __restrict__ bg,
+                                                          const float* __restrict__ brush, uint32_t bw, uint32_t bh,
+                                                          float4* __restrict__ out) {
+  __shared__ float sr[128][kBRend];
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, tid = threadIdx.x;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const bool inside = px < w && py < h;
+  const float aspect = (float)w / (float)h;
+  const float ppx = bin::pixel_px(px, w, aspect), ppy = bin::pixel_py(py, h);
+  const uint32_t key = ty * tiles_x + tx;
+  const uint32_t start = rstart[key], end = rend[key];
+  float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f, C3 = 0.0f;
+  for (uint32_t base = start; base < end; base += 128) {
+    __syncthreads();
+    const uint32_t nb = min(128u, end - base);
+    for (uint32_t e = tid; e < nb * 5; e += 256) {
+      const uint32_t k = e / 5, q = e - k * 5;
+      reinterpret_cast<float4*>(&sr[k][0])[q] = reinterpret_cast<const float4*>(rec + (size_t)vals[base + k] * kBRend)[q];
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < nb; ++j) {
+      const float* f = sr[j];
+      if (!(ppx >= f[8] && ppx < f[9] && ppy > f[10] && ppy <= f[11])) continue;
+      float md = 1e9f, mu = 0.0f, cross = 0.0f;
+      uint32_t mk = 1;
+      float2 prev = make_float2(f[0], f[1]);
+      for (uint32_t s = 1; s <= kNSeg; ++s) {
+        const float2 cur = bezier_at(f, (float)s / (float)kNSeg);
+        const float sx = cur.x - prev.x, sy = cur.y - prev.y;
+        const float len2 = fmaxf(sx * sx + sy * sy, 1e-8f);
+        const float u = clampf(((ppx - prev.x) * sx + (ppy - prev.y) * sy) / len2, 0.0f, 1.0f);
+        const float prx = prev.x + u * sx, pry = prev.y + u * sy;
+        const float dfx = ppx - prx, dfy = ppy - pry;
+        const float d = sqrtf(dfx * dfx + dfy * dfy);
+        if (d < md) {
+          md = d; mk = s; mu = u;
+          const float sl = sqrtf(len2);
+          cross = dfx * (-(sy / sl)) + dfy * (sx / sl);
+        }
+        prev = cur;
+      }
+      const float t = ((float)(mk - 1) + mu) / (float)kNSeg;
+      const float dt = t - 0.5f;
+      const float pressure = 1.0f - 4.0f * dt * dt;
+      const float lw = f[12] * pressure, ls = f[13] * pressure, lo = f[14] * pressure;
+      const float a_geom = 1.0f - smoothstepf(lw - ls, lw + ls, md);
+      const float bv = clampf(cross / fmaxf(lw + ls, 1e-6f) * 0.5f + 0.5f, 0.0f, 1.0f);
+      const float a = clampf(a_geom * brush_sample(brush, bw, bh, t, bv) * lo, 0.0f, 0.999f);
+      if (a < 0.001f) continue;
+      C0 += T * f[15] * a;
+      C1 += T * f[16] * a;
+      C2 += T * f[17] * a;
+      C3 += T * a;
+      T *= (1.0f - a);
+    }
+  }
+  if (inside) {
+    const size_t pix = (size_t)py * w + px;
+    const float4 g = bg ? bg[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+    out[pix] = make_float4(C0 + T * g.x, C1 + T * g.y, C2 + T * g.z, C3 + T * g.w);
+  }
+}
+
 }  // namespace bz
 }  // namespace nps
 
@@ -854,6 +991,10 @@ struct nps_bezier_opt {
   SortWork sw;
   uint32_t pair_cap = 0;
   nps_stats stats{};
+  // display render work buffers
+  DevBuf r_rec, r_counts, r_offsets, r_rects, r_total, r_cam, r_keys, r_vals, r_ranges, r_tabs;
+  SortWork r_sw;
+  uint32_t r_pair_cap = 0;
 };
 
 namespace {
@@ -923,7 +1064,9 @@ int nps_bezier_opt_destroy(nps_bezier_opt* o) {
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->lacc, &o->pixel_loss, &o->dead, &o->stat,
                     &o->views, &o->own[0], &o->own[1], &o->own[2], &o->own[3], &o->own[4], &o->fwd, &o->bwd,
                     &o->counts, &o->offsets, &o->rects, &o->total, &o->keys, &o->vals, &o->ranges, &o->tabs,
-                    &o->sw.hist, &o->sw.partial, &o->sw.keys_alt, &o->sw.vals_alt})
+                    &o->sw.hist, &o->sw.partial, &o->sw.keys_alt, &o->sw.vals_alt, &o->r_rec, &o->r_counts,
+                    &o->r_offsets, &o->r_rects, &o->r_total, &o->r_cam, &o->r_keys, &o->r_vals, &o->r_ranges,
+                    &o->r_tabs, &o->r_sw.hist, &o->r_sw.partial, &o->r_sw.keys_alt, &o->r_sw.vals_alt})
     b->release();
   delete o;
   return NPS_OK;
@@ -1200,6 +1343,66 @@ int nps_bezier_opt_dispatch(nps_bezier_opt* o) {
   NPS_TRY(nps_bezier_opt_step(o));
   o->step_count++;
   if (o->step_count % o->adc_period == 0) NPS_TRY(nps_bezier_opt_adc(o));  // GpuBezierOptimizerManager.ts:398-404
+  return NPS_OK;
+}
+
+int nps_bezier_opt_render(nps_bezier_opt* o, const float* vp, uint32_t w, uint32_t h, const float* bg_rgba,
+                          const float* brush, uint32_t brush_w, uint32_t brush_h, float* out_rgba) {
+  NPS_TRY(check_bz(o));
+  if (!vp || !out_rgba || w == 0 || h == 0 || w > 16 * 65535 || h > 16 * 65535 || (brush && (!brush_w || !brush_h))) {
+    set_error("bezier render: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n, tiles_x = div_up(w, 16), tiles_y = div_up(h, 16), num_tiles = tiles_x * tiles_y;
+  NPS_TRY(o->r_rec.ensure(sizeof(float) * bz::kBRend * n));
+  NPS_TRY(o->r_counts.ensure(sizeof(uint32_t) * n));
+  NPS_TRY(o->r_offsets.ensure(sizeof(uint32_t) * n));
+  NPS_TRY(o->r_rects.ensure(sizeof(uint2) * n));
+  NPS_TRY(o->r_total.ensure(16));
+  NPS_TRY(o->r_cam.ensure(64));
+  NPS_TRY(o->r_ranges.ensure(sizeof(uint32_t) * 2 * num_tiles));
+  NPS_TRY(o->r_tabs.ensure(sizeof(float) * 2 * (tiles_x + tiles_y)));
+  NPS_TRY(copy_in_bz(o->r_cam.p, vp, 64, NPS_MEM_HOST, s));
+  bin::k_tile_tables<<<1, 256, 0, s>>>(o->r_tabs.as<float>(), tiles_x, tiles_y, w, h);
+  bz::k_bz_render_project<<<div_up(n, 256), 256, 0, s>>>(o->params.as<float>(), n, o->r_cam.as<float>(), w, h,
+                                                          o->r_tabs.as<float>(), tiles_x, tiles_y,
+                                                          o->r_rec.as<float>(), o->r_counts.as<uint32_t>(),
+                                                          o->r_rects.as<uint2>());
+  NPS_CHECK_LAUNCH();
+  uint32_t* total = o->r_total.as<uint32_t>();
+  NPS_TRY(exclusive_scan_u32(o->r_counts.as<uint32_t>(), o->r_offsets.as<uint32_t>(), n, total, o->r_sw, s));
+  uint32_t K = 0;
+  NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  if (K > o->r_pair_cap || o->r_pair_cap == 0) {
+    const uint32_t cap = K + K / 4 + 4096;
+    NPS_TRY(o->r_keys.ensure(sizeof(uint32_t) * (size_t)cap));
+    NPS_TRY(o->r_vals.ensure(sizeof(uint32_t) * (size_t)cap));
+    o->r_pair_cap = cap;
+  }
+  uint32_t* rstart = o->r_ranges.as<uint32_t>();
+  uint32_t* rend = rstart + num_tiles;
+  NPS_CUDA(cudaMemsetAsync(rstart, 0, sizeof(uint32_t) * 2 * num_tiles, s));
+  const uint32_t* vs = o->r_vals.as<uint32_t>();
+  if (K > 0) {
+    bin::k_emit<<<div_up(n, 256), 256, 0, s>>>(o->r_counts.as<uint32_t>(), o->r_offsets.as<uint32_t>(),
+                                                o->r_rects.as<uint2>(), n, 1, tiles_x, num_tiles, o->r_pair_cap,
+                                                o->r_keys.as<uint32_t>(), o->r_vals.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+    int bits = 1;
+    while ((1ull << bits) < (uint64_t)num_tiles) ++bits;
+    uint32_t *ks = nullptr, *vv = nullptr;
+    NPS_TRY(radix_sort_u32(o->r_keys.as<uint32_t>(), o->r_vals.as<uint32_t>(), total, o->r_pair_cap, bits, o->r_sw, s,
+                           &ks, &vv));
+    bin::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, o->r_pair_cap, rstart, rend);
+    NPS_CHECK_LAUNCH();
+    vs = vv;
+  }
+  bz::k_bz_render_raster<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(o->r_rec.as<float>(), vs, rstart, rend, w, h, tiles_x,
+                                                                 (const float4*)bg_rgba, brush, brush_w, brush_h,
+                                                                 (float4*)out_rgba);
+  NPS_CHECK_LAUNCH();
   return NPS_OK;
 }
 

@@ -30,6 +30,7 @@
 #include <mutex>
 #include <vector>
 
+#include "binning.cuh"
 #include "common.cuh"
 #include "context.h"
 
@@ -656,14 +657,139 @@ __global__ void __launch_bounds__(kAdcThreads) k_adc(float* __restrict__ splats,
   if (tid == 0 && stats) stats[0] = clones;
 }
 
+
+// ------------------------------------------------------------- display forward
+// splat_forward.wgsl:42-156 (vertex quad, fragment alpha) headless: each splat
+// covers the screen rectangle centre +- R sqrt(cov) (top-left rule); its
+// fragments composite front to back with splat 0 in front (the reference
+// draws instances in reverse order with src-alpha blending).
+constexpr int kRend = 16;  // floats per render record
+
+__global__ void __launch_bounds__(256) k_render_project(const float* __restrict__ splats, uint32_t n,
+                                                        const float* __restrict__ vp, uint32_t w, uint32_t h,
+                                                        const float* __restrict__ tabs, uint32_t tiles_x,
+                                                        uint32_t tiles_y, float* __restrict__ rec,
+                                                        uint32_t* __restrict__ counts, uint2* __restrict__ rects) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s[16];
+  const float4* sp4 = reinterpret_cast<const float4*>(splats + 16 * (size_t)i);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float4 t = sp4[q];
+    s[4 * q] = t.x; s[4 * q + 1] = t.y; s[4 * q + 2] = t.z; s[4 * q + 3] = t.w;
+  }
+  const float aspect = (float)w / (float)h;
+  uint32_t cnt = 0;
+  uint2 rect = make_uint2(0u, 0u);
+  const float sx = fmaxf(s[3], 0.0001f), sy = fmaxf(s[12], 0.0001f), sz = fmaxf(s[15], 0.0001f);
+  const float safe_b = fmaxf(s[14], 0.0001f);
+  const float R = powf(15.0f / safe_b, 1.0f / s[13]);
+  const float4 clip = mulv(vp, s[0], s[1], s[2], 1.0f);
+  const float W = clip.w;
+  float4* r4 = reinterpret_cast<float4*>(rec + (size_t)i * kRend);
+  if (!(W < 0.1f)) {
+    f3 axw = quat_rotate(s[8], s[9], s[10], s[11], {1.0f, 0.0f, 0.0f});
+    f3 ayw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 1.0f, 0.0f});
+    f3 azw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 0.0f, 1.0f});
+    const float2 ax = project_axis(vp, axw, clip.x, clip.y, W, aspect);
+    const float2 ay = project_axis(vp, ayw, clip.x, clip.y, W, aspect);
+    const float2 az = project_axis(vp, azw, clip.x, clip.y, W, aspect);
+    const float m0x = ax.x * sx, m0y = ax.y * sx, m1x = ay.x * sy, m1y = ay.y * sy, m2x = az.x * sz, m2y = az.y * sz;
+    float cov00 = m0x * m0x + m1x * m1x + m2x * m2x;
+    const float cov01 = m0x * m0y + m1x * m1y + m2x * m2y;
+    float cov11 = m0y * m0y + m1y * m1y + m2y * m2y;
+    const float fs = 0.3f * (2.0f / (float)h);
+    cov00 += fs * fs;
+    cov11 += fs * fs;
+    const float det = cov00 * cov11 - cov01 * cov01;
+    const float inv_det = fabsf(det) < 1e-10f ? 0.0f : 1.0f / det;
+    const float A = cov11 * inv_det, B = -cov01 * inv_det, C = cov00 * inv_det;
+    const float ex = R * sqrtf(fmaxf(cov00, 1e-9f)), ey = R * sqrtf(fmaxf(cov11, 1e-9f));
+    const float cx = clip.x / W * aspect, cy = clip.y / W;
+    const float ld = fmaxf(W, 0.1f);
+    const float depth = clampf(1.0f - 0.1f / ld, 0.0f, 1.0f);
+    r4[0] = make_float4(cx, cy, cx - ex, cx + ex);
+    r4[1] = make_float4(cy - ey, cy + ey, A, B);
+    r4[2] = make_float4(C, s[13], s[14], s[7]);
+    r4[3] = make_float4(s[4], s[5], s[6], depth);
+    if (bin::tile_rect(tabs, tiles_x, tiles_y, cx - ex, cy - ey, cx + ex, cy + ey, &rect))
+      cnt = ((rect.x >> 16) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.y & 0xffffu));
+  }
+  counts[i] = cnt;
+  rects[i] = rect;
+}
+
+__global__ void __launch_bounds__(256) k_render_raster(const float* __restrict__ rec, const uint32_t* __restrict__ vals,
+                                                       const uint32_t* __restrict__ rstart,
+                                                       const uint32_t* __restrict__ rend, uint32_t w, uint32_t h,
+                                                       uint32_t tiles_x, float4* __restrict__ out_rgba,
+                                                       float4* __restrict__ out_depth) {
+  __shared__ float4 sr[256][4];
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, tid = threadIdx.x;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const bool inside = px < w && py < h;
+  const float aspect = (float)w / (float)h;
+  const float ppx = pixel_px(px, w, aspect), ppy = pixel_py(py, h);
+  const uint32_t key = ty * tiles_x + tx;
+  const uint32_t start = rstart[key], end = rend[key];
+  float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f, D = 0.0f;
+  for (uint32_t base = start; base < end; base += 256) {
+    __syncthreads();
+    if (base + tid < end) {
+      const float4* src = reinterpret_cast<const float4*>(rec + (size_t)vals[base + tid] * kRend);
+      sr[tid][0] = src[0]; sr[tid][1] = src[1]; sr[tid][2] = src[2]; sr[tid][3] = src[3];
+    }
+    __syncthreads();
+    const uint32_t nb = min(256u, end - base);
+    for (uint32_t j = 0; j < nb; ++j) {
+      const float4 a = sr[j][0], b = sr[j][1];
+      // pixel centre inside the quad (top-left rule)
+      if (!(ppx >= a.z && ppx < a.w && ppy > b.x && ppy <= b.y)) continue;
+      const float4 c = sr[j][2], d = sr[j][3];
+      const float dx = ppx - a.x, dy = ppy - a.y;
+      const float r2 = b.z * dx * dx + 2.0f * b.w * dx * dy + c.x * dy * dy;
+      const float r = sqrtf(fmaxf(r2, 0.0001f));
+      const float pw = -c.z * powf(r, c.y);
+      float al = pw > -15.0f ? expf(pw) * c.w : 0.0f;
+      al = clampf(al, 0.0f, 0.999f);
+      if (al < 0.001f) continue;
+      C0 += T * al * d.x;
+      C1 += T * al * d.y;
+      C2 += T * al * d.z;
+      D += T * al * d.w;
+      T *= (1.0f - al);
+    }
+  }
+  if (inside) {
+    const size_t pix = (size_t)py * w + px;
+    out_rgba[pix] = make_float4(C0 + T * 0.05f, C1 + T * 0.05f, C2 + T * 0.05f, 1.0f);
+    const float dd = D + T * 1.0f;
+    if (out_depth) out_depth[pix] = make_float4(dd, dd, dd, 1.0f);
+  }
+}
+
 }  // namespace compat
 }  // namespace nps
 
 // =================================================================== host side
 using namespace nps;
 
+// work buffers of the display render (kept by the optimiser, on its device)
+struct RenderWork {
+  DevBuf rec, counts, offsets, rects, total, cam, keys, vals, ranges, tabs;
+  SortWork sw;
+  uint32_t pair_cap = 0;
+  void release() {
+    for (DevBuf* b : {&rec, &counts, &offsets, &rects, &total, &cam, &keys, &vals, &ranges, &tabs, &sw.hist,
+                      &sw.partial, &sw.keys_alt, &sw.vals_alt})
+      b->release();
+  }
+};
+
 struct nps_splat_opt {
   nps_ctx* ctx = nullptr;
+  RenderWork* rw = nullptr;
   uint32_t n = 0;
   DevBuf params, grads, am, av, gacc;
   float adam_t = 0.0f;
@@ -752,6 +878,10 @@ int nps_splat_opt_destroy(nps_splat_opt* o) {
                     &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->sw.hist, &o->sw.partial,
                     &o->sw.keys_alt, &o->sw.vals_alt})
     b->release();
+  if (o->rw) {
+    o->rw->release();
+    delete o->rw;
+  }
   delete o;
   return NPS_OK;
 }
@@ -1002,15 +1132,68 @@ int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
   return NPS_OK;
 }
 
-int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
-                         float* out_depth) {
-  (void)vp; (void)w; (void)h; (void)out_rgba; (void)out_depth;
-  NPS_TRY(check_opt(o));
-  set_error("render: not implemented yet");
-  return NPS_ERR_STATE;
-}
-
 }  // extern "C"
+
+// ================================================================ render
+extern "C" int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
+                                    float* out_depth) {
+  NPS_TRY(check_opt(o));
+  if (!vp || !out_rgba || w == 0 || h == 0 || w > 16 * 65535 || h > 16 * 65535) {
+    set_error("splat render: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  if (!o->rw) o->rw = new RenderWork();
+  RenderWork& rw = *o->rw;
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n, tiles_x = div_up(w, 16), tiles_y = div_up(h, 16), num_tiles = tiles_x * tiles_y;
+  NPS_TRY(rw.rec.ensure(sizeof(float) * compat::kRend * n));
+  NPS_TRY(rw.counts.ensure(sizeof(uint32_t) * n));
+  NPS_TRY(rw.offsets.ensure(sizeof(uint32_t) * n));
+  NPS_TRY(rw.rects.ensure(sizeof(uint2) * n));
+  NPS_TRY(rw.total.ensure(16));
+  NPS_TRY(rw.cam.ensure(64));
+  NPS_TRY(rw.ranges.ensure(sizeof(uint32_t) * 2 * num_tiles));
+  NPS_TRY(rw.tabs.ensure(sizeof(float) * 2 * (tiles_x + tiles_y)));
+  NPS_TRY(copy_in(rw.cam.p, vp, 64, NPS_MEM_HOST, s));
+  bin::k_tile_tables<<<1, 256, 0, s>>>(rw.tabs.as<float>(), tiles_x, tiles_y, w, h);
+  compat::k_render_project<<<div_up(n, 256), 256, 0, s>>>(o->params.as<float>(), n, rw.cam.as<float>(), w, h,
+                                                           rw.tabs.as<float>(), tiles_x, tiles_y, rw.rec.as<float>(),
+                                                           rw.counts.as<uint32_t>(), rw.rects.as<uint2>());
+  NPS_CHECK_LAUNCH();
+  uint32_t* total = rw.total.as<uint32_t>();
+  NPS_TRY(exclusive_scan_u32(rw.counts.as<uint32_t>(), rw.offsets.as<uint32_t>(), n, total, rw.sw, s));
+  uint32_t K = 0;
+  NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  if (K > rw.pair_cap || rw.pair_cap == 0) {
+    const uint32_t cap = K + K / 4 + 4096;
+    NPS_TRY(rw.keys.ensure(sizeof(uint32_t) * (size_t)cap));
+    NPS_TRY(rw.vals.ensure(sizeof(uint32_t) * (size_t)cap));
+    rw.pair_cap = cap;
+  }
+  uint32_t* rstart = rw.ranges.as<uint32_t>();
+  uint32_t* rend = rstart + num_tiles;
+  NPS_CUDA(cudaMemsetAsync(rstart, 0, sizeof(uint32_t) * 2 * num_tiles, s));
+  const uint32_t* vs = rw.vals.as<uint32_t>();
+  if (K > 0) {
+    bin::k_emit<<<div_up(n, 256), 256, 0, s>>>(rw.counts.as<uint32_t>(), rw.offsets.as<uint32_t>(),
+                                                rw.rects.as<uint2>(), n, 1, tiles_x, num_tiles, rw.pair_cap,
+                                                rw.keys.as<uint32_t>(), rw.vals.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+    int bits = 1;
+    while ((1ull << bits) < (uint64_t)num_tiles) ++bits;
+    uint32_t *ks = nullptr, *vv = nullptr;
+    NPS_TRY(radix_sort_u32(rw.keys.as<uint32_t>(), rw.vals.as<uint32_t>(), total, rw.pair_cap, bits, rw.sw, s, &ks,
+                           &vv));
+    bin::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, rw.pair_cap, rstart, rend);
+    NPS_CHECK_LAUNCH();
+    vs = vv;
+  }
+  compat::k_render_raster<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(rw.rec.as<float>(), vs, rstart, rend, w, h, tiles_x,
+                                                                  (float4*)out_rgba, (float4*)out_depth);
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
 
 // ============================================ ADC without device allocation
 // Some callers cannot let a library allocate device memory: an application

@@ -162,6 +162,16 @@ class GpuSplatOptimizerManager:
         if out_rgbd is not None:
             self.sync()  # torch reads the image on its own stream
 
+    def render(self, vp, width: int, height: int, out_rgba, out_depth=None):
+        """Headless GpuSplatForwardPipelineManager.dispatch(enc, clear=true):
+        out_rgba / out_depth: torch CUDA [H,W,4] float tensors."""
+        import torch
+        torch.cuda.current_stream(out_rgba.device).synchronize()
+        vp = np.ascontiguousarray(vp, np.float32).reshape(16)
+        call("nps_splat_opt_render", self._h, vp.ctypes.data, width, height, out_rgba.data_ptr(),
+             None if out_depth is None else out_depth.data_ptr())
+        self.sync()
+
     def step(self):
         call("nps_splat_opt_step", self._h)
 

@@ -973,3 +973,176 @@ int orc_bezier_adc(float* beziers, float* m, float* v, float adam_t, float no_ki
 }
 
 }  // extern "C"
+
+// ============================================================ display forwards
+namespace {
+// Point-in-quad with the top-left rule: the quad is the axis-aligned screen
+// rectangle [x0, x1] x [y0, y1] (aspect-corrected, y up); left and top edges
+// are inside, right and bottom edges outside.
+inline bool in_quad(V2 p, float x0, float x1, float y0, float y1) {
+  return p.x >= x0 && p.x < x1 && p.y > y0 && p.y <= y1;
+}
+}  // namespace
+
+extern "C" {
+
+// splat_forward.wgsl:42-156 with GpuSplatForwardPipelineManager.dispatch(clear)
+// (GpuSplatForwardPipelineManager.ts:114-137), headless and in fp32: instances
+// are drawn in reverse index order with src-alpha blending, which equals
+// front-to-back compositing with splat 0 in front.  out_rgba / out_depth:
+// H x W x 4 (colour rgb + alpha; encoded depth in rgb + alpha).
+int orc_splat_render(const float* splats, uint32_t n, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
+                     float* out_depth) {
+  const float aspect = (float)w / (float)h;
+  struct Q { bool ok; float cx, cy, x0, x1, y0, y1, A, B, C, depth; };
+  std::vector<Q> q(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* s = splats + 16 * (size_t)i;
+    Q& o = q[i];
+    o.ok = false;
+    const float sx = std::fmax(s[3], 0.0001f), sy = std::fmax(s[12], 0.0001f), sz = std::fmax(s[15], 0.0001f);
+    const float safe_b = std::fmax(s[14], 0.0001f);
+    const float R = std::pow(15.0f / safe_b, 1.0f / s[13]);
+    V4 clip = mulv(vp, s[0], s[1], s[2], 1.0f);
+    const float W = clip.w;
+    if (W < 0.1f) continue;
+    V4 qq{s[8], s[9], s[10], s[11]};
+    V2 ax = project_axis(vp, quat_rotate(qq, {1, 0, 0}), clip.x, clip.y, W, aspect);
+    V2 ay = project_axis(vp, quat_rotate(qq, {0, 1, 0}), clip.x, clip.y, W, aspect);
+    V2 az = project_axis(vp, quat_rotate(qq, {0, 0, 1}), clip.x, clip.y, W, aspect);
+    const float m0x = ax.x * sx, m0y = ax.y * sx, m1x = ay.x * sy, m1y = ay.y * sy, m2x = az.x * sz, m2y = az.y * sz;
+    float cov00 = m0x * m0x + m1x * m1x + m2x * m2x;
+    float cov01 = m0x * m0y + m1x * m1y + m2x * m2y;
+    float cov11 = m0y * m0y + m1y * m1y + m2y * m2y;
+    const float fs = 0.3f * (2.0f / (float)h);
+    cov00 += fs * fs;
+    cov11 += fs * fs;
+    const float det = cov00 * cov11 - cov01 * cov01;
+    const float inv_det = std::fabs(det) < 1e-10f ? 0.0f : 1.0f / det;
+    o.A = cov11 * inv_det; o.B = -cov01 * inv_det; o.C = cov00 * inv_det;
+    const float ex = R * std::sqrt(std::fmax(cov00, 1e-9f)), ey = R * std::sqrt(std::fmax(cov11, 1e-9f));
+    o.cx = clip.x / W * aspect;
+    o.cy = clip.y / W;
+    o.x0 = o.cx - ex; o.x1 = o.cx + ex; o.y0 = o.cy - ey; o.y1 = o.cy + ey;
+    const float ld = std::fmax(W, 0.1f);
+    o.depth = clampf(1.0f - 0.1f / ld, 0.0f, 1.0f);
+    o.ok = true;
+  }
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long pl = 0; pl < (long)w * h; ++pl) {
+    const uint32_t px = (uint32_t)(pl % w), py = (uint32_t)(pl / w);
+    V2 p = pixel_to_p(px, py, w, h, aspect);
+    float T = 1.0f, C[3] = {0, 0, 0}, D = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+      const Q& o = q[i];
+      if (!o.ok || !in_quad(p, o.x0, o.x1, o.y0, o.y1)) continue;
+      const float* s = splats + 16 * (size_t)i;
+      const float dx = p.x - o.cx, dy = p.y - o.cy;
+      const float r2 = o.A * dx * dx + 2.0f * o.B * dx * dy + o.C * dy * dy;
+      const float r = std::sqrt(std::fmax(r2, 0.0001f));
+      const float pw = -s[14] * std::pow(r, s[13]);
+      float a = pw > -15.0f ? std::exp(pw) * s[7] : 0.0f;
+      a = clampf(a, 0.0f, 0.999f);
+      if (a < 0.001f) continue;
+      for (int c = 0; c < 3; ++c) C[c] += T * a * s[4 + c];
+      D += T * a * o.depth;
+      T *= (1.0f - a);
+    }
+    float* oc = out_rgba + 4 * (size_t)pl;
+    float* od = out_depth + 4 * (size_t)pl;
+    for (int c = 0; c < 3; ++c) oc[c] = C[c] + T * 0.05f;
+    oc[3] = 1.0f;
+    od[0] = od[1] = od[2] = D + T * 1.0f;
+    od[3] = 1.0f;
+  }
+  return 0;
+}
+
+// bezier_forward.wgsl:48-182 with GpuBezierForwardPipelineManager.dispatch
+// (GpuBezierForwardPipelineManager.ts:131-148), headless fp32, premultiplied
+// one / one-minus-src-alpha blending over `bg_rgba` (H x W x 4; the cleared
+// target is 0).  brush: optional single-channel texture bw x bh sampled
+// bilinearly at level 0 with u repeat / v clamp; null = coverage only.
+int orc_bezier_render(const float* bz, uint32_t n, const float* vp, uint32_t w, uint32_t h, const float* bg_rgba,
+                      const float* brush, uint32_t bw, uint32_t bh, float* out_rgba) {
+  const float aspect = (float)w / (float)h;
+  struct Q { bool ok; float p[8]; float x0, x1, y0, y1; };
+  std::vector<Q> q(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* b = bz + 20 * (size_t)i;
+    Q& o = q[i];
+    o.ok = false;
+    PC c[4];
+    for (int k = 0; k < 4; ++k) c[k] = project_center(vp, b + 4 * k, aspect);
+    if (c[0].w <= 0.0f || c[1].w <= 0.0f || c[2].w <= 0.0f || c[3].w <= 0.0f) continue;
+    for (int k = 0; k < 4; ++k) { o.p[2 * k] = c[k].x; o.p[2 * k + 1] = c[k].y; }
+    const float width = std::fmax(b[3], 0.0001f), soft = std::fmax(b[7], 0.0001f), pad = width + soft;
+    const float SB = 4.0f;
+    o.x0 = std::fmax(std::fmin(std::fmin(c[0].x, c[1].x), std::fmin(c[2].x, c[3].x)) - pad, -SB);
+    o.y0 = std::fmax(std::fmin(std::fmin(c[0].y, c[1].y), std::fmin(c[2].y, c[3].y)) - pad, -SB);
+    o.x1 = std::fmin(std::fmax(std::fmax(c[0].x, c[1].x), std::fmax(c[2].x, c[3].x)) + pad, SB);
+    o.y1 = std::fmin(std::fmax(std::fmax(c[0].y, c[1].y), std::fmax(c[2].y, c[3].y)) + pad, SB);
+    o.ok = true;
+  }
+  auto brush_at = [&](float u, float v) -> float {
+    if (!brush) return 1.0f;
+    float x = u * (float)bw - 0.5f, y = v * (float)bh - 0.5f;
+    float fx = std::floor(x), fy = std::floor(y);
+    float ax = x - fx, ay = y - fy;
+    auto at = [&](int ix, int iy) {
+      ix = ((ix % (int)bw) + (int)bw) % (int)bw;
+      iy = std::min(std::max(iy, 0), (int)bh - 1);
+      return brush[(size_t)iy * bw + ix];
+    };
+    int ix = (int)fx, iy = (int)fy;
+    return (1 - ay) * ((1 - ax) * at(ix, iy) + ax * at(ix + 1, iy)) + ay * ((1 - ax) * at(ix, iy + 1) + ax * at(ix + 1, iy + 1));
+  };
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long pl = 0; pl < (long)w * h; ++pl) {
+    const uint32_t px = (uint32_t)(pl % w), py = (uint32_t)(pl / w);
+    V2 p = pixel_to_p(px, py, w, h, aspect);
+    float T = 1.0f, C[4] = {0, 0, 0, 0};
+    for (uint32_t i = 0; i < n; ++i) {
+      const Q& o = q[i];
+      if (!o.ok || !in_quad(p, o.x0, o.x1, o.y0, o.y1)) continue;
+      const float* b = bz + 20 * (size_t)i;
+      V2 p0{o.p[0], o.p[1]}, p1{o.p[2], o.p[3]}, p2{o.p[4], o.p[5]}, p3{o.p[6], o.p[7]};
+      float min_d = 1e9f, min_u = 0.0f, cross = 0.0f;
+      uint32_t min_k = 1;
+      V2 prev = p0;
+      for (uint32_t s = 1; s <= N_SEG; ++s) {
+        V2 cur = bezier_at(p0, p1, p2, p3, (float)s / (float)N_SEG);
+        V2 seg{cur.x - prev.x, cur.y - prev.y};
+        float len2 = std::fmax(seg.x * seg.x + seg.y * seg.y, 1e-8f);
+        float u = clampf(((p.x - prev.x) * seg.x + (p.y - prev.y) * seg.y) / len2, 0.0f, 1.0f);
+        V2 pr{prev.x + u * seg.x, prev.y + u * seg.y};
+        V2 df{p.x - pr.x, p.y - pr.y};
+        float d = std::sqrt(df.x * df.x + df.y * df.y);
+        if (d < min_d) {
+          min_d = d; min_k = s; min_u = u;
+          float sl = std::sqrt(len2);
+          cross = df.x * (-(seg.y / sl)) + df.y * (seg.x / sl);
+        }
+        prev = cur;
+      }
+      float t = ((float)(min_k - 1) + min_u) / (float)N_SEG;
+      float dt = t - 0.5f;
+      float pressure = 1.0f - 4.0f * dt * dt;
+      float width = std::fmax(b[3], 0.0001f), soft = std::fmax(b[7], 0.0001f);
+      float lw = width * pressure, ls = soft * pressure, lo = b[19] * pressure;
+      float a_geom = 1.0f - smoothstepf(lw - ls, lw + ls, min_d);
+      float bv = clampf(cross / std::fmax(lw + ls, 1e-6f) * 0.5f + 0.5f, 0.0f, 1.0f);
+      float a = clampf(a_geom * brush_at(t, bv) * lo, 0.0f, 0.999f);
+      if (a < 0.001f) continue;
+      for (int c = 0; c < 3; ++c) C[c] += T * b[16 + c] * a;
+      C[3] += T * a;
+      T *= (1.0f - a);
+    }
+    const float* bgp = bg_rgba + 4 * (size_t)pl;
+    float* o = out_rgba + 4 * (size_t)pl;
+    for (int c = 0; c < 4; ++c) o[c] = C[c] + T * bgp[c];
+  }
+  return 0;
+}
+
+}  // extern "C"

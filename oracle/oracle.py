@@ -184,3 +184,23 @@ def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=
                          _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam), _p(pidx, U),
                          len(pidx), ctypes.c_double(h_rel), _p(out, D))
     return out
+
+
+# ------------------------------------------------------------ display forwards
+def splat_render(splats, vp, w, h):
+    splats = _f32(splats)
+    rgba = np.zeros((h, w, 4), np.float32)
+    dep = np.zeros((h, w, 4), np.float32)
+    lib().orc_splat_render(_p(splats, F), splats.shape[0], _p(_f32(vp), F), w, h, _p(rgba, F), _p(dep, F))
+    return rgba, dep
+
+
+def bezier_render(beziers, vp, w, h, bg=None, brush=None):
+    beziers = _f32(beziers)
+    bg = np.zeros((h, w, 4), np.float32) if bg is None else _f32(bg)
+    out = np.zeros((h, w, 4), np.float32)
+    bb = None if brush is None else _f32(brush)
+    bh, bw = (0, 0) if brush is None else brush.shape
+    lib().orc_bezier_render(_p(beziers, F), beziers.shape[0], _p(_f32(vp), F), w, h, _p(bg, F), _p(bb, F), bw, bh,
+                            _p(out, F))
+    return out
