@@ -146,6 +146,10 @@ def run_ours(args, rank, world):
         vp, vpi, tg, st = build_scene(dev)
         torch.cuda.synchronize()
         st.set_targets(tg, borrow=True)
+        st.set_graph(not args.no_graph)  # whole step captured as one CUDA graph
+        # stage timers are event-record nodes of the graph, so they must be on
+        # when the first (capturing) step runs
+        st.set_timing(not args.no_stage_timing)
         rng = np.random.default_rng(1234)
         sched = [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(args.warmup + args.steps + 4)]
         flush = torch.empty(64 * 1024 * 1024, device=f"cuda:{dev}")  # 256 MB > L2
@@ -160,7 +164,6 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        st.set_timing(not args.no_stage_timing)
         st.stage_times(reset=True)
         times, pairs = [], []
         with ClockSampler(dev) as clk:
@@ -330,6 +333,7 @@ def main():
     ap.add_argument("--views", type=int, default=None)
     ap.add_argument("--no-flush", action="store_true", help="do not flush L2 between timed steps")
     ap.add_argument("--no-stage-timing", action="store_true", help="no per-stage CUDA events")
+    ap.add_argument("--no-graph", action="store_true", help="launch the step eagerly instead of as a CUDA graph")
     args = ap.parse_args()
     global N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS
     if args.gaussians:
@@ -383,7 +387,8 @@ def main():
                                 "sphere cameras per step, L1 + 0.2 D-SSIM, Adam"), "gaussians": N_GAUSS, "resolution": [WIDTH, HEIGHT],
                    "views_per_step": VIEWS,
                    "l2": "not flushed" if args.no_flush else "flushed between timed steps (256 MB write)",
-                   "pairs_per_step": K, "parallelism": "replicas" if world > 1 else "single GPU"},
+                   "pairs_per_step": K, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "cuda_graph": not args.no_graph},
         "clocks": res["clocks"],
         "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"]},

@@ -227,8 +227,15 @@ int nps_gs_loss(nps_gs* gs, float* loss3);
 /* dl_dimage: device num_views*h*w*4 floats, or null for the fused loss gradient. */
 int nps_gs_backward(nps_gs* gs, const float* dl_dimage_device);
 int nps_gs_adam(nps_gs* gs);
-/* forward + loss + backward + Adam. */
+/* forward + loss + backward + Adam.  In graph mode the first call (and any
+ * call after the step's shape changed: Gaussian count, views, image size,
+ * targets) runs eagerly to size every buffer and then captures the whole
+ * step as one CUDA graph; later calls replay it with no host synchronisation
+ * inside the step.  A replay whose tile pairs exceed the captured capacity
+ * (25% above the capturing step's) skips its parameter update; the next call
+ * grows the capacity and recaptures (nps_stats.reserved[1] counts skips). */
 int nps_gs_train_step(nps_gs* gs, float* loss3);
+int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);

@@ -92,6 +92,7 @@ SIGNATURES = {
     "nps_gs_backward": [P, P],
     "nps_gs_adam": [P],
     "nps_gs_train_step": [P, P],
+    "nps_gs_set_graph": [P, I32],
     "nps_gs_read_image": [P, P, P],
     "nps_gs_buffers": [P, PP, PP, PP, PP, PP, PP],
     "nps_gs_stats": [P, ctypes.POINTER(nps_stats)],

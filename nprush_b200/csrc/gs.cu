@@ -693,8 +693,23 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
 // ------------------------------------------------------------ Adam
 struct AdamArgs {
   float lr[6];  // mean, log-scale, quat, opacity, SH DC, SH rest
-  float b1, b2, eps, bc1, bc2;
+  float b1, b2, eps;
 };
+
+// Step state in device memory (so that a captured graph advances it):
+// [0] step counter, [1] skip flag, [2], [3] bias corrections (f32 bits).
+// The step is skipped when the last forward produced more pairs than the
+// pair buffers hold (only possible in a captured graph, whose capacity is
+// fixed): parameters stay unchanged and the host grows the capacity.
+__global__ void k_adam_prep(uint32_t* st, const uint32_t* total, uint32_t cap) {
+  const bool skip = *total > cap;
+  st[1] = skip ? 1u : 0u;
+  if (skip) return;
+  const uint32_t step = st[0] + 1;
+  st[0] = step;
+  st[2] = __float_as_uint((float)(1.0 - pow(0.9, (double)step)));
+  st[3] = __float_as_uint((float)(1.0 - pow(0.999, (double)step)));
+}
 
 __device__ __forceinline__ float lr_of(const AdamArgs& a, int k) {
   return k < 3 ? a.lr[0] : k < 6 ? a.lr[1] : k < 10 ? a.lr[2] : k < 12 ? a.lr[3] : k < 15 ? a.lr[4] : a.lr[5];
@@ -703,9 +718,10 @@ __device__ __forceinline__ float lr_of(const AdamArgs& a, int k) {
 // one thread per float4 of the parameter record (16 per Gaussian)
 __global__ void __launch_bounds__(256) k_adam(float4* __restrict__ p, const float4* __restrict__ g,
                                               float4* __restrict__ m, float4* __restrict__ v, uint32_t n4,
-                                              AdamArgs a) {
+                                              AdamArgs a, const uint32_t* __restrict__ st) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n4) return;
+  if (t >= n4 || st[1] != 0u) return;
+  const float bc1 = __uint_as_float(st[2]), bc2 = __uint_as_float(st[3]);
   const int k0 = (int)(t & 15u) * 4;
   float4 pp = p[t], gg = g[t], mm = m[t], vv = v[t];
   float* pf = &pp.x;
@@ -719,7 +735,7 @@ __global__ void __launch_bounds__(256) k_adam(float4* __restrict__ p, const floa
     const float gr = gf[c];
     mf[c] = a.b1 * mf[c] + (1.0f - a.b1) * gr;
     vf[c] = a.b2 * vf[c] + (1.0f - a.b2) * gr * gr;
-    const float mh = mf[c] / a.bc1, vh = vf[c] / a.bc2;
+    const float mh = mf[c] / bc1, vh = vf[c] / bc2;
     pf[c] -= lr_of(a, k) * mh / (sqrtf(vh) + a.eps);
   }
   p[t] = pp;
@@ -762,8 +778,18 @@ struct nps_gs {
   const uint32_t* sorted_vals = nullptr;
   bool fwd_valid = false, loss_valid = false;
   nps_stats stats{};
+  // device step state (see k_adam_prep)
+  DevBuf stepst;
+  // CUDA-graph capture of the whole train step
+  bool graph_mode = false, capturing = false;
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t gdone = nullptr;
+  uint32_t* h_status = nullptr;  // pinned: pair count of the last graph replay
+  uint64_t gkey = 0;
+  uint32_t gcap = 0, skipped = 0;
   // optional per-stage timing with CUDA events on the context stream
   bool timing = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> gtimers;  // event nodes of the captured graph
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
   double stage_ms[16] = {0};
@@ -790,14 +816,17 @@ struct StageTimer {
   StageTimer(nps_gs* oo, int i) : o(oo), id(i) {
     if (o->timing) {
       e0 = ev_get(o);
-      cudaEventRecord(e0, o->ctx->stream);
+      cudaEventRecord(e0, o->ctx->stream);  // becomes an event-record node while capturing
     }
   }
   ~StageTimer() {
     if (o->timing) {
       cudaEvent_t e1 = ev_get(o);
       cudaEventRecord(e1, o->ctx->stream);
-      o->ev_used.push_back({id, {e0, e1}});
+      if (o->capturing)
+        o->gtimers.push_back({id, {e0, e1}});
+      else
+        o->ev_used.push_back({id, {e0, e1}});
     }
   }
 };
@@ -862,7 +891,7 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
   if ((rc = o->params.ensure(pb)) || (rc = o->grads.ensure(pb)) || (rc = o->am.ensure(pb)) ||
       (rc = o->av.ensure(pb)) || (rc = o->adc_grad.ensure(sizeof(float) * capacity)) ||
       (rc = o->adc_denom.ensure(sizeof(float) * capacity)) || (rc = o->total.ensure(16)) ||
-      (rc = o->mcount.ensure(16)) || (rc = o->loss.ensure(64))) {
+      (rc = o->mcount.ensure(16)) || (rc = o->loss.ensure(64)) || (rc = o->stepst.ensure(16))) {
     delete o;
     return rc;
   }
@@ -871,6 +900,8 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
   cudaMemsetAsync(o->adc_grad.p, 0, sizeof(float) * capacity, s);
   cudaMemsetAsync(o->adc_denom.p, 0, sizeof(float) * capacity, s);
   cudaMemsetAsync(o->loss.p, 0, 64, s);
+  cudaMemsetAsync(o->stepst.p, 0, 16, s);
+  cudaMemsetAsync(o->total.p, 0, 16, s);
   NPS_CUDA(cudaGetLastError());
   *out = o;
   return NPS_OK;
@@ -880,7 +911,11 @@ int nps_gs_destroy(nps_gs* o) {
   if (!o) return NPS_OK;
   cudaSetDevice(o->ctx->device);
   cudaStreamSynchronize(o->ctx->stream);
+  if (o->gexec) cudaGraphExecDestroy(o->gexec);
+  if (o->gdone) cudaEventDestroy(o->gdone);
+  if (o->h_status) cudaFreeHost(o->h_status);
   for (auto& u : o->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
+  for (auto& u : o->gtimers) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (cudaEvent_t e : o->ev_pool) cudaEventDestroy(e);
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
                     &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
@@ -923,6 +958,8 @@ int nps_gs_write_state(nps_gs* o, const float* adam_m, const float* adam_v, uint
   if (adam_m) NPS_TRY(copy_in_gs(o->am.p, adam_m, pb, mem, o->ctx->stream));
   if (adam_v) NPS_TRY(copy_in_gs(o->av.p, adam_v, pb, mem, o->ctx->stream));
   o->step = step;
+  const uint32_t st[4] = {step, 0u, 0u, 0u};
+  NPS_TRY(copy_in_gs(o->stepst.p, st, sizeof(st), NPS_MEM_HOST, o->ctx->stream));
   return NPS_OK;
 }
 
@@ -1036,8 +1073,13 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
   return NPS_OK;
 }
 
-int nps_gs_forward(nps_gs* o, float* out_rgba) {
-  NPS_TRY(check_gs(o));
+}  // extern "C"
+
+// Forward over all views.  Eager (capture == false): reads the pair count back
+// and grows the pair buffers to fit.  Captured (capture == true): no host
+// synchronisation; the pair buffers keep their capacity and the emit kernel
+// drops pairs beyond it (Adam then skips the step, see k_adam_prep).
+static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   if (o->nv == 0 || o->w == 0) {
     set_error("gs_forward: set_views and set_targets (or set_image_size) first");
     return NPS_ERR_STATE;
@@ -1085,15 +1127,17 @@ int nps_gs_forward(nps_gs* o, float* out_rgba) {
     uint32_t* total = o->total.as<uint32_t>();
     NPS_TRY(exclusive_scan_u32(o->cnt_sorted.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)M, total, o->sw_tile,
                                s));
-    NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    NPS_CUDA(cudaStreamSynchronize(s));
-    if (K > o->pair_cap) {
-      const uint32_t cap = K + K / 4 + 4096;
-      NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
-      NPS_TRY(o->vals.ensure(sizeof(uint32_t) * (size_t)cap));
-      o->pair_cap = cap;
+    if (!capture) {
+      NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      NPS_CUDA(cudaStreamSynchronize(s));
+      if (K > o->pair_cap || o->pair_cap == 0) {
+        const uint32_t cap = K + K / 4 + 4096;
+        NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
+        NPS_TRY(o->vals.ensure(sizeof(uint32_t) * (size_t)cap));
+        o->pair_cap = cap;
+      }
     }
-    if (K > 0) {
+    if (K > 0 || capture) {
       { StageTimer t(o, ST_EMIT);
       gs::k_emit<<<div_up(M, 256), 256, 0, s>>>(dv, o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(),
                                                  o->rects.as<uint2>(), (uint32_t)M, n, tiles_x, num_tiles, o->pair_cap,
@@ -1122,8 +1166,15 @@ int nps_gs_forward(nps_gs* o, float* out_rgba) {
   if (out_rgba) NPS_CUDA(cudaMemcpyAsync(out_rgba, o->img.p, sizeof(float4) * npix, cudaMemcpyDeviceToDevice, s));
   o->fwd_valid = true;
   o->loss_valid = false;
-  o->stats.pairs = K;
+  if (!capture) o->stats.pairs = K;
   return NPS_OK;
+}
+
+extern "C" {
+
+int nps_gs_forward(nps_gs* o, float* out_rgba) {
+  NPS_TRY(check_gs(o));
+  return gs_forward_impl(o, out_rgba, false);
 }
 
 int nps_gs_loss(nps_gs* o, float* loss3_host) {
@@ -1202,26 +1253,137 @@ int nps_gs_adam(nps_gs* o) {
   a.b1 = 0.9f;
   a.b2 = 0.999f;
   a.eps = 1e-15f;
-  a.bc1 = (float)(1.0 - std::pow(0.9, (double)o->step));
-  a.bc2 = (float)(1.0 - std::pow(0.999, (double)o->step));
   const uint32_t n4 = o->n * 16;
   StageTimer t_adam(o, ST_ADAM);
+  gs::k_adam_prep<<<1, 1, 0, o->ctx->stream>>>(o->stepst.as<uint32_t>(), o->total.as<uint32_t>(),
+                                               o->pair_cap ? o->pair_cap : 0xffffffffu);
   gs::k_adam<<<div_up(n4, 256), 256, 0, o->ctx->stream>>>(o->params.as<float4>(), o->grads.as<float4>(),
-                                                           o->am.as<float4>(), o->av.as<float4>(), n4, a);
+                                                           o->am.as<float4>(), o->av.as<float4>(), n4, a,
+                                                           o->stepst.as<uint32_t>());
   NPS_CHECK_LAUNCH();
   o->fwd_valid = false;
   return NPS_OK;
 }
 
-int nps_gs_train_step(nps_gs* o, float* loss3_host) {
-  NPS_TRY(nps_gs_forward(o, nullptr));
+}  // extern "C"
+
+static int gs_step_eager(nps_gs* o) {
+  NPS_TRY(gs_forward_impl(o, nullptr, false));
   NPS_TRY(nps_gs_loss(o, nullptr));
   NPS_TRY(nps_gs_backward(o, nullptr));
   NPS_TRY(nps_gs_adam(o));
+  return NPS_OK;
+}
+
+// Captures forward + loss + backward + Adam (no host synchronisation inside)
+// and instantiates it.  All buffers already have their sizes from an eager
+// step, so nothing is allocated while capturing.
+static int gs_capture(nps_gs* o) {
+  cudaStream_t s = o->ctx->stream;
+  if (o->gexec) {
+    cudaGraphExecDestroy(o->gexec);
+    o->gexec = nullptr;
+  }
+  for (auto& g : o->gtimers) {
+    o->ev_pool.push_back(g.second.first);
+    o->ev_pool.push_back(g.second.second);
+  }
+  o->gtimers.clear();
+  if (!o->h_status) NPS_CUDA(cudaMallocHost((void**)&o->h_status, 16));
+  if (!o->gdone) NPS_CUDA(cudaEventCreateWithFlags(&o->gdone, cudaEventDisableTiming));
+  NPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  o->capturing = true;
+  const uint32_t step_before = o->step;
+  int rc = gs_forward_impl(o, nullptr, true);
+  if (rc == NPS_OK) rc = nps_gs_loss(o, nullptr);
+  if (rc == NPS_OK) rc = nps_gs_backward(o, nullptr);
+  if (rc == NPS_OK) rc = nps_gs_adam(o);
+  if (rc == NPS_OK) {
+    const cudaError_t e = cudaMemcpyAsync(o->h_status, o->total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) {
+      set_error("graph capture: %s", cudaGetErrorString(e));
+      rc = NPS_ERR_CUDA;
+    }
+  }
+  o->capturing = false;
+  o->step = step_before;  // captured, not executed
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+  if (rc != NPS_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ee != cudaSuccess) {
+    set_error("graph capture failed: %s", cudaGetErrorString(ee));
+    return NPS_ERR_CUDA;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&o->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    o->gexec = nullptr;
+    set_error("graph instantiate failed: %s", cudaGetErrorString(ie));
+    return NPS_ERR_CUDA;
+  }
+  o->gcap = o->pair_cap;
+  return NPS_OK;
+}
+
+extern "C" {
+
+int nps_gs_set_graph(nps_gs* o, int enable) {
+  NPS_TRY(check_gs(o));
+  o->graph_mode = enable != 0;
+  if (!o->graph_mode && o->gexec) {
+    NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+    cudaGraphExecDestroy(o->gexec);
+    o->gexec = nullptr;
+  }
+  return NPS_OK;
+}
+
+int nps_gs_train_step(nps_gs* o, float* loss3_host) {
+  NPS_TRY(check_gs(o));
+  cudaStream_t s = o->ctx->stream;
+  if (!o->graph_mode) {
+    NPS_TRY(gs_step_eager(o));
+  } else {
+    // shape of the captured step; anything else in it reads device memory
+    const uint64_t key = ((uint64_t)o->n * 1000003ull) ^ ((uint64_t)o->nv << 40) ^ ((uint64_t)o->w << 20) ^
+                         ((uint64_t)o->h << 4) ^ (uint64_t)o->sh_deg ^ ((uint64_t)(uintptr_t)o->tgt << 7) ^
+                         ((uint64_t)__builtin_bit_cast(uint32_t, o->bg[0]) << 3) ^ (uint64_t)o->lambda * 131ull;
+    if (o->gexec) {
+      NPS_CUDA(cudaEventSynchronize(o->gdone));
+      if (o->h_status[0] > o->gcap) {
+        // the last replay overflowed its pair buffers: it skipped its update
+        o->skipped += 1;
+        o->gkey = 0;
+      }
+    }
+    if (!o->gexec || key != o->gkey) {
+      NPS_TRY(gs_step_eager(o));  // sizes every buffer (and is this call's step)
+      NPS_TRY(gs_capture(o));
+      o->gkey = key;
+    } else {
+      NPS_CUDA(cudaGraphLaunch(o->gexec, s));
+      NPS_CUDA(cudaEventRecord(o->gdone, s));
+      o->step += 1;
+      o->fwd_valid = false;
+      if (o->timing && !o->gtimers.empty()) {
+        // stage times of this replay, from the graph's event-record nodes
+        NPS_CUDA(cudaEventSynchronize(o->gdone));
+        for (auto& g : o->gtimers) {
+          float t = 0.0f;
+          NPS_CUDA(cudaEventElapsedTime(&t, g.second.first, g.second.second));
+          o->stage_ms[g.first] += t;
+          o->stage_calls[g.first] += 1;
+        }
+      }
+    }
+  }
   if (loss3_host) {
     // the step's loss, read once the whole step (Adam included) has finished
-    NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, o->ctx->stream));
-    NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+    NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaStreamSynchronize(s));
   }
   return NPS_OK;
 }
@@ -1291,6 +1453,11 @@ int nps_gs_stats(nps_gs* o, nps_stats* out) {
   NPS_TRY(check_gs(o));
   if (!out) return NPS_ERR_INVALID;
   o->stats.step_count = o->step;
+  o->stats.reserved[1] = o->skipped;
+  if (o->graph_mode && o->gexec && o->h_status) {
+    NPS_CUDA(cudaEventSynchronize(o->gdone));
+    o->stats.pairs = o->h_status[0];  // pairs of the last replay
+  }
   *out = o->stats;
   return NPS_OK;
 }

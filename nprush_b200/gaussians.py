@@ -138,6 +138,10 @@ class GaussianTrainer:
     def adam(self):
         call("nps_gs_adam", self._h)
 
+    def set_graph(self, enable: bool):
+        """Capture the train step as one CUDA graph after the first call."""
+        call("nps_gs_set_graph", self._h, int(bool(enable)))
+
     def train_step(self, read_loss: bool = False):
         l3 = np.zeros(3, np.float32)
         call("nps_gs_train_step", self._h, l3.ctypes.data if read_loss else None)
@@ -169,7 +173,7 @@ class GaussianTrainer:
     def stats(self) -> dict:
         st = _lib.nps_stats()
         call("nps_gs_stats", self._h, ctypes.byref(st))
-        return dict(pairs=st.pairs, step_count=st.step_count)
+        return dict(pairs=st.pairs, step_count=st.step_count, skipped_steps=st.reserved[1])
 
     STAGES = ("preprocess", "depth_sort", "emit", "tile_sort", "ranges", "raster_fwd", "loss", "raster_bwd",
               "project_bwd", "adam")

@@ -143,3 +143,38 @@ def test_training_reduces_loss(trainer_cls):
     for _ in range(150):
         last = t.train_step(read_loss=True)[0]
     assert last < 0.7 * first, (first, last)
+
+
+def test_graph_mode_matches_eager_and_recovers_from_overflow(trainer_cls):
+    """The captured train step equals the eager one (up to the order of float
+    atomics in the backward); a replay whose pairs overflow the captured
+    capacity skips its update and the next call recaptures."""
+    n, w, h, deg = 3000, 96, 80, 2
+    p = gs_scene(n, 40, deg=deg, log_scale_mean=-3.5)
+    eyes = ((0.0, 0.0, 4.0), (3.0, 1.0, 2.5))
+    vp, vpi, _ = gs_views(w, h, eyes)
+    tg = gs_targets(2, w, h, 41)
+    runs = []
+    for graph in (False, True):
+        t = trainer_cls(n, sh_degree=deg, params=p)
+        t.set_targets(tg)
+        t.set_views(vp, vpi, np.arange(2, dtype=np.uint32))
+        t.set_graph(graph)
+        losses = [t.train_step(read_loss=True)[0] for _ in range(6)]
+        runs.append((t.read_state()["params"], losses, t))
+    np.testing.assert_allclose(runs[1][1], runs[0][1], rtol=1e-4)
+    np.testing.assert_allclose(runs[1][0], runs[0][0], rtol=1e-3, atol=1e-5)
+    t = runs[1][2]
+    assert t.stats()["skipped_steps"] == 0
+    # much larger Gaussians: 3x the pairs with the same step shape
+    big = t.read_state()["params"].copy()
+    big[:, 3:6] += 1.5
+    t.write_params(big)
+    before = t.read_state()["params"].copy()
+    t.train_step()                       # replay: overflows, update skipped
+    after = t.read_state()["params"]
+    np.testing.assert_array_equal(after, before)
+    t.train_step()                       # detects the skip, eager step + recapture
+    assert t.stats()["skipped_steps"] == 1
+    t.train_step()                       # replay of the new graph
+    assert not np.array_equal(t.read_state()["params"], before)
