@@ -206,6 +206,9 @@ int nps_gs_set_count(nps_gs* gs, uint32_t count);
 int nps_gs_write_state(nps_gs* gs, const float* adam_m, const float* adam_v, uint32_t step, int mem);
 /* Host copies of the active records (null pointers skipped); adc_grad / adc_denom
  * are the accumulated view-space gradient norms and visibility counts. */
+/* ADC accumulators of the first `count` Gaussians (sum of view-space gradient
+ * norms, number of views that saw each one); null pointers are skipped. */
+int nps_gs_write_adc_stats(nps_gs* gs, const float* adc_grad, const float* adc_denom, int mem);
 int nps_gs_read_state(nps_gs* gs, float* params, float* grads, float* adam_m, float* adam_v, float* adc_grad,
                       float* adc_denom);
 /* Learning rates: mean, log-scale, quaternion, opacity logit, SH DC, SH rest. */
@@ -239,6 +242,17 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
+/* Adaptive density control (north-star plain ADC): prune Gaussians with
+ * opacity < prune_opacity; densify those whose average view-space gradient
+ * norm (accumulated by backward, averaged over the views that saw them) is
+ * >= grad_thresh — split into two (scales / 1.6, means drawn from the parent)
+ * if their largest scale exceeds split_scale, else clone — while the capacity
+ * allows; compacts records and Adam state, resets the accumulators.
+ * counts4 (host, may be null) = {count before, count after, densified, pruned}.
+ * The k-th call on a trainer samples split children with seed k. */
+int nps_gs_adc(nps_gs* gs, float grad_thresh, float split_scale, float prune_opacity, uint32_t* counts4);
+/* PSNR (dB) of each view of the last forward against its target, rgb in [0, 1]. */
+int nps_gs_psnr(nps_gs* gs, float* psnr_host);
 int nps_gs_buffers(nps_gs* gs, float** params, float** grads, float** adam_m, float** adam_v, float** image,
                    float** dl_dimage);
 int nps_gs_stats(nps_gs* gs, nps_stats* out);

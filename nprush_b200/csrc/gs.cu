@@ -743,6 +743,112 @@ __global__ void __launch_bounds__(256) k_adam(float4* __restrict__ p, const floa
   v[t] = vv;
 }
 
+
+// ------------------------------------------------------------ ADC (densify / prune)
+// Classify every Gaussian from its accumulated view-space gradient norm
+// (average over the views that saw it): prune if opacity < prune_opacity;
+// else densify if avg >= grad_thresh — split into two children (scales / 1.6,
+// means drawn from the parent Gaussian) when its largest scale exceeds
+// split_scale, otherwise clone it.  Outputs per Gaussian: 0 (pruned), 1 or 2.
+struct AdcParams {
+  float grad_thresh, split_scale, prune_opacity;
+  uint32_t seed;
+};
+
+// flags: bit 0 keep, bit 1 densify candidate, bit 2 split (else clone)
+__global__ void k_adc_classify(const float* __restrict__ params, const float* __restrict__ adc_grad,
+                               const float* __restrict__ adc_denom, uint32_t n, AdcParams a,
+                               uint32_t* __restrict__ flags, uint32_t* __restrict__ keep_cnt,
+                               uint32_t* __restrict__ cand_cnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* p = params + (size_t)i * kP;
+  const float op = 1.0f / (1.0f + expf(-p[kOpacity]));
+  uint32_t f = 0;
+  if (!(op < a.prune_opacity)) {
+    f = 1;
+    const float d = adc_denom[i];
+    const float avg = d > 0.0f ? adc_grad[i] / d : 0.0f;
+    if (avg >= a.grad_thresh) {
+      f |= 2;
+      const float ms = expf(fmaxf(fmaxf(p[3], p[4]), p[5]));
+      if (ms > a.split_scale) f |= 4;
+    }
+  }
+  flags[i] = f;
+  keep_cnt[i] = f & 1u;
+  cand_cnt[i] = (f >> 1) & 1u;
+}
+
+__global__ void k_adc_count(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ cand_rank, uint32_t n,
+                            uint32_t budget, uint32_t* __restrict__ out_cnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t f = flags[i];
+  out_cnt[i] = (f & 1u) ? ((f & 2u) && cand_rank[i] < budget ? 2u : 1u) : 0u;
+}
+
+// one thread per (Gaussian, float4 of its record)
+__global__ void k_adc_scatter(const float4* __restrict__ p_in, const float4* __restrict__ m_in,
+                              const float4* __restrict__ v_in, const uint32_t* __restrict__ flags,
+                              const uint32_t* __restrict__ out_cnt, const uint32_t* __restrict__ out_off, uint32_t n,
+                              AdcParams a, float4* __restrict__ p_out, float4* __restrict__ m_out,
+                              float4* __restrict__ v_out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 16) return;
+  const uint32_t i = t >> 4, q = t & 15;
+  const uint32_t c = out_cnt[i];
+  if (c == 0) return;
+  const uint32_t o = out_off[i];
+  const float4 pv = p_in[t];
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (c == 1) {
+    p_out[(size_t)o * 16 + q] = pv;
+    m_out[(size_t)o * 16 + q] = m_in[t];
+    v_out[(size_t)o * 16 + q] = v_in[t];
+    return;
+  }
+  const bool split = flags[i] & 4u;
+  if (!split) {
+    // clone: the original keeps its optimiser state, the copy starts at zero
+    p_out[(size_t)o * 16 + q] = pv;
+    m_out[(size_t)o * 16 + q] = m_in[t];
+    v_out[(size_t)o * 16 + q] = v_in[t];
+    p_out[(size_t)(o + 1) * 16 + q] = pv;
+    m_out[(size_t)(o + 1) * 16 + q] = z;
+    v_out[(size_t)(o + 1) * 16 + q] = z;
+    return;
+  }
+  // split: two children, fresh optimiser state
+  for (uint32_t ch = 0; ch < 2; ++ch) {
+    float4 r = pv;
+    if (q <= 1) {
+      float mean[3], ls[3];
+      gsm::adc_split_child(reinterpret_cast<const float*>(p_in + (size_t)i * 16), i, a.seed, ch, mean, ls);
+      if (q == 0) r = make_float4(mean[0], mean[1], mean[2], ls[0]);
+      else r = make_float4(ls[1], ls[2], pv.z, pv.w);
+    }
+    p_out[(size_t)(o + ch) * 16 + q] = r;
+    m_out[(size_t)(o + ch) * 16 + q] = z;
+    v_out[(size_t)(o + ch) * 16 + q] = z;
+  }
+}
+
+// per-view squared error of the last forward against the targets
+__global__ void k_sq_err(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                         const uint32_t* __restrict__ tids, uint32_t W, uint32_t H, double* __restrict__ acc) {
+  const uint32_t v = blockIdx.y;
+  const size_t np = (size_t)W * H;
+  double sum = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+    const float4 a = img[(size_t)v * np + i], b = tgt[(size_t)tids[v] * np + i];
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    sum += (double)(dx * dx + dy * dy + dz * dz);
+  }
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc + v, sum);
+}
+
 }  // namespace gs
 }  // namespace nps
 
@@ -780,6 +886,9 @@ struct nps_gs {
   nps_stats stats{};
   // device step state (see k_adam_prep)
   DevBuf stepst;
+  // ADC work: alternate parameter / optimiser buffers and flags
+  DevBuf p_alt, m_alt, v_alt, aflags, akeep, acand, akeep_off, acand_off, acnt, aoff, atot, psnr_acc;
+  uint32_t adc_seed = 0;
   // CUDA-graph capture of the whole train step
   bool graph_mode = false, capturing = false;
   cudaGraphExec_t gexec = nullptr;
@@ -790,6 +899,7 @@ struct nps_gs {
   // optional per-stage timing with CUDA events on the context stream
   bool timing = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> gtimers;  // event nodes of the captured graph
+  bool gpending = false;  // the last replay's timers are not collected yet
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
   double stage_ms[16] = {0};
@@ -816,13 +926,14 @@ struct StageTimer {
   StageTimer(nps_gs* oo, int i) : o(oo), id(i) {
     if (o->timing) {
       e0 = ev_get(o);
-      cudaEventRecord(e0, o->ctx->stream);  // becomes an event-record node while capturing
+      // External: while capturing, a plain record would only mark a dependency
+      cudaEventRecordWithFlags(e0, o->ctx->stream, o->capturing ? cudaEventRecordExternal : 0);
     }
   }
   ~StageTimer() {
     if (o->timing) {
       cudaEvent_t e1 = ev_get(o);
-      cudaEventRecord(e1, o->ctx->stream);
+      cudaEventRecordWithFlags(e1, o->ctx->stream, o->capturing ? cudaEventRecordExternal : 0);
       if (o->capturing)
         o->gtimers.push_back({id, {e0, e1}});
       else
@@ -917,6 +1028,9 @@ int nps_gs_destroy(nps_gs* o) {
   for (auto& u : o->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (auto& u : o->gtimers) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (cudaEvent_t e : o->ev_pool) cudaEventDestroy(e);
+  for (DevBuf* b : {&o->p_alt, &o->m_alt, &o->v_alt, &o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off,
+                    &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst})
+    b->release();
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
                     &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
                     &o->total, &o->mcount, &o->keys, &o->vals, &o->ranges, &o->img, &o->ncontrib, &o->maps,
@@ -960,6 +1074,14 @@ int nps_gs_write_state(nps_gs* o, const float* adam_m, const float* adam_v, uint
   o->step = step;
   const uint32_t st[4] = {step, 0u, 0u, 0u};
   NPS_TRY(copy_in_gs(o->stepst.p, st, sizeof(st), NPS_MEM_HOST, o->ctx->stream));
+  return NPS_OK;
+}
+
+int nps_gs_write_adc_stats(nps_gs* o, const float* adc_grad, const float* adc_denom, int mem) {
+  NPS_TRY(check_gs(o));
+  const size_t b = sizeof(float) * (size_t)o->n;
+  if (adc_grad) NPS_TRY(copy_in_gs(o->adc_grad.p, adc_grad, b, mem, o->ctx->stream));
+  if (adc_denom) NPS_TRY(copy_in_gs(o->adc_denom.p, adc_denom, b, mem, o->ctx->stream));
   return NPS_OK;
 }
 
@@ -1278,8 +1400,23 @@ static int gs_step_eager(nps_gs* o) {
 // Captures forward + loss + backward + Adam (no host synchronisation inside)
 // and instantiates it.  All buffers already have their sizes from an eager
 // step, so nothing is allocated while capturing.
+// Adds the stage times of the last graph replay (waits for it to finish).
+static int collect_graph_timers(nps_gs* o) {
+  if (!o->gpending) return NPS_OK;
+  o->gpending = false;
+  NPS_CUDA(cudaEventSynchronize(o->gdone));
+  for (auto& g : o->gtimers) {
+    float t = 0.0f;
+    NPS_CUDA(cudaEventElapsedTime(&t, g.second.first, g.second.second));
+    o->stage_ms[g.first] += t;
+    o->stage_calls[g.first] += 1;
+  }
+  return NPS_OK;
+}
+
 static int gs_capture(nps_gs* o) {
   cudaStream_t s = o->ctx->stream;
+  NPS_TRY(collect_graph_timers(o));
   if (o->gexec) {
     cudaGraphExecDestroy(o->gexec);
     o->gexec = nullptr;
@@ -1353,6 +1490,7 @@ int nps_gs_train_step(nps_gs* o, float* loss3_host) {
                          ((uint64_t)__builtin_bit_cast(uint32_t, o->bg[0]) << 3) ^ (uint64_t)o->lambda * 131ull;
     if (o->gexec) {
       NPS_CUDA(cudaEventSynchronize(o->gdone));
+      NPS_TRY(collect_graph_timers(o));
       if (o->h_status[0] > o->gcap) {
         // the last replay overflowed its pair buffers: it skipped its update
         o->skipped += 1;
@@ -1368,16 +1506,9 @@ int nps_gs_train_step(nps_gs* o, float* loss3_host) {
       NPS_CUDA(cudaEventRecord(o->gdone, s));
       o->step += 1;
       o->fwd_valid = false;
-      if (o->timing && !o->gtimers.empty()) {
-        // stage times of this replay, from the graph's event-record nodes
-        NPS_CUDA(cudaEventSynchronize(o->gdone));
-        for (auto& g : o->gtimers) {
-          float t = 0.0f;
-          NPS_CUDA(cudaEventElapsedTime(&t, g.second.first, g.second.second));
-          o->stage_ms[g.first] += t;
-          o->stage_calls[g.first] += 1;
-        }
-      }
+      // stage times are read at the next call (or by nps_gs_stage_times), so
+      // that replays queue back to back
+      o->gpending = o->timing && !o->gtimers.empty();
     }
   }
   if (loss3_host) {
@@ -1422,6 +1553,81 @@ int nps_gs_buffers(nps_gs* o, float** params, float** grads, float** adam_m, flo
   return NPS_OK;
 }
 
+int nps_gs_adc(nps_gs* o, float grad_thresh, float split_scale, float prune_opacity, uint32_t* counts4) {
+  NPS_TRY(check_gs(o));
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n;
+  if (n == 0) return NPS_OK;
+  const size_t pb = sizeof(float) * gsm::kP * (size_t)o->cap;
+  NPS_TRY(o->p_alt.ensure(pb));
+  NPS_TRY(o->m_alt.ensure(pb));
+  NPS_TRY(o->v_alt.ensure(pb));
+  for (DevBuf* b : {&o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off, &o->acnt, &o->aoff})
+    NPS_TRY(b->ensure(sizeof(uint32_t) * (n + 1)));
+  NPS_TRY(o->atot.ensure(16));
+  gs::AdcParams a{grad_thresh, split_scale, prune_opacity, ++o->adc_seed};
+  uint32_t* tot = o->atot.as<uint32_t>();
+  gs::k_adc_classify<<<div_up(n, 256), 256, 0, s>>>(o->params.as<float>(), o->adc_grad.as<float>(),
+                                                    o->adc_denom.as<float>(), n, a, o->aflags.as<uint32_t>(),
+                                                    o->akeep.as<uint32_t>(), o->acand.as<uint32_t>());
+  NPS_CHECK_LAUNCH();
+  NPS_TRY(exclusive_scan_u32(o->akeep.as<uint32_t>(), o->akeep_off.as<uint32_t>(), n, tot, o->sw_tile, s));
+  NPS_TRY(exclusive_scan_u32(o->acand.as<uint32_t>(), o->acand_off.as<uint32_t>(), n, tot + 1, o->sw_tile, s));
+  uint32_t h[2] = {0, 0};
+  NPS_CUDA(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  const uint32_t kept = h[0], cands = h[1];
+  const uint32_t budget = o->cap > kept ? o->cap - kept : 0;  // densify the first candidates that fit
+  gs::k_adc_count<<<div_up(n, 256), 256, 0, s>>>(o->aflags.as<uint32_t>(), o->acand_off.as<uint32_t>(), n, budget,
+                                                 o->acnt.as<uint32_t>());
+  NPS_TRY(exclusive_scan_u32(o->acnt.as<uint32_t>(), o->aoff.as<uint32_t>(), n, tot + 2, o->sw_tile, s));
+  uint32_t nn = 0;
+  NPS_CUDA(cudaMemcpyAsync(&nn, tot + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  gs::k_adc_scatter<<<div_up((size_t)n * 16, 256), 256, 0, s>>>(
+      o->params.as<float4>(), o->am.as<float4>(), o->av.as<float4>(), o->aflags.as<uint32_t>(),
+      o->acnt.as<uint32_t>(), o->aoff.as<uint32_t>(), n, a, o->p_alt.as<float4>(), o->m_alt.as<float4>(),
+      o->v_alt.as<float4>());
+  NPS_CHECK_LAUNCH();
+  NPS_CUDA(cudaStreamSynchronize(s));
+  std::swap(o->params, o->p_alt);
+  std::swap(o->am, o->m_alt);
+  std::swap(o->av, o->v_alt);
+  o->gkey = 0;  // a captured step holds the old buffers and count
+  NPS_CUDA(cudaMemsetAsync(o->adc_grad.p, 0, sizeof(float) * o->cap, s));
+  NPS_CUDA(cudaMemsetAsync(o->adc_denom.p, 0, sizeof(float) * o->cap, s));
+  if (counts4) {
+    counts4[0] = n;
+    counts4[1] = nn;
+    counts4[2] = std::min(cands, budget);
+    counts4[3] = n - kept;
+  }
+  o->n = nn;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_psnr(nps_gs* o, float* psnr_host) {
+  NPS_TRY(check_gs(o));
+  if (!o->fwd_valid || !o->tgt || !psnr_host) {
+    set_error("gs_psnr: forward (and set_targets) first");
+    return NPS_ERR_STATE;
+  }
+  cudaStream_t s = o->ctx->stream;
+  NPS_TRY(o->psnr_acc.ensure(sizeof(double) * o->nv));
+  NPS_CUDA(cudaMemsetAsync(o->psnr_acc.p, 0, sizeof(double) * o->nv, s));
+  gs::k_sq_err<<<dim3(2 * kNumSMs, o->nv), 256, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), o->w,
+                                                        o->h, o->psnr_acc.as<double>());
+  NPS_CHECK_LAUNCH();
+  std::vector<double> acc(o->nv);
+  NPS_CUDA(cudaMemcpyAsync(acc.data(), o->psnr_acc.p, sizeof(double) * o->nv, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t v = 0; v < o->nv; ++v) {
+    const double mse = acc[v] / (3.0 * (double)o->w * o->h);
+    psnr_host[v] = (float)(mse > 0 ? -10.0 * std::log10(mse) : 1e9);
+  }
+  return NPS_OK;
+}
+
 int nps_gs_set_timing(nps_gs* o, int enable) {
   NPS_TRY(check_gs(o));
   o->timing = enable != 0;
@@ -1430,6 +1636,7 @@ int nps_gs_set_timing(nps_gs* o, int enable) {
 
 int nps_gs_stage_times(nps_gs* o, double* ms, uint64_t* calls, uint32_t n, int reset) {
   NPS_TRY(check_gs(o));
+  NPS_TRY(collect_graph_timers(o));
   if (!o->ev_used.empty()) NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
   for (auto& u : o->ev_used) {
     float t = 0.0f;

@@ -29,7 +29,7 @@ namespace gsm {
 // parameter record (floats per Gaussian, padded to 64 = 256 B)
 constexpr int kP = 64;
 constexpr int kMean = 0, kLogScale = 3, kQuat = 6, kOpacity = 10, kSH = 12;
-constexpr int kUsed = 59;  // 3 + 3 + 4 + 1 + 48
+constexpr int kUsed = 60;  // end of the used floats: 3 + 3 + 4 + 1 + pad + 48
 constexpr int kViewRec = 48;  // floats per view: vp[16], vp_inv[16], cam_pos[3], pad
 
 constexpr float SH_C0 = 0.28209479177387814f;
@@ -177,6 +177,38 @@ GSM_HD void project(const float* vp, const T* mean, const T* log_scale, const T*
   P.ca = P.C * id;
   P.cb = -P.B * id;
   P.cc = P.A * id;
+}
+
+// ---- ADC split sampling (shared by the kernel and the oracle)
+// Counter-based hash: child means are a pure function of (index, seed, child).
+GSM_HD uint32_t adc_hash(uint32_t a, uint32_t b) {
+  uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  h *= 0x297A2D39u;
+  h ^= h >> 15;
+  return h;
+}
+GSM_HD float adc_uniform(uint32_t h) { return ((float)(h >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+// Child `ch` (0 or 1) of a split: mean = parent mean + R (s * z), z ~ N(0, I)
+// by Box-Muller from the hash; log-scales = parent - ln 1.6.
+GSM_HD void adc_split_child(const float* P, uint32_t i, uint32_t seed, uint32_t ch, float mean[3], float ls[3]) {
+  float qw = P[6], qx = P[7], qy = P[8], qz = P[9];
+  float ql = sqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
+  ql = ql > 1e-12f ? ql : 1e-12f;
+  float R[3][3];
+  quat_to_rot<float>(qw / ql, qx / ql, qy / ql, qz / ql, R);
+  float z[3];
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t h1 = adc_hash(i, seed * 8u + ch * 4u + (uint32_t)k);
+    const uint32_t h2 = adc_hash(h1, 0x51ED270Bu);
+    z[k] = sqrtf(-2.0f * logf(adc_uniform(h1))) * cosf(6.2831853f * adc_uniform(h2)) * expf(P[3 + k]);
+  }
+  for (int r = 0; r < 3; ++r) mean[r] = P[r] + (R[r][0] * z[0] + R[r][1] * z[1] + R[r][2] * z[2]);
+  const float d = 0.47000363f;  // ln 1.6
+  for (int k = 0; k < 3; ++k) ls[k] = P[3 + k] - d;
 }
 
 }  // namespace gsm

@@ -157,12 +157,36 @@ class GaussianTrainer:
         out["adc_grad"], out["adc_denom"] = ag, ad
         return out
 
-    def read_image(self):
-        """(image [V,H,W,4], dL/dimage [V,H,W,4]) of the last forward / loss."""
+    def write_state(self, adam_m=None, adam_v=None, step: int = 0):
+        m, mem, k1 = _ptr(adam_m)
+        v, mem2, k2 = _ptr(adam_v)
+        call("nps_gs_write_state", self._h, m, v, int(step), mem if adam_m is not None else mem2)
+
+    def write_adc_stats(self, adc_grad, adc_denom):
+        g, mem, k1 = _ptr(adc_grad)
+        d, mem2, k2 = _ptr(adc_denom)
+        assert mem == mem2
+        call("nps_gs_write_adc_stats", self._h, g, d, mem)
+
+    def adc(self, grad_thresh: float = 2e-4, split_scale: float = 0.01, prune_opacity: float = 0.005) -> dict:
+        """Densify (clone / split) and prune; returns the counts."""
+        c = np.zeros(4, np.uint32)
+        call("nps_gs_adc", self._h, float(grad_thresh), float(split_scale), float(prune_opacity), c.ctypes.data)
+        self.count = int(c[1])
+        return dict(before=int(c[0]), after=int(c[1]), densified=int(c[2]), pruned=int(c[3]))
+
+    def psnr(self):
+        """Per-view PSNR (dB) of the last forward."""
+        out = np.zeros(self.num_views, np.float32)
+        call("nps_gs_psnr", self._h, out.ctypes.data)
+        return out
+
+    def read_image(self, with_grad: bool = True):
+        """(image [V,H,W,4], dL/dimage [V,H,W,4] or None) of the last forward / loss."""
         shape = (self.num_views, self.height, self.width, 4)
         img = np.empty(shape, np.float32)
-        dimg = np.empty(shape, np.float32)
-        call("nps_gs_read_image", self._h, img.ctypes.data, dimg.ctypes.data)
+        dimg = np.empty(shape, np.float32) if with_grad else None
+        call("nps_gs_read_image", self._h, img.ctypes.data, None if dimg is None else dimg.ctypes.data)
         return img, dimg
 
     def buffers(self) -> dict:

@@ -554,6 +554,85 @@ int orc_gs_adam(float* params, const float* grads, float* m, float* v, uint32_t 
   return 0;
 }
 
+// Plain threshold ADC, serial: prune opacity < prune_op; densify (avg grad >=
+// thresh) by split (max scale > split_scale) or clone, densifying candidates in
+// index order while the capacity allows; records are compacted in index order,
+// each parent's outputs in place of it.  Split children come from the shared
+// sampling helper; clones keep the parent's Adam state in the first copy.
+int orc_gs_adc(const float* params, const float* m, const float* v, const float* adc_grad, const float* adc_denom,
+               uint32_t n, uint32_t cap, float thresh, float split_scale, float prune_op, uint32_t seed,
+               float* out_p, float* out_m, float* out_v, uint32_t* counts4) {
+  std::vector<uint32_t> flag(n);
+  uint32_t kept = 0, cands = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* P = params + (size_t)i * kP;
+    const float op = 1.0f / (1.0f + std::exp(-P[kOpacity]));
+    uint32_t f = 0;
+    if (!(op < prune_op)) {
+      f = 1;
+      const float d = adc_denom[i];
+      const float avg = d > 0.0f ? adc_grad[i] / d : 0.0f;
+      if (avg >= thresh) {
+        f |= 2;
+        if (std::exp(std::max(std::max(P[3], P[4]), P[5])) > split_scale) f |= 4;
+      }
+    }
+    flag[i] = f;
+    kept += f & 1;
+    cands += (f >> 1) & 1;
+  }
+  const uint32_t budget = cap > kept ? cap - kept : 0;
+  uint32_t o = 0, rank = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t f = flag[i];
+    if (!(f & 1)) continue;
+    const bool dens = (f & 2) && rank < budget;
+    if (f & 2) ++rank;
+    const float* P = params + (size_t)i * kP;
+    const size_t src = (size_t)i * kP;
+    if (!dens) {
+      std::copy(P, P + kP, out_p + (size_t)o * kP);
+      std::copy(m + src, m + src + kP, out_m + (size_t)o * kP);
+      std::copy(v + src, v + src + kP, out_v + (size_t)o * kP);
+      o += 1;
+      continue;
+    }
+    if (!(f & 4)) {
+      for (int c = 0; c < 2; ++c) {
+        std::copy(P, P + kP, out_p + (size_t)(o + c) * kP);
+        if (c == 0) {
+          std::copy(m + src, m + src + kP, out_m + (size_t)o * kP);
+          std::copy(v + src, v + src + kP, out_v + (size_t)o * kP);
+        } else {
+          std::fill(out_m + (size_t)(o + 1) * kP, out_m + (size_t)(o + 2) * kP, 0.0f);
+          std::fill(out_v + (size_t)(o + 1) * kP, out_v + (size_t)(o + 2) * kP, 0.0f);
+        }
+      }
+    } else {
+      for (uint32_t c = 0; c < 2; ++c) {
+        float* Q = out_p + (size_t)(o + c) * kP;
+        std::copy(P, P + kP, Q);
+        float mean[3], ls[3];
+        adc_split_child(P, i, seed, c, mean, ls);
+        for (int k = 0; k < 3; ++k) {
+          Q[k] = mean[k];
+          Q[3 + k] = ls[k];
+        }
+        std::fill(out_m + (size_t)(o + c) * kP, out_m + (size_t)(o + c + 1) * kP, 0.0f);
+        std::fill(out_v + (size_t)(o + c) * kP, out_v + (size_t)(o + c + 1) * kP, 0.0f);
+      }
+    }
+    o += 2;
+  }
+  if (counts4) {
+    counts4[0] = n;
+    counts4[1] = o;
+    counts4[2] = std::min(cands, budget);
+    counts4[3] = n - kept;
+  }
+  return 0;
+}
+
 // FP64 loss (no freezing) — for sanity checks.
 double orc_gs_loss_f64(const float* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W,
                        uint32_t H, const float* bg, const float* tgt_all, const uint32_t* tids, double lambda) {

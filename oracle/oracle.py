@@ -164,6 +164,19 @@ def gs_adam(params, grads, m, v, step, lr6):
     lib().orc_gs_adam(_p(params, F), _p(_f32(grads), F), _p(m, F), _p(v, F), params.shape[0], step, _p(lr, F))
 
 
+def gs_adc(params, m, v, adc_grad, adc_denom, cap, seed, thresh=2e-4, split_scale=0.01, prune_op=0.005):
+    """Plain threshold ADC; returns (params, m, v, counts[before, after, densified, pruned])."""
+    params, m, v = _f32(params), _f32(m), _f32(v)
+    n = params.shape[0]
+    op, om, ov = (np.zeros((cap, params.shape[1]), np.float32) for _ in range(3))
+    c = np.zeros(4, np.uint32)
+    lib().orc_gs_adc(_p(params, F), _p(m, F), _p(v, F), _p(_f32(adc_grad), F), _p(_f32(adc_denom), F), n, cap,
+                     ctypes.c_float(thresh), ctypes.c_float(split_scale), ctypes.c_float(prune_op), seed, _p(op, F),
+                     _p(om, F), _p(ov, F), _p(c, U))
+    k = int(c[1])
+    return op[:k], om[:k], ov[:k], c
+
+
 def gs_loss_f64(params, deg, views48, w, h, targets, tids, lam=0.2, bg=(0.0, 0.0, 0.0)):
     L = _setup_gs()
     params = _f32(params)

@@ -35,3 +35,46 @@ def test_analytic_backward_matches_fp64_central_differences(deg, nviews):
     rel = err / np.maximum(np.abs(cd), 1e-3 * scale)
     assert np.median(rel) < 1e-4, np.median(rel)
     assert np.quantile(rel, 0.98) < 1e-3, np.quantile(rel, 0.98)
+
+
+def test_adc_oracle_invariants():
+    """Plain ADC restatement: prune, clone and split counts, order and state."""
+    import math
+
+    from adc_scenes import adc_case
+
+    n = 4000
+    p, m, v, grad, denom = adc_case(n, 3)
+    op = 1 / (1 + np.exp(-p[:, 10].astype(np.float64)))
+    keep = ~(op < 0.005)
+    avg = np.where(denom > 0, grad / np.maximum(denom, 1), 0)
+    cand = keep & (avg >= 2e-4)
+    split = cand & (np.exp(p[:, 3:6].max(1)) > 0.01)
+    for cap, seed in ((2 * n, 1), (int(keep.sum()) + 100, 2)):
+        q, qm, qv, c = orc.gs_adc(p, m, v, grad, denom, cap, seed)
+        budget = cap - int(keep.sum())
+        dens = min(int(cand.sum()), budget)
+        assert tuple(c) == (n, int(keep.sum()) + dens, dens, int((~keep).sum()))
+        assert len(q) == c[1] <= cap
+        # walk the parents in order and check each one's outputs
+        o, rank = 0, 0
+        for i in np.flatnonzero(keep):
+            d = cand[i] and rank < budget
+            rank += int(cand[i])
+            if not d:
+                assert np.array_equal(q[o], p[i]) and np.array_equal(qm[o], m[i]) and np.array_equal(qv[o], v[i])
+                o += 1
+            elif not split[i]:
+                assert np.array_equal(q[o], p[i]) and np.array_equal(q[o + 1], p[i])
+                assert np.array_equal(qm[o], m[i]) and not qm[o + 1].any() and not qv[o + 1].any()
+                o += 2
+            else:
+                for ch in (0, 1):
+                    np.testing.assert_allclose(q[o + ch, 3:6], p[i, 3:6] - math.log(1.6), atol=1e-6)
+                    assert np.array_equal(q[o + ch, 6:], p[i, 6:])
+                    # children within 6 sigma of the parent along every axis
+                    assert np.linalg.norm(q[o + ch, :3] - p[i, :3]) <= 6 * math.sqrt(3) * np.exp(p[i, 3:6]).max()
+                    assert not qm[o + ch].any() and not qv[o + ch].any()
+                assert not np.array_equal(q[o, :3], q[o + 1, :3])
+                o += 2
+        assert o == c[1]
