@@ -242,6 +242,13 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
+/* Gradient accumulation for views launched one at a time (the plain per-view
+ * trainer): with accumulate != 0 backward adds to the gradient buffer instead
+ * of overwriting it; loss_views (0 = the views of each call) is the number of
+ * views the loss is averaged over, so that V single-view calls sum to the
+ * gradient of one V-view call.  The ADC statistic is always the NDC-space
+ * gradient of each view's own loss. */
+int nps_gs_set_accumulate(nps_gs* gs, int accumulate, uint32_t loss_views);
 /* Adaptive density control (north-star plain ADC): prune Gaussians with
  * opacity < prune_opacity; densify those whose average view-space gradient
  * norm (accumulated by backward, averaged over the views that saw them) is

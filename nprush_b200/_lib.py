@@ -95,6 +95,7 @@ SIGNATURES = {
     "nps_gs_set_graph": [P, I32],
     "nps_gs_read_image": [P, P, P],
     "nps_gs_adc": [P, F32, F32, F32, P],
+    "nps_gs_set_accumulate": [P, I32, U32],
     "nps_gs_write_adc_stats": [P, P, P, I32],
     "nps_gs_psnr": [P, P],
     "nps_gs_buffers": [P, PP, PP, PP, PP, PP, PP],

@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(kThreads) k_ssim_bwd(const float4* __restrict_
 }
 
 __global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblocks, float lambda, float inv_norm,
-                              float* __restrict__ loss) {
+                              float wconst, float* __restrict__ loss) {
   __shared__ float r0[kThreads], r1[kThreads];
   float a = 0, b = 0;
   for (uint32_t i = threadIdx.x; i < nblocks; i += kThreads) {
@@ -429,8 +429,8 @@ __global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblock
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    // inv_norm = 1 / (3 H W V)
-    loss[0] = (1.0f - lambda) * r0[0] * inv_norm + lambda * (1.0f - r1[0] * inv_norm);
+    // inv_norm = 1 / (3 H W V_loss); wconst = V / V_loss (this call's share of the loss)
+    loss[0] = (1.0f - lambda) * r0[0] * inv_norm + lambda * (wconst - r1[0] * inv_norm);
     loss[1] = r0[0] * inv_norm;  // mean L1
     loss[2] = r1[0] * inv_norm;  // mean SSIM
   }
@@ -562,7 +562,8 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
                                                      uint32_t H, const Rec* __restrict__ recs,
                                                      const uint32_t* __restrict__ counts,
                                                      const float* __restrict__ g2, float* __restrict__ grads,
-                                                     float* __restrict__ adc_grad, float* __restrict__ adc_denom) {
+                                                     float* __restrict__ adc_grad, float* __restrict__ adc_denom,
+                                                     int accumulate, float adc_scale) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float* p = params + (size_t)i * kP;
@@ -584,7 +585,8 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
     const float* view = views + (size_t)v * kViewRec;
     Proj<float> P;
     project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
-    adc_g += sqrtf((du * 0.5f * W) * (du * 0.5f * W) + (dv * 0.5f * H) * (dv * 0.5f * H));
+    // NDC-space gradient of this view's own loss (the loss is averaged over adc_scale views)
+    adc_g += adc_scale * sqrtf((du * 0.5f * W) * (du * 0.5f * W) + (dv * 0.5f * H) * (dv * 0.5f * H));
     adc_n += 1.0f;
     gop += dop;
     // colour: clamp at 0 blocks the gradient
@@ -679,13 +681,24 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
     for (int k = 0; k < 4; ++k) gq[k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
   }
   float* out = grads + (size_t)i * kP;
-  out[0] = gmean[0]; out[1] = gmean[1]; out[2] = gmean[2];
-  out[3] = gls[0]; out[4] = gls[1]; out[5] = gls[2];
-  out[6] = gq[0]; out[7] = gq[1]; out[8] = gq[2]; out[9] = gq[3];
-  out[10] = gop * op * (1.0f - op);
-  out[11] = 0.0f;
-  for (int k = 0; k < 48; ++k) out[kSH + k] = gsh[k];
-  out[60] = out[61] = out[62] = out[63] = 0.0f;
+  float g[kP];
+  g[0] = gmean[0]; g[1] = gmean[1]; g[2] = gmean[2];
+  g[3] = gls[0]; g[4] = gls[1]; g[5] = gls[2];
+  g[6] = gq[0]; g[7] = gq[1]; g[8] = gq[2]; g[9] = gq[3];
+  g[10] = gop * op * (1.0f - op);
+  g[11] = 0.0f;
+  for (int k = 0; k < 48; ++k) g[kSH + k] = gsh[k];
+  g[60] = g[61] = g[62] = g[63] = 0.0f;
+  float4* out4 = reinterpret_cast<float4*>(out);
+#pragma unroll
+  for (int k = 0; k < kP / 4; ++k) {
+    float4 w = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+    if (accumulate) {
+      const float4 a = out4[k];
+      w.x += a.x; w.y += a.y; w.z += a.z; w.w += a.w;
+    }
+    out4[k] = w;
+  }
   adc_grad[i] += adc_g;
   adc_denom[i] += adc_n;
 }
@@ -867,6 +880,8 @@ struct nps_gs {
   uint32_t step = 0;
   float lr[6] = {1.6e-4f, 5e-3f, 1e-3f, 5e-2f, 2.5e-3f, 2.5e-3f / 20.0f};
   float lambda = 0.2f;
+  bool accumulate = false;   // backward adds to the gradients instead of replacing them
+  uint32_t loss_views = 0;   // views the loss is averaged over (0: the views of each call)
   float bg[3] = {0.0f, 0.0f, 0.0f};
   // targets
   uint32_t w = 0, h = 0, nt = 0;
@@ -1313,14 +1328,15 @@ int nps_gs_loss(nps_gs* o, float* loss3_host) {
   NPS_TRY(o->maps.ensure(sizeof(float) * 9 * npix));
   NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
   NPS_TRY(o->dimg.ensure(sizeof(float4) * npix));
-  const float inv_norm = (float)(1.0 / (3.0 * (double)W * H * nv));
+  const uint32_t lv = o->loss_views ? o->loss_views : nv;
+  const float inv_norm = (float)(1.0 / (3.0 * (double)W * H * lv));
   { StageTimer t(o, ST_LOSS);
   gs::k_ssim_fwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H, o->lambda,
                                                inv_norm, o->maps.as<float>(), o->partial.as<float>());
   gs::k_ssim_bwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
                                                o->maps.as<float>(), W, H, o->lambda, inv_norm, o->dimg.as<float4>());
   gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->lambda, inv_norm,
-                                               o->loss.as<float>());
+                                               (float)nv / (float)lv, o->loss.as<float>());
   NPS_CHECK_LAUNCH(); }
   if (loss3_host) {
     NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, s));
@@ -1360,7 +1376,8 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
     gs::k_project_bwd<<<div_up(n, 128), 128, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
                                                      H, o->recs.as<gs::Rec>(), o->counts.as<uint32_t>(),
                                                      o->g2.as<float>(), o->grads.as<float>(), o->adc_grad.as<float>(),
-                                                     o->adc_denom.as<float>());
+                                                     o->adc_denom.as<float>(), o->accumulate ? 1 : 0,
+                                                     (float)(o->loss_views ? o->loss_views : nv));
     NPS_CHECK_LAUNCH();
   }
   return NPS_OK;
@@ -1625,6 +1642,14 @@ int nps_gs_psnr(nps_gs* o, float* psnr_host) {
     const double mse = acc[v] / (3.0 * (double)o->w * o->h);
     psnr_host[v] = (float)(mse > 0 ? -10.0 * std::log10(mse) : 1e9);
   }
+  return NPS_OK;
+}
+
+int nps_gs_set_accumulate(nps_gs* o, int accumulate, uint32_t loss_views) {
+  NPS_TRY(check_gs(o));
+  o->accumulate = accumulate != 0;
+  o->loss_views = loss_views;
+  o->gkey = 0;
   return NPS_OK;
 }
 

@@ -162,6 +162,33 @@ class GaussianTrainer:
         v, mem2, k2 = _ptr(adam_v)
         call("nps_gs_write_state", self._h, m, v, int(step), mem if adam_m is not None else mem2)
 
+    def set_accumulate(self, accumulate: bool, loss_views: int = 0):
+        call("nps_gs_set_accumulate", self._h, int(bool(accumulate)), int(loss_views))
+
+    def train_step_per_view(self, vp, vp_inv, target_ids, read_loss: bool = False):
+        """One step of the plain per-view trainer: the step's V views are
+        rendered, differentiated and accumulated one launch at a time (eager),
+        then one Adam update.  Same gradient as train_step over the V views."""
+        vp = np.asarray(vp, np.float32).reshape(-1, 16)
+        vpi = np.asarray(vp_inv, np.float32).reshape(-1, 16)
+        ids = np.ascontiguousarray(target_ids, np.uint32)
+        nv = vp.shape[0]
+        total = np.zeros(3, np.float64)
+        l3 = np.zeros(3, np.float32)
+        for k in range(nv):
+            self.set_accumulate(k > 0, nv)
+            self.set_views(vp[k:k + 1], vpi[k:k + 1], ids[k:k + 1])
+            call("nps_gs_forward", self._h, None)
+            call("nps_gs_loss", self._h, l3.ctypes.data if read_loss else None)
+            total += l3
+            call("nps_gs_backward", self._h, None)
+        call("nps_gs_adam", self._h)
+        self.set_accumulate(False, 0)
+        if read_loss:
+            # each view's terms are its share of the V-view means: they sum to them
+            return tuple(float(x) for x in total)
+        return None
+
     def write_adc_stats(self, adc_grad, adc_denom):
         g, mem, k1 = _ptr(adc_grad)
         d, mem2, k2 = _ptr(adc_denom)

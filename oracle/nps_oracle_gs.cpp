@@ -373,8 +373,12 @@ int orc_gs_loss(const float* img, const float* tgt_all, const uint32_t* tids, ui
 // fp32 backward: screen-space gradients per (view, Gaussian) by reverse
 // traversal from the final T, then the projection chain summed over views.
 // grads: n x 64 (overwritten).
+// adc2 (optional, n x 2): += (sum over the views that see a Gaussian of the
+// NDC-space norm of d(view loss)/d(mean2D), number of those views), where the
+// view loss is the given loss times adc_scale (the views it averages over).
 int orc_gs_backward(const float* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W, uint32_t H,
-                    const float* bg, const float* img, const uint32_t* ncontrib, const float* dimg, float* grads) {
+                    const float* bg, const float* img, const uint32_t* ncontrib, const float* dimg, float* grads,
+                    float* adc2, float adc_scale) {
   const size_t np = (size_t)W * H;
   const uint32_t tx = (W + 15) / 16;
   std::vector<float> g2((size_t)nv * n * 10, 0.0f);
@@ -463,6 +467,11 @@ int orc_gs_backward(const float* params, uint32_t n, int deg, const float* views
       Proj<float> P;
       project<float>(view, p + kMean, p + kLogScale, p + kQuat, (float)W, (float)H, (float)kLowpass, P);
       gop += gr[5];
+      if (adc2) {
+        const float du = gr[0] * 0.5f * (float)W, dv = gr[1] * 0.5f * (float)H;
+        adc2[2 * (size_t)i] += adc_scale * std::sqrt(du * du + dv * dv);
+        adc2[2 * (size_t)i + 1] += 1.0f;
+      }
       float dc[3];
       for (int c = 0; c < 3; ++c) dc[c] = pg.clamped[c] ? 0.0f : gr[6 + c];
       const float ddx = p[0] - view[32], ddy = p[1] - view[33], ddz = p[2] - view[34];

@@ -148,15 +148,18 @@ def gs_loss(img, targets, tids, lam=0.2):
     return l3, dimg
 
 
-def gs_backward(params, deg, views48, w, h, img, ncontrib, dimg, bg=(0.0, 0.0, 0.0)):
+def gs_backward(params, deg, views48, w, h, img, ncontrib, dimg, bg=(0.0, 0.0, 0.0), with_adc=False):
+    """Parameter gradients; with_adc also returns the ADC statistic
+    (n x 2: summed NDC-space view-loss gradient norms, views seen)."""
     params = _f32(params)
     views48 = _f32(views48)
     grads = np.zeros_like(params)
     bgv = _f32(bg)
+    adc2 = np.zeros((params.shape[0], 2), np.float32)
     lib().orc_gs_backward(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h, _p(bgv, F),
                           _p(_f32(img), F), _p(np.ascontiguousarray(ncontrib, np.uint32), U), _p(_f32(dimg), F),
-                          _p(grads, F))
-    return grads
+                          _p(grads, F), _p(adc2, F), ctypes.c_float(views48.shape[0]))
+    return (grads, adc2) if with_adc else grads
 
 
 def gs_adam(params, grads, m, v, step, lr6):
