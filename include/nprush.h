@@ -249,6 +249,16 @@ int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
  * gradient of one V-view call.  The ADC statistic is always the NDC-space
  * gradient of each view's own loss. */
 int nps_gs_set_accumulate(nps_gs* gs, int accumulate, uint32_t loss_views);
+/* Checkpoint (no reference counterpart: the reference never reads its GPU
+ * state back).  File: a 104-byte little-endian header (magic "NPSGSCK1",
+ * version, count, SH degree, Adam step, ADC seed, loss views, learning rates,
+ * background, SSIM weight) followed by params, Adam m, Adam v (count x 64
+ * floats each) and the two ADC accumulators (count floats each).  Load
+ * requires count <= capacity and the same SH degree. */
+int nps_gs_save(nps_gs* gs, const char* path);
+/* Number of Gaussians (changes with write_params, set_count, ADC and load). */
+int nps_gs_count(nps_gs* gs, uint32_t* count);
+int nps_gs_load(nps_gs* gs, const char* path);
 /* Adaptive density control (north-star plain ADC): prune Gaussians with
  * opacity < prune_opacity; densify those whose average view-space gradient
  * norm (accumulated by backward, averaged over the views that saw them) is
@@ -270,6 +280,33 @@ int nps_gs_stats(nps_gs* gs, nps_stats* out);
  * intervals to the totals, and returns totals (ms) and counts per stage. */
 int nps_gs_set_timing(nps_gs* gs, int enable);
 int nps_gs_stage_times(nps_gs* gs, double* ms, uint64_t* calls, uint32_t n, int reset);
+
+
+/* ---- learned ADC policy network (no reference counterpart) ----------------
+ * 16 -> 64 -> 64 -> 3 MLP with ReLU; the three logits (clone, split, prune)
+ * and a fixed 0 logit for keep form a softmax.  Parameters: one fp32 vector of
+ * nps_mlp_num_params() floats: W1 [64x16], b1 [64], W2 [64x64], b2 [64],
+ * W3 [3x64], b3 [3] (row-major, out x in).  Products run on the tensor cores
+ * with bf16 operands and fp32 accumulation. */
+typedef struct nps_mlp nps_mlp;
+int nps_mlp_num_params(void);
+int nps_mlp_create(nps_ctx* ctx, nps_mlp** out);
+int nps_mlp_destroy(nps_mlp* mlp);
+int nps_mlp_init(nps_mlp* mlp, uint64_t seed);
+int nps_mlp_set_params(nps_mlp* mlp, const float* params_host);
+int nps_mlp_get_params(nps_mlp* mlp, float* params_host);
+/* logits_dev [n x 3] of features_dev [n x 16] (device pointers, 16-byte aligned). */
+int nps_mlp_forward(nps_mlp* mlp, const float* features_dev, uint32_t n, float* logits_dev);
+/* Gradient of the mean class-weighted cross-entropy of one batch (labels:
+ * 0 keep, 1 clone, 2 split, 3 prune; class_w4 may be null for 1s). */
+int nps_mlp_grads(nps_mlp* mlp, const float* features_dev, const uint8_t* labels_dev, uint32_t n,
+                  const float* class_w4, float* grads_host, float* loss_host);
+/* Mini-batch Adam (lr, betas 0.9 / 0.999, eps 1e-8) for `epochs` passes over
+ * device-resident samples, reshuffled each epoch from `seed`; per-epoch mean
+ * loss and accuracy to the host arrays when given. */
+int nps_mlp_train(nps_mlp* mlp, const float* features_dev, const uint8_t* labels_dev, uint32_t n,
+                  const float* class_w4, uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
+                  float* loss_curve, float* acc_curve);
 
 #ifdef __cplusplus
 }

@@ -96,12 +96,24 @@ SIGNATURES = {
     "nps_gs_read_image": [P, P, P],
     "nps_gs_adc": [P, F32, F32, F32, P],
     "nps_gs_set_accumulate": [P, I32, U32],
+    "nps_gs_save": [P, ctypes.c_char_p],
+    "nps_gs_load": [P, ctypes.c_char_p],
+    "nps_gs_count": [P, P],
     "nps_gs_write_adc_stats": [P, P, P, I32],
     "nps_gs_psnr": [P, P],
     "nps_gs_buffers": [P, PP, PP, PP, PP, PP, PP],
     "nps_gs_stats": [P, ctypes.POINTER(nps_stats)],
     "nps_gs_set_timing": [P, I32],
     "nps_gs_stage_times": [P, P, P, U32, I32],
+    "nps_mlp_num_params": [],
+    "nps_mlp_create": [P, PP],
+    "nps_mlp_destroy": [P],
+    "nps_mlp_init": [P, ctypes.c_uint64],
+    "nps_mlp_set_params": [P, P],
+    "nps_mlp_get_params": [P, P],
+    "nps_mlp_forward": [P, P, U32, P],
+    "nps_mlp_grads": [P, P, P, U32, P, P, P],
+    "nps_mlp_train": [P, P, P, U32, P, U32, U32, F32, ctypes.c_uint64, P, P],
 }
 _RET = {"nps_last_error": ctypes.c_char_p, "nps_version": ctypes.c_char_p}
 

@@ -717,7 +717,10 @@ struct AdamArgs {
 __global__ void k_adam_prep(uint32_t* st, const uint32_t* total, uint32_t cap) {
   const bool skip = *total > cap;
   st[1] = skip ? 1u : 0u;
-  if (skip) return;
+  if (skip) {
+    st[4] += 1u;  // skipped steps so far (read by the host after graph replays)
+    return;
+  }
   const uint32_t step = st[0] + 1;
   st[0] = step;
   st[2] = __float_as_uint((float)(1.0 - pow(0.9, (double)step)));
@@ -907,7 +910,16 @@ struct nps_gs {
   // CUDA-graph capture of the whole train step
   bool graph_mode = false, capturing = false;
   cudaGraphExec_t gexec = nullptr;
-  cudaEvent_t gdone = nullptr;
+  cudaEvent_t gdone = nullptr;   // recorded after the newest replay
+  cudaEvent_t gprev = nullptr;   // recorded after the replay before it
+  uint32_t skip_seen = 0;        // device skip count already accounted for
+  // pinned staging for set_views (copies leave without a stream sync)
+  struct Stage {
+    void* host = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;
+  } vstage[4];
+  uint32_t vstage_next = 0;
   uint32_t* h_status = nullptr;  // pinned: pair count of the last graph replay
   uint64_t gkey = 0;
   uint32_t gcap = 0, skipped = 0;
@@ -1017,7 +1029,7 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
   if ((rc = o->params.ensure(pb)) || (rc = o->grads.ensure(pb)) || (rc = o->am.ensure(pb)) ||
       (rc = o->av.ensure(pb)) || (rc = o->adc_grad.ensure(sizeof(float) * capacity)) ||
       (rc = o->adc_denom.ensure(sizeof(float) * capacity)) || (rc = o->total.ensure(16)) ||
-      (rc = o->mcount.ensure(16)) || (rc = o->loss.ensure(64)) || (rc = o->stepst.ensure(16))) {
+      (rc = o->mcount.ensure(16)) || (rc = o->loss.ensure(64)) || (rc = o->stepst.ensure(32))) {
     delete o;
     return rc;
   }
@@ -1026,7 +1038,7 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
   cudaMemsetAsync(o->adc_grad.p, 0, sizeof(float) * capacity, s);
   cudaMemsetAsync(o->adc_denom.p, 0, sizeof(float) * capacity, s);
   cudaMemsetAsync(o->loss.p, 0, 64, s);
-  cudaMemsetAsync(o->stepst.p, 0, 16, s);
+  cudaMemsetAsync(o->stepst.p, 0, 32, s);
   cudaMemsetAsync(o->total.p, 0, 16, s);
   NPS_CUDA(cudaGetLastError());
   *out = o;
@@ -1039,6 +1051,11 @@ int nps_gs_destroy(nps_gs* o) {
   cudaStreamSynchronize(o->ctx->stream);
   if (o->gexec) cudaGraphExecDestroy(o->gexec);
   if (o->gdone) cudaEventDestroy(o->gdone);
+  if (o->gprev) cudaEventDestroy(o->gprev);
+  for (auto& st : o->vstage) {
+    if (st.done) cudaEventSynchronize(st.done), cudaEventDestroy(st.done);
+    if (st.host) cudaFreeHost(st.host);
+  }
   if (o->h_status) cudaFreeHost(o->h_status);
   for (auto& u : o->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (auto& u : o->gtimers) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
@@ -1202,9 +1219,25 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
   NPS_TRY(o->views.ensure(sizeof(float) * host.size()));
   NPS_TRY(o->tids.ensure(sizeof(uint32_t) * nv));
   cudaStream_t s = o->ctx->stream;
-  NPS_CUDA(cudaMemcpyAsync(o->views.p, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice, s));
-  NPS_CUDA(cudaMemcpyAsync(o->tids.p, ids.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice, s));
-  NPS_CUDA(cudaStreamSynchronize(s));
+  // stage through a pinned slot so that the copies queue behind in-flight
+  // work instead of waiting for it; a slot is reused once its copies are done
+  nps_gs::Stage& sl = o->vstage[o->vstage_next];
+  o->vstage_next = (o->vstage_next + 1) % 4;
+  const size_t vb = sizeof(float) * host.size(), ib = sizeof(uint32_t) * nv;
+  if (sl.done) NPS_CUDA(cudaEventSynchronize(sl.done));
+  else NPS_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  if (sl.bytes < vb + ib) {
+    if (sl.host) NPS_CUDA(cudaFreeHost(sl.host));
+    sl.host = nullptr;
+    sl.bytes = 0;
+    NPS_CUDA(cudaMallocHost(&sl.host, vb + ib));
+    sl.bytes = vb + ib;
+  }
+  std::memcpy(sl.host, host.data(), vb);
+  std::memcpy(static_cast<char*>(sl.host) + vb, ids.data(), ib);
+  NPS_CUDA(cudaMemcpyAsync(o->views.p, sl.host, vb, cudaMemcpyHostToDevice, s));
+  NPS_CUDA(cudaMemcpyAsync(o->tids.p, static_cast<char*>(sl.host) + vb, ib, cudaMemcpyHostToDevice, s));
+  NPS_CUDA(cudaEventRecord(sl.done, s));
   o->nv = nv;
   o->fwd_valid = false;
   return NPS_OK;
@@ -1445,6 +1478,7 @@ static int gs_capture(nps_gs* o) {
   o->gtimers.clear();
   if (!o->h_status) NPS_CUDA(cudaMallocHost((void**)&o->h_status, 16));
   if (!o->gdone) NPS_CUDA(cudaEventCreateWithFlags(&o->gdone, cudaEventDisableTiming));
+  if (!o->gprev) NPS_CUDA(cudaEventCreateWithFlags(&o->gprev, cudaEventDisableTiming));
   NPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   o->capturing = true;
   const uint32_t step_before = o->step;
@@ -1453,7 +1487,9 @@ static int gs_capture(nps_gs* o) {
   if (rc == NPS_OK) rc = nps_gs_backward(o, nullptr);
   if (rc == NPS_OK) rc = nps_gs_adam(o);
   if (rc == NPS_OK) {
-    const cudaError_t e = cudaMemcpyAsync(o->h_status, o->total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaMemcpyAsync(o->h_status, o->total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(o->h_status + 1, o->stepst.as<uint32_t>() + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) {
       set_error("graph capture: %s", cudaGetErrorString(e));
       rc = NPS_ERR_CUDA;
@@ -1506,25 +1542,33 @@ int nps_gs_train_step(nps_gs* o, float* loss3_host) {
                          ((uint64_t)o->h << 4) ^ (uint64_t)o->sh_deg ^ ((uint64_t)(uintptr_t)o->tgt << 7) ^
                          ((uint64_t)__builtin_bit_cast(uint32_t, o->bg[0]) << 3) ^ (uint64_t)o->lambda * 131ull;
     if (o->gexec) {
-      NPS_CUDA(cudaEventSynchronize(o->gdone));
-      NPS_TRY(collect_graph_timers(o));
-      if (o->h_status[0] > o->gcap) {
-        // the last replay overflowed its pair buffers: it skipped its update
-        o->skipped += 1;
+      // at most two replays in flight (one while stage timers are read, since
+      // their event nodes are shared by all replays)
+      NPS_CUDA(cudaEventSynchronize(o->timing ? o->gdone : o->gprev));
+      if (o->timing) NPS_TRY(collect_graph_timers(o));
+      const uint32_t sk = o->h_status[1];
+      if (sk != o->skip_seen) {
+        // a replay overflowed its pair buffers and skipped its update
+        o->skipped += sk - o->skip_seen;
+        o->skip_seen = sk;
         o->gkey = 0;
       }
     }
     if (!o->gexec || key != o->gkey) {
+      NPS_TRY(collect_graph_timers(o));
       NPS_TRY(gs_step_eager(o));  // sizes every buffer (and is this call's step)
       NPS_TRY(gs_capture(o));
+      NPS_CUDA(cudaStreamSynchronize(s));
+      o->skip_seen = o->h_status[1] = 0;
+      NPS_CUDA(cudaMemsetAsync(o->stepst.as<uint32_t>() + 4, 0, sizeof(uint32_t), s));
       o->gkey = key;
     } else {
       NPS_CUDA(cudaGraphLaunch(o->gexec, s));
+      std::swap(o->gdone, o->gprev);
       NPS_CUDA(cudaEventRecord(o->gdone, s));
       o->step += 1;
       o->fwd_valid = false;
-      // stage times are read at the next call (or by nps_gs_stage_times), so
-      // that replays queue back to back
+      // stage times are read at the next call (or by nps_gs_stage_times)
       o->gpending = o->timing && !o->gtimers.empty();
     }
   }
@@ -1645,6 +1689,121 @@ int nps_gs_psnr(nps_gs* o, float* psnr_host) {
   return NPS_OK;
 }
 
+// ---- checkpoint: little-endian header + params, Adam m, v (n x 64 floats
+// each) + ADC accumulators (n floats each)
+namespace {
+struct GsCkptHeader {
+  char magic[8];
+  uint32_t version, n, sh_deg, step, adc_seed, loss_views;
+  float lr[6], bg[3], lambda;
+  uint32_t reserved[8];
+};
+static_assert(sizeof(GsCkptHeader) == 104, "checkpoint header layout");
+constexpr char kCkptMagic[8] = {'N', 'P', 'S', 'G', 'S', 'C', 'K', '1'};
+}  // namespace
+
+int nps_gs_count(nps_gs* o, uint32_t* count) {
+  NPS_TRY(check_gs(o));
+  if (!count) return NPS_ERR_INVALID;
+  *count = o->n;
+  return NPS_OK;
+}
+
+int nps_gs_save(nps_gs* o, const char* path) {
+  NPS_TRY(check_gs(o));
+  if (!path) return NPS_ERR_INVALID;
+  cudaStream_t s = o->ctx->stream;
+  const size_t n = o->n, pf = (size_t)gsm::kP * n;
+  std::vector<float> buf(3 * pf + 2 * n);
+  uint32_t st[8] = {0};
+  if (n) {
+    NPS_CUDA(cudaMemcpyAsync(buf.data(), o->params.p, sizeof(float) * pf, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaMemcpyAsync(buf.data() + pf, o->am.p, sizeof(float) * pf, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaMemcpyAsync(buf.data() + 2 * pf, o->av.p, sizeof(float) * pf, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaMemcpyAsync(buf.data() + 3 * pf, o->adc_grad.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaMemcpyAsync(buf.data() + 3 * pf + n, o->adc_denom.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+  }
+  NPS_CUDA(cudaMemcpyAsync(st, o->stepst.p, 32, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  GsCkptHeader h{};
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.version = 1;
+  h.n = (uint32_t)n;
+  h.sh_deg = (uint32_t)o->sh_deg;
+  h.step = st[0];
+  h.adc_seed = o->adc_seed;
+  h.loss_views = o->loss_views;
+  for (int k = 0; k < 6; ++k) h.lr[k] = o->lr[k];
+  for (int k = 0; k < 3; ++k) h.bg[k] = o->bg[k];
+  h.lambda = o->lambda;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    set_error("gs_save: cannot open %s", path);
+    return NPS_ERR_INVALID;
+  }
+  const bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 &&
+                  std::fwrite(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed) {
+    set_error("gs_save: write to %s failed", path);
+    return NPS_ERR_INVALID;
+  }
+  return NPS_OK;
+}
+
+int nps_gs_load(nps_gs* o, const char* path) {
+  NPS_TRY(check_gs(o));
+  if (!path) return NPS_ERR_INVALID;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error("gs_load: cannot open %s", path);
+    return NPS_ERR_INVALID;
+  }
+  GsCkptHeader h{};
+  if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) {
+    std::fclose(f);
+    set_error("gs_load: %s is not a Gaussian checkpoint", path);
+    return NPS_ERR_INVALID;
+  }
+  if (h.n > o->cap || h.sh_deg != (uint32_t)o->sh_deg) {
+    std::fclose(f);
+    set_error("gs_load: checkpoint has %u Gaussians of SH degree %u (trainer: capacity %u, degree %d)", h.n,
+              h.sh_deg, o->cap, o->sh_deg);
+    return NPS_ERR_INVALID;
+  }
+  const size_t n = h.n, pf = (size_t)gsm::kP * n;
+  std::vector<float> buf(3 * pf + 2 * n);
+  const bool ok = std::fread(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+  std::fclose(f);
+  if (!ok) {
+    set_error("gs_load: %s is truncated", path);
+    return NPS_ERR_INVALID;
+  }
+  cudaStream_t s = o->ctx->stream;
+  if (n) {
+    NPS_CUDA(cudaMemcpyAsync(o->params.p, buf.data(), sizeof(float) * pf, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(o->am.p, buf.data() + pf, sizeof(float) * pf, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(o->av.p, buf.data() + 2 * pf, sizeof(float) * pf, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(o->adc_grad.p, buf.data() + 3 * pf, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(o->adc_denom.p, buf.data() + 3 * pf + n, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+  }
+  const uint32_t st[8] = {h.step, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  NPS_CUDA(cudaMemcpyAsync(o->stepst.p, st, 32, cudaMemcpyHostToDevice, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  o->n = h.n;
+  o->step = h.step;
+  o->adc_seed = h.adc_seed;
+  o->loss_views = h.loss_views;
+  for (int k = 0; k < 6; ++k) o->lr[k] = h.lr[k];
+  for (int k = 0; k < 3; ++k) o->bg[k] = h.bg[k];
+  o->lambda = h.lambda;
+  o->fwd_valid = o->loss_valid = false;
+  o->gkey = 0;
+  o->skip_seen = 0;
+  if (o->h_status) o->h_status[1] = 0;
+  return NPS_OK;
+}
+
 int nps_gs_set_accumulate(nps_gs* o, int accumulate, uint32_t loss_views) {
   NPS_TRY(check_gs(o));
   o->accumulate = accumulate != 0;
@@ -1689,6 +1848,13 @@ int nps_gs_stats(nps_gs* o, nps_stats* out) {
   if (o->graph_mode && o->gexec && o->h_status) {
     NPS_CUDA(cudaEventSynchronize(o->gdone));
     o->stats.pairs = o->h_status[0];  // pairs of the last replay
+    const uint32_t sk = o->h_status[1];
+    if (sk != o->skip_seen) {
+      o->skipped += sk - o->skip_seen;
+      o->skip_seen = sk;
+      o->gkey = 0;
+    }
+    o->stats.reserved[1] = o->skipped;
   }
   *out = o->stats;
   return NPS_OK;

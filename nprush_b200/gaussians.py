@@ -189,6 +189,19 @@ class GaussianTrainer:
             return tuple(float(x) for x in total)
         return None
 
+    def save(self, path):
+        """Checkpoint: parameters, Adam state and step, ADC accumulators."""
+        call("nps_gs_save", self._h, str(path).encode())
+
+    def load(self, path):
+        call("nps_gs_load", self._h, str(path).encode())
+        self.count = self._count()
+
+    def _count(self) -> int:
+        c = ctypes.c_uint32()
+        call("nps_gs_count", self._h, ctypes.byref(c))
+        return int(c.value)
+
     def write_adc_stats(self, adc_grad, adc_denom):
         g, mem, k1 = _ptr(adc_grad)
         d, mem2, k2 = _ptr(adc_denom)

@@ -15,6 +15,7 @@ Two trainers share the kernels:
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import math
 import time
@@ -48,13 +49,17 @@ class FitResult:
     skipped_steps: int = 0
 
 
+@functools.lru_cache(maxsize=4)
+def _epoch_perm(n_cams: int, seed: int, epoch: int) -> np.ndarray:
+    return np.random.default_rng((seed, epoch)).permutation(n_cams)
+
+
 def view_schedule(step: int, n_cams: int, views: int, seed: int) -> np.ndarray:
     """Cameras of step `step` (0-based): consecutive slices of a permutation
     drawn once per epoch from (seed, epoch)."""
     per_epoch = n_cams // views
     epoch, k = divmod(step, per_epoch)
-    perm = np.random.default_rng((seed, epoch)).permutation(n_cams)
-    return np.sort(perm[k * views:(k + 1) * views])
+    return np.sort(_epoch_perm(n_cams, seed, epoch)[k * views:(k + 1) * views])
 
 
 def evaluate_psnr(trainer, vp, vpi, views: int = 8) -> np.ndarray:

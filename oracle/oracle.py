@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libnps_oracle.so"
-SOURCES = [HERE / "nps_oracle.cpp", HERE / "nps_oracle_gs.cpp"]
+SOURCES = [HERE / "nps_oracle.cpp", HERE / "nps_oracle_gs.cpp", HERE / "nps_oracle_mlp.cpp"]
 
 
 def build(force: bool = False) -> Path:
@@ -220,3 +220,29 @@ def bezier_render(beziers, vp, w, h, bg=None, brush=None):
     lib().orc_bezier_render(_p(beziers, F), beziers.shape[0], _p(_f32(vp), F), w, h, _p(bg, F), _p(bb, F), bw, bh,
                             _p(out, F))
     return out
+
+
+# ------------------------------------------------------------ learned-ADC MLP
+def mlp_grads(params, X, labels, class_w=(1.0, 1.0, 1.0, 1.0), round_bf16=True):
+    """(grads, mean loss, logits [n, 3]) of the policy network on one batch."""
+    L = lib()
+    params, X = _f32(params), _f32(X)
+    n = X.shape[0]
+    g = np.zeros(L.orc_mlp_num_params(), np.float32)
+    loss = np.zeros(1, np.float32)
+    logits = np.zeros((n, 3), np.float32)
+    lab = None if labels is None else np.ascontiguousarray(labels, np.uint8)
+    L.orc_mlp_grads(_p(params, F), _p(X, F), None if lab is None else lab.ctypes.data, n, _p(_f32(class_w), F),
+                    int(round_bf16), _p(g, F), _p(loss, F), _p(logits, F))
+    return g, float(loss[0]), logits
+
+
+def mlp_loss_f64(params, X, labels, class_w=(1.0, 1.0, 1.0, 1.0), with_grads=False):
+    L = lib()
+    L.orc_mlp_loss_f64.restype = ctypes.c_double
+    params, X = _f32(params), _f32(X)
+    lab = np.ascontiguousarray(labels, np.uint8)
+    g = np.zeros(L.orc_mlp_num_params(), np.float64)
+    loss = L.orc_mlp_loss_f64(_p(params, F), _p(X, F), lab.ctypes.data, X.shape[0], _p(_f32(class_w), F),
+                              _p(g, D) if with_grads else None)
+    return (loss, g) if with_grads else loss

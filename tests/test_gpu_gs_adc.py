@@ -123,3 +123,40 @@ def test_adc_inside_graph_captured_training(trainer_cls):
     # a replay whose pairs outgrow the captured buffers skips its update and
     # recaptures; early growth after densifying may cost a step or two
     assert t.stats()["skipped_steps"] <= 3
+
+
+def test_checkpoint_resume(trainer_cls, tmp_path):
+    """Save after ADC mid-run, load into a fresh trainer: state is restored
+    exactly and training continues the same way (to the order of float atomics)."""
+    w = h = 96
+    p = gs_scene(2500, 31, deg=2)
+    vp, vpi, _ = gs_views(w, h, ((0.0, 0.0, 4.0), (2.8, 0.0, 2.8)))
+    tg = gs_targets(2, w, h, 32)
+    t = trainer_cls(6000, sh_degree=2, params=p)
+    t.set_targets(tg)
+    t.set_views(vp, vpi)
+    for _ in range(20):
+        t.train_step()
+    t.adc(grad_thresh=1e-5)
+    for _ in range(5):
+        t.train_step()
+    path = tmp_path / "ck.bin"
+    t.save(path)
+    s0 = t.read_state()
+    u = trainer_cls(6000, sh_degree=2)
+    u.load(path)
+    assert u.count == t.count
+    s1 = u.read_state()
+    for k in ("params", "adam_m", "adam_v", "adc_grad", "adc_denom"):
+        np.testing.assert_array_equal(s1[k], s0[k])
+    assert u.stats()["step_count"] == t.stats()["step_count"]
+    u.set_targets(tg)
+    u.set_views(vp, vpi)
+    la = [t.train_step(read_loss=True)[0] for _ in range(3)]
+    lb = [u.train_step(read_loss=True)[0] for _ in range(3)]
+    np.testing.assert_allclose(lb, la, rtol=1e-4)
+    # a checkpoint that does not fit is refused
+    small = trainer_cls(100, sh_degree=2)
+    from nprush_b200._lib import NpsError
+    with pytest.raises(NpsError):
+        small.load(path)
