@@ -268,6 +268,23 @@ int nps_gs_load(nps_gs* gs, const char* path);
  * counts4 (host, may be null) = {count before, count after, densified, pruned}.
  * The k-th call on a trainer samples split children with seed k. */
 int nps_gs_adc(nps_gs* gs, float grad_thresh, float split_scale, float prune_opacity, uint32_t* counts4);
+/* Learned ADC.  Record float 63 (padding) carries a lineage id: set it with
+ * nps_gs_assign_ids (id = base + index); clones and split children inherit it.
+ * nps_gs_adc_features writes, for the current Gaussians, the policy's 16-float
+ * feature vectors (features_dev, n x 16), the plain rule's decision
+ * (plain_dev, may be null: 0 keep, 1 clone, 2 split, 3 prune) and the ids
+ * (ids_dev, may be null); step_frac is the position in the ADC schedule.
+ * nps_gs_adc_policy applies the network's argmax decision per Gaussian (keep /
+ * clone / split / prune), falling back to the plain rule where a Gaussian's
+ * logits are not finite or for every Gaussian when policy is null; then
+ * densifies within the capacity and compacts like nps_gs_adc.
+ * fallback_host (may be null) = Gaussians decided by the plain rule. */
+int nps_gs_assign_ids(nps_gs* gs, uint32_t base);
+int nps_gs_adc_features(nps_gs* gs, float step_frac, float grad_thresh, float split_scale, float prune_opacity,
+                        float* features_dev, uint8_t* plain_dev, uint32_t* ids_dev);
+typedef struct nps_mlp nps_mlp;
+int nps_gs_adc_policy(nps_gs* gs, nps_mlp* policy, float step_frac, float grad_thresh, float split_scale,
+                      float prune_opacity, uint32_t* counts4, uint32_t* fallback_host);
 /* PSNR (dB) of each view of the last forward against its target, rgb in [0, 1]. */
 int nps_gs_psnr(nps_gs* gs, float* psnr_host);
 int nps_gs_buffers(nps_gs* gs, float** params, float** grads, float** adam_m, float** adam_v, float** image,
@@ -288,7 +305,6 @@ int nps_gs_stage_times(nps_gs* gs, double* ms, uint64_t* calls, uint32_t n, int 
  * nps_mlp_num_params() floats: W1 [64x16], b1 [64], W2 [64x64], b2 [64],
  * W3 [3x64], b3 [3] (row-major, out x in).  Products run on the tensor cores
  * with bf16 operands and fp32 accumulation. */
-typedef struct nps_mlp nps_mlp;
 int nps_mlp_num_params(void);
 int nps_mlp_create(nps_ctx* ctx, nps_mlp** out);
 int nps_mlp_destroy(nps_mlp* mlp);

@@ -804,6 +804,99 @@ __global__ void k_adc_count(const uint32_t* __restrict__ flags, const uint32_t* 
   out_cnt[i] = (f & 1u) ? ((f & 2u) && cand_rank[i] < budget ? 2u : 1u) : 0u;
 }
 
+// ADC feature vector of each Gaussian (16 floats) for the learned policy, the
+// plain rule's decision (0 keep, 1 clone, 2 split, 3 prune) and its lineage id
+// (record float 63: copied to clones and split children, so a family shares it).
+__global__ void k_adc_features(const float* __restrict__ params, const float* __restrict__ am,
+                               const float* __restrict__ av, const float* __restrict__ adc_grad,
+                               const float* __restrict__ adc_denom, uint32_t n, AdcParams a, float step_frac,
+                               float* __restrict__ feat, uint8_t* __restrict__ plain, uint32_t* __restrict__ ids) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* p = params + (size_t)i * kP;
+  const float op = 1.0f / (1.0f + expf(-p[kOpacity]));
+  const float d = adc_denom[i];
+  const float avg = d > 0.0f ? adc_grad[i] / d : 0.0f;
+  float l0 = p[3], l1 = p[4], l2 = p[5];
+  // sorted descending
+  if (l0 < l1) { const float t = l0; l0 = l1; l1 = t; }
+  if (l1 < l2) { const float t = l1; l1 = l2; l2 = t; }
+  if (l0 < l1) { const float t = l0; l0 = l1; l1 = t; }
+  const float* mm = am + (size_t)i * kP;
+  const float* vv = av + (size_t)i * kP;
+  float rest = 0.0f;
+  for (int k = 15; k < 60; ++k) rest += p[k] * p[k];
+  float f[16];
+  f[0] = log10f(avg + 1e-10f) + 4.0f;
+  f[1] = log1pf(d) * 0.25f;
+  f[2] = op;
+  f[3] = p[kOpacity] * 0.25f;
+  f[4] = (l0 + 4.0f) * 0.5f;
+  f[5] = (l1 + 4.0f) * 0.5f;
+  f[6] = (l2 + 4.0f) * 0.5f;
+  f[7] = (l0 - logf(a.split_scale)) * 0.4342945f;
+  f[8] = sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) * 0.5f;
+  f[9] = sqrtf(p[12] * p[12] + p[13] * p[13] + p[14] * p[14]) * 0.28209479f;
+  f[10] = sqrtf(rest);
+  f[11] = step_frac;
+  f[12] = log10f(sqrtf((vv[0] + vv[1] + vv[2]) * (1.0f / 3.0f)) + 1e-12f) + 6.0f;
+  f[13] = log10f(fabsf(mm[kOpacity]) + 1e-10f) + 6.0f;
+  f[14] = fminf(fmaxf(log10f((avg + 1e-12f) / a.grad_thresh), -3.0f), 3.0f) * (1.0f / 3.0f);
+  f[15] = 1.0f;
+  float4* o4 = reinterpret_cast<float4*>(feat + (size_t)i * 16);
+  o4[0] = make_float4(f[0], f[1], f[2], f[3]);
+  o4[1] = make_float4(f[4], f[5], f[6], f[7]);
+  o4[2] = make_float4(f[8], f[9], f[10], f[11]);
+  o4[3] = make_float4(f[12], f[13], f[14], f[15]);
+  if (plain) {
+    uint8_t dec = 0;
+    if (op < a.prune_opacity) dec = 3;
+    else if (avg >= a.grad_thresh) dec = expf(fmaxf(fmaxf(p[3], p[4]), p[5])) > a.split_scale ? 2 : 1;
+    plain[i] = dec;
+  }
+  if (ids) ids[i] = __float_as_uint(p[63]);
+}
+
+// Policy decisions to ADC flags: argmax over {keep (0), clone, split, prune}
+// logits; a row with non-finite logits falls back to the plain rule.
+__global__ void k_adc_policy_flags(const float* __restrict__ logits, const float* __restrict__ params,
+                                   const float* __restrict__ adc_grad, const float* __restrict__ adc_denom,
+                                   uint32_t n, AdcParams a, uint32_t* __restrict__ flags,
+                                   uint32_t* __restrict__ keep_cnt, uint32_t* __restrict__ cand_cnt,
+                                   uint32_t* __restrict__ fallback) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float z1 = logits[3 * (size_t)i], z2 = logits[3 * (size_t)i + 1], z3 = logits[3 * (size_t)i + 2];
+  uint32_t f;
+  if (isfinite(z1) && isfinite(z2) && isfinite(z3)) {
+    int best = 0;
+    float m = 0.0f;
+    if (z1 > m) m = z1, best = 1;
+    if (z2 > m) m = z2, best = 2;
+    if (z3 > m) m = z3, best = 3;
+    f = best == 0 ? 1u : best == 1 ? 3u : best == 2 ? 7u : 0u;
+  } else {
+    const float* p = params + (size_t)i * kP;
+    const float op = 1.0f / (1.0f + expf(-p[kOpacity]));
+    f = 0;
+    if (!(op < a.prune_opacity)) {
+      f = 1;
+      const float d = adc_denom[i];
+      const float avg = d > 0.0f ? adc_grad[i] / d : 0.0f;
+      if (avg >= a.grad_thresh) f |= expf(fmaxf(fmaxf(p[3], p[4]), p[5])) > a.split_scale ? 6u : 2u;
+    }
+    atomicAdd(fallback, 1u);
+  }
+  flags[i] = f;
+  keep_cnt[i] = f & 1u;
+  cand_cnt[i] = (f >> 1) & 1u;
+}
+
+__global__ void k_assign_ids(float* __restrict__ params, uint32_t n, uint32_t base) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) params[(size_t)i * kP + 63] = __uint_as_float(base + i);
+}
+
 // one thread per (Gaussian, float4 of its record)
 __global__ void k_adc_scatter(const float4* __restrict__ p_in, const float4* __restrict__ m_in,
                               const float4* __restrict__ v_in, const uint32_t* __restrict__ flags,
@@ -905,7 +998,7 @@ struct nps_gs {
   // device step state (see k_adam_prep)
   DevBuf stepst;
   // ADC work: alternate parameter / optimiser buffers and flags
-  DevBuf p_alt, m_alt, v_alt, aflags, akeep, acand, akeep_off, acand_off, acnt, aoff, atot, psnr_acc;
+  DevBuf p_alt, m_alt, v_alt, aflags, akeep, acand, akeep_off, acand_off, acnt, aoff, atot, psnr_acc, afeat, alogits;
   uint32_t adc_seed = 0;
   // CUDA-graph capture of the whole train step
   bool graph_mode = false, capturing = false;
@@ -1061,7 +1154,7 @@ int nps_gs_destroy(nps_gs* o) {
   for (auto& u : o->gtimers) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (cudaEvent_t e : o->ev_pool) cudaEventDestroy(e);
   for (DevBuf* b : {&o->p_alt, &o->m_alt, &o->v_alt, &o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off,
-                    &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst})
+                    &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst, &o->afeat, &o->alogits})
     b->release();
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
                     &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
@@ -1614,11 +1707,11 @@ int nps_gs_buffers(nps_gs* o, float** params, float** grads, float** adam_m, flo
   return NPS_OK;
 }
 
-int nps_gs_adc(nps_gs* o, float grad_thresh, float split_scale, float prune_opacity, uint32_t* counts4) {
-  NPS_TRY(check_gs(o));
-  cudaStream_t s = o->ctx->stream;
+}  // extern "C"
+
+namespace {
+int adc_prepare(nps_gs* o) {
   const uint32_t n = o->n;
-  if (n == 0) return NPS_OK;
   const size_t pb = sizeof(float) * gsm::kP * (size_t)o->cap;
   NPS_TRY(o->p_alt.ensure(pb));
   NPS_TRY(o->m_alt.ensure(pb));
@@ -1626,19 +1719,22 @@ int nps_gs_adc(nps_gs* o, float grad_thresh, float split_scale, float prune_opac
   for (DevBuf* b : {&o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off, &o->acnt, &o->aoff})
     NPS_TRY(b->ensure(sizeof(uint32_t) * (n + 1)));
   NPS_TRY(o->atot.ensure(16));
-  gs::AdcParams a{grad_thresh, split_scale, prune_opacity, ++o->adc_seed};
+  return NPS_OK;
+}
+
+// Applies the flags in o->aflags (with keep / candidate indicators in akeep /
+// acand): densify the first candidates that fit the capacity, compact.
+int adc_apply(nps_gs* o, const gs::AdcParams& a, uint32_t* counts4) {
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t n = o->n;
   uint32_t* tot = o->atot.as<uint32_t>();
-  gs::k_adc_classify<<<div_up(n, 256), 256, 0, s>>>(o->params.as<float>(), o->adc_grad.as<float>(),
-                                                    o->adc_denom.as<float>(), n, a, o->aflags.as<uint32_t>(),
-                                                    o->akeep.as<uint32_t>(), o->acand.as<uint32_t>());
-  NPS_CHECK_LAUNCH();
   NPS_TRY(exclusive_scan_u32(o->akeep.as<uint32_t>(), o->akeep_off.as<uint32_t>(), n, tot, o->sw_tile, s));
   NPS_TRY(exclusive_scan_u32(o->acand.as<uint32_t>(), o->acand_off.as<uint32_t>(), n, tot + 1, o->sw_tile, s));
   uint32_t h[2] = {0, 0};
   NPS_CUDA(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, s));
   NPS_CUDA(cudaStreamSynchronize(s));
   const uint32_t kept = h[0], cands = h[1];
-  const uint32_t budget = o->cap > kept ? o->cap - kept : 0;  // densify the first candidates that fit
+  const uint32_t budget = o->cap > kept ? o->cap - kept : 0;
   gs::k_adc_count<<<div_up(n, 256), 256, 0, s>>>(o->aflags.as<uint32_t>(), o->acand_off.as<uint32_t>(), n, budget,
                                                  o->acnt.as<uint32_t>());
   NPS_TRY(exclusive_scan_u32(o->acnt.as<uint32_t>(), o->aoff.as<uint32_t>(), n, tot + 2, o->sw_tile, s));
@@ -1665,6 +1761,78 @@ int nps_gs_adc(nps_gs* o, float grad_thresh, float split_scale, float prune_opac
   o->n = nn;
   o->fwd_valid = false;
   return NPS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int nps_gs_adc(nps_gs* o, float grad_thresh, float split_scale, float prune_opacity, uint32_t* counts4) {
+  NPS_TRY(check_gs(o));
+  if (counts4) counts4[0] = counts4[1] = counts4[2] = counts4[3] = 0;
+  const uint32_t n = o->n;
+  if (n == 0) return NPS_OK;
+  NPS_TRY(adc_prepare(o));
+  gs::AdcParams a{grad_thresh, split_scale, prune_opacity, ++o->adc_seed};
+  gs::k_adc_classify<<<div_up(n, 256), 256, 0, o->ctx->stream>>>(
+      o->params.as<float>(), o->adc_grad.as<float>(), o->adc_denom.as<float>(), n, a, o->aflags.as<uint32_t>(),
+      o->akeep.as<uint32_t>(), o->acand.as<uint32_t>());
+  NPS_CHECK_LAUNCH();
+  return adc_apply(o, a, counts4);
+}
+
+int nps_gs_adc_features(nps_gs* o, float step_frac, float grad_thresh, float split_scale, float prune_opacity,
+                        float* features_dev, uint8_t* plain_dev, uint32_t* ids_dev) {
+  NPS_TRY(check_gs(o));
+  if (!features_dev) return NPS_ERR_INVALID;
+  const uint32_t n = o->n;
+  if (n == 0) return NPS_OK;
+  gs::AdcParams a{grad_thresh, split_scale, prune_opacity, 0};
+  gs::k_adc_features<<<div_up(n, 256), 256, 0, o->ctx->stream>>>(
+      o->params.as<float>(), o->am.as<float>(), o->av.as<float>(), o->adc_grad.as<float>(), o->adc_denom.as<float>(),
+      n, a, step_frac, features_dev, plain_dev, ids_dev);
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
+int nps_gs_assign_ids(nps_gs* o, uint32_t base) {
+  NPS_TRY(check_gs(o));
+  if (o->n == 0) return NPS_OK;
+  gs::k_assign_ids<<<div_up(o->n, 256), 256, 0, o->ctx->stream>>>(o->params.as<float>(), o->n, base);
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
+int nps_gs_adc_policy(nps_gs* o, nps_mlp* policy, float step_frac, float grad_thresh, float split_scale,
+                      float prune_opacity, uint32_t* counts4, uint32_t* fallback_host) {
+  NPS_TRY(check_gs(o));
+  if (counts4) counts4[0] = counts4[1] = counts4[2] = counts4[3] = 0;
+  if (fallback_host) *fallback_host = 0;
+  if (!policy) {
+    // no network: the plain threshold rule
+    if (fallback_host) *fallback_host = o->n;
+    return nps_gs_adc(o, grad_thresh, split_scale, prune_opacity, counts4);
+  }
+  const uint32_t n = o->n;
+  if (n == 0) return NPS_OK;
+  NPS_TRY(adc_prepare(o));
+  cudaStream_t s = o->ctx->stream;
+  NPS_TRY(o->afeat.ensure(sizeof(float) * 16 * (size_t)n));
+  NPS_TRY(o->alogits.ensure(sizeof(float) * 3 * (size_t)n + 16));
+  gs::AdcParams a{grad_thresh, split_scale, prune_opacity, ++o->adc_seed};
+  gs::k_adc_features<<<div_up(n, 256), 256, 0, s>>>(o->params.as<float>(), o->am.as<float>(), o->av.as<float>(),
+                                                    o->adc_grad.as<float>(), o->adc_denom.as<float>(), n, a,
+                                                    step_frac, o->afeat.as<float>(), nullptr, nullptr);
+  NPS_CHECK_LAUNCH();
+  NPS_TRY(nps_mlp_forward(policy, o->afeat.as<float>(), n, o->alogits.as<float>()));
+  uint32_t* fb = o->alogits.as<uint32_t>() + 3 * (size_t)n;
+  NPS_CUDA(cudaMemsetAsync(fb, 0, 4, s));
+  gs::k_adc_policy_flags<<<div_up(n, 256), 256, 0, s>>>(o->alogits.as<float>(), o->params.as<float>(),
+                                                        o->adc_grad.as<float>(), o->adc_denom.as<float>(), n, a,
+                                                        o->aflags.as<uint32_t>(), o->akeep.as<uint32_t>(),
+                                                        o->acand.as<uint32_t>(), fb);
+  NPS_CHECK_LAUNCH();
+  if (fallback_host) NPS_CUDA(cudaMemcpyAsync(fallback_host, fb, 4, cudaMemcpyDeviceToHost, s));
+  return adc_apply(o, a, counts4);
 }
 
 int nps_gs_psnr(nps_gs* o, float* psnr_host) {

@@ -215,6 +215,34 @@ class GaussianTrainer:
         self.count = int(c[1])
         return dict(before=int(c[0]), after=int(c[1]), densified=int(c[2]), pruned=int(c[3]))
 
+    def assign_ids(self, base: int = 0):
+        """Lineage ids (record float 63) = base + index; inherited by clones / children."""
+        call("nps_gs_assign_ids", self._h, int(base))
+
+    def adc_features(self, step_frac: float, grad_thresh: float = 2e-4, split_scale: float = 0.01,
+                     prune_opacity: float = 0.005):
+        """(features [n,16] f32, plain decision [n] u8, lineage id [n] i32) as torch CUDA tensors."""
+        import torch
+        n = self.count
+        dev = f"cuda:{self.device}"
+        feat = torch.empty((max(n, 1), 16), device=dev, dtype=torch.float32)
+        plain = torch.empty(max(n, 1), device=dev, dtype=torch.uint8)
+        ids = torch.empty(max(n, 1), device=dev, dtype=torch.int32)
+        call("nps_gs_adc_features", self._h, float(step_frac), float(grad_thresh), float(split_scale),
+             float(prune_opacity), feat.data_ptr(), plain.data_ptr(), ids.data_ptr())
+        self.sync()
+        return feat[:n], plain[:n], ids[:n]
+
+    def adc_policy(self, policy, step_frac: float, grad_thresh: float = 2e-4, split_scale: float = 0.01,
+                   prune_opacity: float = 0.005) -> dict:
+        """ADC decided by the policy network (None: the plain rule)."""
+        c = np.zeros(4, np.uint32)
+        fb = ctypes.c_uint32(0)
+        call("nps_gs_adc_policy", self._h, None if policy is None else policy._h, float(step_frac),
+             float(grad_thresh), float(split_scale), float(prune_opacity), c.ctypes.data, ctypes.byref(fb))
+        self.count = int(c[1])
+        return dict(before=int(c[0]), after=int(c[1]), densified=int(c[2]), pruned=int(c[3]), fallback=int(fb.value))
+
     def psnr(self):
         """Per-view PSNR (dB) of the last forward."""
         out = np.zeros(self.num_views, np.float32)

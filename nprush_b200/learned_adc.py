@@ -1,0 +1,166 @@
+"""Learned ADC: logging plain-ADC decisions, hindsight labels, training the
+policy network, and running ADC with it.
+
+Labels come from the plain threshold rule's own runs.  At every ADC event the
+16-float features of a sample of Gaussians are logged with the plain decision
+and each Gaussian's lineage id (inherited by clones and split children).  A
+logged decision is then relabelled by what happened to the lineage over the
+next `horizon` events:
+
+  * keep  -> prune  when the plain rule prunes a member of the lineage later
+    (the Gaussian was dead weight: prune it now);
+  * clone / split -> keep  when a member of the lineage is pruned later (the
+    densification did not pay);
+  * prune stays prune.
+
+The network therefore learns the plain rule plus earlier pruning and fewer
+wasted densifications.  The plain rule stays the fallback (no network, or a
+Gaussian whose logits are not finite) and the judge: the A/B run compares
+final PSNR, Gaussian count and wall time against it.
+
+    python -m nprush_b200.learned_adc --log-seeds 100 101 --eval-seed 120 --steps 3000 --out ab.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .train import AdcSchedule, evaluate_psnr, fit
+
+
+@dataclass
+class AdcLog:
+    samples_per_event: int = 20000
+    seed: int = 0
+    features: list = field(default_factory=list)   # per event [k, 16]
+    plain: list = field(default_factory=list)      # per event [k]
+    ids: list = field(default_factory=list)        # per event [k]
+    pruned_ids: list = field(default_factory=list)  # per event: sorted ids the plain rule pruned
+
+    def record(self, trainer, step_frac: float, adc: AdcSchedule):
+        feat, plain, ids = trainer.adc_features(step_frac, adc.grad_thresh, adc.split_scale, adc.prune_opacity)
+        plain_h = plain.cpu().numpy()
+        ids_h = ids.cpu().numpy()
+        n = len(plain_h)
+        rng = np.random.default_rng((self.seed, len(self.features)))
+        k = min(self.samples_per_event, n)
+        sel = np.sort(rng.choice(n, k, replace=False)) if k < n else np.arange(n)
+        self.features.append(feat.cpu().numpy()[sel])
+        self.plain.append(plain_h[sel])
+        self.ids.append(ids_h[sel])
+        self.pruned_ids.append(np.unique(ids_h[plain_h == 3]))
+
+
+def hindsight_labels(log: AdcLog, horizon: int = 3):
+    """(features [N,16], labels [N]) relabelled by the lineages' fate."""
+    X, Y = [], []
+    ev = len(log.features)
+    for e in range(ev):
+        y = log.plain[e].astype(np.uint8).copy()
+        later = [log.pruned_ids[j] for j in range(e + 1, min(ev, e + 1 + horizon))]
+        if later:
+            dead = np.isin(log.ids[e], np.unique(np.concatenate(later)))
+            y[(y == 0) & dead] = 3
+            y[((y == 1) | (y == 2)) & dead] = 0
+        X.append(log.features[e])
+        Y.append(y)
+    return np.concatenate(X), np.concatenate(Y)
+
+
+def class_weights(y, cap: float = 20.0):
+    cnt = np.bincount(y, minlength=4).astype(np.float64)
+    w = np.where(cnt > 0, cnt.sum() / (4.0 * np.maximum(cnt, 1.0)), 1.0)
+    return np.clip(w, 1.0 / cap, cap).astype(np.float32)
+
+
+def logging_adc_fn(log: AdcLog, adc: AdcSchedule):
+    def fn(trainer, step):
+        log.record(trainer, step / adc.stop, adc)
+        return trainer.adc(adc.grad_thresh, adc.split_scale, adc.prune_opacity)
+    return fn
+
+
+def policy_adc_fn(policy, adc: AdcSchedule):
+    def fn(trainer, step):
+        return trainer.adc_policy(policy, step / adc.stop, adc.grad_thresh, adc.split_scale, adc.prune_opacity)
+    return fn
+
+
+def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: str = "batched"):
+    """One training run on a fresh scene; returns (FitResult, mean PSNR)."""
+    vp, vpi, tg, st = scene_fn(seed)
+    st.assign_ids(0)
+    r = fit(st, vp, vpi, steps, seed=seed, adc=adc, mode=mode, adc_fn=adc_fn)
+    psnr = float(np.mean(evaluate_psnr(st, vp, vpi)))
+    st.close()
+    return r, psnr
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--log-seeds", type=int, nargs="+", default=[100, 101])
+    ap.add_argument("--eval-seed", type=int, default=120)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--adc-stop", type=int, default=None)
+    ap.add_argument("--gaussians", type=int, default=200_000)
+    ap.add_argument("--teacher", type=int, default=250_000)
+    ap.add_argument("--res", type=int, default=800)
+    ap.add_argument("--horizon", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--class-weights", action="store_true",
+                    help="weight classes by inverse frequency (default: uniform; a false prune costs more "
+                         "than a missed one)")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    import torch
+
+    from . import _lib
+    from .policy import AdcPolicy
+    from .train import config2_scene
+    stream = torch.cuda.Stream(0)
+    ctx = _lib.context(0)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    adc = AdcSchedule(stop=a.adc_stop or min(15000, a.steps))
+
+    def scene(seed):
+        # student and teacher seeds derived from the run seed
+        return config2_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=4 * a.gaussians,
+                             student_seed=seed, teacher_seed=seed + 1000)
+
+    out = {}
+    with torch.cuda.stream(stream):
+        log = AdcLog(seed=1)
+        for s in a.log_seeds:
+            r, p = run(scene, a.steps, s, adc, logging_adc_fn(log, adc))
+            out.setdefault("log_runs", []).append(dict(seed=s, psnr=p, count=r.count, wall_s=r.wall_s))
+        X, y = hindsight_labels(log, a.horizon)
+        cw = class_weights(y) if a.class_weights else np.ones(4, np.float32)
+        # hold out every 10th sample to score the network
+        hold = np.arange(len(y)) % 10 == 0
+        pol = AdcPolicy(seed=7)
+        lc, ac = pol.train(X[~hold], y[~hold], epochs=a.epochs, batch=8192, lr=2e-3, seed=3, class_w=cw)
+        z = pol.logits(X[hold]).cpu().numpy()
+        pred = np.argmax(np.c_[np.zeros(len(z)), z], axis=1)
+        conf = np.zeros((4, 4), np.int64)
+        np.add.at(conf, (y[hold], pred), 1)
+        out["training"] = dict(samples=int(len(y)), class_counts=np.bincount(y, minlength=4).tolist(),
+                               class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
+                               heldout_confusion=conf.tolist())
+        for name, fn in (("plain", None), ("learned", policy_adc_fn(pol, adc))):
+            r, p = run(scene, a.steps, a.eval_seed, adc, fn)
+            out[name] = dict(psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
+                             skipped=r.skipped_steps, adc_events=r.adc_events[-3:])
+    out["config"] = vars(a)
+    print(json.dumps({k: out[k] for k in ("plain", "learned")}))
+    print(json.dumps(dict(class_counts=out["training"]["class_counts"], acc=out["training"]["acc"][-1],
+                          confusion=out["training"]["heldout_confusion"])))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(out, f)
+
+
+if __name__ == "__main__":
+    main()

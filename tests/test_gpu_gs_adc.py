@@ -160,3 +160,69 @@ def test_checkpoint_resume(trainer_cls, tmp_path):
     from nprush_b200._lib import NpsError
     with pytest.raises(NpsError):
         small.load(path)
+
+
+def features_ref(p, m, v, grad, denom, step_frac, thr=2e-4, split=0.01):
+    """numpy restatement of the policy's 16 ADC features."""
+    p, m, v = p.astype(np.float64), m.astype(np.float64), v.astype(np.float64)
+    avg = np.where(denom > 0, grad / np.maximum(denom, 1e-30), 0.0)
+    ls = -np.sort(-p[:, 3:6], axis=1)
+    op = 1 / (1 + np.exp(-p[:, 10]))
+    f = np.zeros((len(p), 16))
+    f[:, 0] = np.log10(avg + 1e-10) + 4
+    f[:, 1] = np.log1p(denom) / 4
+    f[:, 2] = op
+    f[:, 3] = p[:, 10] / 4
+    f[:, 4:7] = (ls + 4) / 2
+    f[:, 7] = (ls[:, 0] - np.log(split)) / np.log(10)
+    f[:, 8] = np.linalg.norm(p[:, 0:3], axis=1) / 2
+    f[:, 9] = np.linalg.norm(p[:, 12:15], axis=1) * 0.28209479
+    f[:, 10] = np.sqrt((p[:, 15:60] ** 2).sum(1))
+    f[:, 11] = step_frac
+    f[:, 12] = np.log10(np.sqrt(v[:, 0:3].mean(1)) + 1e-12) + 6
+    f[:, 13] = np.log10(np.abs(m[:, 10]) + 1e-10) + 6
+    f[:, 14] = np.clip(np.log10((avg + 1e-12) / thr), -3, 3) / 3
+    f[:, 15] = 1
+    return f
+
+
+def test_adc_features_ids_and_policy_decisions(trainer_cls):
+    from nprush_b200.policy import AdcPolicy
+    n = 4000
+    p, m, v, grad, denom = adc_case(n, 44, deg=3)
+    v = np.abs(v)
+    t = trainer_cls(3 * n, sh_degree=3, params=p)
+    t.write_state(m, v, 9)
+    t.write_adc_stats(grad, denom)
+    t.assign_ids(1000)
+    feat, plain, ids = t.adc_features(0.25)
+    feat, plain, ids = feat.cpu().numpy(), plain.cpu().numpy(), ids.cpu().numpy()
+    np.testing.assert_allclose(feat, features_ref(p, m, v, grad, denom, 0.25), atol=2e-5, rtol=1e-5)
+    np.testing.assert_array_equal(ids, np.arange(n) + 1000)
+    _, _, _, c = orc.gs_adc(p, m, v, grad, denom, 3 * n, 1)
+    assert int((plain == 3).sum()) == int(c[3])
+    assert int(((plain == 1) | (plain == 2)).sum()) == int(c[2])
+    # no network: the plain rule, lineage ids carried to the children
+    st = t.read_state()
+    r = t.adc_policy(None, 0.25)
+    assert r["fallback"] == n and r["after"] == int(c[1])
+    got = t.read_state()["params"]
+    want = orc.gs_adc(st["params"], st["adam_m"], st["adam_v"], grad, denom, 3 * n, 1)[0]
+    np.testing.assert_array_equal(got[:, 63].view(np.int32), want[:, 63].view(np.int32))
+    # a network that always answers "prune" (bias only) / "clone"
+    for b3, expect in (((-9.0, -9.0, 9.0), "prune"), ((9.0, -9.0, -9.0), "clone")):
+        pol = AdcPolicy(params=np.r_[np.zeros(5440, np.float32), np.array(b3, np.float32)])
+        u = trainer_cls(3 * n, sh_degree=3, params=p)
+        u.write_adc_stats(grad, denom)
+        r = u.adc_policy(pol, 0.5)
+        assert r["fallback"] == 0
+        if expect == "prune":
+            assert r["after"] == 0 and r["pruned"] == n
+        else:
+            assert r["densified"] == n and r["after"] == 2 * n
+    # a network with non-finite logits falls back to the plain rule everywhere
+    bad = AdcPolicy(params=np.full(5443, np.nan, np.float32))
+    u = trainer_cls(3 * n, sh_degree=3, params=p)
+    u.write_adc_stats(grad, denom)
+    r = u.adc_policy(bad, 0.5)
+    assert r["fallback"] == n and r["after"] == int(c[1])
