@@ -242,6 +242,11 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
+/* Deterministic mode: the backward reduces each (view, Gaussian) gradient in
+ * two passes (per-pair tile sums stored, then summed per record in sorted-pair
+ * order) instead of with float atomics, so repeated runs are bit-identical.
+ * Costs a pair-sized buffer (40 B per pair) and a second sort. */
+int nps_gs_set_deterministic(nps_gs* gs, int enable);
 /* Gradient accumulation for views launched one at a time (the plain per-view
  * trainer): with accumulate != 0 backward adds to the gradient buffer instead
  * of overwriting it; loss_views (0 = the views of each call) is the number of

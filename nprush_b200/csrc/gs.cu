@@ -437,25 +437,37 @@ __global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblock
 }
 
 // ------------------------------------------------------------ backward raster
+// Reverse-order replay of the forward per pixel.  Default: the per-pair
+// gradients of a warp are reduced by shuffles, summed over the CTA's warps with
+// shared-memory atomics and added to the (view, Gaussian) records with global
+// atomics.  kDet (deterministic two-pass mode): warps stage their sums in
+// shared memory, which are folded in warp order, and each pair's tile sum is
+// stored to `part` (no atomics); k_det_segsum then adds the pairs of each
+// (view, Gaussian) record in sorted-pair order.
+template <bool kDet>
 __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                   const uint32_t* __restrict__ rstart,
                                                   const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                   uint32_t tiles_x, uint32_t num_tiles, float3 bg,
                                                   const float4* __restrict__ img, const uint32_t* __restrict__ ncontrib,
-                                                  const float4* __restrict__ dimg, float* __restrict__ g2) {
+                                                  const float4* __restrict__ dimg, float* __restrict__ g2,
+                                                  float* __restrict__ part) {
   __shared__ float4 s_a[kThreads];
   __shared__ float4 s_b[kThreads];
   __shared__ float4 s_c[kThreads];
   __shared__ uint32_t s_g[kThreads];
   __shared__ float s_acc[kThreads][10];
+  __shared__ float s_stage[kDet ? (kThreads / 32) * 320 : 1];
   __shared__ uint32_t s_max;
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
+  const uint32_t warp = tid >> 5;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
   const bool inside = px < W && py < H;
   const float fx = (float)px, fy = (float)py;
   const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * (tid >> 5));
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key], end = rend[key];
+  (void)end;
   float T = 1.0f, T_final = 1.0f;
   uint32_t last = 0;
   float dC[3] = {0, 0, 0};
@@ -476,6 +488,50 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
   const float bg_dot = bg.x * dC[0] + bg.y * dC[1] + bg.z * dC[2];
   float accum[3] = {0, 0, 0}, last_col[3] = {0, 0, 0};
   float last_alpha = 0.0f;
+
+  // gradient of this pixel w.r.t. pair j of the staged batch (returns false if
+  // the pair does not contribute here); advances the replay state
+  auto pair_grad = [&](int j, uint32_t cur, float* gv) -> bool {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+    if (!(inside && cur < last)) return false;
+    const float4 a = s_a[j];
+    const float4 c4 = s_c[j];
+    const float4 b = s_b[j];
+    const float col[3] = {b.z, b.w, c4.x};
+    const float dx = a.x - fx, dy = a.y - fy;
+    const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+    if (power > 0.0f) return false;
+    const float G = __expf(power);
+    const float araw = b.y * G;
+    const float alpha = fminf(kAlphaMax, araw);
+    if (alpha < kAlphaMin) return false;
+    T = T / (1.0f - alpha);
+    const float wgt = alpha * T;
+    float dL_dalpha = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      accum[c] = last_alpha * last_col[c] + (1.0f - last_alpha) * accum[c];
+      last_col[c] = col[c];
+      dL_dalpha += (col[c] - accum[c]) * dC[c];
+      gv[6 + c] = wgt * dC[c];
+    }
+    dL_dalpha *= T;
+    last_alpha = alpha;
+    dL_dalpha += (-T_final / (1.0f - alpha)) * bg_dot;
+    if (araw <= kAlphaMax) {
+      const float dL_dG = b.y * dL_dalpha;
+      const float gdx = G * dx, gdy = G * dy;
+      gv[0] = dL_dG * (-gdx * a.z - gdy * a.w);   // d/du
+      gv[1] = dL_dG * (-gdy * b.x - gdx * a.w);   // d/dv
+      gv[2] = -0.5f * gdx * dx * dL_dG;           // d/d conic a
+      gv[3] = -gdx * dy * dL_dG;                  // d/d conic b
+      gv[4] = -0.5f * gdy * dy * dL_dG;           // d/d conic c
+      gv[5] = G * dL_dalpha;                      // d/d opacity
+    }
+    return true;
+  };
+
   for (uint32_t bend = start + maxlast; bend > start;) {
     const uint32_t bstart = bend > start + kThreads ? bend - kThreads : start;
     const uint32_t nb = bend - bstart;
@@ -491,68 +547,97 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
 #pragma unroll
     for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
     __syncthreads();
-    for (int j = (int)nb - 1; j >= 0; --j) {
-      const uint32_t cur = bstart + (uint32_t)j - start;
-      const float4 a = s_a[j];
-      const float4 c4 = s_c[j];
-      if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
-      float gv[16];
-#pragma unroll
-      for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
-      bool contrib = false;
-      if (inside && cur < last) {
-        const float4 b = s_b[j];
-        const float col[3] = {b.z, b.w, c4.x};
-        const float dx = a.x - fx, dy = a.y - fy;
-        const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
-        if (power <= 0.0f) {
-          const float G = __expf(power);
-          const float araw = b.y * G;
-          const float alpha = fminf(kAlphaMax, araw);
-          if (alpha >= kAlphaMin) {
-            contrib = true;
-            T = T / (1.0f - alpha);
-            const float wgt = alpha * T;
-            float dL_dalpha = 0.0f;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              accum[c] = last_alpha * last_col[c] + (1.0f - last_alpha) * accum[c];
-              last_col[c] = col[c];
-              dL_dalpha += (col[c] - accum[c]) * dC[c];
-              gv[6 + c] = wgt * dC[c];
-            }
-            dL_dalpha *= T;
-            last_alpha = alpha;
-            dL_dalpha += (-T_final / (1.0f - alpha)) * bg_dot;
-            if (araw <= kAlphaMax) {
-              const float dL_dG = b.y * dL_dalpha;
-              const float gdx = G * dx, gdy = G * dy;
-              gv[0] = dL_dG * (-gdx * a.z - gdy * a.w);   // d/du
-              gv[1] = dL_dG * (-gdy * b.x - gdx * a.w);   // d/dv
-              gv[2] = -0.5f * gdx * dx * dL_dG;           // d/d conic a
-              gv[3] = -gdx * dy * dL_dG;                  // d/d conic b
-              gv[4] = -0.5f * gdy * dy * dL_dG;           // d/d conic c
-              gv[5] = G * dL_dalpha;                      // d/d opacity
-            }
-          }
+    if constexpr (!kDet) {
+      for (int j = (int)nb - 1; j >= 0; --j) {
+        const float4 a = s_a[j];
+        const float4 c4 = s_c[j];
+        if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
+        float gv[16];
+        const bool contrib = pair_grad(j, bstart + (uint32_t)j - start, gv);
+        if (__any_sync(0xffffffffu, contrib)) {
+          const float tot = warp_sum16(gv, lane);
+          const uint32_t k = lane >> 1;
+          if ((lane & 1) == 0 && k < 10) atomicAdd(&s_acc[j][k], tot);
         }
       }
-      if (__any_sync(0xffffffffu, contrib)) {
-        const float tot = warp_sum16(gv, lane);
-        const uint32_t k = lane >> 1;
-        if ((lane & 1) == 0 && k < 10) atomicAdd(&s_acc[j][k], tot);
+    } else {
+      // sub-batches of 32 pairs: warps stage, then one fixed-order fold
+      for (int jhi = (int)nb - 1; jhi >= 0; jhi -= 32) {
+        const int jlo = jhi >= 31 ? jhi - 31 : 0;
+        float* st = s_stage + warp * 320;
+        for (int k = (int)lane; k < 320; k += 32) st[k] = 0.0f;
+        __syncwarp();
+        for (int j = jhi; j >= jlo; --j) {
+          const float4 a = s_a[j];
+          const float4 c4 = s_c[j];
+          if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
+          float gv[16];
+          const bool contrib = pair_grad(j, bstart + (uint32_t)j - start, gv);
+          if (__any_sync(0xffffffffu, contrib)) {
+            const float tot = warp_sum16(gv, lane);
+            const uint32_t k = lane >> 1;
+            if ((lane & 1) == 0 && k < 10) st[(j - jlo) * 10 + (int)k] = tot;
+          }
+        }
+        __syncthreads();
+        for (int t = (int)tid; t < 320; t += kThreads) {
+          const int p = t / 10, k = t % 10;
+          if (jlo + p <= jhi) {
+            float sum = 0.0f;
+#pragma unroll
+            for (int w = 0; w < kThreads / 32; ++w) sum += s_stage[w * 320 + p * 10 + k];
+            s_acc[jlo + p][k] = sum;
+          }
+        }
+        __syncthreads();
       }
     }
     __syncthreads();
     if (tid < nb) {
-      float* dst = g2 + (size_t)s_g[tid] * kG2;
+      if constexpr (kDet) {
+        float* dst = part + (size_t)(bstart + tid) * 10;
 #pragma unroll
-      for (int k = 0; k < 10; ++k) {
-        const float x = s_acc[tid][k];
-        if (x != 0.0f) atomicAdd(dst + k, x);
+        for (int k = 0; k < 10; ++k) dst[k] = s_acc[tid][k];
+      } else {
+        float* dst = g2 + (size_t)s_g[tid] * kG2;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+          const float x = s_acc[tid][k];
+          if (x != 0.0f) atomicAdd(dst + k, x);
+        }
       }
     }
     bend = bstart;
+  }
+}
+
+// deterministic mode: (record, sorted position) pairs to sort by record
+__global__ void k_det_prep(const uint32_t* __restrict__ sorted_vals, const uint32_t* __restrict__ total, uint32_t cap,
+                           uint32_t* __restrict__ keys, uint32_t* __restrict__ pos) {
+  const uint32_t K = min(*total, cap);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < K; p += gridDim.x * blockDim.x) {
+    keys[p] = sorted_vals[p];
+    pos[p] = p;
+  }
+}
+
+// deterministic mode: each record's pair sums added in sorted-pair order
+__global__ void k_det_segsum(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ pos,
+                             const uint32_t* __restrict__ total, uint32_t cap, const float* __restrict__ part,
+                             float* __restrict__ g2) {
+  const uint32_t K = min(*total, cap);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < K; p += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[p];
+    if (p > 0 && keys[p - 1] == k) continue;  // not the first pair of this record
+    float sum[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t q = p; q < K && keys[q] == k; ++q) {
+      const float* src = part + (size_t)pos[q] * 10;
+#pragma unroll
+      for (int c = 0; c < 10; ++c) sum[c] += src[c];
+    }
+    float* dst = g2 + (size_t)k * kG2;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) dst[c] = sum[c];
   }
 }
 
@@ -977,6 +1062,9 @@ struct nps_gs {
   float lr[6] = {1.6e-4f, 5e-3f, 1e-3f, 5e-2f, 2.5e-3f, 2.5e-3f / 20.0f};
   float lambda = 0.2f;
   bool accumulate = false;   // backward adds to the gradients instead of replacing them
+  bool deterministic = false;  // two-pass backward reduction (no float atomics)
+  DevBuf det_part, det_keys, det_pos;
+  SortWork sw_det;
   uint32_t loss_views = 0;   // views the loss is averaged over (0: the views of each call)
   float bg[3] = {0.0f, 0.0f, 0.0f};
   // targets
@@ -1154,7 +1242,9 @@ int nps_gs_destroy(nps_gs* o) {
   for (auto& u : o->gtimers) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (cudaEvent_t e : o->ev_pool) cudaEventDestroy(e);
   for (DevBuf* b : {&o->p_alt, &o->m_alt, &o->v_alt, &o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off,
-                    &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst, &o->afeat, &o->alogits})
+                    &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst, &o->afeat, &o->alogits,
+                    &o->det_part, &o->det_keys, &o->det_pos, &o->sw_det.hist, &o->sw_det.partial,
+                    &o->sw_det.keys_alt, &o->sw_det.vals_alt})
     b->release();
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
                     &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
@@ -1492,11 +1582,35 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   const uint32_t* rend = rstart + (size_t)num_tiles * nv;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
-  { StageTimer t(o, ST_BWD);
-  gs::k_bwd<<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend,
-                                                                 W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
-                                                                 o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>());
-  NPS_CHECK_LAUNCH(); }
+  if (!o->deterministic) {
+    StageTimer t(o, ST_BWD);
+    gs::k_bwd<false><<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(
+        o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
+        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), nullptr);
+    NPS_CHECK_LAUNCH();
+  } else if (o->pair_cap > 0) {
+    StageTimer t(o, ST_BWD);
+    const uint32_t cap = o->pair_cap;
+    NPS_TRY(o->det_part.ensure(sizeof(float) * 10 * (size_t)cap));
+    NPS_TRY(o->det_keys.ensure(sizeof(uint32_t) * (size_t)cap));
+    NPS_TRY(o->det_pos.ensure(sizeof(uint32_t) * (size_t)cap));
+    NPS_CUDA(cudaMemsetAsync(o->det_part.p, 0, sizeof(float) * 10 * (size_t)cap, s));
+    gs::k_bwd<true><<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(
+        o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
+        o->ncontrib.as<uint32_t>(), dimg, nullptr, o->det_part.as<float>());
+    NPS_CHECK_LAUNCH();
+    const uint32_t* total = o->total.as<uint32_t>();
+    gs::k_det_prep<<<4 * kNumSMs, 256, 0, s>>>(o->sorted_vals, total, cap, o->det_keys.as<uint32_t>(),
+                                               o->det_pos.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+    int bits = 1;
+    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)M) ++bits;
+    uint32_t *ko = nullptr, *vo = nullptr;
+    NPS_TRY(radix_sort_u32(o->det_keys.as<uint32_t>(), o->det_pos.as<uint32_t>(), total, cap, bits, o->sw_det, s,
+                           &ko, &vo));
+    gs::k_det_segsum<<<4 * kNumSMs, 256, 0, s>>>(ko, vo, total, cap, o->det_part.as<float>(), o->g2.as<float>());
+    NPS_CHECK_LAUNCH();
+  }
   if (n > 0) {
     StageTimer t(o, ST_PBWD);
     gs::k_project_bwd<<<div_up(n, 128), 128, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
@@ -1969,6 +2083,13 @@ int nps_gs_load(nps_gs* o, const char* path) {
   o->gkey = 0;
   o->skip_seen = 0;
   if (o->h_status) o->h_status[1] = 0;
+  return NPS_OK;
+}
+
+int nps_gs_set_deterministic(nps_gs* o, int enable) {
+  NPS_TRY(check_gs(o));
+  o->deterministic = enable != 0;
+  o->gkey = 0;
   return NPS_OK;
 }
 

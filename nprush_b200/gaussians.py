@@ -162,6 +162,10 @@ class GaussianTrainer:
         v, mem2, k2 = _ptr(adam_v)
         call("nps_gs_write_state", self._h, m, v, int(step), mem if adam_m is not None else mem2)
 
+    def set_deterministic(self, enable: bool):
+        """Two-pass backward reduction without float atomics (bit-reproducible)."""
+        call("nps_gs_set_deterministic", self._h, int(bool(enable)))
+
     def set_accumulate(self, accumulate: bool, loss_views: int = 0):
         call("nps_gs_set_accumulate", self._h, int(bool(accumulate)), int(loss_views))
 
