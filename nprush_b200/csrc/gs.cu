@@ -611,6 +611,156 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
   }
 }
 
+// Per-pixel replay state of the backward.
+struct PixBwd {
+  float T, T_final, bg_dot, last_alpha;
+  float dC[3], accum[3], last_col[3];
+  float fx, fy;
+  uint32_t last;
+  bool inside;
+};
+
+__device__ __forceinline__ void pix_bwd_init(PixBwd& s, uint32_t px, uint32_t py, uint32_t v, uint32_t W, uint32_t H,
+                                             float3 bg, const float4* __restrict__ img,
+                                             const uint32_t* __restrict__ ncontrib,
+                                             const float4* __restrict__ dimg) {
+  s.inside = px < W && py < H;
+  s.fx = (float)px;
+  s.fy = (float)py;
+  s.T = s.T_final = 1.0f;
+  s.last = 0;
+  s.dC[0] = s.dC[1] = s.dC[2] = 0.0f;
+  if (s.inside) {
+    const size_t pix = ((size_t)v * H + py) * W + px;
+    const float4 o = img[pix];
+    s.T = s.T_final = o.w;
+    s.last = ncontrib[pix];
+    const float4 d = dimg[pix];
+    s.dC[0] = d.x; s.dC[1] = d.y; s.dC[2] = d.z;
+  }
+  s.bg_dot = bg.x * s.dC[0] + bg.y * s.dC[1] + bg.z * s.dC[2];
+  s.last_alpha = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) s.accum[c] = s.last_col[c] = 0.0f;
+}
+
+// adds this pixel's gradient w.r.t. the pair (a, b, c4) at sorted offset cur
+// to gv[0..8]; returns whether the pair contributes here
+__device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const float4& b, const float4& c4,
+                                             uint32_t cur, float* gv) {
+  if (!(s.inside && cur < s.last)) return false;
+  const float dx = a.x - s.fx, dy = a.y - s.fy;
+  const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+  if (power > 0.0f) return false;
+  const float G = __expf(power);
+  const float araw = b.y * G;
+  const float alpha = fminf(kAlphaMax, araw);
+  if (alpha < kAlphaMin) return false;
+  s.T = s.T / (1.0f - alpha);
+  const float wgt = alpha * s.T;
+  const float col[3] = {b.z, b.w, c4.x};
+  float dL_dalpha = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    s.accum[c] = s.last_alpha * s.last_col[c] + (1.0f - s.last_alpha) * s.accum[c];
+    s.last_col[c] = col[c];
+    dL_dalpha += (col[c] - s.accum[c]) * s.dC[c];
+    gv[6 + c] += wgt * s.dC[c];
+  }
+  dL_dalpha *= s.T;
+  s.last_alpha = alpha;
+  dL_dalpha += (-s.T_final / (1.0f - alpha)) * s.bg_dot;
+  if (araw <= kAlphaMax) {
+    const float dL_dG = b.y * dL_dalpha;
+    const float gdx = G * dx, gdy = G * dy;
+    gv[0] += dL_dG * (-gdx * a.z - gdy * a.w);
+    gv[1] += dL_dG * (-gdy * b.x - gdx * a.w);
+    gv[2] += -0.5f * gdx * dx * dL_dG;
+    gv[3] += -gdx * dy * dL_dG;
+    gv[4] += -0.5f * gdy * dy * dL_dG;
+    gv[5] += G * dL_dalpha;
+  }
+  return true;
+}
+
+// Backward raster, two vertically adjacent pixels per thread (128 threads per
+// 16 x 16 tile): a warp covers a 16 x 4 strip, and one warp reduction serves
+// 64 pixels.  Per-pair sums go to shared memory (4 warps) and then to the
+// (view, Gaussian) records with global atomics.
+constexpr int kBwdThreads = 128;
+__global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                                      const uint32_t* __restrict__ rstart,
+                                                      const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
+                                                      uint32_t tiles_x, uint32_t num_tiles, float3 bg,
+                                                      const float4* __restrict__ img,
+                                                      const uint32_t* __restrict__ ncontrib,
+                                                      const float4* __restrict__ dimg, float* __restrict__ g2) {
+  __shared__ float4 s_a[kBwdThreads];
+  __shared__ float4 s_b[kBwdThreads];
+  __shared__ float4 s_c[kBwdThreads];
+  __shared__ uint32_t s_g[kBwdThreads];
+  __shared__ float s_acc[kBwdThreads][10];
+  __shared__ uint32_t s_max;
+  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + 2 * (tid >> 4);
+  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 4 * (tid >> 5));
+  const uint32_t key = v * num_tiles + ty * tiles_x + tx;
+  const uint32_t start = rstart[key];
+  PixBwd p0, p1;
+  pix_bwd_init(p0, px, py, v, W, H, bg, img, ncontrib, dimg);
+  pix_bwd_init(p1, px, py + 1, v, W, H, bg, img, ncontrib, dimg);
+  if (tid == 0) s_max = 0;
+  __syncthreads();
+  atomicMax(&s_max, max(p0.last, p1.last));
+  __syncthreads();
+  const uint32_t maxlast = s_max;
+  for (uint32_t bend = start + maxlast; bend > start;) {
+    const uint32_t bstart = bend > start + kBwdThreads ? bend - kBwdThreads : start;
+    const uint32_t nb = bend - bstart;
+    __syncthreads();
+    if (tid < nb) {
+      const uint32_t gg = vals[bstart + tid];
+      const Rec r = recs[gg];
+      s_a[tid] = r.a;
+      s_b[tid] = r.b;
+      s_c[tid] = r.c;
+      s_g[tid] = gg;
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
+    __syncthreads();
+    for (int j = (int)nb - 1; j >= 0; --j) {
+      const float4 a = s_a[j];
+      const float4 c4 = s_c[j];
+      // the pair's alpha >= 1/255 box misses the warp's 16 x 4 strip
+      if ((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + 3.0f))
+        continue;  // warp-uniform
+      const float4 b = s_b[j];
+      const uint32_t cur = bstart + (uint32_t)j - start;
+      float gv[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+      const bool c0 = pix_bwd_pair(p0, a, b, c4, cur, gv);
+      const bool c1 = pix_bwd_pair(p1, a, b, c4, cur, gv);
+      if (__any_sync(0xffffffffu, c0 || c1)) {
+        const float tot = warp_sum16(gv, lane);
+        const uint32_t k = lane >> 1;
+        if ((lane & 1) == 0 && k < 10) atomicAdd(&s_acc[j][k], tot);
+      }
+    }
+    __syncthreads();
+    if (tid < nb) {
+      float* dst = g2 + (size_t)s_g[tid] * kG2;
+#pragma unroll
+      for (int k = 0; k < 10; ++k) {
+        const float x = s_acc[tid][k];
+        if (x != 0.0f) atomicAdd(dst + k, x);
+      }
+    }
+    bend = bstart;
+  }
+}
+
 // deterministic mode: (record, sorted position) pairs to sort by record
 __global__ void k_det_prep(const uint32_t* __restrict__ sorted_vals, const uint32_t* __restrict__ total, uint32_t cap,
                            uint32_t* __restrict__ keys, uint32_t* __restrict__ pos) {
@@ -1584,9 +1734,9 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
   if (!o->deterministic) {
     StageTimer t(o, ST_BWD);
-    gs::k_bwd<false><<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(
+    gs::k_bwd2<<<dim3(tiles_x, tiles_y, nv), gs::kBwdThreads, 0, s>>>(
         o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
-        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), nullptr);
+        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>());
     NPS_CHECK_LAUNCH();
   } else if (o->pair_cap > 0) {
     StageTimer t(o, ST_BWD);
