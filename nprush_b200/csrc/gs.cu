@@ -18,7 +18,7 @@
 //                  (block-wide vote ends the tile), final T and last
 //                  contributor stored per pixel (O(pixels) state, no
 //                  per-pair state)
-//   k_ssim_fwd / k_ssim_bwd / k_loss_reduce: (1 - l) L1 + l (1 - SSIM), 11x11
+//   k_ssim_fwd2 / k_ssim_bwd2 / k_loss_reduce: (1 - l) L1 + l (1 - SSIM), 11x11
 //                  Gaussian window (sigma 1.5), l = 0.2, and dL/dimage
 //   k_bwd          reverse traversal replaying transmittance from the final
 //                  T, per-Gaussian gradients summed over the warp by a
@@ -262,82 +262,114 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
 
 // ------------------------------------------------------------ loss
 // (1 - l) * mean|x - y| + l * (1 - mean SSIM), averaged over views.
-// k_ssim_fwd writes, per pixel and channel, the three maps whose Gaussian
-// correlation gives dL/dx; plus per-block partial sums of |x - y| and SSIM.
+// k_ssim_fwd2 writes, per pixel and channel, the three maps whose Gaussian
+// correlation gives dL/dx, plus per-block partial sums of |x - y| and SSIM;
+// k_ssim_bwd2 correlates the maps and adds the L1 term.
+//
+// 32 x 32 output tiles (input span 42 x 42), zero padding outside the image,
+// register-blocked separable window: the horizontal pass runs 4 consecutive
+// outputs of a row from 14 inputs held in registers, the vertical pass 4
+// consecutive rows of a column.  The gradient maps are planar (V x 9 x H x W)
+// so the backward's halo loads are coalesced.
 constexpr int kHalo = kSsimWin / 2;
-constexpr int kTileP = 16 + 2 * kHalo;  // 26
+constexpr int kLT = 32, kLI = kLT + 2 * kHalo, kLS = kLI + 1;  // 32, 42, row stride 43
+constexpr int kHS = kLT + 1;                                    // row stride of the horizontal sums
+constexpr size_t kSsimFwdSmem = sizeof(float) * (2 * 3 * kLI * kLS + 5 * kLI * kHS);
+constexpr size_t kSsimBwdSmem = sizeof(float) * (3 * kLI * kLS + 3 * kLI * kHS);
 
-__global__ void __launch_bounds__(kThreads) k_ssim_fwd(const float4* __restrict__ img, const float4* __restrict__ tgt,
-                                                       const uint32_t* __restrict__ tgt_ids, uint32_t W, uint32_t H,
-                                                       float lambda, float inv_norm, float* __restrict__ maps,
-                                                       float* __restrict__ partial) {
-  __shared__ float sx[3][kTileP][kTileP];
-  __shared__ float sy[3][kTileP][kTileP];
-  __shared__ float hm[15][kTileP][16];  // horizontal pass: 5 moments x 3 channels
-  __shared__ float red[2][kThreads / 32];
+__global__ void __launch_bounds__(256) k_ssim_fwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                                                   const uint32_t* __restrict__ tgt_ids, uint32_t W, uint32_t H,
+                                                   float lambda, float inv_norm, float* __restrict__ maps,
+                                                   float* __restrict__ partial) {
+  extern __shared__ float sm[];
+  float* sx = sm;                        // [3][kLI][kLS]
+  float* sy = sx + 3 * kLI * kLS;        // [3][kLI][kLS]
+  float* hm = sy + 3 * kLI * kLS;        // [5][kLI][kHS]
+  __shared__ float red[2][8];
   const uint32_t v = blockIdx.z, tid = threadIdx.x;
-  const int ox = blockIdx.x * 16 - kHalo, oy = blockIdx.y * 16 - kHalo;
+  const int ox = blockIdx.x * kLT - kHalo, oy = blockIdx.y * kLT - kHalo;
   const float4* im = img + (size_t)v * W * H;
   const float4* tg = tgt + (size_t)tgt_ids[v] * W * H;
-  for (int e = tid; e < kTileP * kTileP; e += kThreads) {
-    const int ly = e / kTileP, lx = e - ly * kTileP;
+  for (int e = tid; e < kLI * kLI; e += 256) {
+    const int ly = e / kLI, lx = e - ly * kLI;
     const int gx = ox + lx, gy = oy + ly;
     float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0);
     if (gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H) {
       a = im[(size_t)gy * W + gx];
       b = tg[(size_t)gy * W + gx];
     }
-    sx[0][ly][lx] = a.x; sx[1][ly][lx] = a.y; sx[2][ly][lx] = a.z;
-    sy[0][ly][lx] = b.x; sy[1][ly][lx] = b.y; sy[2][ly][lx] = b.z;
+    const int o = ly * kLS + lx;
+    sx[o] = a.x; sx[kLI * kLS + o] = a.y; sx[2 * kLI * kLS + o] = a.z;
+    sy[o] = b.x; sy[kLI * kLS + o] = b.y; sy[2 * kLI * kLS + o] = b.z;
   }
   __syncthreads();
-  for (int e = tid; e < kTileP * 16; e += kThreads) {
-    const int ly = e / 16, lx = e - ly * 16;
-    for (int c = 0; c < 3; ++c) {
-      float m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0;
-#pragma unroll
-      for (int k = 0; k < kSsimWin; ++k) {
-        const float w = c_ssim_w[k];
-        const float x = sx[c][ly][lx + k], y = sy[c][ly][lx + k];
-        m0 += w * x; m1 += w * y; m2 += w * x * x; m3 += w * y * y; m4 += w * x * y;
-      }
-      hm[5 * c + 0][ly][lx] = m0; hm[5 * c + 1][ly][lx] = m1; hm[5 * c + 2][ly][lx] = m2;
-      hm[5 * c + 3][ly][lx] = m3; hm[5 * c + 4][ly][lx] = m4;
-    }
-  }
-  __syncthreads();
-  const int lx = tid & 15, ly = tid >> 4;
-  const int px = blockIdx.x * 16 + lx, py = blockIdx.y * 16 + ly;
-  const bool inside = px < (int)W && py < (int)H;
+  const int col = tid & 31, rg = tid >> 5;  // vertical pass: column, 4-row group
+  const int px = blockIdx.x * kLT + col;
   float l1 = 0.0f, ss = 0.0f;
-  if (inside) {
-    float* mp = maps + (((size_t)v * H + py) * W + px) * 9;
-    for (int c = 0; c < 3; ++c) {
-      float mo[5] = {0, 0, 0, 0, 0};
+  for (int c = 0; c < 3; ++c) {
+    const float* X = sx + c * kLI * kLS;
+    const float* Y = sy + c * kLI * kLS;
+    for (int r = tid; r < kLI * (kLT / 4); r += 256) {
+      const int row = r >> 3, x0 = (r & 7) * 4;
+      float xv[14], yv[14];
 #pragma unroll
-      for (int k = 0; k < kSsimWin; ++k) {
-        const float w = c_ssim_w[k];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) mo[q] += w * hm[5 * c + q][ly + k][lx];
+      for (int j = 0; j < 14; ++j) {
+        xv[j] = X[row * kLS + x0 + j];
+        yv[j] = Y[row * kLS + x0 + j];
       }
-      const float mx = mo[0], my = mo[1];
-      const float sxx = mo[2] - mx * mx, syy = mo[3] - my * my, sxy = mo[4] - mx * my;
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        float m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0;
+#pragma unroll
+        for (int k = 0; k < kSsimWin; ++k) {
+          const float w = c_ssim_w[k], x = xv[o + k], y = yv[o + k];
+          m0 += w * x; m1 += w * y; m2 += w * x * x; m3 += w * y * y; m4 += w * x * y;
+        }
+        const int q = row * kHS + x0 + o;
+        hm[q] = m0; hm[kLI * kHS + q] = m1; hm[2 * kLI * kHS + q] = m2;
+        hm[3 * kLI * kHS + q] = m3; hm[4 * kLI * kHS + q] = m4;
+      }
+    }
+    __syncthreads();
+    float mo[4][5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      float hv[14];
+#pragma unroll
+      for (int j = 0; j < 14; ++j) hv[j] = hm[q * kLI * kHS + (rg * 4 + j) * kHS + col];
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * hv[o + k];
+        mo[o][q] = acc;
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const int py = blockIdx.y * kLT + rg * 4 + o;
+      if (px >= (int)W || py >= (int)H) continue;
+      const float mx = mo[o][0], my = mo[o][1];
+      const float sxx = mo[o][2] - mx * mx, syy = mo[o][3] - my * my, sxy = mo[o][4] - mx * my;
       const float A1 = 2.0f * mx * my + kSsimC1, A2 = 2.0f * sxy + kSsimC2;
       const float B1 = mx * mx + my * my + kSsimC1, B2 = sxx + syy + kSsimC2;
-      const float s = (A1 * A2) / (B1 * B2);
-      ss += s;
+      const float sv = (A1 * A2) / (B1 * B2);
+      ss += sv;
       const float dLds = -lambda * inv_norm;
-      const float ds_dmx = (2.0f * my * A2) / (B1 * B2) - s * 2.0f * mx / B1;
-      const float ds_dsxx = -s / B2;
+      const float ds_dmx = (2.0f * my * A2) / (B1 * B2) - sv * 2.0f * mx / B1;
+      const float ds_dsxx = -sv / B2;
       const float ds_dsxy = 2.0f * A1 / (B1 * B2);
       const float dm = dLds * ds_dmx, d2 = dLds * ds_dsxx, dxy = dLds * ds_dsxy;
-      mp[3 * c + 0] = dm - 2.0f * mx * d2 - my * dxy;
-      mp[3 * c + 1] = d2;
-      mp[3 * c + 2] = dxy;
-      l1 += fabsf(sx[c][ly + kHalo][lx + kHalo] - sy[c][ly + kHalo][lx + kHalo]);
+      const size_t plane = (size_t)W * H, pix = (size_t)py * W + px;
+      float* mp = maps + ((size_t)v * 9 + 3 * c) * plane + pix;
+      mp[0] = dm - 2.0f * mx * d2 - my * dxy;
+      mp[plane] = d2;
+      mp[2 * plane] = dxy;
+      const int cy = rg * 4 + o + kHalo, cx = col + kHalo;
+      l1 += fabsf(X[cy * kLS + cx] - Y[cy * kLS + cx]);
     }
+    __syncthreads();  // before the next channel overwrites the horizontal sums
   }
-  // block partial sums (deterministic order)
   for (int o = 16; o > 0; o >>= 1) {
     l1 += __shfl_xor_sync(0xffffffffu, l1, o);
     ss += __shfl_xor_sync(0xffffffffu, ss, o);
@@ -349,65 +381,96 @@ __global__ void __launch_bounds__(kThreads) k_ssim_fwd(const float4* __restrict_
   __syncthreads();
   if (tid == 0) {
     float a = 0, b = 0;
-    for (int w = 0; w < kThreads / 32; ++w) { a += red[0][w]; b += red[1][w]; }
+    for (int w = 0; w < 8; ++w) { a += red[0][w]; b += red[1][w]; }
     const size_t bi = ((size_t)v * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     partial[2 * bi] = a;
     partial[2 * bi + 1] = b;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_ssim_bwd(const float4* __restrict__ img, const float4* __restrict__ tgt,
-                                                       const uint32_t* __restrict__ tgt_ids, const float* __restrict__ maps,
-                                                       uint32_t W, uint32_t H, float lambda, float inv_norm,
-                                                       float4* __restrict__ dimg) {
-  __shared__ float sm[9][kTileP][kTileP];
-  __shared__ float hm[9][kTileP][16];
+__global__ void __launch_bounds__(256) k_ssim_bwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                                                   const uint32_t* __restrict__ tgt_ids,
+                                                   const float* __restrict__ maps, uint32_t W, uint32_t H,
+                                                   float lambda, float inv_norm, float4* __restrict__ dimg) {
+  extern __shared__ float sm[];
+  float* mp = sm;                    // [3][kLI][kLS]
+  float* hm = mp + 3 * kLI * kLS;    // [3][kLI][kHS]
   const uint32_t v = blockIdx.z, tid = threadIdx.x;
-  const int ox = blockIdx.x * 16 - kHalo, oy = blockIdx.y * 16 - kHalo;
-  const float* mv = maps + (size_t)v * W * H * 9;
-  for (int e = tid; e < kTileP * kTileP; e += kThreads) {
-    const int ly = e / kTileP, lx = e - ly * kTileP;
-    const int gx = ox + lx, gy = oy + ly;
-    const bool ok = gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H;
-    const float* src = mv + ((size_t)(ok ? gy : 0) * W + (ok ? gx : 0)) * 9;
+  const int ox = blockIdx.x * kLT - kHalo, oy = blockIdx.y * kLT - kHalo;
+  const size_t plane = (size_t)W * H;
+  const int col = tid & 31, rg = tid >> 5;
+  const int px = blockIdx.x * kLT + col;
+  const float4* tg = tgt + (size_t)tgt_ids[v] * plane;
+  // this thread's four output pixels
+  float4 xs[4], ys[4];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) sm[q][ly][lx] = ok ? src[q] : 0.0f;
+  for (int o = 0; o < 4; ++o) {
+    const int py = blockIdx.y * kLT + rg * 4 + o;
+    const bool in = px < (int)W && py < (int)H;
+    const size_t pix = in ? (size_t)py * W + px : 0;
+    xs[o] = in ? img[(size_t)v * plane + pix] : make_float4(0, 0, 0, 0);
+    ys[o] = in ? tg[pix] : make_float4(0, 0, 0, 0);
   }
-  __syncthreads();
-  for (int e = tid; e < kTileP * 16; e += kThreads) {
-    const int ly = e / 16, lx = e - ly * 16;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      float acc = 0.0f;
-#pragma unroll
-      for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * sm[q][ly][lx + k];
-      hm[q][ly][lx] = acc;
-    }
-  }
-  __syncthreads();
-  const int lx = tid & 15, ly = tid >> 4;
-  const int px = blockIdx.x * 16 + lx, py = blockIdx.y * 16 + ly;
-  if (px >= (int)W || py >= (int)H) return;
-  float cv[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) {
-    float acc = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * hm[q][ly + k][lx];
-    cv[q] = acc;
-  }
-  const size_t pix = ((size_t)v * H + py) * W + px;
-  const float4 x = img[pix];
-  const float4 y = tgt[(size_t)tgt_ids[v] * W * H + (size_t)py * W + px];
   const float l1w = (1.0f - lambda) * inv_norm;
-  const float xs[3] = {x.x, x.y, x.z}, ys[3] = {y.x, y.y, y.z};
-  float d[3];
+  float d[4][3];
   for (int c = 0; c < 3; ++c) {
-    const float diff = xs[c] - ys[c];
-    const float sgn = diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f);
-    d[c] = cv[3 * c] + 2.0f * xs[c] * cv[3 * c + 1] + ys[c] * cv[3 * c + 2] + l1w * sgn;
+    const float* mv = maps + ((size_t)v * 9 + 3 * c) * plane;
+    for (int e = tid; e < kLI * kLI; e += 256) {
+      const int ly = e / kLI, lx = e - ly * kLI;
+      const int gx = ox + lx, gy = oy + ly;
+      const bool ok = gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H;
+      const size_t g = ok ? (size_t)gy * W + gx : 0;
+      const int o = ly * kLS + lx;
+      mp[o] = ok ? mv[g] : 0.0f;
+      mp[kLI * kLS + o] = ok ? mv[plane + g] : 0.0f;
+      mp[2 * kLI * kLS + o] = ok ? mv[2 * plane + g] : 0.0f;
+    }
+    __syncthreads();
+    for (int r = tid; r < 3 * kLI * (kLT / 4); r += 256) {
+      const int q = r / (kLI * (kLT / 4)), rr = r - q * (kLI * (kLT / 4));
+      const int row = rr >> 3, x0 = (rr & 7) * 4;
+      float mvv[14];
+#pragma unroll
+      for (int j = 0; j < 14; ++j) mvv[j] = mp[q * kLI * kLS + row * kLS + x0 + j];
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * mvv[o + k];
+        hm[q * kLI * kHS + row * kHS + x0 + o] = acc;
+      }
+    }
+    __syncthreads();
+    float cv[4][3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float hv[14];
+#pragma unroll
+      for (int j = 0; j < 14; ++j) hv[j] = hm[q * kLI * kHS + (rg * 4 + j) * kHS + col];
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kSsimWin; ++k) acc += c_ssim_w[k] * hv[o + k];
+        cv[o][q] = acc;
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const float x = c == 0 ? xs[o].x : c == 1 ? xs[o].y : xs[o].z;
+      const float y = c == 0 ? ys[o].x : c == 1 ? ys[o].y : ys[o].z;
+      const float diff = x - y;
+      const float sgn = diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f);
+      d[o][c] = cv[o][0] + 2.0f * x * cv[o][1] + y * cv[o][2] + l1w * sgn;
+    }
+    __syncthreads();  // before the next channel overwrites the staged maps
   }
-  dimg[pix] = make_float4(d[0], d[1], d[2], 0.0f);
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const int py = blockIdx.y * kLT + rg * 4 + o;
+    if (px < (int)W && py < (int)H)
+      dimg[(size_t)v * plane + (size_t)py * W + px] = make_float4(d[o][0], d[o][1], d[o][2], 0.0f);
+  }
 }
 
 __global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblocks, float lambda, float inv_norm,
@@ -1354,6 +1417,15 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
   o->ctx = ctx;
   o->cap = capacity;
   o->n = 0;
+  // kernels with more than 48 KB of dynamic shared memory (set outside any capture)
+  if (cudaFuncSetAttribute(gs::k_ssim_fwd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs::kSsimFwdSmem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(gs::k_ssim_bwd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs::kSsimBwdSmem) !=
+          cudaSuccess) {
+    delete o;
+    set_error("nps_gs_create: cannot raise the loss kernels' shared-memory limit");
+    return NPS_ERR_CUDA;
+  }
   o->sh_deg = (int)sh_degree;
   const size_t pb = sizeof(float) * gsm::kP * (size_t)capacity;
   int rc = NPS_OK;
@@ -1689,7 +1761,7 @@ int nps_gs_loss(nps_gs* o, float* loss3_host) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
   const size_t npix = (size_t)W * H * nv;
-  const dim3 grid(div_up(W, 16), div_up(H, 16), nv);
+  const dim3 grid(div_up(W, gs::kLT), div_up(H, gs::kLT), nv);
   const uint32_t nblocks = grid.x * grid.y * grid.z;
   NPS_TRY(o->maps.ensure(sizeof(float) * 9 * npix));
   NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
@@ -1697,10 +1769,12 @@ int nps_gs_loss(nps_gs* o, float* loss3_host) {
   const uint32_t lv = o->loss_views ? o->loss_views : nv;
   const float inv_norm = (float)(1.0 / (3.0 * (double)W * H * lv));
   { StageTimer t(o, ST_LOSS);
-  gs::k_ssim_fwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H, o->lambda,
-                                               inv_norm, o->maps.as<float>(), o->partial.as<float>());
-  gs::k_ssim_bwd<<<grid, gs::kThreads, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
-                                               o->maps.as<float>(), W, H, o->lambda, inv_norm, o->dimg.as<float4>());
+  gs::k_ssim_fwd2<<<grid, 256, gs::kSsimFwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H,
+                                                     o->lambda, inv_norm, o->maps.as<float>(),
+                                                     o->partial.as<float>());
+  gs::k_ssim_bwd2<<<grid, 256, gs::kSsimBwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
+                                                     o->maps.as<float>(), W, H, o->lambda, inv_norm,
+                                                     o->dimg.as<float4>());
   gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->lambda, inv_norm,
                                                (float)nv / (float)lv, o->loss.as<float>());
   NPS_CHECK_LAUNCH(); }
