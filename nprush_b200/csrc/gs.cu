@@ -855,77 +855,86 @@ __global__ void k_det_segsum(const uint32_t* __restrict__ keys, const uint32_t* 
 }
 
 // ------------------------------------------------------------ projection backward
-__global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ params, uint32_t n, int sh_deg,
+// Eight lanes per Gaussian, each taking the views v = lane, lane + 8, ...: a
+// lane accumulates its views' parameter gradients in record layout (64
+// registers), then the eight partial records are summed by a reduce-scatter
+// over the group (xor 4, 2, 1: 56 shuffles) and lane s writes floats
+// 8s .. 8s + 7 of the Gaussian's gradient record.  The ADC statistic rides in
+// the padding floats 60 and 61 through the reduction.
+template <int DEG>
+__global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ params, uint32_t n,
                                                      const float* __restrict__ views, uint32_t nv, uint32_t W,
-                                                     uint32_t H, const Rec* __restrict__ recs,
-                                                     const uint32_t* __restrict__ counts,
+                                                     uint32_t H, const uint32_t* __restrict__ counts,
                                                      const float* __restrict__ g2, float* __restrict__ grads,
                                                      float* __restrict__ adc_grad, float* __restrict__ adc_denom,
                                                      int accumulate, float adc_scale) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float* p = params + (size_t)i * kP;
+  constexpr int nb = (DEG + 1) * (DEG + 1);
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = t >> 3, sub = t & 7;
+  const bool live = i < n;  // whole groups are live or not (n * 8 threads, groups aligned)
+  if (__all_sync(0xffffffffu, !live)) return;
+  const float* p = params + (size_t)(live ? i : 0) * kP;
   float mean[3] = {p[0], p[1], p[2]};
   float ls[3] = {p[3], p[4], p[5]};
   float q[4] = {p[6], p[7], p[8], p[9]};
-  float gmean[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, gop = 0.0f;
-  float gsh[48];
-  const int nb = (sh_deg + 1) * (sh_deg + 1);
-  for (int k = 0; k < 48; ++k) gsh[k] = 0.0f;
-  float adc_g = 0.0f, adc_n = 0.0f;
-  const float op = sigmoidf(p[kOpacity]);
-  for (uint32_t v = 0; v < nv; ++v) {
-    const size_t g = (size_t)v * n + i;
-    if (counts[g] == 0) continue;
-    const float* gr = g2 + g * kG2;
+  float sh[3 * nb];
+#pragma unroll
+  for (int k = 0; k < 3 * nb; ++k) sh[k] = p[kSH + k];
+  float g[kP];
+#pragma unroll
+  for (int k = 0; k < kP; ++k) g[k] = 0.0f;
+  for (uint32_t v = sub; live && v < nv; v += 8) {
+    const size_t gi = (size_t)v * n + i;
+    if (counts[gi] == 0) continue;
+    const float* gr = g2 + gi * kG2;
     const float du = gr[0], dv = gr[1], dca = gr[2], dcb = gr[3], dcc = gr[4], dop = gr[5];
     const float dcol[3] = {gr[6], gr[7], gr[8]};
     const float* view = views + (size_t)v * kViewRec;
     Proj<float> P;
     project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
     // NDC-space gradient of this view's own loss (the loss is averaged over adc_scale views)
-    adc_g += adc_scale * sqrtf((du * 0.5f * W) * (du * 0.5f * W) + (dv * 0.5f * H) * (dv * 0.5f * H));
-    adc_n += 1.0f;
-    gop += dop;
-    // colour: clamp at 0 blocks the gradient
-    const Rec rc = recs[g];
-    const float colv[3] = {rc.b.z, rc.b.w, rc.c.x};
+    g[60] += adc_scale * sqrtf((du * 0.5f * W) * (du * 0.5f * W) + (dv * 0.5f * H) * (dv * 0.5f * H));
+    g[61] += 1.0f;
+    g[kOpacity] += dop;
     const float ddx = mean[0] - view[32], ddy = mean[1] - view[33], ddz = mean[2] - view[34];
     const float l2 = fmaxf(ddx * ddx + ddy * ddy + ddz * ddz, 1e-20f);
     const float il = rsqrtf(l2);
     const float dir[3] = {ddx * il, ddy * il, ddz * il};
     float basis[16];
-    sh_basis<float>(sh_deg, dir[0], dir[1], dir[2], basis);
+    sh_basis<float>(DEG, dir[0], dir[1], dir[2], basis);
     // the stored colour is clamped; recompute the unclamped value to test the clamp
     float dc[3];
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       float raw = 0.5f;
-      for (int k = 0; k < nb; ++k) raw += basis[k] * p[kSH + 3 * k + c];
+#pragma unroll
+      for (int k = 0; k < nb; ++k) raw += basis[k] * sh[3 * k + c];
       dc[c] = raw < 0.0f ? 0.0f : dcol[c];
-      (void)colv;
     }
-    float ddir[3] = {0, 0, 0};
-    if (sh_deg > 0) {
+    if constexpr (DEG > 0) {
       float bx[16], by[16], bz[16];
-      sh_basis_grad<float>(sh_deg, dir[0], dir[1], dir[2], bx, by, bz);
+      sh_basis_grad<float>(DEG, dir[0], dir[1], dir[2], bx, by, bz);
+      float ddir[3] = {0, 0, 0};
+#pragma unroll
       for (int k = 1; k < nb; ++k) {
-        const float s = p[kSH + 3 * k] * dc[0] + p[kSH + 3 * k + 1] * dc[1] + p[kSH + 3 * k + 2] * dc[2];
+        const float s = sh[3 * k] * dc[0] + sh[3 * k + 1] * dc[1] + sh[3 * k + 2] * dc[2];
         ddir[0] += s * bx[k];
         ddir[1] += s * by[k];
         ddir[2] += s * bz[k];
       }
       const float dd = dir[0] * ddir[0] + dir[1] * ddir[1] + dir[2] * ddir[2];
-      for (int c = 0; c < 3; ++c) gmean[c] += (ddir[c] - dir[c] * dd) * il;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[c] += (ddir[c] - dir[c] * dd) * il;
     }
+#pragma unroll
     for (int k = 0; k < nb; ++k)
-      for (int c = 0; c < 3; ++c) gsh[3 * k + c] += basis[k] * dc[c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[kSH + 3 * k + c] += basis[k] * dc[c];
     // conic -> covariance: dL/dCov = -Inv H Inv, H = [[ga, gb/2], [gb/2, gc]]
     const float ia = P.ca, ib = P.cb, ic = P.cc;
     const float h00 = dca, h01 = 0.5f * dcb, h11 = dcc;
-    // X = H Inv
     const float x00 = h00 * ia + h01 * ib, x01 = h00 * ib + h01 * ic;
     const float x10 = h01 * ia + h11 * ib, x11 = h01 * ib + h11 * ic;
-    // Gc = -Inv X
     const float G00 = -(ia * x00 + ib * x10);
     const float G01 = -(ia * x01 + ib * x11);
     const float G10 = -(ib * x00 + ic * x10);
@@ -933,13 +942,19 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
     const float Gs[2][2] = {{G00, 0.5f * (G01 + G10)}, {0.5f * (G01 + G10), G11}};
     // dL/dSigma = J^T Gs J ; dL/dJ = 2 Gs J Sigma
     float GJ[2][3];
+#pragma unroll
     for (int r = 0; r < 2; ++r)
+#pragma unroll
       for (int c = 0; c < 3; ++c) GJ[r][c] = Gs[r][0] * P.J[0][c] + Gs[r][1] * P.J[1][c];
     float dS[3][3];
+#pragma unroll
     for (int r = 0; r < 3; ++r)
+#pragma unroll
       for (int c = 0; c < 3; ++c) dS[r][c] = P.J[0][r] * GJ[0][c] + P.J[1][r] * GJ[1][c];
     float dJ[2][3];
+#pragma unroll
     for (int r = 0; r < 2; ++r)
+#pragma unroll
       for (int c = 0; c < 3; ++c)
         dJ[r][c] = 2.0f * (GJ[r][0] * P.S[0][c] + GJ[r][1] * P.S[1][c] + GJ[r][2] * P.S[2][c]);
     // J depends on the mean through clip (x, y, w)
@@ -953,52 +968,75 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
       const float d0r3 = dJ[0][0] * r3[0] + dJ[0][1] * r3[1] + dJ[0][2] * r3[2];
       const float d1r1 = dJ[1][0] * r1[0] + dJ[1][1] * r1[1] + dJ[1][2] * r1[2];
       const float d1r3 = dJ[1][0] * r3[0] + dJ[1][1] * r3[1] + dJ[1][2] * r3[2];
+#pragma unroll
       for (int l = 0; l < 3; ++l) {
-        gmean[l] += a * (-d0r0 * r3[l] * iw2 - d0r3 * r0[l] * iw2 + 2.0f * P.cx * d0r3 * r3[l] * iw3);
-        gmean[l] += -b * (-d1r1 * r3[l] * iw2 - d1r3 * r1[l] * iw2 + 2.0f * P.cy * d1r3 * r3[l] * iw3);
-        gmean[l] += P.J[0][l] * du + P.J[1][l] * dv;
+        g[l] += a * (-d0r0 * r3[l] * iw2 - d0r3 * r0[l] * iw2 + 2.0f * P.cx * d0r3 * r3[l] * iw3);
+        g[l] += -b * (-d1r1 * r3[l] * iw2 - d1r3 * r1[l] * iw2 + 2.0f * P.cy * d1r3 * r3[l] * iw3);
+        g[l] += P.J[0][l] * du + P.J[1][l] * dv;
       }
     }
     // Sigma = M M^T, M = R diag(s)
     float dM[3][3];
+#pragma unroll
     for (int r = 0; r < 3; ++r)
+#pragma unroll
       for (int c = 0; c < 3; ++c)
         dM[r][c] = 2.0f * (dS[r][0] * P.M[0][c] + dS[r][1] * P.M[1][c] + dS[r][2] * P.M[2][c]);
     float dR[3][3];
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       float ds = 0.0f;
+#pragma unroll
       for (int r = 0; r < 3; ++r) {
         ds += dM[r][c] * P.R[r][c];
         dR[r][c] = dM[r][c] * P.sc[c];
       }
-      gls[c] += ds * P.sc[c];
+      g[kLogScale + c] += ds * P.sc[c];
     }
     float dqn[4];
     rot_grad_to_quat<float>(P.qn[0], P.qn[1], P.qn[2], P.qn[3], dR, dqn);
     const float qd = P.qn[0] * dqn[0] + P.qn[1] * dqn[1] + P.qn[2] * dqn[2] + P.qn[3] * dqn[3];
-    for (int k = 0; k < 4; ++k) gq[k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
-  }
-  float* out = grads + (size_t)i * kP;
-  float g[kP];
-  g[0] = gmean[0]; g[1] = gmean[1]; g[2] = gmean[2];
-  g[3] = gls[0]; g[4] = gls[1]; g[5] = gls[2];
-  g[6] = gq[0]; g[7] = gq[1]; g[8] = gq[2]; g[9] = gq[3];
-  g[10] = gop * op * (1.0f - op);
-  g[11] = 0.0f;
-  for (int k = 0; k < 48; ++k) g[kSH + k] = gsh[k];
-  g[60] = g[61] = g[62] = g[63] = 0.0f;
-  float4* out4 = reinterpret_cast<float4*>(out);
 #pragma unroll
-  for (int k = 0; k < kP / 4; ++k) {
-    float4 w = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
-    if (accumulate) {
-      const float4 a = out4[k];
-      w.x += a.x; w.y += a.y; w.z += a.z; w.w += a.w;
-    }
-    out4[k] = w;
+    for (int k = 0; k < 4; ++k) g[kQuat + k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
   }
-  adc_grad[i] += adc_g;
-  adc_denom[i] += adc_n;
+  // reduce-scatter over the group's eight lanes
+  const bool b2 = sub & 4, b1 = sub & 2, b0 = sub & 1;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const float send = b2 ? g[j] : g[j + 32], keep = b2 ? g[j + 32] : g[j];
+    g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float send = b1 ? g[j] : g[j + 16], keep = b1 ? g[j + 16] : g[j];
+    g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float send = b0 ? g[j] : g[j + 8], keep = b0 ? g[j + 8] : g[j];
+    g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+  }
+  if (!live) return;
+  // this lane holds record floats 8 * sub .. 8 * sub + 7 in g[0..7]
+  if (sub == 1) {
+    const float op = sigmoidf(p[kOpacity]);
+    g[kOpacity - 8] *= op * (1.0f - op);
+    g[11 - 8] = 0.0f;
+  }
+  if (sub == 7) {
+    adc_grad[i] += g[60 - 56];
+    adc_denom[i] += g[61 - 56];
+    g[4] = g[5] = g[6] = g[7] = 0.0f;
+  }
+  float4* out4 = reinterpret_cast<float4*>(grads + (size_t)i * kP + 8 * sub);
+  float4 w0 = make_float4(g[0], g[1], g[2], g[3]), w1 = make_float4(g[4], g[5], g[6], g[7]);
+  if (accumulate) {
+    const float4 a0 = out4[0], a1 = out4[1];
+    w0.x += a0.x; w0.y += a0.y; w0.z += a0.z; w0.w += a0.w;
+    w1.x += a1.x; w1.y += a1.y; w1.z += a1.z; w1.w += a1.w;
+  }
+  out4[0] = w0;
+  out4[1] = w1;
 }
 
 // ------------------------------------------------------------ Adam
@@ -1837,11 +1875,20 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   }
   if (n > 0) {
     StageTimer t(o, ST_PBWD);
-    gs::k_project_bwd<<<div_up(n, 128), 128, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
-                                                     H, o->recs.as<gs::Rec>(), o->counts.as<uint32_t>(),
-                                                     o->g2.as<float>(), o->grads.as<float>(), o->adc_grad.as<float>(),
-                                                     o->adc_denom.as<float>(), o->accumulate ? 1 : 0,
-                                                     (float)(o->loss_views ? o->loss_views : nv));
+    const uint32_t blocks = div_up((size_t)n * 8, 128);
+    const float adc_scale = (float)(o->loss_views ? o->loss_views : nv);
+#define NPS_PBWD(D)                                                                                             \
+  gs::k_project_bwd<D><<<blocks, 128, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, W, H,         \
+                                               o->counts.as<uint32_t>(), o->g2.as<float>(), o->grads.as<float>(), \
+                                               o->adc_grad.as<float>(), o->adc_denom.as<float>(),                 \
+                                               o->accumulate ? 1 : 0, adc_scale)
+    switch (o->sh_deg) {
+      case 0: NPS_PBWD(0); break;
+      case 1: NPS_PBWD(1); break;
+      case 2: NPS_PBWD(2); break;
+      default: NPS_PBWD(3); break;
+    }
+#undef NPS_PBWD
     NPS_CHECK_LAUNCH();
   }
   return NPS_OK;
