@@ -20,13 +20,14 @@
 //                  per-pair state)
 //   k_ssim_fwd2 / k_ssim_bwd2 / k_loss_reduce: (1 - l) L1 + l (1 - SSIM), 11x11
 //                  Gaussian window (sigma 1.5), l = 0.2, and dL/dimage
-//   k_bwd          reverse traversal replaying transmittance from the final
-//                  T, per-Gaussian gradients summed over the warp by a
-//                  16-shuffle reduce-scatter, then over the CTA in shared memory, then one
-//                  global atomic per (tile, Gaussian, value)
-//   k_project_bwd  one thread per Gaussian looping over the views:
-//                  screen-space gradients -> parameter gradients (no
-//                  atomics: deterministic), ADC statistics
+//   k_bwd2         reverse traversal replaying transmittance from the final
+//                  T, two pixels per thread, per-Gaussian gradients summed
+//                  over the warp by a 16-shuffle reduce-scatter, then over the
+//                  CTA in shared memory, then one global atomic per (tile,
+//                  Gaussian, value); k_bwd<true> + k_det_segsum: the
+//                  deterministic two-pass variant
+//   k_project_bwd  eight lanes per Gaussian over the views: screen-space
+//                  gradients -> parameter gradients, ADC statistics
 //   k_adam         fused Adam over the 59 parameters of every Gaussian
 #include <cuda_runtime.h>
 
@@ -98,7 +99,8 @@ __device__ __forceinline__ float warp_sum16(float (&v)[16], uint32_t lane) {
 __device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(-x)); }
 
 // ------------------------------------------------------------ preprocess
-__global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ params, uint32_t n, int sh_deg,
+template <int DEG>
+__global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ params, uint32_t n,
                                                     const float* __restrict__ views, uint32_t nv, uint32_t W,
                                                     uint32_t H, uint32_t tiles_x, uint32_t tiles_y,
                                                     Rec* __restrict__ recs, uint32_t* __restrict__ counts,
@@ -141,9 +143,10 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
       const float dx = mean[0] - view[32], dy = mean[1] - view[33], dz = mean[2] - view[34];
       const float il = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-20f));
       float basis[16];
-      sh_basis<float>(sh_deg, dx * il, dy * il, dz * il, basis);
-      const int nb = (sh_deg + 1) * (sh_deg + 1);
+      sh_basis<float>(DEG, dx * il, dy * il, dz * il, basis);
+      constexpr int nb = (DEG + 1) * (DEG + 1);
       float col[3] = {0.5f, 0.5f, 0.5f};
+#pragma unroll
       for (int k = 0; k < nb; ++k) {
         col[0] += basis[k] * p[kSH + 3 * k + 0];
         col[1] += basis[k] * p[kSH + 3 * k + 1];
@@ -1723,10 +1726,18 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   const uint32_t* vs = o->counts.as<uint32_t>();
   if (M > 0) {
     { StageTimer t_pre(o, ST_PRE);
-    gs::k_preprocess<<<div_up(M, 256), 256, 0, s>>>(o->params.as<float>(), n, o->sh_deg, o->views.as<float>(), nv, W,
-                                                     H, tiles_x, tiles_y, o->recs.as<gs::Rec>(),
-                                                     o->counts.as<uint32_t>(), o->rects.as<uint2>(),
-                                                     o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>());
+#define NPS_PRE(D)                                                                                          \
+  gs::k_preprocess<D><<<div_up(M, 256), 256, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, W, H, \
+                                                      tiles_x, tiles_y, o->recs.as<gs::Rec>(),                  \
+                                                      o->counts.as<uint32_t>(), o->rects.as<uint2>(),           \
+                                                      o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>())
+    switch (o->sh_deg) {
+      case 0: NPS_PRE(0); break;
+      case 1: NPS_PRE(1); break;
+      case 2: NPS_PRE(2); break;
+      default: NPS_PRE(3); break;
+    }
+#undef NPS_PRE
     NPS_CHECK_LAUNCH(); }
     k_set_u32<<<1, 1, 0, s>>>(o->mcount.as<uint32_t>(), (uint32_t)M);
     uint32_t *dk = nullptr, *dv = nullptr;

@@ -2,8 +2,8 @@
 //
 // Used for the (view, tile[, depth]) keys of the binning stage.  The sort is a
 // fixed-grid reduce-then-scan radix sort: per 8-bit digit, an upsweep kernel
-// histograms each block's contiguous key range, one block scans the
-// digit-major histogram, and a downsweep kernel ranks keys stably
+// histograms each block's contiguous key range, a three-kernel scan turns the
+// digit-major histogram into offsets, and a downsweep kernel ranks keys stably
 // (warp-level __match_any_sync ranking in original order) and scatters them.
 // The grid never depends on the key count (read from device memory), so the
 // whole sort can be captured in a CUDA graph, and there is no inter-block
@@ -219,7 +219,9 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
 template <class K>
 int radix_sort_impl(K* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t cap, int bits, SortWork& w,
                     cudaStream_t s, K** keys_out, uint32_t** vals_out) {
-  NPS_TRY(w.hist.ensure(sizeof(uint32_t) * 256 * kSortGrid));
+  NPS_TRY(w.hist.ensure(sizeof(uint32_t) * (256 * kSortGrid + 1)));
+  constexpr uint32_t kHist = 256 * kSortGrid;
+  NPS_TRY(w.partial.ensure(sizeof(uint32_t) * (div_up(kHist, kScanTile) + 1)));
   NPS_TRY(w.keys_alt.ensure(sizeof(K) * (size_t)cap));
   NPS_TRY(w.vals_alt.ensure(sizeof(uint32_t) * (size_t)cap));
   K* ka = keys;
@@ -229,7 +231,10 @@ int radix_sort_impl(K* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t
   uint32_t* hist = w.hist.as<uint32_t>();
   for (int shift = 0; shift < bits; shift += 8) {
     k_upsweep<K><<<kSortGrid, kSortThreads, 0, s>>>(ka, count_dev, cap, shift, hist);
-    k_scan_single<<<1, kScanThreads, 0, s>>>(hist, 256 * kSortGrid, nullptr);
+    // digit-major histogram -> scatter offsets (multi-block scan, in place)
+    k_scan_reduce<<<div_up(kHist, kScanTile), kScanThreads, 0, s>>>(hist, kHist, w.partial.as<uint32_t>());
+    k_scan_single<<<1, kScanThreads, 0, s>>>(w.partial.as<uint32_t>(), div_up(kHist, kScanTile), hist + kHist);
+    k_scan_down<<<div_up(kHist, kScanTile), kScanThreads, 0, s>>>(hist, kHist, w.partial.as<uint32_t>(), hist);
     k_downsweep<K><<<kSortGrid, kSortThreads, 0, s>>>(ka, va, kb, vb, count_dev, cap, shift, hist);
     NPS_CHECK_LAUNCH();
     K* tk = ka; ka = kb; kb = tk;
