@@ -233,10 +233,27 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
     }
     __syncthreads();
     const uint32_t nb = min((uint32_t)kThreads, end - base);
-    for (uint32_t j = 0; j < nb && !done; ++j) {
+    // staged pairs whose alpha >= 1/255 box meets the warp's two rows (one
+    // lane tests eight pairs; the warp then walks the set bits in order)
+    uint32_t hit[kThreads / 32];
+#pragma unroll
+    for (int qq = 0; qq < kThreads / 32; ++qq) {
+      const uint32_t jj = qq * 32 + (tid & 31);
+      bool h = false;
+      if (jj < nb) {
+        const float4 a = s_a[jj];
+        const float4 c4 = s_c[jj];
+        h = !warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0);
+      }
+      hit[qq] = __ballot_sync(0xffffffffu, h);
+    }
+    for (int qq = 0; qq < kThreads / 32 && !done; ++qq)
+    for (uint32_t m = hit[qq]; m != 0u && !done;) {
+      const int bit = __ffs(m) - 1;
+      m &= m - 1u;
+      const uint32_t j = qq * 32 + bit;
       const float4 a = s_a[j];
       const float4 c4 = s_c[j];
-      if (warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0)) continue;  // warp-uniform
       const float4 b = s_b[j];
       const float dx = a.x - fx, dy = a.y - fy;
       const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
@@ -780,6 +797,9 @@ __global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ re
   atomicMax(&s_max, max(p0.last, p1.last));
   __syncthreads();
   const uint32_t maxlast = s_max;
+  uint32_t wlast = max(p0.last, p1.last);  // pairs at or beyond every pixel's last contributor are skipped
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
   for (uint32_t bend = start + maxlast; bend > start;) {
     const uint32_t bstart = bend > start + kBwdThreads ? bend - kBwdThreads : start;
     const uint32_t nb = bend - bstart;
@@ -795,12 +815,29 @@ __global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ re
 #pragma unroll
     for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
     __syncthreads();
-    for (int j = (int)nb - 1; j >= 0; --j) {
+    // which staged pairs this warp must visit: the pair's alpha >= 1/255 box
+    // meets the warp's 16 x 4 strip and some pixel of the warp reached it
+    // (one lane tests four pairs; the warp then walks the set bits)
+    uint32_t hit[kBwdThreads / 32];
+#pragma unroll
+    for (int qq = 0; qq < kBwdThreads / 32; ++qq) {
+      const uint32_t jj = qq * 32 + lane;
+      bool h = false;
+      if (jj < nb && bstart + jj - start < wlast) {
+        const float4 a = s_a[jj];
+        const float4 c4 = s_c[jj];
+        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + 3.0f));
+      }
+      hit[qq] = __ballot_sync(0xffffffffu, h);
+    }
+#pragma unroll
+    for (int qq = kBwdThreads / 32 - 1; qq >= 0; --qq)
+    for (uint32_t m = hit[qq]; m != 0u;) {
+      const int bit = 31 - __clz(m);
+      m &= ~(1u << bit);
+      const int j = qq * 32 + bit;  // descending within the batch
       const float4 a = s_a[j];
       const float4 c4 = s_c[j];
-      // the pair's alpha >= 1/255 box misses the warp's 16 x 4 strip
-      if ((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + 3.0f))
-        continue;  // warp-uniform
       const float4 b = s_b[j];
       const uint32_t cur = bstart + (uint32_t)j - start;
       float gv[16];
