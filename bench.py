@@ -146,12 +146,17 @@ def run_ours(args, rank, world):
         vp, vpi, tg, st = build_scene(dev)
         torch.cuda.synchronize()
         st.set_targets(tg, borrow=True)
+        rng = np.random.default_rng(1234)
+        sched = [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(args.warmup + args.steps + 4)]
+        tuned = None
+        if not args.no_autotune:
+            # raster variants (pixels per thread) timed on this workload
+            st.set_views(vp[sched[0]], vpi[sched[0]], sched[0])
+            tuned = st.autotune()
         st.set_graph(not args.no_graph)  # whole step captured as one CUDA graph
         # stage timers are event-record nodes of the graph, so they must be on
         # when the first (capturing) step runs
         st.set_timing(not args.no_stage_timing)
-        rng = np.random.default_rng(1234)
-        sched = [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(args.warmup + args.steps + 4)]
         flush = torch.empty(64 * 1024 * 1024, device=f"cuda:{dev}")  # 256 MB > L2
 
         def step(k):
@@ -200,7 +205,7 @@ def run_ours(args, rank, world):
                 e2e_times.append(dt * 1000.0)
         h2d = VIEWS * HEIGHT * WIDTH * 4 * 4 + VIEWS * (32 * 4 + 4)
         d2h = 3 * 4
-    return dict(ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
+    return dict(tuned=tuned, ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
                 clocks=clk.summary(), e2e_ms=float(np.mean(e2e_times)), h2d=h2d, d2h=d2h, loss=loss_last)
 
 
@@ -334,6 +339,7 @@ def main():
     ap.add_argument("--no-flush", action="store_true", help="do not flush L2 between timed steps")
     ap.add_argument("--no-stage-timing", action="store_true", help="no per-stage CUDA events")
     ap.add_argument("--no-graph", action="store_true", help="launch the step eagerly instead of as a CUDA graph")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default raster variants")
     args = ap.parse_args()
     global N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS
     if args.gaussians:
@@ -388,7 +394,10 @@ def main():
                    "views_per_step": VIEWS,
                    "l2": "not flushed" if args.no_flush else "flushed between timed steps (256 MB write)",
                    "pairs_per_step": K, "parallelism": "replicas" if world > 1 else "single GPU",
-                   "cuda_graph": not args.no_graph},
+                   "cuda_graph": not args.no_graph,
+                   "raster_variant": (None if res.get("tuned") is None else
+                                      {"fwd_pixels_per_thread": res["tuned"]["fwd_ppt"],
+                                       "bwd_pixels_per_thread": res["tuned"]["bwd_ppt"], "chosen_by": "autotuner"})},
         "clocks": res["clocks"],
         "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"]},

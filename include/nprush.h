@@ -242,6 +242,16 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
+/* Raster variants (no reference counterpart): forward and backward raster
+ * kernels exist with 1, 2 or 4 vertically adjacent pixels per thread (256,
+ * 128 or 64 threads per 16 x 16 tile, as many records staged per batch).
+ * nps_gs_autotune times all of them on the current views and targets and
+ * keeps the fastest; with cache_path it first looks the workload up in that
+ * text file (device, image size, views, SH degree, Gaussian count to ~19%)
+ * and appends its choice.  times_ms6 (may be null): forward then backward
+ * time of each variant (-1 when the choice came from the cache). */
+int nps_gs_set_variant(nps_gs* gs, int fwd_ppt, int bwd_ppt);
+int nps_gs_autotune(nps_gs* gs, const char* cache_path, int* fwd_ppt_out, int* bwd_ppt_out, float* times_ms6);
 /* Deterministic mode: the backward reduces each (view, Gaussian) gradient in
  * two passes (per-pair tile sums stored, then summed per record in sorted-pair
  * order) instead of with float atomics, so repeated runs are bit-identical.

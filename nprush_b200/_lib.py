@@ -107,6 +107,8 @@ SIGNATURES = {
     "nps_gs_stage_times": [P, P, P, U32, I32],
     "nps_gs_assign_ids": [P, U32],
     "nps_gs_set_deterministic": [P, I32],
+    "nps_gs_set_variant": [P, I32, I32],
+    "nps_gs_autotune": [P, ctypes.c_char_p, P, P, P],
     "nps_gs_adc_features": [P, F32, F32, F32, F32, P, P, P],
     "nps_gs_adc_policy": [P, P, F32, F32, F32, F32, P, P],
     "nps_mlp_num_params": [],

@@ -204,26 +204,42 @@ __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __re
 }
 
 // ------------------------------------------------------------ forward raster
-__global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
-                                                  const uint32_t* __restrict__ rstart,
-                                                  const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
-                                                  uint32_t tiles_x, uint32_t num_tiles, float3 bg,
-                                                  float4* __restrict__ img, uint32_t* __restrict__ ncontrib) {
-  __shared__ float4 s_a[kThreads];
-  __shared__ float4 s_b[kThreads];
-  __shared__ float4 s_c[kThreads];
+// Forward raster, PPT vertically adjacent pixels per thread: 256 / PPT
+// threads per 16 x 16 tile, records staged 256 / PPT at a time, a warp
+// covers a 16 x 2·PPT strip.  PPT is the autotuned variant (1, 2 or 4).
+template <int PPT>
+__global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                                   const uint32_t* __restrict__ rstart,
+                                                   const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
+                                                   uint32_t tiles_x, uint32_t num_tiles, float3 bg,
+                                                   float4* __restrict__ img, uint32_t* __restrict__ ncontrib) {
+  constexpr int NT = 256 / PPT;
+  __shared__ float4 s_a[NT];
+  __shared__ float4 s_b[NT];
+  __shared__ float4 s_c[NT];
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
-  const bool inside = px < W && py < H;
-  const float fx = (float)px, fy = (float)py;
-  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * (tid >> 5));
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
+  const float fx = (float)px;
+  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * (tid >> 5));
+  constexpr float wh = (float)(2 * PPT - 1);
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key], end = rend[key];
-  float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
-  uint32_t last = 0;
-  bool done = !inside;
-  for (uint32_t base = start; base < end; base += kThreads) {
-    if (__syncthreads_count(done) == kThreads) break;
+  float T[PPT], C0[PPT], C1[PPT], C2[PPT];
+  uint32_t last[PPT];
+  bool dn[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    T[k] = 1.0f; C0[k] = C1[k] = C2[k] = 0.0f; last[k] = 0;
+    dn[k] = !(px < W && py + k < H);
+  }
+  auto all_done = [&]() {
+    bool d = true;
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) d = d && dn[k];
+    return d;
+  };
+  for (uint32_t base = start; base < end; base += NT) {
+    if (__syncthreads_count(all_done()) == NT) break;
     const uint32_t idx = base + tid;
     if (idx < end) {
       const Rec r = recs[vals[idx]];
@@ -232,22 +248,23 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
       s_c[tid] = r.c;
     }
     __syncthreads();
-    const uint32_t nb = min((uint32_t)kThreads, end - base);
-    // staged pairs whose alpha >= 1/255 box meets the warp's two rows (one
-    // lane tests eight pairs; the warp then walks the set bits in order)
-    uint32_t hit[kThreads / 32];
+    const uint32_t nb = min((uint32_t)NT, end - base);
+    // staged pairs whose alpha >= 1/255 box meets the warp's strip (one lane
+    // tests NT / 32 pairs; the warp then walks the set bits in order)
+    uint32_t hit[NT / 32];
 #pragma unroll
-    for (int qq = 0; qq < kThreads / 32; ++qq) {
+    for (int qq = 0; qq < NT / 32; ++qq) {
       const uint32_t jj = qq * 32 + (tid & 31);
       bool h = false;
       if (jj < nb) {
         const float4 a = s_a[jj];
         const float4 c4 = s_c[jj];
-        h = !warp_misses(a.x, a.y, c4.z, c4.w, wx0, wy0);
+        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
       }
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
-    for (int qq = 0; qq < kThreads / 32 && !done; ++qq)
+    bool done = all_done();
+    for (int qq = 0; qq < NT / 32 && !done; ++qq)
     for (uint32_t m = hit[qq]; m != 0u && !done;) {
       const int bit = __ffs(m) - 1;
       m &= m - 1u;
@@ -255,28 +272,37 @@ __global__ void __launch_bounds__(kThreads) k_fwd(const Rec* __restrict__ recs, 
       const float4 a = s_a[j];
       const float4 c4 = s_c[j];
       const float4 b = s_b[j];
-      const float dx = a.x - fx, dy = a.y - fy;
-      const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
-      if (power > 0.0f) continue;
-      const float alpha = fminf(kAlphaMax, b.y * __expf(power));
-      if (alpha < kAlphaMin) continue;
-      const float test_T = T * (1.0f - alpha);
-      if (test_T < kTMin) {
-        done = true;
-        break;
+      const float dx = a.x - fx;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        if (dn[k]) continue;
+        const float dy = a.y - (float)(py + k);
+        const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+        if (power > 0.0f) continue;
+        const float alpha = fminf(kAlphaMax, b.y * __expf(power));
+        if (alpha < kAlphaMin) continue;
+        const float test_T = T[k] * (1.0f - alpha);
+        if (test_T < kTMin) {
+          dn[k] = true;
+          continue;
+        }
+        const float w = alpha * T[k];
+        C0[k] += b.z * w;
+        C1[k] += b.w * w;
+        C2[k] += c4.x * w;
+        T[k] = test_T;
+        last[k] = base - start + j + 1;
       }
-      const float w = alpha * T;
-      C0 += b.z * w;
-      C1 += b.w * w;
-      C2 += c4.x * w;
-      T = test_T;
-      last = base - start + j + 1;
+      done = all_done();
     }
   }
-  if (inside) {
-    const size_t pix = ((size_t)v * H + py) * W + px;
-    img[pix] = make_float4(C0 + T * bg.x, C1 + T * bg.y, C2 + T * bg.z, T);
-    ncontrib[pix] = last;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    if (px < W && py + k < H) {
+      const size_t pix = ((size_t)v * H + py + k) * W + px;
+      img[pix] = make_float4(C0[k] + T[k] * bg.x, C1[k] + T[k] * bg.y, C2[k] + T[k] * bg.z, T[k]);
+      ncontrib[pix] = last[k];
+    }
   }
 }
 
@@ -766,42 +792,50 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
   return true;
 }
 
-// Backward raster, two vertically adjacent pixels per thread (128 threads per
-// 16 x 16 tile): a warp covers a 16 x 4 strip, and one warp reduction serves
-// 64 pixels.  Per-pair sums go to shared memory (4 warps) and then to the
-// (view, Gaussian) records with global atomics.
-constexpr int kBwdThreads = 128;
-__global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
-                                                      const uint32_t* __restrict__ rstart,
-                                                      const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
-                                                      uint32_t tiles_x, uint32_t num_tiles, float3 bg,
-                                                      const float4* __restrict__ img,
-                                                      const uint32_t* __restrict__ ncontrib,
-                                                      const float4* __restrict__ dimg, float* __restrict__ g2) {
-  __shared__ float4 s_a[kBwdThreads];
-  __shared__ float4 s_b[kBwdThreads];
-  __shared__ float4 s_c[kBwdThreads];
-  __shared__ uint32_t s_g[kBwdThreads];
-  __shared__ float s_acc[kBwdThreads][10];
+// Backward raster, PPT vertically adjacent pixels per thread (256 / PPT
+// threads per 16 x 16 tile, a warp covers a 16 x 2·PPT strip): one warp
+// reduction serves 32·PPT pixels.  The warp first ballots the staged pairs
+// that meet its strip and that some of its pixels reached, then walks them in
+// reverse order.  Per-pair sums go to shared memory and then to the (view,
+// Gaussian) records with global atomics.  PPT is the autotuned variant.
+template <int PPT>
+__global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                                    const uint32_t* __restrict__ rstart,
+                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
+                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
+                                                    const float4* __restrict__ img,
+                                                    const uint32_t* __restrict__ ncontrib,
+                                                    const float4* __restrict__ dimg, float* __restrict__ g2) {
+  constexpr int NT = 256 / PPT;
+  __shared__ float4 s_a[NT];
+  __shared__ float4 s_b[NT];
+  __shared__ float4 s_c[NT];
+  __shared__ uint32_t s_g[NT];
+  __shared__ float s_acc[NT][10];
   __shared__ uint32_t s_max;
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + 2 * (tid >> 4);
-  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 4 * (tid >> 5));
+  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
+  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * (tid >> 5));
+  constexpr float wh = (float)(2 * PPT - 1);
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key];
-  PixBwd p0, p1;
-  pix_bwd_init(p0, px, py, v, W, H, bg, img, ncontrib, dimg);
-  pix_bwd_init(p1, px, py + 1, v, W, H, bg, img, ncontrib, dimg);
+  PixBwd p[PPT];
+  uint32_t mylast = 0;
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    pix_bwd_init(p[k], px, py + k, v, W, H, bg, img, ncontrib, dimg);
+    mylast = max(mylast, p[k].last);
+  }
   if (tid == 0) s_max = 0;
   __syncthreads();
-  atomicMax(&s_max, max(p0.last, p1.last));
+  atomicMax(&s_max, mylast);
   __syncthreads();
   const uint32_t maxlast = s_max;
-  uint32_t wlast = max(p0.last, p1.last);  // pairs at or beyond every pixel's last contributor are skipped
+  uint32_t wlast = mylast;  // pairs at or beyond every pixel's last contributor are skipped
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
   for (uint32_t bend = start + maxlast; bend > start;) {
-    const uint32_t bstart = bend > start + kBwdThreads ? bend - kBwdThreads : start;
+    const uint32_t bstart = bend > start + NT ? bend - NT : start;
     const uint32_t nb = bend - bstart;
     __syncthreads();
     if (tid < nb) {
@@ -815,23 +849,20 @@ __global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ re
 #pragma unroll
     for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
     __syncthreads();
-    // which staged pairs this warp must visit: the pair's alpha >= 1/255 box
-    // meets the warp's 16 x 4 strip and some pixel of the warp reached it
-    // (one lane tests four pairs; the warp then walks the set bits)
-    uint32_t hit[kBwdThreads / 32];
+    uint32_t hit[NT / 32];
 #pragma unroll
-    for (int qq = 0; qq < kBwdThreads / 32; ++qq) {
+    for (int qq = 0; qq < NT / 32; ++qq) {
       const uint32_t jj = qq * 32 + lane;
       bool h = false;
       if (jj < nb && bstart + jj - start < wlast) {
         const float4 a = s_a[jj];
         const float4 c4 = s_c[jj];
-        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + 3.0f));
+        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
       }
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
 #pragma unroll
-    for (int qq = kBwdThreads / 32 - 1; qq >= 0; --qq)
+    for (int qq = NT / 32 - 1; qq >= 0; --qq)
     for (uint32_t m = hit[qq]; m != 0u;) {
       const int bit = 31 - __clz(m);
       m &= ~(1u << bit);
@@ -843,19 +874,20 @@ __global__ void __launch_bounds__(kBwdThreads) k_bwd2(const Rec* __restrict__ re
       float gv[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
-      const bool c0 = pix_bwd_pair(p0, a, b, c4, cur, gv);
-      const bool c1 = pix_bwd_pair(p1, a, b, c4, cur, gv);
-      if (__any_sync(0xffffffffu, c0 || c1)) {
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, b, c4, cur, gv);
+      if (__any_sync(0xffffffffu, any)) {
         const float tot = warp_sum16(gv, lane);
         const uint32_t k = lane >> 1;
-        if ((lane & 1) == 0 && k < 10) atomicAdd(&s_acc[j][k], tot);
+        if ((lane & 1) == 0 && k < 9) atomicAdd(&s_acc[j][k], tot);
       }
     }
     __syncthreads();
     if (tid < nb) {
       float* dst = g2 + (size_t)s_g[tid] * kG2;
 #pragma unroll
-      for (int k = 0; k < 10; ++k) {
+      for (int k = 0; k < 9; ++k) {
         const float x = s_acc[tid][k];
         if (x != 0.0f) atomicAdd(dst + k, x);
       }
@@ -1354,6 +1386,7 @@ struct nps_gs {
   float lambda = 0.2f;
   bool accumulate = false;   // backward adds to the gradients instead of replacing them
   bool deterministic = false;  // two-pass backward reduction (no float atomics)
+  int fwd_ppt = 1, bwd_ppt = 2;  // raster variants: pixels per thread (1, 2, 4); see nps_gs_autotune
   DevBuf det_part, det_keys, det_pos;
   SortWork sw_det;
   uint32_t loss_views = 0;   // views the loss is averaged over (0: the views of each call)
@@ -1732,6 +1765,50 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 // and grows the pair buffers to fit.  Captured (capture == true): no host
 // synchronisation; the pair buffers keep their capacity and the emit kernel
 // drops pairs beyond it (Adam then skips the step, see k_adam_prep).
+// Raster launches of the current forward state, by variant (pixels per thread).
+static int launch_fwd_raster(nps_gs* o, int ppt) {
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t W = o->w, H = o->h, nv = o->nv;
+  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t* rstart = o->ranges.as<uint32_t>();
+  const uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  const dim3 grid(tiles_x, tiles_y, nv);
+#define NPS_FWD(PPT)                                                                                      \
+  gs::k_fwd<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
+                                            num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>())
+  switch (ppt) {
+    case 2: NPS_FWD(2); break;
+    case 4: NPS_FWD(4); break;
+    default: NPS_FWD(1); break;
+  }
+#undef NPS_FWD
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
+static int launch_bwd_raster(nps_gs* o, int ppt, const float4* dimg) {
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t W = o->w, H = o->h, nv = o->nv;
+  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t* rstart = o->ranges.as<uint32_t>();
+  const uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  const dim3 grid(tiles_x, tiles_y, nv);
+#define NPS_BWD(PPT)                                                                                         \
+  gs::k_bwd2<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
+                                             num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(), dimg, \
+                                             o->g2.as<float>())
+  switch (ppt) {
+    case 1: NPS_BWD(1); break;
+    case 4: NPS_BWD(4); break;
+    default: NPS_BWD(2); break;
+  }
+#undef NPS_BWD
+  NPS_CHECK_LAUNCH();
+  return NPS_OK;
+}
+
 static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   if (o->nv == 0 || o->w == 0) {
     set_error("gs_forward: set_views and set_targets (or set_image_size) first");
@@ -1820,9 +1897,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   o->sorted_vals = vs;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   StageTimer t_fwd(o, ST_FWD);
-  gs::k_fwd<<<dim3(tiles_x, tiles_y, nv), gs::kThreads, 0, s>>>(o->recs.as<gs::Rec>(), vs, rstart, rend, W, H,
-                                                                 tiles_x, num_tiles, bg, o->img.as<float4>(),
-                                                                 o->ncontrib.as<uint32_t>());
+  NPS_TRY(launch_fwd_raster(o, o->fwd_ppt));
   NPS_CHECK_LAUNCH();
   if (out_rgba) NPS_CUDA(cudaMemcpyAsync(out_rgba, o->img.p, sizeof(float4) * npix, cudaMemcpyDeviceToDevice, s));
   o->fwd_valid = true;
@@ -1894,9 +1969,7 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
   if (!o->deterministic) {
     StageTimer t(o, ST_BWD);
-    gs::k_bwd2<<<dim3(tiles_x, tiles_y, nv), gs::kBwdThreads, 0, s>>>(
-        o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),
-        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>());
+    NPS_TRY(launch_bwd_raster(o, o->bwd_ppt, dimg));
     NPS_CHECK_LAUNCH();
   } else if (o->pair_cap > 0) {
     StageTimer t(o, ST_BWD);
@@ -2402,6 +2475,110 @@ int nps_gs_load(nps_gs* o, const char* path) {
   o->gkey = 0;
   o->skip_seen = 0;
   if (o->h_status) o->h_status[1] = 0;
+  return NPS_OK;
+}
+
+int nps_gs_set_variant(nps_gs* o, int fwd_ppt, int bwd_ppt) {
+  NPS_TRY(check_gs(o));
+  auto ok = [](int v) { return v == 1 || v == 2 || v == 4; };
+  if (!ok(fwd_ppt) || !ok(bwd_ppt)) {
+    set_error("gs_set_variant: pixels per thread must be 1, 2 or 4 (got %d, %d)", fwd_ppt, bwd_ppt);
+    return NPS_ERR_INVALID;
+  }
+  o->fwd_ppt = fwd_ppt;
+  o->bwd_ppt = bwd_ppt;
+  o->gkey = 0;
+  return NPS_OK;
+}
+
+// Times every raster variant on the current views and targets (one forward
+// and loss first, then `reps` launches of each variant) and keeps the fastest.
+// The choice is cached in a text file (one line per workload: key, forward
+// and backward pixels per thread) when cache_path is given.
+int nps_gs_autotune(nps_gs* o, const char* cache_path, int* fwd_ppt_out, int* bwd_ppt_out, float* times_ms6) {
+  NPS_TRY(check_gs(o));
+  if (!o->tgt || o->nv == 0) {
+    set_error("gs_autotune: set views and targets first");
+    return NPS_ERR_STATE;
+  }
+  cudaDeviceProp prop;
+  NPS_CUDA(cudaGetDeviceProperties(&prop, o->ctx->device));
+  // workload key: device, image, views, SH degree, Gaussian count (to ~19%)
+  char key[256];
+  const int nbucket = o->n ? (int)std::lround(4.0 * std::log2((double)o->n)) : 0;
+  std::snprintf(key, sizeof(key), "%s|sm%d|%ux%u|v%u|sh%d|n%d", prop.name, prop.multiProcessorCount, o->w, o->h,
+                o->nv, o->sh_deg, nbucket);
+  for (char* c = key; *c; ++c)
+    if (*c == ' ') *c = '_';
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "r")) {
+      char k[256];
+      int a = 0, b = 0;
+      bool found = false;
+      while (std::fscanf(f, "%255s %d %d%*[^\n]", k, &a, &b) == 3)
+        if (std::strcmp(k, key) == 0) found = true, o->fwd_ppt = a, o->bwd_ppt = b;
+      std::fclose(f);
+      if (found) {
+        o->gkey = 0;
+        if (fwd_ppt_out) *fwd_ppt_out = o->fwd_ppt;
+        if (bwd_ppt_out) *bwd_ppt_out = o->bwd_ppt;
+        if (times_ms6)
+          for (int i = 0; i < 6; ++i) times_ms6[i] = -1.0f;  // cached: not timed
+        return NPS_OK;
+      }
+    }
+  }
+  const bool timing = o->timing;
+  o->timing = false;
+  int rc = gs_forward_impl(o, nullptr, false);
+  if (rc == NPS_OK) rc = nps_gs_loss(o, nullptr);
+  o->timing = timing;
+  NPS_TRY(rc);
+  cudaStream_t s = o->ctx->stream;
+  const uint32_t M = o->n * o->nv;
+  NPS_TRY(o->g2.ensure(sizeof(float) * gs::kG2 * ((size_t)M + 1)));
+  cudaEvent_t e0, e1;
+  NPS_CUDA(cudaEventCreate(&e0));
+  NPS_CUDA(cudaEventCreate(&e1));
+  const int ppts[3] = {1, 2, 4};
+  float best[2] = {1e30f, 1e30f};
+  int pick[2] = {o->fwd_ppt, o->bwd_ppt};
+  constexpr int kReps = 3;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int vi = 0; vi < 3; ++vi) {
+      float tot = 0.0f;
+      for (int r = 0; r <= kReps; ++r) {  // the first launch warms up
+        if (pass == 1) NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
+        NPS_CUDA(cudaEventRecord(e0, s));
+        if (pass == 0) NPS_TRY(launch_fwd_raster(o, ppts[vi]));
+        else NPS_TRY(launch_bwd_raster(o, ppts[vi], o->dimg.as<float4>()));
+        NPS_CUDA(cudaEventRecord(e1, s));
+        NPS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        NPS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (r > 0) tot += ms;
+      }
+      const float avg = tot / kReps;
+      if (times_ms6) times_ms6[3 * pass + vi] = avg;
+      if (avg < best[pass]) best[pass] = avg, pick[pass] = ppts[vi];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the variants write identical images; leave a consistent forward state
+  NPS_TRY(launch_fwd_raster(o, pick[0]));
+  o->loss_valid = false;
+  o->fwd_ppt = pick[0];
+  o->bwd_ppt = pick[1];
+  o->gkey = 0;
+  if (fwd_ppt_out) *fwd_ppt_out = pick[0];
+  if (bwd_ppt_out) *bwd_ppt_out = pick[1];
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "a")) {
+      std::fprintf(f, "%s %d %d %.4f %.4f\n", key, pick[0], pick[1], best[0], best[1]);
+      std::fclose(f);
+    }
+  }
   return NPS_OK;
 }
 

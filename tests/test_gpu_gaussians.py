@@ -298,3 +298,44 @@ def test_deterministic_mode_is_bit_reproducible(trainer_cls, tmp_path):
         r.train_step()
     np.testing.assert_array_equal(r.read_state()["params"], runs[0].read_state()["params"])
     np.testing.assert_array_equal(r.read_state()["adam_v"], runs[0].read_state()["adam_v"])
+
+
+def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
+    """Forward images agree across the 1 / 2 / 4 pixels-per-thread raster
+    variants to 1e-6 (the compiler may fuse multiply-adds differently in each
+    instantiation); backward gradients to 1e-5 relative L2; both match the
+    oracle; the autotuner picks a valid variant and
+    reuses its cached choice."""
+    n, w, h, deg = 5000, 112, 96, 2
+    p = gs_scene(n, 61, deg=deg, log_scale_mean=-3.4)
+    eyes = ((0.0, 0.0, 4.0), (2.5, 1.0, 3.0))
+    vp, vpi, views = gs_views(w, h, eyes)
+    tg = gs_targets(2, w, h, 62)
+    t = trainer_cls(n, sh_degree=deg, params=p)
+    t.set_targets(tg)
+    t.set_views(vp, vpi)
+    imgs, grads = {}, {}
+    for ppt in (1, 2, 4):
+        t.set_variant(ppt, ppt)
+        t.forward()
+        t.loss()
+        t.backward()
+        imgs[ppt] = t.read_image(with_grad=False)[0]
+        grads[ppt] = t.read_state()["grads"].astype(np.float64)
+    for ppt in (2, 4):
+        np.testing.assert_allclose(imgs[ppt], imgs[1], atol=1e-6, rtol=0)
+        assert np.linalg.norm(grads[ppt] - grads[1]) / np.linalg.norm(grads[1]) < 1e-5
+    rimg, rnc = orc.gs_forward(p, deg, views, w, h)
+    np.testing.assert_allclose(imgs[4], rimg, atol=1e-5, rtol=0)
+    cache = tmp_path / "autotune.txt"
+    r = t.autotune(cache)
+    assert r["fwd_ppt"] in (1, 2, 4) and r["bwd_ppt"] in (1, 2, 4) and not r["cached"]
+    assert all(x > 0 for x in r["fwd_ms"] + r["bwd_ms"])
+    r2 = t.autotune(cache)
+    assert r2["cached"] and (r2["fwd_ppt"], r2["bwd_ppt"]) == (r["fwd_ppt"], r["bwd_ppt"])
+    # the tuned trainer still trains
+    t.set_graph(True)
+    l0 = t.train_step(read_loss=True)[0]
+    for _ in range(5):
+        t.train_step()
+    assert t.train_step(read_loss=True)[0] < l0
