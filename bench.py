@@ -32,6 +32,9 @@ sys.path.insert(0, str(ROOT))
 
 N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 800, 8, 32, 3  # config 2
 P_USED = 59          # floats per Gaussian used by the model
+# DRAM traffic of one backward-raster launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# 1-pass ncu capture of this workload (13,727,114 pairs): scaled to a launch by its pair count.
+BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 269_891_328 + 15_004_672, 13_727_114
 S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, opacity)
 
 
@@ -403,7 +406,10 @@ def main():
                 "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": launches_per_step(tile_passes) * args.steps,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_kind": pk_kind,
+                     "frac": achieved / pk["hbm_gbs"], "traffic": (BWD_TRAFFIC_BYTES * K / BWD_TRAFFIC_PAIRS
+                                 if dom == "raster_bwd" and N_GAUSS == 200_000 and WIDTH == 800 else None),
+                     "traffic_source": "ncu capture of the same kernel and workload, scaled by pairs",
+                     "peak_kind": pk_kind,
                      "step_algorithmic_bytes": step_bytes(VIEWS, N_GAUSS, K, npx),
                      "step_frac": step_bytes(VIEWS, N_GAUSS, K, npx) / (ms_per_step * 1e-3) / 1e9 / pk["hbm_gbs"]},
         "stages_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in st.items()},
