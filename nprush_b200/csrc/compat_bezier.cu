@@ -180,6 +180,19 @@ __device__ __forceinline__ void walk(const float* q, float ppx, float ppy, float
   *min_d = md; *min_k = mk; *min_u = mu;
 }
 
+// True when the pixel is farther than |width| + |softness| (0.1% + 1e-6
+// margin for rounding) from the bounding box of the four projected control
+// points.  The curve lies in their convex hull, so every segment of the walk
+// is farther still: the coverage smoothstep is exactly 1, alpha exactly 0,
+// and the pair changes nothing at this pixel (it is skipped without the walk).
+__device__ __forceinline__ bool bz_far(const float* f, float ppx, float ppy) {
+  const float mnx = fminf(fminf(f[0], f[2]), fminf(f[4], f[6])), mxx = fmaxf(fmaxf(f[0], f[2]), fmaxf(f[4], f[6]));
+  const float mny = fminf(fminf(f[1], f[3]), fminf(f[5], f[7])), mxy = fmaxf(fmaxf(f[1], f[3]), fmaxf(f[5], f[7]));
+  const float dx = fmaxf(fmaxf(mnx - ppx, ppx - mxx), 0.0f), dy = fmaxf(fmaxf(mny - ppy, ppy - mxy), 0.0f);
+  const float r = (fabsf(f[12]) + fabsf(f[13])) * 1.001f + 1e-6f;
+  return dx * dx + dy * dy > r * r;
+}
+
 // alpha and segment of one (pixel, curve) pair (bezier_backward.wgsl:231-256)
 __device__ __forceinline__ float bz_alpha(const float* f, float ppx, float ppy, uint32_t* kseg, float* dval) {
   float md, mu;
@@ -247,6 +260,7 @@ __global__ void __launch_bounds__(kThreads) k_bz_raster(RasterArgs A) {
     __syncthreads();
     for (uint32_t k = 0; k < cnt; ++k) {
       const float* f = sf + k * kRecF;
+      if (bz_far(f, ppx, ppy)) continue;  // alpha 0: nothing changes
       uint32_t kseg;
       float dv;
       const float a = bz_alpha(f, ppx, ppy, &kseg, &dv);
@@ -345,9 +359,9 @@ __global__ void __launch_bounds__(kThreads) k_bz_raster(RasterArgs A) {
     __syncthreads();
     float Tc = ckpt[c * kThreads + tid];
     for (uint32_t k = 0; k < cnt; ++k) {
-      uint32_t kseg;
-      float dv;
-      const float a = bz_alpha(sf + k * kRecF, ppx, ppy, &kseg, &dv);
+      uint32_t kseg = 1;
+      float dv = 0.0f;
+      const float a = bz_far(sf + k * kRecF, ppx, ppy) ? 0.0f : bz_alpha(sf + k * kRecF, ppx, ppy, &kseg, &dv);
       sA[k * kThreads + tid] = a;
       sT[k * kThreads + tid] = Tc;
       sK[k * kThreads + tid] = (uint8_t)kseg;
@@ -927,6 +941,7 @@ __global__ void __launch_bounds__(256) k_bz_render_raster(const float* __restric
     for (uint32_t j = 0; j < nb; ++j) {
       const float* f = sr[j];
       if (!(ppx >= f[8] && ppx < f[9] && ppy > f[10] && ppy <= f[11])) continue;
+      if (bz_far(f, ppx, ppy)) continue;  // alpha 0
       float md = 1e9f, mu = 0.0f, cross = 0.0f;
       uint32_t mk = 1;
       float2 prev = make_float2(f[0], f[1]);
