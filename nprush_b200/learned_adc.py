@@ -104,6 +104,10 @@ def main(argv=None):
     ap.add_argument("--log-seeds", type=int, nargs="+", default=[100, 101])
     ap.add_argument("--eval-seed", type=int, default=120)
     ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--log-steps", type=int, default=None,
+                    help="length of the logging runs (default: up to the last ADC event)")
+    ap.add_argument("--with-per-view", action="store_true",
+                    help="also run the plain per-view trainer (eager, one view per launch) on the eval seed")
     ap.add_argument("--adc-stop", type=int, default=None)
     ap.add_argument("--gaussians", type=int, default=200_000)
     ap.add_argument("--teacher", type=int, default=250_000)
@@ -133,8 +137,9 @@ def main(argv=None):
     out = {}
     with torch.cuda.stream(stream):
         log = AdcLog(seed=1)
+        log_steps = a.log_steps or min(a.steps, adc.stop)
         for s in a.log_seeds:
-            r, p = run(scene, a.steps, s, adc, logging_adc_fn(log, adc))
+            r, p = run(scene, log_steps, s, adc, logging_adc_fn(log, adc))
             out.setdefault("log_runs", []).append(dict(seed=s, psnr=p, count=r.count, wall_s=r.wall_s))
         X, y = hindsight_labels(log, a.horizon)
         cw = class_weights(y) if a.class_weights else np.ones(4, np.float32)
@@ -149,12 +154,15 @@ def main(argv=None):
         out["training"] = dict(samples=int(len(y)), class_counts=np.bincount(y, minlength=4).tolist(),
                                class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
                                heldout_confusion=conf.tolist())
-        for name, fn in (("plain", None), ("learned", policy_adc_fn(pol, adc))):
-            r, p = run(scene, a.steps, a.eval_seed, adc, fn)
-            out[name] = dict(psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
+        arms = [("plain", None, "batched"), ("learned", policy_adc_fn(pol, adc), "batched")]
+        if a.with_per_view:
+            arms.append(("plain_per_view", None, "per_view"))
+        for name, fn, mode in arms:
+            r, p = run(scene, a.steps, a.eval_seed, adc, fn, mode=mode)
+            out[name] = dict(mode=mode, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
                              skipped=r.skipped_steps, adc_events=r.adc_events[-3:])
     out["config"] = vars(a)
-    print(json.dumps({k: out[k] for k in ("plain", "learned")}))
+    print(json.dumps({k: out[k] for k in ("plain", "learned", "plain_per_view") if k in out}))
     print(json.dumps(dict(class_counts=out["training"]["class_counts"], acc=out["training"]["acc"][-1],
                           confusion=out["training"]["heldout_confusion"])))
     if a.out:
