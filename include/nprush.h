@@ -133,7 +133,8 @@ typedef struct nps_stats {
   uint32_t max_tile_len;   /* longest tile list before the cap */
   uint32_t adc_clones;     /* clones + splits performed by the last ADC */
   uint32_t step_count;     /* dispatch() calls so far */
-  uint32_t reserved[3];
+  uint32_t reserved[3];    /* Bezier: [0] spawns.  Gaussians: [1] graph replays that skipped their
+                              update (pair overflow), [2] record-staging waits that timed out */
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
 

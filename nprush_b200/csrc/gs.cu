@@ -109,11 +109,13 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= nv * n) return;
   const uint32_t v = g / n, i = g - v * n;
-  const float* p = params + (size_t)i * kP;
+  // the record in 16-byte loads (floats 0..11, then the SH coefficients if visible)
+  const float4* p4 = reinterpret_cast<const float4*>(params + (size_t)i * kP);
+  const float4 q0 = p4[0], q1 = p4[1], q2 = p4[2];
   const float* view = views + (size_t)v * kViewRec;
-  float mean[3] = {p[0], p[1], p[2]};
-  float ls[3] = {p[3], p[4], p[5]};
-  float q[4] = {p[6], p[7], p[8], p[9]};
+  float mean[3] = {q0.x, q0.y, q0.z};
+  float ls[3] = {q0.w, q1.x, q1.y};
+  float q[4] = {q1.z, q1.w, q2.x, q2.y};
   Proj<float> P;
   project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
   uint32_t cnt = 0;
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
   r.a = make_float4(0, 0, 0, 0);
   r.b = make_float4(0, 0, 0, 0);
   r.c = make_float4(0, 0, 0, 0);
-  const float op = sigmoidf(p[kOpacity]);
+  const float op = sigmoidf(q2.z);  // opacity logit, float 10
   // A pixel contributes only where o * G >= 1/255, i.e. inside the ellipse
   // d^T Sigma^-1 d <= t2 = 2 ln(255 o).  Its axis-aligned box, centre +-
   // sqrt(t2 * Sigma_xx), +- sqrt(t2 * Sigma_yy), bounds the tile rectangle and
@@ -145,12 +147,18 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
       float basis[16];
       sh_basis<float>(DEG, dx * il, dy * il, dz * il, basis);
       constexpr int nb = (DEG + 1) * (DEG + 1);
+      float sh[(3 * nb + 3) / 4 * 4];
+#pragma unroll
+      for (int k4 = 0; k4 < (3 * nb + 3) / 4; ++k4) {
+        const float4 t = p4[3 + k4];
+        sh[4 * k4] = t.x; sh[4 * k4 + 1] = t.y; sh[4 * k4 + 2] = t.z; sh[4 * k4 + 3] = t.w;
+      }
       float col[3] = {0.5f, 0.5f, 0.5f};
 #pragma unroll
       for (int k = 0; k < nb; ++k) {
-        col[0] += basis[k] * p[kSH + 3 * k + 0];
-        col[1] += basis[k] * p[kSH + 3 * k + 1];
-        col[2] += basis[k] * p[kSH + 3 * k + 2];
+        col[0] += basis[k] * sh[3 * k + 0];
+        col[1] += basis[k] * sh[3 * k + 1];
+        col[2] += basis[k] * sh[3 * k + 2];
       }
       r.a = make_float4(P.u, P.v, P.ca, P.cb);
       r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
@@ -204,6 +212,53 @@ __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __re
 }
 
 // ------------------------------------------------------------ forward raster
+// ---- record staging with bulk asynchronous copies (double-buffered)
+// Each staged record (48 B, 16-byte aligned in global and shared memory) is one
+// cp.async.bulk global -> shared completing on the buffer's mbarrier; thread 0
+// posts the batch's byte count.  Waits are bounded: on a timeout the kernel
+// records it in *err and carries on (the batch is then undefined).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                   smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (uint32_t it = 0; it < (1u << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// stage records vals[b0 .. b0 + nb) into buf (thread tid < nb copies one)
+__device__ __forceinline__ void stage_batch(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+                                            uint32_t b0, uint32_t nb, Rec* buf, uint64_t* bar, uint32_t* gidx) {
+  if (threadIdx.x == 0) mbar_expect_tx(bar, nb * (uint32_t)sizeof(Rec));
+  if (threadIdx.x < nb) {
+    // this buffer was last read through the generic proxy (before a barrier)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const uint32_t g = vals[b0 + threadIdx.x];
+    if (gidx) gidx[threadIdx.x] = g;
+    bulk_g2s(buf + threadIdx.x, recs + g, (uint32_t)sizeof(Rec), bar);
+  }
+}
+
 // Forward raster, PPT vertically adjacent pixels per thread: 256 / PPT
 // threads per 16 x 16 tile, records staged 256 / PPT at a time, a warp
 // covers a 16 x 2·PPT strip.  PPT is the autotuned variant (1, 2 or 4).
@@ -212,11 +267,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
                                                    const uint32_t* __restrict__ rstart,
                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
-                                                   float4* __restrict__ img, uint32_t* __restrict__ ncontrib) {
+                                                   float4* __restrict__ img, uint32_t* __restrict__ ncontrib,
+                                                   uint32_t* __restrict__ err) {
   constexpr int NT = 256 / PPT;
-  __shared__ float4 s_a[NT];
-  __shared__ float4 s_b[NT];
-  __shared__ float4 s_c[NT];
+  __shared__ __align__(16) Rec s_rec[2][NT];
+  __shared__ __align__(8) uint64_t s_bar[2];
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
   const float fx = (float)px;
@@ -238,17 +293,25 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     for (int k = 0; k < PPT; ++k) d = d && dn[k];
     return d;
   };
-  for (uint32_t base = start; base < end; base += NT) {
-    if (__syncthreads_count(all_done()) == NT) break;
-    const uint32_t idx = base + tid;
-    if (idx < end) {
-      const Rec r = recs[vals[idx]];
-      s_a[tid] = r.a;
-      s_b[tid] = r.b;
-      s_c[tid] = r.c;
-    }
-    __syncthreads();
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const uint32_t nbatch = (end - start + NT - 1) / NT;
+  if (nbatch > 0) stage_batch(recs, vals, start, min((uint32_t)NT, end - start), s_rec[0], &s_bar[0], nullptr);
+  bool pending_next = false;
+  for (uint32_t bi = 0; bi < nbatch; ++bi) {
+    const uint32_t base = start + bi * NT, buf = bi & 1u;
     const uint32_t nb = min((uint32_t)NT, end - base);
+    // prefetch the next batch into the other buffer (read two batches ago)
+    pending_next = bi + 1 < nbatch;
+    if (pending_next)
+      stage_batch(recs, vals, base + NT, min((uint32_t)NT, end - base - NT), s_rec[buf ^ 1u], &s_bar[buf ^ 1u],
+                  nullptr);
+    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+    const Rec* sr = s_rec[buf];
     // staged pairs whose alpha >= 1/255 box meets the warp's strip (one lane
     // tests NT / 32 pairs; the warp then walks the set bits in order)
     uint32_t hit[NT / 32];
@@ -257,8 +320,8 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       const uint32_t jj = qq * 32 + (tid & 31);
       bool h = false;
       if (jj < nb) {
-        const float4 a = s_a[jj];
-        const float4 c4 = s_c[jj];
+        const float4 a = sr[jj].a;
+        const float4 c4 = sr[jj].c;
         h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
       }
       hit[qq] = __ballot_sync(0xffffffffu, h);
@@ -269,9 +332,9 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       const int bit = __ffs(m) - 1;
       m &= m - 1u;
       const uint32_t j = qq * 32 + bit;
-      const float4 a = s_a[j];
-      const float4 c4 = s_c[j];
-      const float4 b = s_b[j];
+      const float4 a = sr[j].a;
+      const float4 c4 = sr[j].c;
+      const float4 b = sr[j].b;
       const float dx = a.x - fx;
 #pragma unroll
       for (int k = 0; k < PPT; ++k) {
@@ -294,6 +357,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
         last[k] = base - start + j + 1;
       }
       done = all_done();
+    }
+    // every pixel of the tile done: stop (after the prefetch in flight lands)
+    if (__syncthreads_count(all_done()) == NT) {
+      if (pending_next && !mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+      break;
     }
   }
 #pragma unroll
@@ -805,13 +873,13 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
                                                     uint32_t tiles_x, uint32_t num_tiles, float3 bg,
                                                     const float4* __restrict__ img,
                                                     const uint32_t* __restrict__ ncontrib,
-                                                    const float4* __restrict__ dimg, float* __restrict__ g2) {
+                                                    const float4* __restrict__ dimg, float* __restrict__ g2,
+                                                    uint32_t* __restrict__ err) {
   constexpr int NT = 256 / PPT;
-  __shared__ float4 s_a[NT];
-  __shared__ float4 s_b[NT];
-  __shared__ float4 s_c[NT];
-  __shared__ uint32_t s_g[NT];
+  __shared__ __align__(16) Rec s_rec[2][NT];
+  __shared__ uint32_t s_g[2][NT];
   __shared__ float s_acc[NT][10];
+  __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_max;
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
@@ -826,7 +894,12 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     pix_bwd_init(p[k], px, py + k, v, W, H, bg, img, ncontrib, dimg);
     mylast = max(mylast, p[k].last);
   }
-  if (tid == 0) s_max = 0;
+  if (tid == 0) {
+    s_max = 0;
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   __syncthreads();
   atomicMax(&s_max, mylast);
   __syncthreads();
@@ -834,29 +907,37 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
   uint32_t wlast = mylast;  // pairs at or beyond every pixel's last contributor are skipped
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
-  for (uint32_t bend = start + maxlast; bend > start;) {
-    const uint32_t bstart = bend > start + NT ? bend - NT : start;
+  // batches in reverse: batch i covers [max(start, top - (i+1) NT), top - i NT), top = start + maxlast
+  const uint32_t nbatch = (maxlast + NT - 1) / NT;
+  auto bstart_of = [&](uint32_t i) {
+    const uint32_t hi = start + maxlast - i * NT;
+    return hi > start + NT ? hi - NT : start;
+  };
+  if (nbatch > 0) {
+    const uint32_t b0 = bstart_of(0);
+    stage_batch(recs, vals, b0, start + maxlast - b0, s_rec[0], &s_bar[0], s_g[0]);
+  }
+  for (uint32_t bi = 0; bi < nbatch; ++bi) {
+    const uint32_t buf = bi & 1u;
+    const uint32_t bend = start + maxlast - bi * NT, bstart = bstart_of(bi);
     const uint32_t nb = bend - bstart;
-    __syncthreads();
-    if (tid < nb) {
-      const uint32_t gg = vals[bstart + tid];
-      const Rec r = recs[gg];
-      s_a[tid] = r.a;
-      s_b[tid] = r.b;
-      s_c[tid] = r.c;
-      s_g[tid] = gg;
+    if (bi + 1 < nbatch) {
+      const uint32_t nbs = bstart_of(bi + 1);
+      stage_batch(recs, vals, nbs, bstart - nbs, s_rec[buf ^ 1u], &s_bar[buf ^ 1u], s_g[buf ^ 1u]);
     }
 #pragma unroll
     for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
-    __syncthreads();
+    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+    __syncthreads();  // s_acc cleared, staged indices visible
+    const Rec* sr = s_rec[buf];
     uint32_t hit[NT / 32];
 #pragma unroll
     for (int qq = 0; qq < NT / 32; ++qq) {
       const uint32_t jj = qq * 32 + lane;
       bool h = false;
       if (jj < nb && bstart + jj - start < wlast) {
-        const float4 a = s_a[jj];
-        const float4 c4 = s_c[jj];
+        const float4 a = sr[jj].a;
+        const float4 c4 = sr[jj].c;
         h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
       }
       hit[qq] = __ballot_sync(0xffffffffu, h);
@@ -867,9 +948,9 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       const int bit = 31 - __clz(m);
       m &= ~(1u << bit);
       const int j = qq * 32 + bit;  // descending within the batch
-      const float4 a = s_a[j];
-      const float4 c4 = s_c[j];
-      const float4 b = s_b[j];
+      const float4 a = sr[j].a;
+      const float4 c4 = sr[j].c;
+      const float4 b = sr[j].b;
       const uint32_t cur = bstart + (uint32_t)j - start;
       float gv[16];
 #pragma unroll
@@ -885,14 +966,14 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     }
     __syncthreads();
     if (tid < nb) {
-      float* dst = g2 + (size_t)s_g[tid] * kG2;
+      float* dst = g2 + (size_t)s_g[buf][tid] * kG2;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         const float x = s_acc[tid][k];
         if (x != 0.0f) atomicAdd(dst + k, x);
       }
     }
-    bend = bstart;
+    __syncthreads();  // s_acc and this buffer are reused two batches on
   }
 }
 
@@ -945,13 +1026,18 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
   const uint32_t i = t >> 3, sub = t & 7;
   const bool live = i < n;  // whole groups are live or not (n * 8 threads, groups aligned)
   if (__all_sync(0xffffffffu, !live)) return;
-  const float* p = params + (size_t)(live ? i : 0) * kP;
-  float mean[3] = {p[0], p[1], p[2]};
-  float ls[3] = {p[3], p[4], p[5]};
-  float q[4] = {p[6], p[7], p[8], p[9]};
-  float sh[3 * nb];
+  const float4* p4 = reinterpret_cast<const float4*>(params + (size_t)(live ? i : 0) * kP);
+  const float4 q0 = p4[0], q1 = p4[1], q2 = p4[2];
+  float mean[3] = {q0.x, q0.y, q0.z};
+  float ls[3] = {q0.w, q1.x, q1.y};
+  float q[4] = {q1.z, q1.w, q2.x, q2.y};
+  const float op_logit = q2.z;
+  float sh[(3 * nb + 3) / 4 * 4];
 #pragma unroll
-  for (int k = 0; k < 3 * nb; ++k) sh[k] = p[kSH + k];
+  for (int k4 = 0; k4 < (3 * nb + 3) / 4; ++k4) {
+    const float4 t = p4[3 + k4];
+    sh[4 * k4] = t.x; sh[4 * k4 + 1] = t.y; sh[4 * k4 + 2] = t.z; sh[4 * k4 + 3] = t.w;
+  }
   float g[kP];
 #pragma unroll
   for (int k = 0; k < kP; ++k) g[k] = 0.0f;
@@ -1091,7 +1177,7 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
   if (!live) return;
   // this lane holds record floats 8 * sub .. 8 * sub + 7 in g[0..7]
   if (sub == 1) {
-    const float op = sigmoidf(p[kOpacity]);
+    const float op = sigmoidf(op_logit);
     g[kOpacity - 8] *= op * (1.0f - op);
     g[11 - 8] = 0.0f;
   }
@@ -1776,7 +1862,8 @@ static int launch_fwd_raster(nps_gs* o, int ppt) {
   const dim3 grid(tiles_x, tiles_y, nv);
 #define NPS_FWD(PPT)                                                                                      \
   gs::k_fwd<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
-                                            num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>())
+                                            num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(),  \
+                                            o->stepst.as<uint32_t>() + 6)
   switch (ppt) {
     case 2: NPS_FWD(2); break;
     case 4: NPS_FWD(4); break;
@@ -1798,7 +1885,7 @@ static int launch_bwd_raster(nps_gs* o, int ppt, const float4* dimg) {
 #define NPS_BWD(PPT)                                                                                         \
   gs::k_bwd2<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
                                              num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(), dimg, \
-                                             o->g2.as<float>())
+                                             o->g2.as<float>(), o->stepst.as<uint32_t>() + 6)
   switch (ppt) {
     case 1: NPS_BWD(1); break;
     case 4: NPS_BWD(4); break;
@@ -2630,6 +2717,13 @@ int nps_gs_stats(nps_gs* o, nps_stats* out) {
   if (!out) return NPS_ERR_INVALID;
   o->stats.step_count = o->step;
   o->stats.reserved[1] = o->skipped;
+  {
+    // raster staging waits that timed out (a device counter; 0 unless the hardware misbehaved)
+    uint32_t st[8];
+    NPS_CUDA(cudaMemcpyAsync(st, o->stepst.p, 32, cudaMemcpyDeviceToHost, o->ctx->stream));
+    NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+    o->stats.reserved[2] = st[6];
+  }
   if (o->graph_mode && o->gexec && o->h_status) {
     NPS_CUDA(cudaEventSynchronize(o->gdone));
     o->stats.pairs = o->h_status[0];  // pairs of the last replay

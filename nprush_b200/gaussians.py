@@ -284,7 +284,8 @@ class GaussianTrainer:
     def stats(self) -> dict:
         st = _lib.nps_stats()
         call("nps_gs_stats", self._h, ctypes.byref(st))
-        return dict(pairs=st.pairs, step_count=st.step_count, skipped_steps=st.reserved[1])
+        return dict(pairs=st.pairs, step_count=st.step_count, skipped_steps=st.reserved[1],
+                    staging_timeouts=st.reserved[2])
 
     STAGES = ("preprocess", "depth_sort", "emit", "tile_sort", "ranges", "raster_fwd", "loss", "raster_bwd",
               "project_bwd", "adam")
