@@ -60,8 +60,30 @@ __constant__ float c_ssim_w[kSsimWin];
 struct Rec {  // projected record, 3 x float4 = 48 B
   float4 a;   // u, v, conic a, conic b
   float4 b;   // conic c, opacity, r, g
-  float4 c;   // b, depth, half-extents (x, y) of the alpha >= 1/255 ellipse box
+  float4 c;   // b, level t2 of the alpha >= 1/255 ellipse (q(d) <= t2), half-extents (x, y) of its box
 };
+
+// True if the alpha >= 1/255 ellipse of the record misses the pixel-centre
+// rectangle [x0, x0 + 15] x [y0, y0 + h]: its box misses, or the smallest
+// value of q(d) = ca dx^2 + 2 cb dx dy + cc dy^2 over the rectangle (offsets
+// from the centre) exceeds the level t2.  A conservative skip test: the
+// level carries the footprint's margin.
+__device__ __forceinline__ bool rec_misses_strip(const float4& a, float cc, const float4& c, float x0, float y0,
+                                                 float h) {
+  if ((a.x + c.z < x0) || (a.x - c.z > x0 + 15.0f) || (a.y + c.w < y0) || (a.y - c.w > y0 + h)) return true;
+  const float lx = x0 - a.x, hx = x0 + 15.0f - a.x, ly = y0 - a.y, hy = y0 + h - a.y;
+  if (lx <= 0.0f && hx >= 0.0f && ly <= 0.0f && hy >= 0.0f) return false;  // centre inside
+  const float ca = a.z, cb = a.w;
+  // the form's minimum on each edge (the other coordinate clamped to the edge)
+  const float icc = cc > 0.0f ? 1.0f / cc : 0.0f, ica = ca > 0.0f ? 1.0f / ca : 0.0f;
+  const float y_l = fminf(fmaxf(-cb * lx * icc, ly), hy), y_h = fminf(fmaxf(-cb * hx * icc, ly), hy);
+  const float x_l = fminf(fmaxf(-cb * ly * ica, lx), hx), x_h = fminf(fmaxf(-cb * hy * ica, lx), hx);
+  const float q1 = ca * lx * lx + 2.0f * cb * lx * y_l + cc * y_l * y_l;
+  const float q2 = ca * hx * hx + 2.0f * cb * hx * y_h + cc * y_h * y_h;
+  const float q3 = ca * x_l * x_l + 2.0f * cb * x_l * ly + cc * ly * ly;
+  const float q4 = ca * x_h * x_h + 2.0f * cb * x_h * hy + cc * hy * hy;
+  return fminf(fminf(q1, q2), fminf(q3, q4)) > c.y;
+}
 
 // true if the Gaussian's alpha >= 1/255 box misses the warp's pixels
 // (rows y0, y0 + 1 and columns x0 .. x0 + 15)
@@ -162,7 +184,8 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
       }
       r.a = make_float4(P.u, P.v, P.ca, P.cb);
       r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
-      r.c = make_float4(fmaxf(col[2], 0.0f), P.cw, ex, ey);
+      // c.y: the alpha >= 1/255 level of the conic form (same 1% margin), for exact per-warp culling
+      r.c = make_float4(fmaxf(col[2], 0.0f), t2 + 1e-4f, ex, ey);
     }
   }
   recs[g] = r;
@@ -287,12 +310,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     T[k] = 1.0f; C0[k] = C1[k] = C2[k] = 0.0f; last[k] = 0;
     dn[k] = !(px < W && py + k < H);
   }
-  auto all_done = [&]() {
-    bool d = true;
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) d = d && dn[k];
-    return d;
-  };
+#define NPS_ALL_DONE(d)                      \
+  do {                                       \
+    d = true;                                \
+    _Pragma("unroll") for (int k_ = 0; k_ < PPT; ++k_) d = d && dn[k_]; \
+  } while (0)
   if (tid == 0) {
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
@@ -319,15 +341,13 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     for (int qq = 0; qq < NT / 32; ++qq) {
       const uint32_t jj = qq * 32 + (tid & 31);
       bool h = false;
-      if (jj < nb) {
-        const float4 a = sr[jj].a;
-        const float4 c4 = sr[jj].c;
-        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
-      }
+      if (jj < nb) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
-    bool done = all_done();
-    for (int qq = 0; qq < NT / 32 && !done; ++qq)
+    bool done;
+    NPS_ALL_DONE(done);
+#pragma unroll
+    for (int qq = 0; qq < NT / 32; ++qq)
     for (uint32_t m = hit[qq]; m != 0u && !done;) {
       const int bit = __ffs(m) - 1;
       m &= m - 1u;
@@ -356,10 +376,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
         T[k] = test_T;
         last[k] = base - start + j + 1;
       }
-      done = all_done();
+      NPS_ALL_DONE(done);
     }
     // every pixel of the tile done: stop (after the prefetch in flight lands)
-    if (__syncthreads_count(all_done()) == NT) {
+    NPS_ALL_DONE(done);
+    if (__syncthreads_count(done) == NT) {
       if (pending_next && !mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
       break;
     }
@@ -372,6 +393,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       ncontrib[pix] = last[k];
     }
   }
+#undef NPS_ALL_DONE
 }
 
 // ------------------------------------------------------------ loss
@@ -935,11 +957,7 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     for (int qq = 0; qq < NT / 32; ++qq) {
       const uint32_t jj = qq * 32 + lane;
       bool h = false;
-      if (jj < nb && bstart + jj - start < wlast) {
-        const float4 a = sr[jj].a;
-        const float4 c4 = sr[jj].c;
-        h = !((a.x + c4.z < wx0) || (a.x - c4.z > wx0 + 15.0f) || (a.y + c4.w < wy0) || (a.y - c4.w > wy0 + wh));
-      }
+      if (jj < nb && bstart + jj - start < wlast) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
 #pragma unroll
