@@ -296,6 +296,10 @@ int nps_gs_adc(nps_gs* gs, float grad_thresh, float split_scale, float prune_opa
  * densifies within the capacity and compacts like nps_gs_adc.
  * fallback_host (may be null) = Gaussians decided by the plain rule. */
 int nps_gs_assign_ids(nps_gs* gs, uint32_t base);
+/* Logit given to "keep" in the policy's decision (default 0 = argmax); a
+ * positive margin makes the network clone, split or prune only when that
+ * logit exceeds keep's by the margin. */
+int nps_gs_set_policy_margin(nps_gs* gs, float margin);
 int nps_gs_adc_features(nps_gs* gs, float step_frac, float grad_thresh, float split_scale, float prune_opacity,
                         float* features_dev, uint8_t* plain_dev, uint32_t* ids_dev);
 typedef struct nps_mlp nps_mlp;

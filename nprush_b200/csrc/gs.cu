@@ -1375,14 +1375,14 @@ __global__ void k_adc_policy_flags(const float* __restrict__ logits, const float
                                    const float* __restrict__ adc_grad, const float* __restrict__ adc_denom,
                                    uint32_t n, AdcParams a, uint32_t* __restrict__ flags,
                                    uint32_t* __restrict__ keep_cnt, uint32_t* __restrict__ cand_cnt,
-                                   uint32_t* __restrict__ fallback) {
+                                   uint32_t* __restrict__ fallback, float keep_logit) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float z1 = logits[3 * (size_t)i], z2 = logits[3 * (size_t)i + 1], z3 = logits[3 * (size_t)i + 2];
   uint32_t f;
   if (isfinite(z1) && isfinite(z2) && isfinite(z3)) {
     int best = 0;
-    float m = 0.0f;
+    float m = keep_logit;  // 0: plain argmax; > 0 favours keep (act only when confident)
     if (z1 > m) m = z1, best = 1;
     if (z2 > m) m = z2, best = 2;
     if (z3 > m) m = z3, best = 3;
@@ -1516,6 +1516,7 @@ struct nps_gs {
   // ADC work: alternate parameter / optimiser buffers and flags
   DevBuf p_alt, m_alt, v_alt, aflags, akeep, acand, akeep_off, acand_off, acnt, aoff, atot, psnr_acc, afeat, alogits;
   uint32_t adc_seed = 0;
+  float policy_margin = 0.0f;  // keep's logit in the policy's decision (0: argmax)
   // CUDA-graph capture of the whole train step
   bool graph_mode = false, capturing = false;
   cudaGraphExec_t gexec = nullptr;
@@ -2405,6 +2406,12 @@ int nps_gs_adc_features(nps_gs* o, float step_frac, float grad_thresh, float spl
   return NPS_OK;
 }
 
+int nps_gs_set_policy_margin(nps_gs* o, float margin) {
+  NPS_TRY(check_gs(o));
+  o->policy_margin = margin;
+  return NPS_OK;
+}
+
 int nps_gs_assign_ids(nps_gs* o, uint32_t base) {
   NPS_TRY(check_gs(o));
   if (o->n == 0) return NPS_OK;
@@ -2440,7 +2447,7 @@ int nps_gs_adc_policy(nps_gs* o, nps_mlp* policy, float step_frac, float grad_th
   gs::k_adc_policy_flags<<<div_up(n, 256), 256, 0, s>>>(o->alogits.as<float>(), o->params.as<float>(),
                                                         o->adc_grad.as<float>(), o->adc_denom.as<float>(), n, a,
                                                         o->aflags.as<uint32_t>(), o->akeep.as<uint32_t>(),
-                                                        o->acand.as<uint32_t>(), fb);
+                                                        o->acand.as<uint32_t>(), fb, o->policy_margin);
   NPS_CHECK_LAUNCH();
   if (fallback_host) NPS_CUDA(cudaMemcpyAsync(fallback_host, fb, 4, cudaMemcpyDeviceToHost, s));
   return adc_apply(o, a, counts4);

@@ -252,6 +252,10 @@ class GaussianTrainer:
         self.sync()
         return feat[:n], plain[:n], ids[:n]
 
+    def set_policy_margin(self, margin: float):
+        """Keep's logit in the policy decision (0 = argmax; > 0 acts only when confident)."""
+        call("nps_gs_set_policy_margin", self._h, float(margin))
+
     def adc_policy(self, policy, step_frac: float, grad_thresh: float = 2e-4, split_scale: float = 0.01,
                    prune_opacity: float = 0.005) -> dict:
         """ADC decided by the policy network (None: the plain rule)."""

@@ -83,8 +83,9 @@ def logging_adc_fn(log: AdcLog, adc: AdcSchedule):
     return fn
 
 
-def policy_adc_fn(policy, adc: AdcSchedule):
+def policy_adc_fn(policy, adc: AdcSchedule, margin: float = 0.0):
     def fn(trainer, step):
+        trainer.set_policy_margin(margin)
         return trainer.adc_policy(policy, step / adc.stop, adc.grad_thresh, adc.split_scale, adc.prune_opacity)
     return fn
 
@@ -106,6 +107,9 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--log-steps", type=int, default=None,
                     help="length of the logging runs (default: up to the last ADC event)")
+    ap.add_argument("--margins", type=float, nargs="+", default=[0.0],
+                    help="keep-logit margins of the learned arms (one evaluation run each)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain batched arm")
     ap.add_argument("--with-per-view", action="store_true",
                     help="also run the plain per-view trainer (eager, one view per launch) on the eval seed")
     ap.add_argument("--adc-stop", type=int, default=None)
@@ -154,7 +158,9 @@ def main(argv=None):
         out["training"] = dict(samples=int(len(y)), class_counts=np.bincount(y, minlength=4).tolist(),
                                class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
                                heldout_confusion=conf.tolist())
-        arms = [("plain", None, "batched"), ("learned", policy_adc_fn(pol, adc), "batched")]
+        arms = [] if a.no_plain else [("plain", None, "batched")]
+        for mg in a.margins:
+            arms.append(("learned" if mg == 0.0 else f"learned_m{mg:g}", policy_adc_fn(pol, adc, mg), "batched"))
         if a.with_per_view:
             arms.append(("plain_per_view", None, "per_view"))
         for name, fn, mode in arms:
@@ -162,7 +168,7 @@ def main(argv=None):
             out[name] = dict(mode=mode, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
                              skipped=r.skipped_steps, adc_events=r.adc_events[-3:])
     out["config"] = vars(a)
-    print(json.dumps({k: out[k] for k in ("plain", "learned", "plain_per_view") if k in out}))
+    print(json.dumps({k: v for k, v in out.items() if k not in ("training", "log_runs", "config")}))
     print(json.dumps(dict(class_counts=out["training"]["class_counts"], acc=out["training"]["acc"][-1],
                           confusion=out["training"]["heldout_confusion"])))
     if a.out:

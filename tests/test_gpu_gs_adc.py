@@ -226,3 +226,16 @@ def test_adc_features_ids_and_policy_decisions(trainer_cls):
     u.write_adc_stats(grad, denom)
     r = u.adc_policy(bad, 0.5)
     assert r["fallback"] == n and r["after"] == int(c[1])
+
+
+def test_policy_margin(trainer_cls):
+    """A keep margin above the network's logits turns its decisions into keep."""
+    from nprush_b200.policy import AdcPolicy
+    n = 2000
+    p, m, v, grad, denom = adc_case(n, 45)
+    pol = AdcPolicy(params=np.r_[np.zeros(5440, np.float32), np.array((-9.0, -9.0, 9.0), np.float32)])
+    for margin, after in ((0.0, 0), (8.0, 0), (10.0, n)):
+        u = trainer_cls(2 * n, sh_degree=0, params=p)
+        u.write_adc_stats(grad, denom)
+        u.set_policy_margin(margin)
+        assert u.adc_policy(pol, 0.5)["after"] == after
