@@ -4,7 +4,7 @@
 // fixed-grid reduce-then-scan radix sort: per 8-bit digit, an upsweep kernel
 // histograms each block's contiguous key range, a three-kernel scan turns the
 // digit-major histogram into offsets, and a downsweep kernel ranks keys stably
-// (warp-level __match_any_sync ranking in original order) and scatters them.
+// (warp-level ranking in original order from per-bit ballots) and scatters them.
 // The grid never depends on the key count (read from device memory), so the
 // whole sort can be captured in a CUDA graph, and there is no inter-block
 // waiting anywhere (no decoupled look-back spin), so it cannot hang.
@@ -180,7 +180,15 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const uint32_t d = dg[j];
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      // lanes holding the same digit: intersect the ballots of its nine bits
+      // (bit 8 marks an invalid item), cheaper than a match-any
+      uint32_t peers = 0xffffffffu;
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bal : ~bal;
+      }
       const int leader = __ffs(peers) - 1;
       uint32_t old = 0;
       if (lane == leader && d < 256u) old = wh[wid][d];
