@@ -78,7 +78,6 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* 
 // arrays (either the inputs or the work buffers).
 int radix_sort_u32(uint32_t* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t cap, int bits, SortWork& w,
                    cudaStream_t s, uint32_t** keys_out, uint32_t** vals_out);
-int radix_sort_u64(uint64_t* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t cap, int bits, SortWork& w,
-                   cudaStream_t s, uint64_t** keys_out, uint32_t** vals_out);
+
 
 }  // namespace nps

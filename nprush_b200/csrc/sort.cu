@@ -157,7 +157,13 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
                                                              const uint32_t* __restrict__ offsets) {
   __shared__ uint32_t run[256];
   __shared__ uint32_t tot[256];
+  __shared__ uint32_t toff[256];
   __shared__ uint32_t wh[kSortWarps][256];
+  // the tile in local sorted order, so that the global writes come out as
+  // contiguous runs per digit
+  __shared__ K sk[kTile];
+  __shared__ uint32_t sv[kTile];
+  __shared__ uint32_t scan_total;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   run[threadIdx.x] = offsets[threadIdx.x * gridDim.x + blockIdx.x];
   uint32_t n, t0, t1;
@@ -207,16 +213,26 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
         acc += x;
       }
       tot[threadIdx.x] = acc;
+      toff[threadIdx.x] = block_exclusive_scan<kSortThreads>(acc, &scan_total);
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const uint32_t d = dg[j];
       if (d < 256u) {
-        uint32_t pos = run[d] + wh[wid][d] + rk[j];
-        kout[pos] = k[j];
-        vout[pos] = v[j];
+        const uint32_t lp = toff[d] + wh[wid][d] + rk[j];
+        sk[lp] = k[j];
+        sv[lp] = v[j];
       }
+    }
+    __syncthreads();
+    const uint32_t cnt = scan_total;  // valid items of this tile
+    for (uint32_t i = threadIdx.x; i < cnt; i += kSortThreads) {
+      const K kk = sk[i];
+      const uint32_t d = (uint32_t)(kk >> shift) & 255u;
+      const uint32_t pos = run[d] + (i - toff[d]);
+      kout[pos] = kk;
+      vout[pos] = sv[i];
     }
     __syncthreads();
     run[threadIdx.x] += tot[threadIdx.x];
@@ -275,9 +291,5 @@ int radix_sort_u32(uint32_t* keys, uint32_t* vals, const uint32_t* count_dev, ui
   return radix_sort_impl<uint32_t>(keys, vals, count_dev, cap, bits, w, s, keys_out, vals_out);
 }
 
-int radix_sort_u64(uint64_t* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t cap, int bits, SortWork& w,
-                   cudaStream_t s, uint64_t** keys_out, uint32_t** vals_out) {
-  return radix_sort_impl<uint64_t>(keys, vals, count_dev, cap, bits, w, s, keys_out, vals_out);
-}
 
 }  // namespace nps
