@@ -201,27 +201,48 @@ __global__ void k_gather_counts(const uint32_t* __restrict__ sorted_g, const uin
   if (j < m) out[j] = counts[sorted_g[j]];
 }
 
-__global__ void k_emit(const uint32_t* __restrict__ sorted_g, const uint32_t* __restrict__ counts,
-                       const uint32_t* __restrict__ offsets, const uint2* __restrict__ rects, uint32_t m, uint32_t n,
-                       uint32_t tiles_x, uint32_t num_tiles, uint32_t cap, uint32_t* __restrict__ keys,
-                       uint32_t* __restrict__ vals) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= m) return;
-  const uint32_t g = sorted_g[j];
-  const uint32_t c = counts[g];
-  if (c == 0) return;
-  const uint32_t v = g / n;
-  uint32_t pos = offsets[j];
-  const uint2 r = rects[g];
-  const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
-  for (uint32_t ty = y0; ty < y1; ++ty)
-    for (uint32_t tx = x0; tx < x1; ++tx) {
-      if (pos < cap) {
-        keys[pos] = v * num_tiles + ty * tiles_x + tx;
-        vals[pos] = g;
-      }
-      ++pos;
+// One warp per 32 consecutive depth-sorted (view, Gaussian) entries: their
+// pairs are one contiguous output range, written 32 consecutive slots at a
+// time (coalesced); each lane finds the entry owning its slot by a binary
+// search over the warp's offsets (shuffles).  Output identical to writing
+// each entry's tile rectangle row by row.
+__global__ void __launch_bounds__(256) k_emit(const uint32_t* __restrict__ sorted_g,
+                                              const uint32_t* __restrict__ counts,
+                                              const uint32_t* __restrict__ offsets, const uint2* __restrict__ rects,
+                                              uint32_t m, uint32_t n, uint32_t tiles_x, uint32_t num_tiles,
+                                              uint32_t cap, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+  if (__all_sync(0xffffffffu, j >= m)) return;
+  uint32_t g = 0, c = 0, off = 0xffffffffu, x0 = 0, w = 1, y0 = 0;
+  if (j < m) {
+    g = sorted_g[j];
+    c = counts[g];
+    off = offsets[j];
+    const uint2 r = rects[g];
+    x0 = r.x & 0xffffu;
+    w = max((r.x >> 16) - x0, 1u);
+    y0 = r.y & 0xffffu;
+  }
+  const uint32_t start = __shfl_sync(0xffffffffu, off, 0);
+  const uint32_t end = __reduce_max_sync(0xffffffffu, j < m ? off + c : 0u);
+  for (uint32_t base = start; base < end; base += 32) {
+    const uint32_t sl = base + lane;
+    // largest lane whose offset <= sl (lanes past m carry offset ~0u)
+    uint32_t L = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1) {
+      const uint32_t o2 = __shfl_sync(0xffffffffu, off, L + step);
+      if (o2 <= sl) L += step;
     }
+    const uint32_t gL = __shfl_sync(0xffffffffu, g, L), oL = __shfl_sync(0xffffffffu, off, L);
+    const uint32_t x0L = __shfl_sync(0xffffffffu, x0, L), wL = __shfl_sync(0xffffffffu, w, L);
+    const uint32_t y0L = __shfl_sync(0xffffffffu, y0, L);
+    if (sl < end && sl < cap) {
+      const uint32_t local = sl - oL, ry = local / wL;
+      keys[sl] = (gL / n) * num_tiles + (y0L + ry) * tiles_x + x0L + (local - ry * wL);
+      vals[sl] = gL;
+    }
+  }
 }
 
 __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
