@@ -876,7 +876,9 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
   const float araw = b.y * G;
   const float alpha = fminf(kAlphaMax, araw);
   if (alpha < kAlphaMin) return false;
-  s.T = s.T / (1.0f - alpha);
+  // one reciprocal serves both divisions (approximate, ~2 ulp; alpha <= 0.99)
+  const float inv1ma = __fdividef(1.0f, 1.0f - alpha);
+  s.T = s.T * inv1ma;
   const float wgt = alpha * s.T;
   const float col[3] = {b.z, b.w, c4.x};
   float dL_dalpha = 0.0f;
@@ -889,7 +891,7 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
   }
   dL_dalpha *= s.T;
   s.last_alpha = alpha;
-  dL_dalpha += (-s.T_final / (1.0f - alpha)) * s.bg_dot;
+  dL_dalpha += (-s.T_final * inv1ma) * s.bg_dot;
   if (araw <= kAlphaMax) {
     const float dL_dG = b.y * dL_dalpha;
     const float gdx = G * dx, gdy = G * dy;
