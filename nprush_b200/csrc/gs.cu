@@ -510,12 +510,14 @@ __global__ void __launch_bounds__(256) k_ssim_fwd2(const float4* __restrict__ im
       const float sxx = mo[o][2] - mx * mx, syy = mo[o][3] - my * my, sxy = mo[o][4] - mx * my;
       const float A1 = 2.0f * mx * my + kSsimC1, A2 = 2.0f * sxy + kSsimC2;
       const float B1 = mx * mx + my * my + kSsimC1, B2 = sxx + syy + kSsimC2;
-      const float sv = (A1 * A2) / (B1 * B2);
+      // two fast reciprocals instead of five divisions (B1, B2 >= C1, C2 > 0)
+      const float iB1 = __fdividef(1.0f, B1), iB2 = __fdividef(1.0f, B2), iB = iB1 * iB2;
+      const float sv = (A1 * A2) * iB;
       ss += sv;
       const float dLds = -lambda * inv_norm;
-      const float ds_dmx = (2.0f * my * A2) / (B1 * B2) - sv * 2.0f * mx / B1;
-      const float ds_dsxx = -sv / B2;
-      const float ds_dsxy = 2.0f * A1 / (B1 * B2);
+      const float ds_dmx = (2.0f * my * A2) * iB - sv * 2.0f * mx * iB1;
+      const float ds_dsxx = -sv * iB2;
+      const float ds_dsxy = 2.0f * A1 * iB;
       const float dm = dLds * ds_dmx, d2 = dLds * ds_dsxx, dxy = dLds * ds_dsxy;
       const size_t plane = (size_t)W * H, pix = (size_t)py * W + px;
       float* mp = maps + ((size_t)v * 9 + 3 * c) * plane + pix;
