@@ -218,6 +218,16 @@ int nps_gs_set_background(nps_gs* gs, float r, float g, float b);
 /* Target images: num_targets x h x w x 4 floats (rgb used), resident on the device. */
 int nps_gs_set_targets(nps_gs* gs, const float* rgba, uint32_t width, uint32_t height, uint32_t num_targets, int mem);
 /* Image size for rendering without targets (set_targets sets it too). */
+/* Targets uploaded from host memory without stalling the step in flight: the
+ * images host_images[ids[i]] (W x H x 4 floats each; page-locked memory lets
+ * the copy run concurrently) go to a staging buffer on a copy stream, then to
+ * the targets in stream order, after every step already queued.  Target i is
+ * then ids[i]'s image.  For a training loop that uploads the next step's
+ * targets while the current step runs (no reference counterpart). */
+int nps_gs_upload_targets(nps_gs* gs, const float* host_images, const uint32_t* ids, uint32_t n_ids, uint32_t w,
+                          uint32_t h);
+/* (loss, mean L1, mean SSIM) of the last loss computed, waiting for it. */
+int nps_gs_read_loss(nps_gs* gs, float* loss3_host);
 int nps_gs_set_image_size(nps_gs* gs, uint32_t width, uint32_t height);
 /* Cameras of the next step: num_views view-projection matrices (+ inverses),
  * and for each the index of its target image (null = 0, 1, 2, ...). */
@@ -309,6 +319,9 @@ int nps_gs_adc_policy(nps_gs* gs, nps_mlp* policy, float step_frac, float grad_t
 int nps_gs_psnr(nps_gs* gs, float* psnr_host);
 int nps_gs_buffers(nps_gs* gs, float** params, float** grads, float** adam_m, float** adam_v, float** image,
                    float** dl_dimage);
+/* Device pointers of the ADC accumulators (count floats each; valid until the
+ * next ADC or load, which may swap buffers).  Used to sum them over ranks. */
+int nps_gs_adc_buffers(nps_gs* gs, float** adc_grad, float** adc_denom);
 int nps_gs_stats(nps_gs* gs, nps_stats* out);
 /* Per-stage device timing with CUDA events on the context stream (off by
  * default).  Stages: 0 preprocess, 1 depth sort, 2 pair emit, 3 tile sort,

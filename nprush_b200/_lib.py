@@ -107,6 +107,9 @@ SIGNATURES = {
     "nps_gs_stage_times": [P, P, P, U32, I32],
     "nps_gs_assign_ids": [P, U32],
     "nps_gs_set_policy_margin": [P, F32],
+    "nps_gs_upload_targets": [P, P, P, U32, U32, U32],
+    "nps_gs_read_loss": [P, P],
+    "nps_gs_adc_buffers": [P, PP, PP],
     "nps_gs_set_deterministic": [P, I32],
     "nps_gs_set_variant": [P, I32, I32],
     "nps_gs_autotune": [P, ctypes.c_char_p, P, P, P],

@@ -1523,6 +1523,11 @@ struct nps_gs {
   // targets
   uint32_t w = 0, h = 0, nt = 0;
   DevBuf tgt_own;
+  // overlapped target upload: host -> staging on a copy stream, staging -> targets in stream order
+  DevBuf tgt_stage;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t stage_ready = nullptr, stage_free = nullptr;
+  bool stage_used = false;
   const float4* tgt = nullptr;
   // views of the current step
   uint32_t nv = 0;
@@ -1694,6 +1699,10 @@ int nps_gs_destroy(nps_gs* o) {
   cudaSetDevice(o->ctx->device);
   cudaStreamSynchronize(o->ctx->stream);
   if (o->gexec) cudaGraphExecDestroy(o->gexec);
+  if (o->copy_stream) cudaStreamSynchronize(o->copy_stream), cudaStreamDestroy(o->copy_stream);
+  if (o->stage_ready) cudaEventDestroy(o->stage_ready);
+  if (o->stage_free) cudaEventDestroy(o->stage_free);
+  o->tgt_stage.release();
   if (o->gdone) cudaEventDestroy(o->gdone);
   if (o->gprev) cudaEventDestroy(o->gprev);
   for (auto& st : o->vstage) {
@@ -1815,6 +1824,53 @@ int nps_gs_set_targets(nps_gs* o, const float* rgba, uint32_t w, uint32_t h, uin
   o->h = h;
   o->nt = num_targets;
   o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_upload_targets(nps_gs* o, const float* host_images, const uint32_t* ids, uint32_t n_ids, uint32_t w,
+                          uint32_t h) {
+  NPS_TRY(check_gs(o));
+  if (!host_images || !ids || n_ids == 0 || w == 0 || h == 0 || w > 16 * 4096 || h > 16 * 4096) {
+    set_error("gs_upload_targets: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  cudaStream_t s = o->ctx->stream;
+  const size_t ib = sizeof(float) * 4 * (size_t)w * h, bytes = ib * n_ids;
+  if (!o->copy_stream) {
+    NPS_CUDA(cudaStreamCreateWithFlags(&o->copy_stream, cudaStreamNonBlocking));
+    NPS_CUDA(cudaEventCreateWithFlags(&o->stage_ready, cudaEventDisableTiming));
+    NPS_CUDA(cudaEventCreateWithFlags(&o->stage_free, cudaEventDisableTiming));
+  }
+  if (o->tgt_stage.bytes < bytes || o->tgt_own.bytes < bytes) {
+    NPS_CUDA(cudaStreamSynchronize(s));
+    NPS_CUDA(cudaStreamSynchronize(o->copy_stream));
+    NPS_TRY(o->tgt_stage.ensure(bytes));
+    NPS_TRY(o->tgt_own.ensure(bytes));
+  }
+  // the staging buffer is free once the previous staging -> targets copy ran
+  if (o->stage_used) NPS_CUDA(cudaStreamWaitEvent(o->copy_stream, o->stage_free, 0));
+  for (uint32_t i = 0; i < n_ids; ++i)
+    NPS_CUDA(cudaMemcpyAsync(o->tgt_stage.as<char>() + i * ib, reinterpret_cast<const char*>(host_images) + ids[i] * ib,
+                             ib, cudaMemcpyHostToDevice, o->copy_stream));
+  NPS_CUDA(cudaEventRecord(o->stage_ready, o->copy_stream));
+  // in stream order: after every step queued so far has read the old targets
+  NPS_CUDA(cudaStreamWaitEvent(s, o->stage_ready, 0));
+  NPS_CUDA(cudaMemcpyAsync(o->tgt_own.p, o->tgt_stage.p, bytes, cudaMemcpyDeviceToDevice, s));
+  NPS_CUDA(cudaEventRecord(o->stage_free, s));
+  o->stage_used = true;
+  o->tgt = o->tgt_own.as<float4>();
+  o->w = w;
+  o->h = h;
+  o->nt = n_ids;
+  o->fwd_valid = false;
+  return NPS_OK;
+}
+
+int nps_gs_read_loss(nps_gs* o, float* loss3_host) {
+  NPS_TRY(check_gs(o));
+  if (!loss3_host) return NPS_ERR_INVALID;
+  NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, o->ctx->stream));
+  NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
   return NPS_OK;
 }
 
@@ -2341,6 +2397,13 @@ int nps_gs_buffers(nps_gs* o, float** params, float** grads, float** adam_m, flo
   if (adam_v) *adam_v = o->av.as<float>();
   if (image) *image = o->img.as<float>();
   if (dl_dimage) *dl_dimage = o->dimg.as<float>();
+  return NPS_OK;
+}
+
+int nps_gs_adc_buffers(nps_gs* o, float** adc_grad, float** adc_denom) {
+  NPS_TRY(check_gs(o));
+  if (adc_grad) *adc_grad = o->adc_grad.as<float>();
+  if (adc_denom) *adc_denom = o->adc_denom.as<float>();
   return NPS_OK;
 }
 

@@ -97,6 +97,21 @@ class GaussianTrainer:
         self._keep = [keep] if borrow else []
         self.width, self.height = w, h
 
+    def upload_targets(self, host_images, ids):
+        """Targets = host_images[ids] (numpy [T, H, W, 4] float32, page-locked for
+        overlap, e.g. a pinned torch tensor's .numpy()), copied on a side stream
+        and put in place after the steps already queued."""
+        a = host_images
+        assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"] and a.ndim == 4
+        ids = np.ascontiguousarray(ids, np.uint32)
+        call("nps_gs_upload_targets", self._h, a.ctypes.data, ids.ctypes.data, len(ids), a.shape[2], a.shape[1])
+        self.width, self.height = a.shape[2], a.shape[1]
+
+    def read_loss(self):
+        l3 = np.zeros(3, np.float32)
+        call("nps_gs_read_loss", self._h, l3.ctypes.data)
+        return tuple(float(x) for x in l3)
+
     def set_image_size(self, width: int, height: int):
         call("nps_gs_set_image_size", self._h, width, height)
         self.width, self.height = width, height
@@ -284,6 +299,11 @@ class GaussianTrainer:
         ptrs = [ctypes.c_void_p() for _ in range(6)]
         call("nps_gs_buffers", self._h, *[ctypes.byref(p) for p in ptrs])
         return dict(zip(("params", "grads", "adam_m", "adam_v", "image", "dl_dimage"), [p.value for p in ptrs]))
+
+    def adc_buffers(self) -> dict:
+        ptrs = [ctypes.c_void_p() for _ in range(2)]
+        call("nps_gs_adc_buffers", self._h, *[ctypes.byref(p) for p in ptrs])
+        return dict(adc_grad=ptrs[0].value, adc_denom=ptrs[1].value)
 
     def stats(self) -> dict:
         st = _lib.nps_stats()

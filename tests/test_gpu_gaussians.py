@@ -339,3 +339,77 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
     for _ in range(5):
         t.train_step()
     assert t.train_step(read_loss=True)[0] < l0
+
+
+def test_upload_targets_matches_set_targets(trainer_cls):
+    """Targets uploaded by ids from page-locked host memory (side stream) give
+    the same step as the same images set directly; an upload queued after a
+    step does not change that step."""
+    n, w, h = 3000, 64, 48
+    p = gs_scene(n, 71, deg=1, log_scale_mean=-3.4)
+    vp, vpi, _ = gs_views(w, h, ((0.0, 0.0, 4.0), (2.5, 1.0, 3.0)))
+    allt = torch.from_numpy(gs_targets(5, w, h, 72)).pin_memory()
+    hs = allt.numpy()
+    ids = np.array([3, 1], np.uint32)
+    # deterministic mode: the comparisons below are bit for bit
+    a = trainer_cls(n, sh_degree=1, params=p)
+    a.set_deterministic(True)
+    a.set_targets(hs[ids])
+    a.set_views(vp, vpi)
+    la = a.train_step(read_loss=True)
+    b = trainer_cls(n, sh_degree=1, params=p)
+    b.set_deterministic(True)
+    b.upload_targets(hs, ids)
+    b.set_views(vp, vpi)
+    b.train_step()
+    b.upload_targets(hs, np.array([0, 4], np.uint32))  # queued behind the step
+    lb = b.read_loss()
+    assert la == lb
+    np.testing.assert_array_equal(a.read_state()["params"], b.read_state()["params"])
+    b.train_step()
+    c = trainer_cls(n, sh_degree=1, params=p)
+    c.set_deterministic(True)
+    c.set_targets(hs[ids])
+    c.set_views(vp, vpi)
+    c.train_step()
+    c.set_targets(hs[[0, 4]])
+    assert c.train_step(read_loss=True) == b.read_loss()
+
+
+def test_sharded_trainer_single_rank_nccl(trainer_cls):
+    """The view-sharded trainer on a one-rank NCCL group: the gradient and ADC
+    buffers are all-reduced in place through tensors aliasing the library's
+    device memory; the result equals the plain step bit for bit
+    (deterministic mode)."""
+    import os
+
+    import torch.distributed as dist
+
+    from nprush_b200.distributed import ShardedTrainer, device_tensor
+    n, w, h = 3000, 64, 48
+    p = gs_scene(n, 81, deg=1, log_scale_mean=-3.4)
+    vp, vpi, _ = gs_views(w, h, ((0.0, 0.0, 4.0), (2.5, 1.0, 3.0), (-2.0, 1.0, 3.2)))
+    tg = gs_targets(3, w, h, 82)
+    ids = np.arange(3, dtype=np.uint32)
+    a = trainer_cls(n, sh_degree=1, params=p)
+    a.set_deterministic(True)
+    a.set_targets(tg)
+    a.set_views(vp, vpi, ids)
+    for _ in range(3):
+        a.train_step()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{29400 + os.getpid() % 500}", rank=0,
+                            world_size=1)
+    try:
+        b = trainer_cls(n, sh_degree=1, params=p)
+        b.set_deterministic(True)
+        b.set_targets(tg)
+        st = ShardedTrainer(b)
+        for _ in range(3):
+            st.train_step(vp, vpi, ids)
+        np.testing.assert_array_equal(b.read_state()["params"], a.read_state()["params"])
+        g = device_tensor(b.buffers()["grads"], n * 64, 0)
+        assert g.shape[0] == n * 64 and g.is_cuda
+        c = st.adc(grad_thresh=1e-6)
+        assert c["after"] > 0
+    finally:
+        dist.destroy_process_group()
