@@ -35,7 +35,7 @@ N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 
 P_USED = 59          # floats per Gaussian used by the model
 # DRAM traffic of one backward-raster launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # 1-pass ncu capture of this workload (13,727,114 pairs): scaled to a launch by its pair count.
-BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 269_891_328 + 15_004_672, 13_727_114
+BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 270_533_120 + 15_059_968, 13_727_114
 S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, opacity)
 
 
