@@ -409,7 +409,10 @@ def main():
                    "cuda_graph": not args.no_graph,
                    "raster_variant": (None if res.get("tuned") is None else
                                       {"fwd_pixels_per_thread": res["tuned"]["fwd_ppt"],
-                                       "bwd_pixels_per_thread": res["tuned"]["bwd_ppt"], "chosen_by": "autotuner"})},
+                                       "fwd_records_per_stage": res["tuned"]["fwd_stage"],
+                                       "bwd_pixels_per_thread": res["tuned"]["bwd_ppt"],
+                                       "bwd_records_per_stage": res["tuned"]["bwd_stage"],
+                                       "chosen_by": "autotuner"})},
         "clocks": res["clocks"],
         "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"]},

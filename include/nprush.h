@@ -254,15 +254,17 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
 /* Raster variants (no reference counterpart): forward and backward raster
- * kernels exist with 1, 2 or 4 vertically adjacent pixels per thread (256,
- * 128 or 64 threads per 16 x 16 tile, as many records staged per batch).
- * nps_gs_autotune times all of them on the current views and targets and
- * keeps the fastest; with cache_path it first looks the workload up in that
- * text file (device, image size, views, SH degree, Gaussian count to ~19%)
- * and appends its choice.  times_ms6 (may be null): forward then backward
- * time of each variant (-1 when the choice came from the cache). */
-int nps_gs_set_variant(nps_gs* gs, int fwd_ppt, int bwd_ppt);
-int nps_gs_autotune(nps_gs* gs, const char* cache_path, int* fwd_ppt_out, int* bwd_ppt_out, float* times_ms6);
+ * kernels exist for (pixels per thread, records staged per batch) in
+ * (1, 256), (2, 128), (2, 256), (4, 64), (4, 128): 256 / ppt threads per 16 x
+ * 16 tile.  A stage of 0 means 256 / ppt.  nps_gs_autotune times all of them
+ * on the current views and targets and keeps the fastest; with cache_path it
+ * first looks the workload up in that text file (device, image size, views,
+ * SH degree, Gaussian count to ~19%) and appends its choice.  choice4 (may be
+ * null): forward ppt, forward stage, backward ppt, backward stage; times_ms10
+ * (may be null): forward then backward time of each variant in the order
+ * above (-1 when the choice came from the cache). */
+int nps_gs_set_variant(nps_gs* gs, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage);
+int nps_gs_autotune(nps_gs* gs, const char* cache_path, int* choice4, float* times_ms10);
 /* Deterministic mode: the backward reduces each (view, Gaussian) gradient in
  * two passes (per-pair tile sums stored, then summed per record in sorted-pair
  * order) instead of with float atomics, so repeated runs are bit-identical.

@@ -111,8 +111,8 @@ SIGNATURES = {
     "nps_gs_read_loss": [P, P],
     "nps_gs_adc_buffers": [P, PP, PP],
     "nps_gs_set_deterministic": [P, I32],
-    "nps_gs_set_variant": [P, I32, I32],
-    "nps_gs_autotune": [P, ctypes.c_char_p, P, P, P],
+    "nps_gs_set_variant": [P, I32, I32, I32, I32],
+    "nps_gs_autotune": [P, ctypes.c_char_p, P, P],
     "nps_gs_adc_features": [P, F32, F32, F32, F32, P, P, P],
     "nps_gs_adc_policy": [P, P, F32, F32, F32, F32, P, P],
     "nps_mlp_num_params": [],

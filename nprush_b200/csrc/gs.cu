@@ -290,31 +290,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   }
   return false;
 }
-// stage records vals[b0 .. b0 + nb) into buf (thread tid < nb copies one)
+// stage records vals[b0 .. b0 + nb) into buf (thread t copies records t,
+// t + blockDim.x, ...)
 __device__ __forceinline__ void stage_batch(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                             uint32_t b0, uint32_t nb, Rec* buf, uint64_t* bar, uint32_t* gidx) {
   if (threadIdx.x == 0) mbar_expect_tx(bar, nb * (uint32_t)sizeof(Rec));
-  if (threadIdx.x < nb) {
+  if (threadIdx.x < nb)
     // this buffer was last read through the generic proxy (before a barrier)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    const uint32_t g = vals[b0 + threadIdx.x];
-    if (gidx) gidx[threadIdx.x] = g;
-    bulk_g2s(buf + threadIdx.x, recs + g, (uint32_t)sizeof(Rec), bar);
+  for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+    const uint32_t g = vals[b0 + i];
+    if (gidx) gidx[i] = g;
+    bulk_g2s(buf + i, recs + g, (uint32_t)sizeof(Rec), bar);
   }
 }
 
 // Forward raster, PPT vertically adjacent pixels per thread: 256 / PPT
-// threads per 16 x 16 tile, records staged 256 / PPT at a time, a warp
-// covers a 16 x 2·PPT strip.  PPT is the autotuned variant (1, 2 or 4).
-template <int PPT>
+// threads per 16 x 16 tile, a warp covers a 16 x 2·PPT strip, records staged
+// SB = SPS · 256 / PPT at a time.  (PPT, SB) is the autotuned variant.
+template <int PPT, int SPS>
 __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                    const uint32_t* __restrict__ rstart,
                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
                                                    float4* __restrict__ img, uint32_t* __restrict__ ncontrib,
                                                    uint32_t* __restrict__ err) {
-  constexpr int NT = 256 / PPT;
-  __shared__ __align__(16) Rec s_rec[2][NT];
+  constexpr int NT = 256 / PPT, SB = NT * SPS;
+  static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
+  __shared__ __align__(16) Rec s_rec[2][SB];
   __shared__ __align__(8) uint64_t s_bar[2];
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
@@ -342,24 +345,24 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const uint32_t nbatch = (end - start + NT - 1) / NT;
-  if (nbatch > 0) stage_batch(recs, vals, start, min((uint32_t)NT, end - start), s_rec[0], &s_bar[0], nullptr);
+  const uint32_t nbatch = (end - start + SB - 1) / SB;
+  if (nbatch > 0) stage_batch(recs, vals, start, min((uint32_t)SB, end - start), s_rec[0], &s_bar[0], nullptr);
   bool pending_next = false;
   for (uint32_t bi = 0; bi < nbatch; ++bi) {
-    const uint32_t base = start + bi * NT, buf = bi & 1u;
-    const uint32_t nb = min((uint32_t)NT, end - base);
+    const uint32_t base = start + bi * SB, buf = bi & 1u;
+    const uint32_t nb = min((uint32_t)SB, end - base);
     // prefetch the next batch into the other buffer (read two batches ago)
     pending_next = bi + 1 < nbatch;
     if (pending_next)
-      stage_batch(recs, vals, base + NT, min((uint32_t)NT, end - base - NT), s_rec[buf ^ 1u], &s_bar[buf ^ 1u],
+      stage_batch(recs, vals, base + SB, min((uint32_t)SB, end - base - SB), s_rec[buf ^ 1u], &s_bar[buf ^ 1u],
                   nullptr);
     if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
     const Rec* sr = s_rec[buf];
     // staged pairs whose alpha >= 1/255 box meets the warp's strip (one lane
-    // tests NT / 32 pairs; the warp then walks the set bits in order)
-    uint32_t hit[NT / 32];
+    // tests SB / 32 pairs; the warp then walks the set bits in order)
+    uint32_t hit[SB / 32];
 #pragma unroll
-    for (int qq = 0; qq < NT / 32; ++qq) {
+    for (int qq = 0; qq < SB / 32; ++qq) {
       const uint32_t jj = qq * 32 + (tid & 31);
       bool h = false;
       if (jj < nb) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
@@ -368,7 +371,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     bool done;
     NPS_ALL_DONE(done);
 #pragma unroll
-    for (int qq = 0; qq < NT / 32; ++qq)
+    for (int qq = 0; qq < SB / 32; ++qq)
     for (uint32_t m = hit[qq]; m != 0u && !done;) {
       const int bit = __ffs(m) - 1;
       m &= m - 1u;
@@ -913,7 +916,7 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
 // that meet its strip and that some of its pixels reached, then walks them in
 // reverse order.  Per-pair sums go to shared memory and then to the (view,
 // Gaussian) records with global atomics.  PPT is the autotuned variant.
-template <int PPT>
+template <int PPT, int SPS>
 __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                     const uint32_t* __restrict__ rstart,
                                                     const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
@@ -922,10 +925,11 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
                                                     const uint32_t* __restrict__ ncontrib,
                                                     const float4* __restrict__ dimg, float* __restrict__ g2,
                                                     uint32_t* __restrict__ err) {
-  constexpr int NT = 256 / PPT;
-  __shared__ __align__(16) Rec s_rec[2][NT];
-  __shared__ uint32_t s_g[2][NT];
-  __shared__ float s_acc[NT][10];
+  constexpr int NT = 256 / PPT, SB = NT * SPS;
+  static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
+  __shared__ __align__(16) Rec s_rec[2][SB];
+  __shared__ uint32_t s_g[2][SB];
+  __shared__ float s_acc[SB][10];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_max;
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
@@ -955,10 +959,10 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
   // batches in reverse: batch i covers [max(start, top - (i+1) NT), top - i NT), top = start + maxlast
-  const uint32_t nbatch = (maxlast + NT - 1) / NT;
+  const uint32_t nbatch = (maxlast + SB - 1) / SB;
   auto bstart_of = [&](uint32_t i) {
-    const uint32_t hi = start + maxlast - i * NT;
-    return hi > start + NT ? hi - NT : start;
+    const uint32_t hi = start + maxlast - i * SB;
+    return hi > start + SB ? hi - SB : start;
   };
   if (nbatch > 0) {
     const uint32_t b0 = bstart_of(0);
@@ -966,27 +970,28 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
   }
   for (uint32_t bi = 0; bi < nbatch; ++bi) {
     const uint32_t buf = bi & 1u;
-    const uint32_t bend = start + maxlast - bi * NT, bstart = bstart_of(bi);
+    const uint32_t bend = start + maxlast - bi * SB, bstart = bstart_of(bi);
     const uint32_t nb = bend - bstart;
     if (bi + 1 < nbatch) {
       const uint32_t nbs = bstart_of(bi + 1);
       stage_batch(recs, vals, nbs, bstart - nbs, s_rec[buf ^ 1u], &s_bar[buf ^ 1u], s_g[buf ^ 1u]);
     }
+    for (uint32_t r = tid; r < (uint32_t)SB; r += NT)
 #pragma unroll
-    for (int k = 0; k < 10; ++k) s_acc[tid][k] = 0.0f;
+      for (int k = 0; k < 10; ++k) s_acc[r][k] = 0.0f;
     if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
     __syncthreads();  // s_acc cleared, staged indices visible
     const Rec* sr = s_rec[buf];
-    uint32_t hit[NT / 32];
+    uint32_t hit[SB / 32];
 #pragma unroll
-    for (int qq = 0; qq < NT / 32; ++qq) {
+    for (int qq = 0; qq < SB / 32; ++qq) {
       const uint32_t jj = qq * 32 + lane;
       bool h = false;
       if (jj < nb && bstart + jj - start < wlast) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
 #pragma unroll
-    for (int qq = NT / 32 - 1; qq >= 0; --qq)
+    for (int qq = SB / 32 - 1; qq >= 0; --qq)
     for (uint32_t m = hit[qq]; m != 0u;) {
       const int bit = 31 - __clz(m);
       m &= ~(1u << bit);
@@ -1008,11 +1013,11 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       }
     }
     __syncthreads();
-    if (tid < nb) {
-      float* dst = g2 + (size_t)s_g[buf][tid] * kG2;
+    for (uint32_t r = tid; r < nb; r += NT) {
+      float* dst = g2 + (size_t)s_g[buf][r] * kG2;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const float x = s_acc[tid][k];
+        const float x = s_acc[r][k];
         if (x != 0.0f) atomicAdd(dst + k, x);
       }
     }
@@ -1515,7 +1520,8 @@ struct nps_gs {
   float lambda = 0.2f;
   bool accumulate = false;   // backward adds to the gradients instead of replacing them
   bool deterministic = false;  // two-pass backward reduction (no float atomics)
-  int fwd_ppt = 1, bwd_ppt = 2;  // raster variants: pixels per thread (1, 2, 4); see nps_gs_autotune
+  // raster variants: pixels per thread (1, 2, 4) and records staged per batch; see nps_gs_autotune
+  int fwd_ppt = 1, bwd_ppt = 2, fwd_stage = 256, bwd_stage = 128;
   DevBuf det_part, det_keys, det_pos;
   SortWork sw_det;
   uint32_t loss_views = 0;   // views the loss is averaged over (0: the views of each call)
@@ -1952,7 +1958,19 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 // synchronisation; the pair buffers keep their capacity and the emit kernel
 // drops pairs beyond it (Adam then skips the step, see k_adam_prep).
 // Raster launches of the current forward state, by variant (pixels per thread).
-static int launch_fwd_raster(nps_gs* o, int ppt) {
+// Raster variants: (pixels per thread, records staged per batch).
+struct RasterVariant {
+  int ppt, stage;
+};
+static bool valid_variant(int ppt, int stage) {
+  if (ppt != 1 && ppt != 2 && ppt != 4) return false;
+  return stage == 256 / ppt || (stage == 512 / ppt && stage <= 256);
+}
+constexpr RasterVariant kVariants[] = {{1, 256}, {2, 128}, {2, 256}, {4, 64}, {4, 128}};
+constexpr int kNumVariants = 5;
+
+// Raster launches of the current forward state, by variant.
+static int launch_fwd_raster(nps_gs* o, int ppt, int stage) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
   const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
@@ -1960,21 +1978,22 @@ static int launch_fwd_raster(nps_gs* o, int ppt) {
   const uint32_t* rend = rstart + (size_t)num_tiles * nv;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   const dim3 grid(tiles_x, tiles_y, nv);
-#define NPS_FWD(PPT)                                                                                      \
-  gs::k_fwd<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
-                                            num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(),  \
-                                            o->stepst.as<uint32_t>() + 6)
-  switch (ppt) {
-    case 2: NPS_FWD(2); break;
-    case 4: NPS_FWD(4); break;
-    default: NPS_FWD(1); break;
-  }
+#define NPS_FWD(PPT, SPS)                                                                                   \
+  gs::k_fwd<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,     \
+                                                 tiles_x, num_tiles, bg, o->img.as<float4>(),                   \
+                                                 o->ncontrib.as<uint32_t>(), o->stepst.as<uint32_t>() + 6)
+  const int sps = stage * ppt / 256;
+  if (ppt == 2 && sps == 2) NPS_FWD(2, 2);
+  else if (ppt == 2) NPS_FWD(2, 1);
+  else if (ppt == 4 && sps == 2) NPS_FWD(4, 2);
+  else if (ppt == 4) NPS_FWD(4, 1);
+  else NPS_FWD(1, 1);
 #undef NPS_FWD
   NPS_CHECK_LAUNCH();
   return NPS_OK;
 }
 
-static int launch_bwd_raster(nps_gs* o, int ppt, const float4* dimg) {
+static int launch_bwd_raster(nps_gs* o, int ppt, int stage, const float4* dimg) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
   const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
@@ -1982,15 +2001,17 @@ static int launch_bwd_raster(nps_gs* o, int ppt, const float4* dimg) {
   const uint32_t* rend = rstart + (size_t)num_tiles * nv;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   const dim3 grid(tiles_x, tiles_y, nv);
-#define NPS_BWD(PPT)                                                                                         \
-  gs::k_bwd2<PPT><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, \
-                                             num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(), dimg, \
-                                             o->g2.as<float>(), o->stepst.as<uint32_t>() + 6)
-  switch (ppt) {
-    case 1: NPS_BWD(1); break;
-    case 4: NPS_BWD(4); break;
-    default: NPS_BWD(2); break;
-  }
+#define NPS_BWD(PPT, SPS)                                                                                     \
+  gs::k_bwd2<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,      \
+                                                  tiles_x, num_tiles, bg, o->img.as<float4>(),                    \
+                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(),             \
+                                                  o->stepst.as<uint32_t>() + 6)
+  const int sps = stage * ppt / 256;
+  if (ppt == 1) NPS_BWD(1, 1);
+  else if (ppt == 2 && sps == 2) NPS_BWD(2, 2);
+  else if (ppt == 4 && sps == 2) NPS_BWD(4, 2);
+  else if (ppt == 4) NPS_BWD(4, 1);
+  else NPS_BWD(2, 1);
 #undef NPS_BWD
   NPS_CHECK_LAUNCH();
   return NPS_OK;
@@ -2084,7 +2105,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   o->sorted_vals = vs;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   StageTimer t_fwd(o, ST_FWD);
-  NPS_TRY(launch_fwd_raster(o, o->fwd_ppt));
+  NPS_TRY(launch_fwd_raster(o, o->fwd_ppt, o->fwd_stage));
   NPS_CHECK_LAUNCH();
   if (out_rgba) NPS_CUDA(cudaMemcpyAsync(out_rgba, o->img.p, sizeof(float4) * npix, cudaMemcpyDeviceToDevice, s));
   o->fwd_valid = true;
@@ -2156,7 +2177,7 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
   if (!o->deterministic) {
     StageTimer t(o, ST_BWD);
-    NPS_TRY(launch_bwd_raster(o, o->bwd_ppt, dimg));
+    NPS_TRY(launch_bwd_raster(o, o->bwd_ppt, o->bwd_stage, dimg));
     NPS_CHECK_LAUNCH();
   } else if (o->pair_cap > 0) {
     StageTimer t(o, ST_BWD);
@@ -2678,24 +2699,28 @@ int nps_gs_load(nps_gs* o, const char* path) {
   return NPS_OK;
 }
 
-int nps_gs_set_variant(nps_gs* o, int fwd_ppt, int bwd_ppt) {
+int nps_gs_set_variant(nps_gs* o, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage) {
   NPS_TRY(check_gs(o));
-  auto ok = [](int v) { return v == 1 || v == 2 || v == 4; };
-  if (!ok(fwd_ppt) || !ok(bwd_ppt)) {
-    set_error("gs_set_variant: pixels per thread must be 1, 2 or 4 (got %d, %d)", fwd_ppt, bwd_ppt);
+  if (fwd_stage == 0) fwd_stage = 256 / (fwd_ppt ? fwd_ppt : 1);
+  if (bwd_stage == 0) bwd_stage = 256 / (bwd_ppt ? bwd_ppt : 1);
+  if (!valid_variant(fwd_ppt, fwd_stage) || !valid_variant(bwd_ppt, bwd_stage)) {
+    set_error("gs_set_variant: (pixels per thread, records per stage) must be one of (1, 256), (2, 128), (2, 256), "
+              "(4, 64), (4, 128); got (%d, %d) and (%d, %d)", fwd_ppt, fwd_stage, bwd_ppt, bwd_stage);
     return NPS_ERR_INVALID;
   }
   o->fwd_ppt = fwd_ppt;
+  o->fwd_stage = fwd_stage;
   o->bwd_ppt = bwd_ppt;
+  o->bwd_stage = bwd_stage;
   o->gkey = 0;
   return NPS_OK;
 }
 
 // Times every raster variant on the current views and targets (one forward
 // and loss first, then `reps` launches of each variant) and keeps the fastest.
-// The choice is cached in a text file (one line per workload: key, forward
-// and backward pixels per thread) when cache_path is given.
-int nps_gs_autotune(nps_gs* o, const char* cache_path, int* fwd_ppt_out, int* bwd_ppt_out, float* times_ms6) {
+// The choice is cached in a text file (one line per workload: key and the
+// four numbers) when cache_path is given.
+int nps_gs_autotune(nps_gs* o, const char* cache_path, int* choice4, float* times_ms10) {
   NPS_TRY(check_gs(o));
   if (!o->tgt || o->nv == 0) {
     set_error("gs_autotune: set views and targets first");
@@ -2710,20 +2735,26 @@ int nps_gs_autotune(nps_gs* o, const char* cache_path, int* fwd_ppt_out, int* bw
                 o->nv, o->sh_deg, nbucket);
   for (char* c = key; *c; ++c)
     if (*c == ' ') *c = '_';
+  auto report = [&](bool timed) {
+    if (choice4) {
+      choice4[0] = o->fwd_ppt; choice4[1] = o->fwd_stage;
+      choice4[2] = o->bwd_ppt; choice4[3] = o->bwd_stage;
+    }
+    if (times_ms10 && !timed)
+      for (int i = 0; i < 2 * kNumVariants; ++i) times_ms10[i] = -1.0f;  // from the cache: not timed
+  };
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "r")) {
       char k[256];
-      int a = 0, b = 0;
+      int a = 0, b = 0, c = 0, d = 0;
       bool found = false;
-      while (std::fscanf(f, "%255s %d %d%*[^\n]", k, &a, &b) == 3)
-        if (std::strcmp(k, key) == 0) found = true, o->fwd_ppt = a, o->bwd_ppt = b;
+      while (std::fscanf(f, "%255s %d %d %d %d%*[^\n]", k, &a, &b, &c, &d) == 5)
+        if (std::strcmp(k, key) == 0 && valid_variant(a, b) && valid_variant(c, d))
+          found = true, o->fwd_ppt = a, o->fwd_stage = b, o->bwd_ppt = c, o->bwd_stage = d;
       std::fclose(f);
       if (found) {
         o->gkey = 0;
-        if (fwd_ppt_out) *fwd_ppt_out = o->fwd_ppt;
-        if (bwd_ppt_out) *bwd_ppt_out = o->bwd_ppt;
-        if (times_ms6)
-          for (int i = 0; i < 6; ++i) times_ms6[i] = -1.0f;  // cached: not timed
+        report(false);
         return NPS_OK;
       }
     }
@@ -2740,18 +2771,18 @@ int nps_gs_autotune(nps_gs* o, const char* cache_path, int* fwd_ppt_out, int* bw
   cudaEvent_t e0, e1;
   NPS_CUDA(cudaEventCreate(&e0));
   NPS_CUDA(cudaEventCreate(&e1));
-  const int ppts[3] = {1, 2, 4};
   float best[2] = {1e30f, 1e30f};
-  int pick[2] = {o->fwd_ppt, o->bwd_ppt};
+  RasterVariant pick[2] = {{o->fwd_ppt, o->fwd_stage}, {o->bwd_ppt, o->bwd_stage}};
   constexpr int kReps = 3;
   for (int pass = 0; pass < 2; ++pass) {
-    for (int vi = 0; vi < 3; ++vi) {
+    for (int vi = 0; vi < kNumVariants; ++vi) {
+      const RasterVariant& va = kVariants[vi];
       float tot = 0.0f;
       for (int r = 0; r <= kReps; ++r) {  // the first launch warms up
         if (pass == 1) NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
         NPS_CUDA(cudaEventRecord(e0, s));
-        if (pass == 0) NPS_TRY(launch_fwd_raster(o, ppts[vi]));
-        else NPS_TRY(launch_bwd_raster(o, ppts[vi], o->dimg.as<float4>()));
+        if (pass == 0) NPS_TRY(launch_fwd_raster(o, va.ppt, va.stage));
+        else NPS_TRY(launch_bwd_raster(o, va.ppt, va.stage, o->dimg.as<float4>()));
         NPS_CUDA(cudaEventRecord(e1, s));
         NPS_CUDA(cudaEventSynchronize(e1));
         float ms = 0.0f;
@@ -2759,23 +2790,25 @@ int nps_gs_autotune(nps_gs* o, const char* cache_path, int* fwd_ppt_out, int* bw
         if (r > 0) tot += ms;
       }
       const float avg = tot / kReps;
-      if (times_ms6) times_ms6[3 * pass + vi] = avg;
-      if (avg < best[pass]) best[pass] = avg, pick[pass] = ppts[vi];
+      if (times_ms10) times_ms10[kNumVariants * pass + vi] = avg;
+      if (avg < best[pass]) best[pass] = avg, pick[pass] = va;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // the variants write identical images; leave a consistent forward state
-  NPS_TRY(launch_fwd_raster(o, pick[0]));
+  // the variants write the same images (to rounding); leave a consistent forward state
+  NPS_TRY(launch_fwd_raster(o, pick[0].ppt, pick[0].stage));
   o->loss_valid = false;
-  o->fwd_ppt = pick[0];
-  o->bwd_ppt = pick[1];
+  o->fwd_ppt = pick[0].ppt;
+  o->fwd_stage = pick[0].stage;
+  o->bwd_ppt = pick[1].ppt;
+  o->bwd_stage = pick[1].stage;
   o->gkey = 0;
-  if (fwd_ppt_out) *fwd_ppt_out = pick[0];
-  if (bwd_ppt_out) *bwd_ppt_out = pick[1];
+  report(true);
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "a")) {
-      std::fprintf(f, "%s %d %d %.4f %.4f\n", key, pick[0], pick[1], best[0], best[1]);
+      std::fprintf(f, "%s %d %d %d %d %.4f %.4f\n", key, pick[0].ppt, pick[0].stage, pick[1].ppt, pick[1].stage,
+                   best[0], best[1]);
       std::fclose(f);
     }
   }

@@ -177,20 +177,22 @@ class GaussianTrainer:
         v, mem2, k2 = _ptr(adam_v)
         call("nps_gs_write_state", self._h, m, v, int(step), mem if adam_m is not None else mem2)
 
-    def set_variant(self, fwd_ppt: int, bwd_ppt: int):
-        """Raster kernels with 1, 2 or 4 pixels per thread."""
-        call("nps_gs_set_variant", self._h, int(fwd_ppt), int(bwd_ppt))
+    VARIANTS = ((1, 256), (2, 128), (2, 256), (4, 64), (4, 128))
+
+    def set_variant(self, fwd_ppt: int, bwd_ppt: int, fwd_stage: int = 0, bwd_stage: int = 0):
+        """Raster kernels with 1, 2 or 4 pixels per thread and the given records
+        staged per batch (0: 256 / pixels per thread)."""
+        call("nps_gs_set_variant", self._h, int(fwd_ppt), int(fwd_stage), int(bwd_ppt), int(bwd_stage))
 
     def autotune(self, cache_path=None) -> dict:
         """Times the raster variants on the current views / targets, keeps the
         fastest (looked up in / appended to cache_path when given)."""
-        f = ctypes.c_int()
-        b = ctypes.c_int()
-        t = np.zeros(6, np.float32)
-        call("nps_gs_autotune", self._h, None if cache_path is None else str(cache_path).encode(), ctypes.byref(f),
-             ctypes.byref(b), t.ctypes.data)
-        return dict(fwd_ppt=f.value, bwd_ppt=b.value, fwd_ms=t[:3].tolist(), bwd_ms=t[3:].tolist(),
-                    cached=bool(t[0] < 0))
+        c = np.zeros(4, np.int32)
+        t = np.zeros(10, np.float32)
+        call("nps_gs_autotune", self._h, None if cache_path is None else str(cache_path).encode(), c.ctypes.data,
+             t.ctypes.data)
+        return dict(fwd_ppt=int(c[0]), fwd_stage=int(c[1]), bwd_ppt=int(c[2]), bwd_stage=int(c[3]),
+                    fwd_ms=t[:5].tolist(), bwd_ms=t[5:].tolist(), cached=bool(t[0] < 0))
 
     def set_deterministic(self, enable: bool):
         """Two-pass backward reduction without float atomics (bit-reproducible)."""

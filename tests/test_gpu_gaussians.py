@@ -315,24 +315,29 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
     t.set_targets(tg)
     t.set_views(vp, vpi)
     imgs, grads = {}, {}
-    for ppt in (1, 2, 4):
-        t.set_variant(ppt, ppt)
+    for ppt, stage in t.VARIANTS:
+        t.set_variant(ppt, ppt, stage, stage)
         t.forward()
         t.loss()
         t.backward()
-        imgs[ppt] = t.read_image(with_grad=False)[0]
-        grads[ppt] = t.read_state()["grads"].astype(np.float64)
-    for ppt in (2, 4):
-        np.testing.assert_allclose(imgs[ppt], imgs[1], atol=1e-6, rtol=0)
-        assert np.linalg.norm(grads[ppt] - grads[1]) / np.linalg.norm(grads[1]) < 1e-5
+        imgs[ppt, stage] = t.read_image(with_grad=False)[0]
+        grads[ppt, stage] = t.read_state()["grads"].astype(np.float64)
+    base = (1, 256)
+    for va in t.VARIANTS[1:]:
+        np.testing.assert_allclose(imgs[va], imgs[base], atol=1e-6, rtol=0)
+        assert np.linalg.norm(grads[va] - grads[base]) / np.linalg.norm(grads[base]) < 1e-5
     rimg, rnc = orc.gs_forward(p, deg, views, w, h)
-    np.testing.assert_allclose(imgs[4], rimg, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(imgs[4, 128], rimg, atol=1e-5, rtol=0)
+    from nprush_b200._lib import NpsError
+    with pytest.raises(NpsError):
+        t.set_variant(1, 1, 512, 512)
     cache = tmp_path / "autotune.txt"
     r = t.autotune(cache)
-    assert r["fwd_ppt"] in (1, 2, 4) and r["bwd_ppt"] in (1, 2, 4) and not r["cached"]
-    assert all(x > 0 for x in r["fwd_ms"] + r["bwd_ms"])
+    assert (r["fwd_ppt"], r["fwd_stage"]) in t.VARIANTS and (r["bwd_ppt"], r["bwd_stage"]) in t.VARIANTS
+    assert not r["cached"] and all(x > 0 for x in r["fwd_ms"] + r["bwd_ms"])
     r2 = t.autotune(cache)
-    assert r2["cached"] and (r2["fwd_ppt"], r2["bwd_ppt"]) == (r["fwd_ppt"], r["bwd_ppt"])
+    keys = ("fwd_ppt", "fwd_stage", "bwd_ppt", "bwd_stage")
+    assert r2["cached"] and [r2[k] for k in keys] == [r[k] for k in keys]
     # the tuned trainer still trains
     t.set_graph(True)
     l0 = t.train_step(read_loss=True)[0]
