@@ -334,6 +334,27 @@ int nps_gs_set_timing(nps_gs* gs, int enable);
 int nps_gs_stage_times(nps_gs* gs, double* ms, uint64_t* calls, uint32_t n, int reset);
 
 
+/* ---- target preprocessing --------------------------------------------------
+ * Device images: H x W float4 RGBA, 16-byte aligned (depth images use .x),
+ * processed on the context's stream.  The reference stores into rgba8unorm
+ * textures; quantize != 0 applies that conversion (clamp to [0, 1], round to
+ * the nearest of 256 levels, ties to even), otherwise the stored floats are
+ * returned.  Alpha is written as 1. */
+/* Replaces GpuBlurPipelineManager's pass (src/lib/gpu/blur.wgsl:23-48): 2r+1
+ * taps along (dir_x, dir_y), edge-clamped, weights exp(-i^2 / (2 sigma^2));
+ * flags bit 0: input sRGB, bit 1: output sRGB. */
+int nps_blur(nps_ctx* ctx, const float* src_rgba, float* dst_rgba, uint32_t w, uint32_t h, int32_t dir_x,
+             int32_t dir_y, int32_t radius, uint32_t flags, float sigma, int quantize);
+/* Replaces GpuDepthAwareBlurPipelineManager's pass (depth_aware_blur.wgsl:12-53):
+ * (2r+1)^2 bilateral window with spatial, colour and depth sigmas 10, 0.5, 0.5. */
+int nps_depth_aware_blur(nps_ctx* ctx, const float* color_rgba, const float* depth_rgba, float* dst_rgba, uint32_t w,
+                         uint32_t h, int32_t radius, int quantize);
+/* The splat edge pass (splat_edge.wgsl:13-44): Sobel magnitude of the depth,
+ * edge-clamped, through smoothstep(thr_min, thr_max, .) (the reference's
+ * SPLAT_EDGE_THRESHOLD_MIN / _MAX, constants.ts:40-41: 0.02, 0.06). */
+int nps_splat_edge(nps_ctx* ctx, const float* depth_rgba, float* dst_rgba, uint32_t w, uint32_t h, float thr_min,
+                   float thr_max, int quantize);
+
 /* ---- learned ADC policy network (no reference counterpart) ----------------
  * 16 -> 64 -> 64 -> 3 MLP with ReLU; the three logits (clone, split, prune)
  * and a fixed 0 logit for keep form a softmax.  Parameters: one fp32 vector of

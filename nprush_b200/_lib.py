@@ -115,6 +115,9 @@ SIGNATURES = {
     "nps_gs_autotune": [P, ctypes.c_char_p, P, P],
     "nps_gs_adc_features": [P, F32, F32, F32, F32, P, P, P],
     "nps_gs_adc_policy": [P, P, F32, F32, F32, F32, P, P],
+    "nps_blur": [P, P, P, U32, U32, I32, I32, I32, U32, F32, I32],
+    "nps_depth_aware_blur": [P, P, P, P, U32, U32, I32, I32],
+    "nps_splat_edge": [P, P, P, U32, U32, F32, F32, I32],
     "nps_mlp_num_params": [],
     "nps_mlp_create": [P, PP],
     "nps_mlp_destroy": [P],

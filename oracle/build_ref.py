@@ -10,6 +10,7 @@ object is built per (shader, size) and cached by content hash.
 Each shared object exports:
   wg_bind(group, binding, void*)          storage / uniform buffer binding
   wg_bind_tex(group, binding, rgba*, w, h) texture_2d<f32> binding (fp32 RGBA)
+  wg_bind_storage_tex(group, binding, rgba*, w, h) texture_storage_2d output (the stored floats)
   wg_size(unsigned[3])                    @workgroup_size
   wg_run_one(x, y, z, gx, gy, gz)         run one workgroup to completion
   wg_dispatch(gx, gy, gz)                 run all workgroups in x-fastest order
@@ -26,6 +27,9 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
 SHADERS = ("splat_backward", "splat_step", "splat_adc", "bezier_backward", "bezier_step", "bezier_adc")
+# target preprocessing (GpuBlurPipelineManager, GpuDepthAwareBlurPipelineManager, the splat edge pass):
+# no size baked in (built with n = 0)
+IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge")
 
 
 def reference_root() -> Path:
@@ -71,11 +75,14 @@ def build(shader: str, n: int) -> Path:
     """Translate + compile `shader` with N baked in; returns the .so path."""
     from wgsl2cpp import TRANSLATOR_VERSION, translate  # noqa: local import (sys.path set by caller)
 
-    if shader not in SHADERS:
+    if shader not in SHADERS + IMAGE_SHADERS:
         raise ValueError(shader)
     src_path = reference_root() / "src/lib/gpu" / f"{shader}.wgsl"
     src = src_path.read_text()
-    consts = splat_consts(n) if shader.startswith("splat") else bezier_consts(n)
+    if shader in IMAGE_SHADERS:
+        consts = dict(gpu_constants())
+    else:
+        consts = splat_consts(n) if shader.startswith("splat") else bezier_consts(n)
     rt = (HERE / "wgsl_rt.h").read_text()
     key = hashlib.sha256(
         (src + repr(sorted(consts.items())) + TRANSLATOR_VERSION + rt + (HERE / "wgsl2cpp.py").read_text()).encode()
@@ -106,6 +113,8 @@ class RefModule:
         self.lib = ctypes.CDLL(str(self.path))
         self.lib.wg_bind.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         self.lib.wg_bind_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint]
+        self.lib.wg_bind_storage_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint,
+                                                 ctypes.c_uint]
         self.lib.wg_run_one.argtypes = [ctypes.c_uint] * 6
         self.lib.wg_dispatch.argtypes = [ctypes.c_uint] * 3
         ws = (ctypes.c_uint * 3)()
@@ -126,6 +135,13 @@ class RefModule:
         assert rgba.dtype.name == "float32" and rgba.ndim == 3 and rgba.shape[2] == 4 and rgba.flags.c_contiguous
         self._keep.append(rgba)
         self.lib.wg_bind_tex(group, binding, rgba.ctypes.data, rgba.shape[1], rgba.shape[0])
+
+    def bind_storage_tex(self, binding: int, rgba, group: int = 0):
+        """Output texture: receives the float values the shader stores (before
+        the texture format's conversion)."""
+        assert rgba.dtype.name == "float32" and rgba.ndim == 3 and rgba.shape[2] == 4 and rgba.flags.c_contiguous
+        self._keep.append(rgba)
+        self.lib.wg_bind_storage_tex(group, binding, rgba.ctypes.data, rgba.shape[1], rgba.shape[0])
 
     def dispatch(self, gx: int, gy: int = 1, gz: int = 1):
         self.lib.wg_dispatch(gx, gy, gz)

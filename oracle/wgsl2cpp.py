@@ -22,7 +22,7 @@ from __future__ import annotations
 import re
 from dataclasses import dataclass, field
 
-TRANSLATOR_VERSION = "3"
+TRANSLATOR_VERSION = "4"
 
 
 class TranslateError(RuntimeError):
@@ -97,7 +97,7 @@ BUILTINS = {
     "select", "min", "max", "clamp", "abs", "sqrt", "exp", "log", "pow", "sin", "cos",
     "floor", "fract", "step", "smoothstep", "dot", "cross", "length", "countTrailingZeros",
     "atomicAdd", "atomicOr", "atomicExchange", "atomicLoad", "atomicStore",
-    "textureLoad", "textureDimensions", "workgroupBarrier", "storageBarrier",
+    "textureLoad", "textureStore", "textureDimensions", "workgroupBarrier", "storageBarrier",
 }
 CXX_KEYWORDS = {
     "new", "delete", "this", "class", "template", "typename", "union", "auto", "register",
@@ -210,6 +210,15 @@ class Translator:
             self.parse_type()
             self.close_angle()
             return "texture_2d"
+        if name == "texture_storage_2d":
+            # texture_storage_2d<format, access>: the host side receives the
+            # stored float values (before the format's conversion)
+            self.expect("<")
+            self.next()
+            self.expect(",")
+            self.next()
+            self.close_angle()
+            return "texture_storage_2d"
         if tok.kind == "id":
             return name  # user struct
         raise TranslateError(f"unknown type {name!r}")
@@ -546,8 +555,16 @@ def translate(src: str, subs: dict, origin: str) -> str:
     out.append('extern "C" {')
     out.append("void wg_bind(int group, int binding, void* p) {")
     for g, b, name, space, ctype in m.bindings:
-        if ctype != "texture_2d":
+        if ctype not in ("texture_2d", "texture_storage_2d"):
             out.append(f"  if (group == {g} && binding == {b}) refmod::{name}__b = (decltype(refmod::{name}__b))p;")
+    out.append("}")
+    out.append("void wg_bind_storage_tex(int group, int binding, float* rgba, unsigned w, unsigned h) {")
+    for g, b, name, space, ctype in m.bindings:
+        if ctype == "texture_storage_2d":
+            out.append(
+                f"  if (group == {g} && binding == {b}) {{ static wgsl::texture_storage_2d t; t.rgba = rgba; t.w = w;"
+                f" t.h = h; refmod::{name}__b = &t; }}"
+            )
     out.append("}")
     out.append("void wg_bind_tex(int group, int binding, const float* rgba, unsigned w, unsigned h) {")
     for g, b, name, space, ctype in m.bindings:

@@ -199,6 +199,23 @@ inline bool bool_(bool a) { return a; }
 
 // ---- builtins -------------------------------------------------------------------
 template <class F, class T> inline auto select(const F& f, const T& t, bool c) -> F { return c ? (F)t : f; }
+// component-wise comparison and selection
+#define WGSL_VCMP(OP)                                                                             \
+  template <class T, int N> inline vec<bool, N> operator OP(const vec<T, N>& a, const vec<T, N>& b) { \
+    vec<bool, N> o;                                                                               \
+    for (int i = 0; i < N; ++i) o[i] = a[i] OP b[i];                                              \
+    return o;                                                                                     \
+  }
+WGSL_VCMP(>)
+WGSL_VCMP(<)
+WGSL_VCMP(>=)
+WGSL_VCMP(<=)
+#undef WGSL_VCMP
+template <class T, int N> inline vec<T, N> select(const vec<T, N>& f, const vec<T, N>& t, const vec<bool, N>& c) {
+  vec<T, N> o;
+  for (int i = 0; i < N; ++i) o[i] = c[i] ? t[i] : f[i];
+  return o;
+}
 
 inline f32 min(f32 a, f32 b) { return std::fmin(a, b); }
 inline f32 max(f32 a, f32 b) { return std::fmax(a, b); }
@@ -226,6 +243,10 @@ inline f32 sqrt(f32 a) { return std::sqrt(a); }
 inline f32 exp(f32 a) { return std::exp(a); }
 inline f32 log(f32 a) { return std::log(a); }
 inline f32 pow(f32 a, f32 b) { return std::pow(a, b); }
+template <int N> inline vec<f32, N> pow(vec<f32, N> a, const vec<f32, N>& b) {
+  for (int i = 0; i < N; ++i) a[i] = std::pow(a[i], b[i]);
+  return a;
+}
 inline f32 sin(f32 a) { return std::sin(a); }
 inline f32 cos(f32 a) { return std::cos(a); }
 inline f32 floor(f32 a) { return std::floor(a); }
@@ -273,6 +294,19 @@ template <class C> inline vec4f textureLoad(const texture_2d& t, const C& c, int
   return o;
 }
 inline vec2u textureDimensions(const texture_2d& t) { vec2u o; o.x = t.w; o.y = t.h; return o; }
+// texture_storage_2d<..., write>: textureStore keeps the float value handed to
+// it (the format conversion, e.g. rgba8unorm, is applied by the caller)
+struct texture_storage_2d {
+  float* rgba = nullptr;  // H*W*4 floats
+  u32 w = 0, h = 0;
+};
+template <class C> inline void textureStore(const texture_storage_2d& t, const C& c, const vec4f& v) {
+  i32 x = (i32)c.x, y = (i32)c.y;
+  if (x < 0 || y < 0 || x >= (i32)t.w || y >= (i32)t.h) return;
+  float* p = t.rgba + ((size_t)y * t.w + (size_t)x) * 4;
+  p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+}
+inline vec2u textureDimensions(const texture_storage_2d& t) { vec2u o; o.x = t.w; o.y = t.h; return o; }
 
 // ---- workgroup execution with fibers ------------------------------------------------
 struct FiberPool {
