@@ -315,6 +315,7 @@ int nps_gs_set_policy_margin(nps_gs* gs, float margin);
 int nps_gs_adc_features(nps_gs* gs, float step_frac, float grad_thresh, float split_scale, float prune_opacity,
                         float* features_dev, uint8_t* plain_dev, uint32_t* ids_dev);
 typedef struct nps_mlp nps_mlp;
+typedef struct nps_pt nps_pt;
 int nps_gs_adc_policy(nps_gs* gs, nps_mlp* policy, float step_frac, float grad_thresh, float split_scale,
                       float prune_opacity, uint32_t* counts4, uint32_t* fallback_host);
 /* PSNR (dB) of each view of the last forward against its target, rgb in [0, 1]. */
@@ -379,6 +380,42 @@ int nps_mlp_grads(nps_mlp* mlp, const float* features_dev, const uint8_t* labels
 int nps_mlp_train(nps_mlp* mlp, const float* features_dev, const uint8_t* labels_dev, uint32_t n,
                   const float* class_w4, uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
                   float* loss_curve, float* acc_curve);
+
+/* ---- path-traced targets (GpuPathTracePipelineManager.ts) -------------------
+ * buildBvh (bvh.ts:202-223) alone, on the host (no device needed):
+ * `vertices` are n_vertices x 12 floats [px py pz, nx ny nz, r g b a, u v],
+ * `indices` n_tris x 3; nodes must hold max(1, 2 n_tris - 1) x 8 floats,
+ * tri_indices n_tris x 3.  The SAH tree is the reference's bit for bit
+ * (8 floats per node, leaf flag 0x80000000 in data1). */
+int nps_bvh_build(const float* vertices, uint32_t n_vertices, const uint32_t* indices, uint32_t n_tris,
+                  float* nodes, uint32_t* tri_indices, uint32_t* n_nodes);
+/* Replaces setMeshes (GpuPathTracePipelineManager.ts:103-151): the
+ * concatenated meshes (host arrays, layout as nps_bvh_build; colour alpha
+ * below 0.5 marks a perfect mirror), their BVH built on the host and
+ * uploaded with the geometry.  The environment starts as one white texel. */
+int nps_pt_create(nps_ctx* ctx, const float* vertices, uint32_t n_vertices, const uint32_t* indices, uint32_t n_tris,
+                  nps_pt** out);
+int nps_pt_destroy(nps_pt* pt);
+/* The uploaded BVH, as buildBvh returns it (BvhResult.nodes / triIndices). */
+int nps_pt_bvh_size(nps_pt* pt, uint32_t* n_nodes, uint32_t* n_tris);
+int nps_pt_read_bvh(nps_pt* pt, float* nodes, uint32_t* tri_indices);
+/* The env_tex binding (path_trace.wgsl:31): w x h float4, host or device
+ * pointer; sampled bilinearly, u repeating, v clamped (:204-208). */
+int nps_pt_set_env(nps_pt* pt, const float* rgba, uint32_t w, uint32_t h);
+/* Replaces dispatch()'s path-trace pass (path_trace.wgsl:222-268) for
+ * n_frames consecutive frames starting at `frame`: each adds one sample per
+ * pixel to accum_rgba (device, w x h float4: radiance sums and the sample
+ * count), as n_frames dispatches would.  inv_view_proj: 16 floats,
+ * column-major (writeInvViewProjMat).  Asynchronous on the context stream. */
+int nps_pt_trace(nps_pt* pt, const float* inv_view_proj, uint32_t frame, uint32_t n_frames, float* accum_rgba,
+                 uint32_t w, uint32_t h);
+/* Rays that gave up because the traversal visited more nodes than the tree
+ * has (cannot happen for a BVH built here; a guard against corruption). */
+int nps_pt_overflows(nps_pt* pt, uint32_t* count);
+/* dispatch()'s resolve pass (path_trace_resolve.wgsl:20-30): mean radiance
+ * x 4 through c / (c + 1), alpha 1; quantize != 0 rounds to the rgba8unorm
+ * levels the reference's output texture holds. */
+int nps_pt_resolve(nps_ctx* ctx, const float* accum_rgba, float* out_rgba, uint32_t w, uint32_t h, int quantize);
 
 #ifdef __cplusplus
 }

@@ -118,6 +118,15 @@ SIGNATURES = {
     "nps_blur": [P, P, P, U32, U32, I32, I32, I32, U32, F32, I32],
     "nps_depth_aware_blur": [P, P, P, P, U32, U32, I32, I32],
     "nps_splat_edge": [P, P, P, U32, U32, F32, F32, I32],
+    "nps_bvh_build": [P, U32, P, U32, P, P, P],
+    "nps_pt_create": [P, P, U32, P, U32, PP],
+    "nps_pt_destroy": [P],
+    "nps_pt_bvh_size": [P, P, P],
+    "nps_pt_read_bvh": [P, P, P],
+    "nps_pt_set_env": [P, P, U32, U32],
+    "nps_pt_trace": [P, P, U32, U32, P, U32, U32],
+    "nps_pt_overflows": [P, P],
+    "nps_pt_resolve": [P, P, P, U32, U32, I32],
     "nps_mlp_num_params": [],
     "nps_mlp_create": [P, PP],
     "nps_mlp_destroy": [P],

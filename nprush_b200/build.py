@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default",
           f"-I{HERE.parent / 'include'}"]
 # reference-semantics kernels: keep every fp32 operation separately rounded
-NO_FMAD = {"compat_splat.cu", "compat_bezier.cu", "binning.cu"}
+NO_FMAD = {"compat_splat.cu", "compat_bezier.cu", "binning.cu", "path_trace.cu"}
 
 
 def sources():
@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             continue
         flags = list(COMMON) + ARCH
         if src.name in NO_FMAD:
-            flags.append("--fmad=false")
+            flags += ["--fmad=false", "-Xcompiler", "-ffp-contract=off"]
         cmd = [NVCC] + flags + ["-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd))

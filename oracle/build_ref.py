@@ -11,6 +11,7 @@ Each shared object exports:
   wg_bind(group, binding, void*)          storage / uniform buffer binding
   wg_bind_tex(group, binding, rgba*, w, h) texture_2d<f32> binding (fp32 RGBA)
   wg_bind_storage_tex(group, binding, rgba*, w, h) texture_storage_2d output (the stored floats)
+  wg_bind_sampler(group, binding, linear, address_u, address_v)  sampler state (address 0 clamp, 1 repeat)
   wg_size(unsigned[3])                    @workgroup_size
   wg_run_one(x, y, z, gx, gy, gz)         run one workgroup to completion
   wg_dispatch(gx, gy, gz)                 run all workgroups in x-fastest order
@@ -29,7 +30,7 @@ REF_OUT = HERE / "_ref"
 SHADERS = ("splat_backward", "splat_step", "splat_adc", "bezier_backward", "bezier_step", "bezier_adc")
 # target preprocessing (GpuBlurPipelineManager, GpuDepthAwareBlurPipelineManager, the splat edge pass):
 # no size baked in (built with n = 0)
-IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge")
+IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge", "path_trace", "path_trace_resolve")
 
 
 def reference_root() -> Path:
@@ -115,6 +116,7 @@ class RefModule:
         self.lib.wg_bind_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint]
         self.lib.wg_bind_storage_tex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint,
                                                  ctypes.c_uint]
+        self.lib.wg_bind_sampler.argtypes = [ctypes.c_int] * 5
         self.lib.wg_run_one.argtypes = [ctypes.c_uint] * 6
         self.lib.wg_dispatch.argtypes = [ctypes.c_uint] * 3
         ws = (ctypes.c_uint * 3)()
@@ -142,6 +144,11 @@ class RefModule:
         assert rgba.dtype.name == "float32" and rgba.ndim == 3 and rgba.shape[2] == 4 and rgba.flags.c_contiguous
         self._keep.append(rgba)
         self.lib.wg_bind_storage_tex(group, binding, rgba.ctypes.data, rgba.shape[1], rgba.shape[0])
+
+    def bind_sampler(self, binding: int, linear: bool = True, address_u: str = "clamp-to-edge",
+                     address_v: str = "clamp-to-edge", group: int = 0):
+        mode = {"clamp-to-edge": 0, "repeat": 1}
+        self.lib.wg_bind_sampler(group, binding, int(bool(linear)), mode[address_u], mode[address_v])
 
     def dispatch(self, gx: int, gy: int = 1, gz: int = 1):
         self.lib.wg_dispatch(gx, gy, gz)

@@ -173,3 +173,40 @@ def bezier_adc(beziers, m_, v_, adam_t, no_kill, grad_accum, loss_accum, pixel_l
     md.bind(4, uni)
     md.dispatch(1, 1, 1)
     return b, adam[:18 * n].reshape(n, 18), adam[18 * n:36 * n].reshape(n, 18), adc[:n], adc[n:], pl
+
+
+def path_trace(vertices, nodes, tri_indices, env_rgba, inv_view_proj, frame, accum):
+    """One dispatch of path_trace.wgsl (GpuPathTracePipelineManager.ts:222-240):
+    adds one sample per pixel to accum (h, w, 4) float32 in place.  Bindings
+    as the manager creates them (:60-72, 196-210): uniforms 80 B
+    [invViewProjMat, frame, num_tris, out_w, out_h], vertices, bvh nodes,
+    bvh triangle indices, accum, env texture + linear sampler (u repeat, v
+    clamp-to-edge)."""
+    h, w = accum.shape[:2]
+    m = mod("path_trace", 0)
+    uni = np.zeros(20, np.uint32)
+    uni[:16] = np.ascontiguousarray(inv_view_proj, np.float32).reshape(16).view(np.uint32)
+    uni[16:20] = [frame, tri_indices.shape[0], w, h]
+    m.bind(0, uni)
+    m.bind(1, np.ascontiguousarray(vertices, np.float32).reshape(-1))
+    m.bind(2, np.ascontiguousarray(nodes, np.float32).reshape(-1))
+    m.bind(3, np.ascontiguousarray(tri_indices, np.uint32).reshape(-1))
+    assert accum.dtype == np.float32 and accum.flags.c_contiguous
+    m.bind(4, accum)
+    m.bind_tex(5, _tex(env_rgba))
+    m.bind_sampler(6, True, "repeat", "clamp-to-edge")
+    m.dispatch(-(-w // 8), -(-h // 8))
+    return accum
+
+
+def path_trace_resolve(accum):
+    """path_trace_resolve.wgsl: the stored floats of the rgba8unorm output."""
+    h, w = accum.shape[:2]
+    m = mod("path_trace_resolve", 0)
+    out = np.zeros((h, w, 4), np.float32)
+    uni = np.array([w, h, 0, 0], np.uint32)
+    m.bind(0, np.ascontiguousarray(accum, np.float32))
+    m.bind_storage_tex(1, out)
+    m.bind(2, uni)
+    m.dispatch(-(-w // 8), -(-h // 8))
+    return out

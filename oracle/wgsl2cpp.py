@@ -22,7 +22,7 @@ from __future__ import annotations
 import re
 from dataclasses import dataclass, field
 
-TRANSLATOR_VERSION = "4"
+TRANSLATOR_VERSION = "5"
 
 
 class TranslateError(RuntimeError):
@@ -98,6 +98,7 @@ BUILTINS = {
     "floor", "fract", "step", "smoothstep", "dot", "cross", "length", "countTrailingZeros",
     "atomicAdd", "atomicOr", "atomicExchange", "atomicLoad", "atomicStore",
     "textureLoad", "textureStore", "textureDimensions", "workgroupBarrier", "storageBarrier",
+    "textureSampleLevel", "atan2", "asin", "acos", "atan", "tan", "reflect", "normalize", "sign",
 }
 CXX_KEYWORDS = {
     "new", "delete", "this", "class", "template", "typename", "union", "auto", "register",
@@ -202,6 +203,9 @@ class Translator:
         if name == "array":
             self.expect("<")
             inner = self.parse_type()
+            if self.peek().text == ">":  # runtime-sized: indexes the bound buffer
+                self.close_angle()
+                return f"rtarray<{inner}>"
             self.expect(",")
             n = self.expr_until_angle()
             return f"warray<{inner}, {n}>"
@@ -219,6 +223,15 @@ class Translator:
             self.next()
             self.close_angle()
             return "texture_storage_2d"
+        if name == "sampler":
+            return "sampler"
+        if name == "ptr":  # ptr<function, T>
+            self.expect("<")
+            self.next()
+            self.expect(",")
+            inner = self.parse_type()
+            self.close_angle()
+            return f"{inner}*"
         if tok.kind == "id":
             return name  # user struct
         raise TranslateError(f"unknown type {name!r}")
@@ -482,6 +495,12 @@ class Translator:
         if tok.kind == "num":
             return self.cxx_literal(tok)
         if tok.kind == "op":
+            # the tokenizer splits '>>' (it cannot tell a shift from two
+            # closing template brackets); in an expression it is a shift
+            if tok.text == ">" and self.peek().text in (">", ">="):
+                return ">" + self.next().text
+            if tok.text == "," and self.peek().text == ")":  # trailing comma in a call
+                return ""
             if tok.text == ".":
                 nxt = self.peek()
                 if nxt.kind == "id" and len(nxt.text) >= 2 and nxt.text not in self.m.field_names and (
@@ -505,10 +524,21 @@ class Translator:
             if self.peek().text != "(":
                 raise TranslateError("array<> type outside constructor/declaration")
             return f"mkarr<{inner}, {n}>"
+        if name == "bitcast" and nxt.text == "<":
+            self.next()
+            inner = self.parse_type()
+            self.close_angle()
+            return f"wgsl::bitcast<{inner}>"
         if name in ("vec2", "vec3", "vec4") and nxt.text == "<":
             self.i -= 1
             t = self.parse_type()
             return t + "_"
+        if nxt.text == "(" and any(name == sn for sn, _ in self.m.structs):
+            # struct constructor: aggregate initialisation
+            self.next()
+            body = self.expr_tokens_until(")")
+            self.expect(")")
+            return f"{self.ident(name)}{{{body}}}"
         if name in SCALARS and nxt.text == "(":
             return f"wgsl::{name}_"
         if name in VECS and nxt.text == "(":
@@ -555,7 +585,7 @@ def translate(src: str, subs: dict, origin: str) -> str:
     out.append('extern "C" {')
     out.append("void wg_bind(int group, int binding, void* p) {")
     for g, b, name, space, ctype in m.bindings:
-        if ctype not in ("texture_2d", "texture_storage_2d"):
+        if ctype not in ("texture_2d", "texture_storage_2d", "sampler"):
             out.append(f"  if (group == {g} && binding == {b}) refmod::{name}__b = (decltype(refmod::{name}__b))p;")
     out.append("}")
     out.append("void wg_bind_storage_tex(int group, int binding, float* rgba, unsigned w, unsigned h) {")
@@ -572,6 +602,14 @@ def translate(src: str, subs: dict, origin: str) -> str:
             out.append(
                 f"  if (group == {g} && binding == {b}) {{ static wgsl::texture_2d t; t.rgba = rgba; t.w = w; t.h = h;"
                 f" refmod::{name}__b = &t; }}"
+            )
+    out.append("}")
+    out.append("void wg_bind_sampler(int group, int binding, int linear, int address_u, int address_v) {")
+    for g, b, name, space, ctype in m.bindings:
+        if ctype == "sampler":
+            out.append(
+                f"  if (group == {g} && binding == {b}) {{ static wgsl::sampler s; s.linear = linear;"
+                f" s.address_u = address_u; s.address_v = address_v; refmod::{name}__b = &s; }}"
             )
     out.append("}")
     out.append(f"void wg_size(unsigned* o) {{ o[0] = {wx}; o[1] = {wy}; o[2] = {wz}; }}")

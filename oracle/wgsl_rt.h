@@ -261,6 +261,27 @@ template <class T, int N> inline T dot(const vec<T, N>& a, const vec<T, N>& b) {
   for (int i = 1; i < N; ++i) s = s + a[i] * b[i];
   return s;
 }
+template <class T, int N> inline vec<T, N> abs(vec<T, N> a) {
+  for (int i = 0; i < N; ++i) a[i] = abs(a[i]);
+  return a;
+}
+inline f32 atan2(f32 y, f32 x) { return std::atan2(y, x); }
+inline f32 asin(f32 a) { return std::asin(a); }
+inline f32 acos(f32 a) { return std::acos(a); }
+inline f32 atan(f32 a) { return std::atan(a); }
+inline f32 tan(f32 a) { return std::tan(a); }
+inline f32 sign(f32 a) { return a > 0.0f ? 1.0f : (a < 0.0f ? -1.0f : 0.0f); }
+template <int N> inline vec<f32, N> normalize(const vec<f32, N>& a) { return a * (1.0f / std::sqrt(dot(a, a))); }
+template <int N> inline vec<f32, N> reflect(const vec<f32, N>& e, const vec<f32, N>& n) {
+  return e - 2.0f * dot(n, e) * n;
+}
+// bitcast<T>(x) between 32-bit scalar types
+template <class T, class S> inline T bitcast(const S& s) {
+  static_assert(sizeof(T) == sizeof(S), "bitcast between 32-bit scalars");
+  T t;
+  std::memcpy(&t, &s, sizeof t);
+  return t;
+}
 inline vec3f cross(const vec3f& a, const vec3f& b) {
   vec3f o;
   o.x = a.y * b.z - a.z * b.y;
@@ -307,6 +328,55 @@ template <class C> inline void textureStore(const texture_storage_2d& t, const C
   p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
 }
 inline vec2u textureDimensions(const texture_storage_2d& t) { vec2u o; o.x = t.w; o.y = t.h; return o; }
+
+// runtime-sized array<T> bound to a storage buffer: indexes the buffer itself
+template <class T> struct rtarray {
+  T& operator[](u32 i) { return reinterpret_cast<T*>(this)[i]; }
+  const T& operator[](u32 i) const { return reinterpret_cast<const T*>(this)[i]; }
+};
+// sampler + textureSampleLevel (level 0): WebGPU's filtering with nearest or
+// linear magnification and the repeat / clamp-to-edge address modes; the
+// bilinear weights are exact f32 fractions
+enum { ADDRESS_CLAMP = 0, ADDRESS_REPEAT = 1 };
+struct sampler {
+  int linear = 1;
+  int address_u = ADDRESS_CLAMP, address_v = ADDRESS_CLAMP;
+};
+inline i32 address_texel(i32 i, i32 n, int mode) {
+  if (mode == ADDRESS_REPEAT) {
+    i32 r = i % n;
+    return r < 0 ? r + n : r;
+  }
+  return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+inline f32 address_coord(f32 u, int mode) { return mode == ADDRESS_REPEAT ? u - std::floor(u) : u; }
+inline vec4f texel(const texture_2d& t, i32 x, i32 y) {
+  const float* p = t.rgba + ((size_t)y * t.w + (size_t)x) * 4;
+  vec4f o;
+  o.x = p[0]; o.y = p[1]; o.z = p[2]; o.w = p[3];
+  return o;
+}
+inline vec4f textureSampleLevel(const texture_2d& t, const sampler& s, const vec2f& uv, f32) {
+  const i32 w = (i32)t.w, h = (i32)t.h;
+  const f32 u = address_coord(uv.x, s.address_u) * (f32)w, v = address_coord(uv.y, s.address_v) * (f32)h;
+  if (!s.linear) {
+    const i32 x = address_texel((i32)std::floor(u), w, s.address_u);
+    const i32 y = address_texel((i32)std::floor(v), h, s.address_v);
+    return texel(t, x, y);
+  }
+  const f32 fx = u - 0.5f, fy = v - 0.5f;
+  const f32 x0f = std::floor(fx), y0f = std::floor(fy);
+  const f32 ax = fx - x0f, ay = fy - y0f;
+  const i32 x0 = address_texel((i32)x0f, w, s.address_u), x1 = address_texel((i32)x0f + 1, w, s.address_u);
+  const i32 y0 = address_texel((i32)y0f, h, s.address_v), y1 = address_texel((i32)y0f + 1, h, s.address_v);
+  const vec4f a = texel(t, x0, y0), b = texel(t, x1, y0), c = texel(t, x0, y1), d = texel(t, x1, y1);
+  vec4f o;
+  for (int i = 0; i < 4; ++i) {
+    const f32 top = a[i] + (b[i] - a[i]) * ax, bot = c[i] + (d[i] - c[i]) * ax;
+    o[i] = top + (bot - top) * ay;
+  }
+  return o;
+}
 
 // ---- workgroup execution with fibers ------------------------------------------------
 struct FiberPool {
