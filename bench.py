@@ -329,6 +329,126 @@ def run_reference(args):
 
 METRIC = "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)"
 
+# ------------------------------------------------- path-traced target workload
+PT_W, PT_H, PT_OBJECTS, PT_DETAIL, PT_BATCH = 1024, 768, 16, 20, 8
+PT_METRIC = "path-traced samples/s (1 sample per pixel per frame, <= 8 bounces, 12k-triangle scene, 1024x768)"
+
+
+def pt_scene():
+    from nprush_b200 import camera, meshes
+    sc = meshes.demo_scene(PT_OBJECTS, seed=7, mirror_fraction=0.3, sphere_detail=PT_DETAIL)
+    env = meshes.sky_env(256, 128)
+    _, inv = camera.view_proj((4.0, -3.5, 2.6), (0.0, 0.0, 0.3), 0.9, PT_W / PT_H, up=(0.0, 0.0, 1.0))
+    return sc, env, inv
+
+
+def pt_reference_sample(args):
+    """The reference's own path_trace.wgsl (translated to C++, oracle/_ref) on
+    the host: a spread of its 8 x 8 workgroups of one frame, extrapolated to
+    the frame.  Returns (samples/s, description) or (None, why)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import build_ref
+    sc, env, inv = pt_scene()
+    so = sorted((ROOT / "oracle" / "_ref").glob("path_trace_n0_*.so"))
+    if not so and not build_ref.reference_available():
+        return None, "oracle/_ref path_trace was not built (no reference checkout)"
+    from bvh import build_bvh
+    nodes, tris = build_bvh(sc.vertices, sc.indices)
+    mod = build_ref.RefModule.from_path(so[-1]) if so else build_ref.RefModule("path_trace", 0)
+    acc = np.zeros((PT_H, PT_W, 4), np.float32)
+    uni = np.zeros(20, np.uint32)
+    uni[:16] = np.ascontiguousarray(inv, np.float32).view(np.uint32)
+    uni[16:20] = [0, tris.shape[0], PT_W, PT_H]
+    mod.bind(0, uni)
+    mod.bind(1, np.ascontiguousarray(sc.vertices, np.float32).reshape(-1))
+    mod.bind(2, np.ascontiguousarray(nodes).reshape(-1))
+    mod.bind(3, np.ascontiguousarray(tris).reshape(-1))
+    mod.bind(4, acc)
+    mod.bind_tex(5, env)
+    mod.bind_sampler(6, True, "repeat", "clamp-to-edge")
+    gx, gy = PT_W // 8, PT_H // 8
+    groups = [(x, y) for y in range(3, gy, 11) for x in range(5, gx, 13)]
+    per = []
+    for _ in range(max(1, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        for x, y in groups:
+            mod.run_one(x, y, 0, gx, gy, 1)
+        per.append((time.perf_counter() - t0) / (len(groups) * 64))
+    t_sample = float(np.median(per))
+    return 1.0 / t_sample, (f"{len(groups)} of {gx * gy} 8x8 workgroups of one frame per timed sample "
+                            f"({t_sample * 1e6:.1f} us per path), extrapolated; single host thread")
+
+
+def run_path_trace(args):
+    import torch
+
+    from nprush_b200 import _lib
+    from nprush_b200.path_trace import PathTracer
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = _lib.context(dev)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    sc, env, inv = pt_scene()
+    with torch.cuda.stream(stream):
+        pt = PathTracer(env_texture=env, device=dev)
+        pt.set_meshes(sc)
+        pt.set_output_size(PT_W, PT_H)
+        pt.write_inv_view_proj_mat(inv)
+        torch.cuda.synchronize()
+
+        def timed(frames_per_launch, launches):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            for _ in range(launches):
+                pt.trace(frames_per_launch)
+            ev[1].record(stream)
+            ev[1].synchronize()
+            return ev[0].elapsed_time(ev[1])
+
+        timed(1, args.warmup)
+        with ClockSampler(dev) as clk:
+            ms = timed(1, args.steps)
+            ms_batch = timed(PT_BATCH, max(1, args.steps // PT_BATCH))
+        # end to end through the public API: the camera matrix goes up with
+        # the launch, the resolved 8-bit image comes back to the host
+        host = torch.empty((PT_H, PT_W, 4), dtype=torch.float32, pin_memory=True)
+        pt.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pt.write_inv_view_proj_mat(inv)
+            pt.dispatch(frames=1, sync=False)
+            host.copy_(pt.output, non_blocking=True)
+            stream.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+        overflows = pt.overflows()
+        pt.close()
+    npx = PT_W * PT_H
+    ms_step = ms / args.steps
+    line = {
+        "metric": PT_METRIC, "value": npx / (ms_step * 1e-3), "unit": "samples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded ground + 16 spheres and boxes (30% mirrors), procedural sky environment",
+        "config": {"workload": f"path-traced targets: {sc.n_tris} triangles, {PT_W}x{PT_H}, one frame per step",
+                   "triangles": sc.n_tris, "resolution": [PT_W, PT_H], "l2": "scene resident (BVH < L2)",
+                   "batched": {"frames_per_launch": PT_BATCH,
+                               "samples_per_s": npx * PT_BATCH * max(1, args.steps // PT_BATCH) / (ms_batch * 1e-3)}},
+        "clocks": clk.summary(),
+        "e2e": {"value": npx / (e2e_ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": 64,
+                "d2h_bytes_per_step": npx * 16},
+        "gpu_launches": args.steps,
+        "roofline": None,
+        "bound": "latency / issue (divergent BVH traversal; the BVH and vertices sit in L2)",
+        "traversal_overflows": overflows,
+    }
+    if not args.no_cpu_baseline:
+        v, why = pt_reference_sample(args)
+        line["cpu_baseline"] = (None if v is None else
+                                {"value": v, "unit": "samples/s", "cores": 1, "kind": "reference", "sample": why})
+    return line
+
 
 def launches_per_step(tile_passes: int) -> int:
     # preprocess, set count, depth sort (4 passes x 3), gather, scan (3), emit,
@@ -343,6 +463,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="train", choices=["train", "path_trace"],
+                    help="train: the Gaussian train step (headline); path_trace: path-traced target generation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # smaller shapes for profiler captures (the bench number is config 2 only)
     ap.add_argument("--gaussians", type=int, default=None)
@@ -363,6 +485,21 @@ def main():
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "path_trace":
+        if rank != 0:
+            return
+        if args.impl == "reference":
+            v, why = pt_reference_sample(args)
+            line = ({"impl": "reference", "unavailable": why} if v is None else
+                    {"impl": "reference", "metric": PT_METRIC, "value": v, "unit": "samples/s",
+                     "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                     "config": {"workload": "reference path_trace.wgsl (translated to C++) on the same scene"},
+                     "cpu_baseline": {"value": v, "unit": "samples/s", "cores": 1, "kind": "reference", "sample": why},
+                     "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        else:
+            line = run_path_trace(args)
+        print(json.dumps(line))
+        return
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))
