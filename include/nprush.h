@@ -316,6 +316,7 @@ int nps_gs_adc_features(nps_gs* gs, float step_frac, float grad_thresh, float sp
                         float* features_dev, uint8_t* plain_dev, uint32_t* ids_dev);
 typedef struct nps_mlp nps_mlp;
 typedef struct nps_pt nps_pt;
+typedef struct nps_mesh nps_mesh;
 int nps_gs_adc_policy(nps_gs* gs, nps_mlp* policy, float step_frac, float grad_thresh, float split_scale,
                       float prune_opacity, uint32_t* counts4, uint32_t* fallback_host);
 /* PSNR (dB) of each view of the last forward against its target, rgb in [0, 1]. */
@@ -416,6 +417,33 @@ int nps_pt_overflows(nps_pt* pt, uint32_t* count);
  * x 4 through c / (c + 1), alpha 1; quantize != 0 rounds to the rgba8unorm
  * levels the reference's output texture holds. */
 int nps_pt_resolve(nps_ctx* ctx, const float* accum_rgba, float* out_rgba, uint32_t w, uint32_t h, int quantize);
+
+/* ---- mesh render pass (GpuMeshRenderPipelineManager.ts, envmap.wgsl) --------
+ * nps_mesh_create replaces the manager's constructor mesh plus setGroundMesh
+ * (GpuMeshRenderPipelineManager.ts:41-160): the meshes concatenated in draw
+ * order, vertices n_vertices x 12 floats [pos, normal, rgba, uv], indices
+ * n_tris x 3 (host arrays). */
+int nps_mesh_create(nps_ctx* ctx, const float* vertices, uint32_t n_vertices, const uint32_t* indices,
+                    uint32_t n_tris, nps_mesh** out);
+int nps_mesh_destroy(nps_mesh* mesh);
+/* The matcap texture (mesh.wgsl:9-10, linear, clamped) and the environment
+ * panorama (envmap.wgsl:17-18, linear, u repeating, v clamped): w x h
+ * float4, host or device pointer; both start as one white texel. */
+int nps_mesh_set_matcap(nps_mesh* mesh, const float* rgba, uint32_t w, uint32_t h);
+int nps_mesh_set_env(nps_mesh* mesh, const float* rgba, uint32_t w, uint32_t h);
+/* One mesh render pass as the viewer's optimisation pass draws it
+ * (GpuRunner.svelte.ts:611-634): the environment background (draw_env = 0:
+ * the clear colour 0.05), then the mesh through mesh.wgsl's vert / frag with
+ * back faces culled (counter-clockwise front) and depth "less" in draw order.
+ * uniforms52: the shared uniform buffer (GpuUniformsBufferManager.ts, 208
+ * bytes: viewProj, view, shadingMode (0 normals, 1 matcap), 3 pad,
+ * invViewProj; matrices column-major).  Writes color_rgba (the shaded colour)
+ * and depth_rgba (1 - 0.1 / max(w, 0.1) per fragment, 1 where no triangle):
+ * device w x h float4 images, at most 16384 x 16384; quantize != 0 rounds
+ * them to the 8-bit levels of the reference's targets.  Asynchronous on the
+ * context stream. */
+int nps_mesh_render(nps_mesh* mesh, const float* uniforms52, float* color_rgba, float* depth_rgba, uint32_t w,
+                    uint32_t h, int draw_env, int quantize);
 
 #ifdef __cplusplus
 }

@@ -127,6 +127,11 @@ SIGNATURES = {
     "nps_pt_trace": [P, P, U32, U32, P, U32, U32],
     "nps_pt_overflows": [P, P],
     "nps_pt_resolve": [P, P, P, U32, U32, I32],
+    "nps_mesh_create": [P, P, U32, P, U32, PP],
+    "nps_mesh_destroy": [P],
+    "nps_mesh_set_matcap": [P, P, U32, U32],
+    "nps_mesh_set_env": [P, P, U32, U32],
+    "nps_mesh_render": [P, P, P, P, U32, U32, I32, I32],
     "nps_mlp_num_params": [],
     "nps_mlp_create": [P, PP],
     "nps_mlp_destroy": [P],

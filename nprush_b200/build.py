@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default",
           f"-I{HERE.parent / 'include'}"]
 # reference-semantics kernels: keep every fp32 operation separately rounded
-NO_FMAD = {"compat_splat.cu", "compat_bezier.cu", "binning.cu", "path_trace.cu"}
+NO_FMAD = {"compat_splat.cu", "compat_bezier.cu", "binning.cu", "path_trace.cu", "mesh_raster.cu"}
 
 
 def sources():

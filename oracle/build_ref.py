@@ -15,6 +15,7 @@ Each shared object exports:
   wg_size(unsigned[3])                    @workgroup_size
   wg_run_one(x, y, z, gx, gy, gz)         run one workgroup to completion
   wg_dispatch(gx, gy, gz)                 run all workgroups in x-fastest order
+  call_<fn>(in*, out*), size_<fn>(o[2])   a @vertex / @fragment function of one input
 """
 from __future__ import annotations
 
@@ -25,12 +26,16 @@ import re
 import subprocess
 from pathlib import Path
 
+import numpy as np
+
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
 SHADERS = ("splat_backward", "splat_step", "splat_adc", "bezier_backward", "bezier_step", "bezier_adc")
 # target preprocessing (GpuBlurPipelineManager, GpuDepthAwareBlurPipelineManager, the splat edge pass):
 # no size baked in (built with n = 0)
 IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge", "path_trace", "path_trace_resolve")
+# render pipelines: their @vertex / @fragment functions, callable one invocation at a time
+STAGE_SHADERS = ("mesh", "envmap")
 
 
 def reference_root() -> Path:
@@ -76,11 +81,11 @@ def build(shader: str, n: int) -> Path:
     """Translate + compile `shader` with N baked in; returns the .so path."""
     from wgsl2cpp import TRANSLATOR_VERSION, translate  # noqa: local import (sys.path set by caller)
 
-    if shader not in SHADERS + IMAGE_SHADERS:
+    if shader not in SHADERS + IMAGE_SHADERS + STAGE_SHADERS:
         raise ValueError(shader)
     src_path = reference_root() / "src/lib/gpu" / f"{shader}.wgsl"
     src = src_path.read_text()
-    if shader in IMAGE_SHADERS:
+    if shader in IMAGE_SHADERS + STAGE_SHADERS:
         consts = dict(gpu_constants())
     else:
         consts = splat_consts(n) if shader.startswith("splat") else bezier_consts(n)
@@ -149,6 +154,19 @@ class RefModule:
                      address_v: str = "clamp-to-edge", group: int = 0):
         mode = {"clamp-to-edge": 0, "repeat": 1}
         self.lib.wg_bind_sampler(group, binding, int(bool(linear)), mode[address_u], mode[address_v])
+
+    def call(self, fn: str, arg):
+        """Runs the @vertex / @fragment function `fn` on one input (its bytes
+        in `arg`); returns the result as float32."""
+        sizes = (ctypes.c_uint * 2)()
+        getattr(self.lib, f"size_{fn}")(sizes)
+        a = np.ascontiguousarray(arg)
+        assert a.nbytes == sizes[0], (fn, a.nbytes, sizes[0])
+        out = np.zeros(sizes[1] // 4, np.float32)
+        f = getattr(self.lib, f"call_{fn}")
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        f(a.ctypes.data, out.ctypes.data)
+        return out
 
     def dispatch(self, gx: int, gy: int = 1, gz: int = 1):
         self.lib.wg_dispatch(gx, gy, gz)

@@ -98,7 +98,7 @@ BUILTINS = {
     "floor", "fract", "step", "smoothstep", "dot", "cross", "length", "countTrailingZeros",
     "atomicAdd", "atomicOr", "atomicExchange", "atomicLoad", "atomicStore",
     "textureLoad", "textureStore", "textureDimensions", "workgroupBarrier", "storageBarrier",
-    "textureSampleLevel", "atan2", "asin", "acos", "atan", "tan", "reflect", "normalize", "sign",
+    "textureSampleLevel", "textureSample", "atan2", "asin", "acos", "atan", "tan", "reflect", "normalize", "sign",
 }
 CXX_KEYWORDS = {
     "new", "delete", "this", "class", "template", "typename", "union", "auto", "register",
@@ -123,6 +123,7 @@ class Module:
     wgsize: tuple = (1, 1, 1)
     field_names: set = field(default_factory=set)
     fn_names: set = field(default_factory=set)
+    stage_fns: list = field(default_factory=list)    # (name, [param types]) of @vertex / @fragment functions
 
 
 class Translator:
@@ -412,8 +413,12 @@ class Translator:
                 + body + "\n}\n"
             )
         else:
+            # plain functions, and @vertex / @fragment stages as plain functions
+            # of their (attribute-annotated) inputs
             plist = ", ".join(f"{pt} {self.ident(pn)}" for pn, pt, _ in params)
             self.m.funcs.append(f"static {ret} {self.ident(name)}({plist}) {{\n{body}\n}}\n")
+            if "vertex" in adict or "fragment" in adict:
+                self.m.stage_fns.append((self.ident(name), [pt for _, pt, _ in params]))
 
     # -- statements / expressions (token rewriting)
     def expr_tokens_until(self, stop: str) -> str:
@@ -556,8 +561,8 @@ def translate(src: str, subs: dict, origin: str) -> str:
     text = inject(src, subs)
     tr = Translator(tokenize(text))
     m = tr.run()
-    if m.entry is None:
-        raise TranslateError("no @compute entry point")
+    if m.entry is None and not m.stage_fns:
+        raise TranslateError("no @compute, @vertex or @fragment entry point")
     out = []
     out.append(f"// Generated by oracle/wgsl2cpp.py v{TRANSLATOR_VERSION} from {origin}.")
     out.append("// Build artefact of the test oracle; not part of the product.")
@@ -580,6 +585,19 @@ def translate(src: str, subs: dict, origin: str) -> str:
         out.append(f"  std::memset((void*)&{name}, 0, sizeof({name}));")
     out.append("}")
     out.extend(m.funcs)
+    # @vertex / @fragment stages with one input: call_<name>(in, out) copies
+    # the result out; size_<name>(o) gives sizeof(input), sizeof(result)
+    for fname, ptypes in m.stage_fns:
+        if len(ptypes) != 1:
+            continue
+        pt = ptypes[0]
+        out.append(f'extern "C" void call_{fname}(const void* in, void* out) {{')
+        out.append(f"  const auto r = {fname}(*(const {pt}*)in);")
+        out.append("  std::memcpy(out, &r, sizeof r);")
+        out.append("}")
+        out.append(f'extern "C" void size_{fname}(unsigned* o) {{')
+        out.append(f"  o[0] = sizeof({pt}); o[1] = sizeof({fname}(std::declval<{pt}>()));")
+        out.append("}")
     out.append("}  // namespace refmod")
     wx, wy, wz = m.wgsize
     out.append('extern "C" {')
@@ -614,11 +632,14 @@ def translate(src: str, subs: dict, origin: str) -> str:
     out.append("}")
     out.append(f"void wg_size(unsigned* o) {{ o[0] = {wx}; o[1] = {wy}; o[2] = {wz}; }}")
     out.append("void wg_run_one(unsigned x, unsigned y, unsigned z, unsigned gx, unsigned gy, unsigned gz) {")
-    out.append("  refmod::wg_zero__();")
-    out.append(
-        f"  wgsl::run_workgroup(refmod::{m.entry}, wgsl::mk<wgsl::u32,3>(x, y, z),"
-        f" wgsl::mk<wgsl::u32,3>({wx}u, {wy}u, {wz}u), wgsl::mk<wgsl::u32,3>(gx, gy, gz));"
-    )
+    if m.entry is not None:
+        out.append("  refmod::wg_zero__();")
+        out.append(
+            f"  wgsl::run_workgroup(refmod::{m.entry}, wgsl::mk<wgsl::u32,3>(x, y, z),"
+            f" wgsl::mk<wgsl::u32,3>({wx}u, {wy}u, {wz}u), wgsl::mk<wgsl::u32,3>(gx, gy, gz));"
+        )
+    else:  # a vertex / fragment module: no compute entry point
+        out.append("  (void)x; (void)y; (void)z; (void)gx; (void)gy; (void)gz;")
     out.append("}")
     out.append("void wg_dispatch(unsigned gx, unsigned gy, unsigned gz) {")
     out.append("  for (unsigned z = 0; z < gz; ++z) for (unsigned y = 0; y < gy; ++y) for (unsigned x = 0; x < gx; ++x)")

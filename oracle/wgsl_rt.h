@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <type_traits>
 #include <ucontext.h>
+#include <utility>
 #include <vector>
 
 namespace wgsl {
@@ -376,6 +377,12 @@ inline vec4f textureSampleLevel(const texture_2d& t, const sampler& s, const vec
     o[i] = top + (bot - top) * ay;
   }
   return o;
+}
+
+// textureSample (implicit level of detail): the textures bound here have one
+// level, so it samples level 0
+inline vec4f textureSample(const texture_2d& t, const sampler& s, const vec2f& uv) {
+  return textureSampleLevel(t, s, uv, 0.0f);
 }
 
 // ---- workgroup execution with fibers ------------------------------------------------
