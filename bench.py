@@ -379,6 +379,95 @@ def pt_reference_sample(args):
                             f"({t_sample * 1e6:.1f} us per path), extrapolated; single host thread")
 
 
+MR_W, MR_H, MR_OBJECTS, MR_DETAIL = 1024, 768, 40, 32
+MR_METRIC = "mesh render passes/s (environment + ~80k-triangle mesh, colour + reciprocal depth targets, 1024x768)"
+
+
+def mr_scene():
+    from nprush_b200 import camera, meshes
+    sc = meshes.demo_scene(MR_OBJECTS, seed=7, mirror_fraction=0.0, sphere_detail=MR_DETAIL)
+    eye, tgt = (4.0, -3.5, 2.6), (0.0, 0.0, 0.3)
+    vp, inv = camera.view_proj(eye, tgt, 0.9, MR_W / MR_H, up=(0.0, 0.0, 1.0))
+    u = np.zeros(52, np.float32)
+    u[0:16], u[16:32], u[36:52] = vp, camera.col_major(camera.look_at(eye, tgt, (0.0, 0.0, 1.0))), inv
+    return sc, meshes.sky_env(256, 128), u
+
+
+def run_mesh_raster(args):
+    """The viewer's mesh render pass (nps_mesh_render): CUDA events around
+    each pass on the library's stream; the CPU leg is the float32 restatement
+    (oracle/mesh_raster.py) at 64 x 48 on the same scene, per pixel scaled."""
+    import torch
+
+    from nprush_b200 import _lib
+    from nprush_b200.mesh_render import MeshRenderer
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = _lib.context(dev)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    sc, env, uni = mr_scene()
+    with torch.cuda.stream(stream):
+        r = MeshRenderer(sc, matcap=env, env=env, device=dev)
+        r.uniforms[:] = uni
+        col = torch.empty((MR_H, MR_W, 4), dtype=torch.float32, device=f"cuda:{dev}")
+        dep = torch.empty_like(col)
+        torch.cuda.synchronize()
+
+        def one():
+            _lib.call("nps_mesh_render", r._h, r.uniforms.ctypes.data, col.data_ptr(), dep.data_ptr(), MR_W, MR_H,
+                      1, 1)
+
+        for _ in range(args.warmup):
+            one()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        with ClockSampler(dev) as clk:
+            ev[0].record(stream)
+            for _ in range(args.steps):
+                one()
+            ev[1].record(stream)
+            ev[1].synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        host_c = torch.empty((MR_H, MR_W, 4), dtype=torch.float32, pin_memory=True)
+        host_d = torch.empty_like(host_c)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one()
+            host_c.copy_(col, non_blocking=True)
+            host_d.copy_(dep, non_blocking=True)
+            stream.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+        r.close()
+    line = {
+        "metric": MR_METRIC, "value": 1000.0 / ms, "unit": "passes/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic: seeded ground + 40 spheres and boxes, procedural sky and matcap",
+        "config": {"workload": f"mesh render pass: {sc.n_tris} triangles, {MR_W}x{MR_H}, 8-bit targets",
+                   "triangles": sc.n_tris, "resolution": [MR_W, MR_H]},
+        "clocks": clk.summary(),
+        "e2e": {"value": 1000.0 / e2e_ms, "unit": "passes/s", "h2d_bytes_per_step": 208,
+                "d2h_bytes_per_step": 2 * MR_W * MR_H * 16},
+        "gpu_launches": 7 * args.steps,  # vertex, setup, 3 scan passes, raster, shade
+        "roofline": None,
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import mesh_raster as mr
+        w, h = 64, 48
+        su = uni.copy()
+        from nprush_b200 import camera
+        vp, inv = camera.view_proj((4.0, -3.5, 2.6), (0.0, 0.0, 0.3), 0.9, w / h, up=(0.0, 0.0, 1.0))
+        su[0:16], su[36:52] = vp, inv
+        t0 = time.perf_counter()
+        mr.render(sc.vertices, sc.indices, su, w, h, mr.RestatedStages(env, env))
+        t = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / (t * (MR_W * MR_H) / (w * h)), "unit": "passes/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"the float32 restatement at {w}x{h} ({t:.1f} s), scaled by pixel count; "
+                                          "one host thread (numpy)"}
+    return line
+
+
 def run_path_trace(args):
     import torch
 
@@ -463,8 +552,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="train", choices=["train", "path_trace"],
-                    help="train: the Gaussian train step (headline); path_trace: path-traced target generation")
+    ap.add_argument("--workload", default="train", choices=["train", "path_trace", "mesh_raster"],
+                    help="train: the Gaussian train step (headline); path_trace: path-traced target generation; "
+                         "mesh_raster: the viewer's mesh render pass (colour + depth targets)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # smaller shapes for profiler captures (the bench number is config 2 only)
     ap.add_argument("--gaussians", type=int, default=None)
@@ -485,6 +575,12 @@ def main():
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "mesh_raster":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's mesh pass is a WebGPU render "
+                              "pipeline: no graphics stack on this box"} if args.impl == "reference"
+                             else run_mesh_raster(args)))
+        return
     if args.workload == "path_trace":
         if rank != 0:
             return
