@@ -137,6 +137,10 @@ typedef struct nps_stats {
                               update (pair overflow), [2] record-staging waits that timed out */
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
+/* Sets the manager's stepCount (GpuSplatOptimizerManager.ts:380, dispatch()
+ * calls so far; ADC runs when it reaches a multiple of 25): a restored
+ * checkpoint continues the ADC schedule. */
+int nps_splat_opt_set_step_count(nps_splat_opt* opt, uint32_t count);
 
 /* ========================================== Bezier strokes, reference semantics
  * Record: 20 floats per curve (bezier_forward.wgsl:1-7): p0.xyz, width |
@@ -190,6 +194,8 @@ int nps_bezier_opt_render(nps_bezier_opt* opt, const float* vp, uint32_t width, 
 int nps_bezier_opt_buffers(nps_bezier_opt* opt, float** beziers, int32_t** grads, float** adam_m, float** adam_v,
                            float** grad_accum, float** loss_accum, int32_t** pixel_loss);
 int nps_bezier_opt_stats(nps_bezier_opt* opt, nps_stats* out);
+/* Sets the manager's stepCount (GpuBezierOptimizerManager.ts:398). */
+int nps_bezier_opt_set_step_count(nps_bezier_opt* opt, uint32_t count);
 
 /* ====================================== 3D Gaussians (north-star trainer)
  * No counterpart in the reference, which fits linear-parameter generalised

@@ -55,6 +55,7 @@ SIGNATURES = {
     "nps_splat_opt_render": [P, P, U32, U32, P, P],
     "nps_splat_opt_buffers": [P, PP, PP, PP, PP, PP],
     "nps_splat_opt_stats": [P, ctypes.POINTER(nps_stats)],
+    "nps_splat_opt_set_step_count": [P, U32],
     "nps_splat_adc_noalloc": [P, P, P, P, U32, F32, P, P],
     "nps_bezier_opt_create": [P, U32, PP],
     "nps_bezier_opt_destroy": [P],
@@ -76,6 +77,7 @@ SIGNATURES = {
     "nps_bezier_opt_render": [P, P, U32, U32, P, P, U32, U32, P],
     "nps_bezier_opt_buffers": [P, PP, PP, PP, PP, PP, PP, PP],
     "nps_bezier_opt_stats": [P, ctypes.POINTER(nps_stats)],
+    "nps_bezier_opt_set_step_count": [P, U32],
     "nps_gs_create": [P, U32, U32, PP],
     "nps_gs_destroy": [P],
     "nps_gs_write_params": [P, P, U32, U32, I32],

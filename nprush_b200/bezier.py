@@ -164,6 +164,10 @@ class GpuBezierOptimizerManager:
         call("nps_bezier_opt_stats", self._h, ctypes.byref(st))
         return dict(pairs=st.pairs, adc_clones=st.adc_clones, spawns=st.reserved[0], step_count=st.step_count)
 
+    def set_step_count(self, count: int):
+        """stepCount (dispatch() calls so far; ADC every adc_period)."""
+        call("nps_bezier_opt_set_step_count", self._h, int(count))
+
     def close(self):
         if getattr(self, "_h", None):
             call("nps_bezier_opt_destroy", self._h)

@@ -1434,6 +1434,14 @@ int nps_bezier_opt_buffers(nps_bezier_opt* o, float** bzp, int32_t** grads, floa
   return NPS_OK;
 }
 
+// the manager's stepCount (GpuBezierOptimizerManager.ts:398): dispatch() calls so far, which decide
+// when ADC runs; restoring a checkpoint sets it back
+int nps_bezier_opt_set_step_count(nps_bezier_opt* o, uint32_t count) {
+  NPS_TRY(check_bz(o));
+  o->step_count = count;
+  return NPS_OK;
+}
+
 int nps_bezier_opt_stats(nps_bezier_opt* o, nps_stats* out) {
   NPS_TRY(check_bz(o));
   if (!out) return NPS_ERR_INVALID;

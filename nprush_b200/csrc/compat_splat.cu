@@ -1120,6 +1120,14 @@ int nps_splat_opt_buffers(nps_splat_opt* o, float** splats, int32_t** grads, flo
   return NPS_OK;
 }
 
+// the manager's stepCount (GpuSplatOptimizerManager.ts:380): dispatch() calls so far, which decide
+// when ADC runs; restoring a checkpoint sets it back
+int nps_splat_opt_set_step_count(nps_splat_opt* o, uint32_t count) {
+  NPS_TRY(check_opt(o));
+  o->step_count = count;
+  return NPS_OK;
+}
+
 int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
   NPS_TRY(check_opt(o));
   if (!out) return NPS_ERR_INVALID;

@@ -183,6 +183,10 @@ class GpuSplatOptimizerManager:
         call("nps_splat_opt_stats", self._h, ctypes.byref(st))
         return dict(pairs=st.pairs, adc_clones=st.adc_clones, step_count=st.step_count)
 
+    def set_step_count(self, count: int):
+        """stepCount (dispatch() calls so far; ADC every 25th)."""
+        call("nps_splat_opt_set_step_count", self._h, int(count))
+
     def sync(self):
         call("nps_sync", self._ctx)
 
