@@ -450,17 +450,32 @@ __global__ void __launch_bounds__(256) k_ssim_fwd2(const float4* __restrict__ im
   const int ox = blockIdx.x * kLT - kHalo, oy = blockIdx.y * kLT - kHalo;
   const float4* im = img + (size_t)v * W * H;
   const float4* tg = tgt + (size_t)tgt_ids[v] * W * H;
-  for (int e = tid; e < kLI * kLI; e += 256) {
-    const int ly = e / kLI, lx = e - ly * kLI;
-    const int gx = ox + lx, gy = oy + ly;
-    float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0);
-    if (gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H) {
-      a = im[(size_t)gy * W + gx];
-      b = tg[(size_t)gy * W + gx];
+  // staging in two halves, each issuing all its loads before its stores, so
+  // the load latency is paid twice rather than once per element
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    constexpr int kIt = (kLI * kLI + 511) / 512;  // 4 elements per thread per half
+    float4 a[kIt], b[kIt];
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+      const int e = tid + (half * kIt + i) * 256;
+      const int ly = e / kLI, lx = e - ly * kLI;
+      const int gx = ox + lx, gy = oy + ly;
+      a[i] = b[i] = make_float4(0, 0, 0, 0);
+      if (e < kLI * kLI && gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H) {
+        a[i] = im[(size_t)gy * W + gx];
+        b[i] = tg[(size_t)gy * W + gx];
+      }
     }
-    const int o = ly * kLS + lx;
-    sx[o] = a.x; sx[kLI * kLS + o] = a.y; sx[2 * kLI * kLS + o] = a.z;
-    sy[o] = b.x; sy[kLI * kLS + o] = b.y; sy[2 * kLI * kLS + o] = b.z;
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+      const int e = tid + (half * kIt + i) * 256;
+      if (e >= kLI * kLI) continue;
+      const int ly = e / kLI, lx = e - ly * kLI;
+      const int o = ly * kLS + lx;
+      sx[o] = a[i].x; sx[kLI * kLS + o] = a[i].y; sx[2 * kLI * kLS + o] = a[i].z;
+      sy[o] = b[i].x; sy[kLI * kLS + o] = b[i].y; sy[2 * kLI * kLS + o] = b[i].z;
+    }
   }
   __syncthreads();
   const int col = tid & 31, rg = tid >> 5;  // vertical pass: column, 4-row group
@@ -550,7 +565,7 @@ __global__ void __launch_bounds__(256) k_ssim_fwd2(const float4* __restrict__ im
   }
 }
 
-__global__ void __launch_bounds__(256) k_ssim_bwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
+__global__ void __launch_bounds__(256, 3) k_ssim_bwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
                                                    const uint32_t* __restrict__ tgt_ids,
                                                    const float* __restrict__ maps, uint32_t W, uint32_t H,
                                                    float lambda, float inv_norm, float4* __restrict__ dimg) {
@@ -562,30 +577,38 @@ __global__ void __launch_bounds__(256) k_ssim_bwd2(const float4* __restrict__ im
   const size_t plane = (size_t)W * H;
   const int col = tid & 31, rg = tid >> 5;
   const int px = blockIdx.x * kLT + col;
-  const float4* tg = tgt + (size_t)tgt_ids[v] * plane;
-  // this thread's four output pixels
-  float4 xs[4], ys[4];
-#pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const int py = blockIdx.y * kLT + rg * 4 + o;
-    const bool in = px < (int)W && py < (int)H;
-    const size_t pix = in ? (size_t)py * W + px : 0;
-    xs[o] = in ? img[(size_t)v * plane + pix] : make_float4(0, 0, 0, 0);
-    ys[o] = in ? tg[pix] : make_float4(0, 0, 0, 0);
-  }
+  // the image and target are read per channel where they are used (they
+  // come from L2), so no registers hold them across the kernel
+  const float* imf = reinterpret_cast<const float*>(img + (size_t)v * plane);
+  const float* tgf = reinterpret_cast<const float*>(tgt + (size_t)tgt_ids[v] * plane);
   const float l1w = (1.0f - lambda) * inv_norm;
   float d[4][3];
   for (int c = 0; c < 3; ++c) {
     const float* mv = maps + ((size_t)v * 9 + 3 * c) * plane;
-    for (int e = tid; e < kLI * kLI; e += 256) {
-      const int ly = e / kLI, lx = e - ly * kLI;
-      const int gx = ox + lx, gy = oy + ly;
-      const bool ok = gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H;
-      const size_t g = ok ? (size_t)gy * W + gx : 0;
-      const int o = ly * kLS + lx;
-      mp[o] = ok ? mv[g] : 0.0f;
-      mp[kLI * kLS + o] = ok ? mv[plane + g] : 0.0f;
-      mp[2 * kLI * kLS + o] = ok ? mv[2 * plane + g] : 0.0f;
+    {  // stage the channel's three maps: every load issued before the stores
+      constexpr int kIt = (kLI * kLI + 255) / 256;  // 7 elements per thread
+      float m0[kIt], m1[kIt], m2[kIt];
+#pragma unroll
+      for (int i = 0; i < kIt; ++i) {
+        const int e = tid + i * 256;
+        const int ly = e / kLI, lx = e - ly * kLI;
+        const int gx = ox + lx, gy = oy + ly;
+        const bool ok = e < kLI * kLI && gx >= 0 && gy >= 0 && gx < (int)W && gy < (int)H;
+        const size_t g = ok ? (size_t)gy * W + gx : 0;
+        m0[i] = ok ? mv[g] : 0.0f;
+        m1[i] = ok ? mv[plane + g] : 0.0f;
+        m2[i] = ok ? mv[2 * plane + g] : 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < kIt; ++i) {
+        const int e = tid + i * 256;
+        if (e >= kLI * kLI) continue;
+        const int ly = e / kLI, lx = e - ly * kLI;
+        const int o = ly * kLS + lx;
+        mp[o] = m0[i];
+        mp[kLI * kLS + o] = m1[i];
+        mp[2 * kLI * kLS + o] = m2[i];
+      }
     }
     __syncthreads();
     for (int r = tid; r < 3 * kLI * (kLT / 4); r += 256) {
@@ -619,8 +642,11 @@ __global__ void __launch_bounds__(256) k_ssim_bwd2(const float4* __restrict__ im
     }
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
-      const float x = c == 0 ? xs[o].x : c == 1 ? xs[o].y : xs[o].z;
-      const float y = c == 0 ? ys[o].x : c == 1 ? ys[o].y : ys[o].z;
+      const int py = blockIdx.y * kLT + rg * 4 + o;
+      const bool in = px < (int)W && py < (int)H;
+      const size_t pix = in ? (size_t)py * W + px : 0;
+      const float x = in ? __ldg(imf + 4 * pix + c) : 0.0f;
+      const float y = in ? __ldg(tgf + 4 * pix + c) : 0.0f;
       const float diff = x - y;
       const float sgn = diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f);
       d[o][c] = cv[o][0] + 2.0f * x * cv[o][1] + y * cv[o][2] + l1w * sgn;
