@@ -12,8 +12,9 @@
 //   k_mesh_setup    one thread per triangle: clip against 0 <= z <= w and a
 //                   guard band |x|, |y| <= 64 w (Sutherland-Hodgman, fan of
 //                   <= 7 sub-triangles), project, snap to 1/256 pixel, cull
-//                   back faces, count 1024-pixel chunks of each sub-triangle's
-//                   pixel box
+//                   back faces; rasterise small unclipped triangles (box of
+//                   <= 32 pixels) itself, count 1024-pixel chunks of the
+//                   other sub-triangles' pixel boxes
 //   exclusive scan  chunk offsets
 //   k_mesh_raster   one warp per chunk (32 pixels per lane): exact 64-bit
 //                   edge functions at pixel centres (watertight, top-left
@@ -229,8 +230,20 @@ __device__ __forceinline__ bool cover(const Sub& s, int px, int py, float l[3], 
   return in;
 }
 
+// depth test of one covered sample: "less" in draw order
+__device__ __forceinline__ void depth_min(unsigned long long* zbuf, int W, int px, int py, float z, uint32_t sub) {
+  const unsigned long long key = ((unsigned long long)__float_as_uint(z) << 32) | sub;
+  atomicMin(zbuf + (size_t)py * W + px, key);
+}
+
+// Counts the 1024-pixel chunks of each sub-triangle for k_mesh_raster.  An
+// unclipped triangle whose pixel box holds at most kSmallBox pixels (most
+// triangles of a detailed mesh) is rasterised here by its own thread and
+// gets no chunks: a warp task would spend more on finding and setting up the
+// triangle than on its few pixels.
+constexpr uint32_t kSmallBox = 32;
 __global__ void k_mesh_setup(const float4* __restrict__ vout, const uint32_t* __restrict__ idx, uint32_t n_tris,
-                             int W, int H, uint32_t* __restrict__ chunks) {
+                             int W, int H, uint32_t* __restrict__ chunks, unsigned long long* __restrict__ zbuf) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_tris) return;
   CV poly[kMaxPoly];
@@ -239,8 +252,17 @@ __global__ void k_mesh_setup(const float4* __restrict__ vout, const uint32_t* __
     Sub s;
     uint32_t c = 0;
     if (setup_sub(poly, n, k, W, H, s)) {
-      const uint32_t pixels = (uint32_t)(s.bx1 - s.bx0 + 1) * (uint32_t)(s.by1 - s.by0 + 1);
-      c = (pixels + kChunk - 1) / kChunk;
+      const uint32_t bw = (uint32_t)(s.bx1 - s.bx0 + 1), pixels = bw * (uint32_t)(s.by1 - s.by0 + 1);
+      if (n == 3 && pixels <= kSmallBox) {
+        const uint32_t sub = (uint32_t)kMaxSubs * t + k;
+        for (uint32_t p = 0; p < pixels; ++p) {
+          const int px = s.bx0 + (int)(p % bw), py = s.by0 + (int)(p / bw);
+          float l[3], z;
+          if (cover(s, px, py, l, z) && z < 1.0f) depth_min(zbuf, W, px, py, z, sub);
+        }
+      } else {
+        c = (pixels + kChunk - 1) / kChunk;
+      }
     }
     chunks[(size_t)kMaxSubs * t + k] = c;
   }
@@ -279,10 +301,7 @@ __global__ void __launch_bounds__(kRasterThreads) k_mesh_raster(const float4* __
       if (p >= count) break;
       const int px = s.bx0 + (int)(p % bw), py = s.by0 + (int)(p / bw);
       float l[3], z;
-      if (cover(s, px, py, l, z) && z < 1.0f) {
-        const unsigned long long key = ((unsigned long long)__float_as_uint(z) << 32) | sub;
-        atomicMin(zbuf + (size_t)py * W + px, key);
-      }
+      if (cover(s, px, py, l, z) && z < 1.0f) depth_min(zbuf, W, px, py, z, sub);
     }
   }
 }
@@ -487,7 +506,8 @@ int nps_mesh_render(nps_mesh* o, const float* uniforms52, float* color_rgba, flo
   if (o->n_tris) {
     const uint32_t n_subs = mr::kMaxSubs * o->n_tris;
     mr::k_mesh_setup<<<div_up(o->n_tris, 128), 128, 0, s>>>(vout, o->idx.as<uint32_t>(), o->n_tris, (int)w, (int)h,
-                                                            o->chunks.as<uint32_t>());
+                                                            o->chunks.as<uint32_t>(),
+                                                            o->zbuf.as<unsigned long long>());
     NPS_CHECK_LAUNCH();
     NPS_TRY(exclusive_scan_u32(o->chunks.as<uint32_t>(), o->offsets.as<uint32_t>(), n_subs, o->total.as<uint32_t>(),
                                o->work, s));
