@@ -464,7 +464,7 @@ __device__ __forceinline__ float3 trace_pixel(const Scene& sc, const Camera& cam
   return radiance;
 }
 
-__global__ void __launch_bounds__(128) k_path_trace(Scene sc, Camera cam, float4* __restrict__ accum, uint32_t w,
+__global__ void __launch_bounds__(128, 10) k_path_trace(Scene sc, Camera cam, float4* __restrict__ accum, uint32_t w,
                                                     uint32_t h, uint32_t frame0, uint32_t frames,
                                                     uint32_t* overflow) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
