@@ -17,9 +17,9 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kItems = 16;
-constexpr int kTile = kSortThreads * kItems;  // 4096 keys
-constexpr int kSortGrid = 2 * kNumSMs;
+constexpr int kItems = 12;
+constexpr int kTile = kSortThreads * kItems;  // 3072 keys
+constexpr int kSortGrid = 4 * kNumSMs;  // four resident blocks per SM (64 registers)
 
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
