@@ -75,8 +75,12 @@ def test_bezier_run_resumes_from_scene(lib, tmp_path):
     for _ in range(5):  # through the ADC at dispatch 10
         a.dispatch()
         b.dispatch()
-    _same(a.read_state(), b.read_state(),
-          ("beziers", "adam_m", "adam_v", "grad_accum", "loss_accum", "grads", "pixel_loss"))
+    sa, sb = a.read_state(), b.read_state()
+    _same(sa, sb, ("beziers", "adam_m", "adam_v", "grad_accum", "grads", "pixel_loss"))
+    # loss_accum is a float sum of per-tile contributions added with atomics (the reference
+    # adds them without, bezier_backward.wgsl:562): its last bit depends on the order in
+    # which the tiles arrive, run to run
+    np.testing.assert_allclose(sa["loss_accum"], sb["loss_accum"], rtol=1e-6, atol=0)
 
 
 def test_gaussian_run_resumes_from_scene(lib, tmp_path):
