@@ -437,6 +437,13 @@ int nps_mesh_destroy(nps_mesh* mesh);
  * float4, host or device pointer; both start as one white texel. */
 int nps_mesh_set_matcap(nps_mesh* mesh, const float* rgba, uint32_t w, uint32_t h);
 int nps_mesh_set_env(nps_mesh* mesh, const float* rgba, uint32_t w, uint32_t h);
+/* setPbrMesh (GpuMeshRenderPipelineManager.ts:161-248): triangles from
+ * first_tri on (the PBR mesh, drawn last) use mesh.wgsl's vert_pbr / frag_pbr
+ * (:72-121): albedo and tangent-space normal map (w x h float4, host
+ * pointers), sampled linearly with repeat; srgb != 0 decodes the albedo
+ * texels from sRGB first, as the reference's sRGB texture view does. */
+int nps_mesh_set_pbr(nps_mesh* mesh, uint32_t first_tri, const float* albedo_rgba, uint32_t aw, uint32_t ah, int srgb,
+                     const float* normal_rgba, uint32_t nw, uint32_t nh);
 /* One mesh render pass as the viewer's optimisation pass draws it
  * (GpuRunner.svelte.ts:611-634): the environment background (draw_env = 0:
  * the clear colour 0.05), then the mesh through mesh.wgsl's vert / frag with

@@ -133,6 +133,7 @@ SIGNATURES = {
     "nps_mesh_destroy": [P],
     "nps_mesh_set_matcap": [P, P, U32, U32],
     "nps_mesh_set_env": [P, P, U32, U32],
+    "nps_mesh_set_pbr": [P, U32, P, U32, U32, I32, P, U32, U32],
     "nps_mesh_render": [P, P, P, P, U32, U32, I32, I32],
     "nps_mlp_num_params": [],
     "nps_mlp_create": [P, PP],

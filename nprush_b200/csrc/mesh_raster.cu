@@ -31,6 +31,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "context.h"
@@ -306,10 +307,38 @@ __global__ void __launch_bounds__(kRasterThreads) k_mesh_raster(const float4* __
   }
 }
 
+__device__ __forceinline__ float3 cross3(const float3& a, const float3& b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// mesh.wgsl:87-121, the PBR stage of the ground (setPbrMesh): albedo and a
+// tangent-space normal map sampled linearly with repeat, a TBN frame from the
+// interpolated normal, the matcap lit by the perturbed view-space normal
+__device__ __forceinline__ float3 frag_pbr(const Uniforms& u, const Tex& matcap, const Tex& albedo, const Tex& nmap,
+                                           const float4& nrm, const float4& uv) {
+  const float3 alb = sample(albedo, uv.x, uv.y, true, true);
+  const float3 t3 = sample(nmap, uv.x, uv.y, true, true);
+  const float tsx = t3.x * 2.0f - 1.0f, tsy = t3.y * 2.0f - 1.0f, tsz = t3.z * 2.0f - 1.0f;
+  const float3 N = normalize3(nrm.x, nrm.y, nrm.z);
+  float3 up = make_float3(0.0f, 0.0f, 1.0f);
+  if (fabsf(N.x * up.x + N.y * up.y + N.z * up.z) > 0.99f) up = make_float3(1.0f, 0.0f, 0.0f);
+  const float3 tc = cross3(up, N);
+  const float3 T = normalize3(tc.x, tc.y, tc.z);
+  const float3 B = cross3(N, T);
+  const float3 wn = normalize3(T.x * tsx + B.x * tsy + N.x * tsz, T.y * tsx + B.y * tsy + N.y * tsz,
+                               T.z * tsx + B.z * tsy + N.z * tsz);
+  const float3 vn = normalize3(mrow(u.view, 0, wn.x, wn.y, wn.z, 0.0f), mrow(u.view, 1, wn.x, wn.y, wn.z, 0.0f),
+                               mrow(u.view, 2, wn.x, wn.y, wn.z, 0.0f));
+  if (u.shading_mode < 0.5f) return make_float3((wn.x + 1.0f) * 0.5f, (wn.y + 1.0f) * 0.5f, (wn.z + 1.0f) * 0.5f);
+  const float mx = vn.x * 0.5f + 0.5f, my = vn.y * 0.5f + 0.5f;
+  const float3 mc = sample(matcap, mx, 1.0f - my, false, false);
+  return make_float3(mc.x * alb.x, mc.y * alb.y, mc.z * alb.z);
+}
+
 __global__ void k_mesh_shade(const float4* __restrict__ vout, const uint32_t* __restrict__ idx,
                              const unsigned long long* __restrict__ zbuf, int W, int H, Uniforms u, Tex matcap,
-                             Tex env, int draw_env, int quantize, float4* __restrict__ color,
-                             float4* __restrict__ depth) {
+                             Tex env, Tex albedo, Tex nmap, uint32_t first_pbr, int draw_env, int quantize,
+                             float4* __restrict__ color, float4* __restrict__ depth) {
   const int x = blockIdx.x * 16 + threadIdx.x, y = blockIdx.y * 16 + threadIdx.y;
   if (x >= W || y >= H) return;
   const size_t pix = (size_t)y * W + x;
@@ -355,13 +384,14 @@ __global__ void k_mesh_shade(const float4* __restrict__ vout, const uint32_t* __
                          wt[0] * a.z + wt[1] * b.z + wt[2] * c.z, wt[0] * a.w + wt[1] * b.w + wt[2] * c.w);
     };
     const float4 nrm_vd = lerp4(1), vnrm = lerp4(2), vcol = lerp4(3);
-    // mesh.wgsl:52-70
-    const float3 nn = normalize3(nrm_vd.x, nrm_vd.y, nrm_vd.z);
-    const float3 vn = normalize3(vnrm.x, vnrm.y, vnrm.z);
     float3 fin;
-    if (u.shading_mode < 0.5f) {
+    if (t >= first_pbr) {
+      fin = frag_pbr(u, matcap, albedo, nmap, nrm_vd, lerp4(4));
+    } else if (u.shading_mode < 0.5f) {  // mesh.wgsl:52-70
+      const float3 nn = normalize3(nrm_vd.x, nrm_vd.y, nrm_vd.z);
       fin = make_float3((nn.x + 1.0f) * 0.5f, (nn.y + 1.0f) * 0.5f, (nn.z + 1.0f) * 0.5f);
     } else {
+      const float3 vn = normalize3(vnrm.x, vnrm.y, vnrm.z);
       const float uvx = vn.x * 0.5f + 0.5f, uvy = vn.y * 0.5f + 0.5f;
       const float3 mc = sample(matcap, uvx, 1.0f - uvy, false, false);
       fin = make_float3(mc.x * vcol.x, mc.y * vcol.y, mc.z * vcol.z);
@@ -385,12 +415,13 @@ using namespace nps;
 struct nps_mesh {
   nps_ctx* ctx = nullptr;
   uint32_t n_verts = 0, n_tris = 0;
-  DevBuf verts, idx, vout, chunks, offsets, total, zbuf, matcap, env;
+  DevBuf verts, idx, vout, chunks, offsets, total, zbuf, matcap, env, albedo, nmap;
   SortWork work;
-  int matcap_w = 1, matcap_h = 1, env_w = 1, env_h = 1;
+  int matcap_w = 1, matcap_h = 1, env_w = 1, env_h = 1, albedo_w = 1, albedo_h = 1, nmap_w = 1, nmap_h = 1;
+  uint32_t first_pbr = 0xffffffffu;  // triangles from here on use the PBR stage
   ~nps_mesh() {
-    for (DevBuf* b : {&verts, &idx, &vout, &chunks, &offsets, &total, &zbuf, &matcap, &env, &work.hist, &work.partial,
-                      &work.keys_alt, &work.vals_alt})
+    for (DevBuf* b : {&verts, &idx, &vout, &chunks, &offsets, &total, &zbuf, &matcap, &env, &albedo, &nmap, &work.hist,
+                      &work.partial, &work.keys_alt, &work.vals_alt})
       b->release();
   }
 };
@@ -437,6 +468,7 @@ int nps_mesh_create(nps_ctx* ctx, const float* vertices, uint32_t n_vertices, co
   const float white[4] = {1.0f, 1.0f, 1.0f, 1.0f};
   int rc = NPS_OK;
   if ((rc = o->verts.ensure((size_t)n_vertices * 48 + 16)) || (rc = o->idx.ensure((size_t)n_tris * 12 + 16)) ||
+      (rc = o->albedo.ensure(16)) || (rc = o->nmap.ensure(16)) ||
       (rc = o->vout.ensure((size_t)n_vertices * 80 + 16)) ||
       (rc = o->chunks.ensure((size_t)n_tris * 4 * mr::kMaxSubs + 16)) ||
       (rc = o->offsets.ensure((size_t)n_tris * 4 * mr::kMaxSubs + 16)) || (rc = o->total.ensure(16)) ||
@@ -451,6 +483,8 @@ int nps_mesh_create(nps_ctx* ctx, const float* vertices, uint32_t n_vertices, co
     e = cudaMemcpyAsync(o->idx.p, indices, (size_t)n_tris * 12, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(o->matcap.p, white, 16, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(o->env.p, white, 16, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(o->albedo.p, white, 16, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(o->nmap.p, white, 16, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     set_error("nps_mesh_create: upload failed: %s", cudaGetErrorString(e));
@@ -483,6 +517,30 @@ int nps_mesh_set_env(nps_mesh* o, const float* rgba, uint32_t w, uint32_t h) {
     return NPS_ERR_INVALID;
   }
   return upload_tex(o, o->env, rgba, w, h, o->env_w, o->env_h);
+}
+
+int nps_mesh_set_pbr(nps_mesh* o, uint32_t first_tri, const float* albedo_rgba, uint32_t aw, uint32_t ah, int srgb,
+                     const float* normal_rgba, uint32_t nw, uint32_t nh) {
+  if (!o || !albedo_rgba || !normal_rgba || aw == 0 || ah == 0 || nw == 0 || nh == 0 || aw > 65536 || ah > 65536 ||
+      nw > 65536 || nh > 65536) {
+    set_error("nps_mesh_set_pbr: bad arguments");
+    return NPS_ERR_INVALID;
+  }
+  const float* alb = albedo_rgba;
+  std::vector<float> lin;
+  if (srgb) {  // an sRGB texture view: each texel decoded to linear before filtering
+    lin.assign(albedo_rgba, albedo_rgba + (size_t)aw * ah * 4);
+    for (size_t i = 0; i < lin.size(); ++i) {
+      if (i % 4 == 3) continue;  // alpha is not encoded
+      const float c = lin[i];
+      lin[i] = c > 0.04045f ? std::pow((c + 0.055f) / 1.055f, 2.4f) : c / 12.92f;
+    }
+    alb = lin.data();
+  }
+  NPS_TRY(upload_tex(o, o->albedo, alb, aw, ah, o->albedo_w, o->albedo_h));
+  NPS_TRY(upload_tex(o, o->nmap, normal_rgba, nw, nh, o->nmap_w, o->nmap_h));
+  o->first_pbr = first_tri;
+  return NPS_OK;
 }
 
 int nps_mesh_render(nps_mesh* o, const float* uniforms52, float* color_rgba, float* depth_rgba, uint32_t w,
@@ -518,10 +576,11 @@ int nps_mesh_render(nps_mesh* o, const float* uniforms52, float* color_rgba, flo
     NPS_CHECK_LAUNCH();
   }
   const mr::Tex mt{o->matcap.as<float4>(), o->matcap_w, o->matcap_h}, et{o->env.as<float4>(), o->env_w, o->env_h};
+  const mr::Tex at{o->albedo.as<float4>(), o->albedo_w, o->albedo_h}, nt{o->nmap.as<float4>(), o->nmap_w, o->nmap_h};
   const dim3 grid(div_up(w, 16), div_up(h, 16));
   mr::k_mesh_shade<<<grid, dim3(16, 16), 0, s>>>(vout, o->idx.as<uint32_t>(), o->zbuf.as<unsigned long long>(),
-                                                 (int)w, (int)h, u, mt, et, draw_env, quantize, (float4*)color_rgba,
-                                                 (float4*)depth_rgba);
+                                                 (int)w, (int)h, u, mt, et, at, nt, o->first_pbr, draw_env, quantize,
+                                                 (float4*)color_rgba, (float4*)depth_rgba);
   NPS_CHECK_LAUNCH();
   return NPS_OK;
 }

@@ -6,6 +6,7 @@ them (GpuRunner.svelte.ts:611-634).
 
     r = MeshRenderer(mesh, matcap=..., env=...)    # constructor({mesh}), matcap / env textures
     r.set_ground_mesh(ground)                       # setGroundMesh: drawn after the mesh
+    r.set_pbr_mesh(mesh, albedo, normal_map)        # setPbrMesh: drawn last with the PBR stage
     r.write_view_proj_mat(vp); r.write_view_mat(v); r.write_inv_view_proj_mat(vpi)
     r.write_shading_mode("normals" | "shaded")
     color, depth = r.render(w, h)                   # envmap draw + addDraw into colour / depth targets
@@ -30,14 +31,18 @@ class MeshRenderer:
         self.device = device
         self.ctx = _lib.context(device)
         self._h = ctypes.c_void_p()
-        self.mesh, self.ground = mesh, None
+        self.mesh, self.ground, self.pbr = mesh, None, None
         self.matcap = None if matcap is None else np.ascontiguousarray(matcap, np.float32)
         self.env = None if env is None else np.ascontiguousarray(env, np.float32)
         self.uniforms = np.zeros(52, np.float32)  # GpuUniformsBufferManager: 208 bytes
         self._rebuild()
 
     def _rebuild(self):
-        m = concat([self.mesh] + ([self.ground] if self.ground is not None else []))
+        parts = [self.mesh] + ([self.ground] if self.ground is not None else [])
+        first_pbr = sum(p.n_tris for p in parts)
+        if self.pbr is not None:
+            parts.append(self.pbr[0])
+        m = concat(parts)
         v = np.ascontiguousarray(m.vertices, np.float32)
         idx = np.ascontiguousarray(m.indices, np.uint32)
         self._destroy()
@@ -47,9 +52,21 @@ class MeshRenderer:
             self.set_matcap(self.matcap)
         if self.env is not None:
             self.set_env(self.env)
+        if self.pbr is not None:
+            _, alb, nm, srgb = self.pbr
+            call("nps_mesh_set_pbr", self._h, first_pbr, alb.ctypes.data, alb.shape[1], alb.shape[0], int(bool(srgb)),
+                 nm.ctypes.data, nm.shape[1], nm.shape[0])
 
     def set_ground_mesh(self, mesh: MeshData):
         self.ground = mesh
+        self._rebuild()
+
+    def set_pbr_mesh(self, mesh: MeshData, albedo, normal_map, srgb: bool = True):
+        """The PBR-shaded mesh (the reference's textured ground), drawn last:
+        albedo (sRGB-encoded unless srgb=False) and tangent-space normal map,
+        (h, w, 4) float arrays."""
+        self.pbr = (mesh, np.ascontiguousarray(albedo, np.float32), np.ascontiguousarray(normal_map, np.float32),
+                    bool(srgb))
         self._rebuild()
 
     def set_matcap(self, rgba):

@@ -114,6 +114,35 @@ def frag(vo, uni, matcap):
     return col, np.array([d, d, d, 1.0], np.float32)
 
 
+def cross(a, b):
+    return np.array([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]], np.float32)
+
+
+def frag_pbr(vo, uni, matcap, albedo_tex, normal_tex):
+    """mesh.wgsl:87-121 (the ground's PBR stage): albedo and tangent-space
+    normal map (linear, repeating), TBN from the interpolated normal, matcap
+    lit by the perturbed view-space normal."""
+    uv = vo[15:17]
+    albedo = sample(albedo_tex, uv[0], uv[1], True, True)[:3]
+    ts = (sample(normal_tex, uv[0], uv[1], True, True)[:3] * F(2.0) - F(1.0)).astype(np.float32)
+    N = normalize(vo[4:7])
+    up = np.array([0.0, 0.0, 1.0], np.float32)
+    if abs(N[0] * up[0] + N[1] * up[1] + N[2] * up[2]) > F(0.99):
+        up = np.array([1.0, 0.0, 0.0], np.float32)
+    T = normalize(cross(up, N))
+    B = cross(N, T)
+    wn = normalize((T * ts[0] + B * ts[1] + N * ts[2]).astype(np.float32))
+    vn = normalize(mat_vec(uni[16:32], (wn[0], wn[1], wn[2], 0.0))[:3])
+    mx, my = vn[0] * F(0.5) + F(0.5), vn[1] * F(0.5) + F(0.5)
+    mc = sample(matcap, mx, F(1.0) - my, False, False)[:3]
+    lit = (mc * albedo).astype(np.float32)
+    nc = ((wn + F(1.0)) * F(0.5)).astype(np.float32)
+    final = nc if uni[32] < F(0.5) else lit
+    col = np.concatenate([reinhard(final * F(4.0)), [1.0]]).astype(np.float32)
+    d = vo[7]
+    return col, np.array([d, d, d, 1.0], np.float32)
+
+
 def env_frag(ndc, uni, env):
     """envmap.wgsl:36-52."""
     inv = uni[36:52]
@@ -131,16 +160,21 @@ def env_frag(ndc, uni, env):
 
 
 class RestatedStages:
-    """The stage functions above, with the textures they sample."""
+    """The stage functions above, with the textures they sample (albedo and
+    normal map for the PBR stage)."""
 
-    def __init__(self, matcap, env):
+    def __init__(self, matcap, env, albedo=None, normal_map=None):
         self.matcap = np.ascontiguousarray(matcap, np.float32)
         self.env = np.ascontiguousarray(env, np.float32)
+        self.albedo = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+        self.normal_map = None if normal_map is None else np.ascontiguousarray(normal_map, np.float32)
 
     def vert(self, vin, uni):
-        return vert(vin, uni)
+        return vert(vin, uni)  # vert_pbr is the same function
 
-    def frag(self, vo, uni):
+    def frag(self, vo, uni, pbr=False):
+        if pbr:
+            return frag_pbr(vo, uni, self.matcap, self.albedo, self.normal_map)
         return frag(vo, uni, self.matcap)
 
     def env_frag(self, ndc, uni):
@@ -243,9 +277,10 @@ def coverage(st, px, py):
     return ins, (l0, l1, l2), z
 
 
-def render(vertices, indices, uni, w, h, stages, draw_env=True):
+def render(vertices, indices, uni, w, h, stages, draw_env=True, first_pbr=None):
     """The pass: (colour, depth) float32 (h, w, 4) images (the stored floats,
-    before an 8-bit target rounds them)."""
+    before an 8-bit target rounds them).  Triangles from first_pbr on are
+    drawn with the PBR stage (the reference draws its PBR mesh last)."""
     uni = np.asarray(uni, np.float32)
     v = np.asarray(vertices, np.float32).reshape(-1, 12)
     idx = np.asarray(indices, np.uint32).reshape(-1, 3)
@@ -289,7 +324,8 @@ def render(vertices, indices, uni, w, h, stages, draw_env=True):
             vo = vout[idx[t]]
             interp = (wts[0] * vo[0] + wts[1] * vo[1] + wts[2] * vo[2]).astype(np.float32)
             interp[0:4] = (F(x) + F(0.5), F(y) + F(0.5), z[0], F(0.0))  # builtin position (unused)
-            col, dep = stages.frag(interp, uni)
+            pbr = first_pbr is not None and t >= first_pbr
+            col, dep = stages.frag(interp, uni, pbr) if pbr else stages.frag(interp, uni)
             color[y, x], depth[y, x] = col, dep
     return color, depth
 

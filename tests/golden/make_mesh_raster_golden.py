@@ -35,7 +35,7 @@ EYE, TARGET = (3.2, -2.6, 1.9), (0.0, 0.0, 0.4)
 class ReferenceStages:
     """mesh.wgsl vert / frag and envmap.wgsl frag, the reference's own code."""
 
-    def __init__(self, uni, matcap, env):
+    def __init__(self, uni, matcap, env, albedo=None, normal_map=None):
         self.mesh = RefModule("mesh", 0)
         self.envm = RefModule("envmap", 0)
         self.uni = np.ascontiguousarray(uni, np.float32)
@@ -43,14 +43,18 @@ class ReferenceStages:
             m.bind(0, self.uni)
         self.mesh.bind_tex(1, np.ascontiguousarray(matcap, np.float32))
         self.mesh.bind_sampler(2, True, "clamp-to-edge", "clamp-to-edge")
+        if albedo is not None:  # the PBR stage's textures (GpuMeshRenderPipelineManager.ts:226-246)
+            self.mesh.bind_tex(3, np.ascontiguousarray(albedo, np.float32))
+            self.mesh.bind_tex(4, np.ascontiguousarray(normal_map, np.float32))
+            self.mesh.bind_sampler(5, True, "repeat", "repeat")
         self.envm.bind_tex(1, np.ascontiguousarray(env, np.float32))
         self.envm.bind_sampler(2, True, "repeat", "clamp-to-edge")
 
     def vert(self, vin, uni):
         return self.mesh.call("vert", np.asarray(vin, np.float32))
 
-    def frag(self, vo, uni):
-        r = self.mesh.call("frag", np.asarray(vo, np.float32))
+    def frag(self, vo, uni, pbr=False):
+        r = self.mesh.call("frag_pbr" if pbr else "frag", np.asarray(vo, np.float32))
         return r[0:4], r[4:8]
 
     def env_frag(self, ndc, uni):
@@ -79,6 +83,27 @@ def scene():
     sc = meshes.demo_scene(6, seed=3, mirror_fraction=0.0, sphere_detail=8)
     slab = meshes.quad((0.0, 0.0, -0.01), 400.0, (0.3, 0.35, 0.3, 1.0))
     return meshes.concat([sc, wall(), slab])
+
+
+def pbr_ground():
+    """A ground quad drawn with the PBR stage, its uv repeating the maps 3 x 3."""
+    q = meshes.quad((0.0, 0.0, -0.005), 12.0, (1.0, 1.0, 1.0, 1.0))
+    q.vertices[:, 10:12] *= 3.0
+    return q
+
+
+def pbr_textures(n=24):
+    """Linear albedo (checker + tint) and a tangent-space normal map of bumps."""
+    yy, xx = np.mgrid[0:n, 0:n]
+    u, v = (xx + 0.5) / n, (yy + 0.5) / n
+    alb = np.zeros((n, n, 4), np.float32)
+    chk = ((xx // 6 + yy // 6) % 2).astype(np.float32)
+    alb[..., 0], alb[..., 1], alb[..., 2], alb[..., 3] = 0.3 + 0.4 * chk, 0.35 + 0.2 * u, 0.25 + 0.3 * v, 1.0
+    nx, ny = 0.4 * np.sin(2 * np.pi * 2 * u), 0.4 * np.cos(2 * np.pi * 3 * v)
+    nz = np.sqrt(1 - nx * nx - ny * ny)
+    nm = np.zeros((n, n, 4), np.float32)
+    nm[..., 0], nm[..., 1], nm[..., 2], nm[..., 3] = nx * 0.5 + 0.5, ny * 0.5 + 0.5, nz * 0.5 + 0.5, 1.0
+    return alb, nm
 
 
 def matcap_image(n=32):
@@ -111,6 +136,17 @@ def main():
         out[f"uniforms_{name}"] = uni
         out[f"color_{name}"] = col
         out[f"depth_{name}"] = dep
+    # the same scene with a PBR-shaded ground drawn last (setPbrMesh)
+    pbr = meshes.concat([sc, pbr_ground()])
+    alb, nm = pbr_textures()
+    out.update(pbr_vertices=pbr.vertices, pbr_indices=pbr.indices, pbr_first=np.uint32(sc.n_tris), albedo=alb,
+               normal_map=nm)
+    for name, mode in (("normals", 0.0), ("shaded", 1.0)):
+        uni = uniforms(mode)
+        col, dep = mr.render(pbr.vertices, pbr.indices, uni, W, H, ReferenceStages(uni, matcap, env, alb, nm),
+                             first_pbr=sc.n_tris)
+        out[f"pbr_color_{name}"] = col
+        out[f"pbr_depth_{name}"] = dep
     np.savez_compressed(HERE / "mesh_raster.npz", **out)
 
 

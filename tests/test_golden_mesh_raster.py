@@ -28,6 +28,19 @@ def test_restatement_matches_fixture(gold, mode):
     np.testing.assert_array_equal(d, gold[f"depth_{mode}"])
 
 
+@pytest.mark.parametrize("mode", ["normals", "shaded"])
+def test_restatement_matches_fixture_pbr(gold, mode):
+    """The scene with a ground drawn last through the PBR stage (albedo and
+    normal map repeating 3 x 3); the fixture ran the reference's frag_pbr."""
+    h, w = gold[f"pbr_color_{mode}"].shape[:2]
+    st = mr.RestatedStages(gold["matcap"], gold["env"], gold["albedo"], gold["normal_map"])
+    c, d = mr.render(gold["pbr_vertices"], gold["pbr_indices"], gold[f"uniforms_{mode}"], w, h, st,
+                     first_pbr=int(gold["pbr_first"]))
+    np.testing.assert_array_equal(c, gold[f"pbr_color_{mode}"])
+    np.testing.assert_array_equal(d, gold[f"pbr_depth_{mode}"])
+    assert np.abs(c - gold[f"color_{mode}"]).max() > 0.05  # the textured ground shows
+
+
 def test_fixture_sanity(gold):
     d = gold["depth_normals"][..., 0]
     assert 0.5 < (d < 1).mean() < 0.98      # geometry and sky both present

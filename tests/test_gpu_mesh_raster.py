@@ -66,6 +66,31 @@ def test_matches_reference_fixture(mrmod, gold, mode):
         assert np.all((np.abs(got - wq) < 1e-6) | (np.abs(frac - 0.5) < 1e-3))
 
 
+@pytest.mark.parametrize("mode", ["normals", "shaded"])
+def test_pbr_ground_matches_reference_fixture(mrmod, gold, mode):
+    from nprush_b200.meshes import MeshData
+    h, w = gold[f"pbr_color_{mode}"].shape[:2]
+    first = int(gold["pbr_first"])
+    v, idx = gold["pbr_vertices"], gold["pbr_indices"]
+    # the scene split as the manager holds it: mesh, then the PBR mesh (linear albedo)
+    r = mrmod.MeshRenderer(MeshData(v[:v.shape[0] - 4], idx[:3 * first]), matcap=gold["matcap"], env=gold["env"])
+    r.set_pbr_mesh(MeshData(v[v.shape[0] - 4:], idx[3 * first:] - np.uint32(v.shape[0] - 4)), gold["albedo"],
+                   gold["normal_map"], srgb=False)
+    r.uniforms[:] = gold[f"uniforms_{mode}"]
+    c, d = (t.cpu().numpy() for t in r.render(w, h, quantize=False))
+    check(c, d, gold[f"pbr_color_{mode}"], gold[f"pbr_depth_{mode}"])
+    # an sRGB-encoded albedo gives the linear one's image (decoded per texel)
+    enc = gold["albedo"].copy()
+    lin = enc[..., :3].astype(np.float64)
+    enc[..., :3] = np.where(lin > 0.0031308, 1.055 * lin ** (1 / 2.4) - 0.055, lin * 12.92)
+    r.set_pbr_mesh(r.pbr[0], enc, gold["normal_map"], srgb=True)
+    r.uniforms[:] = gold[f"uniforms_{mode}"]
+    c2, d2 = (t.cpu().numpy() for t in r.render(w, h, quantize=False))
+    np.testing.assert_array_equal(d2, d)
+    np.testing.assert_allclose(c2, c, atol=1e-5, rtol=0)
+    r.close()
+
+
 def _scene_uniforms(w, h, eye=(4.0, -3.5, 2.6), target=(0.0, 0.0, 0.3), mode=0.0):
     from nprush_b200 import camera
     vp, inv = camera.view_proj(eye, target, 0.9, w / h, up=(0.0, 0.0, 1.0))
