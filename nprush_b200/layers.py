@@ -20,6 +20,43 @@ from __future__ import annotations
 import numpy as np
 
 
+def mesh_targets(mesh, eye, center, width, height, fovy, up=(0.0, 0.0, 1.0), env=None, matcap=None,
+                 path_trace_frames=0, shading_mode="normals"):
+    """A frame's targets rendered from a mesh as the reference's viewer makes
+    them (GpuRunner.svelte.ts:611-641): the mesh pass gives the colour target
+    (normals or matcap shading) and the reciprocal-encoded depth; with
+    path_trace_frames > 0 the path tracer's resolved output (that many samples
+    per pixel) replaces the colour target, as the runner prefers it.  The
+    Bezier layers' normal texture is the mesh pass's colour
+    (GpuRunner.svelte.ts:400-430).  All three are rounded to 8 bits like the
+    reference's render targets.
+
+    Returns (target_rgba [H, W, 4], target_depth [H, W], normal_rgba [H, W, 4],
+    vp, vp_inv) — torch CUDA tensors and the camera's column-major matrices."""
+    from . import camera
+    from .mesh_render import MeshRenderer
+    from .path_trace import PathTracer
+    vp, vpi = camera.view_proj(eye, center, fovy, width / height, up=up)
+    view = camera.col_major(camera.look_at(eye, center, up))
+    r = MeshRenderer(mesh, matcap=matcap, env=env)
+    r.write_view_proj_mat(vp)
+    r.write_view_mat(view)
+    r.write_inv_view_proj_mat(vpi)
+    r.write_shading_mode(shading_mode)
+    color, depth4 = r.render(width, height, quantize=True)
+    r.close()
+    target = color
+    if path_trace_frames > 0:
+        pt = PathTracer(env_texture=env)
+        pt.set_meshes(mesh)
+        pt.set_output_size(width, height)
+        pt.write_inv_view_proj_mat(vpi)
+        pt.dispatch(frames=int(path_trace_frames), quantize=True)
+        target = pt.output.clone()
+        pt.close()
+    return target, depth4[..., 0].contiguous(), color, vp, vpi
+
+
 class LayeredFit:
     def __init__(self, target_rgba, target_depth, normal_rgba, vp, vp_inv, num_splats=512, num_beziers=256,
                  blur_radius=4, seed=0, layers=("edge", "base", "color")):

@@ -58,3 +58,34 @@ def test_layered_fit_trains_every_layer():
     mse = float(torch.mean((out[..., :3] - t[..., :3]) ** 2))
     assert mse < 0.8 * mse0, (mse0, mse)
     fit.close()
+
+
+def test_layered_fit_on_mesh_targets():
+    """The reference's whole per-frame chain on a mesh: mesh pass (normals
+    shading, reciprocal depth) and path-traced colour as targets, then the
+    preprocessing, the splats and the three Bezier layers."""
+    from nprush_b200 import build
+    build.build()
+    from nprush_b200 import meshes
+    from nprush_b200.layers import LayeredFit, mesh_targets
+    w = h = 96
+    scene = meshes.concat([meshes.uv_sphere((0.0, 0.0, 0.0), 0.35, (0.8, 0.3, 0.2, 1.0), 12, 24),
+                           meshes.box((0.3, 0.25, -0.2), 0.15, (0.2, 0.6, 0.8, 1.0))])
+    env = meshes.sky_env(64, 32)
+    t, d, n, vp, vpi = mesh_targets(scene, (1.2, -1.0, 0.6), (0.0, 0.0, 0.0), w, h, math.pi / 3, env=env,
+                                    path_trace_frames=16)
+    fg = d < 1.0
+    assert 0.1 < float(fg.float().mean()) < 0.9                    # the mesh and the sky
+    assert float((t[..., :3] - n[..., :3]).abs().max()) > 0.1       # path-traced colour, not the raster's
+    assert torch.all((t * 255 - torch.round(t * 255)).abs() < 1e-3)  # 8-bit levels
+    fit = LayeredFit(t, d, n, vp, vpi, num_splats=512, num_beziers=128, seed=5)
+    assert float(fit.edge[..., 0].max()) == 1.0  # the silhouette from the rendered depth
+    mse0 = float(torch.mean((fit.composite()[..., :3] - t[..., :3]) ** 2))
+    for _ in range(40):
+        fit.frame()
+    torch.cuda.synchronize()
+    out = fit.composite()
+    assert torch.isfinite(out).all()
+    mse = float(torch.mean((out[..., :3] - t[..., :3]) ** 2))
+    assert mse < 0.8 * mse0, (mse0, mse)
+    fit.close()
