@@ -1088,8 +1088,12 @@ __global__ void k_det_segsum(const uint32_t* __restrict__ keys, const uint32_t* 
 // over the group (xor 4, 2, 1: 56 shuffles) and lane s writes floats
 // 8s .. 8s + 7 of the Gaussian's gradient record.  The ADC statistic rides in
 // the padding floats 60 and 61 through the reduction.
-template <int DEG>
-__global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ params, uint32_t n,
+// ONE: at most eight views, so each lane has at most one view.  Its SH
+// gradient is then basis[k] * dc[c] exactly (a sum of one term), which is
+// formed just before the reduction instead of being accumulated through the
+// view's projection arithmetic: 48 fewer live registers there.
+template <int DEG, bool ONE>
+__global__ void __launch_bounds__(128, ONE ? 4 : 1) k_project_bwd(const float* __restrict__ params, uint32_t n,
                                                      const float* __restrict__ views, uint32_t nv, uint32_t W,
                                                      uint32_t H, const uint32_t* __restrict__ counts,
                                                      const float* __restrict__ g2, float* __restrict__ grads,
@@ -1115,6 +1119,8 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
   float g[kP];
 #pragma unroll
   for (int k = 0; k < kP; ++k) g[k] = 0.0f;
+  float one_basis[ONE ? nb : 1], one_dc[3] = {0.0f, 0.0f, 0.0f};
+  bool one_has = false;
   for (uint32_t v = sub; live && v < nv; v += 8) {
     const size_t gi = (size_t)v * n + i;
     if (counts[gi] == 0) continue;
@@ -1158,10 +1164,18 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
 #pragma unroll
       for (int c = 0; c < 3; ++c) g[c] += (ddir[c] - dir[c] * dd) * il;
     }
+    if constexpr (ONE) {
 #pragma unroll
-    for (int k = 0; k < nb; ++k)
+      for (int k = 0; k < nb; ++k) one_basis[k] = basis[k];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) g[kSH + 3 * k + c] += basis[k] * dc[c];
+      for (int c = 0; c < 3; ++c) one_dc[c] = dc[c];
+      one_has = true;
+    } else {
+#pragma unroll
+      for (int k = 0; k < nb; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) g[kSH + 3 * k + c] += basis[k] * dc[c];
+    }
     // conic -> covariance: dL/dCov = -Inv H Inv, H = [[ga, gb/2], [gb/2, gc]]
     const float ia = P.ca, ib = P.cb, ic = P.cc;
     const float h00 = dca, h01 = 0.5f * dcb, h11 = dcc;
@@ -1230,6 +1244,15 @@ __global__ void __launch_bounds__(128) k_project_bwd(const float* __restrict__ p
     const float qd = P.qn[0] * dqn[0] + P.qn[1] * dqn[1] + P.qn[2] * dqn[2] + P.qn[3] * dqn[3];
 #pragma unroll
     for (int k = 0; k < 4; ++k) g[kQuat + k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
+    if constexpr (ONE) break;  // a lane's only view
+  }
+  if constexpr (ONE) {
+    if (one_has) {
+#pragma unroll
+      for (int k = 0; k < nb; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) g[kSH + 3 * k + c] = one_basis[k] * one_dc[c];
+    }
   }
   // reduce-scatter over the group's eight lanes
   const bool b2 = sub & 4, b1 = sub & 2, b0 = sub & 1;
@@ -2232,11 +2255,17 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
     StageTimer t(o, ST_PBWD);
     const uint32_t blocks = div_up((size_t)n * 8, 128);
     const float adc_scale = (float)(o->loss_views ? o->loss_views : nv);
-#define NPS_PBWD(D)                                                                                             \
-  gs::k_project_bwd<D><<<blocks, 128, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, W, H,         \
-                                               o->counts.as<uint32_t>(), o->g2.as<float>(), o->grads.as<float>(), \
-                                               o->adc_grad.as<float>(), o->adc_denom.as<float>(),                 \
-                                               o->accumulate ? 1 : 0, adc_scale)
+#define NPS_PBWD1(D, ONE)                                                                                        \
+  gs::k_project_bwd<D, ONE><<<blocks, 128, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, W, H,     \
+                                                    o->counts.as<uint32_t>(), o->g2.as<float>(),                  \
+                                                    o->grads.as<float>(), o->adc_grad.as<float>(),                \
+                                                    o->adc_denom.as<float>(), o->accumulate ? 1 : 0, adc_scale)
+#define NPS_PBWD(D)            \
+  if (nv <= 8) {               \
+    NPS_PBWD1(D, true);        \
+  } else {                     \
+    NPS_PBWD1(D, false);       \
+  }
     switch (o->sh_deg) {
       case 0: NPS_PBWD(0); break;
       case 1: NPS_PBWD(1); break;
