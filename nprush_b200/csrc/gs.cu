@@ -245,13 +245,32 @@ __global__ void __launch_bounds__(256) k_emit(const uint32_t* __restrict__ sorte
   }
 }
 
+// Four consecutive sorted keys per thread from one 16-byte load (the key
+// buffers are 256-byte aligned), with the neighbours on either side.
 __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
                          uint32_t* __restrict__ rstart, uint32_t* __restrict__ rend) {
   const uint32_t K = min(*total, cap);
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < K; p += gridDim.x * blockDim.x) {
-    const uint32_t k = keys[p];
-    if (p == 0 || keys[p - 1] != k) rstart[k] = p;
-    if (p == K - 1 || keys[p + 1] != k) rend[k] = p + 1;
+  const uint32_t n4 = (K + 3) / 4;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += gridDim.x * blockDim.x) {
+    const uint32_t p0 = 4 * q;
+    uint32_t k[4];
+    if (p0 + 3 < K) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(keys) + q);
+      k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) k[j] = p0 + j < K ? __ldg(keys + p0 + j) : 0u;
+    }
+    const uint32_t prev = p0 > 0 ? __ldg(keys + p0 - 1) : 0u;
+    const uint32_t next = p0 + 4 < K ? __ldg(keys + p0 + 4) : 0u;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t p = p0 + j;
+      if (p >= K) break;
+      const uint32_t before = j == 0 ? prev : k[j - 1], after = j == 3 ? next : k[j + 1];
+      if (p == 0 || before != k[j]) rstart[k[j]] = p;
+      if (p == K - 1 || after != k[j]) rend[k[j]] = p + 1;
+    }
   }
 }
 
@@ -2145,7 +2164,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
       NPS_TRY(radix_sort_u32(o->keys.as<uint32_t>(), o->vals.as<uint32_t>(), total, o->pair_cap, bits, o->sw_tile, s,
                              &ks, &vv)); }
       { StageTimer t(o, ST_RANGES);
-      gs::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, o->pair_cap, rstart, rend);
+      gs::k_ranges<<<16 * kNumSMs, 256, 0, s>>>(ks, total, o->pair_cap, rstart, rend);
       NPS_CHECK_LAUNCH(); }
       vs = vv;
     }
