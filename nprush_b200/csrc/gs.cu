@@ -1347,6 +1347,7 @@ __global__ void __launch_bounds__(256) k_adam(float4* __restrict__ p, const floa
                                               AdamArgs a, const uint32_t* __restrict__ st) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n4 || st[1] != 0u) return;
+  if ((t & 15u) * 4u >= (uint32_t)kUsed) return;  // floats 60-63: nothing to update, nothing to move
   const float bc1 = __uint_as_float(st[2]), bc2 = __uint_as_float(st[3]);
   const int k0 = (int)(t & 15u) * 4;
   float4 pp = p[t], gg = g[t], mm = m[t], vv = v[t];
