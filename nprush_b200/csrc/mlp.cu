@@ -61,8 +61,10 @@ constexpr uint32_t sW3 = sW2 + 64 * 64 * 2;       // B  [16 x 64]    W3 (3 rows 
 constexpr uint32_t sW2T = sW3 + 16 * 64 * 2;      // B  [64 x 64]    W2^T
 constexpr uint32_t sW3T = sW2T + 64 * 64 * 2;     // B  [64 x 16]    W3^T (3 columns used)
 constexpr uint32_t sBias = sW3T + 64 * 16 * 2;    // fp32 b1[64], b2[64], b3[4]
-constexpr uint32_t sRed = sBias + 132 * 4;        // fp32 bias-gradient sums db1[64], db2[64], db3[4]
-constexpr uint32_t sBar = (sRed + 132 * 4 + 15) / 16 * 16;  // mbarrier (8 B) + TMEM address (4 B)
+// per warp: fp32 bias-gradient sums db1[64], db2[64], db3[4], then the loss and the correct count
+constexpr uint32_t kRedSlot = 136;
+constexpr uint32_t sRed = sBias + 132 * 4;
+constexpr uint32_t sBar = (sRed + (kThreads / 32) * kRedSlot * 4 + 15) / 16 * 16;  // mbarrier (8 B) + TMEM address
 constexpr uint32_t kSmemBytes = sBar + 16;
 static_assert(kSmemBytes <= 227 * 1024, "shared memory budget");
 
@@ -155,10 +157,13 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+// Each block writes its sums to its own row of `partial` (kPartial floats:
+// the kNumParams gradient sums, the loss, the correct count); k_mlp_reduce
+// then adds the rows in block order, so a batch's gradient is the same bits
+// on every run.
+constexpr uint32_t kPartial = kNumParams + 2;
 struct TrainOut {
-  float* grads;      // kNumParams, accumulated with atomics
-  float* loss;       // sum of weighted cross-entropy / batch rows
-  uint32_t* correct; // rows whose argmax equals the label
+  float* partial;    // gridDim.x x kPartial
 };
 
 // kTrain: forward + softmax cross-entropy + backward, gradients accumulated;
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + sBar + 8);
   float* bias = reinterpret_cast<float*>(smem + sBias);
   float* red = reinterpret_cast<float*>(smem + sRed);
+  float* redw = red + warp * kRedSlot;  // this warp's sums (only its lane 0 writes them)
 
   // weights to bf16 operand tiles, biases to fp32
   for (uint32_t i = tid; i < kH * kIn; i += kThreads) {
@@ -193,10 +199,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     st_one(smem + sW3, o, k, kH, w);
     st_one(smem + sW3T, k, o, kOutPad, w);
   }
-  for (uint32_t i = tid; i < 132; i += kThreads) {
+  for (uint32_t i = tid; i < 132; i += kThreads)
     bias[i] = i < 64 ? params[oB1 + i] : i < 128 ? params[oB2 + i - 64] : (i - 128 < 3 ? params[oB3 + i - 128] : 0.f);
-    red[i] = 0.0f;
-  }
+  for (uint32_t i = tid; i < (kThreads / 32) * kRedSlot; i += kThreads) red[i] = 0.0f;
   // rows 3..15 of dZ3^T stay zero
   for (uint32_t i = tid; i < 16 * 128; i += kThreads) {
     const uint32_t c = i / 128, r = i % 128;
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int k = 0; k < 3; ++k) {
       const float s = warp_sum(d3[k]);
-      if (lane == 0) atomicAdd(&red[128 + k], s);
+      if (lane == 0) redw[128 + k] += s;
     }
     st_row8(smem + sdZ3, tid, 0, kOutPad, d3);
     st_row8(smem + sdZ3, tid, 8, kOutPad, d3 + 8);
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int i = 0; i < 16; ++i) {
         v[i] = ((mask2 >> (c + i)) & 1ull) ? v[i] : 0.0f;
         const float s = warp_sum(v[i]);
-        if (lane == 0) atomicAdd(&red[64 + c + i], s);
+        if (lane == 0) redw[64 + c + i] += s;
       }
       st_row8(smem + sdZ2, tid, c, kH, v);
       st_row8(smem + sdZ2, tid, c + 8, kH, v + 8);
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int i = 0; i < 16; ++i) {
         v[i] = ((mask1 >> (c + i)) & 1ull) ? v[i] : 0.0f;
         const float s = warp_sum(v[i]);
-        if (lane == 0) atomicAdd(&red[c + i], s);
+        if (lane == 0) redw[c + i] += s;
       }
 #pragma unroll
       for (int i = 0; i < 16; ++i) st_one(smem + sAdz, 64 + c + i, tid, kRows, v[i]);
@@ -379,36 +384,55 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
 
-  if (kTrain && ok && !first) {
-    // accumulated weight gradients: TMEM -> global
-    if (warp < 2) {
-      const uint32_t o = tid;  // output feature of W2, input feature of W3
-      for (int c = 0; c < kH; c += 16) {
+  if (kTrain) {
+    float* part = out.partial + (size_t)blockIdx.x * kPartial;
+    if (ok && !first) {
+      // accumulated weight gradients: TMEM -> this block's row
+      if (warp < 2) {
+        const uint32_t o = tid;  // output feature of W2, input feature of W3
+        for (int c = 0; c < kH; c += 16) {
+          float v[16];
+          tmem_ld16(tl + cDA + c, v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) part[oW2 + o * kH + c + i] = v[i];
+        }
         float v[16];
-        tmem_ld16(tl + cDA + c, v);
+        tmem_ld16(tl + cDC, v);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) atomicAdd(&out.grads[oW2 + o * kH + c + i], v[i]);
+        for (int k = 0; k < kOut; ++k) part[oW3 + k * kH + o] = v[k];
+      } else {
+        const uint32_t o = tid - 64;  // output feature of W1
+        float v[16];
+        tmem_ld16(tl + cDB, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) part[oW1 + o * kIn + i] = v[i];
       }
-      float v[16];
-      tmem_ld16(tl + cDC, v);
+      const float ls = warp_sum(loss_acc), cs = warp_sum(correct_acc);
+      if (lane == 0) {
+        redw[132] = ls;
+        redw[133] = cs;
+      }
+      __syncthreads();
+      // bias gradients, loss and count: the warps' sums in warp order
+      for (uint32_t i = tid; i < 133; i += kThreads) {
+        const uint32_t src = i < 131 ? i : 132;
+        float t = 0.0f;
 #pragma unroll
-      for (int k = 0; k < kOut; ++k) atomicAdd(&out.grads[oW3 + k * kH + o], v[k]);
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w * kRedSlot + src];
+        if (i < 131) {
+          const int dst = i < 64 ? oB1 + i : i < 128 ? oB2 + (i - 64) : oB3 + (i - 128);
+          part[dst] = t;
+        } else {
+          part[kNumParams] = t;
+        }
+      }
+      if (tid == 0) {
+        float c = 0.0f;
+        for (int w = 0; w < kThreads / 32; ++w) c += red[w * kRedSlot + 133];
+        part[kNumParams + 1] = c;
+      }
     } else {
-      const uint32_t o = tid - 64;  // output feature of W1
-      float v[16];
-      tmem_ld16(tl + cDB, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) atomicAdd(&out.grads[oW1 + o * kIn + i], v[i]);
-    }
-    __syncthreads();
-    for (uint32_t i = tid; i < 131; i += kThreads) {
-      const int dst = i < 64 ? oB1 + i : i < 128 ? oB2 + (i - 64) : oB3 + (i - 128);
-      atomicAdd(&out.grads[dst], red[i]);
-    }
-    const float ls = warp_sum(loss_acc), cs = warp_sum(correct_acc);
-    if (lane == 0) {
-      atomicAdd(out.loss, ls);
-      atomicAdd(out.correct, (uint32_t)(cs + 0.5f));
+      for (uint32_t i = tid; i < kPartial; i += kThreads) part[i] = 0.0f;
     }
   }
   if (!ok) {
@@ -437,6 +461,20 @@ __global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, f
   p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
 }
 
+// Adds the blocks' rows of `partial` in block order: gradient sums into
+// grads (zeroed by the caller per batch), loss and count into the running
+// sums of the epoch.
+__global__ void k_mlp_reduce(const float* __restrict__ partial, uint32_t nblocks, float* __restrict__ grads,
+                             float* __restrict__ loss, uint32_t* __restrict__ correct) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kPartial) return;
+  float t = 0.0f;
+  for (uint32_t b = 0; b < nblocks; ++b) t += partial[(size_t)b * kPartial + i];
+  if (i < kNumParams) grads[i] += t;
+  else if (i == kNumParams) *loss += t;
+  else *correct += (uint32_t)(t + 0.5f);
+}
+
 }  // namespace mlp
 }  // namespace nps
 
@@ -444,7 +482,7 @@ using namespace nps;
 
 struct nps_mlp {
   nps_ctx* ctx = nullptr;
-  DevBuf params, grads, m, v, loss, rows, err;
+  DevBuf params, grads, m, v, loss, rows, err, partial;
   uint32_t step = 0;
   float last_loss = 0.0f, last_acc = 0.0f;
 };
@@ -467,14 +505,18 @@ int launch_mlp(nps_mlp* o, bool train, const float* X, const uint32_t* rows, con
     NPS_CUDA(cudaFuncSetAttribute(mlp::k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes));
   const uint32_t ntiles = div_up(n, mlp::kRows);
   const uint32_t grid = ntiles < (uint32_t)o->ctx->sm_count ? ntiles : (uint32_t)o->ctx->sm_count;
-  mlp::TrainOut out{o->grads.as<float>(), o->loss.as<float>(), o->loss.as<uint32_t>() + 1};
+  if (train) NPS_TRY(o->partial.ensure(sizeof(float) * (size_t)grid * mlp::kPartial));
+  mlp::TrainOut out{train ? o->partial.as<float>() : nullptr};
   const float4 cw = cw4 ? make_float4(cw4[0], cw4[1], cw4[2], cw4[3]) : make_float4(1, 1, 1, 1);
-  if (train)
+  if (train) {
     mlp::k_mlp<true><<<grid, mlp::kThreads, mlp::kSmemBytes, s>>>(o->params.as<float>(), X, rows, labels, n, cw,
                                                                  inv_batch, out, nullptr, o->err.as<uint32_t>());
-  else
+    mlp::k_mlp_reduce<<<div_up(mlp::kPartial, 256), 256, 0, s>>>(o->partial.as<float>(), grid, o->grads.as<float>(),
+                                                                 o->loss.as<float>(), o->loss.as<uint32_t>() + 1);
+  } else {
     mlp::k_mlp<false><<<grid, mlp::kThreads, mlp::kSmemBytes, s>>>(o->params.as<float>(), X, rows, labels, n, cw,
                                                                   inv_batch, out, logits, o->err.as<uint32_t>());
+  }
   NPS_CHECK_LAUNCH();
   return NPS_OK;
 }
@@ -519,7 +561,7 @@ int nps_mlp_destroy(nps_mlp* o) {
   if (!o) return NPS_OK;
   bind_device(o->ctx);
   cudaStreamSynchronize(o->ctx->stream);
-  for (DevBuf* b : {&o->params, &o->grads, &o->m, &o->v, &o->loss, &o->rows, &o->err}) b->release();
+  for (DevBuf* b : {&o->params, &o->grads, &o->m, &o->v, &o->loss, &o->rows, &o->err, &o->partial}) b->release();
   delete o;
   return NPS_OK;
 }

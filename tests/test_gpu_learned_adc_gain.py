@@ -3,14 +3,14 @@ small seeded scene (20k-Gaussian student, 30k teacher, 256 x 256, 16
 cameras, 4 views per step, 1200 steps, ADC every 100 from step 300): the
 policy is trained on hindsight-labelled decisions logged from two plain runs
 on other seeds, then both rules train the held-out scene.  Deterministic
-mode makes each training run reproducible, but the policy's own training sums
-its mini-batch gradients with float atomics, so its weights (and with them the
-learned run) vary slightly from run to run.  Checked: the learned rule ends
+mode makes each training run reproducible, and the policy's training is too
+(its gradients are summed in a fixed order).  Checked: the learned rule ends
 with no more Gaussians than the plain one (1% slack) and no worse PSNR (0.2 dB
-slack).  At this scale the difference is within that noise (measured in
-different runs: 41302 vs 41402 Gaussians and 39.05 vs 38.63 dB; 41411 vs 41402
-and 38.61 vs 38.63 dB); the 30k-step comparison at config 2 is where the
-policy's effect shows."""
+slack).  At this scale the two rules differ by less than a run-to-run change
+of the scene or the policy's seeds moves them (measured with earlier builds:
+41302 vs 41402 Gaussians and 39.05 vs 38.63 dB; 41411 vs 41402 and 38.61 vs
+38.63 dB), so no strict gain is asserted; the 30k-step comparison at config 2
+is where the policy's effect shows."""
 import numpy as np
 import pytest
 
