@@ -453,8 +453,10 @@ int nps_mesh_set_pbr(nps_mesh* mesh, uint32_t first_tri, const float* albedo_rgb
  * invViewProj; matrices column-major).  Writes color_rgba (the shaded colour)
  * and depth_rgba (1 - 0.1 / max(w, 0.1) per fragment, 1 where no triangle):
  * device w x h float4 images, at most 16384 x 16384; quantize != 0 rounds
- * them to the 8-bit levels of the reference's targets.  Asynchronous on the
- * context stream. */
+ * them to the 8-bit levels of the reference's targets.  The triangles'
+ * clamped pixel boxes together must hold fewer than 2^42 pixels (2^32 work
+ * chunks of 1024 pixels; e.g. four million full-screen triangles at
+ * 1024 x 1024).  Asynchronous on the context stream. */
 int nps_mesh_render(nps_mesh* mesh, const float* uniforms52, float* color_rgba, float* depth_rgba, uint32_t w,
                     uint32_t h, int draw_env, int quantize);
 
