@@ -117,6 +117,17 @@ def test_restatement_matches_reference_radiance(gold, case):
     assert np.all(want[..., 3] == 1.0)
 
 
+def test_restatement_matches_every_mirror_pixel(gold):
+    """All 45 x 37 pixels of the all-mirror fixture (paths of up to 8 mirror
+    bounces, no random directions) from the scalar restatement."""
+    sc = opt.Scene(gold["mirror_vertices"], gold["nodes"], gold["tris"], gold["env"])
+    want = gold["mirror_accum_f5"]
+    h, w = want.shape[:2]
+    got = np.array([[opt.trace_pixel(sc, gold["inv_view_proj"], x, y, w, h, 5) for x in range(w)]
+                    for y in range(h)], np.float32)
+    np.testing.assert_allclose(got, want[..., :3], atol=1e-5, rtol=0)
+
+
 def test_restatement_resolve(gold):
     np.testing.assert_array_equal(opt.resolve(gold["accum_f012"]), gold["resolved_f012"])
 
