@@ -127,3 +127,48 @@ def test_reference_stages_reproduce_the_fixtures(tmp_path, monkeypatch):
     a, b = np.load(GOLD), np.load(tmp_path / "mesh_raster.npz")
     for k in a.files:
         np.testing.assert_array_equal(a[k], b[k])
+
+
+def _uni(eye, target, w, h, fovy=0.9):
+    from nprush_b200 import camera
+    vp, inv = camera.view_proj(eye, target, fovy, w / h, up=(0.0, 0.0, 1.0))
+    u = np.zeros(52, np.float32)
+    u[0:16], u[36:52] = vp, inv
+    u[16:32] = camera.col_major(camera.look_at(eye, target, (0.0, 0.0, 1.0)))
+    return u
+
+
+def _tri(p0, p1, p2):
+    v = np.zeros((3, 12), np.float32)
+    v[:, 0:3] = (p0, p1, p2)
+    v[:, 5] = 1.0
+    v[:, 6:10] = (0.5, 0.5, 0.5, 1.0)
+    return v
+
+
+def _both_windings(v):
+    return np.concatenate([v, v]), np.array([0, 1, 2, 3, 5, 4], np.uint32)
+
+
+def test_clipping_and_culling_edge_cases():
+    w, h = 40, 30
+    st = mr.RestatedStages(np.ones((1, 1, 4), np.float32), np.ones((1, 1, 4), np.float32))
+    uni = _uni((0.0, -3.0, 0.0), (0.0, 0.0, 0.0), w, h)  # looking along +y
+    # behind the eye: nothing drawn
+    v, idx = _both_windings(_tri((-1, -5, -1), (1, -5, -1), (0, -5, 1)))
+    _, d = mr.render(v, idx, uni, w, h, st)
+    assert np.all(d == 1.0)
+    # a huge triangle around the view (vertices far outside the frustum): guard-band
+    # clipping leaves the part in front, which covers the screen
+    v, idx = _both_windings(_tri((-1e4, 2.0, -1e4), (1e4, 2.0, -1e4), (0.0, 2.0, 1e4)))
+    _, d = mr.render(v, idx, uni, w, h, st)
+    assert np.all(d[..., 0] < 1.0)
+    # reaching past the far plane (100): the far part is clipped, the near part drawn
+    v, idx = _both_windings(_tri((-0.5, 1.0, -0.5), (0.5, 1.0, -0.5), (0.0, 500.0, 0.3)))
+    _, d = mr.render(v, idx, uni, w, h, st)
+    assert 0 < (d[..., 0] < 1.0).sum() < w * h
+    # degenerate (collinear) and offscreen triangles: nothing drawn
+    for t in (_tri((0, 1, 0), (0.5, 1, 0), (1, 1, 0)), _tri((50, 1, 0), (51, 1, 0), (50, 1, 1))):
+        v, idx = _both_windings(t)
+        _, d = mr.render(v, idx, uni, w, h, st)
+        assert np.all(d == 1.0)
