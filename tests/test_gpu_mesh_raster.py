@@ -148,3 +148,32 @@ def test_bad_arguments(mrmod):
     from nprush_b200.meshes import MeshData
     with pytest.raises(_lib.NpsError):
         mrmod.MeshRenderer(MeshData(np.zeros((3, 12), np.float32), np.array([0, 1, 3], np.uint32)))
+
+
+def test_clipping_edge_cases_match_restatement(mrmod):
+    """Behind the eye, guard-band and far-plane clipping, degenerate and
+    offscreen triangles: the kernels draw exactly what the restatement does."""
+    import mesh_raster as mr
+    from nprush_b200 import camera
+    w, h = 40, 30
+    eye, tgt = (0.0, -3.0, 0.0), (0.0, 0.0, 0.0)
+    vp, inv = camera.view_proj(eye, tgt, 0.9, w / h, up=(0.0, 0.0, 1.0))
+    u = np.zeros(52, np.float32)
+    u[0:16], u[36:52] = vp, inv
+    u[16:32] = camera.col_major(camera.look_at(eye, tgt, (0.0, 0.0, 1.0)))
+    tris = [((-1, -5, -1), (1, -5, -1), (0, -5, 1)),
+            ((-1e4, 2.0, -1e4), (1e4, 2.0, -1e4), (0.0, 2.0, 1e4)),
+            ((-0.5, 1.0, -0.5), (0.5, 1.0, -0.5), (0.0, 500.0, 0.3)),
+            ((0, 1, 0), (0.5, 1, 0), (1, 1, 0)),
+            ((50, 1, 0), (51, 1, 0), (50, 1, 1))]
+    one = np.ones((1, 1, 4), np.float32)
+    for t in tris:
+        v = np.zeros((6, 12), np.float32)
+        v[:3, 0:3] = t
+        v[3:, 0:3] = t
+        v[:, 5] = 1.0
+        v[:, 6:10] = (0.5, 0.5, 0.5, 1.0)
+        idx = np.array([0, 1, 2, 3, 5, 4], np.uint32)
+        c, d = render(mrmod, v, idx, u, w, h, one, one)
+        wc, wd = mr.render(v, idx, u, w, h, mr.RestatedStages(one, one))
+        check(c, d, wc, wd)
