@@ -149,3 +149,29 @@ def test_bad_arguments(ptmod, gold):
     pt = ptmod.PathTracer()
     with pytest.raises(_lib.NpsError):
         pt.set_meshes(MeshData(np.zeros((3, 12), np.float32), np.array([0, 1, 5], np.uint32)))
+
+
+def test_camera_inside_a_closed_box(ptmod):
+    """Inside a closed box no path reaches the environment: every path ends at
+    the eighth bounce with zero radiance (diffuse walls and a mirror wall),
+    the sample count still advances, and sampled pixels equal the
+    restatement.  No environment set: the default single white texel."""
+    import path_trace as opt
+    from nprush_b200 import camera, meshes
+    box = meshes.box((0.0, 0.0, 0.0), 1.0, (0.7, 0.6, 0.5, 1.0))
+    box.vertices[:4, 9] = 0.0  # one wall a mirror
+    w, h = 32, 24
+    _, inv = camera.view_proj((0.2, -0.3, 0.1), (0.0, 1.0, 0.2), 1.2, w / h, up=(0.0, 0.0, 1.0))
+    pt = ptmod.PathTracer()
+    pt.set_meshes(box)
+    pt.set_output_size(w, h)
+    pt.write_inv_view_proj_mat(inv)
+    pt.dispatch(frames=2)
+    acc = pt.accum.cpu().numpy()
+    assert np.all(acc[..., :3] == 0.0) and np.all(acc[..., 3] == 2.0)
+    nodes, tris = pt.bvh()
+    o = opt.Scene(box.vertices, nodes, tris, np.ones((1, 1, 4), np.float32))
+    for x, y in ((0, 0), (15, 11), (31, 23)):
+        assert np.all(opt.trace_pixel(o, inv, x, y, w, h, 0) == 0.0)
+    assert pt.overflows() == 0
+    pt.close()
