@@ -19,7 +19,7 @@
 // code run on the host (oracle/_ref, built by oracle/build_ref.py).  That
 // comparison is what pins this restatement (tests/test_oracle_pin.py).
 //
-// Part 2 ("gs") is the north-star model, which has no reference counterpart:
+// Part 2 ("gs") is the 3D Gaussian training model, which has no reference counterpart:
 // standard 3D Gaussians (log-scales, logit opacity, SH up to degree 3), depth
 // ordered compositing and L1 / L2 / D-SSIM losses, templated on the scalar so
 // the double instantiation is the FP64 central-difference oracle.

@@ -1,10 +1,11 @@
-// nps_oracle_gs.cpp — CPU oracle of the north-star Gaussian model.
+// nps_oracle_gs.cpp — CPU oracle of the 3D Gaussian training model.
 //
 // TEST INFRASTRUCTURE ONLY (tests, smoke, and bench.py's CPU-baseline leg).
 // The model has no counterpart in the reference (which fits generalised
 // linear-parameter splats, splat_backward.wgsl:92-134); it is the model the
-// build's Gaussian trainer implements, restated here independently of the CUDA
-// code:
+// library's Gaussian trainer implements, restated here independently of the
+// CUDA code (the per-primitive math — SH basis, rotation, projection, split
+// sampling — in gs_model.h, which includes nothing of the library):
 //   * standard 3D Gaussians: mean, log-scales, quaternion, opacity logit,
 //     real SH up to degree 3 (colour = SH + 0.5, clamped at 0);
 //   * EWA projection with +0.3 px^2 low-pass; tile rectangle from the box of
@@ -28,9 +29,9 @@
 #include <cstring>
 #include <vector>
 
-#include "../nprush_b200/csrc/gs_math.cuh"
+#include "gs_model.h"
 
-using namespace nps::gsm;
+using namespace orc_gm;
 
 namespace {
 
@@ -53,8 +54,8 @@ void preprocess(const T* params, uint32_t n, int deg, const float* view, uint32_
   const uint32_t tx = (W + 15) / 16, ty = (H + 15) / 16;
   for (uint32_t i = 0; i < n; ++i) {
     const T* p = params + (size_t)i * kP;
-    Proj<T> P;
-    project<T>(view, p + kMean, p + kLogScale, p + kQuat, (T)W, (T)H, (T)kLowpass, P);
+    Footprint<T> P;
+    project_gaussian<T>(view, p, (T)W, (T)H, (T)kLowpass, P);
     PreG<T>& g = out[i];
     // every field is filled even for culled Gaussians (frozen replays read them)
     g.u = P.u; g.v = P.v; g.ca = P.ca; g.cb = P.cb; g.cc = P.cc;
@@ -64,7 +65,7 @@ void preprocess(const T* params, uint32_t n, int deg, const float* view, uint32_
     const T dx = p[0] - (T)view[32], dy = p[1] - (T)view[33], dz = p[2] - (T)view[34];
     const T il = (T)1 / std::sqrt(std::max(dx * dx + dy * dy + dz * dz, (T)1e-20));
     T basis[16];
-    sh_basis<T>(deg, dx * il, dy * il, dz * il, basis);
+    real_sh<T>(deg, dx * il, dy * il, dz * il, basis);
     const int nb = (deg + 1) * (deg + 1);
     for (int c = 0; c < 3; ++c) {
       T col = (T)0.5;
@@ -222,7 +223,7 @@ void render_view(const T* params, uint32_t n, int deg, const float* view, uint32
           const T dx = p[0] - (T)view[32], dy = p[1] - (T)view[33], dz = p[2] - (T)view[34];
           const T il = (T)1 / std::sqrt(std::max(dx * dx + dy * dy + dz * dz, (T)1e-20));
           T basis[16];
-          sh_basis<T>(deg, dx * il, dy * il, dz * il, basis);
+          real_sh<T>(deg, dx * il, dy * il, dz * il, basis);
           T col = (T)0.5;
           for (int k = 0; k < (deg + 1) * (deg + 1); ++k) col += basis[k] * p[kSH + 3 * k + c];
           pre[i].col[c] = col;
@@ -314,6 +315,29 @@ T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t 
 }  // namespace
 
 extern "C" {
+
+// FP64 probes of the model's building blocks, for checks of gs_model.h on
+// its own terms.  SH basis of degree 3 and its partials at n directions
+// (dirs n x 3; each output n x 16).
+int orc_gs_sh(const double* dirs, uint32_t n, double* b, double* gx, double* gy, double* gz) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const double* d = dirs + 3 * (size_t)i;
+    real_sh<double>(3, d[0], d[1], d[2], b + 16 * (size_t)i);
+    real_sh_grad<double>(3, d[0], d[1], d[2], gx + 16 * (size_t)i, gy + 16 * (size_t)i, gz + 16 * (size_t)i);
+  }
+  return 0;
+}
+
+// Rotation of the unit quaternion q (R 9, row-major) and the vector-Jacobian
+// product dq = sum G[r][c] dR[r][c]/dq (G 9, dq 4).
+int orc_gs_rot(const double* q, const double* G9, double* R9, double* dq) {
+  double R[3][3], G[3][3];
+  for (int k = 0; k < 9; ++k) G[k / 3][k % 3] = G9[k];
+  quat_rotation<double>(q[0], q[1], q[2], q[3], R);
+  for (int k = 0; k < 9; ++k) R9[k] = R[k / 3][k % 3];
+  quat_rotation_vjp<double>(q[0], q[1], q[2], q[3], G, dq);
+  return 0;
+}
 
 // fp32 forward of V views: img V x H x W x 4 (rgb, final T), ncontrib V x H x W
 int orc_gs_forward(const float* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W, uint32_t H,
@@ -464,8 +488,8 @@ int orc_gs_backward(const float* params, uint32_t n, int deg, const float* views
       if (!pg.vis) continue;
       const float* gr = &g2[((size_t)v * n + i) * 10];
       const float* view = views + (size_t)kViewRec * v;
-      Proj<float> P;
-      project<float>(view, p + kMean, p + kLogScale, p + kQuat, (float)W, (float)H, (float)kLowpass, P);
+      Footprint<float> P;
+      project_gaussian<float>(view, p, (float)W, (float)H, (float)kLowpass, P);
       gop += gr[5];
       if (adc2) {
         const float du = gr[0] * 0.5f * (float)W, dv = gr[1] * 0.5f * (float)H;
@@ -478,10 +502,10 @@ int orc_gs_backward(const float* params, uint32_t n, int deg, const float* views
       const float il2 = 1.0f / std::sqrt(std::max(ddx * ddx + ddy * ddy + ddz * ddz, 1e-20f));
       const float dir[3] = {ddx * il2, ddy * il2, ddz * il2};
       float basis[16];
-      sh_basis<float>(deg, dir[0], dir[1], dir[2], basis);
+      real_sh<float>(deg, dir[0], dir[1], dir[2], basis);
       if (deg > 0) {
         float bx[16], by[16], bz[16], ddir[3] = {0, 0, 0};
-        sh_basis_grad<float>(deg, dir[0], dir[1], dir[2], bx, by, bz);
+        real_sh_grad<float>(deg, dir[0], dir[1], dir[2], bx, by, bz);
         for (int k = 1; k < nb; ++k) {
           const float s = p[kSH + 3 * k] * dc[0] + p[kSH + 3 * k + 1] * dc[1] + p[kSH + 3 * k + 2] * dc[2];
           ddir[0] += s * bx[k]; ddir[1] += s * by[k]; ddir[2] += s * bz[k];
@@ -530,7 +554,7 @@ int orc_gs_backward(const float* params, uint32_t n, int deg, const float* views
         gls[c] += ds * P.sc[c];
       }
       float dqn[4];
-      rot_grad_to_quat<float>(P.qn[0], P.qn[1], P.qn[2], P.qn[3], dR, dqn);
+      quat_rotation_vjp<float>(P.qn[0], P.qn[1], P.qn[2], P.qn[3], dR, dqn);
       const float qd = P.qn[0] * dqn[0] + P.qn[1] * dqn[1] + P.qn[2] * dqn[2] + P.qn[3] * dqn[3];
       for (int k = 0; k < 4; ++k) gq[k] += (dqn[k] - P.qn[k] * qd) / P.qlen;
     }
@@ -566,8 +590,8 @@ int orc_gs_adam(float* params, const float* grads, float* m, float* v, uint32_t 
 // Plain threshold ADC, serial: prune opacity < prune_op; densify (avg grad >=
 // thresh) by split (max scale > split_scale) or clone, densifying candidates in
 // index order while the capacity allows; records are compacted in index order,
-// each parent's outputs in place of it.  Split children come from the shared
-// sampling helper; clones keep the parent's Adam state in the first copy.
+// each parent's outputs in place of it.  Split children come from
+// split_child (gs_model.h); clones keep the parent's Adam state in the first copy.
 int orc_gs_adc(const float* params, const float* m, const float* v, const float* adc_grad, const float* adc_denom,
                uint32_t n, uint32_t cap, float thresh, float split_scale, float prune_op, uint32_t seed,
                float* out_p, float* out_m, float* out_v, uint32_t* counts4) {
@@ -622,7 +646,7 @@ int orc_gs_adc(const float* params, const float* m, const float* v, const float*
         float* Q = out_p + (size_t)(o + c) * kP;
         std::copy(P, P + kP, Q);
         float mean[3], ls[3];
-        adc_split_child(P, i, seed, c, mean, ls);
+        split_child(P, i, seed, c, mean, ls);
         for (int k = 0; k < 3; ++k) {
           Q[k] = mean[k];
           Q[3 + k] = ls[k];

@@ -16,18 +16,20 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libnps_oracle.so"
 SOURCES = [HERE / "nps_oracle.cpp", HERE / "nps_oracle_gs.cpp", HERE / "nps_oracle_mlp.cpp"]
+HEADERS = [HERE / "gs_model.h"]
 
 
 def build(force: bool = False) -> Path:
-    newest = max(s.stat().st_mtime for s in SOURCES if s.exists())
+    newest = max(s.stat().st_mtime for s in SOURCES + HEADERS if s.exists())
     if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
         return LIB
+    tmp = f"{LIB}.{os.getpid()}.tmp"  # concurrent builders each write their own file
     cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
-           "-shared", "-o", str(LIB) + ".tmp"] + [str(s) for s in SOURCES if s.exists()]
+           "-shared", "-o", tmp] + [str(s) for s in SOURCES if s.exists()]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stderr[-4000:])
-    os.replace(str(LIB) + ".tmp", LIB)
+    os.replace(tmp, LIB)
     return LIB
 
 
@@ -41,8 +43,7 @@ D = ctypes.POINTER(ctypes.c_double)
 def lib():
     global _lib
     if _lib is None:
-        if not LIB.exists():
-            build()
+        build()  # no-op unless a source or header is newer than the library
         _lib = ctypes.CDLL(str(LIB))
     return _lib
 
@@ -200,6 +201,23 @@ def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=
                          _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam), _p(pidx, U),
                          len(pidx), ctypes.c_double(h_rel), _p(out, D))
     return out
+
+
+def gs_sh(dirs):
+    """FP64 degree-3 SH basis and its x / y / z partials at dirs (n x 3): four n x 16 arrays."""
+    dirs = np.ascontiguousarray(dirs, np.float64).reshape(-1, 3)
+    out = [np.zeros((len(dirs), 16), np.float64) for _ in range(4)]
+    lib().orc_gs_sh(_p(dirs, D), len(dirs), *(_p(o, D) for o in out))
+    return out
+
+
+def gs_rot(q, G):
+    """FP64 rotation matrix of the unit quaternion q and dq = sum G * dR/dq."""
+    q = np.ascontiguousarray(q, np.float64)
+    G = np.ascontiguousarray(G, np.float64).reshape(9)
+    R, dq = np.zeros(9, np.float64), np.zeros(4, np.float64)
+    lib().orc_gs_rot(_p(q, D), _p(G, D), _p(R, D), _p(dq, D))
+    return R.reshape(3, 3), dq
 
 
 # ------------------------------------------------------------ display forwards

@@ -78,3 +78,62 @@ def test_adc_oracle_invariants():
                 assert not np.array_equal(q[o, :3], q[o + 1, :3])
                 o += 2
         assert o == c[1]
+
+
+def _sphere_quadrature():
+    """Gauss-Legendre in z (8 nodes) x 16 uniform angles: exact for the
+    products of two SH of degree <= 3 (degree 6 in z, trigonometric degree
+    6 in phi)."""
+    z, wz = np.polynomial.legendre.leggauss(8)
+    phi = 2 * np.pi * np.arange(16) / 16
+    s = np.sqrt(1 - z * z)
+    dirs = np.stack([np.outer(s, np.cos(phi)), np.outer(s, np.sin(phi)), np.repeat(z[:, None], 16, 1)], -1)
+    w = np.repeat(wz[:, None] * (2 * np.pi / 16), 16, 1)
+    return dirs.reshape(-1, 3), w.reshape(-1)
+
+
+def test_sh_basis_is_orthonormal_on_the_sphere():
+    """The oracle's SH table comes from the closed-form normalisations; over
+    the sphere the 16 functions are orthonormal, and degree 1 carries the
+    Condon-Shortley signs (-y, z, -x)."""
+    dirs, w = _sphere_quadrature()
+    b = orc.gs_sh(dirs)[0]
+    gram = (b * w[:, None]).T @ b
+    np.testing.assert_allclose(gram, np.eye(16), atol=1e-12)
+    k1 = np.sqrt(3 / (4 * np.pi))
+    np.testing.assert_allclose(b[:, 1:4], k1 * np.stack([-dirs[:, 1], dirs[:, 2], -dirs[:, 0]], 1), atol=1e-15)
+    np.testing.assert_allclose(b[:, 0], 0.5 / np.sqrt(np.pi), atol=1e-16)
+
+
+def test_sh_partials_match_central_differences():
+    rng = np.random.default_rng(3)
+    pts = rng.normal(size=(50, 3))
+    _, gx, gy, gz = orc.gs_sh(pts)
+    h = 1e-6
+    for axis, g in enumerate((gx, gy, gz)):
+        e = np.zeros(3)
+        e[axis] = h
+        fd = (orc.gs_sh(pts + e)[0] - orc.gs_sh(pts - e)[0]) / (2 * h)
+        np.testing.assert_allclose(g, fd, atol=1e-7, rtol=1e-7)
+
+
+def test_quaternion_rotation_and_its_gradient():
+    rng = np.random.default_rng(4)
+    # a quarter turn about z takes x to y
+    q = np.array([np.cos(np.pi / 4), 0, 0, np.sin(np.pi / 4)])
+    R, _ = orc.gs_rot(q, np.zeros(9))
+    np.testing.assert_allclose(R @ [1, 0, 0], [0, 1, 0], atol=1e-15)
+    for _ in range(20):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        G = rng.normal(size=(3, 3))
+        R, dq = orc.gs_rot(q, G)
+        np.testing.assert_allclose(R @ R.T, np.eye(3), atol=1e-14)
+        assert abs(np.linalg.det(R) - 1) < 1e-14
+        # R(q) is a polynomial in q; differentiate sum G * R without renormalising
+        fd = np.zeros(4)
+        for k in range(4):
+            e = np.zeros(4)
+            e[k] = 1e-6
+            fd[k] = ((G * orc.gs_rot(q + e, G)[0]).sum() - (G * orc.gs_rot(q - e, G)[0]).sum()) / 2e-6
+        np.testing.assert_allclose(dq, fd, atol=1e-8)
