@@ -31,7 +31,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 800, 8, 32, 3  # config 2
+N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 800, 8, 32, 3  # 200k Gaussians SH3, 800x800, 8 of 32 views
 P_USED = 59          # floats per Gaussian used by the model
 # DRAM traffic of one backward-raster launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # 1-pass ncu capture of this workload (13,727,114 pairs): scaled to a launch by its pair count.
@@ -123,8 +123,8 @@ def step_bytes(V, N, K, npx):
 def build_scene(dev):
     import torch
 
-    from nprush_b200.gaussians import GaussianTrainer, config2_cameras, random_gaussians
-    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    from nprush_b200.gaussians import GaussianTrainer, orbit_cameras, random_gaussians
+    vp, vpi = orbit_cameras(CAMS, WIDTH, HEIGHT)
     teacher = GaussianTrainer(N_TEACHER, sh_degree=SH_DEG, device=dev, params=random_gaussians(N_TEACHER, 11))
     tg = torch.zeros((CAMS, HEIGHT, WIDTH, 4), device=f"cuda:{dev}")
     teacher.set_image_size(WIDTH, HEIGHT)
@@ -228,8 +228,8 @@ def cpu_baseline_port():
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc  # checker / baseline only
 
-    from nprush_b200.gaussians import config2_cameras, random_gaussians, view_records
-    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    from nprush_b200.gaussians import orbit_cameras, random_gaussians, view_records
+    vp, vpi = orbit_cameras(CAMS, WIDTH, HEIGHT)
     views = view_records(vp[:1], vpi[:1])
     teacher = random_gaussians(N_TEACHER, 11)
     timg, _ = orc.gs_forward(teacher, SH_DEG, views, WIDTH, HEIGHT)
@@ -262,7 +262,7 @@ def run_reference(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import build_ref
 
-    from nprush_b200.gaussians import config2_cameras
+    from nprush_b200.gaussians import orbit_cameras
     n = N_GAUSS
     so = sorted((ROOT / "oracle" / "_ref").glob(f"splat_backward_n{n}_*.so"))
     so_step = sorted((ROOT / "oracle" / "_ref").glob(f"splat_step_n{n}_*.so"))
@@ -281,7 +281,7 @@ def run_reference(args):
     q = rng.normal(size=(n, 4))
     s[:, 8:12] = q / np.linalg.norm(q, axis=1, keepdims=True)
     s[:, 13], s[:, 14] = 2.0, 0.5
-    vp, vpi = config2_cameras(CAMS, WIDTH, HEIGHT)
+    vp, vpi = orbit_cameras(CAMS, WIDTH, HEIGHT)
     tgt = np.zeros((HEIGHT, WIDTH, 4), np.float32)
     tgt[..., :3] = rng.random((HEIGHT, WIDTH, 3))
     dep = np.zeros((HEIGHT, WIDTH, 4), np.float32)
@@ -319,7 +319,7 @@ def run_reference(args):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "higher_is_better": True,
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": "reference splat_backward + splat_step (its own WGSL, translated to C++) at the "
-                                   "config-2 shape: 200k splats, 800x800, 8 views per step"},
+                                   "headline shape: 200k splats, 800x800, 8 views per step"},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "reference",
                              "sample": f"{len(tiles)} of {gx * gy} tiles of one view per timed sample "
                                        f"({t_tile * 1000:.0f} ms per tile), extrapolated x{gx * gy} tiles x{VIEWS} "
@@ -556,7 +556,7 @@ def main():
                     help="train: the Gaussian train step (headline); path_trace: path-traced target generation; "
                          "mesh_raster: the viewer's mesh render pass (colour + depth targets)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    # smaller shapes for profiler captures (the bench number is config 2 only)
+    # smaller shapes for profiler captures (the bench number is the 200k / 800x800 workload only)
     ap.add_argument("--gaussians", type=int, default=None)
     ap.add_argument("--res", type=int, default=None)
     ap.add_argument("--views", type=int, default=None)
@@ -634,7 +634,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded 200k-Gaussian student, targets rendered from a seeded 250k-Gaussian teacher",
-        "config": {"workload": (f"config 2: {N_GAUSS // 1000}k Gaussians SH3, {WIDTH}x{HEIGHT}, {VIEWS} of {CAMS} "
+        "config": {"workload": (f"{N_GAUSS // 1000}k Gaussians SH3, {WIDTH}x{HEIGHT}, {VIEWS} of {CAMS} "
                                 "sphere cameras per step, L1 + 0.2 D-SSIM, Adam"), "gaussians": N_GAUSS, "resolution": [WIDTH, HEIGHT],
                    "views_per_step": VIEWS,
                    "l2": "not flushed" if args.no_flush else "flushed between timed steps (256 MB write)",

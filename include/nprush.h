@@ -197,7 +197,7 @@ int nps_bezier_opt_stats(nps_bezier_opt* opt, nps_stats* out);
 /* Sets the manager's stepCount (GpuBezierOptimizerManager.ts:398). */
 int nps_bezier_opt_set_step_count(nps_bezier_opt* opt, uint32_t count);
 
-/* ====================================== 3D Gaussians (north-star trainer)
+/* ====================================== 3D Gaussians (the trainer)
  * No counterpart in the reference, which fits linear-parameter generalised
  * splats; this trainer keeps the reference's fit-a-scene call pattern
  * (GpuSplatOptimizerManager: write params, write camera(s), set target(s),
@@ -293,7 +293,7 @@ int nps_gs_save(nps_gs* gs, const char* path);
 /* Number of Gaussians (changes with write_params, set_count, ADC and load). */
 int nps_gs_count(nps_gs* gs, uint32_t* count);
 int nps_gs_load(nps_gs* gs, const char* path);
-/* Adaptive density control (north-star plain ADC): prune Gaussians with
+/* Adaptive density control (the plain threshold rule): prune Gaussians with
  * opacity < prune_opacity; densify those whose average view-space gradient
  * norm (accumulated by backward, averaged over the views that saw them) is
  * >= grad_thresh — split into two (scales / 1.6, means drawn from the parent)

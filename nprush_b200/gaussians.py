@@ -1,4 +1,4 @@
-"""3D Gaussian trainer over libnprush_cuda (the north-star model).
+"""3D Gaussian trainer over libnprush_cuda (3D Gaussians with SH colour).
 
 Keeps the reference's fit-a-scene call pattern (GpuSplatOptimizerManager:
 write params -> write camera(s) -> set target(s) -> dispatch), for standard
@@ -341,6 +341,6 @@ class GaussianTrainer:
             pass
 
 
-def config2_cameras(n: int = 32, width: int = 800, height: int = 800, fov_deg: float = 50.0, radius: float = 4.0):
+def orbit_cameras(n: int = 32, width: int = 800, height: int = 800, fov_deg: float = 50.0, radius: float = 4.0):
     from .camera import sphere_cameras
     return sphere_cameras(n, radius, math.radians(fov_deg), width / height)

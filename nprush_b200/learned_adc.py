@@ -127,7 +127,7 @@ def main(argv=None):
 
     from . import _lib
     from .policy import AdcPolicy
-    from .train import config2_scene
+    from .train import teacher_scene
     stream = torch.cuda.Stream(0)
     ctx = _lib.context(0)
     _lib.call("nps_set_stream", ctx, stream.cuda_stream)
@@ -135,7 +135,7 @@ def main(argv=None):
 
     def scene(seed):
         # student and teacher seeds derived from the run seed
-        return config2_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=4 * a.gaussians,
+        return teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=4 * a.gaussians,
                              student_seed=seed, teacher_seed=seed + 1000)
 
     out = {}

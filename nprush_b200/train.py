@@ -1,6 +1,6 @@
 """Training driver for the Gaussian trainer (the fit-a-scene loop).
 
-Config-2 schedule: each step trains on `views` cameras taken from a per-epoch
+Schedule: each step trains on `views` cameras taken from a per-epoch
 seeded permutation of all cameras; ADC (densify / prune) every `adc.every`
 steps from `adc.start` up to `adc.stop`; PSNR over every camera at the end.
 
@@ -114,15 +114,15 @@ def fit(trainer, vp, vpi, steps: int, views: int = 8, seed: int = 0, adc: AdcSch
     return res
 
 
-def config2_scene(device: int = 0, n_student: int = 200_000, n_teacher: int = 250_000, width: int = 800,
+def teacher_scene(device: int = 0, n_student: int = 200_000, n_teacher: int = 250_000, width: int = 800,
                   height: int = 800, n_cams: int = 32, sh_degree: int = 3, capacity: int | None = None,
                   student_seed: int = 10, teacher_seed: int = 11):
-    """Seeded config-2 scene: cameras on a sphere, targets rendered on the GPU
+    """Seeded 200k / 800x800 training scene: cameras on a sphere, targets rendered on the GPU
     from a seeded teacher, a seeded student trainer with every target resident."""
     import torch
 
-    from .gaussians import GaussianTrainer, config2_cameras, random_gaussians
-    vp, vpi = config2_cameras(n_cams, width, height)
+    from .gaussians import GaussianTrainer, orbit_cameras, random_gaussians
+    vp, vpi = orbit_cameras(n_cams, width, height)
     teacher = GaussianTrainer(n_teacher, sh_degree=sh_degree, device=device,
                               params=random_gaussians(n_teacher, teacher_seed))
     tg = torch.zeros((n_cams, height, width, 4), device=f"cuda:{device}")
@@ -161,7 +161,7 @@ def main(argv=None):
     ctx = _lib.context(0)
     _lib.call("nps_set_stream", ctx, stream.cuda_stream)
     with torch.cuda.stream(stream):
-        vp, vpi, tg, st = config2_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=a.capacity)
+        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=a.capacity)
         adc = AdcSchedule(every=0 if a.no_adc else 100, start=a.adc_start, stop=a.adc_stop)
         psnr0 = evaluate_psnr(st, vp, vpi)
         r = fit(st, vp, vpi, a.steps, seed=a.seed, adc=adc, mode=a.mode, log_every=a.log_every)

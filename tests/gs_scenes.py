@@ -1,4 +1,4 @@
-"""Seeded Gaussian scenes for the tests (config-0/1 distribution: means
+"""Seeded Gaussian scenes for the tests (the small-case distribution: means
 U[-1,1]^3, log-scales N(-4, 0.5), random unit quaternions, opacity logits
 N(0,1), RGB U[0,1]; camera fov 60 deg at (0, 0, 4) looking at the origin)."""
 import math

@@ -120,7 +120,7 @@ def test_per_view_accumulation_matches_batched(trainer_cls):
 
 
 def test_gradients_match_fp64_central_differences(trainer_cls):
-    """Config-1 style check: 1024 Gaussians, 64x64, L1 + D-SSIM loss, CUDA
+    """Small-case check: 1024 Gaussians, 64x64, L1 + D-SSIM loss, CUDA
     gradients against FP64 central differences (h = 1e-4 relative)."""
     n, w, h, deg = 1024, 64, 64, 0
     p = gs_scene(n, 2, deg=deg, log_scale_mean=-3.5)
@@ -221,7 +221,7 @@ def test_graph_mode_matches_eager_and_recovers_from_overflow(trainer_cls):
 
 
 def test_deterministic_mode_is_bit_reproducible(trainer_cls, tmp_path):
-    """Config-1 setting (1024 Gaussians, 64x64) and a larger multi-view case:
+    """The small case (1024 Gaussians, 64x64) and a larger multi-view case:
     the two-pass backward gives bit-identical gradients run to run, agrees
     with the atomic reduction and the FP64 central differences, and a
     checkpointed run resumes bit-exactly."""
@@ -250,7 +250,7 @@ def test_deterministic_mode_is_bit_reproducible(trainer_cls, tmp_path):
         np.testing.assert_array_equal(grads[0][1], grads[1][1])
         a, b = grads[0][0].astype(np.float64), grads[2][0].astype(np.float64)
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
-    # config 1: deterministic gradients against FP64 central differences
+    # 1024 Gaussians at 64x64: deterministic gradients against FP64 central differences
     n, w, h = 1024, 64, 64
     p = gs_scene(n, 2, deg=0, log_scale_mean=-3.5)
     vp, vpi, views = gs_views(w, h)

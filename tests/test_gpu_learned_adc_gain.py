@@ -7,10 +7,10 @@ mode makes each training run reproducible, and the policy's training is too
 (its gradients are summed in a fixed order).  Checked: the learned rule ends
 with no more Gaussians than the plain one (1% slack) and no worse PSNR (0.2 dB
 slack).  At this scale the two rules differ by less than a change of the
-scene or of the policy's seeds moves them (this build: 41421 vs 41402
-Gaussians and 38.74 vs 38.63 dB; earlier builds 41302 vs 41402 and 39.05 vs
-38.63 dB, 41411 vs 41402 and 38.61 vs 38.63 dB), so no strict gain is
-asserted; the 30k-step comparison at config 2 is where the policy's effect
+scene or of the policy's seeds moves them (measured: 41421 vs 41402
+Gaussians and 38.74 vs 38.63 dB; with earlier kernel versions 41302 vs 41402
+and 39.05 vs 38.63 dB, 41411 vs 41402 and 38.61 vs 38.63 dB), so no strict gain is
+asserted; the 30k-step comparison at 200k Gaussians, 800x800, is where the policy's effect
 shows."""
 import numpy as np
 import pytest
@@ -25,13 +25,13 @@ def test_learned_adc_keeps_psnr_with_fewer_gaussians():
     build.build()
     from nprush_b200.learned_adc import AdcLog, hindsight_labels, logging_adc_fn, policy_adc_fn
     from nprush_b200.policy import AdcPolicy
-    from nprush_b200.train import AdcSchedule, config2_scene, evaluate_psnr, fit
+    from nprush_b200.train import AdcSchedule, teacher_scene, evaluate_psnr, fit
 
     adc = AdcSchedule(every=100, start=300, stop=1200)
     steps, views = 1200, 4
 
     def run(seed, adc_fn):
-        vp, vpi, tg, st = config2_scene(0, 20_000, 30_000, 256, 256, n_cams=16, sh_degree=1, capacity=60_000,
+        vp, vpi, tg, st = teacher_scene(0, 20_000, 30_000, 256, 256, n_cams=16, sh_degree=1, capacity=60_000,
                                         student_seed=seed, teacher_seed=seed + 1000)
         st.set_deterministic(True)
         st.assign_ids(0)

@@ -1,6 +1,6 @@
-"""CPU tests of the host-side logic around the kernels: the config-2 view
+"""CPU tests of the host-side logic around the kernels: the training view
 schedule, the ADC schedule, hindsight relabelling of logged ADC decisions,
-class weights and the config-3 curve generator."""
+class weights and the Bezier-fit curve generator."""
 import math
 
 import numpy as np
