@@ -54,7 +54,7 @@ class GpuBezierOptimizerManager:
         call("nps_bezier_opt_create", self._ctx, self.num_beziers, ctypes.byref(h))
         self._h = h.value
         self._keep = []
-        self._vp = None
+        self._vp = self._vp_inv = None  # last matrices written (host copies)
         if init is None:
             init = reference_init(self.num_beziers, seed)
         if init is not False:
@@ -92,9 +92,33 @@ class GpuBezierOptimizerManager:
 
     # ---- reference API
     def write_vp(self, vp, vp_inv):
+        """Both matrices at once ([V,]16 each, one pair per view)."""
         vp = np.ascontiguousarray(vp, np.float32).reshape(-1, 16)
         vpi = np.ascontiguousarray(vp_inv, np.float32).reshape(-1, 16)
+        if vp.shape != vpi.shape:
+            raise ValueError("vp and vp_inv must have the same number of views")
         call("nps_bezier_opt_write_vp", self._h, vp.ctypes.data, vpi.ctypes.data, vp.shape[0])
+        self._vp, self._vp_inv = vp.copy(), vpi.copy()
+
+    def write_vp_matrix(self, mat):
+        """writeVPMatrix (GpuBezierOptimizerManager.ts:269-277): the view-projection
+        alone.  The inverse keeps its last value; one never written reads as
+        zeros, as in the reference's zero-initialised uniform buffer (also when
+        the number of views changes, until write_vp_inv_matrix follows)."""
+        vp = np.ascontiguousarray(mat, np.float32).reshape(-1, 16)
+        vpi = self._vp_inv
+        if vpi is None or vpi.shape != vp.shape:
+            vpi = np.zeros_like(vp)
+        self.write_vp(vp, vpi)
+
+    def write_vp_inv_matrix(self, mat):
+        """writeVPInvMatrix (GpuBezierOptimizerManager.ts:279-288): the inverse
+        alone, the view-projection kept (zeros if never written)."""
+        vpi = np.ascontiguousarray(mat, np.float32).reshape(-1, 16)
+        vp = self._vp
+        if vp is None or vp.shape != vpi.shape:
+            vp = np.zeros_like(vpi)
+        self.write_vp(vp, vpi)
 
     def write_mode(self, mode: float = 0.0):
         call("nps_bezier_opt_write_mode", self._h, float(mode))
@@ -180,6 +204,8 @@ class GpuBezierOptimizerManager:
             pass
 
     # camelCase aliases (the reference's method names)
+    writeVPMatrix = write_vp_matrix
+    writeVPInvMatrix = write_vp_inv_matrix
     writeMode = write_mode
     writeBgPenalty = write_bg_penalty
     writeMaxWidth = write_max_width

@@ -5,6 +5,8 @@ GpuSplatOptimizerManager  <->  src/lib/gpu/GpuSplatOptimizerManager.ts
     writeSplatVPMatrix(vp, vpInv)   -> write_splat_vp_matrix(vp, vp_inv)
     setBackwardTarget(c, d, w, h)   -> set_backward_target(rgba, depth, w, h)
     dispatch(encoder)               -> dispatch()
+    setEdgeTarget(depth, edge)      -> set_edge_target(depth, edge)
+    dispatchEdge(encoder, w, h)     -> dispatch_edge(w, h)
 Same names (camelCase aliases included), same argument meaning; the reference
 reports errors asynchronously and silently skips dispatch without a target
 (GpuSplatOptimizerManager.ts:366) — here every call raises NpsError instead.
@@ -81,6 +83,7 @@ class GpuSplatOptimizerManager:
         call("nps_splat_opt_create", self._ctx, self.num_splats, ctypes.byref(h))
         self._h = h.value
         self._keep = []
+        self._edge = None
         self.dims = (0, 0)
         if init is None:
             init = reference_init(self.num_splats, seed)
@@ -149,6 +152,32 @@ class GpuSplatOptimizerManager:
     def dispatch(self):
         call("nps_splat_opt_dispatch", self._h)
 
+    def set_edge_target(self, depth, edge):
+        """setEdgeTarget(depthView, edgeView) (GpuSplatOptimizerManager.ts:319-328):
+        binds a depth image and the edge image that dispatch_edge writes, both
+        torch CUDA float32 [H,W,4] tensors (depth in channel 0), held like the
+        texture views of a bind group."""
+        if tuple(depth.shape) != tuple(edge.shape):
+            raise ValueError(f"depth {tuple(depth.shape)} and edge {tuple(edge.shape)} images differ in shape")
+        self._edge = (depth, edge)
+
+    def dispatch_edge(self, width: int, height: int, quantize: bool = True):
+        """dispatchEdge(encoder, width, height) (GpuSplatOptimizerManager.ts:390-400):
+        the Sobel depth-edge pass (splat_edge.wgsl) over the bound images.  The
+        reference dispatches ceil(w/16) x ceil(h/16) workgroups and the shader
+        stops at the depth texture's size; its viewer always passes that size
+        (GpuRunner.svelte.ts:686, :760), and a dispatch that does not cover the
+        image is refused here.  quantize: the edge texture is rgba8unorm."""
+        from . import targets
+        edge = self._edge
+        if edge is None:
+            raise _lib.NpsError(-6, "dispatch_edge: no edge target (set_edge_target first)")
+        depth, out = edge
+        h, w = int(depth.shape[0]), int(depth.shape[1])
+        if (int(width) + 15) // 16 * 16 < w or (int(height) + 15) // 16 * 16 < h:
+            raise ValueError(f"dispatch_edge({width}, {height}) does not cover the {w}x{h} edge target")
+        targets.splat_edge(depth, out, quantize=quantize)
+
     # ---- the three stages of dispatch, separately
     def backward(self, out_rgbd=None):
         """splat_backward over all views; out_rgbd: optional torch CUDA tensor
@@ -204,3 +233,5 @@ class GpuSplatOptimizerManager:
     # camelCase aliases (the reference's method names)
     writeSplatVPMatrix = write_splat_vp_matrix
     setBackwardTarget = set_backward_target
+    setEdgeTarget = set_edge_target
+    dispatchEdge = dispatch_edge

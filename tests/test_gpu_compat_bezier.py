@@ -155,3 +155,33 @@ def test_dispatch_runs_and_learns(cls):
     m.backward(out_rgbd=img)
     e1 = float(np.abs(img.cpu().numpy()[0, ..., :3] - 0.8).mean())
     assert e1 < e0, (e0, e1)
+
+
+def test_separate_vp_writes_equal_the_combined_write(cls):
+    """writeVPMatrix then writeVPInvMatrix (either order) leaves the same
+    uniforms as writing both at once: the dispatched states are bit-identical."""
+    n, w, h = 500, 64, 48
+    from nprush_b200.bezier import reference_init
+    b = reference_init(n, 5)
+    vp, vpi = camera(w, h, dist=1.5, eye=(0.3, -0.2, 1.5))
+    tgt, depth, bg, bgd, nrm = bezier_textures(w, h, 6)
+    states = []
+    for order in ("both", "vp_first", "inv_first"):
+        m = cls(n, init=b)
+        if order == "both":
+            m.write_vp(vp, vpi)
+        elif order == "vp_first":
+            m.writeVPMatrix(vp)
+            m.writeVPInvMatrix(vpi)
+        else:
+            m.write_vp_inv_matrix(vpi)
+            m.write_vp_matrix(vp)
+        m.write_mode(1.0)
+        m.set_backward_target(tgt, depth, bg, bgd, nrm, w, h)
+        for _ in range(3):
+            m.dispatch()
+        states.append(m.read_state())
+        m.close()
+    for st in states[1:]:
+        for k in ("beziers", "adam_m", "adam_v", "grad_accum"):
+            np.testing.assert_array_equal(st[k], states[0][k])

@@ -198,3 +198,29 @@ def test_dispatch_tracks_oracle(mgr_cls):
     assert (live_ref != live_gpu).sum() <= 3
     both = live_ref & live_gpu
     assert np.abs(st["splats"][both] - rs[both]).max() < 0.05
+
+
+def test_edge_target_and_dispatch_edge(mgr_cls):
+    """setEdgeTarget + dispatchEdge: the splat edge pass over the bound depth
+    image into an rgba8unorm-like edge image equals the reference shader's
+    output (tests/golden/preprocess.npz) at 8-bit levels; no target, or a
+    dispatch that does not cover the image, raises."""
+    from pathlib import Path
+
+    from nprush_b200._lib import NpsError
+    d = np.load(Path(__file__).resolve().parent / "golden" / "preprocess.npz")
+    z = torch.from_numpy(d["depth"]).cuda()
+    h, w = z.shape[:2]
+    m = mgr_cls(64)
+    with pytest.raises(NpsError):
+        m.dispatch_edge(w, h)
+    out = torch.zeros_like(z)
+    m.setEdgeTarget(z, out)
+    with pytest.raises(ValueError):
+        m.dispatch_edge(w - 16, h)
+    m.dispatchEdge(w, h)
+    got = out.cpu().numpy()
+    raw = np.clip(d["edge"], 0, 1) * 255
+    on_edge = np.abs(raw - np.floor(raw) - 0.5) < 1e-5 * 255
+    assert np.all((got == np.rint(raw) / 255) | on_edge)
+    m.close()
