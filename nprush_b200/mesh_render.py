@@ -85,6 +85,8 @@ class MeshRenderer:
         self.uniforms[16:32] = np.asarray(m, np.float32).reshape(16)
 
     def write_shading_mode(self, mode: str):
+        if mode not in ("normals", "shaded"):  # the reference's parameter type
+            raise ValueError(f"shading mode {mode!r}: 'normals' or 'shaded'")
         self.uniforms[32] = 0.0 if mode == "normals" else 1.0
 
     def write_inv_view_proj_mat(self, m):
@@ -117,3 +119,14 @@ class MeshRenderer:
             self._destroy()
         except Exception:
             pass
+
+    # camelCase aliases (the reference's method names)
+    setGroundMesh = set_ground_mesh
+    setPbrMesh = set_pbr_mesh
+    writeViewProjMat = write_view_proj_mat
+    writeViewMat = write_view_mat
+    writeShadingMode = write_shading_mode
+    writeInvViewProjMat = write_inv_view_proj_mat
+
+
+GpuMeshRenderPipelineManager = MeshRenderer

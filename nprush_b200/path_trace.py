@@ -138,3 +138,11 @@ class PathTracer:
             self._destroy()
         except Exception:
             pass
+
+    # camelCase aliases (the reference's method names)
+    setMeshes = set_meshes
+    setOutputSize = set_output_size
+    writeInvViewProjMat = write_inv_view_proj_mat
+
+
+GpuPathTracePipelineManager = PathTracer
