@@ -213,3 +213,41 @@ class GpuBezierOptimizerManager:
     setAdcPeriod = set_adc_period
     writeNoKill = write_no_kill
     setBackwardTarget = set_backward_target
+
+
+class GpuBezierForwardPipelineManager:
+    """GpuBezierForwardPipelineManager (src/lib/gpu/GpuBezierForwardPipelineManager.ts),
+    headless: draws the curves of an optimiser's bezierBuffer into one RGBA
+    image.  The reference's constructor({device, numBeziers, bezierBuffer,
+    brushTexture}) takes the optimiser's buffer and the brush texture
+    (GpuRunner.svelte.ts:210-229); here the optimiser and the brush as a torch
+    CUDA [bh, bw] float32 image (None: analytic coverage only)."""
+
+    def __init__(self, optimizer: GpuBezierOptimizerManager, brush=None):
+        self._opt = optimizer
+        self._brush = brush
+        self._vp = np.zeros(16, np.float32)  # the uniform buffer starts zeroed
+        self._target = None
+
+    def write_vp_matrix(self, mat):
+        """writeVPMatrix (:102-110)."""
+        self._vp = np.ascontiguousarray(mat, np.float32).reshape(16).copy()
+
+    def set_target(self, target, width: int, height: int):
+        """setTarget(view, w, h) (:112-129): a torch CUDA float32 [H,W,4] image."""
+        if tuple(target.shape) != (height, width, 4):
+            raise ValueError(f"target shape {tuple(target.shape)} does not match {height}x{width}x4")
+        self._target = (target, int(width), int(height))
+
+    def dispatch(self, clear: bool = True):
+        """dispatch(encoder, clear) (:131-148): clear = cleared to 0 first;
+        otherwise the curves are composited over the image's current contents
+        (the render pass's "load")."""
+        if self._target is None:
+            raise _lib.NpsError(-6, "bezier forward dispatch: no target (set_target first)")
+        out, w, h = self._target
+        background = None if clear else out.clone()
+        self._opt.render(self._vp, w, h, out, background=background, brush=self._brush)
+
+    writeVPMatrix = write_vp_matrix
+    setTarget = set_target

@@ -235,3 +235,43 @@ class GpuSplatOptimizerManager:
     setBackwardTarget = set_backward_target
     setEdgeTarget = set_edge_target
     dispatchEdge = dispatch_edge
+
+
+class GpuSplatForwardPipelineManager:
+    """GpuSplatForwardPipelineManager (src/lib/gpu/GpuSplatForwardPipelineManager.ts),
+    headless: draws the splats of an optimiser's splatBuffer into a colour and
+    a depth image.  The reference's constructor({device, numSplats,
+    splatBuffer}) takes the optimiser's buffer (GpuRunner.svelte.ts:204-208);
+    here the optimiser itself."""
+
+    def __init__(self, optimizer: GpuSplatOptimizerManager):
+        self._opt = optimizer
+        self._vp = np.zeros(16, np.float32)  # the uniform buffer starts zeroed
+        self._target = None
+
+    def write_vp_matrix(self, mat):
+        """writeVPMatrix (:94-102)."""
+        self._vp = np.ascontiguousarray(mat, np.float32).reshape(16).copy()
+
+    def set_target(self, color, depth, width: int, height: int):
+        """setTarget(colorView, depthView, w, h) (:104-112): torch CUDA float32
+        [H,W,4] images."""
+        for t in (color, depth):
+            if tuple(t.shape) != (height, width, 4):
+                raise ValueError(f"target shape {tuple(t.shape)} does not match {height}x{width}x4")
+        self._target = (color, depth, int(width), int(height))
+
+    def dispatch(self, clear: bool = False):
+        """dispatch(encoder, clear) (:114-137).  Only the cleared pass exists
+        here (colour 0.05, depth 1, then every splat), the one the viewer draws
+        (GpuRunner.svelte.ts:706); a pass that loads the previous contents is
+        refused rather than approximated."""
+        if self._target is None:
+            raise _lib.NpsError(-6, "splat forward dispatch: no target (set_target first)")
+        if not clear:
+            raise ValueError("splat forward dispatch: only clear=True is provided")
+        color, depth, w, h = self._target
+        self._opt.render(self._vp, w, h, color, depth)
+
+    writeVPMatrix = write_vp_matrix
+    setTarget = set_target

@@ -43,3 +43,44 @@ def test_bezier_render_matches_oracle(n, w, h, seed, use_bg, use_brush):
     ref = orc.bezier_render(b, vp, w, h, bg=bg if use_bg else None, brush=brush)
     np.testing.assert_allclose(out.cpu().numpy(), ref, atol=1e-5, rtol=0)
     assert ref[..., 3].max() > 0.3  # strokes visible
+
+
+def test_forward_pipeline_managers():
+    """GpuSplatForwardPipelineManager / GpuBezierForwardPipelineManager
+    (writeVPMatrix, setTarget, dispatch) against the oracle: the cleared
+    splat pass, the cleared Bezier pass and the Bezier pass that loads the
+    target's contents (composited over them)."""
+    from nprush_b200._lib import NpsError
+    from nprush_b200.bezier import GpuBezierForwardPipelineManager, GpuBezierOptimizerManager
+    from nprush_b200.splat import GpuSplatForwardPipelineManager, GpuSplatOptimizerManager
+    w, h = 80, 64
+    s = splat_scene(500, 5, alive=480, random_shape=True)
+    vp, _ = camera(w, h)
+    fwd = GpuSplatForwardPipelineManager(GpuSplatOptimizerManager(500, init=s))
+    with pytest.raises(NpsError):
+        fwd.dispatch(True)
+    rgba = torch.zeros((h, w, 4), device="cuda")
+    dep = torch.zeros((h, w, 4), device="cuda")
+    fwd.writeVPMatrix(vp)
+    fwd.setTarget(rgba, dep, w, h)
+    with pytest.raises(ValueError):
+        fwd.dispatch()  # the reference's default is a loading pass
+    fwd.dispatch(True)
+    r_rgba, r_dep = orc.splat_render(s, vp, w, h)
+    np.testing.assert_allclose(rgba.cpu().numpy(), r_rgba, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(dep.cpu().numpy(), r_dep, atol=1e-5, rtol=0)
+
+    b = bezier_scene(400, 6)
+    vp, _ = camera(w, h, dist=1.4)
+    brush = np.random.default_rng(6).random((16, 32)).astype(np.float32)
+    bfwd = GpuBezierForwardPipelineManager(GpuBezierOptimizerManager(400, init=b), brush=torch.from_numpy(brush).cuda())
+    out = torch.full((h, w, 4), 0.7, device="cuda")
+    bfwd.writeVPMatrix(vp)
+    bfwd.setTarget(out, w, h)
+    bfwd.dispatch()  # cleared
+    np.testing.assert_allclose(out.cpu().numpy(), orc.bezier_render(b, vp, w, h, bg=None, brush=brush), atol=1e-5, rtol=0)
+    _, _, bg, _, _ = bezier_textures(w, h, 7)
+    bg[..., 3] = 1.0
+    out.copy_(torch.from_numpy(bg))
+    bfwd.dispatch(clear=False)
+    np.testing.assert_allclose(out.cpu().numpy(), orc.bezier_render(b, vp, w, h, bg=bg, brush=brush), atol=1e-5, rtol=0)

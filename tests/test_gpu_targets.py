@@ -72,3 +72,27 @@ def test_bad_arguments_are_rejected(tg):
         tg.blur(a, a, (1, 0), 2, 1.0)  # in place
     with pytest.raises(NpsError):
         tg.blur(a, torch.zeros_like(a), (1, 0), 2, 0.0)  # sigma 0
+
+
+def test_blur_manager_classes(tg):
+    """GpuBlurPipelineManager.blur runs the horizontal pass into the temp
+    image and the vertical pass into dst, with 8-bit levels between them:
+    equal to those two single passes (each pinned to the reference shader by
+    test_blur).  The depth-aware manager at radius 3 matches the reference's
+    8-bit levels of the fixture."""
+    d = np.load(GOLD)
+    src = torch.from_numpy(d["color"]).cuda()
+    h, w = src.shape[:2]
+    temp, dst = torch.zeros_like(src), torch.zeros_like(src)
+    tg.GpuBlurPipelineManager().blur(src, dst, temp, w, h, 6, 3.0, is_srgb=True)
+    t2, d2 = torch.zeros_like(src), torch.zeros_like(src)
+    tg.blur(src, t2, (1, 0), 6, 3.0, tg.SRGB_IN, quantize=True)
+    tg.blur(t2, d2, (0, 1), 6, 3.0, tg.SRGB_OUT, quantize=True)
+    assert torch.equal(temp, t2) and torch.equal(dst, d2)
+    with pytest.raises(ValueError):
+        tg.GpuBlurPipelineManager().blur(src, dst, temp, w + 1, h, 6, 3.0)
+    z = torch.from_numpy(d["depth"]).cuda()
+    k = [int(r) for r in d["depth_blur_radii"]].index(3)
+    out = torch.zeros_like(src)
+    tg.GpuDepthAwareBlurPipelineManager().blur(src, z, out, w, h, 3)
+    check_q(out.cpu().numpy(), d[f"depth_blur{k}"])

@@ -7,7 +7,7 @@ import types
 import numpy as np
 import pytest
 
-from nprush_b200 import bezier, mesh_render, path_trace, splat
+from nprush_b200 import bezier, mesh_render, path_trace, splat, targets
 
 # reference class -> (mirror class, public methods of the reference class)
 REFERENCE_METHODS = {
@@ -23,6 +23,13 @@ REFERENCE_METHODS = {
     # GpuPathTracePipelineManager.ts:101-247
     "GpuPathTracePipelineManager": (path_trace.GpuPathTracePipelineManager,
                                     ["setMeshes", "setOutputSize", "reset", "writeInvViewProjMat", "dispatch"]),
+    # GpuSplatForwardPipelineManager.ts:94-137, GpuBezierForwardPipelineManager.ts:102-148
+    "GpuSplatForwardPipelineManager": (splat.GpuSplatForwardPipelineManager, ["writeVPMatrix", "setTarget", "dispatch"]),
+    "GpuBezierForwardPipelineManager": (bezier.GpuBezierForwardPipelineManager,
+                                        ["writeVPMatrix", "setTarget", "dispatch"]),
+    # GpuBlurPipelineManager.ts:46-99, GpuDepthAwareBlurPipelineManager.ts:41-70
+    "GpuBlurPipelineManager": (targets.GpuBlurPipelineManager, ["blur"]),
+    "GpuDepthAwareBlurPipelineManager": (targets.GpuDepthAwareBlurPipelineManager, ["blur"]),
     # GpuMeshRenderPipelineManager.ts:127-247 and GpuUniformsBufferManager.ts:59-93
     # (addDraw of the mesh and envmap managers: render())
     "GpuMeshRenderPipelineManager": (mesh_render.GpuMeshRenderPipelineManager,
