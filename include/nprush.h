@@ -102,6 +102,13 @@ int nps_splat_opt_adc(nps_splat_opt* opt);
  * are device buffers of h*w*4 floats each (depth replicated in rgb, alpha in a). */
 int nps_splat_opt_render(nps_splat_opt* opt, const float* vp, uint32_t width, uint32_t height, float* out_rgba,
                          float* out_depth);
+/* GpuSplatForwardPipelineManager.dispatch(enc, clear=false), the pass that
+ * loads its attachments: the same draw blended over the current contents of
+ * rgba and depth (device h*w*4 floats each, read and written in place; depth
+ * may be null), colour alpha and depth alpha accumulating as a + dst.a (1 - a)
+ * per fragment (the pipeline's blend state, GpuSplatForwardPipelineManager.ts:64-77). */
+int nps_splat_opt_render_load(nps_splat_opt* opt, const float* vp, uint32_t width, uint32_t height, float* rgba,
+                              float* depth);
 /* Device pointers of the library-owned buffers (splatBuffer, gradBuffer,
  * Adam m / v, grad_accum), for zero-copy access; valid until destroy. */
 int nps_splat_opt_buffers(nps_splat_opt* opt, float** splats, int32_t** grads, float** adam_m, float** adam_v,

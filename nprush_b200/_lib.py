@@ -53,6 +53,7 @@ SIGNATURES = {
     "nps_splat_opt_step": [P],
     "nps_splat_opt_adc": [P],
     "nps_splat_opt_render": [P, P, U32, U32, P, P],
+    "nps_splat_opt_render_load": [P, P, U32, U32, P, P],
     "nps_splat_opt_buffers": [P, PP, PP, PP, PP, PP],
     "nps_splat_opt_stats": [P, ctypes.POINTER(nps_stats)],
     "nps_splat_opt_set_step_count": [P, U32],

@@ -724,7 +724,7 @@ __global__ void __launch_bounds__(256) k_render_raster(const float* __restrict__
                                                        const uint32_t* __restrict__ rstart,
                                                        const uint32_t* __restrict__ rend, uint32_t w, uint32_t h,
                                                        uint32_t tiles_x, float4* __restrict__ out_rgba,
-                                                       float4* __restrict__ out_depth) {
+                                                       float4* __restrict__ out_depth, int load) {
   __shared__ float4 sr[256][4];
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, tid = threadIdx.x;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
@@ -763,9 +763,18 @@ __global__ void __launch_bounds__(256) k_render_raster(const float* __restrict__
   }
   if (inside) {
     const size_t pix = (size_t)py * w + px;
-    out_rgba[pix] = make_float4(C0 + T * 0.05f, C1 + T * 0.05f, C2 + T * 0.05f, 1.0f);
-    const float dd = D + T * 1.0f;
-    if (out_depth) out_depth[pix] = make_float4(dd, dd, dd, 1.0f);
+    if (!load) {  // attachments cleared to colour (0.05, 0.05, 0.05, 1), depth 1
+      out_rgba[pix] = make_float4(C0 + T * 0.05f, C1 + T * 0.05f, C2 + T * 0.05f, 1.0f);
+      const float dd = D + T * 1.0f;
+      if (out_depth) out_depth[pix] = make_float4(dd, dd, dd, 1.0f);
+    } else {  // over the attachments' current contents; alpha = a + dst.a (1 - a) per fragment
+      const float4 c = out_rgba[pix];
+      out_rgba[pix] = make_float4(C0 + T * c.x, C1 + T * c.y, C2 + T * c.z, (1.0f - T) + T * c.w);
+      if (out_depth) {
+        const float4 d = out_depth[pix];
+        out_depth[pix] = make_float4(D + T * d.x, D + T * d.y, D + T * d.z, (1.0f - T) + T * d.w);
+      }
+    }
   }
 }
 
@@ -1143,8 +1152,8 @@ int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
 }  // extern "C"
 
 // ================================================================ render
-extern "C" int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
-                                    float* out_depth) {
+static int splat_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba, float* out_depth,
+                        int load) {
   NPS_TRY(check_opt(o));
   if (!vp || !out_rgba || w == 0 || h == 0 || w > 16 * 65535 || h > 16 * 65535) {
     set_error("splat render: bad arguments");
@@ -1198,9 +1207,19 @@ extern "C" int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t 
     vs = vv;
   }
   compat::k_render_raster<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(rw.rec.as<float>(), vs, rstart, rend, w, h, tiles_x,
-                                                                  (float4*)out_rgba, (float4*)out_depth);
+                                                                  (float4*)out_rgba, (float4*)out_depth, load);
   NPS_CHECK_LAUNCH();
   return NPS_OK;
+}
+
+extern "C" int nps_splat_opt_render(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
+                                    float* out_depth) {
+  return splat_render(o, vp, w, h, out_rgba, out_depth, 0);
+}
+
+extern "C" int nps_splat_opt_render_load(nps_splat_opt* o, const float* vp, uint32_t w, uint32_t h, float* rgba,
+                                         float* depth) {
+  return splat_render(o, vp, w, h, rgba, depth, 1);
 }
 
 // ============================================ ADC without device allocation

@@ -191,14 +191,19 @@ class GpuSplatOptimizerManager:
         if out_rgbd is not None:
             self.sync()  # torch reads the image on its own stream
 
-    def render(self, vp, width: int, height: int, out_rgba, out_depth=None):
-        """Headless GpuSplatForwardPipelineManager.dispatch(enc, clear=true):
-        out_rgba / out_depth: torch CUDA [H,W,4] float tensors."""
+    def render(self, vp, width: int, height: int, out_rgba, out_depth=None, load: bool = False):
+        """Headless GpuSplatForwardPipelineManager.dispatch(enc, clear=not load):
+        out_rgba / out_depth: torch CUDA [H,W,4] float tensors, cleared first
+        or, with load=True, blended over in place."""
         import torch
         torch.cuda.current_stream(out_rgba.device).synchronize()
+        for t in (out_rgba, out_depth):
+            if t is not None and (tuple(t.shape) != (height, width, 4) or t.dtype != torch.float32
+                                  or not t.is_cuda or not t.is_contiguous()):
+                raise ValueError(f"render target must be a contiguous CUDA float32 [{height},{width},4] tensor")
         vp = np.ascontiguousarray(vp, np.float32).reshape(16)
-        call("nps_splat_opt_render", self._h, vp.ctypes.data, width, height, out_rgba.data_ptr(),
-             None if out_depth is None else out_depth.data_ptr())
+        call("nps_splat_opt_render_load" if load else "nps_splat_opt_render", self._h, vp.ctypes.data, width, height,
+             out_rgba.data_ptr(), None if out_depth is None else out_depth.data_ptr())
         self.sync()
 
     def step(self):
@@ -262,16 +267,14 @@ class GpuSplatForwardPipelineManager:
         self._target = (color, depth, int(width), int(height))
 
     def dispatch(self, clear: bool = False):
-        """dispatch(encoder, clear) (:114-137).  Only the cleared pass exists
-        here (colour 0.05, depth 1, then every splat), the one the viewer draws
-        (GpuRunner.svelte.ts:706); a pass that loads the previous contents is
-        refused rather than approximated."""
+        """dispatch(encoder, clear) (:114-137): clear = attachments cleared to
+        colour (0.05, 0.05, 0.05, 1) and depth 1 first (the pass the viewer
+        draws, GpuRunner.svelte.ts:706); otherwise the splats are blended over
+        the images' current contents."""
         if self._target is None:
             raise _lib.NpsError(-6, "splat forward dispatch: no target (set_target first)")
-        if not clear:
-            raise ValueError("splat forward dispatch: only clear=True is provided")
         color, depth, w, h = self._target
-        self._opt.render(self._vp, w, h, color, depth)
+        self._opt.render(self._vp, w, h, color, depth, load=not clear)
 
     writeVPMatrix = write_vp_matrix
     setTarget = set_target

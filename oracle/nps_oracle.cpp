@@ -982,23 +982,16 @@ namespace {
 inline bool in_quad(V2 p, float x0, float x1, float y0, float y1) {
   return p.x >= x0 && p.x < x1 && p.y > y0 && p.y <= y1;
 }
-}  // namespace
+// Per-splat screen quad of splat_forward.wgsl's vertex stage (vert, :43-117):
+// centre, extent rectangle, conic and encoded depth; ok = false when culled.
+struct SplatQuad { bool ok; float cx, cy, x0, x1, y0, y1, A, B, C, depth; };
 
-extern "C" {
-
-// splat_forward.wgsl:42-156 with GpuSplatForwardPipelineManager.dispatch(clear)
-// (GpuSplatForwardPipelineManager.ts:114-137), headless and in fp32: instances
-// are drawn in reverse index order with src-alpha blending, which equals
-// front-to-back compositing with splat 0 in front.  out_rgba / out_depth:
-// H x W x 4 (colour rgb + alpha; encoded depth in rgb + alpha).
-int orc_splat_render(const float* splats, uint32_t n, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
-                     float* out_depth) {
+std::vector<SplatQuad> splat_quads(const float* splats, uint32_t n, const float* vp, uint32_t w, uint32_t h) {
   const float aspect = (float)w / (float)h;
-  struct Q { bool ok; float cx, cy, x0, x1, y0, y1, A, B, C, depth; };
-  std::vector<Q> q(n);
+  std::vector<SplatQuad> q(n);
   for (uint32_t i = 0; i < n; ++i) {
     const float* s = splats + 16 * (size_t)i;
-    Q& o = q[i];
+    SplatQuad& o = q[i];
     o.ok = false;
     const float sx = std::fmax(s[3], 0.0001f), sy = std::fmax(s[12], 0.0001f), sz = std::fmax(s[15], 0.0001f);
     const float safe_b = std::fmax(s[14], 0.0001f);
@@ -1028,13 +1021,28 @@ int orc_splat_render(const float* splats, uint32_t n, const float* vp, uint32_t 
     o.depth = clampf(1.0f - 0.1f / ld, 0.0f, 1.0f);
     o.ok = true;
   }
+  return q;
+}
+}  // namespace
+
+extern "C" {
+
+// splat_forward.wgsl:42-156 with GpuSplatForwardPipelineManager.dispatch(clear)
+// (GpuSplatForwardPipelineManager.ts:114-137), headless and in fp32: instances
+// are drawn in reverse index order with src-alpha blending, which equals
+// front-to-back compositing with splat 0 in front.  out_rgba / out_depth:
+// H x W x 4 (colour rgb + alpha; encoded depth in rgb + alpha).
+int orc_splat_render(const float* splats, uint32_t n, const float* vp, uint32_t w, uint32_t h, float* out_rgba,
+                     float* out_depth) {
+  const float aspect = (float)w / (float)h;
+  const std::vector<SplatQuad> q = splat_quads(splats, n, vp, w, h);
 #pragma omp parallel for schedule(dynamic, 8)
   for (long pl = 0; pl < (long)w * h; ++pl) {
     const uint32_t px = (uint32_t)(pl % w), py = (uint32_t)(pl / w);
     V2 p = pixel_to_p(px, py, w, h, aspect);
     float T = 1.0f, C[3] = {0, 0, 0}, D = 0.0f;
     for (uint32_t i = 0; i < n; ++i) {
-      const Q& o = q[i];
+      const SplatQuad& o = q[i];
       if (!o.ok || !in_quad(p, o.x0, o.x1, o.y0, o.y1)) continue;
       const float* s = splats + 16 * (size_t)i;
       const float dx = p.x - o.cx, dy = p.y - o.cy;
@@ -1054,6 +1062,47 @@ int orc_splat_render(const float* splats, uint32_t n, const float* vp, uint32_t 
     oc[3] = 1.0f;
     od[0] = od[1] = od[2] = D + T * 1.0f;
     od[3] = 1.0f;
+  }
+  return 0;
+}
+
+// The same pass as the render pipeline runs it: instance ii draws splat
+// n - 1 - ii (splat_forward.wgsl:44), and each fragment that survives the
+// discard (alpha >= 0.001, :143-145) is blended over the attachment's current
+// value with the pipeline's blend state (GpuSplatForwardPipelineManager.ts:64-77):
+// rgb = src.rgb * a + dst.rgb * (1 - a), alpha = a + dst.a * (1 - a); colour
+// src = (splat rgb, a), depth src = (enc, enc, enc, a) (:150-153).  rgba and
+// depth hold the attachments' starting values (the clear colours, or the
+// loaded contents) and receive the result; depth may be null.
+int orc_splat_render_blend(const float* splats, uint32_t n, const float* vp, uint32_t w, uint32_t h, float* rgba,
+                           float* depth) {
+  const float aspect = (float)w / (float)h;
+  const std::vector<SplatQuad> q = splat_quads(splats, n, vp, w, h);
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long pl = 0; pl < (long)w * h; ++pl) {
+    const uint32_t px = (uint32_t)(pl % w), py = (uint32_t)(pl / w);
+    const V2 p = pixel_to_p(px, py, w, h, aspect);
+    float* c = rgba + 4 * (size_t)pl;
+    float* d = depth ? depth + 4 * (size_t)pl : nullptr;
+    for (uint32_t ii = 0; ii < n; ++ii) {
+      const uint32_t i = n - 1 - ii;
+      const SplatQuad& o = q[i];
+      if (!o.ok || !in_quad(p, o.x0, o.x1, o.y0, o.y1)) continue;
+      const float* s = splats + 16 * (size_t)i;
+      const float dx = p.x - o.cx, dy = p.y - o.cy;
+      const float r2 = o.A * dx * dx + 2.0f * o.B * dx * dy + o.C * dy * dy;
+      const float r = std::sqrt(std::fmax(r2, 0.0001f));
+      const float pw = -s[14] * std::pow(r, s[13]);
+      float a = pw > -15.0f ? std::exp(pw) * s[7] : 0.0f;
+      a = clampf(a, 0.0f, 0.999f);
+      if (a < 0.001f) continue;
+      for (int k = 0; k < 3; ++k) c[k] = s[4 + k] * a + c[k] * (1.0f - a);
+      c[3] = a + c[3] * (1.0f - a);
+      if (d) {
+        for (int k = 0; k < 3; ++k) d[k] = o.depth * a + d[k] * (1.0f - a);
+        d[3] = a + d[3] * (1.0f - a);
+      }
+    }
   }
   return 0;
 }

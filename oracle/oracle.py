@@ -229,6 +229,16 @@ def splat_render(splats, vp, w, h):
     return rgba, dep
 
 
+def splat_render_blend(splats, vp, w, h, rgba, depth=None):
+    """The splat forward pass blended fragment by fragment in draw order over
+    the given starting images (H x W x 4, copied); returns (rgba, depth)."""
+    splats = _f32(splats)
+    rgba = np.array(rgba, np.float32, copy=True, order="C")
+    dep = None if depth is None else np.array(depth, np.float32, copy=True, order="C")
+    lib().orc_splat_render_blend(_p(splats, F), splats.shape[0], _p(_f32(vp), F), w, h, _p(rgba, F), _p(dep, F))
+    return rgba, dep
+
+
 def bezier_render(beziers, vp, w, h, bg=None, brush=None):
     beziers = _f32(beziers)
     bg = np.zeros((h, w, 4), np.float32) if bg is None else _f32(bg)

@@ -47,9 +47,8 @@ def test_bezier_render_matches_oracle(n, w, h, seed, use_bg, use_brush):
 
 def test_forward_pipeline_managers():
     """GpuSplatForwardPipelineManager / GpuBezierForwardPipelineManager
-    (writeVPMatrix, setTarget, dispatch) against the oracle: the cleared
-    splat pass, the cleared Bezier pass and the Bezier pass that loads the
-    target's contents (composited over them)."""
+    (writeVPMatrix, setTarget, dispatch) against the oracle: the cleared and
+    the loading splat pass, the cleared and the loading Bezier pass."""
     from nprush_b200._lib import NpsError
     from nprush_b200.bezier import GpuBezierForwardPipelineManager, GpuBezierOptimizerManager
     from nprush_b200.splat import GpuSplatForwardPipelineManager, GpuSplatOptimizerManager
@@ -63,12 +62,21 @@ def test_forward_pipeline_managers():
     dep = torch.zeros((h, w, 4), device="cuda")
     fwd.writeVPMatrix(vp)
     fwd.setTarget(rgba, dep, w, h)
-    with pytest.raises(ValueError):
-        fwd.dispatch()  # the reference's default is a loading pass
     fwd.dispatch(True)
     r_rgba, r_dep = orc.splat_render(s, vp, w, h)
     np.testing.assert_allclose(rgba.cpu().numpy(), r_rgba, atol=1e-5, rtol=0)
     np.testing.assert_allclose(dep.cpu().numpy(), r_dep, atol=1e-5, rtol=0)
+    # the loading pass (the reference's default): blended over the current
+    # contents, checked against the fragment-by-fragment draw-order blend
+    rng = np.random.default_rng(9)
+    c0 = rng.random((h, w, 4)).astype(np.float32)
+    d0 = rng.random((h, w, 4)).astype(np.float32)
+    rgba.copy_(torch.from_numpy(c0))
+    dep.copy_(torch.from_numpy(d0))
+    fwd.dispatch()
+    want_c, want_d = orc.splat_render_blend(s, vp, w, h, c0, d0)
+    np.testing.assert_allclose(rgba.cpu().numpy(), want_c, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(dep.cpu().numpy(), want_d, atol=1e-5, rtol=0)
 
     b = bezier_scene(400, 6)
     vp, _ = camera(w, h, dist=1.4)
