@@ -688,7 +688,10 @@ __global__ void __launch_bounds__(256) k_render_project(const float* __restrict_
   const float4 clip = mulv(vp, s[0], s[1], s[2], 1.0f);
   const float W = clip.w;
   float4* r4 = reinterpret_cast<float4*>(rec + (size_t)i * kRend);
-  if (!(W < 0.1f)) {
+  // the vertex stage collapses splats with w < 0.1 (splat_forward.wgsl:61-66); every vertex
+  // of the quad has the centre's clip z and w, so the pipeline's clipping against
+  // 0 <= z <= w keeps or drops the whole quad (a splat past the far plane is not drawn)
+  if (!(W < 0.1f) && clip.z >= 0.0f && clip.z <= W) {
     f3 axw = quat_rotate(s[8], s[9], s[10], s[11], {1.0f, 0.0f, 0.0f});
     f3 ayw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 1.0f, 0.0f});
     f3 azw = quat_rotate(s[8], s[9], s[10], s[11], {0.0f, 0.0f, 1.0f});

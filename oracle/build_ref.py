@@ -35,7 +35,8 @@ SHADERS = ("splat_backward", "splat_step", "splat_adc", "bezier_backward", "bezi
 # no size baked in (built with n = 0)
 IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge", "path_trace", "path_trace_resolve")
 # render pipelines: their @vertex / @fragment functions, callable one invocation at a time
-STAGE_SHADERS = ("mesh", "envmap")
+# (the display forwards with their instance count baked in, as their managers inject it)
+STAGE_SHADERS = ("mesh", "envmap", "splat_forward", "bezier_forward")
 
 
 def reference_root() -> Path:
@@ -87,6 +88,10 @@ def build(shader: str, n: int) -> Path:
     src = src_path.read_text()
     if shader in IMAGE_SHADERS + STAGE_SHADERS:
         consts = dict(gpu_constants())
+        if shader == "splat_forward":  # GpuSplatForwardPipelineManager.ts:45-48
+            consts["NUM_SPLATS"] = n
+        elif shader == "bezier_forward":  # GpuBezierForwardPipelineManager.ts:58-61
+            consts["NUM_BEZIERS"] = n
     else:
         consts = splat_consts(n) if shader.startswith("splat") else bezier_consts(n)
     rt = (HERE / "wgsl_rt.h").read_text()
@@ -167,6 +172,10 @@ class RefModule:
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         f(a.ctypes.data, out.ctypes.data)
         return out
+
+    def discarded(self) -> bool:
+        """Whether the last call() ended in `discard`."""
+        return bool(self.lib.wg_discarded())
 
     def dispatch(self, gx: int, gy: int = 1, gz: int = 1):
         self.lib.wg_dispatch(gx, gy, gz)

@@ -999,6 +999,9 @@ std::vector<SplatQuad> splat_quads(const float* splats, uint32_t n, const float*
     V4 clip = mulv(vp, s[0], s[1], s[2], 1.0f);
     const float W = clip.w;
     if (W < 0.1f) continue;
+    // all six vertices carry the centre's clip z and w: clipping against
+    // 0 <= z <= w keeps or drops the whole quad
+    if (!(clip.z >= 0.0f && clip.z <= W)) continue;
     V4 qq{s[8], s[9], s[10], s[11]};
     V2 ax = project_axis(vp, quat_rotate(qq, {1, 0, 0}), clip.x, clip.y, W, aspect);
     V2 ay = project_axis(vp, quat_rotate(qq, {0, 1, 0}), clip.x, clip.y, W, aspect);

@@ -22,7 +22,7 @@ from __future__ import annotations
 import re
 from dataclasses import dataclass, field
 
-TRANSLATOR_VERSION = "5"
+TRANSLATOR_VERSION = "6"
 
 
 class TranslateError(RuntimeError):
@@ -390,6 +390,7 @@ class Translator:
             self.attrs()
             ret = self.parse_type()
         adict = {a[0]: a[1] for a in at}
+        self.cur_ret = ret  # for `discard`
         body = self.block()
         if "compute" in adict:
             ws = [int(re.sub(r"[ui]$", "", x.strip())) for x in adict["workgroup_size"]]
@@ -458,7 +459,14 @@ class Translator:
             if tok.text in ("let", "var", "const") and self.peek(1).kind == "id":
                 out.append(self.decl())
                 continue
-            if tok.text in ("loop", "switch", "discard", "continuing"):
+            if tok.text == "discard":
+                # the invocation ends without output; call_<fn> reports it through wg_discarded()
+                self.next()
+                self.expect(";")
+                out.append("{ discard__ = true; return; }" if self.cur_ret == "void"
+                           else "{ discard__ = true; return {}; }")
+                continue
+            if tok.text in ("loop", "switch", "continuing"):
                 raise TranslateError(f"unsupported statement {tok.text}")
             out.append(self.rewrite_one())
         return " ".join(x for x in out if x)
@@ -580,6 +588,7 @@ def translate(src: str, subs: dict, origin: str) -> str:
         out.append(f"static {ctype}* {name}__b = nullptr;  // @group({g}) @binding({b}) var<{space}>")
     for name, ctype in m.workgroup:
         out.append(f"static {ctype} {name};  // var<workgroup>")
+    out.append("static bool discard__ = false;  // set by `discard` in a fragment stage")
     out.append("static void wg_zero__() {")
     for name, ctype in m.workgroup:
         out.append(f"  std::memset((void*)&{name}, 0, sizeof({name}));")
@@ -587,20 +596,28 @@ def translate(src: str, subs: dict, origin: str) -> str:
     out.extend(m.funcs)
     # @vertex / @fragment stages with one input: call_<name>(in, out) copies
     # the result out; size_<name>(o) gives sizeof(input), sizeof(result)
+    # Several inputs (e.g. @builtin(vertex_index), @builtin(instance_index))
+    # are packed in order as the members of one struct.
     for fname, ptypes in m.stage_fns:
-        if len(ptypes) != 1:
+        if not ptypes:
             continue
-        pt = ptypes[0]
-        out.append(f'extern "C" void call_{fname}(const void* in, void* out) {{')
-        out.append(f"  const auto r = {fname}(*(const {pt}*)in);")
+        members = " ".join(f"{pt} a{k};" for k, pt in enumerate(ptypes))
+        out.append(f"struct in__{fname} {{ {members} }};")
+        args = ", ".join(f"in.a{k}" for k in range(len(ptypes)))
+        out.append(f'extern "C" void call_{fname}(const void* in_, void* out) {{')
+        out.append(f"  const in__{fname}& in = *(const in__{fname}*)in_;")
+        out.append("  discard__ = false;")
+        out.append(f"  const auto r = {fname}({args});")
         out.append("  std::memcpy(out, &r, sizeof r);")
         out.append("}")
         out.append(f'extern "C" void size_{fname}(unsigned* o) {{')
-        out.append(f"  o[0] = sizeof({pt}); o[1] = sizeof({fname}(std::declval<{pt}>()));")
+        decl = ", ".join(f"std::declval<{pt}>()" for pt in ptypes)
+        out.append(f"  o[0] = sizeof(in__{fname}); o[1] = sizeof({fname}({decl}));")
         out.append("}")
     out.append("}  // namespace refmod")
     wx, wy, wz = m.wgsize
     out.append('extern "C" {')
+    out.append("int wg_discarded() { return refmod::discard__ ? 1 : 0; }")
     out.append("void wg_bind(int group, int binding, void* p) {")
     for g, b, name, space, ctype in m.bindings:
         if ctype not in ("texture_2d", "texture_storage_2d", "sampler"):
