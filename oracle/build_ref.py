@@ -110,6 +110,11 @@ def build(shader: str, n: int) -> Path:
     if r.returncode != 0:
         raise RuntimeError(f"g++ failed for {shader}:\n{r.stderr[-4000:]}")
     os.replace(str(so) + ".tmp", so)
+    # one build per (shader, n): readers without the reference checkout (bench.py on
+    # another machine) find it by name
+    for old in REF_OUT.glob(f"{shader}_n{n}_*"):
+        if not old.name.startswith(f"{shader}_n{n}_{key}"):
+            old.unlink(missing_ok=True)
     return so
 
 
