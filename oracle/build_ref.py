@@ -118,6 +118,42 @@ def build(shader: str, n: int) -> Path:
     return so
 
 
+def load_ts(name: str):
+    """The reference's host-side TypeScript module src/lib/gpu/<name>.ts,
+    translated to Python by oracle/ts2py.py (cached under oracle/_ref, one
+    translation per source) and imported."""
+    import importlib.util
+    import sys
+
+    from ts2py import TS2PY_VERSION, translate  # noqa: local import (sys.path set by caller)
+
+    if str(HERE) not in sys.path:
+        sys.path.insert(0, str(HERE))  # js_rt
+    REF_OUT.mkdir(exist_ok=True)
+    src_path = reference_root() / "src/lib/gpu" / f"{name}.ts"
+    if src_path.exists():
+        src = src_path.read_text()
+        key = hashlib.sha256((src + TS2PY_VERSION + (HERE / "ts2py.py").read_text()
+                              + (HERE / "js_rt.py").read_text()).encode()).hexdigest()[:16]
+        py = REF_OUT / f"{name}_ts_{key}.py"
+        if not py.exists():
+            tmp = py.with_suffix(f".{os.getpid()}.tmp")
+            tmp.write_text(translate(src, f"src/lib/gpu/{name}.ts"))
+            os.replace(tmp, py)
+            for old in REF_OUT.glob(f"{name}_ts_*.py"):
+                if old != py:
+                    old.unlink(missing_ok=True)
+    else:
+        found = sorted(REF_OUT.glob(f"{name}_ts_*.py"))
+        if not found:
+            raise FileNotFoundError(f"{src_path} absent and no translation in {REF_OUT}")
+        py = found[-1]
+    spec = importlib.util.spec_from_file_location(py.stem, py)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 class RefModule:
     """ctypes handle on one compiled reference shader."""
 

@@ -175,6 +175,22 @@ def bezier_adc(beziers, m_, v_, adam_t, no_kill, grad_accum, loss_accum, pixel_l
     return b, adam[:18 * n].reshape(n, 18), adam[18 * n:36 * n].reshape(n, 18), adc[:n], adc[n:], pl
 
 
+def build_bvh(vertices, indices):
+    """The reference's own buildBvh (bvh.ts:202-223, translated by
+    oracle/ts2py.py) on MeshData-layout vertices (V x 12 f32) and triangle
+    indices: (nodes (N, 8) float32 holding the u32 fields' bits in columns 3
+    and 7, tri_indices (T, 3) uint32), the layout of oracle/bvh.py."""
+    import js_rt
+    from build_ref import load_ts
+    if "bvh" not in _cache:
+        _cache["bvh"] = load_ts("bvh")
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    r = _cache["bvh"].buildBvh(js_rt.Float32Array(v.tolist()), js_rt.Uint32Array(i.tolist()))
+    nodes = np.frombuffer(bytes(r.nodes.b), np.float32).reshape(-1, 8).copy()
+    return nodes, r.triIndices.a.reshape(-1, 3).copy()
+
+
 def path_trace(vertices, nodes, tri_indices, env_rgba, inv_view_proj, frame, accum):
     """One dispatch of path_trace.wgsl (GpuPathTracePipelineManager.ts:222-240):
     adds one sample per pixel to accum (h, w, 4) float32 in place.  Bindings

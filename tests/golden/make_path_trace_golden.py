@@ -1,9 +1,10 @@
 """Generates tests/golden/path_trace.npz: scenes, their BVHs and the outputs of
 the reference's own path tracer (src/lib/gpu/path_trace.wgsl and
 path_trace_resolve.wgsl, translated to C++ and run on the host by
-oracle/build_ref.py).  The BVHs come from the restatement of bvh.ts in
-oracle/bvh.py.  Needs the reference checkout (NPRUSH_REFERENCE, default
-/root/reference); the GPU tests read only the .npz.
+oracle/build_ref.py).  The BVHs come from the reference's own builder
+(src/lib/gpu/bvh.ts, translated to Python by oracle/ts2py.py).  Needs the
+reference checkout (NPRUSH_REFERENCE, default /root/reference); the GPU tests
+read only the .npz.
 
 Cases (image 45 x 37, not a multiple of the 8 x 8 workgroup):
   diffuse  ground + spheres and boxes (one box a mirror), sky environment;
@@ -26,7 +27,6 @@ sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(ROOT))
 
 import refrun  # noqa: E402
-from bvh import build_bvh  # noqa: E402
 from nprush_b200 import camera, meshes  # noqa: E402
 
 W, H = 45, 37
@@ -41,7 +41,7 @@ def scene():
 
 
 def trace(mesh, env, inv, frames):
-    nodes, tris = build_bvh(mesh.vertices, mesh.indices)
+    nodes, tris = refrun.build_bvh(mesh.vertices, mesh.indices)
     acc = np.zeros((H, W, 4), np.float32)
     snaps = []
     for f in frames:

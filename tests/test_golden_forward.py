@@ -70,3 +70,22 @@ def test_quad_coverage_is_watertight():
                 if r is not None:
                     np.add.at(hits, (r[1], r[0]), 1)
             assert hits.max() <= 1
+
+
+def test_reference_stages_reproduce_the_fixture(tmp_path, monkeypatch):
+    """Regenerating tests/golden/forward.npz from the reference checkout gives
+    the committed arrays (skipped without the checkout)."""
+    import importlib.util
+
+    import build_ref
+    if not build_ref.reference_available():
+        pytest.skip("reference checkout not present")
+    spec = importlib.util.spec_from_file_location("mk", GOLD.parent / "make_forward_golden.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    monkeypatch.setattr(mk, "HERE", tmp_path)
+    mk.main()
+    a, b = np.load(GOLD), np.load(tmp_path / "forward.npz")
+    assert set(a.files) == set(b.files)
+    for k in a.files:
+        np.testing.assert_array_equal(a[k], b[k])

@@ -151,3 +151,41 @@ def test_reference_shaders_reproduce_the_fixtures(tmp_path, monkeypatch):
     a, b = np.load(GOLD), np.load(tmp_path / "path_trace.npz")
     for k in a.files:
         np.testing.assert_array_equal(a[k], b[k])
+
+
+@requires_reference
+@pytest.mark.parametrize("case", ["soups", "degenerate", "same_centroid", "scene", "empty"])
+def test_reference_bvh_builder_equals_restatement(case):
+    """The reference's own buildBvh (bvh.ts, translated by oracle/ts2py.py)
+    and the restatement in oracle/bvh.py give the same bytes."""
+    import refrun
+    from nprush_b200 import meshes
+    rng = np.random.default_rng(11)
+    if case == "soups":  # coordinates rounded to repeat, so centroid ties and equal bounds occur
+        inputs = []
+        for k in range(8):
+            nv, nt = int(rng.integers(3, 80)), int(rng.integers(1, 120))
+            v = np.zeros((nv, 12), np.float32)
+            v[:, :3] = np.round(rng.normal(size=(nv, 3)) * 3, k % 3)
+            inputs.append((v, rng.integers(0, nv, size=(nt, 3)).astype(np.uint32)))
+    elif case == "degenerate":  # repeated vertex indices and flat (zero-extent) triangles
+        v = np.zeros((10, 12), np.float32)
+        v[:, 0] = np.arange(10)
+        idx = np.array([[0, 0, 0], [1, 1, 2], [2, 3, 4], [5, 6, 7], [7, 8, 9], [0, 9, 5]] * 3, np.uint32)
+        inputs = [(v, idx)]
+    elif case == "same_centroid":  # every centroid equal: the split falls back to halves
+        v = np.zeros((3 * 40, 12), np.float32)
+        for t in range(40):
+            s = 0.1 + 0.05 * t
+            v[3 * t:3 * t + 3, :3] = [[-s, -s, 0], [s, -s, 0], [0, 2 * s, 0]]
+        inputs = [(v, np.arange(120, dtype=np.uint32).reshape(-1, 3))]
+    elif case == "scene":
+        sc = meshes.demo_scene(5, seed=9, mirror_fraction=0.2, sphere_detail=8)
+        inputs = [(sc.vertices, sc.indices)]
+    else:
+        inputs = [(np.zeros((3, 12), np.float32), np.zeros((0, 3), np.uint32))]
+    for v, idx in inputs:
+        n_ref, t_ref = refrun.build_bvh(v, idx)
+        n_res, t_res = obvh.build_bvh(v, idx)
+        np.testing.assert_array_equal(n_ref.view(np.uint32), np.asarray(n_res, np.float32).view(np.uint32))
+        np.testing.assert_array_equal(t_ref, t_res)
