@@ -151,8 +151,6 @@ class Translator:
                 depth += 1
             elif tok.text in (")", "]", "}", ">"):
                 depth -= 1
-            elif tok.text == "=>" and depth == 0 and "=>" not in stops:
-                pass
             self.next()
 
     def skip_balanced(self):
@@ -166,7 +164,8 @@ class Translator:
             elif tok.text == "}":
                 depth -= 1
 
-    # -- expressions: each returns (python_text, pre_statements)
+    # -- expressions: each returns the Python text; statements that must run first
+    #    (hoisted post-increments) are appended to `pre`
     def expr(self, pre, min_prec=0):
         left = self.unary(pre)
         while True:
@@ -181,8 +180,6 @@ class Translator:
                 b = self.expr(pre, 1)
                 left = f"({a} if {left} else {b})"
                 continue
-            if op == "as":  # not reached: `as` is an identifier token
-                return left
             prec = _BIN.get(op)
             if prec is None or prec < min_prec or prec <= 2:
                 return left
