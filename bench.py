@@ -393,6 +393,33 @@ def mr_scene():
     return sc, meshes.sky_env(256, 128), u
 
 
+def mr_cpu_sample(stages_for):
+    """Host timing of the mesh pass on the same scene through oracle/mesh_raster.py
+    with the stage functions stages_for(uniforms, env) returns: one pass at
+    64x48 and one at 128x96, fitted as t = a + b * pixels (a: the per-vertex and
+    per-triangle work, b: the per-pixel work) and evaluated at the workload's
+    1024x768.  Returns (passes/s, description)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import mesh_raster as mr
+    from nprush_b200 import camera
+    sc, env, uni = mr_scene()
+    ts = {}
+    for w, h in ((64, 48), (128, 96)):
+        su = uni.copy()
+        vp, inv = camera.view_proj((4.0, -3.5, 2.6), (0.0, 0.0, 0.3), 0.9, w / h, up=(0.0, 0.0, 1.0))
+        su[0:16], su[36:52] = vp, inv
+        stages = stages_for(su, env)
+        t0 = time.perf_counter()
+        mr.render(sc.vertices, sc.indices, su, w, h, stages)
+        ts[w * h] = time.perf_counter() - t0
+    (p0, t0_), (p1, t1_) = sorted(ts.items())
+    b = max((t1_ - t0_) / (p1 - p0), 0.0)
+    a = max(t0_ - b * p0, 0.0)
+    t_full = a + b * MR_W * MR_H
+    return 1.0 / t_full, (f"passes at 64x48 ({t0_:.1f} s) and 128x96 ({t1_:.1f} s) fitted as {a:.1f} s + "
+                          f"{b * 1e6:.1f} us per pixel, evaluated at {MR_W}x{MR_H} ({t_full:.0f} s); one host thread")
+
+
 def run_mesh_raster(args):
     """The viewer's mesh render pass (nps_mesh_render): CUDA events around
     each pass on the library's stream; the CPU leg is the float32 restatement
@@ -453,19 +480,30 @@ def run_mesh_raster(args):
     if not args.no_cpu_baseline:
         sys.path.insert(0, str(ROOT / "oracle"))
         import mesh_raster as mr
-        w, h = 64, 48
-        su = uni.copy()
-        from nprush_b200 import camera
-        vp, inv = camera.view_proj((4.0, -3.5, 2.6), (0.0, 0.0, 0.3), 0.9, w / h, up=(0.0, 0.0, 1.0))
-        su[0:16], su[36:52] = vp, inv
-        t0 = time.perf_counter()
-        mr.render(sc.vertices, sc.indices, su, w, h, mr.RestatedStages(env, env))
-        t = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": 1.0 / (t * (MR_W * MR_H) / (w * h)), "unit": "passes/s", "cores": 1,
-                                "kind": "port",
-                                "sample": f"the float32 restatement at {w}x{h} ({t:.1f} s), scaled by pixel count; "
-                                          "one host thread (numpy)"}
+        v, why = mr_cpu_sample(lambda su, env_: mr.RestatedStages(env_, env_))
+        line["cpu_baseline"] = {"value": v, "unit": "passes/s", "cores": 1, "kind": "port",
+                                "sample": "the float32 restatement (numpy): " + why}
     return line
+
+
+def mr_reference(args):
+    """The reference's own mesh.wgsl / envmap.wgsl stage functions (translated
+    to C++, oracle/_ref) between the restated fixed-function steps, on the
+    host; its render pipeline itself needs a graphics stack, which this box
+    does not have."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    try:
+        import refrun
+        refrun.stage_module("mesh")
+    except FileNotFoundError as e:
+        return {"impl": "reference", "unavailable": str(e)}
+    v, why = mr_cpu_sample(lambda su, env_: refrun.MeshStages(su, env_, env_))
+    return {"impl": "reference", "metric": MR_METRIC, "value": v, "unit": "passes/s", "higher_is_better": True,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "reference mesh.wgsl / envmap.wgsl stages (translated to C++) with the restated "
+                                   "fixed-function steps, same scene"},
+            "cpu_baseline": {"value": v, "unit": "passes/s", "cores": 1, "kind": "reference", "sample": why},
+            "e2e": {"value": v, "unit": "passes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def run_path_trace(args):
@@ -577,9 +615,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.workload == "mesh_raster":
         if rank == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "the reference's mesh pass is a WebGPU render "
-                              "pipeline: no graphics stack on this box"} if args.impl == "reference"
-                             else run_mesh_raster(args)))
+            print(json.dumps(mr_reference(args) if args.impl == "reference" else run_mesh_raster(args)))
         return
     if args.workload == "path_trace":
         if rank != 0:

@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from build_ref import RefModule
+from build_ref import REF_OUT, RefModule, reference_available
 
 _cache: dict = {}
 
@@ -189,6 +189,51 @@ def build_bvh(vertices, indices):
     r = _cache["bvh"].buildBvh(js_rt.Float32Array(v.tolist()), js_rt.Uint32Array(i.tolist()))
     nodes = np.frombuffer(bytes(r.nodes.b), np.float32).reshape(-1, 8).copy()
     return nodes, r.triIndices.a.reshape(-1, 3).copy()
+
+
+def stage_module(shader: str) -> RefModule:
+    """A render pipeline's translated stages: built from the reference checkout
+    when present, else the build already under oracle/_ref."""
+    if reference_available():
+        return RefModule(shader, 0)
+    found = sorted(REF_OUT.glob(f"{shader}_n0_*.so"))
+    if not found:
+        raise FileNotFoundError(f"oracle/_ref has no {shader} build and the reference checkout is absent")
+    return RefModule.from_path(found[-1])
+
+
+class MeshStages:
+    """mesh.wgsl vert / frag / frag_pbr and envmap.wgsl frag, the reference's
+    own functions, with the bindings the managers create (uniforms at 0,
+    matcap + clamped linear sampler at 1-2, the PBR textures + repeating
+    sampler at 3-5, GpuMeshRenderPipelineManager.ts:226-246; environment +
+    u-repeating sampler, GpuEnvmapPipelineManager.ts): the stage interface
+    that oracle/mesh_raster.render drives."""
+
+    def __init__(self, uni, matcap, env, albedo=None, normal_map=None):
+        self.mesh = stage_module("mesh")
+        self.envm = stage_module("envmap")
+        self.uni = np.ascontiguousarray(uni, np.float32)
+        for m in (self.mesh, self.envm):
+            m.bind(0, self.uni)
+        self.mesh.bind_tex(1, np.ascontiguousarray(matcap, np.float32))
+        self.mesh.bind_sampler(2, True, "clamp-to-edge", "clamp-to-edge")
+        if albedo is not None:
+            self.mesh.bind_tex(3, np.ascontiguousarray(albedo, np.float32))
+            self.mesh.bind_tex(4, np.ascontiguousarray(normal_map, np.float32))
+            self.mesh.bind_sampler(5, True, "repeat", "repeat")
+        self.envm.bind_tex(1, np.ascontiguousarray(env, np.float32))
+        self.envm.bind_sampler(2, True, "repeat", "clamp-to-edge")
+
+    def vert(self, vin, uni):
+        return self.mesh.call("vert", np.asarray(vin, np.float32))
+
+    def frag(self, vo, uni, pbr=False):
+        r = self.mesh.call("frag_pbr" if pbr else "frag", np.asarray(vo, np.float32))
+        return r[0:4], r[4:8]
+
+    def env_frag(self, ndc, uni):
+        return self.envm.call("frag", np.array([0, 0, 0, 1, ndc[0], ndc[1]], np.float32))
 
 
 def path_trace(vertices, nodes, tri_indices, env_rgba, inv_view_proj, frame, accum):

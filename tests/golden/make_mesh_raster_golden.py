@@ -25,40 +25,15 @@ sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(ROOT))
 
 import mesh_raster as mr  # noqa: E402
-from build_ref import RefModule  # noqa: E402
+import refrun  # noqa: E402
 from nprush_b200 import camera, meshes  # noqa: E402
 
 W, H = 61, 45
 EYE, TARGET = (3.2, -2.6, 1.9), (0.0, 0.0, 0.4)
 
 
-class ReferenceStages:
-    """mesh.wgsl vert / frag and envmap.wgsl frag, the reference's own code."""
-
-    def __init__(self, uni, matcap, env, albedo=None, normal_map=None):
-        self.mesh = RefModule("mesh", 0)
-        self.envm = RefModule("envmap", 0)
-        self.uni = np.ascontiguousarray(uni, np.float32)
-        for m in (self.mesh, self.envm):
-            m.bind(0, self.uni)
-        self.mesh.bind_tex(1, np.ascontiguousarray(matcap, np.float32))
-        self.mesh.bind_sampler(2, True, "clamp-to-edge", "clamp-to-edge")
-        if albedo is not None:  # the PBR stage's textures (GpuMeshRenderPipelineManager.ts:226-246)
-            self.mesh.bind_tex(3, np.ascontiguousarray(albedo, np.float32))
-            self.mesh.bind_tex(4, np.ascontiguousarray(normal_map, np.float32))
-            self.mesh.bind_sampler(5, True, "repeat", "repeat")
-        self.envm.bind_tex(1, np.ascontiguousarray(env, np.float32))
-        self.envm.bind_sampler(2, True, "repeat", "clamp-to-edge")
-
-    def vert(self, vin, uni):
-        return self.mesh.call("vert", np.asarray(vin, np.float32))
-
-    def frag(self, vo, uni, pbr=False):
-        r = self.mesh.call("frag_pbr" if pbr else "frag", np.asarray(vo, np.float32))
-        return r[0:4], r[4:8]
-
-    def env_frag(self, ndc, uni):
-        return self.envm.call("frag", np.array([0, 0, 0, 1, ndc[0], ndc[1]], np.float32))
+# mesh.wgsl vert / frag and envmap.wgsl frag, the reference's own code
+ReferenceStages = refrun.MeshStages
 
 
 def wall():
