@@ -97,8 +97,10 @@ int nps_splat_opt_step(nps_splat_opt* opt);
 int nps_splat_opt_adc(nps_splat_opt* opt);
 /* Headless GpuSplatForwardPipelineManager.dispatch(enc, clear=true)
  * (GpuSplatForwardPipelineManager.ts:114-137, splat_forward.wgsl:42-156):
- * fp32 composite of all splats (index 0 in front), w < 0.1 culled, alpha
- * < 0.001 discarded, cleared to colour 0.05 / depth 1.  out_rgba and out_depth
+ * fp32 composite of all splats (index 0 in front), w < 0.1 culled, splats
+ * whose centre lies outside 0 <= z <= w (past the far plane) clipped away as
+ * the pipeline clips their quads, alpha < 0.001 discarded, cleared to
+ * colour 0.05 / depth 1.  out_rgba and out_depth
  * are device buffers of h*w*4 floats each (depth replicated in rgb, alpha in a). */
 int nps_splat_opt_render(nps_splat_opt* opt, const float* vp, uint32_t width, uint32_t height, float* out_rgba,
                          float* out_depth);
