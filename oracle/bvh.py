@@ -5,7 +5,8 @@ JavaScript numbers are IEEE doubles and Python floats are too, so every
 quantity is computed here as bvh.ts computes it; node bounds are rounded to
 float32 when written (DataView.setFloat32, bvh.ts:90-97) and the data words
 hold u32 bits (setUint32, :99-103).  There is no JavaScript runtime on this
-machine, so the restatement is pinned by reading bvh.ts, not by running it.
+machine; bvh.ts itself runs here through oracle/ts2py.py (refrun.build_bvh),
+and this restatement equals it bit for bit (tests/test_golden_path_trace.py).
 
     nodes, tris = build_bvh(vertices, indices)
         vertices: (V, 12) float32 [pos, normal, rgba, uv]; indices: (T*3,) u32
