@@ -189,3 +189,21 @@ def test_reference_bvh_builder_equals_restatement(case):
         n_res, t_res = obvh.build_bvh(v, idx)
         np.testing.assert_array_equal(n_ref.view(np.uint32), np.asarray(n_res, np.float32).view(np.uint32))
         np.testing.assert_array_equal(t_ref, t_res)
+
+
+@requires_reference
+def test_library_bvh_builder_equals_reference_on_the_benchmark_scene(lib_bvh):
+    """The library's host builder against the reference's own buildBvh on the
+    path-tracer benchmark's 12k-triangle scene: the same bytes."""
+    import importlib.util
+
+    import refrun
+    spec = importlib.util.spec_from_file_location("bench", Path(__file__).resolve().parent.parent / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    sc, _, _ = bench.pt_scene()
+    n_ref, t_ref = refrun.build_bvh(sc.vertices, sc.indices)
+    n_lib, t_lib = lib_bvh(sc.vertices, sc.indices)
+    assert t_ref.shape[0] > 10_000
+    np.testing.assert_array_equal(n_lib.view(np.uint32), n_ref.view(np.uint32))
+    np.testing.assert_array_equal(t_lib, t_ref)
