@@ -1,7 +1,7 @@
 """Benchmark: train steps/s (fwd + bwd + Adam, 200k Gaussians SH3, 800x800,
 8 views per step) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path gs|compat]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
 
 Prints ONE JSON line (rank 0).  A step is one full training iteration over 8
 of 32 sphere cameras (forward + L1/D-SSIM loss + backward + Adam) on seeded
@@ -137,6 +137,13 @@ def build_scene(dev):
     return vp, vpi, tg, student
 
 
+def view_schedule(steps: int):
+    """The cameras of each step: VIEWS of the CAMS sphere cameras, drawn by a
+    seeded permutation per step, in ascending order."""
+    rng = np.random.default_rng(1234)
+    return [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(steps)]
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -150,8 +157,7 @@ def run_ours(args, rank, world):
         vp, vpi, tg, st = build_scene(dev)
         torch.cuda.synchronize()
         st.set_targets(tg, borrow=True)
-        rng = np.random.default_rng(1234)
-        sched = [np.sort(rng.permutation(CAMS)[:VIEWS]) for _ in range(args.warmup + args.steps + 4)]
+        sched = view_schedule(args.warmup + args.steps + 4)
         tuned = None
         if not args.no_autotune:
             # raster variants (pixels per thread) timed on this workload
@@ -187,6 +193,8 @@ def run_ours(args, rank, world):
                 times.append(e0.elapsed_time(e1))
                 pairs.append(st.stats()["pairs"])
         stages = st.stage_times(reset=True)
+        # kernels launched per step: the captured step's kernel nodes (graph mode)
+        graph_kernels = st.stats()["graph_kernels"] if not args.no_graph else None
         st.set_timing(False)
         torch.cuda.synchronize()
         if world > 1:
@@ -218,6 +226,7 @@ def run_ours(args, rank, world):
         h2d = VIEWS * HEIGHT * WIDTH * 4 * 4 + VIEWS * (32 * 4 + 4)
         d2h = 3 * 4
     return dict(tuned=tuned, ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
+                graph_kernels=graph_kernels,
                 clocks=clk.summary(), e2e_ms=float(np.mean(e2e_times)), h2d=h2d, d2h=d2h, loss=loss_last)
 
 
@@ -577,13 +586,6 @@ def run_path_trace(args):
     return line
 
 
-def launches_per_step(tile_passes: int) -> int:
-    # preprocess, set count, depth sort (4 passes x 3), gather, scan (3), emit,
-    # tile sort (passes x 3), ranges, forward, ssim fwd / bwd / reduce,
-    # backward, projection backward, Adam
-    return 1 + 1 + 12 + 1 + 3 + 1 + 3 * tile_passes + 1 + 1 + 3 + 1 + 1 + 1
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -685,7 +687,8 @@ def main():
         "clocks": res["clocks"],
         "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"]},
-        "gpu_launches": launches_per_step(tile_passes) * args.steps,
+        "gpu_launches": None if res["graph_kernels"] is None else res["graph_kernels"] * args.steps,
+        "gpu_launches_source": "kernel nodes of the captured train-step graph x timed steps",
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": (BWD_TRAFFIC_BYTES * K / BWD_TRAFFIC_PAIRS
                                  if dom == "raster_bwd" and N_GAUSS == 200_000 and WIDTH == 800 else None),

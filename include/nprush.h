@@ -122,13 +122,16 @@ int nps_splat_opt_buffers(nps_splat_opt* opt, float** splats, int32_t** grads, f
  * ones that share the GPU with latency-critical work (a render loop), where
  * cudaMalloc / cudaFree may synchronise the device.  Runs the splat ADC
  * (splat_adc.wgsl:28-87, same kernel as nps_splat_opt_adc) on caller-owned
- * device buffers: splats N*16, adam_m / adam_v N*16, grad_accum N floats.
- * Its scratch (dead-slot list + result word) is a fixed array compiled into
- * the library: at most 262144 splats (larger N returns NPS_ERR_CAPACITY), and
- * every GPU that loads the library holds that 1 MiB until exit.  Allocates
- * nothing.  The first call on a device looks up the array's device address
- * (with that device current), so make the first call before any stream
- * capture.  Calls share the array, which keeps the last call's contents;
+ * device buffers: splats N*16, adam_m / adam_v N*16 (16-byte aligned),
+ * grad_accum N floats (4-byte aligned); misaligned pointers return
+ * NPS_ERR_INVALID.  Its scratch (dead-slot list + result word) is a fixed
+ * array compiled into the library: at most 262144 splats (larger N returns
+ * NPS_ERR_CAPACITY), and every GPU that loads the library holds that 1 MiB
+ * until exit.  Allocates nothing.  The first call on a device looks up the
+ * array's device address (with that device current) and keeps it for the
+ * process, so make the first call before any stream capture, and do not call
+ * it again on a device after cudaDeviceReset (the kept address belongs to the
+ * destroyed context).  Calls share the array, which keeps the last call's contents;
  * calls that overlap on the GPU (different streams, or different host
  * threads) race on it.  Runs on cuda_stream (null = legacy default stream) of
  * the current device; clones_host (may be null) receives the number of clones
@@ -142,8 +145,10 @@ typedef struct nps_stats {
   uint32_t max_tile_len;   /* longest tile list before the cap */
   uint32_t adc_clones;     /* clones + splits performed by the last ADC */
   uint32_t step_count;     /* dispatch() calls so far */
-  uint32_t reserved[3];    /* Bezier: [0] spawns.  Gaussians: [1] graph replays that skipped their
-                              update (pair overflow), [2] record-staging waits that timed out */
+  uint32_t reserved[3];    /* Bezier: [0] spawns.  Gaussians: [0] kernel launches per replay of the
+                              captured train step (its graph's kernel nodes), [1] graph replays that
+                              skipped their update (pair overflow), [2] record-staging waits that
+                              timed out */
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
 /* Sets the manager's stepCount (GpuSplatOptimizerManager.ts:380, dispatch()
@@ -213,7 +218,8 @@ int nps_bezier_opt_set_step_count(nps_bezier_opt* opt, uint32_t count);
  * dispatch) for standard 3D Gaussians.  Parameter record: 64 floats per
  * Gaussian (256 B): mean xyz | log-scale xyz | quaternion wxyz | opacity logit |
  * pad | SH coefficients 16 x rgb (coefficient-major) | pad.  Loss: 0.8 L1 +
- * 0.2 (1 - SSIM).  All views of a step are processed by every launch. */
+ * 0.2 (1 - SSIM) unless nps_gs_set_loss chooses another.  All views of a step
+ * are processed by every launch. */
 int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** out);
 int nps_gs_destroy(nps_gs* gs);
 /* Upload records [first, first+count); the active count grows to cover them. */
@@ -251,8 +257,18 @@ int nps_gs_set_views(nps_gs* gs, const float* vp, const float* vp_inv, const uin
  * state (final transmittance + last contributor); backward replays. */
 int nps_gs_forward(nps_gs* gs, float* out_rgba_device);
 /* Fused loss of the last forward against the targets; loss3 (host, may be
- * null) = {loss, mean L1, mean SSIM}.  Also stores dL/dimage for backward. */
+ * null) = {loss, mean L1, mean SSIM} (L1 + D-SSIM) or {loss, mean L1, mean
+ * squared error} (L1, L2).  Also stores dL/dimage for backward. */
 int nps_gs_loss(nps_gs* gs, float* loss3);
+/* Loss of the fused path (no reference counterpart; the reference's splat
+ * loss is L2 on colour plus a depth term, splat_backward.wgsl:250-257):
+ * kind NPS_GS_LOSS_L1_DSSIM = (1 - w) mean|x - y| + w (1 - mean SSIM) with an
+ * 11 x 11 Gaussian window (sigma 1.5) and w = ssim_weight (default: this
+ * kind, w = 0.2); NPS_GS_LOSS_L1 = mean|x - y|; NPS_GS_LOSS_L2 = mean
+ * (x - y)^2; means over the 3 H W colour values of the views.  ssim_weight
+ * in [0, 1] (ignored by L1 and L2). */
+enum { NPS_GS_LOSS_L1_DSSIM = 0, NPS_GS_LOSS_L1 = 1, NPS_GS_LOSS_L2 = 2 };
+int nps_gs_set_loss(nps_gs* gs, int kind, float ssim_weight);
 /* dl_dimage: device num_views*h*w*4 floats, or null for the fused loss gradient. */
 int nps_gs_backward(nps_gs* gs, const float* dl_dimage_device);
 int nps_gs_adam(nps_gs* gs);
@@ -295,7 +311,7 @@ int nps_gs_set_accumulate(nps_gs* gs, int accumulate, uint32_t loss_views);
 /* Checkpoint (no reference counterpart: the reference never reads its GPU
  * state back).  File: a 104-byte little-endian header (magic "NPSGSCK1",
  * version, count, SH degree, Adam step, ADC seed, loss views, learning rates,
- * background, SSIM weight) followed by params, Adam m, Adam v (count x 64
+ * background, SSIM weight, loss kind) followed by params, Adam m, Adam v (count x 64
  * floats each) and the two ADC accumulators (count floats each).  Load
  * requires count <= capacity and the same SH degree. */
 int nps_gs_save(nps_gs* gs, const char* path);

@@ -92,6 +92,7 @@ SIGNATURES = {
     "nps_gs_set_image_size": [P, U32, U32],
     "nps_gs_forward": [P, P],
     "nps_gs_loss": [P, P],
+    "nps_gs_set_loss": [P, I32, F32],
     "nps_gs_backward": [P, P],
     "nps_gs_adam": [P],
     "nps_gs_train_step": [P, P],

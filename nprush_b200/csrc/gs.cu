@@ -680,8 +680,62 @@ __global__ void __launch_bounds__(256, 3) k_ssim_bwd2(const float4* __restrict__
   }
 }
 
-__global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblocks, float lambda, float inv_norm,
-                              float wconst, float* __restrict__ loss) {
+// Per-pixel losses without the SSIM term: mean |x - y| (KIND = kLossL1) or
+// mean (x - y)^2 (KIND = kLossL2) over the colour channels.  A fixed grid of
+// blocks per view strides over the view's pixels; each block writes its sums
+// of |x - y| and (x - y)^2 to partial (in block order, so k_loss_reduce adds
+// them in a fixed order), and every pixel its dL/dimage.
+constexpr int kLossL1Dssim = 0, kLossL1 = 1, kLossL2 = 2;
+constexpr uint32_t kPixLossBlocks = 128;  // per view
+template <int KIND>
+__global__ void __launch_bounds__(256) k_pix_loss(const float4* __restrict__ img, const float4* __restrict__ tgt,
+                                                  const uint32_t* __restrict__ tgt_ids, uint32_t npix,
+                                                  float inv_norm, float4* __restrict__ dimg,
+                                                  float* __restrict__ partial) {
+  __shared__ float red[2][8];
+  const uint32_t v = blockIdx.y, tid = threadIdx.x;
+  const float4* im = img + (size_t)v * npix;
+  const float4* tg = tgt + (size_t)tgt_ids[v] * npix;
+  float4* dm = dimg + (size_t)v * npix;
+  float a = 0.0f, b = 0.0f;
+  for (uint32_t i = blockIdx.x * 256 + tid; i < npix; i += gridDim.x * 256) {
+    const float4 x = __ldg(im + i), y = __ldg(tg + i);
+    const float d0 = x.x - y.x, d1 = x.y - y.y, d2 = x.z - y.z;
+    a += fabsf(d0) + fabsf(d1) + fabsf(d2);
+    b += d0 * d0 + d1 * d1 + d2 * d2;
+    float4 g;
+    if (KIND == kLossL2) {
+      const float s = 2.0f * inv_norm;
+      g = make_float4(s * d0, s * d1, s * d2, 0.0f);
+    } else {
+      auto sg = [](float d) { return d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f); };
+      g = make_float4(sg(d0) * inv_norm, sg(d1) * inv_norm, sg(d2) * inv_norm, 0.0f);
+    }
+    dm[i] = g;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = a;
+    red[1][tid >> 5] = b;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float sa = 0.0f, sb = 0.0f;
+    for (int w = 0; w < 8; ++w) { sa += red[0][w]; sb += red[1][w]; }
+    const size_t bi = (size_t)v * gridDim.x + blockIdx.x;
+    partial[2 * bi] = sa;
+    partial[2 * bi + 1] = sb;
+  }
+}
+
+// Sums the per-block partials (|x - y| and SSIM sums for kind 0, |x - y| and
+// (x - y)^2 sums otherwise) into loss[0..2] = (loss, mean L1, mean SSIM or
+// mean squared error).
+__global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblocks, int kind, float lambda,
+                              float inv_norm, float wconst, float* __restrict__ loss) {
   __shared__ float r0[kThreads], r1[kThreads];
   float a = 0, b = 0;
   for (uint32_t i = threadIdx.x; i < nblocks; i += kThreads) {
@@ -700,9 +754,11 @@ __global__ void k_loss_reduce(const float* __restrict__ partial, uint32_t nblock
   }
   if (threadIdx.x == 0) {
     // inv_norm = 1 / (3 H W V_loss); wconst = V / V_loss (this call's share of the loss)
-    loss[0] = (1.0f - lambda) * r0[0] * inv_norm + lambda * (wconst - r1[0] * inv_norm);
+    loss[0] = kind == kLossL1   ? r0[0] * inv_norm
+              : kind == kLossL2 ? r1[0] * inv_norm
+                                : (1.0f - lambda) * r0[0] * inv_norm + lambda * (wconst - r1[0] * inv_norm);
     loss[1] = r0[0] * inv_norm;  // mean L1
-    loss[2] = r1[0] * inv_norm;  // mean SSIM
+    loss[2] = r1[0] * inv_norm;  // mean SSIM (kind 0) or mean squared error
   }
 }
 
@@ -1587,6 +1643,7 @@ struct nps_gs {
   uint32_t step = 0;
   float lr[6] = {1.6e-4f, 5e-3f, 1e-3f, 5e-2f, 2.5e-3f, 2.5e-3f / 20.0f};
   float lambda = 0.2f;
+  int loss_kind = gs::kLossL1Dssim;  // NPS_GS_LOSS_*
   bool accumulate = false;   // backward adds to the gradients instead of replacing them
   bool deterministic = false;  // two-pass backward reduction (no float atomics)
   // raster variants: pixels per thread (1, 2, 4) and records staged per batch; see nps_gs_autotune
@@ -1638,6 +1695,7 @@ struct nps_gs {
   uint32_t* h_status = nullptr;  // pinned: pair count of the last graph replay
   uint64_t gkey = 0;
   uint32_t gcap = 0, skipped = 0;
+  uint32_t graph_kernels = 0;  // kernel nodes of the captured step (launches per replay)
   // optional per-stage timing with CUDA events on the context stream
   bool timing = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> gtimers;  // event nodes of the captured graph
@@ -2199,23 +2257,39 @@ int nps_gs_loss(nps_gs* o, float* loss3_host) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
   const size_t npix = (size_t)W * H * nv;
-  const dim3 grid(div_up(W, gs::kLT), div_up(H, gs::kLT), nv);
-  const uint32_t nblocks = grid.x * grid.y * grid.z;
-  NPS_TRY(o->maps.ensure(sizeof(float) * 9 * npix));
-  NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
-  NPS_TRY(o->dimg.ensure(sizeof(float4) * npix));
   const uint32_t lv = o->loss_views ? o->loss_views : nv;
   const float inv_norm = (float)(1.0 / (3.0 * (double)W * H * lv));
-  { StageTimer t(o, ST_LOSS);
-  gs::k_ssim_fwd2<<<grid, 256, gs::kSsimFwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H,
-                                                     o->lambda, inv_norm, o->maps.as<float>(),
-                                                     o->partial.as<float>());
-  gs::k_ssim_bwd2<<<grid, 256, gs::kSsimBwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
-                                                     o->maps.as<float>(), W, H, o->lambda, inv_norm,
-                                                     o->dimg.as<float4>());
-  gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->lambda, inv_norm,
-                                               (float)nv / (float)lv, o->loss.as<float>());
-  NPS_CHECK_LAUNCH(); }
+  NPS_TRY(o->dimg.ensure(sizeof(float4) * npix));
+  if (o->loss_kind != gs::kLossL1Dssim) {
+    const dim3 grid(std::min(gs::kPixLossBlocks, div_up((size_t)W * H, 256)), nv);
+    const uint32_t nblocks = grid.x * grid.y;
+    NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
+    StageTimer t(o, ST_LOSS);
+    if (o->loss_kind == gs::kLossL2)
+      gs::k_pix_loss<gs::kLossL2><<<grid, 256, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W * H,
+                                                       inv_norm, o->dimg.as<float4>(), o->partial.as<float>());
+    else
+      gs::k_pix_loss<gs::kLossL1><<<grid, 256, 0, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W * H,
+                                                       inv_norm, o->dimg.as<float4>(), o->partial.as<float>());
+    gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->loss_kind, 0.0f, inv_norm,
+                                                 (float)nv / (float)lv, o->loss.as<float>());
+    NPS_CHECK_LAUNCH();
+  } else {
+    const dim3 grid(div_up(W, gs::kLT), div_up(H, gs::kLT), nv);
+    const uint32_t nblocks = grid.x * grid.y * grid.z;
+    NPS_TRY(o->maps.ensure(sizeof(float) * 9 * npix));
+    NPS_TRY(o->partial.ensure(sizeof(float) * 2 * nblocks));
+    StageTimer t(o, ST_LOSS);
+    gs::k_ssim_fwd2<<<grid, 256, gs::kSsimFwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(), W, H,
+                                                       o->lambda, inv_norm, o->maps.as<float>(),
+                                                       o->partial.as<float>());
+    gs::k_ssim_bwd2<<<grid, 256, gs::kSsimBwdSmem, s>>>(o->img.as<float4>(), o->tgt, o->tids.as<uint32_t>(),
+                                                       o->maps.as<float>(), W, H, o->lambda, inv_norm,
+                                                       o->dimg.as<float4>());
+    gs::k_loss_reduce<<<1, gs::kThreads, 0, s>>>(o->partial.as<float>(), nblocks, o->loss_kind, o->lambda,
+                                                 inv_norm, (float)nv / (float)lv, o->loss.as<float>());
+    NPS_CHECK_LAUNCH();
+  }
   if (loss3_host) {
     NPS_CUDA(cudaMemcpyAsync(loss3_host, o->loss.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, s));
     NPS_CUDA(cudaStreamSynchronize(s));
@@ -2389,6 +2463,18 @@ static int gs_capture(nps_gs* o) {
     set_error("graph capture failed: %s", cudaGetErrorString(ee));
     return NPS_ERR_CUDA;
   }
+  // kernel launches per replay: the graph's kernel nodes
+  size_t nn = 0;
+  uint32_t nk = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+      for (size_t i = 0; i < nn; ++i) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++nk;
+      }
+  }
+  o->graph_kernels = nk;
   const cudaError_t ie = cudaGraphInstantiate(&o->gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (ie != cudaSuccess) {
@@ -2706,6 +2792,7 @@ int nps_gs_save(nps_gs* o, const char* path) {
   for (int k = 0; k < 6; ++k) h.lr[k] = o->lr[k];
   for (int k = 0; k < 3; ++k) h.bg[k] = o->bg[k];
   h.lambda = o->lambda;
+  h.reserved[0] = (uint32_t)o->loss_kind;
   FILE* f = std::fopen(path, "wb");
   if (!f) {
     set_error("gs_save: cannot open %s", path);
@@ -2767,6 +2854,7 @@ int nps_gs_load(nps_gs* o, const char* path) {
   for (int k = 0; k < 6; ++k) o->lr[k] = h.lr[k];
   for (int k = 0; k < 3; ++k) o->bg[k] = h.bg[k];
   o->lambda = h.lambda;
+  o->loss_kind = h.reserved[0] <= (uint32_t)gs::kLossL2 ? (int)h.reserved[0] : gs::kLossL1Dssim;
   o->fwd_valid = o->loss_valid = false;
   o->gkey = 0;
   o->skip_seen = 0;
@@ -2890,6 +2978,19 @@ int nps_gs_autotune(nps_gs* o, const char* cache_path, int* choice4, float* time
   return NPS_OK;
 }
 
+int nps_gs_set_loss(nps_gs* o, int kind, float ssim_weight) {
+  NPS_TRY(check_gs(o));
+  if (kind < gs::kLossL1Dssim || kind > gs::kLossL2 || !(ssim_weight >= 0.0f && ssim_weight <= 1.0f)) {
+    set_error("gs_set_loss: kind %d (0: L1 + D-SSIM, 1: L1, 2: L2), SSIM weight %g (0..1)", kind, ssim_weight);
+    return NPS_ERR_INVALID;
+  }
+  o->loss_kind = kind;
+  o->lambda = ssim_weight;
+  o->loss_valid = false;
+  o->gkey = 0;
+  return NPS_OK;
+}
+
 int nps_gs_set_deterministic(nps_gs* o, int enable) {
   NPS_TRY(check_gs(o));
   o->deterministic = enable != 0;
@@ -2937,6 +3038,7 @@ int nps_gs_stats(nps_gs* o, nps_stats* out) {
   NPS_TRY(check_gs(o));
   if (!out) return NPS_ERR_INVALID;
   o->stats.step_count = o->step;
+  o->stats.reserved[0] = o->graph_kernels;
   o->stats.reserved[1] = o->skipped;
   {
     // raster staging waits that timed out (a device counter; 0 unless the hardware misbehaved)

@@ -142,6 +142,12 @@ class GaussianTrainer:
         call("nps_gs_loss", self._h, l3.ctypes.data if read_back else None)
         return tuple(float(x) for x in l3) if read_back else None
 
+    LOSS_KINDS = {"l1_dssim": 0, "l1": 1, "l2": 2}
+
+    def set_loss(self, kind: str = "l1_dssim", ssim_weight: float = 0.2):
+        """Loss of the fused path: "l1_dssim" ((1 - w) L1 + w D-SSIM), "l1" or "l2"."""
+        call("nps_gs_set_loss", self._h, self.LOSS_KINDS[kind], float(ssim_weight))
+
     def backward(self, dl_dimage=None):
         p = None
         if dl_dimage is not None:
@@ -310,8 +316,8 @@ class GaussianTrainer:
     def stats(self) -> dict:
         st = _lib.nps_stats()
         call("nps_gs_stats", self._h, ctypes.byref(st))
-        return dict(pairs=st.pairs, step_count=st.step_count, skipped_steps=st.reserved[1],
-                    staging_timeouts=st.reserved[2])
+        return dict(pairs=st.pairs, step_count=st.step_count, graph_kernels=st.reserved[0],
+                    skipped_steps=st.reserved[1], staging_timeouts=st.reserved[2])
 
     STAGES = ("preprocess", "depth_sort", "emit", "tile_sort", "ranges", "raster_fwd", "loss", "raster_bwd",
               "project_bwd", "adam")

@@ -13,9 +13,10 @@
 //     16x16, per-tile lists ordered by (f32 view depth, index);
 //   * compositing with alpha = min(0.99, o * G), skip alpha < 1/255, stop
 //     before T would fall below 1e-4;
-//   * loss (1 - l) mean|x - y| + l (1 - mean SSIM), 11x11 Gaussian window
-//     (sigma 1.5), zero padding, C1 = 0.01^2, C2 = 0.03^2, l = 0.2, mean over
-//     views.
+//   * loss, by kind: 0 = (1 - l) mean|x - y| + l (1 - mean SSIM), 11x11
+//     Gaussian window (sigma 1.5), zero padding, C1 = 0.01^2, C2 = 0.03^2,
+//     l = 0.2 by default; 1 = mean|x - y|; 2 = mean (x - y)^2; means over the
+//     3 H W V colour values.
 // Two products:
 //   orc_gs_forward / orc_gs_loss / orc_gs_backward / orc_gs_adam: the fp32
 //     training step (also the timed CPU baseline, OpenMP over tiles);
@@ -37,6 +38,8 @@ namespace {
 
 constexpr double kLowpass = 0.3, kNear = 0.2, kAlphaMin = 1.0 / 255.0, kAlphaMax = 0.99, kTMin = 1e-4;
 constexpr int kWin = 11;
+// loss kinds (the library's NPS_GS_LOSS_* values)
+constexpr int kLossL1Dssim = 0, kLossL1 = 1, kLossL2 = 2;
 
 template <class T>
 struct PreG {
@@ -287,10 +290,11 @@ void render_view(const T* params, uint32_t n, int deg, const float* view, uint32
 
 template <class T>
 T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W, uint32_t H,
-             const float* bg, const float* tgt_all, const uint32_t* tids, double lambda, Frozen* frz, bool replay) {
+             const float* bg, const float* tgt_all, const uint32_t* tids, double lambda, int kind, Frozen* frz,
+             bool replay) {
   const size_t np = (size_t)W * H;
   std::vector<T> img(3 * np);
-  T l1 = 0, ss = 0;
+  T l1 = 0, ss = 0, sq = 0;
   if (frz && !replay) frz->l1sign.assign(3 * np * nv, 0);
   for (uint32_t v = 0; v < nv; ++v) {
     render_view<T>(params, n, deg, views + (size_t)kViewRec * v, W, H, bg, v, img.data(), nullptr, nullptr, frz,
@@ -302,6 +306,23 @@ T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t 
           T d = img[3 * i + c] - (T)y4[4 * i + c];
           frz->l1sign[(size_t)v * 3 * np + 3 * i + c] = d > 0 ? 1 : (d < 0 ? -1 : 0);
         }
+    if (kind == kLossL2) {
+      for (size_t i = 0; i < np; ++i)
+        for (int c = 0; c < 3; ++c) {
+          const T d = img[3 * i + c] - (T)y4[4 * i + c];
+          sq += d * d;
+        }
+      continue;
+    }
+    if (kind == kLossL1) {
+      const int8_t* sg = (frz && replay) ? &frz->l1sign[(size_t)v * 3 * np] : nullptr;
+      for (size_t i = 0; i < np; ++i)
+        for (int c = 0; c < 3; ++c) {
+          const T d = img[3 * i + c] - (T)y4[4 * i + c];
+          l1 += sg ? (T)sg[3 * i + c] * d : (d < 0 ? -d : d);
+        }
+      continue;
+    }
     T a, b;
     ssim_terms<T>(img.data(), y4, W, H, &a, &b, nullptr, 0,
                   (frz && replay) ? &frz->l1sign[(size_t)v * 3 * np] : nullptr);
@@ -309,6 +330,8 @@ T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t 
     ss += b;
   }
   const T inv = (T)1 / ((T)3 * (T)np * (T)nv);
+  if (kind == kLossL2) return sq * inv;
+  if (kind == kLossL1) return l1 * inv;
   return ((T)1 - (T)lambda) * l1 * inv + (T)lambda * ((T)1 - ss * inv);
 }
 
@@ -355,18 +378,35 @@ int orc_gs_forward(const float* params, uint32_t n, int deg, const float* views,
   return 0;
 }
 
-// fp32 loss and dL/dimage (V x H x W x 4, alpha channel 0); loss3 = (loss, mean L1, mean SSIM)
+// fp32 loss and dL/dimage (V x H x W x 4, alpha channel 0).  loss3 =
+// (loss, mean |x - y|, mean SSIM) for kind 0, (loss, mean |x - y|, mean
+// (x - y)^2) for kinds 1 and 2.
 int orc_gs_loss(const float* img, const float* tgt_all, const uint32_t* tids, uint32_t nv, uint32_t W, uint32_t H,
-                float lambda, float* loss3, float* dimg) {
+                float lambda, int kind, float* loss3, float* dimg) {
   const size_t np = (size_t)W * H;
   const auto w = ssim_window();
   const float inv = (float)(1.0 / (3.0 * (double)np * nv));
-  double l1 = 0, ss = 0;
+  double l1 = 0, ss = 0, sq = 0;
   std::vector<float> x3(3 * np), P, c1(np), c2(np), c3(np), tmp(np);
   for (uint32_t v = 0; v < nv; ++v) {
     for (size_t i = 0; i < np; ++i)
       for (int c = 0; c < 3; ++c) x3[3 * i + c] = img[((size_t)v * np + i) * 4 + c];
     const float* y4 = tgt_all + (size_t)tids[v] * np * 4;
+    if (kind != kLossL1Dssim) {
+      for (size_t i = 0; i < np; ++i) {
+        for (int c = 0; c < 3; ++c) {
+          const float d = x3[3 * i + c] - y4[4 * i + c];
+          l1 += std::fabs(d);
+          sq += (double)d * d;
+          if (dimg) {
+            const float sgn = d > 0 ? 1.0f : (d < 0 ? -1.0f : 0.0f);
+            dimg[((size_t)v * np + i) * 4 + c] = kind == kLossL2 ? 2.0f * d * inv : sgn * inv;
+          }
+        }
+        if (dimg) dimg[((size_t)v * np + i) * 4 + 3] = 0.0f;
+      }
+      continue;
+    }
     float a, b;
     ssim_terms<float>(x3.data(), y4, W, H, &a, &b, &P, -lambda * inv, nullptr);
     l1 += a;
@@ -387,9 +427,14 @@ int orc_gs_loss(const float* img, const float* tgt_all, const uint32_t* tids, ui
     for (size_t i = 0; i < np; ++i) dimg[((size_t)v * np + i) * 4 + 3] = 0.0f;
   }
   if (loss3) {
-    loss3[0] = (float)((1.0 - lambda) * l1 * inv + lambda * (1.0 - ss * inv));
+    if (kind == kLossL1Dssim) {
+      loss3[0] = (float)((1.0 - lambda) * l1 * inv + lambda * (1.0 - ss * inv));
+      loss3[2] = (float)(ss * inv);
+    } else {
+      loss3[0] = (float)((kind == kLossL2 ? sq : l1) * inv);
+      loss3[2] = (float)(sq * inv);
+    }
     loss3[1] = (float)(l1 * inv);
-    loss3[2] = (float)(ss * inv);
   }
   return 0;
 }
@@ -668,31 +713,34 @@ int orc_gs_adc(const float* params, const float* m, const float* v, const float*
 
 // FP64 loss (no freezing) — for sanity checks.
 double orc_gs_loss_f64(const float* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W,
-                       uint32_t H, const float* bg, const float* tgt_all, const uint32_t* tids, double lambda) {
+                       uint32_t H, const float* bg, const float* tgt_all, const uint32_t* tids, double lambda,
+                       int kind) {
   std::vector<double> p((size_t)n * kP);
   for (size_t i = 0; i < p.size(); ++i) p[i] = params[i];
-  return total_loss<double>(p.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, nullptr, false);
+  return total_loss<double>(p.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, kind, nullptr, false);
 }
 
 // FP64 central differences of the loss w.r.t. the flat parameter indices
 // pidx[0..np) (index = gaussian * 64 + field), step h = h_rel * max(|p|, 1e-3),
 // with the base point's discrete decisions frozen.
 int orc_gs_loss_cd(const float* params, uint32_t n, int deg, const float* views, uint32_t nv, uint32_t W, uint32_t H,
-                   const float* bg, const float* tgt_all, const uint32_t* tids, double lambda, const uint32_t* pidx,
-                   uint32_t npidx, double h_rel, double* out) {
+                   const float* bg, const float* tgt_all, const uint32_t* tids, double lambda, int kind,
+                   const uint32_t* pidx, uint32_t npidx, double h_rel, double* out) {
   std::vector<double> p((size_t)n * kP);
   for (size_t i = 0; i < p.size(); ++i) p[i] = params[i];
   Frozen frz;
-  total_loss<double>(p.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, &frz, false);
+  total_loss<double>(p.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, kind, &frz, false);
 #pragma omp parallel for schedule(dynamic, 1)
   for (long k = 0; k < (long)npidx; ++k) {
     std::vector<double> q(p);
     const size_t j = pidx[k];
     const double h = h_rel * std::max(std::fabs(p[j]), 1e-3);
     q[j] = p[j] + h;
-    const double lp = total_loss<double>(q.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, &frz, true);
+    const double lp =
+        total_loss<double>(q.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, kind, &frz, true);
     q[j] = p[j] - h;
-    const double lm = total_loss<double>(q.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, &frz, true);
+    const double lm =
+        total_loss<double>(q.data(), n, deg, views, nv, W, H, bg, tgt_all, tids, lambda, kind, &frz, true);
     out[k] = (lp - lm) / (2 * h);
   }
   return 0;

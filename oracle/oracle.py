@@ -138,14 +138,21 @@ def gs_forward(params, deg, views48, w, h, bg=(0.0, 0.0, 0.0)):
     return img, nc
 
 
-def gs_loss(img, targets, tids, lam=0.2):
+LOSS_KINDS = {"l1_dssim": 0, "l1": 1, "l2": 2}
+
+
+def gs_loss(img, targets, tids, lam=0.2, loss="l1_dssim"):
+    """fp32 loss and dL/dimage.  loss: "l1_dssim" ((1 - lam) L1 + lam D-SSIM;
+    l3 = loss, mean L1, mean SSIM), "l1" or "l2" (l3 = loss, mean L1, mean
+    squared error)."""
     img = _f32(img)
     nv, h, w, _ = img.shape
     targets = _f32(targets)
     tids = np.ascontiguousarray(tids, np.uint32)
     l3 = np.zeros(3, np.float32)
     dimg = np.zeros_like(img)
-    lib().orc_gs_loss(_p(img, F), _p(targets, F), _p(tids, U), nv, w, h, ctypes.c_float(lam), _p(l3, F), _p(dimg, F))
+    lib().orc_gs_loss(_p(img, F), _p(targets, F), _p(tids, U), nv, w, h, ctypes.c_float(lam), LOSS_KINDS[loss],
+                      _p(l3, F), _p(dimg, F))
     return l3, dimg
 
 
@@ -181,16 +188,18 @@ def gs_adc(params, m, v, adc_grad, adc_denom, cap, seed, thresh=2e-4, split_scal
     return op[:k], om[:k], ov[:k], c
 
 
-def gs_loss_f64(params, deg, views48, w, h, targets, tids, lam=0.2, bg=(0.0, 0.0, 0.0)):
+def gs_loss_f64(params, deg, views48, w, h, targets, tids, lam=0.2, bg=(0.0, 0.0, 0.0), loss="l1_dssim"):
     L = _setup_gs()
     params = _f32(params)
     views48 = _f32(views48)
     tids = np.ascontiguousarray(tids, np.uint32)
     return L.orc_gs_loss_f64(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h,
-                             _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam))
+                             _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam),
+                             LOSS_KINDS[loss])
 
 
-def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=0.2, bg=(0.0, 0.0, 0.0)):
+def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=0.2, bg=(0.0, 0.0, 0.0),
+               loss="l1_dssim"):
     """FP64 central differences of the loss w.r.t. flat parameter indices."""
     params = _f32(params)
     views48 = _f32(views48)
@@ -198,8 +207,8 @@ def gs_loss_cd(params, deg, views48, w, h, targets, tids, pidx, h_rel=1e-4, lam=
     pidx = np.ascontiguousarray(pidx, np.uint32)
     out = np.zeros(len(pidx), np.float64)
     lib().orc_gs_loss_cd(_p(params, F), params.shape[0], deg, _p(views48, F), views48.shape[0], w, h,
-                         _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam), _p(pidx, U),
-                         len(pidx), ctypes.c_double(h_rel), _p(out, D))
+                         _p(_f32(bg), F), _p(_f32(targets), F), _p(tids, U), ctypes.c_double(lam), LOSS_KINDS[loss],
+                         _p(pidx, U), len(pidx), ctypes.c_double(h_rel), _p(out, D))
     return out
 
 

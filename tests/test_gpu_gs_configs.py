@@ -1,0 +1,240 @@
+"""The Gaussian trainer on the benchmark workloads, checked against the CPU
+oracle (oracle/nps_oracle_gs.cpp):
+
+* the 1,024-Gaussian gradient check at 64 x 64 as specified: L2 loss against
+  a random fp32 target, deterministic two-pass backward, gradients against
+  FP64 central differences (h = 1e-4 relative);
+* the 16,384-Gaussian single-view fit at 256 x 256 with the L1 loss;
+* the headline workload itself (200k Gaussians SH3, 800 x 800, 8 of 32
+  sphere cameras, L1 + 0.2 D-SSIM): the images, loss and gradients of the
+  benchmark's first step against the oracle's;
+* the paired differentiation call: a backward given an external dL/dimage.
+
+Tolerances are stated per test."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+import oracle as orc  # noqa: E402
+from gs_scenes import gs_scene, gs_targets, gs_views  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def trainer_cls():
+    from nprush_b200 import build
+    build.build()
+    from nprush_b200.gaussians import GaussianTrainer
+    return GaussianTrainer
+
+
+def _rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("loss", ["l1", "l2"])
+def test_pixel_losses_match_oracle(trainer_cls, loss):
+    """L1 and L2 losses: loss values 1e-6 relative, dL/dimage 1e-6 relative
+    (exact arithmetic of one term per value), gradients 1e-4 relative L2."""
+    n, w, h, deg = 3000, 96, 80, 2
+    p = gs_scene(n, 91, deg=deg, log_scale_mean=-3.5)
+    eyes = ((0.0, 0.0, 4.0), (3.0, 1.0, 2.5))
+    vp, vpi, views = gs_views(w, h, eyes)
+    tg = gs_targets(3, w, h, 92)
+    tids = np.array([2, 0], np.uint32)
+    t = trainer_cls(n, sh_degree=deg, params=p)
+    t.set_loss(loss)
+    t.set_targets(tg)
+    t.set_views(vp, vpi, tids)
+    t.forward()
+    l3 = t.loss()
+    t.backward()
+    img, dimg = t.read_image()
+    g = t.read_state()["grads"]
+    rimg, rnc = orc.gs_forward(p, deg, views, w, h)
+    np.testing.assert_allclose(img, rimg, atol=1e-5, rtol=0)
+    rl3, rdimg = orc.gs_loss(rimg, tg, tids, loss=loss)
+    np.testing.assert_allclose(l3, rl3, rtol=1e-5, atol=1e-9)
+    # dL/dimage from the device's image (the oracle's differs from it by 1e-7)
+    _, rdimg_dev = orc.gs_loss(img, tg, tids, loss=loss)
+    np.testing.assert_allclose(dimg, rdimg_dev, rtol=1e-6, atol=1e-12)
+    rg = orc.gs_backward(p, deg, views, w, h, rimg, rnc, rdimg)
+    used = np.r_[0:11, 12:12 + 3 * (deg + 1) ** 2]
+    assert _rel_l2(g[:, used], rg[:, used]) < 1e-4
+    # the mean squared error is what the L2 loss is
+    if loss == "l2":
+        assert abs(l3[0] - l3[2]) <= 1e-7 * abs(l3[0])
+
+
+def test_gradient_check_l2_fp64_central_differences(trainer_cls):
+    """1,024 Gaussians at 64 x 64, one view, L2 loss against a random fp32
+    target (N(0.5, 0.2) clamped to [0, 1]), deterministic two-pass reduction:
+    the parameter gradients against FP64 central differences of the loss (h =
+    1e-4 relative).  The oracle freezes the base point's discrete decisions
+    (tile lists, alpha skips and clamps, early termination, colour clamps), so
+    every sampled parameter lies on a smooth piece of the loss and the central
+    difference is that piece's derivative.  Bars: relative L2 error at most
+    1e-4 over all sampled values and over each parameter field; per value,
+    relative to max(|cd|, 1e-3 max|cd|), at most 1e-4 at the 99th percentile
+    and 1e-3 at the maximum.  The fp32 oracle's own backward, checked the
+    same way on the CPU, is within 3e-6 relative L2."""
+    n, w, h, deg = 1024, 64, 64, 0
+    p = gs_scene(n, 2, deg=deg)
+    vp, vpi, views = gs_views(w, h)
+    tg = gs_targets(1, w, h, 3)
+    tids = np.zeros(1, np.uint32)
+    t = trainer_cls(n, sh_degree=deg, params=p)
+    t.set_loss("l2")
+    t.set_deterministic(True)
+    t.set_targets(tg)
+    t.set_views(vp, vpi, tids)
+    t.forward()
+    l3 = t.loss()
+    t.backward()
+    g = t.read_state()["grads"]
+    assert abs(l3[0] - orc.gs_loss_f64(p, deg, views, w, h, tg, tids, loss="l2")) < 1e-6 * l3[0]
+    rng = np.random.default_rng(1)
+    touched = np.nonzero(np.abs(g[:, 0]) > 0)[0]
+    assert len(touched) > 500
+    gi = rng.choice(touched, 120, replace=False)
+    fields = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 13, 14]
+    pidx = np.array([i * 64 + f for i in gi for f in fields], np.uint32)
+    cd = orc.gs_loss_cd(p, deg, views, w, h, tg, tids, pidx, loss="l2")
+    an = g.reshape(-1)[pidx].astype(np.float64)
+    rel_l2 = _rel_l2(an, cd)
+    A, C = an.reshape(-1, len(fields)), cd.reshape(-1, len(fields))
+    per_field = [_rel_l2(A[:, k], C[:, k]) for k in range(len(fields))]
+    rel = np.abs(an - cd) / np.maximum(np.abs(cd), 1e-3 * np.abs(cd).max())
+    q99, mx = float(np.quantile(rel, 0.99)), float(rel.max())
+    report = f"rel L2 {rel_l2:.2e}, worst field {max(per_field):.2e}, q99 {q99:.2e}, max {mx:.2e}"
+    print(report)
+    assert rel_l2 <= 1e-4, report
+    assert max(per_field) <= 1e-4, report
+    assert q99 <= 1e-4, report
+    assert mx <= 1e-3, report
+    # and the same gradient as the fp32 oracle's backward
+    rimg, rnc = orc.gs_forward(p, deg, views, w, h)
+    _, rdimg = orc.gs_loss(rimg, tg, tids, loss="l2")
+    rg = orc.gs_backward(p, deg, views, w, h, rimg, rnc, rdimg)
+    used = np.r_[0:11, 12:15]
+    assert _rel_l2(g[:, used], rg[:, used]) < 1e-5
+
+
+def test_single_view_l1_fit(trainer_cls):
+    """16,384 Gaussians (means U[-1,1]^3, log-scales N(-4, 0.5), opacity
+    logits N(0,1), RGB U[0,1]) fitted by Adam with the L1 loss to a 256 x 256
+    target rendered from a separately seeded teacher (camera fov 60 deg at
+    (0, 0, 4)), 1000 steps: the first step equals the oracle's (image 1e-5,
+    loss 1e-5 relative, gradients 1e-4 relative L2, Adam update 1e-5
+    relative), and the fit lowers the L1 loss by at least a third."""
+    n, w, h, deg = 16384, 256, 256, 0
+    teacher = gs_scene(n, 1, deg=deg)
+    student = gs_scene(n, 0, deg=deg)
+    vp, vpi, views = gs_views(w, h)
+    timg, _ = orc.gs_forward(teacher, deg, views, w, h)
+    tg = timg.copy()
+    tg[..., 3] = 1.0
+    tids = np.zeros(1, np.uint32)
+    t = trainer_cls(n, sh_degree=deg, params=student)
+    t.set_loss("l1")
+    t.set_targets(tg)
+    t.set_views(vp, vpi, tids)
+    t.forward()
+    l3 = t.loss()
+    t.backward()
+    img, _ = t.read_image()
+    g = t.read_state()["grads"]
+    rimg, rnc = orc.gs_forward(student, deg, views, w, h)
+    np.testing.assert_allclose(img, rimg, atol=1e-5, rtol=0)
+    rl3, rdimg = orc.gs_loss(rimg, tg, tids, loss="l1")
+    np.testing.assert_allclose(l3[0], rl3[0], rtol=1e-5)
+    rg = orc.gs_backward(student, deg, views, w, h, rimg, rnc, rdimg)
+    used = np.r_[0:11, 12:15]
+    assert _rel_l2(g[:, used], rg[:, used]) < 1e-4
+    t.adam()
+    pp, mm, vv = student.copy(), np.zeros_like(student), np.zeros_like(student)
+    orc.gs_adam(pp, g, mm, vv, 1, t.LR_DEFAULT)
+    np.testing.assert_allclose(t.read_state()["params"], pp, rtol=1e-5, atol=1e-6)
+    t.set_graph(True)
+    first = l3[0]
+    for _ in range(998):
+        t.train_step()
+    last = t.train_step(read_loss=True)[0]
+    assert last < (2.0 / 3.0) * first, (first, last)
+
+
+def test_external_image_gradient(trainer_cls):
+    """nps_gs_backward with an external dL/dimage: given the fused loss's own
+    dL/dimage it reproduces the fused backward bit for bit (deterministic
+    mode); given any other image gradient it matches the oracle's backward of
+    that gradient (1e-4 relative L2)."""
+    n, w, h, deg = 4000, 96, 80, 1
+    p = gs_scene(n, 95, deg=deg, log_scale_mean=-3.5)
+    eyes = ((0.0, 0.0, 4.0), (2.5, 1.0, 3.0))
+    vp, vpi, views = gs_views(w, h, eyes)
+    tg = gs_targets(2, w, h, 96)
+    t = trainer_cls(n, sh_degree=deg, params=p)
+    t.set_deterministic(True)
+    t.set_targets(tg)
+    t.set_views(vp, vpi)
+    t.forward()
+    t.loss()
+    t.backward()
+    g_fused = t.read_state()["grads"]
+    img, dimg = t.read_image()
+    t.backward(torch.from_numpy(dimg).cuda())
+    np.testing.assert_array_equal(t.read_state()["grads"], g_fused)
+    rng = np.random.default_rng(97)
+    ext = rng.normal(0, 1e-5, dimg.shape).astype(np.float32)
+    ext[..., 3] = 0.0
+    t.backward(torch.from_numpy(ext).cuda())
+    g_ext = t.read_state()["grads"]
+    rimg, rnc = orc.gs_forward(p, deg, views, w, h)
+    rg = orc.gs_backward(p, deg, views, w, h, rimg, rnc, ext)
+    used = np.r_[0:11, 12:12 + 3 * (deg + 1) ** 2]
+    assert _rel_l2(g_ext[:, used], rg[:, used]) < 1e-4
+
+
+def test_benchmark_workload_matches_oracle(trainer_cls):
+    """The benchmark's own first step (bench.py: 200k-Gaussian SH3 student of
+    seed 10, targets rendered on the GPU from the 250k-Gaussian teacher of
+    seed 11, 800 x 800, the first 8 of the 32 sphere cameras the schedule
+    draws, L1 + 0.2 D-SSIM) against the oracle on the same inputs: the
+    teacher's render of one target view and all 8 student images within 1e-5
+    absolute per channel, the loss within 1e-5 relative, dL/dimage within
+    1e-6 absolute, the parameter gradients within 1e-4 relative L2."""
+    import bench
+    from nprush_b200.gaussians import random_gaussians, view_records
+
+    vp, vpi, tg, st = bench.build_scene(0)
+    sel = bench.view_schedule(1)[0]
+    V, W, H = bench.VIEWS, bench.WIDTH, bench.HEIGHT
+    views = view_records(vp[sel], vpi[sel])
+    tgn = tg.cpu().numpy()
+    timg, _ = orc.gs_forward(random_gaussians(bench.N_TEACHER, 11), bench.SH_DEG, views[:1], W, H)
+    np.testing.assert_allclose(tgn[sel[0], ..., :3], timg[0, ..., :3], atol=1e-5, rtol=0)
+    st.set_targets(tg, borrow=True)
+    st.set_views(vp[sel], vpi[sel], sel)
+    img = torch.zeros((V, H, W, 4), device="cuda")
+    st.forward(out=img)
+    l3 = st.loss()
+    st.backward()
+    g = st.read_state()["grads"]
+    _, dimg = st.read_image()
+    img = img.cpu().numpy()
+    p = random_gaussians(bench.N_GAUSS, 10)
+    rimg, rnc = orc.gs_forward(p, bench.SH_DEG, views, W, H)
+    err = np.abs(img - rimg)
+    assert err.max() <= 1e-5, (float(err.max()), int((err > 1e-5).sum()))
+    rl3, rdimg = orc.gs_loss(rimg, tgn, sel)
+    np.testing.assert_allclose(l3[0], rl3[0], rtol=1e-5)
+    np.testing.assert_allclose(dimg[..., :3], rdimg[..., :3], atol=1e-6, rtol=0)
+    rg = orc.gs_backward(p, bench.SH_DEG, views, W, H, rimg, rnc, rdimg)
+    used = np.r_[0:11, 12:60]
+    rel = _rel_l2(g[:, used], rg[:, used])
+    print(f"benchmark workload: image max err {err.max():.2e}, loss {l3[0]:.6f} vs {rl3[0]:.6f}, grad rel L2 {rel:.2e}")
+    assert rel < 1e-4, rel
+    st.close()
