@@ -1282,12 +1282,19 @@ extern "C" int nps_splat_adc_noalloc(float* splats, float* adam_m, float* adam_v
               kNoAllocMaxSplats);
     return NPS_ERR_CAPACITY;
   }
+  // the kernel moves whole records as float4 (16-byte loads and stores) and
+  // the accumulators as floats: an offset view that breaks either alignment
+  // is rejected here rather than faulting on the device
+  if ((((uintptr_t)splats | (uintptr_t)adam_m | (uintptr_t)adam_v) & 15u) != 0 || ((uintptr_t)grad_accum & 3u) != 0) {
+    set_error("splat_adc_noalloc: splats, adam_m and adam_v must be 16-byte aligned, grad_accum 4-byte aligned");
+    return NPS_ERR_INVALID;
+  }
   uint32_t* scratch = nullptr;
   NPS_TRY(adc_scratch_address(&scratch));
   cudaStream_t s = (cudaStream_t)cuda_stream;
   uint32_t* stats = scratch + kNoAllocMaxSplats;
-  // the dead-slot list is written before it is read; the result word is cleared
-  NPS_CUDA(cudaMemsetAsync(stats, 0, sizeof(uint32_t), s));
+  // no clearing needed: the kernel writes the dead-slot list before reading
+  // it, and writes the result word at its end on every call
   compat::k_adc<<<1, compat::kAdcThreads, 0, s>>>(splats, adam_m, adam_v, grad_accum, scratch, n, adam_t, stats);
   NPS_CHECK_LAUNCH();
   if (clones_host) {

@@ -23,10 +23,10 @@ torch = pytest.importorskip("torch")
 from scenes import splat_scene  # noqa: E402
 
 
-def state(n, seed):
+def state(n, seed, dead_fraction=0.35):
     rng = np.random.default_rng(seed)
     s = splat_scene(n, seed)
-    dead = rng.random(n) < 0.35
+    dead = rng.random(n) < dead_fraction
     s[dead, 7] = 0.0
     s[::7, 3] = 0.002; s[::7, 12] = 0.002; s[::7, 15] = 0.002
     ga = (rng.random(n) * 4e-3).astype(np.float32)
@@ -35,13 +35,12 @@ def state(n, seed):
     return s, m, v, ga
 
 
-def test_noalloc_adc_matches_allocating_entry_point():
+def check_against_allocating(n, seed, dead_fraction=0.35):
     from nprush_b200 import _lib, build
     build.build()
     from nprush_b200.splat import GpuSplatOptimizerManager
     lib = _lib.load()
-    n = 20000
-    s, m, v, ga = state(n, 31)
+    s, m, v, ga = state(n, seed, dead_fraction)
     ref = GpuSplatOptimizerManager(n, init=s)
     dev = [torch.from_numpy(x.copy()).cuda() for x in (s, m, v, ga)]
     stream = torch.cuda.current_stream()
@@ -49,7 +48,7 @@ def test_noalloc_adc_matches_allocating_entry_point():
         if call == 1:
             # the first call filled every dead slot: kill a third of the splats
             # and draw fresh accumulators, identically on both sides
-            rng = np.random.default_rng(32)
+            rng = np.random.default_rng(seed + 1)
             st = ref.read_state()
             s2 = st["splats"].copy()
             s2[rng.random(n) < 0.33, 7] = 0.0
@@ -73,6 +72,29 @@ def test_noalloc_adc_matches_allocating_entry_point():
         np.testing.assert_array_equal(got[1], want["adam_m"])
         np.testing.assert_array_equal(got[2], want["adam_v"])
         np.testing.assert_array_equal(got[3], want["grad_accum"])
+
+
+def test_noalloc_adc_matches_allocating_entry_point():
+    check_against_allocating(20000, 31)
+
+
+def test_noalloc_adc_at_its_capacity():
+    """At the scratch's limit of 262144 splats with most of them dead, the
+    dead-slot list fills nearly the whole array up to the result words."""
+    check_against_allocating(262144, 33, dead_fraction=0.97)
+
+
+def test_noalloc_adc_rejects_misaligned_buffers():
+    """Offset views that break the kernel's 16-byte (records) or 4-byte
+    (accumulators) alignment are rejected on the host, before any launch."""
+    from nprush_b200 import _lib
+    lib = _lib.load()
+    buf = torch.zeros(4096, device="cuda")
+    p = buf.data_ptr()
+    for args in ((p + 4, p, p, p), (p, p + 8, p, p), (p, p, p + 12, p), (p, p, p, p + 2)):
+        rc = lib.nps_splat_adc_noalloc(*args, 16, ctypes.c_float(0.0), None, None)
+        assert rc == -1  # NPS_ERR_INVALID
+        assert b"aligned" in lib.nps_last_error()
 
 
 def test_noalloc_adc_rejects_sizes_beyond_its_scratch():
