@@ -1,8 +1,9 @@
 """Build recipe for oracle/_ref: the reference's own WGSL compute shaders,
 translated to C++ (oracle/wgsl2cpp.py) and compiled with g++ for the host.
 
-TEST INFRASTRUCTURE ONLY.  Reads the reference checkout (default
-/root/reference, override with NPRUSH_REFERENCE) at build time; outputs go only
+TEST INFRASTRUCTURE ONLY.  Reads the reference checkout (the directory named
+by NPRUSH_REFERENCE, else the one in oracle/reference_path.txt) at build time;
+outputs go only
 to oracle/_ref/ (git-ignored).  Sizes are baked into the shaders exactly as the
 reference bakes them at pipeline creation (`{@NUM_SPLATS}` etc.), so one shared
 object is built per (shader, size) and cached by content hash.
@@ -39,8 +40,21 @@ IMAGE_SHADERS = ("blur", "depth_aware_blur", "splat_edge", "path_trace", "path_t
 STAGE_SHADERS = ("mesh", "envmap", "splat_forward", "bezier_forward")
 
 
+REF_PATH_FILE = HERE / "reference_path.txt"
+
+
 def reference_root() -> Path:
-    return Path(os.environ.get("NPRUSH_REFERENCE", "/root/reference"))
+    """The reference checkout: $NPRUSH_REFERENCE, else the first line of
+    oracle/reference_path.txt (where this build's checkout lies)."""
+    env = os.environ.get("NPRUSH_REFERENCE")
+    if env:
+        return Path(env)
+    if REF_PATH_FILE.is_file():
+        line = REF_PATH_FILE.read_text().strip().splitlines()
+        if line:
+            return Path(line[0].strip())
+    return HERE / "_no_reference_configured"
+
 
 
 def reference_available() -> bool:

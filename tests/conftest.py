@@ -1,4 +1,3 @@
-import os
 import sys
 from pathlib import Path
 
@@ -20,6 +19,11 @@ def reference_available() -> bool:
     return ra()
 
 
+def _reference_root() -> Path:
+    from build_ref import reference_root
+    return reference_root()
+
+
 requires_reference = pytest.mark.skipif(
-    not (Path(os.environ.get("NPRUSH_REFERENCE", "/root/reference")) / "src/lib/gpu").is_dir(),
+    not (_reference_root() / "src/lib/gpu").is_dir(),
     reason="reference checkout not present (oracle/_ref cannot be built)")

@@ -5,7 +5,7 @@ src/lib/gpu/bezier_forward.wgsl vs_main / fs_main, translated to C++ by
 oracle/build_ref.py with the instance counts baked in as their managers bake
 them); the fixed-function steps between them are the restatement in
 oracle/forward_raster.py.  Needs the reference checkout (NPRUSH_REFERENCE,
-default /root/reference); the tests read only the .npz.
+else oracle/reference_path.txt); the tests read only the .npz.
 
 Cases (48 x 40 pixels):
 * splats: 46 seeded splats of random shape, plus one of view depth 110 (past

@@ -5,7 +5,7 @@ reference's own functions (src/lib/gpu/mesh.wgsl vert / frag,
 src/lib/gpu/envmap.wgsl frag, translated to C++ by oracle/build_ref.py); the
 fixed-function rasterisation between them is the restatement in
 oracle/mesh_raster.py.  Needs the reference checkout (NPRUSH_REFERENCE,
-default /root/reference); the GPU tests read only the .npz.
+else oracle/reference_path.txt); the GPU tests read only the .npz.
 
 Scene: ground + spheres and boxes, a long thin wall that runs from behind the
 camera into the view (near-plane clipping) and a 400-unit ground slab that

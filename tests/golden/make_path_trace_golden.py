@@ -3,7 +3,7 @@ the reference's own path tracer (src/lib/gpu/path_trace.wgsl and
 path_trace_resolve.wgsl, translated to C++ and run on the host by
 oracle/build_ref.py).  The BVHs come from the reference's own builder
 (src/lib/gpu/bvh.ts, translated to Python by oracle/ts2py.py).  Needs the
-reference checkout (NPRUSH_REFERENCE, default /root/reference); the GPU tests
+reference checkout (NPRUSH_REFERENCE, else oracle/reference_path.txt); the GPU tests
 read only the .npz.
 
 Cases (image 45 x 37, not a multiple of the 8 x 8 workgroup):

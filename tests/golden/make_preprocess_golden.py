@@ -2,7 +2,7 @@
 own target-preprocessing shaders (src/lib/gpu/blur.wgsl,
 depth_aware_blur.wgsl, splat_edge.wgsl), translated to C++ and run on the
 host by oracle/build_ref.py.  Needs the reference checkout (NPRUSH_REFERENCE,
-default /root/reference); the GPU tests read only the .npz.
+else oracle/reference_path.txt); the GPU tests read only the .npz.
 
     python tests/golden/make_preprocess_golden.py
 """
