@@ -54,6 +54,19 @@ int nps_destroy(nps_ctx* ctx);
 int nps_sync(nps_ctx* ctx);
 /* Uses an external CUDA stream (cudaStream_t) instead of the context's own. */
 int nps_set_stream(nps_ctx* ctx, void* cuda_stream);
+/* Stable sort of n (key, value) pairs of device memory by the low `bits`
+ * bits of the keys (1..32), in place, on the context's stream; waits for it.
+ * The library's onesweep radix sort (no reference counterpart: the reference
+ * builds its tile lists without sorting, splat_backward.wgsl:199-210): one
+ * histogram kernel, then one kernel per 8-bit digit whose tiles find their
+ * output offsets by a bounded decoupled look-back.  spin_limit bounds the
+ * polls of one unpublished tile status (0 = the default, 2^20); stall_tile
+ * (tests; 0xffffffff = none) is treated as never published.  Returns
+ * NPS_ERR_TIMEOUT when a look-back gave up (the output is then unsorted but
+ * nothing outside the buffers is written).  Allocates its work buffers per
+ * call. */
+int nps_sort_pairs(nps_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t n, int bits, uint32_t spin_limit,
+                   uint32_t stall_tile);
 const char* nps_last_error(void);
 const char* nps_version(void);
 
@@ -147,8 +160,8 @@ typedef struct nps_stats {
   uint32_t step_count;     /* dispatch() calls so far */
   uint32_t reserved[3];    /* Bezier: [0] spawns.  Gaussians: [0] kernel launches per replay of the
                               captured train step (its graph's kernel nodes), [1] graph replays that
-                              skipped their update (pair overflow), [2] record-staging waits that
-                              timed out */
+                              skipped their update (pair overflow), [2] bounded device waits
+                              that gave up (raster record staging, sort look-back) */
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
 /* Sets the manager's stepCount (GpuSplatOptimizerManager.ts:380, dispatch()
@@ -271,6 +284,10 @@ enum { NPS_GS_LOSS_L1_DSSIM = 0, NPS_GS_LOSS_L1 = 1, NPS_GS_LOSS_L2 = 2 };
 int nps_gs_set_loss(nps_gs* gs, int kind, float ssim_weight);
 /* dl_dimage: device num_views*h*w*4 floats, or null for the fused loss gradient. */
 int nps_gs_backward(nps_gs* gs, const float* dl_dimage_device);
+/* The same backward with dL/dimage in host memory (num_views*h*w*4 floats,
+ * copied before the backward runs): the paired call for hosts that hold no
+ * device memory of their own (a TypeScript caller through Deno FFI). */
+int nps_gs_backward_host(nps_gs* gs, const float* dl_dimage_host);
 int nps_gs_adam(nps_gs* gs);
 /* forward + loss + backward + Adam.  In graph mode the first call (and any
  * call after the step's shape changed: Gaussian count, views, image size,
@@ -284,18 +301,59 @@ int nps_gs_set_graph(nps_gs* gs, int enable);
 /* Host copies of the last forward's image (num_views*h*w*4: rgb, final T) and
  * of dL/dimage from the last nps_gs_loss (null pointers skipped). */
 int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
-/* Raster variants (no reference counterpart): forward and backward raster
- * kernels exist for (pixels per thread, records staged per batch) in
- * (1, 256), (2, 128), (2, 256), (4, 64), (4, 128): 256 / ppt threads per 16 x
- * 16 tile.  A stage of 0 means 256 / ppt.  nps_gs_autotune times all of them
- * on the current views and targets and keeps the fastest; with cache_path it
- * first looks the workload up in that text file (device, image size, views,
- * SH degree, Gaussian count to ~19%) and appends its choice.  choice4 (may be
- * null): forward ppt, forward stage, backward ppt, backward stage; times_ms10
- * (may be null): forward then backward time of each variant in the order
- * above (-1 when the choice came from the cache). */
+/* Tiles and raster variants (no reference counterpart; the reference's
+ * tile is its 16 x 16 workgroup, splat_backward.wgsl:136).  The binning
+ * cuts the image into T x T tiles, T = 8, 16 (default) or 32
+ * (nps_gs_set_tile); the deterministic backward and form 0 below need 16.
+ * Two forms of the forward and backward raster kernels, each for several
+ * (pixels per thread, records staged per batch); T * T / ppt threads cover a
+ * tile:
+ *   form 0, one CTA per (tile, view), records double-buffered, T = 16:
+ *     (1, 256), (2, 128), (2, 256), (4, 64), (4, 128);
+ *   form 1, persistent and warp-specialised: a fixed grid of CTAs pulls the
+ *     (view, tile) items of all views from a queue ordered longest first; in
+ *     each CTA one producer warp stages batches of records into a 3-slot ring
+ *     (bulk copies completing on mbarriers) while the consumer warps
+ *     composite or differentiate, with no CTA-wide barrier in the loop:
+ *     T = 8: (1 or 2, 64 or 128); T = 16: (1, 128), (2 or 4, 64 or 128);
+ *     T = 32: (4, 64 or 128).
+ * nps_gs_set_raster selects one per pass for the current tile (a stage of 0
+ * means the form's default: 256 / ppt for form 0, 128 for form 1);
+ * nps_gs_set_variant selects form 0; nps_gs_set_tile changes the tile (and
+ * switches to that tile's default persistent variants where the current ones
+ * do not serve it); nps_gs_get_raster reports tile, forward form, ppt, stage,
+ * backward form, ppt, stage (choice7).  nps_gs_autotune_raster bins the
+ * current views at every tile size (timing the binning), times every variant
+ * of each tile, forward and backward, and keeps the tile with the smallest
+ * binning + fastest forward + fastest backward, with those variants; with
+ * cache_path it first looks the workload up in that text file (device,
+ * image size, views, SH degree, Gaussian count to ~19%, deterministic mode)
+ * and appends its choice.  choice7 (may be null) as nps_gs_get_raster;
+ * times_ms69 (may be null): for T = 8, 16, 32 in turn, 23 floats: binning,
+ * then the forward and then the backward time of the 11 variants (0, 1,
+ * 256), (0, 2, 128), (0, 2, 256), (0, 4, 64), (0, 4, 128), (1, 1, 64),
+ * (1, 1, 128), (1, 2, 64), (1, 2, 128), (1, 4, 64), (1, 4, 128) (0 where a
+ * variant does not serve the tile; -1 throughout when the choice came from
+ * the cache).  nps_gs_autotune is the same tuner reporting only ppt and stage
+ * (choice4) and the 16 x 16 form-0 times (times_ms10). */
+int nps_gs_set_tile(nps_gs* gs, uint32_t tile);
+int nps_gs_set_raster(nps_gs* gs, int fwd_form, int fwd_ppt, int fwd_stage, int bwd_form, int bwd_ppt,
+                      int bwd_stage);
 int nps_gs_set_variant(nps_gs* gs, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage);
+int nps_gs_get_raster(nps_gs* gs, int* choice7);
+int nps_gs_autotune_raster(nps_gs* gs, const char* cache_path, int* choice7, float* times_ms69);
 int nps_gs_autotune(nps_gs* gs, const char* cache_path, int* choice4, float* times_ms10);
+/* Bounded waits of the radix sorts (depth keys, tile keys).  The sorts are
+ * onesweep radix sorts: each tile of keys finds its output offsets by a
+ * decoupled look-back over the tiles before it, polling each unpublished
+ * tile status at most spin_limit times (0 = the default, 2^20).  A
+ * look-back that gives up counts a timeout (nps_stats.reserved[2]); the
+ * sort's output is then wrong but stays inside its buffers, the train step
+ * skips its Adam update, and the next forward or train step returns
+ * NPS_ERR_TIMEOUT.  stall_tile (tests; 0xffffffff = none) names one tile whose
+ * status is treated as never published, which makes a look-back run out on a
+ * normal input. */
+int nps_gs_set_sort_guard(nps_gs* gs, uint32_t spin_limit, uint32_t stall_tile);
 /* Deterministic mode: the backward reduces each (view, Gaussian) gradient in
  * two passes (per-pair tile sums stored, then summed per record in sorted-pair
  * order) instead of with float atomics, so repeated runs are bit-identical.

@@ -41,6 +41,7 @@ SIGNATURES = {
     "nps_destroy": [P],
     "nps_sync": [P],
     "nps_set_stream": [P, P],
+    "nps_sort_pairs": [P, P, P, U32, I32, U32, U32],
     "nps_splat_opt_create": [P, U32, PP],
     "nps_splat_opt_destroy": [P],
     "nps_splat_opt_write_params": [P, P, U32, U32, I32],
@@ -94,6 +95,7 @@ SIGNATURES = {
     "nps_gs_loss": [P, P],
     "nps_gs_set_loss": [P, I32, F32],
     "nps_gs_backward": [P, P],
+    "nps_gs_backward_host": [P, P],
     "nps_gs_adam": [P],
     "nps_gs_train_step": [P, P],
     "nps_gs_set_graph": [P, I32],
@@ -116,6 +118,11 @@ SIGNATURES = {
     "nps_gs_adc_buffers": [P, PP, PP],
     "nps_gs_set_deterministic": [P, I32],
     "nps_gs_set_variant": [P, I32, I32, I32, I32],
+    "nps_gs_set_raster": [P, I32, I32, I32, I32, I32, I32],
+    "nps_gs_set_tile": [P, U32],
+    "nps_gs_get_raster": [P, P],
+    "nps_gs_autotune_raster": [P, ctypes.c_char_p, P, P],
+    "nps_gs_set_sort_guard": [P, U32, U32],
     "nps_gs_autotune": [P, ctypes.c_char_p, P, P],
     "nps_gs_adc_features": [P, F32, F32, F32, F32, P, P, P],
     "nps_gs_adc_policy": [P, P, F32, F32, F32, F32, P, P],

@@ -64,15 +64,23 @@ inline unsigned div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b);
 // Work buffers for the device-wide scan and the radix sort.  Sizes depend only
 // on the grid, never on the number of keys, so no host sync is needed.
 struct SortWork {
-  DevBuf hist;      // 256 * grid u32
+  DevBuf hist;      // per-pass digit histograms, tile counters, own timeout counter
   DevBuf partial;   // scan partial sums
+  DevBuf lookback;  // per pass and tile: the published per-digit counts
   DevBuf keys_alt, vals_alt;
+  // bounded look-back: polls of an unpublished tile status before giving up
+  // (counted in *err, or in the work's own counter when err is null); tests
+  // may name one tile whose status is treated as never published
+  uint32_t* err = nullptr;
+  uint32_t spin_limit = 1u << 20;
+  uint32_t stall_tile = 0xffffffffu;
 };
 
 // Exclusive scan of n u32 (n read on the host); writes out[0..n) and *total.
 int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, SortWork& w, cudaStream_t s);
 
-// Stable LSD radix sort of (key, value) pairs by the low `bits` key bits.
+// Stable LSD radix sort (onesweep) of (key, value) pairs by the low `bits`
+// key bits (at most 32, at most 2^30 - 1 pairs).
 // The number of pairs is read from device memory (*count_dev, clamped to cap).
 // keys/vals hold the input; on return *keys_out / *vals_out point at the sorted
 // arrays (either the inputs or the work buffers).

@@ -1079,9 +1079,10 @@ int nps_bezier_opt_destroy(nps_bezier_opt* o) {
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->lacc, &o->pixel_loss, &o->dead, &o->stat,
                     &o->views, &o->own[0], &o->own[1], &o->own[2], &o->own[3], &o->own[4], &o->fwd, &o->bwd,
                     &o->counts, &o->offsets, &o->rects, &o->total, &o->keys, &o->vals, &o->ranges, &o->tabs,
-                    &o->sw.hist, &o->sw.partial, &o->sw.keys_alt, &o->sw.vals_alt, &o->r_rec, &o->r_counts,
+                    &o->sw.hist, &o->sw.partial, &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt, &o->r_rec, &o->r_counts,
                     &o->r_offsets, &o->r_rects, &o->r_total, &o->r_cam, &o->r_keys, &o->r_vals, &o->r_ranges,
-                    &o->r_tabs, &o->r_sw.hist, &o->r_sw.partial, &o->r_sw.keys_alt, &o->r_sw.vals_alt})
+                    &o->r_tabs, &o->r_sw.hist, &o->r_sw.partial, &o->r_sw.lookback, &o->r_sw.keys_alt,
+                    &o->r_sw.vals_alt})
     b->release();
   delete o;
   return NPS_OK;

@@ -794,7 +794,7 @@ struct RenderWork {
   uint32_t pair_cap = 0;
   void release() {
     for (DevBuf* b : {&rec, &counts, &offsets, &rects, &total, &cam, &keys, &vals, &ranges, &tabs, &sw.hist,
-                      &sw.partial, &sw.keys_alt, &sw.vals_alt})
+                      &sw.partial, &sw.lookback, &sw.keys_alt, &sw.vals_alt})
       b->release();
   }
 };
@@ -888,7 +888,7 @@ int nps_splat_opt_destroy(nps_splat_opt* o) {
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->views, &o->tgt_rgba_own,
                     &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->offsets, &o->rects, &o->total,
                     &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->sw.hist, &o->sw.partial,
-                    &o->sw.keys_alt, &o->sw.vals_alt})
+                    &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt})
     b->release();
   if (o->rw) {
     o->rw->release();

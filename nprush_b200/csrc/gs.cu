@@ -64,14 +64,14 @@ struct Rec {  // projected record, 3 x float4 = 48 B
 };
 
 // True if the alpha >= 1/255 ellipse of the record misses the pixel-centre
-// rectangle [x0, x0 + 15] x [y0, y0 + h]: its box misses, or the smallest
+// rectangle [x0, x0 + w] x [y0, y0 + h]: its box misses, or the smallest
 // value of q(d) = ca dx^2 + 2 cb dx dy + cc dy^2 over the rectangle (offsets
 // from the centre) exceeds the level t2.  A conservative skip test: the
 // level carries the footprint's margin.
-__device__ __forceinline__ bool rec_misses_strip(const float4& a, float cc, const float4& c, float x0, float y0,
-                                                 float h) {
-  if ((a.x + c.z < x0) || (a.x - c.z > x0 + 15.0f) || (a.y + c.w < y0) || (a.y - c.w > y0 + h)) return true;
-  const float lx = x0 - a.x, hx = x0 + 15.0f - a.x, ly = y0 - a.y, hy = y0 + h - a.y;
+__device__ __forceinline__ bool rec_misses_box(const float4& a, float cc, const float4& c, float x0, float y0,
+                                               float w, float h) {
+  if ((a.x + c.z < x0) || (a.x - c.z > x0 + w) || (a.y + c.w < y0) || (a.y - c.w > y0 + h)) return true;
+  const float lx = x0 - a.x, hx = x0 + w - a.x, ly = y0 - a.y, hy = y0 + h - a.y;
   if (lx <= 0.0f && hx >= 0.0f && ly <= 0.0f && hy >= 0.0f) return false;  // centre inside
   const float ca = a.z, cb = a.w;
   // the form's minimum on each edge (the other coordinate clamped to the edge)
@@ -83,6 +83,10 @@ __device__ __forceinline__ bool rec_misses_strip(const float4& a, float cc, cons
   const float q3 = ca * x_l * x_l + 2.0f * cb * x_l * ly + cc * ly * ly;
   const float q4 = ca * x_h * x_h + 2.0f * cb * x_h * hy + cc * hy * hy;
   return fminf(fminf(q1, q2), fminf(q3, q4)) > c.y;
+}
+__device__ __forceinline__ bool rec_misses_strip(const float4& a, float cc, const float4& c, float x0, float y0,
+                                                 float h) {
+  return rec_misses_box(a, cc, c, x0, y0, 15.0f, h);
 }
 
 // true if the Gaussian's alpha >= 1/255 box misses the warp's pixels
@@ -124,7 +128,7 @@ __device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(
 template <int DEG>
 __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ params, uint32_t n,
                                                     const float* __restrict__ views, uint32_t nv, uint32_t W,
-                                                    uint32_t H, uint32_t tiles_x, uint32_t tiles_y,
+                                                    uint32_t H, uint32_t tiles_x, uint32_t tiles_y, float inv_tile,
                                                     Rec* __restrict__ recs, uint32_t* __restrict__ counts,
                                                     uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
                                                     uint32_t* __restrict__ dvals) {
@@ -155,10 +159,10 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
   if (P.cw > kNear && P.det > 0.0f && op * 255.0f > 1.0f) {
     const float t2 = 2.0f * logf(255.0f * op) * 1.01f;
     const float ex = sqrtf(t2 * P.A), ey = sqrtf(t2 * P.C);
-    const int x0 = max(0, min((int)tiles_x, (int)floorf((P.u - ex) / 16.0f)));
-    const int x1 = max(0, min((int)tiles_x, (int)floorf((P.u + ex) / 16.0f) + 1));
-    const int y0 = max(0, min((int)tiles_y, (int)floorf((P.v - ey) / 16.0f)));
-    const int y1 = max(0, min((int)tiles_y, (int)floorf((P.v + ey) / 16.0f) + 1));
+    const int x0 = max(0, min((int)tiles_x, (int)floorf((P.u - ex) * inv_tile)));
+    const int x1 = max(0, min((int)tiles_x, (int)floorf((P.u + ex) * inv_tile) + 1));
+    const int y0 = max(0, min((int)tiles_y, (int)floorf((P.v - ey) * inv_tile)));
+    const int y1 = max(0, min((int)tiles_y, (int)floorf((P.v + ey) * inv_tile) + 1));
     if (x1 > x0 && y1 > y0) {
       cnt = (uint32_t)((x1 - x0) * (y1 - y0));
       rect = make_uint2((uint32_t)x0 | ((uint32_t)x1 << 16), (uint32_t)y0 | ((uint32_t)y1 << 16));
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
                                                    float4* __restrict__ img, uint32_t* __restrict__ ncontrib,
-                                                   uint32_t* __restrict__ err) {
+                                                   uint32_t* __restrict__ tile_last, uint32_t* __restrict__ err) {
   constexpr int NT = 256 / PPT, SB = NT * SPS;
   static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
   __shared__ __align__(16) Rec s_rec[2][SB];
@@ -428,6 +432,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       break;
     }
   }
+  uint32_t wmax = 0;
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     if (px < W && py + k < H) {
@@ -435,7 +440,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       img[pix] = make_float4(C0[k] + T[k] * bg.x, C1[k] + T[k] * bg.y, C2[k] + T[k] * bg.z, T[k]);
       ncontrib[pix] = last[k];
     }
+    wmax = max(wmax, last[k]);
   }
+  // the tile's last contributor over its pixels (the backward's batch range)
+  wmax = __reduce_max_sync(0xffffffffu, wmax);
+  if ((tid & 31) == 0 && wmax > 0) atomicMax(tile_last + key, wmax);
 #undef NPS_ALL_DONE
 }
 
@@ -1126,6 +1135,8 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
   }
 }
 
+#include "gs_raster_ws.cuh"
+
 // deterministic mode: (record, sorted position) pairs to sort by record
 __global__ void k_det_prep(const uint32_t* __restrict__ sorted_vals, const uint32_t* __restrict__ total, uint32_t cap,
                            uint32_t* __restrict__ keys, uint32_t* __restrict__ pos) {
@@ -1376,17 +1387,23 @@ struct AdamArgs {
 };
 
 // Step state in device memory (so that a captured graph advances it):
-// [0] step counter, [1] skip flag, [2], [3] bias corrections (f32 bits).
+// [0] step counter, [1] skip flag, [2], [3] bias corrections (f32 bits),
+// [4] steps skipped for pair overflow, [6] bounded device waits that gave up
+// (raster staging, sort look-back), [7] the value of [6] the last Adam step saw.
 // The step is skipped when the last forward produced more pairs than the
 // pair buffers hold (only possible in a captured graph, whose capacity is
-// fixed): parameters stay unchanged and the host grows the capacity.
+// fixed: parameters stay unchanged and the host grows the capacity), or when
+// a bounded wait gave up since the last step (its results are incomplete).
 __global__ void k_adam_prep(uint32_t* st, const uint32_t* total, uint32_t cap) {
-  const bool skip = *total > cap;
-  st[1] = skip ? 1u : 0u;
-  if (skip) {
+  const bool overflow = *total > cap;
+  const bool timed_out = st[6] != st[7];
+  st[7] = st[6];
+  st[1] = (overflow || timed_out) ? 1u : 0u;
+  if (overflow) {
     st[4] += 1u;  // skipped steps so far (read by the host after graph replays)
     return;
   }
+  if (timed_out) return;
   const uint32_t step = st[0] + 1;
   st[0] = step;
   st[2] = __float_as_uint((float)(1.0 - pow(0.9, (double)step)));
@@ -1648,6 +1665,10 @@ struct nps_gs {
   bool deterministic = false;  // two-pass backward reduction (no float atomics)
   // raster variants: pixels per thread (1, 2, 4) and records staged per batch; see nps_gs_autotune
   int fwd_ppt = 1, bwd_ppt = 2, fwd_stage = 256, bwd_stage = 128;
+  // raster form: 0 = one CTA per (tile, view), 1 = persistent warp-specialised kernel over a work queue
+  int fwd_form = 0, bwd_form = 0;
+  uint32_t tile = 16;  // tile edge in pixels (8, 16, 32); form 0 and the deterministic backward need 16
+  DevBuf tile_last, ws_order_f, ws_order_b, ws_q;  // per-item last contributor, work queues, queue control
   DevBuf det_part, det_keys, det_pos;
   SortWork sw_det;
   uint32_t loss_views = 0;   // views the loss is averaged over (0: the views of each call)
@@ -1696,6 +1717,7 @@ struct nps_gs {
   uint64_t gkey = 0;
   uint32_t gcap = 0, skipped = 0;
   uint32_t graph_kernels = 0;  // kernel nodes of the captured step (launches per replay)
+  uint32_t timeouts_seen = 0;  // bounded-wait timeouts already reported (device counter stepst[6])
   // optional per-stage timing with CUDA events on the context stream
   bool timing = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> gtimers;  // event nodes of the captured graph
@@ -1816,6 +1838,8 @@ int nps_gs_create(nps_ctx* ctx, uint32_t capacity, uint32_t sh_degree, nps_gs** 
     return rc;
   }
   cudaStream_t s = ctx->stream;
+  // the sorts' look-back timeouts count with the raster kernels' (reported as NPS_ERR_TIMEOUT)
+  o->sw_depth.err = o->sw_tile.err = o->sw_det.err = o->stepst.as<uint32_t>() + 6;
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av}) cudaMemsetAsync(b->p, 0, pb, s);
   cudaMemsetAsync(o->adc_grad.p, 0, sizeof(float) * capacity, s);
   cudaMemsetAsync(o->adc_denom.p, 0, sizeof(float) * capacity, s);
@@ -1849,14 +1873,15 @@ int nps_gs_destroy(nps_gs* o) {
   for (DevBuf* b : {&o->p_alt, &o->m_alt, &o->v_alt, &o->aflags, &o->akeep, &o->acand, &o->akeep_off, &o->acand_off,
                     &o->acnt, &o->aoff, &o->atot, &o->psnr_acc, &o->stepst, &o->afeat, &o->alogits,
                     &o->det_part, &o->det_keys, &o->det_pos, &o->sw_det.hist, &o->sw_det.partial,
-                    &o->sw_det.keys_alt, &o->sw_det.vals_alt})
+                    &o->sw_det.lookback, &o->sw_det.keys_alt, &o->sw_det.vals_alt})
     b->release();
+  for (DevBuf* b : {&o->tile_last, &o->ws_order_f, &o->ws_order_b, &o->ws_q}) b->release();
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
                     &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
                     &o->total, &o->mcount, &o->keys, &o->vals, &o->ranges, &o->img, &o->ncontrib, &o->maps,
                     &o->partial, &o->loss, &o->dimg, &o->g2, &o->sw_depth.hist, &o->sw_depth.partial,
-                    &o->sw_depth.keys_alt, &o->sw_depth.vals_alt, &o->sw_tile.hist, &o->sw_tile.partial,
-                    &o->sw_tile.keys_alt, &o->sw_tile.vals_alt})
+                    &o->sw_depth.lookback, &o->sw_depth.keys_alt, &o->sw_depth.vals_alt, &o->sw_tile.hist,
+                    &o->sw_tile.partial, &o->sw_tile.lookback, &o->sw_tile.keys_alt, &o->sw_tile.vals_alt})
     b->release();
   delete o;
   return NPS_OK;
@@ -2085,30 +2110,107 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 // synchronisation; the pair buffers keep their capacity and the emit kernel
 // drops pairs beyond it (Adam then skips the step, see k_adam_prep).
 // Raster launches of the current forward state, by variant (pixels per thread).
-// Raster variants: (pixels per thread, records staged per batch).
+// Raster variants: (form, pixels per thread, records staged per batch), for
+// a tile edge T.  Form 0: one CTA per (tile, view), records double-buffered
+// (k_fwd, k_bwd2), T = 16 only; form 1: persistent warp-specialised kernels
+// over a longest-first work queue (k_fwd_ws, k_bwd_ws), a 3-slot ring of
+// staged records, T = 8 (1 or 2 pixels per thread), 16 (1, 2, 4) or 32 (4).
 struct RasterVariant {
-  int ppt, stage;
+  int form, ppt, stage;
 };
-static bool valid_variant(int ppt, int stage) {
-  if (ppt != 1 && ppt != 2 && ppt != 4) return false;
-  return stage == 256 / ppt || (stage == 512 / ppt && stage <= 256);
+static bool valid_variant(uint32_t tile, int form, int ppt, int stage) {
+  if (form == 0) {
+    if (tile != 16 || (ppt != 1 && ppt != 2 && ppt != 4)) return false;
+    return stage == 256 / ppt || (stage == 512 / ppt && stage <= 256);
+  }
+  if (form != 1 || (stage != 64 && stage != 128)) return false;
+  if (tile == 8) return ppt == 1 || ppt == 2;
+  if (tile == 16) return (ppt == 1 && stage == 128) || ppt == 2 || ppt == 4;
+  if (tile == 32) return ppt == 4;
+  return false;
 }
-constexpr RasterVariant kVariants[] = {{1, 256}, {2, 128}, {2, 256}, {4, 64}, {4, 128}};
-constexpr int kNumVariants = 5;
+constexpr RasterVariant kVariants[] = {{0, 1, 256}, {0, 2, 128}, {0, 2, 256}, {0, 4, 64}, {0, 4, 128}, {1, 1, 64},
+                                       {1, 1, 128}, {1, 2, 64},  {1, 2, 128}, {1, 4, 64}, {1, 4, 128}};
+constexpr int kNumVariants = 11;
+constexpr uint32_t kTiles[] = {8, 16, 32};
+constexpr int kNumTiles = 3;
+// per tile in the autotuner's times: binning, then the forward and backward time of each variant
+constexpr int kTuneStride = 1 + 2 * kNumVariants;
 
-// Raster launches of the current forward state, by variant.
-static int launch_fwd_raster(nps_gs* o, int ppt, int stage) {
+// Resident CTAs of a persistent kernel on the device (queried once per kernel).
+template <class K>
+static int persistent_grid(nps_gs* o, K kernel, int threads, int* cache) {
+  if (*cache == 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    *cache = per_sm * o->ctx->sm_count;
+  }
+  return *cache;
+}
+
+static int ensure_ws_buffers(nps_gs* o, uint32_t nitems) {
+  NPS_TRY(o->tile_last.ensure(sizeof(uint32_t) * (size_t)nitems));
+  NPS_TRY(o->ws_order_f.ensure(sizeof(uint32_t) * (size_t)nitems));
+  NPS_TRY(o->ws_order_b.ensure(sizeof(uint32_t) * (size_t)nitems));
+  NPS_TRY(o->ws_q.ensure(64));
+  return NPS_OK;
+}
+
+// Raster launches of the current forward state, by variant.  Both forms
+// write every tile's last contributor (tile_last), which orders and bounds
+// the persistent backward whatever form the forward took.
+static int launch_fwd_raster(nps_gs* o, int form, int ppt, int stage) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
-  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t tiles_x = div_up(W, o->tile), tiles_y = div_up(H, o->tile), num_tiles = tiles_x * tiles_y;
+  const uint32_t nitems = num_tiles * nv;
   const uint32_t* rstart = o->ranges.as<uint32_t>();
   const uint32_t* rend = rstart + (size_t)num_tiles * nv;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  NPS_TRY(ensure_ws_buffers(o, nitems));
+  NPS_CUDA(cudaMemsetAsync(o->tile_last.p, 0, sizeof(uint32_t) * (size_t)nitems, s));
+  uint32_t* err = o->stepst.as<uint32_t>() + 6;
+  if (form == 1) {
+    uint32_t* q = o->ws_q.as<uint32_t>();
+    gs::k_order_items<false><<<1, 1024, 0, s>>>(rstart, rend, nullptr, nitems, o->ws_order_f.as<uint32_t>(), q);
+    NPS_CHECK_LAUNCH();
+#define NPS_FWD_WS(TS, PPT, SB)                                                                                \
+  do {                                                                                                         \
+    static int grid_cache = 0;                                                                                 \
+    const int grid = persistent_grid(o, gs::k_fwd_ws<TS, PPT, SB>, TS * TS / PPT + 32, &grid_cache);           \
+    gs::k_fwd_ws<TS, PPT, SB><<<grid, TS * TS / PPT + 32, 0, s>>>(                                             \
+        o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, o->ws_order_f.as<uint32_t>(), q, W, H, tiles_x,   \
+        num_tiles, bg, o->img.as<float4>(), o->ncontrib.as<uint32_t>(), o->tile_last.as<uint32_t>(), err);     \
+  } while (0)
+    if (o->tile == 8) {
+      if (ppt == 1 && stage == 64) NPS_FWD_WS(8, 1, 64);
+      else if (ppt == 1) NPS_FWD_WS(8, 1, 128);
+      else if (stage == 64) NPS_FWD_WS(8, 2, 64);
+      else NPS_FWD_WS(8, 2, 128);
+    } else if (o->tile == 32) {
+      if (stage == 64) NPS_FWD_WS(32, 4, 64);
+      else NPS_FWD_WS(32, 4, 128);
+    } else {
+      if (ppt == 1) NPS_FWD_WS(16, 1, 128);
+      else if (ppt == 2 && stage == 64) NPS_FWD_WS(16, 2, 64);
+      else if (ppt == 2) NPS_FWD_WS(16, 2, 128);
+      else if (stage == 64) NPS_FWD_WS(16, 4, 64);
+      else NPS_FWD_WS(16, 4, 128);
+    }
+#undef NPS_FWD_WS
+    NPS_CHECK_LAUNCH();
+    return NPS_OK;
+  }
+  if (o->tile != 16) {
+    set_error("gs raster: the one-CTA-per-tile kernels need 16 x 16 tiles (tile is %u)", o->tile);
+    return NPS_ERR_STATE;
+  }
   const dim3 grid(tiles_x, tiles_y, nv);
 #define NPS_FWD(PPT, SPS)                                                                                   \
   gs::k_fwd<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,     \
                                                  tiles_x, num_tiles, bg, o->img.as<float4>(),                   \
-                                                 o->ncontrib.as<uint32_t>(), o->stepst.as<uint32_t>() + 6)
+                                                 o->ncontrib.as<uint32_t>(), o->tile_last.as<uint32_t>(), err)
   const int sps = stage * ppt / 256;
   if (ppt == 2 && sps == 2) NPS_FWD(2, 2);
   else if (ppt == 2) NPS_FWD(2, 1);
@@ -2120,19 +2222,58 @@ static int launch_fwd_raster(nps_gs* o, int ppt, int stage) {
   return NPS_OK;
 }
 
-static int launch_bwd_raster(nps_gs* o, int ppt, int stage, const float4* dimg) {
+static int launch_bwd_raster(nps_gs* o, int form, int ppt, int stage, const float4* dimg) {
   cudaStream_t s = o->ctx->stream;
   const uint32_t W = o->w, H = o->h, nv = o->nv;
-  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t tiles_x = div_up(W, o->tile), tiles_y = div_up(H, o->tile), num_tiles = tiles_x * tiles_y;
+  const uint32_t nitems = num_tiles * nv;
   const uint32_t* rstart = o->ranges.as<uint32_t>();
   const uint32_t* rend = rstart + (size_t)num_tiles * nv;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
+  uint32_t* err = o->stepst.as<uint32_t>() + 6;
+  if (form == 1) {
+    NPS_TRY(ensure_ws_buffers(o, nitems));
+    uint32_t* q = o->ws_q.as<uint32_t>() + 2;
+    gs::k_order_items<true><<<1, 1024, 0, s>>>(nullptr, nullptr, o->tile_last.as<uint32_t>(), nitems,
+                                               o->ws_order_b.as<uint32_t>(), q);
+    NPS_CHECK_LAUNCH();
+#define NPS_BWD_WS(TS, PPT, SB)                                                                                \
+  do {                                                                                                         \
+    static int grid_cache = 0;                                                                                 \
+    const int grid = persistent_grid(o, gs::k_bwd_ws<TS, PPT, SB>, TS * TS / PPT + 32, &grid_cache);           \
+    gs::k_bwd_ws<TS, PPT, SB><<<grid, TS * TS / PPT + 32, 0, s>>>(                                             \
+        o->recs.as<gs::Rec>(), o->sorted_vals, rstart, o->tile_last.as<uint32_t>(),                            \
+        o->ws_order_b.as<uint32_t>(), q, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),                    \
+        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err);                                             \
+  } while (0)
+    if (o->tile == 8) {
+      if (ppt == 1 && stage == 64) NPS_BWD_WS(8, 1, 64);
+      else if (ppt == 1) NPS_BWD_WS(8, 1, 128);
+      else if (stage == 64) NPS_BWD_WS(8, 2, 64);
+      else NPS_BWD_WS(8, 2, 128);
+    } else if (o->tile == 32) {
+      if (stage == 64) NPS_BWD_WS(32, 4, 64);
+      else NPS_BWD_WS(32, 4, 128);
+    } else {
+      if (ppt == 1) NPS_BWD_WS(16, 1, 128);
+      else if (ppt == 2 && stage == 64) NPS_BWD_WS(16, 2, 64);
+      else if (ppt == 2) NPS_BWD_WS(16, 2, 128);
+      else if (stage == 64) NPS_BWD_WS(16, 4, 64);
+      else NPS_BWD_WS(16, 4, 128);
+    }
+#undef NPS_BWD_WS
+    NPS_CHECK_LAUNCH();
+    return NPS_OK;
+  }
+  if (o->tile != 16) {
+    set_error("gs raster: the one-CTA-per-tile kernels need 16 x 16 tiles (tile is %u)", o->tile);
+    return NPS_ERR_STATE;
+  }
   const dim3 grid(tiles_x, tiles_y, nv);
 #define NPS_BWD(PPT, SPS)                                                                                     \
   gs::k_bwd2<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,      \
                                                   tiles_x, num_tiles, bg, o->img.as<float4>(),                    \
-                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(),             \
-                                                  o->stepst.as<uint32_t>() + 6)
+                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err)
   const int sps = stage * ppt / 256;
   if (ppt == 1) NPS_BWD(1, 1);
   else if (ppt == 2 && sps == 2) NPS_BWD(2, 2);
@@ -2151,7 +2292,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   }
   cudaStream_t s = o->ctx->stream;
   const uint32_t n = o->n, nv = o->nv, W = o->w, H = o->h;
-  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t tiles_x = div_up(W, o->tile), tiles_y = div_up(H, o->tile), num_tiles = tiles_x * tiles_y;
   const size_t M = (size_t)n * nv;
   const size_t npix = (size_t)W * H * nv;
   if (M >= (1ull << 31) || (uint64_t)num_tiles * nv >= (1ull << 31)) {
@@ -2177,7 +2318,8 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
     { StageTimer t_pre(o, ST_PRE);
 #define NPS_PRE(D)                                                                                          \
   gs::k_preprocess<D><<<div_up(M, 256), 256, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, W, H, \
-                                                      tiles_x, tiles_y, o->recs.as<gs::Rec>(),                  \
+                                                      tiles_x, tiles_y, 1.0f / (float)o->tile,                  \
+                                                      o->recs.as<gs::Rec>(),                                    \
                                                       o->counts.as<uint32_t>(), o->rects.as<uint2>(),           \
                                                       o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>())
     switch (o->sh_deg) {
@@ -2201,8 +2343,18 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
     NPS_TRY(exclusive_scan_u32(o->cnt_sorted.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)M, total, o->sw_tile,
                                s));
     if (!capture) {
+      uint32_t tmo = 0;
       NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      NPS_CUDA(cudaMemcpyAsync(&tmo, o->stepst.as<uint32_t>() + 6, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       NPS_CUDA(cudaStreamSynchronize(s));
+      if (tmo != o->timeouts_seen) {
+        // reported here: the next Adam step must not skip for it again
+        o->timeouts_seen = tmo;
+        k_set_u32<<<1, 1, 0, s>>>(o->stepst.as<uint32_t>() + 7, tmo);
+        set_error("gs_forward: a bounded device wait (sort look-back or raster staging) gave up in this or an "
+                  "earlier call; its results were incomplete and no update used them");
+        return NPS_ERR_TIMEOUT;
+      }
       if (K > o->pair_cap || o->pair_cap == 0) {
         const uint32_t cap = K + K / 4 + 4096;
         NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
@@ -2232,7 +2384,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   o->sorted_vals = vs;
   const float3 bg = make_float3(o->bg[0], o->bg[1], o->bg[2]);
   StageTimer t_fwd(o, ST_FWD);
-  NPS_TRY(launch_fwd_raster(o, o->fwd_ppt, o->fwd_stage));
+  NPS_TRY(launch_fwd_raster(o, o->fwd_form, o->fwd_ppt, o->fwd_stage));
   NPS_CHECK_LAUNCH();
   if (out_rgba) NPS_CUDA(cudaMemcpyAsync(out_rgba, o->img.p, sizeof(float4) * npix, cudaMemcpyDeviceToDevice, s));
   o->fwd_valid = true;
@@ -2310,7 +2462,7 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   }
   cudaStream_t s = o->ctx->stream;
   const uint32_t n = o->n, nv = o->nv, W = o->w, H = o->h;
-  const uint32_t tiles_x = div_up(W, 16), tiles_y = div_up(H, 16), num_tiles = tiles_x * tiles_y;
+  const uint32_t tiles_x = div_up(W, o->tile), tiles_y = div_up(H, o->tile), num_tiles = tiles_x * tiles_y;
   const size_t M = (size_t)n * nv;
   NPS_TRY(o->g2.ensure(sizeof(float) * gs::kG2 * (M + 1)));
   NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
@@ -2320,9 +2472,13 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
   const float4* dimg = dl_dimg ? (const float4*)dl_dimg : o->dimg.as<float4>();
   if (!o->deterministic) {
     StageTimer t(o, ST_BWD);
-    NPS_TRY(launch_bwd_raster(o, o->bwd_ppt, o->bwd_stage, dimg));
+    NPS_TRY(launch_bwd_raster(o, o->bwd_form, o->bwd_ppt, o->bwd_stage, dimg));
     NPS_CHECK_LAUNCH();
   } else if (o->pair_cap > 0) {
+    if (o->tile != 16) {
+      set_error("gs_backward: the deterministic backward needs 16 x 16 tiles (tile is %u)", o->tile);
+      return NPS_ERR_STATE;
+    }
     StageTimer t(o, ST_BWD);
     const uint32_t cap = o->pair_cap;
     NPS_TRY(o->det_part.ensure(sizeof(float) * 10 * (size_t)cap));
@@ -2370,6 +2526,23 @@ int nps_gs_backward(nps_gs* o, const float* dl_dimg) {
     NPS_CHECK_LAUNCH();
   }
   return NPS_OK;
+}
+
+int nps_gs_backward_host(nps_gs* o, const float* dl_dimg_host) {
+  NPS_TRY(check_gs(o));
+  if (!dl_dimg_host) {
+    set_error("gs_backward_host: null image gradient");
+    return NPS_ERR_INVALID;
+  }
+  if (!o->fwd_valid) {
+    set_error("gs_backward: forward first");
+    return NPS_ERR_STATE;
+  }
+  const size_t bytes = sizeof(float4) * (size_t)o->w * o->h * o->nv;
+  NPS_TRY(o->dimg.ensure(bytes));
+  NPS_TRY(copy_in_gs(o->dimg.p, dl_dimg_host, bytes, NPS_MEM_HOST, o->ctx->stream));
+  o->loss_valid = false;  // the stored gradient is no longer the fused loss's
+  return nps_gs_backward(o, o->dimg.as<float>());
 }
 
 int nps_gs_adam(nps_gs* o) {
@@ -2446,6 +2619,8 @@ static int gs_capture(nps_gs* o) {
     cudaError_t e = cudaMemcpyAsync(o->h_status, o->total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(o->h_status + 1, o->stepst.as<uint32_t>() + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(o->h_status + 2, o->stepst.as<uint32_t>() + 6, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) {
       set_error("graph capture: %s", cudaGetErrorString(e));
       rc = NPS_ERR_CUDA;
@@ -2520,6 +2695,12 @@ int nps_gs_train_step(nps_gs* o, float* loss3_host) {
         o->skipped += sk - o->skip_seen;
         o->skip_seen = sk;
         o->gkey = 0;
+      }
+      if (o->h_status[2] != o->timeouts_seen) {
+        o->timeouts_seen = o->h_status[2];
+        set_error("gs_train_step: a bounded device wait (sort look-back or raster staging) gave up in an earlier "
+                  "step (its update was skipped); this step was not run");
+        return NPS_ERR_TIMEOUT;
       }
     }
     if (!o->gexec || key != o->gkey) {
@@ -2854,6 +3035,7 @@ int nps_gs_load(nps_gs* o, const char* path) {
   for (int k = 0; k < 6; ++k) o->lr[k] = h.lr[k];
   for (int k = 0; k < 3; ++k) o->bg[k] = h.bg[k];
   o->lambda = h.lambda;
+  o->timeouts_seen = 0;
   o->loss_kind = h.reserved[0] <= (uint32_t)gs::kLossL2 ? (int)h.reserved[0] : gs::kLossL1Dssim;
   o->fwd_valid = o->loss_valid = false;
   o->gkey = 0;
@@ -2862,28 +3044,102 @@ int nps_gs_load(nps_gs* o, const char* path) {
   return NPS_OK;
 }
 
-int nps_gs_set_variant(nps_gs* o, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage) {
+int nps_gs_set_raster(nps_gs* o, int fwd_form, int fwd_ppt, int fwd_stage, int bwd_form, int bwd_ppt,
+                      int bwd_stage) {
   NPS_TRY(check_gs(o));
-  if (fwd_stage == 0) fwd_stage = 256 / (fwd_ppt ? fwd_ppt : 1);
-  if (bwd_stage == 0) bwd_stage = 256 / (bwd_ppt ? bwd_ppt : 1);
-  if (!valid_variant(fwd_ppt, fwd_stage) || !valid_variant(bwd_ppt, bwd_stage)) {
-    set_error("gs_set_variant: (pixels per thread, records per stage) must be one of (1, 256), (2, 128), (2, 256), "
-              "(4, 64), (4, 128); got (%d, %d) and (%d, %d)", fwd_ppt, fwd_stage, bwd_ppt, bwd_stage);
+  if (fwd_stage == 0) fwd_stage = fwd_form == 1 ? 128 : 256 / (fwd_ppt ? fwd_ppt : 1);
+  if (bwd_stage == 0) bwd_stage = bwd_form == 1 ? 128 : 256 / (bwd_ppt ? bwd_ppt : 1);
+  if (!valid_variant(o->tile, fwd_form, fwd_ppt, fwd_stage) || !valid_variant(o->tile, bwd_form, bwd_ppt, bwd_stage)) {
+    set_error("gs_set_raster: (form, pixels per thread, records per stage) (%d, %d, %d) / (%d, %d, %d) is not a "
+              "variant for %u x %u tiles: form 0 (tile 16) (1, 256), (2, 128), (2, 256), (4, 64), (4, 128); form 1 "
+              "tile 8 (1 or 2, 64 or 128), tile 16 (1, 128), (2 or 4, 64 or 128), tile 32 (4, 64 or 128)",
+              fwd_form, fwd_ppt, fwd_stage, bwd_form, bwd_ppt, bwd_stage, o->tile, o->tile);
     return NPS_ERR_INVALID;
   }
+  o->fwd_form = fwd_form;
   o->fwd_ppt = fwd_ppt;
   o->fwd_stage = fwd_stage;
+  o->bwd_form = bwd_form;
   o->bwd_ppt = bwd_ppt;
   o->bwd_stage = bwd_stage;
   o->gkey = 0;
   return NPS_OK;
 }
 
-// Times every raster variant on the current views and targets (one forward
-// and loss first, then `reps` launches of each variant) and keeps the fastest.
-// The choice is cached in a text file (one line per workload: key and the
-// four numbers) when cache_path is given.
-int nps_gs_autotune(nps_gs* o, const char* cache_path, int* choice4, float* times_ms10) {
+int nps_gs_set_variant(nps_gs* o, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage) {
+  return nps_gs_set_raster(o, 0, fwd_ppt, fwd_stage, 0, bwd_ppt, bwd_stage);
+}
+
+int nps_gs_set_tile(nps_gs* o, uint32_t tile) {
+  NPS_TRY(check_gs(o));
+  if (tile != 8 && tile != 16 && tile != 32) {
+    set_error("gs_set_tile: tile edge %u (8, 16 or 32)", tile);
+    return NPS_ERR_INVALID;
+  }
+  if (tile != 16 && o->deterministic) {
+    set_error("gs_set_tile: the deterministic backward needs 16 x 16 tiles");
+    return NPS_ERR_STATE;
+  }
+  o->tile = tile;
+  // keep the raster variants if they serve the new tile, else its default persistent ones
+  const RasterVariant def = tile == 8 ? RasterVariant{1, 1, 128} : tile == 32 ? RasterVariant{1, 4, 128}
+                                                                              : RasterVariant{1, 2, 128};
+  if (!valid_variant(tile, o->fwd_form, o->fwd_ppt, o->fwd_stage))
+    o->fwd_form = def.form, o->fwd_ppt = def.ppt, o->fwd_stage = def.stage;
+  if (!valid_variant(tile, o->bwd_form, o->bwd_ppt, o->bwd_stage))
+    o->bwd_form = def.form, o->bwd_ppt = def.ppt, o->bwd_stage = def.stage;
+  o->fwd_valid = o->loss_valid = false;
+  o->gkey = 0;
+  return NPS_OK;
+}
+
+int nps_gs_get_raster(nps_gs* o, int* choice7) {
+  NPS_TRY(check_gs(o));
+  if (!choice7) return NPS_ERR_INVALID;
+  choice7[0] = (int)o->tile;
+  choice7[1] = o->fwd_form; choice7[2] = o->fwd_ppt; choice7[3] = o->fwd_stage;
+  choice7[4] = o->bwd_form; choice7[5] = o->bwd_ppt; choice7[6] = o->bwd_stage;
+  return NPS_OK;
+}
+
+// GPU time of the binning stages (projection, depth sort, pair emission, tile
+// sort, ranges) of one eager forward at the current tile size, in ms.
+static int binning_ms(nps_gs* o, float* ms) {
+  const bool timing = o->timing;
+  for (auto& u : o->ev_used) {
+    o->ev_pool.push_back(u.second.first);
+    o->ev_pool.push_back(u.second.second);
+  }
+  o->ev_used.clear();
+  o->timing = true;
+  int rc = gs_forward_impl(o, nullptr, false);
+  o->timing = timing;
+  NPS_TRY(rc);
+  NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  float tot = 0.0f;
+  for (auto& u : o->ev_used) {
+    if (u.first == ST_PRE || u.first == ST_DSORT || u.first == ST_EMIT || u.first == ST_TSORT ||
+        u.first == ST_RANGES) {
+      float t = 0.0f;
+      NPS_CUDA(cudaEventElapsedTime(&t, u.second.first, u.second.second));
+      tot += t;
+    }
+    o->ev_pool.push_back(u.second.first);
+    o->ev_pool.push_back(u.second.second);
+  }
+  o->ev_used.clear();
+  *ms = tot;
+  return NPS_OK;
+}
+
+// The autotuner: for each tile edge (8, 16, 32; 16 only in deterministic
+// mode) it bins the current views (timing the binning), then times every
+// raster variant valid for that tile, forward and backward (three launches
+// each after a warm-up launch), and keeps the tile whose binning + fastest
+// forward + fastest backward is smallest, with those variants.  The choice
+// is cached in a text file (one line per workload: key, tile and the six
+// variant numbers) when cache_path is given.
+int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, float* times_ms69) {
   NPS_TRY(check_gs(o));
   if (!o->tgt || o->nv == 0) {
     set_error("gs_autotune: set views and targets first");
@@ -2891,90 +3147,134 @@ int nps_gs_autotune(nps_gs* o, const char* cache_path, int* choice4, float* time
   }
   cudaDeviceProp prop;
   NPS_CUDA(cudaGetDeviceProperties(&prop, o->ctx->device));
-  // workload key: device, image, views, SH degree, Gaussian count (to ~19%)
+  // workload key: device, image, views, SH degree, Gaussian count (to ~19%), deterministic mode
   char key[256];
   const int nbucket = o->n ? (int)std::lround(4.0 * std::log2((double)o->n)) : 0;
-  std::snprintf(key, sizeof(key), "%s|sm%d|%ux%u|v%u|sh%d|n%d", prop.name, prop.multiProcessorCount, o->w, o->h,
-                o->nv, o->sh_deg, nbucket);
+  std::snprintf(key, sizeof(key), "%s|sm%d|%ux%u|v%u|sh%d|n%d|det%d", prop.name, prop.multiProcessorCount, o->w,
+                o->h, o->nv, o->sh_deg, nbucket, o->deterministic ? 1 : 0);
   for (char* c = key; *c; ++c)
     if (*c == ' ') *c = '_';
-  auto report = [&](bool timed) {
-    if (choice4) {
-      choice4[0] = o->fwd_ppt; choice4[1] = o->fwd_stage;
-      choice4[2] = o->bwd_ppt; choice4[3] = o->bwd_stage;
-    }
-    if (times_ms10 && !timed)
-      for (int i = 0; i < 2 * kNumVariants; ++i) times_ms10[i] = -1.0f;  // from the cache: not timed
+  auto report = [&](bool timed) -> int {
+    if (choice7) NPS_TRY(nps_gs_get_raster(o, choice7));
+    if (times_ms69 && !timed)
+      for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms69[i] = -1.0f;  // from the cache: not timed
+    return NPS_OK;
   };
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "r")) {
-      char k[256];
-      int a = 0, b = 0, c = 0, d = 0;
+      char line[512], k[256];
+      int a[7];
       bool found = false;
-      while (std::fscanf(f, "%255s %d %d %d %d%*[^\n]", k, &a, &b, &c, &d) == 5)
-        if (std::strcmp(k, key) == 0 && valid_variant(a, b) && valid_variant(c, d))
-          found = true, o->fwd_ppt = a, o->fwd_stage = b, o->bwd_ppt = c, o->bwd_stage = d;
+      while (std::fgets(line, sizeof(line), f))
+        if (std::sscanf(line, "%255s %d %d %d %d %d %d %d", k, &a[0], &a[1], &a[2], &a[3], &a[4], &a[5], &a[6]) ==
+                8 &&
+            std::strcmp(k, key) == 0 && valid_variant((uint32_t)a[0], a[1], a[2], a[3]) &&
+            valid_variant((uint32_t)a[0], a[4], a[5], a[6])) {
+          found = true;
+          o->tile = (uint32_t)a[0];
+          o->fwd_form = a[1], o->fwd_ppt = a[2], o->fwd_stage = a[3];
+          o->bwd_form = a[4], o->bwd_ppt = a[5], o->bwd_stage = a[6];
+        }
       std::fclose(f);
       if (found) {
         o->gkey = 0;
-        report(false);
-        return NPS_OK;
+        o->fwd_valid = o->loss_valid = false;
+        return report(false);
       }
     }
   }
-  const bool timing = o->timing;
-  o->timing = false;
-  int rc = gs_forward_impl(o, nullptr, false);
-  if (rc == NPS_OK) rc = nps_gs_loss(o, nullptr);
-  o->timing = timing;
-  NPS_TRY(rc);
+  if (times_ms69)
+    for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms69[i] = 0.0f;  // 0: not a variant of that tile
   cudaStream_t s = o->ctx->stream;
   const uint32_t M = o->n * o->nv;
   NPS_TRY(o->g2.ensure(sizeof(float) * gs::kG2 * ((size_t)M + 1)));
   cudaEvent_t e0, e1;
   NPS_CUDA(cudaEventCreate(&e0));
   NPS_CUDA(cudaEventCreate(&e1));
-  float best[2] = {1e30f, 1e30f};
-  RasterVariant pick[2] = {{o->fwd_ppt, o->fwd_stage}, {o->bwd_ppt, o->bwd_stage}};
+  float best_total = 1e30f;
+  uint32_t best_tile = o->tile;
+  RasterVariant best_pick[2] = {{o->fwd_form, o->fwd_ppt, o->fwd_stage}, {o->bwd_form, o->bwd_ppt, o->bwd_stage}};
   constexpr int kReps = 3;
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int vi = 0; vi < kNumVariants; ++vi) {
-      const RasterVariant& va = kVariants[vi];
-      float tot = 0.0f;
-      for (int r = 0; r <= kReps; ++r) {  // the first launch warms up
-        if (pass == 1) NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
-        NPS_CUDA(cudaEventRecord(e0, s));
-        if (pass == 0) NPS_TRY(launch_fwd_raster(o, va.ppt, va.stage));
-        else NPS_TRY(launch_bwd_raster(o, va.ppt, va.stage, o->dimg.as<float4>()));
-        NPS_CUDA(cudaEventRecord(e1, s));
-        NPS_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.0f;
-        NPS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (r > 0) tot += ms;
+  int rc = NPS_OK;
+  for (int ti = 0; ti < kNumTiles && rc == NPS_OK; ++ti) {
+    const uint32_t tile = kTiles[ti];
+    if (o->deterministic && tile != 16) continue;
+    o->tile = tile;
+    o->fwd_form = 1;  // a variant every tile has, for the binning runs
+    o->fwd_ppt = tile == 8 ? 1 : tile == 32 ? 4 : 2;
+    o->fwd_stage = 128;
+    float bin = 0.0f;
+    if ((rc = binning_ms(o, &bin)) != NPS_OK || (rc = binning_ms(o, &bin)) != NPS_OK) break;  // warm-up, timed
+    if ((rc = nps_gs_loss(o, nullptr)) != NPS_OK) break;
+    float* tt = times_ms69 ? times_ms69 + ti * kTuneStride : nullptr;
+    if (tt) tt[0] = bin;
+    float best[2] = {1e30f, 1e30f};
+    RasterVariant pick[2] = {{1, o->fwd_ppt, 128}, {1, o->fwd_ppt, 128}};
+    for (int pass = 0; pass < 2 && rc == NPS_OK; ++pass) {
+      for (int vi = 0; vi < kNumVariants && rc == NPS_OK; ++vi) {
+        const RasterVariant& va = kVariants[vi];
+        if (!valid_variant(tile, va.form, va.ppt, va.stage)) continue;
+        float tot = 0.0f;
+        for (int r = 0; r <= kReps && rc == NPS_OK; ++r) {  // the first launch warms up
+          if (pass == 1) NPS_CUDA(cudaMemsetAsync(o->g2.p, 0, sizeof(float) * gs::kG2 * M, s));
+          NPS_CUDA(cudaEventRecord(e0, s));
+          rc = pass == 0 ? launch_fwd_raster(o, va.form, va.ppt, va.stage)
+                         : launch_bwd_raster(o, va.form, va.ppt, va.stage, o->dimg.as<float4>());
+          NPS_CUDA(cudaEventRecord(e1, s));
+          NPS_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          NPS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (r > 0) tot += ms;
+        }
+        const float avg = tot / kReps;
+        if (tt) tt[1 + kNumVariants * pass + vi] = avg;
+        if (avg < best[pass]) best[pass] = avg, pick[pass] = va;
       }
-      const float avg = tot / kReps;
-      if (times_ms10) times_ms10[kNumVariants * pass + vi] = avg;
-      if (avg < best[pass]) best[pass] = avg, pick[pass] = va;
+      // the backward is timed after the chosen forward (the persistent
+      // backward's work order comes from the forward's per-tile results)
+      if (pass == 0 && rc == NPS_OK) rc = launch_fwd_raster(o, pick[0].form, pick[0].ppt, pick[0].stage);
+    }
+    const float total = bin + best[0] + best[1];
+    if (rc == NPS_OK && total < best_total) {
+      best_total = total;
+      best_tile = tile;
+      best_pick[0] = pick[0];
+      best_pick[1] = pick[1];
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // the variants write the same images (to rounding); leave a consistent forward state
-  NPS_TRY(launch_fwd_raster(o, pick[0].ppt, pick[0].stage));
-  o->loss_valid = false;
-  o->fwd_ppt = pick[0].ppt;
-  o->fwd_stage = pick[0].stage;
-  o->bwd_ppt = pick[1].ppt;
-  o->bwd_stage = pick[1].stage;
+  o->tile = best_tile;
+  o->fwd_form = best_pick[0].form, o->fwd_ppt = best_pick[0].ppt, o->fwd_stage = best_pick[0].stage;
+  o->bwd_form = best_pick[1].form, o->bwd_ppt = best_pick[1].ppt, o->bwd_stage = best_pick[1].stage;
+  o->fwd_valid = o->loss_valid = false;
   o->gkey = 0;
-  report(true);
+  NPS_TRY(rc);
+  NPS_TRY(report(true));
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "a")) {
-      std::fprintf(f, "%s %d %d %d %d %.4f %.4f\n", key, pick[0].ppt, pick[0].stage, pick[1].ppt, pick[1].stage,
-                   best[0], best[1]);
+      std::fprintf(f, "%s %u %d %d %d %d %d %d %.4f\n", key, best_tile, best_pick[0].form, best_pick[0].ppt,
+                   best_pick[0].stage, best_pick[1].form, best_pick[1].ppt, best_pick[1].stage, best_total);
       std::fclose(f);
     }
   }
+  return NPS_OK;
+}
+
+// The earlier interface: the chosen (pixels per thread, records per stage)
+// of each pass (choice4) and, per pass, the time of the five 16 x 16
+// one-CTA-per-tile variants (times_ms10).
+int nps_gs_autotune(nps_gs* o, const char* cache_path, int* choice4, float* times_ms10) {
+  int c7[7];
+  float t[kNumTiles * kTuneStride];
+  NPS_TRY(nps_gs_autotune_raster(o, cache_path, c7, t));
+  if (choice4) {
+    choice4[0] = c7[2]; choice4[1] = c7[3];
+    choice4[2] = c7[5]; choice4[3] = c7[6];
+  }
+  if (times_ms10)
+    for (int pass = 0; pass < 2; ++pass)
+      for (int vi = 0; vi < 5; ++vi) times_ms10[5 * pass + vi] = t[1 * kTuneStride + 1 + kNumVariants * pass + vi];
   return NPS_OK;
 }
 
@@ -2991,8 +3291,19 @@ int nps_gs_set_loss(nps_gs* o, int kind, float ssim_weight) {
   return NPS_OK;
 }
 
+int nps_gs_set_sort_guard(nps_gs* o, uint32_t spin_limit, uint32_t stall_tile) {
+  NPS_TRY(check_gs(o));
+  for (SortWork* w : {&o->sw_depth, &o->sw_tile}) {
+    w->spin_limit = spin_limit ? spin_limit : (1u << 20);
+    w->stall_tile = stall_tile;
+  }
+  o->gkey = 0;
+  return NPS_OK;
+}
+
 int nps_gs_set_deterministic(nps_gs* o, int enable) {
   NPS_TRY(check_gs(o));
+  if (enable && o->tile != 16) NPS_TRY(nps_gs_set_tile(o, 16));  // the two-pass backward's tiles
   o->deterministic = enable != 0;
   o->gkey = 0;
   return NPS_OK;

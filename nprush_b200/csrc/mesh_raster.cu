@@ -421,7 +421,7 @@ struct nps_mesh {
   uint32_t first_pbr = 0xffffffffu;  // triangles from here on use the PBR stage
   ~nps_mesh() {
     for (DevBuf* b : {&verts, &idx, &vout, &chunks, &offsets, &total, &zbuf, &matcap, &env, &albedo, &nmap, &work.hist,
-                      &work.partial, &work.keys_alt, &work.vals_alt})
+                      &work.partial, &work.lookback, &work.keys_alt, &work.vals_alt})
       b->release();
   }
 };

@@ -1,16 +1,16 @@
 // sort.cu — device-wide exclusive scan and stable LSD radix sort.
 //
-// Used for the (view, tile[, depth]) keys of the binning stage.  The sort is a
-// fixed-grid reduce-then-scan radix sort: per 8-bit digit, an upsweep kernel
-// histograms each block's contiguous key range, a three-kernel scan turns the
-// digit-major histogram into offsets, and a downsweep kernel ranks keys stably
-// (warp-level ranking in original order from per-bit ballots) and scatters them.
-// The grid never depends on the key count (read from device memory), so the
-// whole sort can be captured in a CUDA graph, and there is no inter-block
-// waiting anywhere (no decoupled look-back spin), so it cannot hang.
+// Used for the (view, tile[, depth]) keys of the binning stage.  The sort is
+// a onesweep radix sort: one histogram kernel for all 8-bit digits, then one
+// kernel per digit that ranks each tile of keys stably (warp-level ranking in
+// original order from per-bit ballots), finds the tile's global offsets by a
+// bounded decoupled look-back over the earlier tiles, and scatters.  The grid
+// never depends on the key count (read from device memory), so the whole sort
+// can be captured in a CUDA graph.  The exclusive scan is reduce-then-scan.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "context.h"
 
 namespace nps {
 namespace {
@@ -131,63 +131,100 @@ __device__ __forceinline__ void block_range(const uint32_t* count_dev, uint32_t 
   *t1 = min(*t0 + per, tiles);
 }
 
+// ---------------------------------------------------------------- onesweep
+// One launch per 8-bit digit (Adinets and Merrill's onesweep): a CTA claims
+// the next tile of kTile keys from a counter (tiles are claimed in order, so
+// every tile a CTA waits for belongs to a CTA that is already running), ranks
+// its keys locally and stably, publishes its per-digit counts, and finds the
+// number of keys of each digit in all earlier tiles by looking back through
+// their published counts (decoupled look-back: an aggregate adds and the
+// search goes on, an inclusive prefix adds and ends it), then publishes its
+// own inclusive prefix and scatters.  The digit offsets of a pass come from a
+// histogram of every pass taken in one read of the keys beforehand.
+//
+// Status word per (tile, digit): bits 31..30 flag (0 none yet, 1 aggregate,
+// 2 inclusive prefix), bits 29..0 the count.  The look-back is bounded: a
+// status that stays unpublished for spin_limit polls makes the CTA count a
+// timeout in *err and carry on as if the count were 0; it still publishes
+// its own prefix (so no later tile waits on it) and scatters only inside the
+// output (positions are clamped to the key count), so the results are wrong
+// but the kernel ends and never writes outside its buffers.  For tests,
+// stall_tile names one tile whose status is treated as never published.
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
+
+__device__ __forceinline__ uint32_t ld_status(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Digit histograms of every pass in one read: ghist[pass * 256 + digit].
 template <class K>
-__global__ void __launch_bounds__(kSortThreads) k_upsweep(const K* __restrict__ keys, const uint32_t* count_dev,
-                                                           uint32_t cap, int shift, uint32_t* __restrict__ hist) {
-  __shared__ uint32_t h[kSortWarps][256];
-  const int wid = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&h[0][0])[i] = 0;
+__global__ void __launch_bounds__(kSortThreads) k_hist_all(const K* __restrict__ keys, const uint32_t* count_dev,
+                                                            uint32_t cap, int passes, uint32_t* __restrict__ ghist) {
+  __shared__ uint32_t h[4][256];
+  for (int i = threadIdx.x; i < 4 * 256; i += kSortThreads) (&h[0][0])[i] = 0;
   __syncthreads();
-  uint32_t n, t0, t1;
-  block_range(count_dev, cap, &n, &t0, &t1);
-  const uint32_t end = min(t1 * (uint32_t)kTile, n);
-  for (uint32_t i = t0 * kTile + threadIdx.x; i < end; i += kSortThreads)
-    atomicAdd(&h[wid][(uint32_t)(keys[i] >> shift) & 255u], 1u);
+  const uint32_t n = min(*count_dev, cap);
+  for (uint32_t i = blockIdx.x * kSortThreads + threadIdx.x; i < n; i += gridDim.x * kSortThreads) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(uint32_t)(k >> (8 * p)) & 255u], 1u);
+  }
   __syncthreads();
-  uint32_t s = 0;
-#pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) s += h[w][threadIdx.x];
-  hist[threadIdx.x * gridDim.x + blockIdx.x] = s;  // digit-major
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t c = h[p][threadIdx.x];
+    if (c) atomicAdd(ghist + p * 256 + threadIdx.x, c);
+  }
 }
 
 template <class K>
-__global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                                             K* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                             const uint32_t* count_dev, uint32_t cap, int shift,
-                                                             const uint32_t* __restrict__ offsets) {
+__global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const K* __restrict__ kin,
+                                                               const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                                                               uint32_t* __restrict__ vout, const uint32_t* count_dev,
+                                                               uint32_t cap, int shift,
+                                                               const uint32_t* __restrict__ ghist,
+                                                               uint32_t* __restrict__ status,
+                                                               uint32_t* __restrict__ tile_counter,
+                                                               uint32_t* __restrict__ err, uint32_t spin_limit,
+                                                               uint32_t stall_tile) {
+  __shared__ uint32_t pass_off[256];
   __shared__ uint32_t run[256];
-  __shared__ uint32_t tot[256];
   __shared__ uint32_t toff[256];
   __shared__ uint32_t wh[kSortWarps][256];
-  // the tile in local sorted order, so that the global writes come out as
-  // contiguous runs per digit
   __shared__ K sk[kTile];
   __shared__ uint32_t sv[kTile];
-  __shared__ uint32_t scan_total;
+  __shared__ uint32_t scan_total, s_tile;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  run[threadIdx.x] = offsets[threadIdx.x * gridDim.x + blockIdx.x];
-  uint32_t n, t0, t1;
-  block_range(count_dev, cap, &n, &t0, &t1);
+  const uint32_t d_own = threadIdx.x;  // the digit this thread publishes and looks back for
+  const uint32_t n = min(*count_dev, cap);
+  const uint32_t tiles = (n + kTile - 1) / kTile;
+  // this pass's digit offsets: exclusive scan of its histogram
+  pass_off[d_own] = block_exclusive_scan<kSortThreads>(ghist[d_own], &scan_total);
   const uint32_t lt = lanemask_lt();
-  for (uint32_t tile = t0; tile < t1; ++tile) {
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&wh[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= tiles) break;
     const uint32_t base = tile * kTile + wid * (32 * kItems);
     K k[kItems];
     uint32_t v[kItems], dg[kItems], rk[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-      uint32_t idx = base + j * 32 + lane;
-      bool ok = idx < n;
+      const uint32_t idx = base + j * 32 + lane;
+      const bool ok = idx < n;
       k[j] = ok ? kin[idx] : (K)0;
       v[j] = ok ? vin[idx] : 0u;
       dg[j] = ok ? ((uint32_t)(k[j] >> shift) & 255u) : 256u;
     }
-    __syncthreads();
+    // stable local rank: per warp in (item, lane) order, warps in order
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const uint32_t d = dg[j];
-      // lanes holding the same digit: intersect the ballots of its nine bits
-      // (bit 8 marks an invalid item), cheaper than a match-any
       uint32_t peers = 0xffffffffu;
 #pragma unroll
       for (int b = 0; b < 9; ++b) {
@@ -204,18 +241,23 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
       __syncwarp();
     }
     __syncthreads();
+    uint32_t tot;
     {
       uint32_t acc = 0;
 #pragma unroll
       for (int w = 0; w < kSortWarps; ++w) {
-        uint32_t x = wh[w][threadIdx.x];
-        wh[w][threadIdx.x] = acc;
+        const uint32_t x = wh[w][d_own];
+        wh[w][d_own] = acc;
         acc += x;
       }
-      tot[threadIdx.x] = acc;
-      toff[threadIdx.x] = block_exclusive_scan<kSortThreads>(acc, &scan_total);
+      tot = acc;
+      toff[d_own] = block_exclusive_scan<kSortThreads>(acc, &scan_total);
     }
+    // publish this tile's count of digit d_own (tile 0: already the prefix)
+    uint32_t* st = status + (size_t)tile * 256 + d_own;
+    st_status(st, (tile == 0 ? kFlagInc : kFlagAgg) | tot);
     __syncthreads();
+    // local sort into shared memory while the look-back runs
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const uint32_t d = dg[j];
@@ -225,17 +267,39 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
         sv[lp] = v[j];
       }
     }
-    __syncthreads();
+    // decoupled look-back for digit d_own
+    uint32_t excl = 0;
+    bool gave_up = false;
+    if (tile > 0) {
+      uint32_t j = tile - 1, polls = 0;
+      for (;;) {
+        uint32_t w = ld_status(status + (size_t)j * 256 + d_own);
+        if (j == stall_tile) w = 0u;
+        if ((w & ~kCountMask) == 0u) {
+          if (++polls > spin_limit) {
+            gave_up = true;
+            break;
+          }
+          continue;
+        }
+        excl += w & kCountMask;
+        if ((w & ~kCountMask) == kFlagInc || j == 0) break;
+        --j;
+      }
+      st_status(st, kFlagInc | ((excl + tot) & kCountMask));
+    }
+    run[d_own] = pass_off[d_own] + excl;
+    if (__syncthreads_or(gave_up) && threadIdx.x == 0) atomicAdd(err, 1u);
     const uint32_t cnt = scan_total;  // valid items of this tile
     for (uint32_t i = threadIdx.x; i < cnt; i += kSortThreads) {
       const K kk = sk[i];
       const uint32_t d = (uint32_t)(kk >> shift) & 255u;
       const uint32_t pos = run[d] + (i - toff[d]);
-      kout[pos] = kk;
-      vout[pos] = sv[i];
+      if (pos < n) {
+        kout[pos] = kk;
+        vout[pos] = sv[i];
+      }
     }
-    __syncthreads();
-    run[threadIdx.x] += tot[threadIdx.x];
     __syncthreads();
   }
 }
@@ -243,23 +307,33 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const K* __restrict_
 template <class K>
 int radix_sort_impl(K* keys, uint32_t* vals, const uint32_t* count_dev, uint32_t cap, int bits, SortWork& w,
                     cudaStream_t s, K** keys_out, uint32_t** vals_out) {
-  NPS_TRY(w.hist.ensure(sizeof(uint32_t) * (256 * kSortGrid + 1)));
-  constexpr uint32_t kHist = 256 * kSortGrid;
-  NPS_TRY(w.partial.ensure(sizeof(uint32_t) * (div_up(kHist, kScanTile) + 1)));
+  if (cap >= (1u << 30)) {
+    set_error("radix sort: capacity %u beyond the look-back's 30-bit counts", cap);
+    return NPS_ERR_INVALID;
+  }
+  const int passes = (bits + 7) / 8;
+  const uint32_t max_tiles = (cap + kTile - 1) / kTile;
+  // hist: the per-pass histograms, the per-pass tile counters and the
+  // timeout counter of callers without their own; lookback: per pass and tile
+  NPS_TRY(w.hist.ensure(sizeof(uint32_t) * (4 * 256 + 4 + 1)));
+  NPS_TRY(w.lookback.ensure(sizeof(uint32_t) * 256 * (size_t)max_tiles * 4 + 256));
   NPS_TRY(w.keys_alt.ensure(sizeof(K) * (size_t)cap));
   NPS_TRY(w.vals_alt.ensure(sizeof(uint32_t) * (size_t)cap));
+  uint32_t* ghist = w.hist.as<uint32_t>();
+  uint32_t* counters = ghist + 4 * 256;
+  uint32_t* err = w.err ? w.err : counters + 4;
+  NPS_CUDA(cudaMemsetAsync(ghist, 0, sizeof(uint32_t) * (4 * 256 + 4), s));
+  NPS_CUDA(cudaMemsetAsync(w.lookback.p, 0, sizeof(uint32_t) * 256 * (size_t)max_tiles * passes, s));
+  k_hist_all<K><<<kSortGrid, kSortThreads, 0, s>>>(keys, count_dev, cap, passes, ghist);
+  NPS_CHECK_LAUNCH();
   K* ka = keys;
   uint32_t* va = vals;
   K* kb = w.keys_alt.as<K>();
   uint32_t* vb = w.vals_alt.as<uint32_t>();
-  uint32_t* hist = w.hist.as<uint32_t>();
-  for (int shift = 0; shift < bits; shift += 8) {
-    k_upsweep<K><<<kSortGrid, kSortThreads, 0, s>>>(ka, count_dev, cap, shift, hist);
-    // digit-major histogram -> scatter offsets (multi-block scan, in place)
-    k_scan_reduce<<<div_up(kHist, kScanTile), kScanThreads, 0, s>>>(hist, kHist, w.partial.as<uint32_t>());
-    k_scan_single<<<1, kScanThreads, 0, s>>>(w.partial.as<uint32_t>(), div_up(kHist, kScanTile), hist + kHist);
-    k_scan_down<<<div_up(kHist, kScanTile), kScanThreads, 0, s>>>(hist, kHist, w.partial.as<uint32_t>(), hist);
-    k_downsweep<K><<<kSortGrid, kSortThreads, 0, s>>>(ka, va, kb, vb, count_dev, cap, shift, hist);
+  for (int p = 0; p < passes; ++p) {
+    k_onesweep<K><<<kSortGrid, kSortThreads, 0, s>>>(ka, va, kb, vb, count_dev, cap, 8 * p, ghist + 256 * p,
+                                                     w.lookback.as<uint32_t>() + (size_t)256 * max_tiles * p,
+                                                     counters + p, err, w.spin_limit, w.stall_tile);
     NPS_CHECK_LAUNCH();
     K* tk = ka; ka = kb; kb = tk;
     uint32_t* tv = va; va = vb; vb = tv;
@@ -293,3 +367,53 @@ int radix_sort_u32(uint32_t* keys, uint32_t* vals, const uint32_t* count_dev, ui
 
 
 }  // namespace nps
+
+// ------------------------------------------------------------- C ABI
+extern "C" int nps_sort_pairs(nps_ctx* ctx, uint32_t* keys, uint32_t* vals, uint32_t n, int bits,
+                              uint32_t spin_limit, uint32_t stall_tile) {
+  using namespace nps;
+  NPS_TRY(bind_device(ctx));
+  if (!keys || !vals || bits < 1 || bits > 32 || n >= (1u << 30)) {
+    set_error("sort_pairs: null buffer, bits %d outside 1..32 or %u pairs beyond 2^30 - 1", bits, n);
+    return NPS_ERR_INVALID;
+  }
+  if ((((uintptr_t)keys | (uintptr_t)vals) & 3u) != 0) {
+    set_error("sort_pairs: keys and values must be 4-byte aligned");
+    return NPS_ERR_INVALID;
+  }
+  if (n == 0) return NPS_OK;
+  cudaStream_t s = ctx->stream;
+  SortWork w;
+  DevBuf count;
+  int rc = count.ensure(16);
+  uint32_t* ko = nullptr;
+  uint32_t* vo = nullptr;
+  w.spin_limit = spin_limit ? spin_limit : (1u << 20);
+  w.stall_tile = stall_tile;
+  if (rc == NPS_OK) {
+    const uint32_t cnt[4] = {n, 0u, 0u, 0u};
+    rc = cudaMemcpyAsync(count.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s) == cudaSuccess ? NPS_OK : NPS_ERR_CUDA;
+    w.err = count.as<uint32_t>() + 1;  // zero: the look-back's timeouts
+  }
+  if (rc == NPS_OK) rc = radix_sort_u32(keys, vals, count.as<uint32_t>(), n, bits, w, s, &ko, &vo);
+  if (rc == NPS_OK && ko != keys) {
+    if (cudaMemcpyAsync(keys, ko, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(vals, vo, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      rc = NPS_ERR_CUDA;
+  }
+  uint32_t timeouts = 0;
+  if (rc == NPS_OK &&
+      (cudaMemcpyAsync(&timeouts, count.as<uint32_t>() + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(s) != cudaSuccess))
+    rc = NPS_ERR_CUDA;
+  if (rc == NPS_ERR_CUDA) set_error("sort_pairs: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaStreamSynchronize(s);
+  for (DevBuf* b : {&w.hist, &w.partial, &w.lookback, &w.keys_alt, &w.vals_alt, &count}) b->release();
+  if (rc == NPS_OK && timeouts) {
+    set_error("sort_pairs: %u look-back waits gave up (the output is not sorted)", timeouts);
+    return NPS_ERR_TIMEOUT;
+  }
+  return rc;
+}
+

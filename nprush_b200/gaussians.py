@@ -149,6 +149,12 @@ class GaussianTrainer:
         call("nps_gs_set_loss", self._h, self.LOSS_KINDS[kind], float(ssim_weight))
 
     def backward(self, dl_dimage=None):
+        """dl_dimage: None (the fused loss's gradient), a torch CUDA tensor or
+        a numpy array [V,H,W,4] (copied from host memory)."""
+        if isinstance(dl_dimage, np.ndarray):
+            a = np.ascontiguousarray(dl_dimage, np.float32)
+            call("nps_gs_backward_host", self._h, a.ctypes.data)
+            return
         p = None
         if dl_dimage is not None:
             import torch
@@ -183,22 +189,53 @@ class GaussianTrainer:
         v, mem2, k2 = _ptr(adam_v)
         call("nps_gs_write_state", self._h, m, v, int(step), mem if adam_m is not None else mem2)
 
-    VARIANTS = ((1, 256), (2, 128), (2, 256), (4, 64), (4, 128))
+    VARIANTS = ((1, 256), (2, 128), (2, 256), (4, 64), (4, 128))  # form 0 (16 x 16 tiles): one CTA per (tile, view)
+    # form 1: persistent, warp-specialised, per tile edge
+    PERSISTENT_VARIANTS = {8: ((1, 64), (1, 128), (2, 64), (2, 128)),
+                           16: ((1, 128), (2, 64), (2, 128), (4, 64), (4, 128)),
+                           32: ((4, 64), (4, 128))}
+    TUNE_VARIANTS = tuple((0,) + v for v in VARIANTS) + ((1, 1, 64), (1, 1, 128), (1, 2, 64), (1, 2, 128),
+                                                         (1, 4, 64), (1, 4, 128))
 
     def set_variant(self, fwd_ppt: int, bwd_ppt: int, fwd_stage: int = 0, bwd_stage: int = 0):
-        """Raster kernels with 1, 2 or 4 pixels per thread and the given records
-        staged per batch (0: 256 / pixels per thread)."""
+        """Form-0 raster kernels with 1, 2 or 4 pixels per thread and the given
+        records staged per batch (0: 256 / pixels per thread)."""
         call("nps_gs_set_variant", self._h, int(fwd_ppt), int(fwd_stage), int(bwd_ppt), int(bwd_stage))
 
+    def set_raster(self, fwd=(0, 1, 256), bwd=(0, 2, 128)):
+        """(form, pixels per thread, records per stage) of the forward and the
+        backward raster; form 1 is the persistent warp-specialised kernel."""
+        call("nps_gs_set_raster", self._h, *[int(x) for x in fwd], *[int(x) for x in bwd])
+
+    def set_tile(self, tile: int):
+        """Tile edge of the binning and raster (8, 16 or 32)."""
+        call("nps_gs_set_tile", self._h, int(tile))
+
+    def raster(self) -> dict:
+        c = np.zeros(7, np.int32)
+        call("nps_gs_get_raster", self._h, c.ctypes.data)
+        return dict(tile=int(c[0]), fwd=tuple(int(x) for x in c[1:4]), bwd=tuple(int(x) for x in c[4:7]))
+
     def autotune(self, cache_path=None) -> dict:
-        """Times the raster variants on the current views / targets, keeps the
-        fastest (looked up in / appended to cache_path when given)."""
-        c = np.zeros(4, np.int32)
-        t = np.zeros(10, np.float32)
-        call("nps_gs_autotune", self._h, None if cache_path is None else str(cache_path).encode(), c.ctypes.data,
-             t.ctypes.data)
-        return dict(fwd_ppt=int(c[0]), fwd_stage=int(c[1]), bwd_ppt=int(c[2]), bwd_stage=int(c[3]),
-                    fwd_ms=t[:5].tolist(), bwd_ms=t[5:].tolist(), cached=bool(t[0] < 0))
+        """Times binning at every tile size and the raster variants of both
+        forms of each tile on the current views / targets; keeps the fastest
+        (looked up in / appended to cache_path when given)."""
+        c = np.zeros(7, np.int32)
+        t = np.zeros(69, np.float32)
+        call("nps_gs_autotune_raster", self._h, None if cache_path is None else str(cache_path).encode(),
+             c.ctypes.data, t.ctypes.data)
+        per_tile = {}
+        for k, tile in enumerate((8, 16, 32)):
+            row = t[23 * k:23 * (k + 1)]
+            per_tile[tile] = dict(binning_ms=float(row[0]), fwd_ms=row[1:12].tolist(), bwd_ms=row[12:23].tolist())
+        return dict(tile=int(c[0]), fwd_form=int(c[1]), fwd_ppt=int(c[2]), fwd_stage=int(c[3]),
+                    bwd_form=int(c[4]), bwd_ppt=int(c[5]), bwd_stage=int(c[6]), per_tile=per_tile,
+                    cached=bool(t[0] < 0))
+
+    def set_sort_guard(self, spin_limit: int = 0, stall_tile: int = 0xFFFFFFFF):
+        """Look-back bound of the onesweep sorts (0: the default); stall_tile
+        (tests) is a tile whose status is treated as never published."""
+        call("nps_gs_set_sort_guard", self._h, int(spin_limit), int(stall_tile))
 
     def set_deterministic(self, enable: bool):
         """Two-pass backward reduction without float atomics (bit-reproducible)."""

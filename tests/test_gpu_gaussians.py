@@ -301,11 +301,14 @@ def test_deterministic_mode_is_bit_reproducible(trainer_cls, tmp_path):
 
 
 def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
-    """Forward images agree across the 1 / 2 / 4 pixels-per-thread raster
-    variants to 1e-6 (the compiler may fuse multiply-adds differently in each
-    instantiation); backward gradients to 1e-5 relative L2; both match the
-    oracle; the autotuner picks a valid variant and
-    reuses its cached choice."""
+    """Forward images agree across tile sizes (8, 16, 32) and the raster
+    variants of both forms (one CTA per tile; persistent warp-specialised)
+    and 1 / 2 / 4 pixels per thread to 1e-6 (the compiler may fuse
+    multiply-adds differently in each instantiation; each pixel composites
+    the same Gaussians in the same depth order whatever the tile); backward
+    gradients to 1e-5 relative L2, also with the forward and backward in
+    different forms; both match the oracle; the autotuner times every
+    variant of every tile, picks a valid one and reuses its cached choice."""
     n, w, h, deg = 5000, 112, 96, 2
     p = gs_scene(n, 61, deg=deg, log_scale_mean=-3.4)
     eyes = ((0.0, 0.0, 4.0), (2.5, 1.0, 3.0))
@@ -314,29 +317,55 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
     t = trainer_cls(n, sh_degree=deg, params=p)
     t.set_targets(tg)
     t.set_views(vp, vpi)
-    imgs, grads = {}, {}
-    for ppt, stage in t.VARIANTS:
-        t.set_variant(ppt, ppt, stage, stage)
+    imgs, grads, ncs = {}, {}, {}
+    variants = [(16, 0) + va for va in t.VARIANTS]
+    variants += [(tile, 1) + va for tile, vs in t.PERSISTENT_VARIANTS.items() for va in vs]
+    for va in variants:
+        t.set_tile(va[0])
+        t.set_raster(va[1:], va[1:])
         t.forward()
         t.loss()
         t.backward()
-        imgs[ppt, stage] = t.read_image(with_grad=False)[0]
-        grads[ppt, stage] = t.read_state()["grads"].astype(np.float64)
-    base = (1, 256)
-    for va in t.VARIANTS[1:]:
+        imgs[va] = t.read_image(with_grad=False)[0]
+        grads[va] = t.read_state()["grads"].astype(np.float64)
+        if va[0] == 16:
+            # the persistent backward after a grid forward (and the reverse): the
+            # per-tile last contributors both forms write drive either backward
+            other = (1,) + t.PERSISTENT_VARIANTS[16][1] if va[1] == 0 else (0,) + t.VARIANTS[1]
+            t.set_raster(other, va[1:])
+            t.forward()
+            t.loss()
+            t.backward()
+            ncs[va] = t.read_state()["grads"].astype(np.float64)
+    base = (16, 0, 1, 256)
+    for va in variants[1:]:
         np.testing.assert_allclose(imgs[va], imgs[base], atol=1e-6, rtol=0)
-        assert np.linalg.norm(grads[va] - grads[base]) / np.linalg.norm(grads[base]) < 1e-5
+        assert np.linalg.norm(grads[va] - grads[base]) / np.linalg.norm(grads[base]) < 1e-5, va
+    for va, g in ncs.items():
+        assert np.linalg.norm(g - grads[base]) / np.linalg.norm(grads[base]) < 1e-5, va
     rimg, rnc = orc.gs_forward(p, deg, views, w, h)
-    np.testing.assert_allclose(imgs[4, 128], rimg, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(imgs[16, 0, 4, 128], rimg, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(imgs[16, 1, 2, 128], rimg, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(imgs[32, 1, 4, 128], rimg, atol=1e-5, rtol=0)
+    np.testing.assert_allclose(imgs[8, 1, 1, 64], rimg, atol=1e-5, rtol=0)
+    t.set_tile(16)
     from nprush_b200._lib import NpsError
     with pytest.raises(NpsError):
         t.set_variant(1, 1, 512, 512)
     cache = tmp_path / "autotune.txt"
     r = t.autotune(cache)
-    assert (r["fwd_ppt"], r["fwd_stage"]) in t.VARIANTS and (r["bwd_ppt"], r["bwd_stage"]) in t.VARIANTS
-    assert not r["cached"] and all(x > 0 for x in r["fwd_ms"] + r["bwd_ms"])
+    for pas in ("fwd", "bwd"):
+        table = t.VARIANTS if r[f"{pas}_form"] == 0 else t.PERSISTENT_VARIANTS[r["tile"]]
+        assert (r[f"{pas}_ppt"], r[f"{pas}_stage"]) in table
+        assert r[f"{pas}_form"] == 1 or r["tile"] == 16
+    assert not r["cached"]
+    for tile, row in r["per_tile"].items():
+        assert row["binning_ms"] > 0
+        served = [(v[0] == 0 and tile == 16) or (v[0] == 1 and v[1:] in t.PERSISTENT_VARIANTS[tile])
+                  for v in t.TUNE_VARIANTS]
+        assert [x > 0 for x in row["fwd_ms"]] == served and [x > 0 for x in row["bwd_ms"]] == served, (tile, row)
     r2 = t.autotune(cache)
-    keys = ("fwd_ppt", "fwd_stage", "bwd_ppt", "bwd_stage")
+    keys = ("tile", "fwd_form", "fwd_ppt", "fwd_stage", "bwd_form", "bwd_ppt", "bwd_stage")
     assert r2["cached"] and [r2[k] for k in keys] == [r[k] for k in keys]
     # the tuned trainer still trains
     t.set_graph(True)
@@ -418,3 +447,33 @@ def test_sharded_trainer_single_rank_nccl(trainer_cls):
         assert c["after"] > 0
     finally:
         dist.destroy_process_group()
+
+
+def test_sort_lookback_timeout_is_reported(trainer_cls):
+    """The onesweep sorts' bounded look-back, made to run out on a normal
+    input (tile 2 of each sort treated as never published, 1000 polls): the
+    train step raises NPS_ERR_TIMEOUT, the parameters are not updated, and once
+    the guard is back to normal the trainer continues exactly as a fresh one
+    (deterministic mode)."""
+    from nprush_b200._lib import NpsError
+    n, w, h = 20000, 256, 256
+    p = gs_scene(n, 101, deg=0, log_scale_mean=-3.5)
+    vp, vpi, _ = gs_views(w, h)
+    tg = gs_targets(1, w, h, 102)
+    runs = []
+    for stall in (True, False):
+        t = trainer_cls(n, sh_degree=0, params=p)
+        t.set_deterministic(True)
+        t.set_targets(tg)
+        t.set_views(vp, vpi)
+        if stall:
+            t.set_sort_guard(1000, 2)
+            with pytest.raises(NpsError) as e:
+                t.train_step()
+            assert e.value.code == -5 and t.stats()["staging_timeouts"] > 0
+            np.testing.assert_array_equal(t.read_state()["params"], p)
+            t.set_sort_guard()
+        for _ in range(3):
+            t.train_step()
+        runs.append(t.read_state()["params"])
+    np.testing.assert_array_equal(runs[0], runs[1])

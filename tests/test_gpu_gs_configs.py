@@ -167,7 +167,8 @@ def test_single_view_l1_fit(trainer_cls):
 
 
 def test_external_image_gradient(trainer_cls):
-    """nps_gs_backward with an external dL/dimage: given the fused loss's own
+    """nps_gs_backward with an external dL/dimage (device memory, and host
+    memory through nps_gs_backward_host): given the fused loss's own
     dL/dimage it reproduces the fused backward bit for bit (deterministic
     mode); given any other image gradient it matches the oracle's backward of
     that gradient (1e-4 relative L2)."""
@@ -186,6 +187,8 @@ def test_external_image_gradient(trainer_cls):
     g_fused = t.read_state()["grads"]
     img, dimg = t.read_image()
     t.backward(torch.from_numpy(dimg).cuda())
+    np.testing.assert_array_equal(t.read_state()["grads"], g_fused)
+    t.backward(dimg)  # host memory (nps_gs_backward_host)
     np.testing.assert_array_equal(t.read_state()["grads"], g_fused)
     rng = np.random.default_rng(97)
     ext = rng.normal(0, 1e-5, dimg.shape).astype(np.float32)
