@@ -9,6 +9,10 @@ next `horizon` events:
 
   * keep  -> prune  when the plain rule prunes a member of the lineage later
     (the Gaussian was dead weight: prune it now);
+  * keep  -> clone / split (by the Gaussian's own largest scale, as the plain
+    rule chooses) when the plain rule densifies the lineage at the next event
+    and prunes none of it within the horizon (it was going to be densified:
+    do it one event earlier);
   * clone / split -> keep  when a member of the lineage is pruned later (the
     densification did not pay);
   * prune stays prune.
@@ -18,7 +22,7 @@ wasted densifications.  The plain rule stays the fallback (no network, or a
 Gaussian whose logits are not finite) and the judge: the A/B run compares
 final PSNR, Gaussian count and wall time against it.
 
-    python -m nprush_b200.learned_adc --log-seeds 100 101 --eval-seed 120 --steps 3000 --out ab.json
+    python -m nprush_b200.learned_adc --log-seeds 100 101 --eval-seeds 120 121 122 --steps 3000 --out ab.json
 """
 from __future__ import annotations
 
@@ -39,6 +43,8 @@ class AdcLog:
     plain: list = field(default_factory=list)      # per event [k]
     ids: list = field(default_factory=list)        # per event [k]
     pruned_ids: list = field(default_factory=list)  # per event: sorted ids the plain rule pruned
+    densified_ids: list = field(default_factory=list)  # per event: sorted ids the plain rule cloned or split
+    split_pref: list = field(default_factory=list)  # per event [k]: 2 if the Gaussian's largest scale calls for a split
 
     def record(self, trainer, step_frac: float, adc: AdcSchedule):
         feat, plain, ids = trainer.adc_features(step_frac, adc.grad_thresh, adc.split_scale, adc.prune_opacity)
@@ -52,22 +58,35 @@ class AdcLog:
         self.plain.append(plain_h[sel])
         self.ids.append(ids_h[sel])
         self.pruned_ids.append(np.unique(ids_h[plain_h == 3]))
+        self.densified_ids.append(np.unique(ids_h[(plain_h == 1) | (plain_h == 2)]))
+        # feature 7 is (largest log-scale - log split_scale) / ln 10: > 0 means split
+        self.split_pref.append(np.where(feat.cpu().numpy()[sel][:, 7] > 0, 2, 1).astype(np.uint8))
 
 
-def hindsight_labels(log: AdcLog, horizon: int = 3):
+def hindsight_labels(log: AdcLog, horizon: int = 3, densify_early: bool = True):
     """(features [N,16], labels [N]) relabelled by the lineages' fate."""
     X, Y = [], []
     ev = len(log.features)
     for e in range(ev):
         y = log.plain[e].astype(np.uint8).copy()
         later = [log.pruned_ids[j] for j in range(e + 1, min(ev, e + 1 + horizon))]
-        if later:
-            dead = np.isin(log.ids[e], np.unique(np.concatenate(later)))
-            y[(y == 0) & dead] = 3
-            y[((y == 1) | (y == 2)) & dead] = 0
+        dead = np.isin(log.ids[e], np.unique(np.concatenate(later))) if later else np.zeros(len(y), bool)
+        if densify_early and e + 1 < ev and log.densified_ids:
+            soon = np.isin(log.ids[e], log.densified_ids[e + 1]) & ~dead
+            keep = y == 0
+            y[keep & soon] = log.split_pref[e][keep & soon]
+        y[(y == 0) & dead] = 3
+        y[((y == 1) | (y == 2)) & dead] = 0
         X.append(log.features[e])
         Y.append(y)
     return np.concatenate(X), np.concatenate(Y)
+
+
+def per_class_recall(conf: np.ndarray) -> list:
+    """Recall of each class (keep, clone, split, prune) from a confusion
+    matrix [true, predicted]; None for a class with no samples."""
+    tot = conf.sum(axis=1)
+    return [None if tot[k] == 0 else float(conf[k, k] / tot[k]) for k in range(conf.shape[0])]
 
 
 def class_weights(y, cap: float = 20.0):
@@ -90,12 +109,12 @@ def policy_adc_fn(policy, adc: AdcSchedule, margin: float = 0.0):
     return fn
 
 
-def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: str = "batched"):
+def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: str = "batched", views: int = 8):
     """One training run on a fresh scene; returns (FitResult, mean PSNR)."""
     vp, vpi, tg, st = scene_fn(seed)
     st.assign_ids(0)
-    r = fit(st, vp, vpi, steps, seed=seed, adc=adc, mode=mode, adc_fn=adc_fn)
-    psnr = float(np.mean(evaluate_psnr(st, vp, vpi)))
+    r = fit(st, vp, vpi, steps, views=views, seed=seed, adc=adc, mode=mode, adc_fn=adc_fn)
+    psnr = float(np.mean(evaluate_psnr(st, vp, vpi, views=views)))
     st.close()
     return r, psnr
 
@@ -103,7 +122,8 @@ def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: st
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--log-seeds", type=int, nargs="+", default=[100, 101])
-    ap.add_argument("--eval-seed", type=int, default=120)
+    ap.add_argument("--eval-seeds", type=int, nargs="+", default=[120],
+                    help="held-out scenes: every arm trains each of them")
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--log-steps", type=int, default=None,
                     help="length of the logging runs (default: up to the last ADC event)")
@@ -118,6 +138,10 @@ def main(argv=None):
     ap.add_argument("--res", type=int, default=800)
     ap.add_argument("--horizon", type=int, default=3)
     ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--no-densify-early", action="store_true",
+                    help="leave out the keep -> densify relabelling (densified at the next event anyway)")
+    ap.add_argument("--views", type=int, default=8, help="views per step")
+    ap.add_argument("--cams", type=int, default=32, help="cameras on the sphere")
     ap.add_argument("--class-weights", action="store_true",
                     help="weight classes by inverse frequency (default: uniform; a false prune costs more "
                          "than a missed one)")
@@ -135,7 +159,7 @@ def main(argv=None):
 
     def scene(seed):
         # student and teacher seeds derived from the run seed
-        return teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=4 * a.gaussians,
+        return teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, n_cams=a.cams, capacity=4 * a.gaussians,
                              student_seed=seed, teacher_seed=seed + 1000)
 
     out = {}
@@ -145,7 +169,7 @@ def main(argv=None):
         for s in a.log_seeds:
             r, p = run(scene, log_steps, s, adc, logging_adc_fn(log, adc))
             out.setdefault("log_runs", []).append(dict(seed=s, psnr=p, count=r.count, wall_s=r.wall_s))
-        X, y = hindsight_labels(log, a.horizon)
+        X, y = hindsight_labels(log, a.horizon, densify_early=not a.no_densify_early)
         cw = class_weights(y) if a.class_weights else np.ones(4, np.float32)
         # hold out every 10th sample to score the network
         hold = np.arange(len(y)) % 10 == 0
@@ -157,20 +181,31 @@ def main(argv=None):
         np.add.at(conf, (y[hold], pred), 1)
         out["training"] = dict(samples=int(len(y)), class_counts=np.bincount(y, minlength=4).tolist(),
                                class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
-                               heldout_confusion=conf.tolist())
+                               heldout_confusion=conf.tolist(), heldout_recall=per_class_recall(conf))
         arms = [] if a.no_plain else [("plain", None, "batched")]
         for mg in a.margins:
             arms.append(("learned" if mg == 0.0 else f"learned_m{mg:g}", policy_adc_fn(pol, adc, mg), "batched"))
         if a.with_per_view:
             arms.append(("plain_per_view", None, "per_view"))
         for name, fn, mode in arms:
-            r, p = run(scene, a.steps, a.eval_seed, adc, fn, mode=mode)
-            out[name] = dict(mode=mode, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
-                             skipped=r.skipped_steps, adc_events=r.adc_events[-3:])
+            runs = []
+            for es in a.eval_seeds:
+                r, p = run(scene, a.steps, es, adc, fn, mode=mode, views=a.views)
+                runs.append(dict(seed=es, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
+                                 skipped=r.skipped_steps, adc_events=r.adc_events[-3:]))
+            out[name] = dict(mode=mode, runs=runs, psnr=float(np.mean([x["psnr"] for x in runs])),
+                             count=float(np.mean([x["count"] for x in runs])),
+                             wall_s=float(np.mean([x["wall_s"] for x in runs])))
+        if "plain" in out:
+            for name in [k for k in out if k.startswith("learned")]:
+                d_psnr = [x["psnr"] - y["psnr"] for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
+                d_cnt = [x["count"] / y["count"] - 1.0 for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
+                out[name]["vs_plain"] = dict(psnr_db=d_psnr, count_frac=d_cnt)
     out["config"] = vars(a)
     print(json.dumps({k: v for k, v in out.items() if k not in ("training", "log_runs", "config")}))
     print(json.dumps(dict(class_counts=out["training"]["class_counts"], acc=out["training"]["acc"][-1],
-                          confusion=out["training"]["heldout_confusion"])))
+                          confusion=out["training"]["heldout_confusion"],
+                          recall=out["training"]["heldout_recall"])))
     if a.out:
         with open(a.out, "w") as f:
             json.dump(out, f)
