@@ -2605,7 +2605,10 @@ static int gs_capture(nps_gs* o) {
     o->ev_pool.push_back(g.second.second);
   }
   o->gtimers.clear();
-  if (!o->h_status) NPS_CUDA(cudaMallocHost((void**)&o->h_status, 16));
+  if (!o->h_status) {
+    NPS_CUDA(cudaMallocHost((void**)&o->h_status, 16));
+    std::memset(o->h_status, 0, 16);  // page-locked memory may be reused: no stale status words
+  }
   if (!o->gdone) NPS_CUDA(cudaEventCreateWithFlags(&o->gdone, cudaEventDisableTiming));
   if (!o->gprev) NPS_CUDA(cudaEventCreateWithFlags(&o->gprev, cudaEventDisableTiming));
   NPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2709,6 +2712,7 @@ int nps_gs_train_step(nps_gs* o, float* loss3_host) {
       NPS_TRY(gs_capture(o));
       NPS_CUDA(cudaStreamSynchronize(s));
       o->skip_seen = o->h_status[1] = 0;
+      o->h_status[2] = o->timeouts_seen;  // what the replays report until a wait gives up
       NPS_CUDA(cudaMemsetAsync(o->stepst.as<uint32_t>() + 4, 0, sizeof(uint32_t), s));
       o->gkey = key;
     } else {
@@ -3040,7 +3044,7 @@ int nps_gs_load(nps_gs* o, const char* path) {
   o->fwd_valid = o->loss_valid = false;
   o->gkey = 0;
   o->skip_seen = 0;
-  if (o->h_status) o->h_status[1] = 0;
+  if (o->h_status) o->h_status[1] = o->h_status[2] = 0;
   return NPS_OK;
 }
 

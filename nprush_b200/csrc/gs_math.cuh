@@ -129,6 +129,20 @@ struct Proj {
   T ca, cb, cc;      // conic (inverse 2D covariance)
 };
 
+// a0 m0 + a1 m1 + a2 m2 + c with every product and sum rounded on its own
+// (no fused multiply-add), left to right: the view depth that orders the
+// tile lists is then the plain float evaluation bit for bit, so two Gaussians
+// whose depths differ in the last place keep the order a plain evaluation
+// gives them.
+template <class T>
+GSM_HD T dot3_plus_rounded(const T* a, const T* m, T c) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(T) == sizeof(float))
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a[0], m[0]), __fmul_rn(a[1], m[1])), __fmul_rn(a[2], m[2])), c);
+#endif
+  return a[0] * m[0] + a[1] * m[1] + a[2] * m[2] + c;
+}
+
 template <class T>
 GSM_HD void project(const float* vp, const T* mean, const T* log_scale, const T* quat, T W, T H, T lowpass, Proj<T>& P) {
   const T r0[3] = {(T)vp[0], (T)vp[4], (T)vp[8]};
@@ -136,7 +150,7 @@ GSM_HD void project(const float* vp, const T* mean, const T* log_scale, const T*
   const T r3[3] = {(T)vp[3], (T)vp[7], (T)vp[11]};
   P.cx = r0[0] * mean[0] + r0[1] * mean[1] + r0[2] * mean[2] + (T)vp[12];
   P.cy = r1[0] * mean[0] + r1[1] * mean[1] + r1[2] * mean[2] + (T)vp[13];
-  P.cw = r3[0] * mean[0] + r3[1] * mean[1] + r3[2] * mean[2] + (T)vp[15];
+  P.cw = dot3_plus_rounded<T>(r3, mean, (T)vp[15]);
   const T iw = (T)1 / P.cw;
   const T a = W * (T)0.5, b = H * (T)0.5;
   P.u = (P.cx * iw + 1) * a - (T)0.5;
