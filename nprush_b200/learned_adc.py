@@ -102,6 +102,12 @@ def logging_adc_fn(log: AdcLog, adc: AdcSchedule):
     return fn
 
 
+def plain_adc_fn(adc: AdcSchedule):
+    def fn(trainer, step):
+        return trainer.adc(adc.grad_thresh, adc.split_scale, adc.prune_opacity)
+    return fn
+
+
 def policy_adc_fn(policy, adc: AdcSchedule, margin: float = 0.0):
     def fn(trainer, step):
         trainer.set_policy_margin(margin)
@@ -133,6 +139,13 @@ def main(argv=None):
     ap.add_argument("--with-per-view", action="store_true",
                     help="also run the plain per-view trainer (eager, one view per launch) on the eval seed")
     ap.add_argument("--adc-stop", type=int, default=None)
+    ap.add_argument("--adc-start", type=int, default=500)
+    ap.add_argument("--adc-every", type=int, default=100)
+    ap.add_argument("--sh-degree", type=int, default=3)
+    ap.add_argument("--deterministic", action="store_true", help="bit-reproducible training runs")
+    ap.add_argument("--plain-thresholds", type=float, nargs="*", default=[],
+                    help="extra plain arms with these densification thresholds (the count / PSNR trade-off "
+                         "the plain rule itself offers)")
     ap.add_argument("--gaussians", type=int, default=200_000)
     ap.add_argument("--teacher", type=int, default=250_000)
     ap.add_argument("--res", type=int, default=800)
@@ -155,12 +168,16 @@ def main(argv=None):
     stream = torch.cuda.Stream(0)
     ctx = _lib.context(0)
     _lib.call("nps_set_stream", ctx, stream.cuda_stream)
-    adc = AdcSchedule(stop=a.adc_stop or min(15000, a.steps))
+    adc = AdcSchedule(every=a.adc_every, start=a.adc_start, stop=a.adc_stop or min(15000, a.steps))
 
     def scene(seed):
         # student and teacher seeds derived from the run seed
-        return teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, n_cams=a.cams, capacity=4 * a.gaussians,
-                             student_seed=seed, teacher_seed=seed + 1000)
+        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, n_cams=a.cams,
+                                        sh_degree=a.sh_degree, capacity=4 * a.gaussians, student_seed=seed,
+                                        teacher_seed=seed + 1000)
+        if a.deterministic:
+            st.set_deterministic(True)
+        return vp, vpi, tg, st
 
     out = {}
     with torch.cuda.stream(stream):
@@ -183,6 +200,9 @@ def main(argv=None):
                                class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
                                heldout_confusion=conf.tolist(), heldout_recall=per_class_recall(conf))
         arms = [] if a.no_plain else [("plain", None, "batched")]
+        for thr in a.plain_thresholds:
+            arms.append((f"plain_t{thr:g}", plain_adc_fn(AdcSchedule(every=adc.every, start=adc.start,
+                                                                     stop=adc.stop, grad_thresh=thr)), "batched"))
         for mg in a.margins:
             arms.append(("learned" if mg == 0.0 else f"learned_m{mg:g}", policy_adc_fn(pol, adc, mg), "batched"))
         if a.with_per_view:
@@ -197,7 +217,7 @@ def main(argv=None):
                              count=float(np.mean([x["count"] for x in runs])),
                              wall_s=float(np.mean([x["wall_s"] for x in runs])))
         if "plain" in out:
-            for name in [k for k in out if k.startswith("learned")]:
+            for name in [k for k in out if k.startswith("learned") or k.startswith("plain_t")]:
                 d_psnr = [x["psnr"] - y["psnr"] for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
                 d_cnt = [x["count"] / y["count"] - 1.0 for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
                 out[name]["vs_plain"] = dict(psnr_db=d_psnr, count_frac=d_cnt)
