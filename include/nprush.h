@@ -304,7 +304,8 @@ int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
 /* Tiles and raster variants (no reference counterpart; the reference's
  * tile is its 16 x 16 workgroup, splat_backward.wgsl:136).  The binning
  * cuts the image into T x T tiles, T = 8, 16 (default) or 32
- * (nps_gs_set_tile); the deterministic backward and form 0 below need 16.
+ * (nps_gs_set_tile); the deterministic backward and forms 0 and 2 below
+ * need 16.
  * Two forms of the forward and backward raster kernels, each for several
  * (pixels per thread, records staged per batch); T * T / ppt threads cover a
  * tile:
@@ -316,7 +317,12 @@ int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
  *     (bulk copies completing on mbarriers) while the consumer warps
  *     composite or differentiate, with no CTA-wide barrier in the loop:
  *     T = 8: (1 or 2, 64 or 128); T = 16: (1, 128), (2 or 4, 64 or 128);
- *     T = 32: (4, 64 or 128).
+ *     T = 32: (4, 64 or 128);
+ *   form 2, one CTA per (tile, view) with the blocks taking the items
+ *     longest first; its backward has no CTA-wide barrier in the loop (each
+ *     warp waits for its own data; the last warp to finish a batch adds the
+ *     batch's sums to the records and stages the batch after next), T = 16,
+ *     the (ppt, stage) of form 0.
  * nps_gs_set_raster selects one per pass for the current tile (a stage of 0
  * means the form's default: 256 / ppt for form 0, 128 for form 1);
  * nps_gs_set_variant selects form 0; nps_gs_set_tile changes the tile (and
@@ -329,19 +335,20 @@ int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
  * cache_path it first looks the workload up in that text file (device,
  * image size, views, SH degree, Gaussian count to ~19%, deterministic mode)
  * and appends its choice.  choice7 (may be null) as nps_gs_get_raster;
- * times_ms69 (may be null): for T = 8, 16, 32 in turn, 23 floats: binning,
- * then the forward and then the backward time of the 11 variants (0, 1,
+ * times_ms99 (may be null): for T = 8, 16, 32 in turn, 33 floats: binning,
+ * then the forward and then the backward time of the 16 variants (0, 1,
  * 256), (0, 2, 128), (0, 2, 256), (0, 4, 64), (0, 4, 128), (1, 1, 64),
- * (1, 1, 128), (1, 2, 64), (1, 2, 128), (1, 4, 64), (1, 4, 128) (0 where a
- * variant does not serve the tile; -1 throughout when the choice came from
- * the cache).  nps_gs_autotune is the same tuner reporting only ppt and stage
+ * (1, 1, 128), (1, 2, 64), (1, 2, 128), (1, 4, 64), (1, 4, 128), (2, 1,
+ * 256), (2, 2, 128), (2, 2, 256), (2, 4, 64), (2, 4, 128) (0 where a variant
+ * does not serve the tile; -1 throughout when the choice came from the
+ * cache).  nps_gs_autotune is the same tuner reporting only ppt and stage
  * (choice4) and the 16 x 16 form-0 times (times_ms10). */
 int nps_gs_set_tile(nps_gs* gs, uint32_t tile);
 int nps_gs_set_raster(nps_gs* gs, int fwd_form, int fwd_ppt, int fwd_stage, int bwd_form, int bwd_ppt,
                       int bwd_stage);
 int nps_gs_set_variant(nps_gs* gs, int fwd_ppt, int fwd_stage, int bwd_ppt, int bwd_stage);
 int nps_gs_get_raster(nps_gs* gs, int* choice7);
-int nps_gs_autotune_raster(nps_gs* gs, const char* cache_path, int* choice7, float* times_ms69);
+int nps_gs_autotune_raster(nps_gs* gs, const char* cache_path, int* choice7, float* times_ms99);
 int nps_gs_autotune(nps_gs* gs, const char* cache_path, int* choice4, float* times_ms10);
 /* Bounded waits of the radix sorts (depth keys, tile keys).  The sorts are
  * onesweep radix sorts: each tile of keys finds its output offsets by a

@@ -331,18 +331,29 @@ __device__ __forceinline__ void stage_batch(const Rec* __restrict__ recs, const 
 // Forward raster, PPT vertically adjacent pixels per thread: 256 / PPT
 // threads per 16 x 16 tile, a warp covers a 16 x 2·PPT strip, records staged
 // SB = SPS · 256 / PPT at a time.  (PPT, SB) is the autotuned variant.
-template <int PPT, int SPS>
+// kOrd: a 1D grid whose block b takes work item order[b] (longest tile
+// lists first), else the grid is (tiles x, tiles y, views).
+template <int PPT, int SPS, bool kOrd>
 __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                    const uint32_t* __restrict__ rstart,
                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
                                                    float4* __restrict__ img, uint32_t* __restrict__ ncontrib,
-                                                   uint32_t* __restrict__ tile_last, uint32_t* __restrict__ err) {
+                                                   uint32_t* __restrict__ tile_last, uint32_t* __restrict__ err,
+                                                   const uint32_t* __restrict__ order) {
   constexpr int NT = 256 / PPT, SB = NT * SPS;
   static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
   __shared__ __align__(16) Rec s_rec[2][SB];
   __shared__ __align__(8) uint64_t s_bar[2];
-  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x;
+  uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z;
+  if constexpr (kOrd) {
+    const uint32_t it = order[blockIdx.x];
+    v = it / num_tiles;
+    const uint32_t tile = it - v * num_tiles;
+    ty = tile / tiles_x;
+    tx = tile - ty * tiles_x;
+  }
+  const uint32_t tid = threadIdx.x;
   const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
   const float fx = (float)px;
   const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * (tid >> 5));
@@ -2114,12 +2125,14 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 // a tile edge T.  Form 0: one CTA per (tile, view), records double-buffered
 // (k_fwd, k_bwd2), T = 16 only; form 1: persistent warp-specialised kernels
 // over a longest-first work queue (k_fwd_ws, k_bwd_ws), a 3-slot ring of
-// staged records, T = 8 (1 or 2 pixels per thread), 16 (1, 2, 4) or 32 (4).
+// staged records, T = 8 (1 or 2 pixels per thread), 16 (1, 2, 4) or 32 (4);
+// form 2: one CTA per work item, blocks taking the items longest first
+// (k_fwd ordered, k_bwd3: no CTA-wide barrier in the backward's loop), T = 16.
 struct RasterVariant {
   int form, ppt, stage;
 };
 static bool valid_variant(uint32_t tile, int form, int ppt, int stage) {
-  if (form == 0) {
+  if (form == 0 || form == 2) {
     if (tile != 16 || (ppt != 1 && ppt != 2 && ppt != 4)) return false;
     return stage == 256 / ppt || (stage == 512 / ppt && stage <= 256);
   }
@@ -2130,8 +2143,9 @@ static bool valid_variant(uint32_t tile, int form, int ppt, int stage) {
   return false;
 }
 constexpr RasterVariant kVariants[] = {{0, 1, 256}, {0, 2, 128}, {0, 2, 256}, {0, 4, 64}, {0, 4, 128}, {1, 1, 64},
-                                       {1, 1, 128}, {1, 2, 64},  {1, 2, 128}, {1, 4, 64}, {1, 4, 128}};
-constexpr int kNumVariants = 11;
+                                       {1, 1, 128}, {1, 2, 64},  {1, 2, 128}, {1, 4, 64}, {1, 4, 128}, {2, 1, 256},
+                                       {2, 2, 128}, {2, 2, 256}, {2, 4, 64},  {2, 4, 128}};
+constexpr int kNumVariants = 16;
 constexpr uint32_t kTiles[] = {8, 16, 32};
 constexpr int kNumTiles = 3;
 // per tile in the autotuner's times: binning, then the forward and backward time of each variant
@@ -2206,11 +2220,24 @@ static int launch_fwd_raster(nps_gs* o, int form, int ppt, int stage) {
     set_error("gs raster: the one-CTA-per-tile kernels need 16 x 16 tiles (tile is %u)", o->tile);
     return NPS_ERR_STATE;
   }
-  const dim3 grid(tiles_x, tiles_y, nv);
-#define NPS_FWD(PPT, SPS)                                                                                   \
-  gs::k_fwd<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,     \
-                                                 tiles_x, num_tiles, bg, o->img.as<float4>(),                   \
-                                                 o->ncontrib.as<uint32_t>(), o->tile_last.as<uint32_t>(), err)
+  const bool ord = form == 2;
+  if (ord) {
+    gs::k_order_items<false><<<1, 1024, 0, s>>>(rstart, rend, nullptr, nitems, o->ws_order_f.as<uint32_t>(),
+                                                o->ws_q.as<uint32_t>());
+    NPS_CHECK_LAUNCH();
+  }
+  const dim3 grid = ord ? dim3(nitems, 1, 1) : dim3(tiles_x, tiles_y, nv);
+#define NPS_FWD(PPT, SPS)                                                                                     \
+  do {                                                                                                        \
+    if (ord)                                                                                                  \
+      gs::k_fwd<PPT, SPS, true><<<grid, 256 / PPT, 0, s>>>(                                                   \
+          o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(), \
+          o->ncontrib.as<uint32_t>(), o->tile_last.as<uint32_t>(), err, o->ws_order_f.as<uint32_t>());        \
+    else                                                                                                      \
+      gs::k_fwd<PPT, SPS, false><<<grid, 256 / PPT, 0, s>>>(                                                  \
+          o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, tiles_x, num_tiles, bg, o->img.as<float4>(), \
+          o->ncontrib.as<uint32_t>(), o->tile_last.as<uint32_t>(), err, nullptr);                             \
+  } while (0)
   const int sps = stage * ppt / 256;
   if (ppt == 2 && sps == 2) NPS_FWD(2, 2);
   else if (ppt == 2) NPS_FWD(2, 1);
@@ -2268,6 +2295,26 @@ static int launch_bwd_raster(nps_gs* o, int form, int ppt, int stage, const floa
   if (o->tile != 16) {
     set_error("gs raster: the one-CTA-per-tile kernels need 16 x 16 tiles (tile is %u)", o->tile);
     return NPS_ERR_STATE;
+  }
+  if (form == 2) {
+    NPS_TRY(ensure_ws_buffers(o, nitems));
+    uint32_t* q = o->ws_q.as<uint32_t>() + 2;
+    gs::k_order_items<true><<<1, 1024, 0, s>>>(nullptr, nullptr, o->tile_last.as<uint32_t>(), nitems,
+                                               o->ws_order_b.as<uint32_t>(), q);
+    NPS_CHECK_LAUNCH();
+#define NPS_BWD3(PPT, SB)                                                                                     \
+  gs::k_bwd3<PPT, SB><<<nitems, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart,                \
+                                                  o->tile_last.as<uint32_t>(), o->ws_order_b.as<uint32_t>(), q,   \
+                                                  W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),              \
+                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err)
+    if (ppt == 1) NPS_BWD3(1, 256);
+    else if (ppt == 2 && stage == 256) NPS_BWD3(2, 256);
+    else if (ppt == 2) NPS_BWD3(2, 128);
+    else if (stage == 128) NPS_BWD3(4, 128);
+    else NPS_BWD3(4, 64);
+#undef NPS_BWD3
+    NPS_CHECK_LAUNCH();
+    return NPS_OK;
   }
   const dim3 grid(tiles_x, tiles_y, nv);
 #define NPS_BWD(PPT, SPS)                                                                                     \
@@ -3143,7 +3190,7 @@ static int binning_ms(nps_gs* o, float* ms) {
 // forward + fastest backward is smallest, with those variants.  The choice
 // is cached in a text file (one line per workload: key, tile and the six
 // variant numbers) when cache_path is given.
-int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, float* times_ms69) {
+int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, float* times_ms99) {
   NPS_TRY(check_gs(o));
   if (!o->tgt || o->nv == 0) {
     set_error("gs_autotune: set views and targets first");
@@ -3160,8 +3207,8 @@ int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, floa
     if (*c == ' ') *c = '_';
   auto report = [&](bool timed) -> int {
     if (choice7) NPS_TRY(nps_gs_get_raster(o, choice7));
-    if (times_ms69 && !timed)
-      for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms69[i] = -1.0f;  // from the cache: not timed
+    if (times_ms99 && !timed)
+      for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms99[i] = -1.0f;  // from the cache: not timed
     return NPS_OK;
   };
   if (cache_path) {
@@ -3187,8 +3234,8 @@ int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, floa
       }
     }
   }
-  if (times_ms69)
-    for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms69[i] = 0.0f;  // 0: not a variant of that tile
+  if (times_ms99)
+    for (int i = 0; i < kNumTiles * kTuneStride; ++i) times_ms99[i] = 0.0f;  // 0: not a variant of that tile
   cudaStream_t s = o->ctx->stream;
   const uint32_t M = o->n * o->nv;
   NPS_TRY(o->g2.ensure(sizeof(float) * gs::kG2 * ((size_t)M + 1)));
@@ -3210,7 +3257,7 @@ int nps_gs_autotune_raster(nps_gs* o, const char* cache_path, int* choice7, floa
     float bin = 0.0f;
     if ((rc = binning_ms(o, &bin)) != NPS_OK || (rc = binning_ms(o, &bin)) != NPS_OK) break;  // warm-up, timed
     if ((rc = nps_gs_loss(o, nullptr)) != NPS_OK) break;
-    float* tt = times_ms69 ? times_ms69 + ti * kTuneStride : nullptr;
+    float* tt = times_ms99 ? times_ms99 + ti * kTuneStride : nullptr;
     if (tt) tt[0] = bin;
     float best[2] = {1e30f, 1e30f};
     RasterVariant pick[2] = {{1, o->fwd_ppt, 128}, {1, o->fwd_ppt, 128}};

@@ -194,8 +194,8 @@ class GaussianTrainer:
     PERSISTENT_VARIANTS = {8: ((1, 64), (1, 128), (2, 64), (2, 128)),
                            16: ((1, 128), (2, 64), (2, 128), (4, 64), (4, 128)),
                            32: ((4, 64), (4, 128))}
-    TUNE_VARIANTS = tuple((0,) + v for v in VARIANTS) + ((1, 1, 64), (1, 1, 128), (1, 2, 64), (1, 2, 128),
-                                                         (1, 4, 64), (1, 4, 128))
+    TUNE_VARIANTS = (tuple((0,) + v for v in VARIANTS) + ((1, 1, 64), (1, 1, 128), (1, 2, 64), (1, 2, 128),
+                                                          (1, 4, 64), (1, 4, 128)) + tuple((2,) + v for v in VARIANTS))
 
     def set_variant(self, fwd_ppt: int, bwd_ppt: int, fwd_stage: int = 0, bwd_stage: int = 0):
         """Form-0 raster kernels with 1, 2 or 4 pixels per thread and the given
@@ -204,7 +204,8 @@ class GaussianTrainer:
 
     def set_raster(self, fwd=(0, 1, 256), bwd=(0, 2, 128)):
         """(form, pixels per thread, records per stage) of the forward and the
-        backward raster; form 1 is the persistent warp-specialised kernel."""
+        backward raster; form 1 is the persistent warp-specialised kernel,
+        form 2 one CTA per tile taking the tiles longest first."""
         call("nps_gs_set_raster", self._h, *[int(x) for x in fwd], *[int(x) for x in bwd])
 
     def set_tile(self, tile: int):
@@ -220,14 +221,16 @@ class GaussianTrainer:
         """Times binning at every tile size and the raster variants of both
         forms of each tile on the current views / targets; keeps the fastest
         (looked up in / appended to cache_path when given)."""
+        nv = len(self.TUNE_VARIANTS)
         c = np.zeros(7, np.int32)
-        t = np.zeros(69, np.float32)
+        t = np.zeros(3 * (1 + 2 * nv), np.float32)
         call("nps_gs_autotune_raster", self._h, None if cache_path is None else str(cache_path).encode(),
              c.ctypes.data, t.ctypes.data)
         per_tile = {}
         for k, tile in enumerate((8, 16, 32)):
-            row = t[23 * k:23 * (k + 1)]
-            per_tile[tile] = dict(binning_ms=float(row[0]), fwd_ms=row[1:12].tolist(), bwd_ms=row[12:23].tolist())
+            row = t[(1 + 2 * nv) * k:(1 + 2 * nv) * (k + 1)]
+            per_tile[tile] = dict(binning_ms=float(row[0]), fwd_ms=row[1:1 + nv].tolist(),
+                                  bwd_ms=row[1 + nv:1 + 2 * nv].tolist())
         return dict(tile=int(c[0]), fwd_form=int(c[1]), fwd_ppt=int(c[2]), fwd_stage=int(c[3]),
                     bwd_form=int(c[4]), bwd_ppt=int(c[5]), bwd_stage=int(c[6]), per_tile=per_tile,
                     cached=bool(t[0] < 0))

@@ -318,7 +318,7 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
     t.set_targets(tg)
     t.set_views(vp, vpi)
     imgs, grads, ncs = {}, {}, {}
-    variants = [(16, 0) + va for va in t.VARIANTS]
+    variants = [(16, 0) + va for va in t.VARIANTS] + [(16, 2) + va for va in t.VARIANTS]
     variants += [(tile, 1) + va for tile, vs in t.PERSISTENT_VARIANTS.items() for va in vs]
     for va in variants:
         t.set_tile(va[0])
@@ -331,7 +331,7 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
         if va[0] == 16:
             # the persistent backward after a grid forward (and the reverse): the
             # per-tile last contributors both forms write drive either backward
-            other = (1,) + t.PERSISTENT_VARIANTS[16][1] if va[1] == 0 else (0,) + t.VARIANTS[1]
+            other = (0,) + t.VARIANTS[1] if va[1] != 0 else (1,) + t.PERSISTENT_VARIANTS[16][1]
             t.set_raster(other, va[1:])
             t.forward()
             t.loss()
@@ -355,13 +355,13 @@ def test_raster_variants_agree_and_autotune(trainer_cls, tmp_path):
     cache = tmp_path / "autotune.txt"
     r = t.autotune(cache)
     for pas in ("fwd", "bwd"):
-        table = t.VARIANTS if r[f"{pas}_form"] == 0 else t.PERSISTENT_VARIANTS[r["tile"]]
+        table = t.PERSISTENT_VARIANTS[r["tile"]] if r[f"{pas}_form"] == 1 else t.VARIANTS
         assert (r[f"{pas}_ppt"], r[f"{pas}_stage"]) in table
         assert r[f"{pas}_form"] == 1 or r["tile"] == 16
     assert not r["cached"]
     for tile, row in r["per_tile"].items():
         assert row["binning_ms"] > 0
-        served = [(v[0] == 0 and tile == 16) or (v[0] == 1 and v[1:] in t.PERSISTENT_VARIANTS[tile])
+        served = [(v[0] != 1 and tile == 16) or (v[0] == 1 and v[1:] in t.PERSISTENT_VARIANTS[tile])
                   for v in t.TUNE_VARIANTS]
         assert [x > 0 for x in row["fwd_ms"]] == served and [x > 0 for x in row["bwd_ms"]] == served, (tile, row)
     r2 = t.autotune(cache)
