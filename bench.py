@@ -12,8 +12,9 @@ the step's 8 target images uploaded from page-locked host memory every step
 (the next step's upload overlapping the current step) and the loss read back
 every step.  `--impl reference` times the reference's own shader code
 for this path (translated to C++, oracle/_ref) on the host, on a bounded
-sample of the same shape.  Multi-GPU runs are independent replicas (weak
-scaling, no collective).
+sample of the same shape.  With N > 1 GPUs each step's 8 views are split
+over the ranks (view-sharded data parallelism: one NCCL all-reduce of the
+gradients per step, Adam on every replica; strong scaling).
 """
 from __future__ import annotations
 
@@ -238,6 +239,96 @@ def run_ours(args, rank, world):
                 trained=trained,
                 graph_kernels=graph_kernels,
                 clocks=clk.summary(), e2e_ms=float(np.mean(e2e_times)), h2d=h2d, d2h=d2h, loss=loss_last)
+
+
+def run_sharded(args, rank, world):
+    """N > 1: the view-sharded trainer (nprush_b200.distributed): each rank
+    renders its share of a step's 8 views on a full replica of the 200k
+    Gaussians, one NCCL all-reduce of the gradient buffer per step, Adam on
+    every replica (strong scaling: the step's work is fixed, split over the
+    ranks).  Timed like the single-GPU line: CUDA events around each step,
+    L2 flushed between steps, the max over ranks taken by the caller."""
+    import torch
+
+    from nprush_b200 import _lib
+    from nprush_b200.distributed import ShardedTrainer, shard_views
+    from nprush_b200.gaussians import random_gaussians
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = _lib.context(dev)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    mine = shard_views(VIEWS, rank, world)
+    with torch.cuda.stream(stream):
+        vp, vpi, tg, st = build_scene(dev)
+        torch.cuda.synchronize()
+        st.set_targets(tg, borrow=True)
+        sched = view_schedule(args.warmup + args.steps + 4)
+        tuned = None
+        sel0 = sched[0][mine]
+        if not args.no_autotune and len(mine):
+            st.set_views(vp[sel0], vpi[sel0], sel0)
+            tuned = st.autotune()
+        # kernels of this rank's step: its graph captured once (the sharded
+        # step launches the same kernels eagerly), then eager steps
+        graph_kernels = 0
+        if len(mine):
+            st.set_graph(True)
+            st.set_views(vp[sel0], vpi[sel0], sel0)
+            st.train_step()
+            st.train_step()
+            graph_kernels = st.stats()["graph_kernels"]
+            st.set_graph(False)
+            # back to the common starting point (those two steps saw only this rank's views)
+            zeros = np.zeros((N_GAUSS, 64), np.float32)
+            st.write_params(random_gaussians(N_GAUSS, 10))
+            st.write_state(zeros, zeros, 0)
+            st.write_adc_stats(np.zeros(N_GAUSS, np.float32), np.zeros(N_GAUSS, np.float32))
+        sh = ShardedTrainer(st)
+        st.set_timing(True)
+        flush = torch.empty(64 * 1024 * 1024, device=f"cuda:{dev}")
+        for k in range(args.warmup):
+            sh.train_step(vp[sched[k]], vpi[sched[k]], sched[k])
+        torch.cuda.synchronize()
+        torch.distributed.barrier()
+        st.stage_times(reset=True)
+        times, pairs = [], []
+        with ClockSampler(dev) as clk:
+            for k in range(args.steps):
+                sel = sched[args.warmup + k]
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                sh.train_step(vp[sel], vpi[sel], sel)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                pairs.append(st.stats()["pairs"])
+        stages = st.stage_times(reset=True)
+        st.set_timing(False)
+        torch.cuda.synchronize()
+        torch.distributed.barrier()
+        # end to end: each rank uploads its own views' targets from page-locked host memory and reads its
+        # share of the loss back every step
+        host_all = torch.empty((CAMS, HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
+        host_all.copy_(tg.cpu())
+        hs = host_all.numpy()
+        ids = np.zeros(VIEWS, np.uint32)
+        ids[mine] = np.arange(len(mine), dtype=np.uint32)
+        torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            sel = sched[k]
+            if len(mine):
+                st.upload_targets(hs, sel[mine])
+            loss_last = sh.train_step(vp[sel], vpi[sel], ids)
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+        st.close()
+    return dict(tuned=tuned, ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
+                trained=None, graph_kernels=graph_kernels * world, views_local=len(mine), scaling="strong",
+                clocks=clk.summary(), e2e_ms=e2e_ms, h2d=len(mine) * HEIGHT * WIDTH * 16 * world,
+                d2h=4 * world, loss=[loss_last])
 
 
 def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush):
@@ -537,7 +628,8 @@ def run_splat_compat(args):
 
 
 METRIC = "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)"
-FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue")
+FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
+         "one CTA per (tile, view), longest first, barrier-free backward")
 
 # ------------------------------------------------- path-traced target workload
 PT_W, PT_H, PT_OBJECTS, PT_DETAIL, PT_BATCH = 1024, 768, 16, 20, 8
@@ -861,7 +953,7 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    res = run_ours(args, rank, world)
+    res = run_sharded(args, rank, world) if world > 1 else run_ours(args, rank, world)
     ms = res["ms_total"]
     if world > 1:
         import torch
@@ -874,7 +966,8 @@ def main():
     if rank != 0:
         return
     ms_per_step = ms / args.steps
-    value = world * 1000.0 / ms_per_step
+    strong = res.get("scaling") == "strong"
+    value = (1.0 if strong else world) * 1000.0 / ms_per_step
     pk, pk_kind = peaks()
     npx = WIDTH * HEIGHT
     K = res["pairs"]
@@ -885,18 +978,21 @@ def main():
         st = {k: (1.0, 1) for k in st}  # stage timing disabled
     dom = max(st, key=lambda k: st[k][0])
     dom_ms = st[dom][0] / max(st[dom][1], 1)
-    achieved = stage_bytes(dom, VIEWS, N_GAUSS, K, npx, tile_passes) / (dom_ms * 1e-3) / 1e9
+    v_local = res.get("views_local", VIEWS)  # views this rank rendered per step
+    achieved = stage_bytes(dom, v_local, N_GAUSS, K, npx, tile_passes) / (dom_ms * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if strong else "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded 200k-Gaussian student, targets rendered from a seeded 250k-Gaussian teacher",
         "config": {"workload": (f"{N_GAUSS // 1000}k Gaussians SH3, {WIDTH}x{HEIGHT}, {VIEWS} of {CAMS} "
                                 "sphere cameras per step, L1 + 0.2 D-SSIM, Adam"), "gaussians": N_GAUSS, "resolution": [WIDTH, HEIGHT],
                    "views_per_step": VIEWS,
                    "l2": "not flushed" if args.no_flush else "flushed between timed steps (256 MB write)",
-                   "pairs_per_step": K, "parallelism": "replicas" if world > 1 else "single GPU",
-                   "cuda_graph": not args.no_graph,
+                   "pairs_per_step": K, "parallelism": (f"view-sharded over {world} GPUs (NCCL all-reduce of the gradients per step)"
+                                   if world > 1 else "single GPU"),
+                   "cuda_graph": not args.no_graph and world == 1,
                    "raster_variant": (None if res.get("tuned") is None else
                                       {"tile": res["tuned"]["tile"],
                                        "fwd_form": FORMS[res["tuned"]["fwd_form"]],
@@ -908,7 +1004,8 @@ def main():
                                        "bwd_records_per_stage": res["tuned"]["bwd_stage"],
                                        "chosen_by": "autotuner"})},
         "clocks": res["clocks"],
-        "e2e": {"value": world * 1000.0 / res["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
+        "e2e": {"value": (1.0 if strong else world) * 1000.0 / res["e2e_ms"], "unit": "steps/s",
+                "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"]},
         "gpu_launches": None if res["graph_kernels"] is None else res["graph_kernels"] * args.steps,
         "gpu_launches_source": "kernel nodes of the captured train-step graph x timed steps",
