@@ -1,17 +1,24 @@
-"""What the trained ADC policy gains over the plain threshold rule, on a
-small seeded scene (20k-Gaussian student, 30k teacher, 256 x 256, 16
-cameras, 4 views per step, 1200 steps, ADC every 100 from step 300): the
-policy is trained on hindsight-labelled decisions logged from two plain runs
-on other seeds, then both rules train the held-out scene.  Deterministic
-mode makes each training run reproducible, and the policy's training is too
-(its gradients are summed in a fixed order).  Checked: the learned rule ends
-with no more Gaussians than the plain one (1% slack) and no worse PSNR (0.2 dB
-slack).  At this scale the two rules differ by less than a change of the
-scene or of the policy's seeds moves them (measured: 41421 vs 41402
-Gaussians and 38.74 vs 38.63 dB; with earlier kernel versions 41302 vs 41402
-and 39.05 vs 38.63 dB, 41411 vs 41402 and 38.61 vs 38.63 dB), so no strict gain is
-asserted; the 30k-step comparison at 200k Gaussians, 800x800, is where the policy's effect
-shows."""
+"""What the trained ADC policy gains over the plain threshold rule, measured
+on a small seeded scene (20k-Gaussian student, 30k teacher, SH degree 1,
+256 x 256, 16 cameras, 4 views per step, 1200 steps, ADC every 100 steps
+from step 300), deterministic mode so that every run is reproducible.
+
+The policy is trained on hindsight-labelled decisions logged from two plain
+runs on other seeds (keep -> prune when the lineage is pruned later, keep ->
+clone / split when the plain rule densifies it at the next event, densify ->
+keep when the lineage is pruned later).  Then, on three held-out scenes, the
+plain rule (densify when the view-space gradient >= 2e-4), the learned rule
+and the plain rule at thresholds 1.7e-4 and 1.6e-4 train the scene.
+
+What the network gains, per scene: the learned rule densifies earlier, ends
+with more Gaussians (+18 to +19% measured) and a higher PSNR (+1.1 to
++1.5 dB measured) than the plain rule it was trained from.  Against the
+plain rule's own count / quality trade-off, the PSNR the plain rule reaches
+at the learned rule's Gaussian count (interpolated between the 1.7e-4 and
+1.6e-4 thresholds), the difference is within that trade-off's own noise
+(measured +0.19, +0.31, -0.20 dB): the policy moves along the plain rule's
+curve rather than beyond it, and the test asserts no gain at matched count.
+"""
 import numpy as np
 import pytest
 
@@ -20,36 +27,59 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def test_learned_adc_keeps_psnr_with_fewer_gaussians():
+def test_learned_adc_gain_against_the_plain_rule():
     from nprush_b200 import build
     build.build()
-    from nprush_b200.learned_adc import AdcLog, hindsight_labels, logging_adc_fn, policy_adc_fn
+    from nprush_b200.learned_adc import AdcLog, hindsight_labels, logging_adc_fn, per_class_recall, policy_adc_fn
     from nprush_b200.policy import AdcPolicy
-    from nprush_b200.train import AdcSchedule, teacher_scene, evaluate_psnr, fit
+    from nprush_b200.train import AdcSchedule, evaluate_psnr, fit, teacher_scene
 
     adc = AdcSchedule(every=100, start=300, stop=1200)
     steps, views = 1200, 4
 
-    def run(seed, adc_fn):
-        vp, vpi, tg, st = teacher_scene(0, 20_000, 30_000, 256, 256, n_cams=16, sh_degree=1, capacity=60_000,
+    def run(seed, adc_fn, sched=adc):
+        vp, vpi, tg, st = teacher_scene(0, 20_000, 30_000, 256, 256, n_cams=16, sh_degree=1, capacity=80_000,
                                         student_seed=seed, teacher_seed=seed + 1000)
         st.set_deterministic(True)
         st.assign_ids(0)
-        r = fit(st, vp, vpi, steps, views=views, seed=seed, adc=adc, mode="batched", adc_fn=adc_fn)
+        r = fit(st, vp, vpi, steps, views=views, seed=seed, adc=sched, mode="batched", adc_fn=adc_fn)
         psnr = float(np.mean(evaluate_psnr(st, vp, vpi, views=views)))
         st.close()
-        return r, psnr
+        return r.count, psnr
 
     log = AdcLog(samples_per_event=5000, seed=1)
     for s in (201, 202):
         run(s, logging_adc_fn(log, adc))
     X, y = hindsight_labels(log, horizon=3)
-    assert (y == 3).sum() > 0 and (y == 0).sum() > 0
+    counts = np.bincount(y, minlength=4)
+    assert (counts > 0).all(), counts  # keep, clone, split and prune all labelled
+    hold = np.arange(len(y)) % 10 == 0
     pol = AdcPolicy(seed=7)
-    lc, ac = pol.train(X, y, epochs=20, batch=4096, lr=2e-3, seed=3)
-    assert lc[-1] < lc[0] and ac[-1] > 0.9
-    plain, p_psnr = run(203, None)
-    learned, l_psnr = run(203, policy_adc_fn(pol, adc))
-    print(f"plain: {plain.count} Gaussians, {p_psnr:.2f} dB; learned: {learned.count} Gaussians, {l_psnr:.2f} dB")
-    assert learned.count <= 1.01 * plain.count
-    assert l_psnr > p_psnr - 0.2
+    lc, ac = pol.train(X[~hold], y[~hold], epochs=20, batch=4096, lr=2e-3, seed=3)
+    assert lc[-1] < lc[0]
+    z = pol.logits(X[hold]).cpu().numpy()
+    pred = np.argmax(np.c_[np.zeros(len(z)), z], axis=1)
+    conf = np.zeros((4, 4), np.int64)
+    np.add.at(conf, (y[hold], pred), 1)
+    recall = per_class_recall(conf)
+    assert (pred == y[hold]).mean() > 0.9 and recall[0] > 0.95 and recall[2] > 0.4, recall
+
+    def thresh(t):
+        return AdcSchedule(every=adc.every, start=adc.start, stop=adc.stop, grad_thresh=t)
+
+    rows = []
+    for seed in (203, 204, 205):
+        plain = run(seed, None)
+        learned = run(seed, policy_adc_fn(pol, adc))
+        lo, hi = run(seed, None, thresh(1.7e-4)), run(seed, None, thresh(1.6e-4))
+        # the plain rule's PSNR at the learned rule's Gaussian count (linear between the two thresholds)
+        frac = (learned[0] - lo[0]) / (hi[0] - lo[0])
+        matched = lo[1] + frac * (hi[1] - lo[1])
+        rows.append((seed, plain, learned, lo, hi, matched))
+        print(f"seed {seed}: plain {plain[0]} / {plain[1]:.2f} dB, learned {learned[0]} / {learned[1]:.2f} dB, "
+              f"plain 1.7e-4 {lo[0]} / {lo[1]:.2f}, plain 1.6e-4 {hi[0]} / {hi[1]:.2f}; "
+              f"plain at the learned count {matched:.2f} dB")
+    for seed, plain, learned, lo, hi, matched in rows:
+        assert learned[0] > 1.1 * plain[0], (seed, plain, learned)        # densifies earlier
+        assert learned[1] > plain[1] + 0.8, (seed, plain, learned)        # and gains PSNR for it
+        assert abs(learned[1] - matched) < 0.6, (seed, learned, matched)  # along the plain rule's own curve
