@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
                                                     uint32_t H, uint32_t tiles_x, uint32_t tiles_y, float inv_tile,
                                                     Rec* __restrict__ recs, uint32_t* __restrict__ counts,
                                                     uint2* __restrict__ rects, uint32_t* __restrict__ dkeys,
-                                                    uint32_t* __restrict__ dvals) {
+                                                    uint32_t* __restrict__ dvals, uint32_t* __restrict__ ecounts,
+                                                    uint32_t* __restrict__ tmasks) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= nv * n) return;
   const uint32_t v = g / n, i = g - v * n;
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
   float q[4] = {q1.z, q1.w, q2.x, q2.y};
   Proj<float> P;
   project<float>(view, mean, ls, q, (float)W, (float)H, kLowpass, P);
-  uint32_t cnt = 0;
+  uint32_t cnt = 0, ecnt = 0, tmask = 0;
   uint2 rect = make_uint2(0, 0);
   uint32_t key = 0xffffffffu;
   Rec r;
@@ -190,10 +191,27 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
       r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
       // c.y: the alpha >= 1/255 level of the conic form (same 1% margin), for exact per-warp culling
       r.c = make_float4(fmaxf(col[2], 0.0f), t2 + 1e-4f, ex, ey);
+      // Pairs are emitted only for the tiles of the box that the alpha >=
+      // 1/255 ellipse meets (the same conservative test as the raster's
+      // per-warp culling, on the tile's pixel-centre square), for boxes of at
+      // most 32 tiles; a tile the ellipse misses gets no contribution from
+      // this Gaussian, so the images are unchanged and the lists shorter.
+      ecnt = cnt;
+      if (cnt <= 32) {
+        const float tm1 = 1.0f / inv_tile - 1.0f;
+        uint32_t bit = 0;
+        for (int ty = y0; ty < y1; ++ty)
+          for (int tx = x0; tx < x1; ++tx, ++bit)
+            if (!rec_misses_box(r.a, r.b.x, r.c, (float)tx / inv_tile, (float)ty / inv_tile, tm1, tm1))
+              tmask |= 1u << bit;
+        ecnt = (uint32_t)__popc(tmask);
+      }
     }
   }
   recs[g] = r;
   counts[g] = cnt;
+  ecounts[g] = ecnt;
+  tmasks[g] = tmask;
   rects[g] = rect;
   dkeys[g] = key;
   dvals[g] = g;
@@ -211,21 +229,25 @@ __global__ void k_gather_counts(const uint32_t* __restrict__ sorted_g, const uin
 // search over the warp's offsets (shuffles).  Output identical to writing
 // each entry's tile rectangle row by row.
 __global__ void __launch_bounds__(256) k_emit(const uint32_t* __restrict__ sorted_g,
-                                              const uint32_t* __restrict__ counts,
+                                              const uint32_t* __restrict__ ecounts,
                                               const uint32_t* __restrict__ offsets, const uint2* __restrict__ rects,
-                                              uint32_t m, uint32_t n, uint32_t tiles_x, uint32_t num_tiles,
-                                              uint32_t cap, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                              const uint32_t* __restrict__ tmasks, uint32_t m, uint32_t n,
+                                              uint32_t tiles_x, uint32_t num_tiles, uint32_t cap,
+                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
   if (__all_sync(0xffffffffu, j >= m)) return;
-  uint32_t g = 0, c = 0, off = 0xffffffffu, x0 = 0, w = 1, y0 = 0;
+  uint32_t g = 0, c = 0, off = 0xffffffffu, x0 = 0, w = 1, y0 = 0, tm = 0;
   if (j < m) {
     g = sorted_g[j];
-    c = counts[g];
+    c = ecounts[g];
     off = offsets[j];
     const uint2 r = rects[g];
     x0 = r.x & 0xffffu;
     w = max((r.x >> 16) - x0, 1u);
     y0 = r.y & 0xffffu;
+    // boxes of at most 32 tiles emit only the tiles of their mask
+    if (((r.y >> 16) - y0) * ((r.x >> 16) - x0) <= 32u) tm = tmasks[g];
+    else tm = 0xffffffffu;
   }
   const uint32_t start = __shfl_sync(0xffffffffu, off, 0);
   const uint32_t end = __reduce_max_sync(0xffffffffu, j < m ? off + c : 0u);
@@ -240,9 +262,16 @@ __global__ void __launch_bounds__(256) k_emit(const uint32_t* __restrict__ sorte
     }
     const uint32_t gL = __shfl_sync(0xffffffffu, g, L), oL = __shfl_sync(0xffffffffu, off, L);
     const uint32_t x0L = __shfl_sync(0xffffffffu, x0, L), wL = __shfl_sync(0xffffffffu, w, L);
-    const uint32_t y0L = __shfl_sync(0xffffffffu, y0, L);
+    const uint32_t y0L = __shfl_sync(0xffffffffu, y0, L), tmL = __shfl_sync(0xffffffffu, tm, L);
     if (sl < end && sl < cap) {
-      const uint32_t local = sl - oL, ry = local / wL;
+      uint32_t local = sl - oL;
+      if (tmL != 0xffffffffu) {
+        // the local-th set bit of the mask is the tile's index in the box
+        uint32_t mk = tmL;
+        for (uint32_t t = 0; t < local; ++t) mk &= mk - 1u;
+        local = (uint32_t)(__ffs(mk) - 1);
+      }
+      const uint32_t ry = local / wL;
       keys[sl] = (gL / n) * num_tiles + (y0L + ry) * tiles_x + x0L + (local - ry * wL);
       vals[sl] = gL;
     }
@@ -1697,7 +1726,8 @@ struct nps_gs {
   uint32_t nv = 0;
   DevBuf views, tids;
   // forward state
-  DevBuf recs, counts, rects, dkeys, dvals, cnt_sorted, offsets, total, mcount, keys, vals, ranges, img, ncontrib;
+  DevBuf recs, counts, ecounts, tmasks, rects, dkeys, dvals, cnt_sorted, offsets, total, mcount, keys, vals, ranges;
+  DevBuf img, ncontrib;
   DevBuf maps, partial, loss, dimg, g2;
   SortWork sw_depth, sw_tile;
   uint32_t pair_cap = 0;
@@ -1888,8 +1918,9 @@ int nps_gs_destroy(nps_gs* o) {
     b->release();
   for (DevBuf* b : {&o->tile_last, &o->ws_order_f, &o->ws_order_b, &o->ws_q}) b->release();
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->adc_grad, &o->adc_denom, &o->tgt_own, &o->views,
-                    &o->tids, &o->recs, &o->counts, &o->rects, &o->dkeys, &o->dvals, &o->cnt_sorted, &o->offsets,
-                    &o->total, &o->mcount, &o->keys, &o->vals, &o->ranges, &o->img, &o->ncontrib, &o->maps,
+                    &o->tids, &o->recs, &o->counts, &o->ecounts, &o->tmasks, &o->rects, &o->dkeys, &o->dvals,
+                    &o->cnt_sorted, &o->offsets, &o->total, &o->mcount, &o->keys, &o->vals, &o->ranges, &o->img,
+                    &o->ncontrib, &o->maps,
                     &o->partial, &o->loss, &o->dimg, &o->g2, &o->sw_depth.hist, &o->sw_depth.partial,
                     &o->sw_depth.lookback, &o->sw_depth.keys_alt, &o->sw_depth.vals_alt, &o->sw_tile.hist,
                     &o->sw_tile.partial, &o->sw_tile.lookback, &o->sw_tile.keys_alt, &o->sw_tile.vals_alt})
@@ -2348,6 +2379,8 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
   }
   NPS_TRY(o->recs.ensure(sizeof(gs::Rec) * (M + 1)));
   NPS_TRY(o->counts.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->ecounts.ensure(sizeof(uint32_t) * (M + 1)));
+  NPS_TRY(o->tmasks.ensure(sizeof(uint32_t) * (M + 1)));
   NPS_TRY(o->rects.ensure(sizeof(uint2) * (M + 1)));
   NPS_TRY(o->dkeys.ensure(sizeof(uint32_t) * (M + 1)));
   NPS_TRY(o->dvals.ensure(sizeof(uint32_t) * (M + 1)));
@@ -2368,7 +2401,8 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
                                                       tiles_x, tiles_y, 1.0f / (float)o->tile,                  \
                                                       o->recs.as<gs::Rec>(),                                    \
                                                       o->counts.as<uint32_t>(), o->rects.as<uint2>(),           \
-                                                      o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>())
+                                                      o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>(),         \
+                                                      o->ecounts.as<uint32_t>(), o->tmasks.as<uint32_t>())
     switch (o->sh_deg) {
       case 0: NPS_PRE(0); break;
       case 1: NPS_PRE(1); break;
@@ -2383,7 +2417,7 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
     NPS_TRY(radix_sort_u32(o->dkeys.as<uint32_t>(), o->dvals.as<uint32_t>(), o->mcount.as<uint32_t>(), (uint32_t)M, 32,
                            o->sw_depth, s, &dk, &dv)); }
     o->sorted_vals = dv;
-    gs::k_gather_counts<<<div_up(M, 256), 256, 0, s>>>(dv, o->counts.as<uint32_t>(), (uint32_t)M,
+    gs::k_gather_counts<<<div_up(M, 256), 256, 0, s>>>(dv, o->ecounts.as<uint32_t>(), (uint32_t)M,
                                                         o->cnt_sorted.as<uint32_t>());
     NPS_CHECK_LAUNCH();
     uint32_t* total = o->total.as<uint32_t>();
@@ -2411,8 +2445,9 @@ static int gs_forward_impl(nps_gs* o, float* out_rgba, bool capture) {
     }
     if (K > 0 || capture) {
       { StageTimer t(o, ST_EMIT);
-      gs::k_emit<<<div_up(M, 256), 256, 0, s>>>(dv, o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(),
-                                                 o->rects.as<uint2>(), (uint32_t)M, n, tiles_x, num_tiles, o->pair_cap,
+      gs::k_emit<<<div_up(M, 256), 256, 0, s>>>(dv, o->ecounts.as<uint32_t>(), o->offsets.as<uint32_t>(),
+                                                 o->rects.as<uint2>(), o->tmasks.as<uint32_t>(), (uint32_t)M, n,
+                                                 tiles_x, num_tiles, o->pair_cap,
                                                  o->keys.as<uint32_t>(), o->vals.as<uint32_t>());
       NPS_CHECK_LAUNCH(); }
       int bits = 1;
