@@ -38,6 +38,11 @@ P_USED = 59          # floats per Gaussian used by the model
 # 1-pass ncu capture of this workload (13,727,114 pairs): scaled to a launch by its pair count.
 BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 270_533_120 + 15_059_968, 13_727_114
 S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, opacity)
+# Warp instructions issued by one launch of each raster kernel (smsp__inst_executed.sum) in a 1-pass
+# ncu capture of this workload with the variant named, and that launch's pair count: scaled to a
+# launch by its pair count.  Key: (stage, form, pixels per thread, records per stage) at 16 x 16 tiles.
+RASTER_INST = {("raster_fwd", 2, 2, 128): (531_319_934, 11_433_806)}
+SMS, ISSUE_PER_SM_CLK = 148, 4  # B200: 148 SMs, four warp schedulers each issuing one instruction per clock
 
 
 def peaks():
@@ -111,6 +116,26 @@ def stage_bytes(stage: str, V: int, N: int, K: int, npx: int, tile_passes: int) 
         "project_bwd": V * N * (40 + S_REC) + 2 * N * P_USED * 4,
         "adam": N * P_USED * 4 * 7,
     }[stage]
+
+
+def issue_roofline(stage, tuned, K, ms, sm_mhz):
+    """Issue-slot roofline of a raster stage: its warp instructions per launch (the ncu count of the same
+    variant, scaled by pairs) over its CUDA-event duration, against SMs x 4 schedulers x the SM clock
+    sampled during the timed steps.  None when no count of the variant that ran is recorded."""
+    if tuned is None or tuned["tile"] != 16:
+        return None
+    form, ppt, sps = ((tuned["fwd_form"], tuned["fwd_ppt"], tuned["fwd_stage"]) if stage == "raster_fwd" else
+                      (tuned["bwd_form"], tuned["bwd_ppt"], tuned["bwd_stage"]))
+    rec = RASTER_INST.get((stage, form, ppt, sps))
+    if rec is None or not ms:
+        return None
+    inst = rec[0] * K / rec[1]
+    mhz = sm_mhz or 1965.0
+    achieved = inst / (ms * 1e-3) / 1e9
+    peak = SMS * ISSUE_PER_SM_CLK * mhz * 1e-3
+    return {"bound": "issue", "kernel": stage, "achieved": achieved, "peak": peak, "unit": "G warp-inst/s",
+            "frac": achieved / peak, "inst_per_launch": inst, "sm_mhz": mhz,
+            "source": "ncu smsp__inst_executed.sum of the same variant at this workload, scaled by pairs"}
 
 
 def step_bytes(V, N, K, npx):
@@ -627,9 +652,209 @@ def run_splat_compat(args):
     return line
 
 
+# ------------------------------------------------- Bezier curve optimiser workload
+BZ_N, BZ_TEACHER, BZ_RES, BZ_VIEWS, BZ_CAMS = 50_000, 60_000, 512, 4, 32
+BZ_METRIC = ("Bezier optimiser dispatches/s (reference semantics: backward over 4 views + step + ADC every 50th; "
+             "50k cubic curves, 512^2)")
+
+
+def _bz_cameras():
+    from nprush_b200.camera import sphere_cameras
+    return sphere_cameras(BZ_CAMS, 4.0, math.radians(50.0), 1.0)
+
+
+def run_bezier(args):
+    """The reference-semantics Bezier optimiser (nps_bezier_opt_dispatch: the
+    reference's bezier_backward / bezier_step / bezier_adc, 16-segment
+    ribbons, 1024 curves per tile, i32 fixed-point gradients) on the GPU: 50k
+    random-walk curves (seed 20) fitting the 512 x 512 renders of a seeded
+    60k-curve teacher, 4 of 32 sphere cameras per dispatch.  CUDA events
+    around each dispatch on the library's stream, L2 flushed between them."""
+    import torch
+
+    from nprush_b200 import _lib
+    from nprush_b200.bezier import GpuBezierOptimizerManager
+    from nprush_b200.bezier_fit import random_walk_curves
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = _lib.context(dev)
+    _lib.call("nps_set_stream", ctx, stream.cuda_stream)
+    W = H = BZ_RES
+    V = BZ_VIEWS
+    vp, vpi = _bz_cameras()
+    rng = np.random.default_rng(5)
+    sels = [np.sort(rng.permutation(BZ_CAMS)[:V]) for _ in range(args.warmup + 2 * args.steps)]
+    with torch.cuda.stream(stream):
+        teacher = GpuBezierOptimizerManager(BZ_TEACHER, init=random_walk_curves(BZ_TEACHER, 21, H))
+        tg = torch.zeros((BZ_CAMS, H, W, 4), device="cuda")
+        for c in range(BZ_CAMS):
+            teacher.render(vp[c], W, H, tg[c])
+        teacher.close()
+        m = GpuBezierOptimizerManager(BZ_N, init=random_walk_curves(BZ_N, 20, H))
+        m.write_mode(1.0)
+        depth = torch.ones((V, H, W, 4), device="cuda")
+        zeros = torch.zeros((V, H, W, 4), device="cuda")
+        tgs = [tg[torch.as_tensor(sel, device="cuda")].contiguous() for sel in sels]
+
+        def step(k):
+            m.write_vp(vp[sels[k]], vpi[sels[k]])
+            m.set_backward_target(tgs[k], depth, zeros, depth, zeros, W, H, borrow=True)
+            m.dispatch()
+
+        for k in range(args.warmup):
+            step(k)
+        flush = torch.empty(64 * 1024 * 1024, device=f"cuda:{dev}")
+        times = []
+        with ClockSampler(dev) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ev[0].record(stream)
+                step(args.warmup + k)
+                ev[1].record(stream)
+                ev[1].synchronize()
+                times.append(ev[0].elapsed_time(ev[1]))
+        st = m.stats()
+        # end to end: the caller's four targets (rgba + depth, background, normals) from page-locked host memory
+        host = [torch.from_numpy(tgs[0].cpu().numpy()).pin_memory().numpy()]
+        hd, hz = (torch.from_numpy(x.cpu().numpy()).pin_memory().numpy() for x in (depth, zeros))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            m.write_vp(vp[sels[args.warmup + args.steps + k]], vpi[sels[args.warmup + args.steps + k]])
+            m.set_backward_target(host[0], hd, hz, hd, hz, W, H)
+            m.dispatch()
+            _lib.call("nps_sync", ctx)
+        e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+        m.close()
+    ms = float(np.mean(times))
+    line = {
+        "metric": BZ_METRIC, "value": 1000.0 / ms, "unit": "dispatches/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (i32 fixed-point gradients)",
+        "data": "synthetic: seeded random-walk curves; targets rendered from a seeded 60k-curve teacher",
+        "config": {"workload": f"reference-semantics Bezier dispatch: {BZ_N // 1000}k cubic curves, {W}x{H}, "
+                               f"{V} of {BZ_CAMS} sphere cameras per dispatch, ADC every 50th",
+                   "pairs_per_dispatch": int(st["pairs"]), "l2": "flushed between timed dispatches (256 MB write)"},
+        "clocks": clk.summary(),
+        "e2e": {"value": 1000.0 / e2e_ms, "unit": "dispatches/s",
+                "h2d_bytes_per_step": int(host[0].nbytes + 4 * hd.nbytes), "d2h_bytes_per_step": 0},
+    }
+    if not args.no_cpu_baseline:
+        r = reference_bezier_rate(3)
+        if "value" in r:
+            line["cpu_baseline"] = {"value": r["value"], "unit": "dispatches/s", "cores": r["cores"],
+                                    "kind": "reference", "sample": r["sample"]}
+    return line
+
+
+def _bz_ref_worker_init(so_path, n):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import build_ref
+    import refrun
+    from nprush_b200.bezier_fit import random_walk_curves
+    mod = build_ref.RefModule.from_path(so_path)
+    vp, vpi = _bz_cameras()
+    rng = np.random.default_rng(11)
+    tgt = np.zeros((BZ_RES, BZ_RES, 4), np.float32)
+    tgt[..., :3] = rng.random((BZ_RES, BZ_RES, 3))
+    tgt[..., 3] = 1.0
+    one = np.zeros((BZ_RES, BZ_RES, 4), np.float32)
+    one[..., 0] = 1.0
+    zero = np.zeros((BZ_RES, BZ_RES, 4), np.float32)
+    keep = [random_walk_curves(n, 20, BZ_RES), np.zeros(n * 18, np.int32), tgt, one,
+            refrun.bezier_uniforms(vp[0], vpi[0], mode=1.0), zero, one, np.zeros(2 * n, np.float32), zero,
+            np.zeros(512 * 512, np.int32)]
+    for slot, a in enumerate(keep):
+        (mod.bind_tex if slot in (2, 3, 5, 6, 8) else mod.bind)(slot, a)
+    _REF["bz"] = (mod, keep)
+
+
+def _bz_ref_worker_run(tiles, gx, gy):
+    mod = _REF["bz"][0]
+    for tx, ty in tiles:
+        mod.run_one(tx, ty, 0, gx, gy, 1)
+    return len(tiles)
+
+
+def reference_bezier_rate(samples: int) -> dict:
+    """Dispatches/s of the reference's bezier_backward + bezier_step at 50k
+    curves, 512 x 512, 4 views per dispatch (the reference fits one view per
+    backward dispatch, so one of these dispatches is 4 of its backward
+    dispatches and one step): each timed sample runs a lattice of the 16 x 16
+    workgroups of one view on a process pool over all host cores; the
+    dispatch time is the tile throughput extrapolated to every tile of the 4
+    views, plus one full bezier_step dispatch.  ADC (every 50th) not counted."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import build_ref
+
+    n = BZ_N
+    so = sorted((ROOT / "oracle" / "_ref").glob(f"bezier_backward_n{n}_*.so"))
+    so_step = sorted((ROOT / "oracle" / "_ref").glob(f"bezier_step_n{n}_*.so"))
+    if not so or not so_step:
+        if not build_ref.reference_available():
+            return {"unavailable": "oracle/_ref for 50k curves was not built (no reference checkout)"}
+        so = [build_ref.build("bezier_backward", n)]
+        so_step = [build_ref.build("bezier_step", n)]
+    gx = gy = (BZ_RES + 15) // 16
+    workers = os.cpu_count() or 1
+    stride = 5
+    tiles = [(x, y) for y in range(stride // 2, gy, stride) for x in range(stride // 2, gx, stride)]
+    per_worker = max(1, -(-len(tiles) // workers))
+    shares = [tiles[k:k + per_worker] for k in range(0, len(tiles), per_worker)]
+    rates = []
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
+                                initializer=_bz_ref_worker_init, initargs=(str(so[-1]), n)) as ex:
+        list(ex.map(_bz_ref_worker_run, [shares[0][:1]] * workers, [gx] * workers, [gy] * workers))  # warm-up
+        for _ in range(max(1, samples)):
+            t0 = time.perf_counter()
+            done = sum(ex.map(_bz_ref_worker_run, shares, [gx] * len(shares), [gy] * len(shares)))
+            rates.append(done / (time.perf_counter() - t0))
+    tile_rate = float(np.median(rates))
+    from nprush_b200.bezier_fit import random_walk_curves
+    import refrun
+    vp, vpi = _bz_cameras()
+    mod_s = build_ref.RefModule.from_path(so_step[-1])
+    b = random_walk_curves(n, 20, BZ_RES)
+    adam = np.zeros(36 * n + 8, np.float32)
+    adam[36 * n + 1] = 1.0
+    arrs = [b, np.zeros(n * 18, np.int32), adam, np.zeros(2 * n, np.float32),
+            refrun.bezier_uniforms(vp[0], vpi[0], mode=1.0)]
+    for slot, a in enumerate(arrs):
+        mod_s.bind(slot, a)
+    t0 = time.perf_counter()
+    mod_s.dispatch((n + 63) // 64, 1, 1)
+    t_step = time.perf_counter() - t0
+    disp_s = gx * gy * BZ_VIEWS / tile_rate + t_step
+    return {"value": 1.0 / disp_s, "cores": workers,
+            "sample": f"{len(tiles)} of {gx * gy} tiles of one view (a lattice, every {stride}th tile each way) per "
+                      f"timed sample on {workers} processes ({tile_rate:.1f} tiles/s), extrapolated to {gx * gy} "
+                      f"tiles x {BZ_VIEWS} views + one full bezier_step ({t_step:.3f} s, one thread); ADC not "
+                      "counted; random target (its values do not change the per-pixel work)"}
+
+
+def run_bezier_reference(args):
+    r = reference_bezier_rate(args.steps)
+    if "unavailable" in r:
+        return {"impl": "reference", "unavailable": r["unavailable"]}
+    v = r["value"]
+    return {"impl": "reference", "metric": BZ_METRIC, "value": v, "unit": "dispatches/s", "higher_is_better": True,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "reference bezier_backward + bezier_step (its own WGSL, translated to C++): "
+                                   "50k cubic curves, 512x512, 4 views per dispatch"},
+            "cpu_baseline": {"value": v, "unit": "dispatches/s", "cores": r["cores"], "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "dispatches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 METRIC = "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)"
-FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
-         "one CTA per (tile, view), longest first, barrier-free backward")
+FWD_FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
+             "one CTA per (tile, view), longest first")
+BWD_FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
+             "one CTA per (tile, view), longest first, no CTA barrier")
 
 # ------------------------------------------------- path-traced target workload
 PT_W, PT_H, PT_OBJECTS, PT_DETAIL, PT_BATCH = 1024, 768, 16, 20, 8
@@ -885,7 +1110,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="train", choices=["train", "splat_compat", "path_trace", "mesh_raster"],
+    ap.add_argument("--workload", default="train", choices=["train", "splat_compat", "bezier", "path_trace", "mesh_raster"],
                     help="train: the Gaussian train step (headline); splat_compat: the reference-semantics splat "
                          "optimiser at the reference arm's shape; path_trace: path-traced target generation; "
                          "mesh_raster: the viewer's mesh render pass (colour + depth targets)")
@@ -928,6 +1153,10 @@ def main():
                 print(json.dumps(r))
             else:
                 print(json.dumps(run_splat_compat(args)))
+        return
+    if args.workload == "bezier":
+        if rank == 0:
+            print(json.dumps(run_bezier_reference(args) if args.impl == "reference" else run_bezier(args)))
         return
     if args.workload == "path_trace":
         if rank != 0:
@@ -995,8 +1224,8 @@ def main():
                    "cuda_graph": not args.no_graph and world == 1,
                    "raster_variant": (None if res.get("tuned") is None else
                                       {"tile": res["tuned"]["tile"],
-                                       "fwd_form": FORMS[res["tuned"]["fwd_form"]],
-                                       "bwd_form": FORMS[res["tuned"]["bwd_form"]],
+                                       "fwd_form": FWD_FORMS[res["tuned"]["fwd_form"]],
+                                       "bwd_form": BWD_FORMS[res["tuned"]["bwd_form"]],
                                        "per_tile": res["tuned"]["per_tile"],
                                        "fwd_pixels_per_thread": res["tuned"]["fwd_ppt"],
                                        "fwd_records_per_stage": res["tuned"]["fwd_stage"],
@@ -1015,7 +1244,10 @@ def main():
                      "traffic_source": "ncu capture of the same kernel and workload, scaled by pairs",
                      "peak_kind": pk_kind,
                      "step_algorithmic_bytes": step_bytes(VIEWS, N_GAUSS, K, npx),
-                     "step_frac": step_bytes(VIEWS, N_GAUSS, K, npx) / (ms_per_step * 1e-3) / 1e9 / pk["hbm_gbs"]},
+                     "step_frac": step_bytes(VIEWS, N_GAUSS, K, npx) / (ms_per_step * 1e-3) / 1e9 / pk["hbm_gbs"],
+                     "issue": {k: issue_roofline(k, res.get("tuned"), K, st[k][0] / max(st[k][1], 1),
+                                                 (res["clocks"] or {}).get("sm_mhz"))
+                               for k in ("raster_fwd", "raster_bwd") if k in st}},
         "stages_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in st.items()},
         "trained_state": res["trained"],
         "final_loss": res["loss"],

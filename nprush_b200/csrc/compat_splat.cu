@@ -227,6 +227,28 @@ __global__ void k_emit(const uint32_t* __restrict__ counts, const uint32_t* __re
     }
 }
 
+// Statistics of the last backward's tile lists: out[0] += sum of
+// min(length, kCap) (pairs composited), out[1] = longest list.
+__global__ void k_tile_stats(const uint32_t* __restrict__ rstart, const uint32_t* __restrict__ rend, uint32_t m,
+                             unsigned long long* __restrict__ out) {
+  unsigned long long sum = 0;
+  uint32_t mx = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const uint32_t len = rend[i] - rstart[i];
+    sum += min(len, kCap);
+    mx = max(mx, len);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, sum);
+    atomicMax(out + 1, (unsigned long long)mx);
+  }
+}
+
 // Tile list bounds in the sorted key array.
 __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
                          uint32_t* __restrict__ rstart, uint32_t* __restrict__ rend) {
@@ -815,9 +837,10 @@ struct nps_splat_opt {
   const float* tgt_rgba = nullptr;
   const float* tgt_depth = nullptr;
   // work
-  DevBuf fwd, bwd, counts, offsets, rects, total, keys, vals, ranges, tabs, dead, stat;
+  DevBuf fwd, bwd, counts, offsets, rects, total, keys, vals, ranges, tabs, dead, stat, tstat;
   SortWork sw;
   uint32_t pair_cap = 0;
+  uint32_t last_ranges = 0;  // (view, tile) entries of the last backward's ranges
   nps_stats stats{};
 };
 
@@ -887,8 +910,8 @@ int nps_splat_opt_destroy(nps_splat_opt* o) {
   cudaStreamSynchronize(o->ctx->stream);
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->views, &o->tgt_rgba_own,
                     &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->offsets, &o->rects, &o->total,
-                    &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->sw.hist, &o->sw.partial,
-                    &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt})
+                    &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->tstat, &o->sw.hist,
+                    &o->sw.partial, &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt})
     b->release();
   if (o->rw) {
     o->rw->release();
@@ -1088,6 +1111,7 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
     NPS_CHECK_LAUNCH();
   }
   o->stats.pairs = K;
+  o->last_ranges = num_tiles * nv;
   return NPS_OK;
 }
 
@@ -1143,9 +1167,22 @@ int nps_splat_opt_set_step_count(nps_splat_opt* o, uint32_t count) {
 int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
   NPS_TRY(check_opt(o));
   if (!out) return NPS_ERR_INVALID;
+  cudaStream_t s = o->ctx->stream;
   uint32_t clones = 0;
-  NPS_CUDA(cudaMemcpyAsync(&clones, o->stat.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, o->ctx->stream));
-  NPS_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  uint64_t ts[2] = {0, 0};  // pairs composited (each tile list capped), longest list
+  NPS_CUDA(cudaMemcpyAsync(&clones, o->stat.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (o->last_ranges > 0) {
+    NPS_TRY(o->tstat.ensure(2 * sizeof(uint64_t)));
+    NPS_CUDA(cudaMemsetAsync(o->tstat.p, 0, 2 * sizeof(uint64_t), s));
+    const uint32_t* rstart = o->ranges.as<uint32_t>();
+    compat::k_tile_stats<<<std::min(div_up(o->last_ranges, 256), 4u * kNumSMs), 256, 0, s>>>(
+        rstart, rstart + o->last_ranges, o->last_ranges, o->tstat.as<unsigned long long>());
+    NPS_CHECK_LAUNCH();
+    NPS_CUDA(cudaMemcpyAsync(ts, o->tstat.p, sizeof(ts), cudaMemcpyDeviceToHost, s));
+  }
+  NPS_CUDA(cudaStreamSynchronize(s));
+  o->stats.pairs_capped = ts[0];
+  o->stats.max_tile_len = (uint32_t)ts[1];
   o->stats.adc_clones = clones;
   o->stats.step_count = o->step_count;
   *out = o->stats;

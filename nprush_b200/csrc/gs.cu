@@ -84,9 +84,37 @@ __device__ __forceinline__ bool rec_misses_box(const float4& a, float cc, const 
   const float q4 = ca * x_h * x_h + 2.0f * cb * x_h * hy + cc * hy * hy;
   return fminf(fminf(q1, q2), fminf(q3, q4)) > c.y;
 }
-__device__ __forceinline__ bool rec_misses_strip(const float4& a, float cc, const float4& c, float x0, float y0,
-                                                 float h) {
-  return rec_misses_box(a, cc, c, x0, y0, 15.0f, h);
+
+#ifndef NPS_GS_STRIP_W
+#define NPS_GS_STRIP_W 8
+#endif
+// Thread-to-pixel map of the 16 x 16 tile kernels (forms 0 and 2): thread tid
+// shades PPT vertically adjacent pixels from (x, y) of the tile, and its warp
+// covers a kW x kH strip at (wx, wy), the region its per-warp culling tests.
+// NPS_GS_STRIP_W 8 (default): 8 x 4·PPT strips, two side by side, closer to
+// square, so a small footprint meets fewer warps (backward -9%, forward -5%
+// at 200k Gaussians, 800 x 800, 8 views, against 16); 16: full-width
+// 16 x 2·PPT strips.
+template <int PPT>
+struct TileMap16 {
+  static constexpr int kW = NPS_GS_STRIP_W, kH = 32 * PPT / NPS_GS_STRIP_W;
+  static constexpr int kWarpsX = 16 / kW;
+  static_assert(kW == 16 || kW == 8, "strip width");
+  __device__ static uint32_t wx(uint32_t tid) { return ((tid >> 5) % kWarpsX) * kW; }
+  __device__ static uint32_t wy(uint32_t tid) { return ((tid >> 5) / kWarpsX) * kH; }
+  __device__ static uint32_t x(uint32_t tid) { return wx(tid) + (tid & (kW - 1)); }
+  __device__ static uint32_t y(uint32_t tid) { return wy(tid) + PPT * ((tid & 31) / kW); }
+};
+
+// Exponent of the Gaussian at offset d = (dx, dy) from its centre, -q(d) / 2
+// with q(d) = dx u + dy w and (u, w) the conic (a.z, a.w; a.w, cc) times d.
+// Every raster kernel evaluates it in this one order, so the forward and the
+// backward take the same alpha >= 1/255 decisions; u and w are reused by the
+// backward's mean gradient.
+__device__ __forceinline__ float gs_power(const float4& a, float cc, float dx, float dy, float& u, float& w) {
+  u = fmaf(a.w, dy, a.z * dx);
+  w = fmaf(cc, dy, a.w * dx);
+  return -0.5f * fmaf(dy, w, dx * u);
 }
 
 // true if the Gaussian's alpha >= 1/255 box misses the warp's pixels
@@ -120,6 +148,44 @@ __device__ __forceinline__ float warp_sum16(float (&v)[16], uint32_t lane) {
     v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
   }
   return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// Sum of 9 values over the warp by uneven recursive halving: at each level a
+// lane keeps the first ceil(m/2) of its m partial values (lower half of the
+// lane pair) or the rest (upper half, padded with a zero), 5 + 3 + 2 + 1 + 1
+// = 12 shuffles.  On return, lanes 2q and 2q + 1 hold the warp total of value
+// warp_sum9_index(lane) when that is below 9 (every value has one q).
+__device__ __forceinline__ float warp_sum9(const float (&v)[9], uint32_t lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+  float w[5], x[3], y[2];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    const float hi = j + 5 < 9 ? v[j + 5] : 0.0f;
+    const float send = b4 ? v[j] : hi, keep = b4 ? hi : v[j];
+    w[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float hi = j + 3 < 5 ? w[j + 3] : 0.0f;
+    const float send = b3 ? w[j] : hi, keep = b3 ? hi : w[j];
+    x[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const float hi = j + 2 < 3 ? x[j + 2] : 0.0f;
+    const float send = b2 ? x[j] : hi, keep = b2 ? hi : x[j];
+    y[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  const float send = b1 ? y[0] : y[1], keep = b1 ? y[1] : y[0];
+  const float z = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  return z + __shfl_xor_sync(0xffffffffu, z, 1);
+}
+
+// The value whose total warp_sum9 leaves in this lane; 15 for a padding slot.
+// Nibble q of the table is the index kept by lanes 2q, 2q + 1 (the
+// partition above traced through its four uneven levels).
+__device__ __forceinline__ uint32_t warp_sum9_index(uint32_t lane) {
+  return (uint32_t)(0xfff8f765ff43f210ull >> (4u * ((lane >> 1) & 15u))) & 15u;
 }
 
 __device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(-x)); }
@@ -191,19 +257,34 @@ __global__ void __launch_bounds__(256) k_preprocess(const float* __restrict__ pa
       r.b = make_float4(P.cc, op, fmaxf(col[0], 0.0f), fmaxf(col[1], 0.0f));
       // c.y: the alpha >= 1/255 level of the conic form (same 1% margin), for exact per-warp culling
       r.c = make_float4(fmaxf(col[2], 0.0f), t2 + 1e-4f, ex, ey);
-      // Pairs are emitted only for the tiles of the box that the alpha >=
-      // 1/255 ellipse meets (the same conservative test as the raster's
-      // per-warp culling, on the tile's pixel-centre square), for boxes of at
-      // most 32 tiles; a tile the ellipse misses gets no contribution from
-      // this Gaussian, so the images are unchanged and the lists shorter.
+      // Pairs are emitted only for the tiles of the box whose pixel-centre
+      // square the alpha >= 1/255 ellipse meets, for boxes of at most 32
+      // tiles; a tile the ellipse misses gets no contribution from this
+      // Gaussian, so the images are unchanged and the lists shorter.  Per tile
+      // row, the ellipse's x-extent over the row's pixel-centre band
+      // [y, y + T - 1] is exact: the left boundary x = k dy - hw(dy) (k =
+      // Sigma_xy / Sigma_yy, hw^2 = (t2 - dy^2 / Sigma_yy) det / Sigma_yy) is
+      // convex in dy with its minimum at the leftmost point dy = -Sigma_xy
+      // sqrt(t2 / Sigma_xx), so the band's minimum is there clamped to the
+      // band (the right boundary mirrors it); widened by 1e-3 px + 1e-6 |u|
+      // for rounding.  The tiles of the row meeting that extent are set in a
+      // 32-bit mask, row-major over the box.
       ecnt = cnt;
       if (cnt <= 32) {
-        const float tm1 = 1.0f / inv_tile - 1.0f;
-        uint32_t bit = 0;
-        for (int ty = y0; ty < y1; ++ty)
-          for (int tx = x0; tx < x1; ++tx, ++bit)
-            if (!rec_misses_box(r.a, r.b.x, r.c, (float)tx / inv_tile, (float)ty / inv_tile, tm1, tm1))
-              tmask |= 1u << bit;
+        const float T = 1.0f / inv_tile, tm1 = T - 1.0f;
+        const float kx = P.B / P.C, hw2 = P.det / P.C, ic = 1.0f / P.C;
+        const float dyx = P.B * sqrtf(t2 / P.A), eps = 1e-3f + 1e-6f * fabsf(P.u);
+        const uint32_t w = (uint32_t)(x1 - x0);
+        for (int ty = y0; ty < y1; ++ty) {
+          const float ly = fmaxf((float)ty * T - P.v, -ey), hy = fminf((float)ty * T + tm1 - P.v, ey);
+          if (ly > hy) continue;
+          const float dl = fminf(fmaxf(-dyx, ly), hy), dr = fminf(fmaxf(dyx, ly), hy);
+          const float xl = P.u + kx * dl - sqrtf(fmaxf(t2 - dl * dl * ic, 0.0f) * hw2) - eps;
+          const float xr = P.u + kx * dr + sqrtf(fmaxf(t2 - dr * dr * ic, 0.0f) * hw2) + eps;
+          const int c0 = max(x0, (int)ceilf((xl - tm1) * inv_tile)), c1 = min(x1, (int)floorf(xr * inv_tile) + 1);
+          if (c1 > c0) tmask |= ((c1 - c0 == 32) ? 0xffffffffu : ((1u << (c1 - c0)) - 1u))
+                                << ((uint32_t)(ty - y0) * w + (uint32_t)(c0 - x0));
+        }
         ecnt = (uint32_t)__popc(tmask);
       }
     }
@@ -383,10 +464,11 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     tx = tile - ty * tiles_x;
   }
   const uint32_t tid = threadIdx.x;
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
+  using TM = TileMap16<PPT>;
+  const uint32_t px = tx * 16 + TM::x(tid), py = ty * 16 + TM::y(tid);
   const float fx = (float)px;
-  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * (tid >> 5));
-  constexpr float wh = (float)(2 * PPT - 1);
+  const float wx0 = (float)(tx * 16 + TM::wx(tid)), wy0 = (float)(ty * 16 + TM::wy(tid));
+  constexpr float ww = (float)(TM::kW - 1), wh = (float)(TM::kH - 1);
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key], end = rend[key];
   float T[PPT], C0[PPT], C1[PPT], C2[PPT];
@@ -428,7 +510,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     for (int qq = 0; qq < SB / 32; ++qq) {
       const uint32_t jj = qq * 32 + (tid & 31);
       bool h = false;
-      if (jj < nb) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
+      if (jj < nb) h = !rec_misses_box(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, ww, wh);
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
     bool done;
@@ -442,13 +524,14 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
       const float4 a = sr[j].a;
       const float4 c4 = sr[j].c;
       const float4 b = sr[j].b;
-      const float dx = a.x - fx;
+      const float dx = a.x - fx, pmin = -0.5f * c4.y;
 #pragma unroll
       for (int k = 0; k < PPT; ++k) {
         if (dn[k]) continue;
         const float dy = a.y - (float)(py + k);
-        const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
-        if (power > 0.0f) continue;
+        float cu, cw;
+        const float power = gs_power(a, b.x, dx, dy, cu, cw);
+        if (power > 0.0f || power < pmin) continue;  // pmin: alpha < 1/255 below it (see pix_bwd_pair)
         const float alpha = fminf(kAlphaMax, b.y * __expf(power));
         if (alpha < kAlphaMin) continue;
         const float test_T = T[k] * (1.0f - alpha);
@@ -875,7 +958,8 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
     const float4 b = s_b[j];
     const float col[3] = {b.z, b.w, c4.x};
     const float dx = a.x - fx, dy = a.y - fy;
-    const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
+    float u, w;
+    const float power = gs_power(a, b.x, dx, dy, u, w);
     if (power > 0.0f) return false;
     const float G = __expf(power);
     const float araw = b.y * G;
@@ -986,47 +1070,59 @@ __global__ void __launch_bounds__(kThreads) k_bwd(const Rec* __restrict__ recs, 
   }
 }
 
-// Per-pixel replay state of the backward.
+// Per-pixel replay state of the backward.  The colour behind the current
+// pair enters the gradient only through its dot product with dL/dpixel, so the
+// replay carries that scalar (acc_dot) instead of the colour itself.
 struct PixBwd {
-  float T, T_final, bg_dot, last_alpha;
-  float dC[3], accum[3], last_col[3];
+  float T;          // transmittance in front of the pair being replayed
+  float nbg;        // -T_final (background . dL/dpixel)
+  float last_alpha, acc_dot, last_dot;
+  float dC[3];
   float fx, fy;
-  uint32_t last;
-  bool inside;
+  uint32_t last;    // contributors of the pixel; 0 outside the image
 };
 
 __device__ __forceinline__ void pix_bwd_init(PixBwd& s, uint32_t px, uint32_t py, uint32_t v, uint32_t W, uint32_t H,
                                              float3 bg, const float4* __restrict__ img,
                                              const uint32_t* __restrict__ ncontrib,
                                              const float4* __restrict__ dimg) {
-  s.inside = px < W && py < H;
   s.fx = (float)px;
   s.fy = (float)py;
-  s.T = s.T_final = 1.0f;
+  s.T = 1.0f;
   s.last = 0;
   s.dC[0] = s.dC[1] = s.dC[2] = 0.0f;
-  if (s.inside) {
+  if (px < W && py < H) {
     const size_t pix = ((size_t)v * H + py) * W + px;
     const float4 o = img[pix];
-    s.T = s.T_final = o.w;
+    s.T = o.w;
     s.last = ncontrib[pix];
     const float4 d = dimg[pix];
     s.dC[0] = d.x; s.dC[1] = d.y; s.dC[2] = d.z;
   }
-  s.bg_dot = bg.x * s.dC[0] + bg.y * s.dC[1] + bg.z * s.dC[2];
-  s.last_alpha = 0.0f;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) s.accum[c] = s.last_col[c] = 0.0f;
+  s.nbg = -s.T * (bg.x * s.dC[0] + bg.y * s.dC[1] + bg.z * s.dC[2]);
+  s.last_alpha = s.acc_dot = s.last_dot = 0.0f;
+}
+
+// Scale of gradient term k that pix_bwd_pair leaves out of its per-pixel sums
+// (applied once to the warp total): terms 0..4 are accumulated with their
+// common factor -1 and terms 2 and 4 with twice their value.
+__device__ __forceinline__ float bwd_term_scale(uint32_t k) {
+  return k < 5u ? ((k == 2u || k == 4u) ? -0.5f : -1.0f) : 1.0f;
 }
 
 // adds this pixel's gradient w.r.t. the pair (a, b, c4) at sorted offset cur
-// to gv[0..8]; returns whether the pair contributes here
+// to gv[0..8] (terms 0..4 without their bwd_term_scale); returns whether the
+// pair contributes here
 __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const float4& b, const float4& c4,
                                              uint32_t cur, float* gv) {
-  if (!(s.inside && cur < s.last)) return false;
+  if (cur >= s.last) return false;
   const float dx = a.x - s.fx, dy = a.y - s.fy;
-  const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
-  if (power > 0.0f) return false;
+  float u, w;
+  const float power = gs_power(a, b.x, dx, dy, u, w);
+  // power < -c4.y / 2 (outside the alpha >= 1/255 ellipse with its margin)
+  // implies alpha < 1/255, so skipping those pixels before the exponential
+  // leaves every decision of the alpha test below unchanged
+  if (power > 0.0f || power < -0.5f * c4.y) return false;
   const float G = __expf(power);
   const float araw = b.y * G;
   const float alpha = fminf(kAlphaMax, araw);
@@ -1035,27 +1131,23 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
   const float inv1ma = __fdividef(1.0f, 1.0f - alpha);
   s.T = s.T * inv1ma;
   const float wgt = alpha * s.T;
-  const float col[3] = {b.z, b.w, c4.x};
-  float dL_dalpha = 0.0f;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    s.accum[c] = s.last_alpha * s.last_col[c] + (1.0f - s.last_alpha) * s.accum[c];
-    s.last_col[c] = col[c];
-    dL_dalpha += (col[c] - s.accum[c]) * s.dC[c];
-    gv[6 + c] += wgt * s.dC[c];
-  }
-  dL_dalpha *= s.T;
+  // colour behind this pair, dotted with dL/dpixel: last_alpha * last + (1 - last_alpha) * acc
+  const float cdot = fmaf(c4.x, s.dC[2], fmaf(b.w, s.dC[1], b.z * s.dC[0]));
+  s.acc_dot = fmaf(s.last_alpha, s.last_dot - s.acc_dot, s.acc_dot);
+  s.last_dot = cdot;
   s.last_alpha = alpha;
-  dL_dalpha += (-s.T_final * inv1ma) * s.bg_dot;
+  const float dL_dalpha = fmaf(s.nbg, inv1ma, (cdot - s.acc_dot) * s.T);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) gv[6 + c] = fmaf(wgt, s.dC[c], gv[6 + c]);
   if (araw <= kAlphaMax) {
-    const float dL_dG = b.y * dL_dalpha;
-    const float gdx = G * dx, gdy = G * dy;
-    gv[0] += dL_dG * (-gdx * a.z - gdy * a.w);
-    gv[1] += dL_dG * (-gdy * b.x - gdx * a.w);
-    gv[2] += -0.5f * gdx * dx * dL_dG;
-    gv[3] += -gdx * dy * dL_dG;
-    gv[4] += -0.5f * gdy * dy * dL_dG;
-    gv[5] += G * dL_dalpha;
+    // dL/dG = opacity dL/dalpha; h = G dL/dG
+    const float h = araw * dL_dalpha, hx = h * dx, hy = h * dy;
+    gv[0] = fmaf(h, u, gv[0]);     // d/du:  -h u
+    gv[1] = fmaf(h, w, gv[1]);     // d/dv:  -h w
+    gv[2] = fmaf(hx, dx, gv[2]);   // d/d conic a: -h dx dx / 2
+    gv[3] = fmaf(hx, dy, gv[3]);   // d/d conic b: -h dx dy
+    gv[4] = fmaf(hy, dy, gv[4]);   // d/d conic c: -h dy dy / 2
+    gv[5] = fmaf(G, dL_dalpha, gv[5]);  // d/d opacity
   }
   return true;
 }
@@ -1078,14 +1170,15 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
   constexpr int NT = 256 / PPT, SB = NT * SPS;
   static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
   __shared__ __align__(16) Rec s_rec[2][SB];
-  __shared__ uint32_t s_g[2][SB];
-  __shared__ float s_acc[SB][10];
+  __shared__ uint32_t s_g[3][SB];
+  __shared__ float s_acc[2][SB][9];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_max;
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
-  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * (tid >> 5));
-  constexpr float wh = (float)(2 * PPT - 1);
+  using TM = TileMap16<PPT>;
+  const uint32_t px = tx * 16 + TM::x(tid), py = ty * 16 + TM::y(tid);
+  const float wx0 = (float)(tx * 16 + TM::wx(tid)), wy0 = (float)(ty * 16 + TM::wy(tid));
+  constexpr float ww = (float)(TM::kW - 1), wh = (float)(TM::kH - 1);
   const uint32_t key = v * num_tiles + ty * tiles_x + tx;
   const uint32_t start = rstart[key];
   PixBwd p[PPT];
@@ -1101,6 +1194,7 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     mbar_init(&s_bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  for (uint32_t r = tid; r < (uint32_t)(2 * SB * 9); r += NT) (&s_acc[0][0][0])[r] = 0.0f;
   __syncthreads();
   atomicMax(&s_max, mylast);
   __syncthreads();
@@ -1118,26 +1212,32 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     const uint32_t b0 = bstart_of(0);
     stage_batch(recs, vals, b0, start + maxlast - b0, s_rec[0], &s_bar[0], s_g[0]);
   }
+  // One CTA barrier per batch: batch bi accumulates into s_acc[bi & 1]; after
+  // the barrier each thread flushes and clears its rows of that buffer while
+  // others may already walk batch bi + 1 into the other one.  The barrier also
+  // orders the re-staging of s_rec[bi & 1] (issued at batch bi + 1, after the
+  // barrier of batch bi) after every read of it, and the record ids rotate
+  // through three buffers so that staging batch bi + 2 never overwrites the
+  // ids the flush of batch bi is still reading.
+  uint32_t gb = 0;  // bi % 3
   for (uint32_t bi = 0; bi < nbatch; ++bi) {
-    const uint32_t buf = bi & 1u;
+    const uint32_t buf = bi & 1u, gnext = gb == 2u ? 0u : gb + 1u;
     const uint32_t bend = start + maxlast - bi * SB, bstart = bstart_of(bi);
     const uint32_t nb = bend - bstart;
     if (bi + 1 < nbatch) {
       const uint32_t nbs = bstart_of(bi + 1);
-      stage_batch(recs, vals, nbs, bstart - nbs, s_rec[buf ^ 1u], &s_bar[buf ^ 1u], s_g[buf ^ 1u]);
+      stage_batch(recs, vals, nbs, bstart - nbs, s_rec[buf ^ 1u], &s_bar[buf ^ 1u], s_g[gnext]);
     }
-    for (uint32_t r = tid; r < (uint32_t)SB; r += NT)
-#pragma unroll
-      for (int k = 0; k < 10; ++k) s_acc[r][k] = 0.0f;
     if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
-    __syncthreads();  // s_acc cleared, staged indices visible
     const Rec* sr = s_rec[buf];
+    float(*acc)[9] = s_acc[buf];
     uint32_t hit[SB / 32];
 #pragma unroll
     for (int qq = 0; qq < SB / 32; ++qq) {
       const uint32_t jj = qq * 32 + lane;
       bool h = false;
-      if (jj < nb && bstart + jj - start < wlast) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
+      if (jj < nb && bstart + jj - start < wlast)
+        h = !rec_misses_box(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, ww, wh);
       hit[qq] = __ballot_sync(0xffffffffu, h);
     }
 #pragma unroll
@@ -1150,28 +1250,31 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       const float4 c4 = sr[j].c;
       const float4 b = sr[j].b;
       const uint32_t cur = bstart + (uint32_t)j - start;
-      float gv[16];
+      float gv[9];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+      for (int k = 0; k < 9; ++k) gv[k] = 0.0f;
       bool any = false;
 #pragma unroll
       for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, b, c4, cur, gv);
       if (__any_sync(0xffffffffu, any)) {
-        const float tot = warp_sum16(gv, lane);
-        const uint32_t k = lane >> 1;
-        if ((lane & 1) == 0 && k < 9) atomicAdd(&s_acc[j][k], tot);
+        const float tot = warp_sum9(gv, lane);
+        const uint32_t k = warp_sum9_index(lane);
+        if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot * bwd_term_scale(k));
       }
     }
     __syncthreads();
     for (uint32_t r = tid; r < nb; r += NT) {
-      float* dst = g2 + (size_t)s_g[buf][r] * kG2;
+      float* dst = g2 + (size_t)s_g[gb][r] * kG2;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
-        const float x = s_acc[r][k];
-        if (x != 0.0f) atomicAdd(dst + k, x);
+        const float x = acc[r][k];
+        if (x != 0.0f) {
+          atomicAdd(dst + k, x);
+          acc[r][k] = 0.0f;
+        }
       }
     }
-    __syncthreads();  // s_acc and this buffer are reused two batches on
+    gb = gnext;
   }
 }
 

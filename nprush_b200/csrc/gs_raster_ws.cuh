@@ -299,13 +299,14 @@ __global__ void __launch_bounds__(TS * TS / PPT + 32) k_fwd_ws(
           const float4 a = sr[j].a;
           const float4 c4 = sr[j].c;
           const float4 b = sr[j].b;
-          const float dx = a.x - fx;
+          const float dx = a.x - fx, pmin = -0.5f * c4.y;
 #pragma unroll
           for (int k = 0; k < PPT; ++k) {
             if (dn[k]) continue;
             const float dy = a.y - (float)(py + k);
-            const float power = -0.5f * (a.z * dx * dx + b.x * dy * dy) - a.w * dx * dy;
-            if (power > 0.0f) continue;
+            float cu, cw;
+            const float power = gs_power(a, b.x, dx, dy, cu, cw);
+            if (power > 0.0f || power < pmin) continue;  // alpha < 1/255 below pmin
             const float alpha = fminf(kAlphaMax, b.y * __expf(power));
             if (alpha < kAlphaMin) continue;
             const float test_T = T[k] * (1.0f - alpha);
@@ -480,16 +481,16 @@ __global__ void __launch_bounds__(TS * TS / PPT + 32) k_bwd_ws(
           const float4 c4 = sr[j].c;
           const float4 b = sr[j].b;
           const uint32_t cur = m.off + (uint32_t)j;
-          float gv[16];
+          float gv[9];
 #pragma unroll
-          for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+for (int k = 0; k < 9; ++k) gv[k] = 0.0f;
           bool any = false;
 #pragma unroll
           for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, b, c4, cur, gv);
           if (__any_sync(0xffffffffu, any)) {
-            const float tot = warp_sum16(gv, lane);
-            const uint32_t k = lane >> 1;
-            if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot);
+            const float tot = warp_sum9(gv, lane);
+            const uint32_t k = warp_sum9_index(lane);
+            if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot * bwd_term_scale(k));
           }
         }
     }
@@ -599,9 +600,10 @@ __global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 1) k_bwd3(
     stage(0);
     if (nbatch > 1) stage(1);
   }
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + PPT * (tid >> 4);
-  const float wx0 = (float)(tx * 16), wy0 = (float)(ty * 16 + 2 * PPT * warp);
-  constexpr float wh = (float)(2 * PPT - 1);
+  using TM = TileMap16<PPT>;
+  const uint32_t px = tx * 16 + TM::x(tid), py = ty * 16 + TM::y(tid);
+  const float wx0 = (float)(tx * 16 + TM::wx(tid)), wy0 = (float)(ty * 16 + TM::wy(tid));
+  constexpr float ww = (float)(TM::kW - 1), wh = (float)(TM::kH - 1);
   PixBwd p[PPT];
   uint32_t mylast = 0;
 #pragma unroll
@@ -627,7 +629,7 @@ __global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 1) k_bwd3(
       for (int qq = 0; qq < SB / 32; ++qq) {
         const uint32_t jj = qq * 32 + lane;
         bool h = false;
-        if (jj < nb && lo + jj < wlast) h = !rec_misses_strip(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, wh);
+        if (jj < nb && lo + jj < wlast) h = !rec_misses_box(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, ww, wh);
         hit[qq] = __ballot_sync(0xffffffffu, h);
       }
 #pragma unroll
@@ -640,16 +642,16 @@ __global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 1) k_bwd3(
           const float4 c4 = sr[j].c;
           const float4 bb = sr[j].b;
           const uint32_t cur = lo + (uint32_t)j;
-          float gv[16];
+          float gv[9];
 #pragma unroll
-          for (int k = 0; k < 16; ++k) gv[k] = 0.0f;
+for (int k = 0; k < 9; ++k) gv[k] = 0.0f;
           bool any = false;
 #pragma unroll
           for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, bb, c4, cur, gv);
           if (__any_sync(0xffffffffu, any)) {
-            const float tot = warp_sum16(gv, lane);
-            const uint32_t k = lane >> 1;
-            if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot);
+            const float tot = warp_sum9(gv, lane);
+            const uint32_t k = warp_sum9_index(lane);
+            if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot * bwd_term_scale(k));
           }
         }
     }

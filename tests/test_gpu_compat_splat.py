@@ -104,8 +104,13 @@ def test_tile_cap_1024(mgr_cls):
     tgt, depth = targets(32, 32, 6)
     ref = orc.splat_backward(s, vp, vpi, tgt, depth)
     assert ref["tile_count"].max() == 1024
-    g, img, _ = run_backward(mgr_cls, s, [vp], [vpi], [tgt], [depth])
+    g, img, m = run_backward(mgr_cls, s, [vp], [vpi], [tgt], [depth])
     np.testing.assert_allclose(img[0], ref["image"], atol=1e-5, rtol=0)
+    # pairs composited after the cap = the oracle's capped list lengths; the longest list reaches the cap
+    st = m.stats()
+    assert st["pairs_capped"] == int(ref["tile_count"].sum()), (st, int(ref["tile_count"].sum()))
+    assert st["max_tile_len"] >= 1024 and st["pairs_capped"] <= st["pairs"], st
+    m.close()
     # splats beyond the cap get no gradient on either side
     beyond = np.arange(n) >= 1100
     assert (g[beyond] == ref["grads_q"][beyond]).all()
