@@ -853,8 +853,7 @@ def run_bezier_reference(args):
 METRIC = "train steps/s (fwd+bwd+Adam, 200k splats, 800^2, 8 views)"
 FWD_FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
              "one CTA per (tile, view), longest first")
-BWD_FORMS = ("one CTA per (tile, view)", "persistent warp-specialised, longest-first queue",
-             "one CTA per (tile, view), longest first, no CTA barrier")
+BWD_FORMS = FWD_FORMS
 
 # ------------------------------------------------- path-traced target workload
 PT_W, PT_H, PT_OBJECTS, PT_DETAIL, PT_BATCH = 1024, 768, 16, 20, 8

@@ -318,11 +318,10 @@ int nps_gs_read_image(nps_gs* gs, float* rgba_host, float* dl_dimage_host);
  *     composite or differentiate, with no CTA-wide barrier in the loop:
  *     T = 8: (1 or 2, 64 or 128); T = 16: (1, 128), (2 or 4, 64 or 128);
  *     T = 32: (4, 64 or 128);
- *   form 2, one CTA per (tile, view) with the blocks taking the items
- *     longest first; its backward has no CTA-wide barrier in the loop (each
- *     warp waits for its own data; the last warp to finish a batch adds the
- *     batch's sums to the records and stages the batch after next), T = 16,
- *     the (ppt, stage) of form 0.
+ *   form 2, the kernels of form 0 with a 1D grid whose blocks take the
+ *     (view, tile) items longest first (the forward by list length, the
+ *     backward by its last contributor), so the longest tiles start first
+ *     and the grid's tail is short: T = 16, the (ppt, stage) of form 0.
  * nps_gs_set_raster selects one per pass for the current tile (a stage of 0
  * means the form's default: 256 / ppt for form 0, 128 for form 1);
  * nps_gs_set_variant selects form 0; nps_gs_set_tile changes the tile (and

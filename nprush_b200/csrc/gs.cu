@@ -91,13 +91,13 @@ __device__ __forceinline__ bool rec_misses_box(const float4& a, float cc, const 
 // Thread-to-pixel map of the 16 x 16 tile kernels (forms 0 and 2): thread tid
 // shades PPT vertically adjacent pixels from (x, y) of the tile, and its warp
 // covers a kW x kH strip at (wx, wy), the region its per-warp culling tests.
-// NPS_GS_STRIP_W 8 (default): 8 x 4·PPT strips, two side by side, closer to
-// square, so a small footprint meets fewer warps (backward -9%, forward -5%
-// at 200k Gaussians, 800 x 800, 8 views, against 16); 16: full-width
-// 16 x 2·PPT strips.
+// NPS_GS_STRIP_W 8 (default): the strips closest to square, 8 x 4 (PPT 1),
+// 8 x 8 (PPT 2) and 16 x 8 (PPT 4), so a small footprint meets fewer warps
+// (backward -9%, forward -5% at 200k Gaussians, 800 x 800, 8 views, PPT 2,
+// against 16 x 4); 16: full-width 16 x 2·PPT strips.
 template <int PPT>
 struct TileMap16 {
-  static constexpr int kW = NPS_GS_STRIP_W, kH = 32 * PPT / NPS_GS_STRIP_W;
+  static constexpr int kW = (NPS_GS_STRIP_W == 8 && PPT == 4) ? 16 : NPS_GS_STRIP_W, kH = 32 * PPT / kW;
   static constexpr int kWarpsX = 16 / kW;
   static_assert(kW == 16 || kW == 8, "strip width");
   __device__ static uint32_t wx(uint32_t tid) { return ((tid >> 5) % kWarpsX) * kW; }
@@ -1158,7 +1158,7 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
 // that meet its strip and that some of its pixels reached, then walks them in
 // reverse order.  Per-pair sums go to shared memory and then to the (view,
 // Gaussian) records with global atomics.  PPT is the autotuned variant.
-template <int PPT, int SPS>
+template <int PPT, int SPS, bool kOrd>
 __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                     const uint32_t* __restrict__ rstart,
                                                     const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
@@ -1166,7 +1166,8 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
                                                     const float4* __restrict__ img,
                                                     const uint32_t* __restrict__ ncontrib,
                                                     const float4* __restrict__ dimg, float* __restrict__ g2,
-                                                    uint32_t* __restrict__ err) {
+                                                    uint32_t* __restrict__ err, const uint32_t* __restrict__ order,
+                                                    const uint32_t* __restrict__ qctl) {
   constexpr int NT = 256 / PPT, SB = NT * SPS;
   static_assert(SB <= 256, "staging buffers beyond the static shared-memory budget");
   __shared__ __align__(16) Rec s_rec[2][SB];
@@ -1174,7 +1175,17 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
   __shared__ float s_acc[2][SB][9];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_max;
-  const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z, tid = threadIdx.x, lane = tid & 31;
+  uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z;
+  if constexpr (kOrd) {
+    // 1D grid over the items with contributors, longest first
+    if (blockIdx.x >= qctl[0]) return;
+    const uint32_t it = order[blockIdx.x];
+    v = it / num_tiles;
+    const uint32_t tile = it - v * num_tiles;
+    ty = tile / tiles_x;
+    tx = tile - ty * tiles_x;
+  }
+  const uint32_t tid = threadIdx.x, lane = tid & 31;
   using TM = TileMap16<PPT>;
   const uint32_t px = tx * 16 + TM::x(tid), py = ty * 16 + TM::y(tid);
   const float wx0 = (float)(tx * 16 + TM::wx(tid)), wy0 = (float)(ty * 16 + TM::wy(tid));
@@ -2261,7 +2272,7 @@ int nps_gs_set_views(nps_gs* o, const float* vp, const float* vp_inv, const uint
 // over a longest-first work queue (k_fwd_ws, k_bwd_ws), a 3-slot ring of
 // staged records, T = 8 (1 or 2 pixels per thread), 16 (1, 2, 4) or 32 (4);
 // form 2: one CTA per work item, blocks taking the items longest first
-// (k_fwd ordered, k_bwd3: no CTA-wide barrier in the backward's loop), T = 16.
+// (k_fwd and k_bwd2 ordered), T = 16.
 struct RasterVariant {
   int form, ppt, stage;
 };
@@ -2436,25 +2447,27 @@ static int launch_bwd_raster(nps_gs* o, int form, int ppt, int stage, const floa
     gs::k_order_items<true><<<1, 1024, 0, s>>>(nullptr, nullptr, o->tile_last.as<uint32_t>(), nitems,
                                                o->ws_order_b.as<uint32_t>(), q);
     NPS_CHECK_LAUNCH();
-#define NPS_BWD3(PPT, SB)                                                                                     \
-  gs::k_bwd3<PPT, SB><<<nitems, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart,                \
-                                                  o->tile_last.as<uint32_t>(), o->ws_order_b.as<uint32_t>(), q,   \
-                                                  W, H, tiles_x, num_tiles, bg, o->img.as<float4>(),              \
-                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err)
-    if (ppt == 1) NPS_BWD3(1, 256);
-    else if (ppt == 2 && stage == 256) NPS_BWD3(2, 256);
-    else if (ppt == 2) NPS_BWD3(2, 128);
-    else if (stage == 128) NPS_BWD3(4, 128);
-    else NPS_BWD3(4, 64);
-#undef NPS_BWD3
+#define NPS_BWD2O(PPT, SPS)                                                                                   \
+  gs::k_bwd2<PPT, SPS, true><<<nitems, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, \
+                                                        tiles_x, num_tiles, bg, o->img.as<float4>(),              \
+                                                        o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err, \
+                                                        o->ws_order_b.as<uint32_t>(), q)
+    const int sps2 = stage * ppt / 256;
+    if (ppt == 1) NPS_BWD2O(1, 1);
+    else if (ppt == 2 && sps2 == 2) NPS_BWD2O(2, 2);
+    else if (ppt == 2) NPS_BWD2O(2, 1);
+    else if (sps2 == 2) NPS_BWD2O(4, 2);
+    else NPS_BWD2O(4, 1);
+#undef NPS_BWD2O
     NPS_CHECK_LAUNCH();
     return NPS_OK;
   }
   const dim3 grid(tiles_x, tiles_y, nv);
 #define NPS_BWD(PPT, SPS)                                                                                     \
-  gs::k_bwd2<PPT, SPS><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H,      \
-                                                  tiles_x, num_tiles, bg, o->img.as<float4>(),                    \
-                                                  o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err)
+  gs::k_bwd2<PPT, SPS, false><<<grid, 256 / PPT, 0, s>>>(o->recs.as<gs::Rec>(), o->sorted_vals, rstart, rend, W, H, \
+                                                         tiles_x, num_tiles, bg, o->img.as<float4>(),             \
+                                                         o->ncontrib.as<uint32_t>(), dimg, o->g2.as<float>(), err, \
+                                                         nullptr, nullptr)
   const int sps = stage * ppt / 256;
   if (ppt == 1) NPS_BWD(1, 1);
   else if (ppt == 2 && sps == 2) NPS_BWD(2, 2);

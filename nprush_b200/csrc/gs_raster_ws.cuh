@@ -521,170 +521,3 @@ for (int k = 0; k < 9; ++k) gv[k] = 0.0f;
     }
   }
 }
-
-// ------------------------------------------------------------ backward, one CTA per tile, no CTA barrier
-// Form 2 of the backward: one CTA per (view, tile) work item, blocks taking
-// the items longest first (order[], from k_order_items<true>), 16 x 16 tiles
-// and 256 / PPT threads as the form-0 kernel, but no CTA-wide barrier after
-// set-up.  Batches of SB records from the back of the tile's contributors go
-// through two slots: each warp waits for its slot's bulk copies, gathers its
-// per-record sums in the slot's shared accumulator, and counts itself done
-// with the batch; the last warp to finish batch b adds the batch's sums to
-// the (view, Gaussian) records with global atomics, clears the accumulator
-// and stages batch b + 2 into the slot.  A batch's range is a function of
-// its index, so whichever warp stages it needs no shared producer state.
-template <int PPT, int SB>
-__global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 1) k_bwd3(
-    const Rec* __restrict__ recs, const uint32_t* __restrict__ vals, const uint32_t* __restrict__ rstart,
-    const uint32_t* __restrict__ tile_last, const uint32_t* __restrict__ order, const uint32_t* __restrict__ qctl,
-    uint32_t W, uint32_t H, uint32_t tiles_x, uint32_t num_tiles, float3 bg, const float4* __restrict__ img,
-    const uint32_t* __restrict__ ncontrib, const float4* __restrict__ dimg, float* __restrict__ g2,
-    uint32_t* __restrict__ err) {
-  constexpr int NT = 256 / PPT, NW = NT / 32;
-  static_assert(SB % 32 == 0 && SB <= 256, "batch size");
-  __shared__ __align__(16) Rec s_rec[2][SB];
-  __shared__ uint32_t s_g[2][SB];
-  __shared__ float s_acc[2][SB][9];
-  __shared__ __align__(8) uint64_t s_full[2];
-  __shared__ uint32_t s_cnt[2];
-  __shared__ volatile uint32_t s_abort;
-  __shared__ volatile uint32_t s_staged;  // batches staged so far
-  if (blockIdx.x >= qctl[0]) return;      // only tiles with contributors are queued
-  const uint32_t item = __ldg(order + blockIdx.x);
-  const uint32_t v = item / num_tiles, tile = item - v * num_tiles, ty = tile / tiles_x, tx = tile - ty * tiles_x;
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t start = __ldg(rstart + item), top = __ldg(tile_last + item);
-  const uint32_t nbatch = (top + SB - 1) / SB;
-  // batch i covers contributors [lo, hi) of the tile list, from the back
-  auto batch_range = [&](uint32_t i, uint32_t* lo, uint32_t* nb) {
-    const uint32_t hi = top - i * SB;
-    *lo = hi > (uint32_t)SB ? hi - SB : 0u;
-    *nb = hi - *lo;
-  };
-  // one warp stages batch i into slot i & 1 (its range, record ids, bulk copies)
-  auto stage = [&](uint32_t i) {
-    const uint32_t slot = i & 1u;
-    uint32_t lo, nb;
-    batch_range(i, &lo, &nb);
-    uint32_t g[SB / 32];
-#pragma unroll
-    for (int k = 0; k < SB / 32; ++k) {
-      const uint32_t r = lane + 32u * k;
-      g[k] = r < nb ? __ldg(vals + start + lo + r) : 0u;
-      if (r < nb) s_g[slot][r] = g[k];
-    }
-    __syncwarp();
-    if (lane == 0) {
-      s_staged = i + 1;
-      mbar_expect_tx(&s_full[slot], nb * (uint32_t)sizeof(Rec));
-    }
-    __syncwarp();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < SB / 32; ++k) {
-      const uint32_t r = lane + 32u * k;
-      if (r < nb) bulk_g2s(&s_rec[slot][r], recs + g[k], (uint32_t)sizeof(Rec), &s_full[slot]);
-    }
-  };
-  if (tid == 0) {
-    mbar_init(&s_full[0], 1);
-    mbar_init(&s_full[1], 1);
-    s_cnt[0] = s_cnt[1] = 0u;
-    s_abort = 0u;
-    s_staged = 0u;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  for (uint32_t r = tid; r < (uint32_t)(2 * SB * 9); r += NT) (&s_acc[0][0][0])[r] = 0.0f;
-  __syncthreads();
-  if (warp == 0) {
-    stage(0);
-    if (nbatch > 1) stage(1);
-  }
-  using TM = TileMap16<PPT>;
-  const uint32_t px = tx * 16 + TM::x(tid), py = ty * 16 + TM::y(tid);
-  const float wx0 = (float)(tx * 16 + TM::wx(tid)), wy0 = (float)(ty * 16 + TM::wy(tid));
-  constexpr float ww = (float)(TM::kW - 1), wh = (float)(TM::kH - 1);
-  PixBwd p[PPT];
-  uint32_t mylast = 0;
-#pragma unroll
-  for (int k = 0; k < PPT; ++k) {
-    pix_bwd_init(p[k], px, py + k, v, W, H, bg, img, ncontrib, dimg);
-    mylast = max(mylast, p[k].last);
-  }
-  const uint32_t wlast = __reduce_max_sync(0xffffffffu, mylast);
-  bool aborted = false;
-  for (uint32_t b = 0; b < nbatch; ++b) {
-    const uint32_t slot = b & 1u;
-    if (!ws_wait(&s_full[slot], (b >> 1) & 1u, &s_abort, err)) {
-      aborted = true;
-      break;
-    }
-    uint32_t lo, nb;
-    batch_range(b, &lo, &nb);
-    const Rec* sr = s_rec[slot];
-    float(*acc)[9] = s_acc[slot];
-    if (lo < wlast) {
-      uint32_t hit[SB / 32];
-#pragma unroll
-      for (int qq = 0; qq < SB / 32; ++qq) {
-        const uint32_t jj = qq * 32 + lane;
-        bool h = false;
-        if (jj < nb && lo + jj < wlast) h = !rec_misses_box(sr[jj].a, sr[jj].b.x, sr[jj].c, wx0, wy0, ww, wh);
-        hit[qq] = __ballot_sync(0xffffffffu, h);
-      }
-#pragma unroll
-      for (int qq = SB / 32 - 1; qq >= 0; --qq)
-        for (uint32_t mk = hit[qq]; mk != 0u;) {
-          const int bit = 31 - __clz(mk);
-          mk &= ~(1u << bit);
-          const int j = qq * 32 + bit;  // descending within the batch
-          const float4 a = sr[j].a;
-          const float4 c4 = sr[j].c;
-          const float4 bb = sr[j].b;
-          const uint32_t cur = lo + (uint32_t)j;
-          float gv[9];
-#pragma unroll
-for (int k = 0; k < 9; ++k) gv[k] = 0.0f;
-          bool any = false;
-#pragma unroll
-          for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, bb, c4, cur, gv);
-          if (__any_sync(0xffffffffu, any)) {
-            const float tot = warp_sum9(gv, lane);
-            const uint32_t k = warp_sum9_index(lane);
-            if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot * bwd_term_scale(k));
-          }
-        }
-    }
-    // count this warp done with the batch; the last one flushes and restages the slot
-    __syncwarp();
-    __threadfence_block();
-    uint32_t c = 0;
-    if (lane == 0) {
-      c = atomicAdd(&s_cnt[slot], 1u);
-      __threadfence_block();
-    }
-    c = __shfl_sync(0xffffffffu, c, 0);
-    __syncwarp();
-    if (c == (uint32_t)NW - 1) {
-      __threadfence_block();
-      for (uint32_t e = lane; e < nb * 9u; e += 32) {
-        const uint32_t j = e / 9u, k = e - 9u * j;
-        const float x = acc[j][k];
-        if (x != 0.0f) {
-          atomicAdd(g2 + (size_t)s_g[slot][j] * kG2 + k, x);
-          acc[j][k] = 0.0f;
-        }
-      }
-      if (lane == 0) s_cnt[slot] = 0u;
-      __syncwarp();
-      __threadfence_block();
-      if (b + 2 < nbatch && !s_abort) stage(b + 2);
-    }
-  }
-  if (aborted) {
-    // wait (bounded) for the copies of the batches staged last, so that none
-    // lands in shared memory after the CTA has exited
-    const uint32_t staged = s_staged;
-    for (uint32_t j = staged > 2 ? staged - 2 : 0u; j < staged; ++j) (void)mbar_wait(&s_full[j & 1u], (j >> 1) & 1u);
-  }
-}

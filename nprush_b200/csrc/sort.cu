@@ -15,6 +15,9 @@
 namespace nps {
 namespace {
 
+#ifndef NPS_SORT_MATCH
+#define NPS_SORT_MATCH 0
+#endif
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kItems = 12;
@@ -225,6 +228,9 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const K* __restric
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const uint32_t d = dg[j];
+#if NPS_SORT_MATCH
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+#else
       uint32_t peers = 0xffffffffu;
 #pragma unroll
       for (int b = 0; b < 9; ++b) {
@@ -232,6 +238,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const K* __restric
         const uint32_t bal = __ballot_sync(0xffffffffu, bit);
         peers &= bit ? bal : ~bal;
       }
+#endif
       const int leader = __ffs(peers) - 1;
       uint32_t old = 0;
       if (lane == leader && d < 256u) old = wh[wid][d];

@@ -149,6 +149,8 @@ def main(argv=None):
     ap.add_argument("--gaussians", type=int, default=200_000)
     ap.add_argument("--teacher", type=int, default=250_000)
     ap.add_argument("--res", type=int, default=800)
+    ap.add_argument("--width", type=int, default=None, help="image width (default: --res)")
+    ap.add_argument("--height", type=int, default=None, help="image height (default: --res)")
     ap.add_argument("--horizon", type=int, default=3)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--no-densify-early", action="store_true",
@@ -172,7 +174,7 @@ def main(argv=None):
 
     def scene(seed):
         # student and teacher seeds derived from the run seed
-        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, n_cams=a.cams,
+        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.width or a.res, a.height or a.res, n_cams=a.cams,
                                         sh_degree=a.sh_degree, capacity=4 * a.gaussians, student_seed=seed,
                                         teacher_seed=seed + 1000)
         if a.deterministic:
