@@ -85,6 +85,9 @@ __device__ __forceinline__ bool rec_misses_box(const float4& a, float cc, const 
   return fminf(fminf(q1, q2), fminf(q3, q4)) > c.y;
 }
 
+#ifndef NPS_GS_SOLO
+#define NPS_GS_SOLO 0
+#endif
 #ifndef NPS_GS_STRIP_W
 #define NPS_GS_STRIP_W 8
 #endif
@@ -1267,7 +1270,17 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       bool any = false;
 #pragma unroll
       for (int k = 0; k < PPT; ++k) any |= pix_bwd_pair(p[k], a, b, c4, cur, gv);
-      if (__any_sync(0xffffffffu, any)) {
+      const uint32_t cm = __ballot_sync(0xffffffffu, any);
+#if NPS_GS_SOLO
+      if (cm != 0u && (cm & (cm - 1u)) == 0u) {
+        // one contributing lane: its values are the warp totals
+        if (any) {
+#pragma unroll
+          for (int k = 0; k < 9; ++k) atomicAdd(&acc[j][k], gv[k] * bwd_term_scale((uint32_t)k));
+        }
+      } else
+#endif
+      if (cm != 0u) {
         const float tot = warp_sum9(gv, lane);
         const uint32_t k = warp_sum9_index(lane);
         if ((lane & 1) == 0 && k < 9) atomicAdd(&acc[j][k], tot * bwd_term_scale(k));
