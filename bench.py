@@ -376,9 +376,12 @@ def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush):
     r = fit(tr, vp, vpi, args.trained_steps, views=VIEWS, seed=0,
             adc=AdcSchedule(stop=min(15000, args.trained_steps)))
     sched = view_schedule(args.warmup + args.steps)
+    tr.set_timing(not args.no_stage_timing)
     for k in range(args.warmup):
         tr.set_views(vp[sched[k]], vpi[sched[k]], sched[k])
         tr.train_step()
+    torch.cuda.synchronize()
+    tr.stage_times(reset=True)
     times, pairs = [], []
     for k in range(args.steps):
         sel = sched[args.warmup + k]
@@ -391,10 +394,13 @@ def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush):
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
         pairs.append(tr.stats()["pairs"])
+    stages = tr.stage_times(reset=True)
+    tr.set_timing(False)
     psnr = float(np.mean(evaluate_psnr(tr, vp, vpi)))
     out = {"after_steps": args.trained_steps, "gaussians": tr.count, "pairs_per_step": int(np.mean(pairs)),
            "ms_per_step": float(np.mean(times)), "steps_per_s": 1000.0 / float(np.mean(times)),
-           "psnr_db": psnr, "fit_wall_s": r.wall_s, "fit_steps_per_s": args.trained_steps / r.wall_s}
+           "psnr_db": psnr, "fit_wall_s": r.wall_s, "fit_steps_per_s": args.trained_steps / r.wall_s,
+           "stages_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in stages.items() if v[1]}}
     tr.close()
     return out
 

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "binning.cuh"
+#include "bulk.cuh"
 #include "common.cuh"
 #include "context.h"
 
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splat
   f4[0] = make_float4(scx, scy, A, B);
   f4[1] = make_float4(C, s[13], s[14], s[7]);
   f4[2] = make_float4(s[4], s[5], s[6], depth);
-  f4[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  f4[3] = make_float4(0.5f * s[13], 0.0f, 0.0f, 0.0f);  // a / 2 for pow(r, a) = 2^((a / 2) log2 r^2)
   float4* b4 = reinterpret_cast<float4*>(bwd + (size_t)g * kBwd);
   b4[0] = make_float4(W, clip.x, clip.y, sx);
   b4[1] = make_float4(sy, sz, m0x, m0y);
@@ -206,35 +207,136 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splat
   rects[g] = rect;
 }
 
-__global__ void k_emit(const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                       const uint2* __restrict__ rects, uint32_t n, uint32_t nv, uint32_t tiles_x, uint32_t num_tiles,
-                       uint32_t cap, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+// ---- cap-aware binning
+// Only the first kCap entries of a tile list (in splat index order) are ever
+// composited, and at 200k splats most of a scene's (tile, splat) overlaps lie
+// beyond them.  The splats are cut into nb index blocks of bs splats:
+// k_bin_diff adds every splat's tile rectangle to a 2D difference grid of its
+// (view, block), k_bin_rows / k_bin_cols turn each grid into per-tile counts,
+// k_bin_cutoff finds for every (view, tile) the block in which its running
+// count reaches kCap (every later block lies beyond the cap) and the full list
+// length, and k_bin_pairs counts, then writes, only the pairs whose splat
+// block is at or before its tile's cutoff block.  Pairs are written in
+// (view, splat) order, so the stable sort by tile key still gives every tile
+// list in index order, and its first kCap entries are exactly those of the
+// full list.  Without a cutoff array (nb = 1) every overlapped tile is kept.
+__global__ void k_bin_diff(const uint2* __restrict__ rects, const uint32_t* __restrict__ counts, uint32_t n,
+                           uint32_t nv, uint32_t bs, uint32_t nb, uint32_t gx, uint32_t gy, int32_t* __restrict__ grid) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= nv * n) return;
-  const uint32_t c = counts[g];
-  if (c == 0) return;
+  if (g >= nv * n || counts[g] == 0) return;
   const uint32_t v = g / n, i = g - v * n;
-  uint32_t pos = offsets[g];
   const uint2 r = rects[g];
   const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
-  for (uint32_t ty = y0; ty < y1; ++ty)
-    for (uint32_t tx = x0; tx < x1; ++tx) {
-      if (pos < cap) {
-        keys[pos] = v * num_tiles + ty * tiles_x + tx;
-        vals[pos] = i;
-      }
-      ++pos;
-    }
+  int32_t* G = grid + ((size_t)v * nb + i / bs) * gx * gy;
+  atomicAdd(G + y0 * gx + x0, 1);
+  atomicAdd(G + y0 * gx + x1, -1);
+  atomicAdd(G + y1 * gx + x0, -1);
+  atomicAdd(G + y1 * gx + x1, 1);
 }
 
-// Statistics of the last backward's tile lists: out[0] += sum of
-// min(length, kCap) (pairs composited), out[1] = longest list.
-__global__ void k_tile_stats(const uint32_t* __restrict__ rstart, const uint32_t* __restrict__ rend, uint32_t m,
-                             unsigned long long* __restrict__ out) {
+// In-place inclusive prefix of every grid row (along x), one thread per row.
+__global__ void k_bin_rows(int32_t* __restrict__ grid, uint32_t rows, uint32_t gx) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  int32_t* p = grid + (size_t)r * gx;
+  int32_t acc = 0;
+  for (uint32_t x = 0; x < gx; ++x) p[x] = acc += p[x];
+}
+
+// In-place inclusive prefix of every grid column (along y), one thread per
+// (grid, column).
+__global__ void k_bin_cols(int32_t* __restrict__ grid, uint32_t grids, uint32_t gx, uint32_t gy) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= grids * gx) return;
+  const uint32_t gi = t / gx, x = t - gi * gx;
+  int32_t* p = grid + (size_t)gi * gx * gy + x;
+  int32_t acc = 0;
+  for (uint32_t y = 0; y < gy; ++y) p[(size_t)y * gx] = acc += p[(size_t)y * gx];
+}
+
+// Per (view, tile): the last splat block its first kCap entries need, and the
+// full list length.  Also sums the lengths (pairs overlapped) into *total.
+__global__ void k_bin_cutoff(const int32_t* __restrict__ grid, uint32_t nv, uint32_t nb, uint32_t tiles_x,
+                             uint32_t num_tiles, uint32_t gx, uint32_t gy, uint32_t* __restrict__ cutoff,
+                             uint32_t* __restrict__ tile_len, unsigned long long* __restrict__ total) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t len = 0;
+  if (t < nv * num_tiles) {
+    const uint32_t v = t / num_tiles, tile = t - v * num_tiles;
+    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    const int32_t* G = grid + (size_t)v * nb * gx * gy + (size_t)ty * gx + tx;
+    uint32_t cut = nb - 1;
+    bool found = false;
+    for (uint32_t b = 0; b < nb; ++b) {
+      len += (uint32_t)G[(size_t)b * gx * gy];
+      if (!found && len >= kCap) {
+        cut = b;
+        found = true;
+      }
+    }
+    cutoff[t] = cut;
+    tile_len[t] = len;
+  }
+  unsigned long long s = len;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0 && s != 0) atomicAdd(total, s);
+}
+
+// One warp per (view, splat) item, its lanes over the item's tile rectangle:
+// kWrite = false counts the kept pairs into out_counts, kWrite = true writes
+// them at offsets[item] onwards (positions beyond cap are dropped).
+template <bool kWrite>
+__global__ void __launch_bounds__(256) k_bin_pairs(const uint2* __restrict__ rects, const uint32_t* __restrict__ counts,
+                                                   const uint32_t* __restrict__ cutoff, uint32_t n, uint32_t nv,
+                                                   uint32_t bs, uint32_t tiles_x, uint32_t num_tiles,
+                                                   uint32_t* __restrict__ out_counts,
+                                                   const uint32_t* __restrict__ offsets, uint32_t cap,
+                                                   uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nv * n; g += nw) {
+    const uint32_t c = counts[g];
+    if (c == 0) {
+      if (!kWrite && lane == 0) out_counts[g] = 0;
+      continue;
+    }
+    const uint32_t v = g / n, i = g - v * n, b = i / bs;
+    const uint2 r = rects[g];
+    const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
+    const uint32_t w = x1 - x0;
+    const uint32_t* cut = cutoff ? cutoff + (size_t)v * num_tiles : nullptr;
+    uint32_t pos = kWrite ? offsets[g] : 0u;
+    for (uint32_t base = 0; base < c; base += 32) {
+      const uint32_t k = base + lane;
+      uint32_t tile = 0;
+      bool keep = false;
+      if (k < c) {
+        const uint32_t ry = k / w;
+        tile = (y0 + ry) * tiles_x + x0 + (k - ry * w);
+        keep = !cut || cut[tile] >= b;
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, keep);
+      if (kWrite && keep) {
+        const uint32_t p = pos + __popc(m & ((1u << lane) - 1u));
+        if (p < cap) {
+          keys[p] = v * num_tiles + tile;
+          vals[p] = i;
+        }
+      }
+      pos += __popc(m);
+    }
+    if (!kWrite && lane == 0) out_counts[g] = pos;
+  }
+}
+
+// Statistics of the last backward's tile lists from their full lengths:
+// out[0] += sum of min(length, kCap) (pairs composited), out[1] = longest.
+__global__ void k_tile_stats(const uint32_t* __restrict__ tile_len, uint32_t m, unsigned long long* __restrict__ out) {
   unsigned long long sum = 0;
   uint32_t mx = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const uint32_t len = rend[i] - rstart[i];
+    const uint32_t len = tile_len[i];
     sum += min(len, kCap);
     mx = max(mx, len);
   }
@@ -247,6 +349,13 @@ __global__ void k_tile_stats(const uint32_t* __restrict__ rstart, const uint32_t
     atomicAdd(out, sum);
     atomicMax(out + 1, (unsigned long long)mx);
   }
+}
+
+// Full list lengths when every pair was emitted (no cutoff): rend - rstart.
+__global__ void k_range_len(const uint32_t* __restrict__ rstart, const uint32_t* __restrict__ rend, uint32_t m,
+                            uint32_t* __restrict__ tile_len) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    tile_len[i] = rend[i] - rstart[i];
 }
 
 // Tile list bounds in the sorted key array.
@@ -271,77 +380,198 @@ struct RasterArgs {
   const float* tgt_depth;
   int32_t* grads;
   float* out_rgbd;
+  uint32_t* err;  // bounded waits that gave up (the output of such a tile is not written)
   uint32_t n, w, h, tiles_x, num_tiles;
 };
 
-constexpr size_t kRasterSmem = sizeof(uint32_t) * kChunk + sizeof(float) * kChunk * (kFwd + kBwd) +
-                               sizeof(float) * 3 * kChunk * kThreads + sizeof(int32_t) * kChunk * 16;
+constexpr uint32_t kNumChunks = kCap / kChunk;
+constexpr uint32_t kFwdBytes = sizeof(float) * kFwd, kBwdBytes = sizeof(float) * kBwd;
 
-__device__ __forceinline__ float splat_alpha(const float* f, float px, float py) {
-  const float dx = px - f[0], dy = py - f[1];
-  const float spx = f[2] * dx + f[3] * dy;
-  const float spy = f[3] * dx + f[4] * dy;
-  const float r2 = dx * spx + dy * spy;
-  const float r = sqrtf(fmaxf(r2, 0.0001f));
-  const float power = -f[6] * powf(r, f[5]);
-  return clampf(power > -15.0f ? expf(power) * f[7] : 0.0f, 0.0f, 0.999f);
+// Shared memory of one k_raster CTA (dynamic, ~82 KB: two CTAs per SM).
+struct __align__(16) RasterSmem {
+  float fwd[2][kChunk][kFwd];          // staged forward records (double-buffered)
+  float bwd[2][kChunk][kBwd];          // staged backward records
+  float ckpt[kNumChunks][kThreads];    // T of every pixel at the start of each chunk
+  float tprev[kChunk][kThreads];       // T before each pair of the chunk being differentiated
+  int32_t gacc[2][kChunk][16];         // per-chunk CTA sums of the i32 gradient terms
+  uint32_t ids[3][kChunk];             // splat index of each staged record
+  uint64_t bar[2];                     // one mbarrier per record buffer
+  float vpm[16];
+  int abort;
+};
+
+// Approximate base-2 logarithm and exponential on the special-function unit.
+// WGSL defines pow(x, y)'s accuracy as that of exp2(y * log2(x)), and exp's
+// and log's by a few ULP: the reference's shaders are not bit-defined here.
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kHalfLn2 = 0.34657359027997264f;
+
+// Per-pixel part of eval_splat (splat_backward.wgsl:127-132) for forward
+// record f at pixel (ppx, ppy): r = sqrt(max(r2, 1e-4)), pow(r, a) evaluated
+// as 2^((a / 2) log2 max(r2, 1e-4)) (f[12] = a / 2), exp(x) as 2^(x log2 e).
+// Every caller evaluates the same instruction sequence, so the forward, its
+// replay and the backward see bit-identical alphas.
+struct PixEval {
+  float spx, spy, r2c, lg, rpa, power, a_un, al;
+  bool above;
+};
+__device__ __forceinline__ PixEval eval_px(const float* f, float ppx, float ppy) {
+  PixEval e;
+  const float dx = ppx - f[0], dy = ppy - f[1];
+  e.spx = fmaf(f[2], dx, f[3] * dy);
+  e.spy = fmaf(f[3], dx, f[4] * dy);
+  e.r2c = fmaxf(fmaf(dx, e.spx, dy * e.spy), 0.0001f);
+  e.lg = lg2_approx(e.r2c);
+  e.rpa = ex2_approx(f[12] * e.lg);
+  e.power = -f[6] * e.rpa;
+  e.above = e.power > -15.0f;
+  e.a_un = e.above ? ex2_approx(e.power * kLog2e) : 0.0f;
+  e.al = clampf(e.above ? e.a_un * f[7] : 0.0f, 0.0f, 0.999f);
+  return e;
 }
 
-__global__ void __launch_bounds__(kThreads) k_raster(RasterArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  uint32_t* ids = reinterpret_cast<uint32_t*>(smem);
-  float* sf = reinterpret_cast<float*>(smem + sizeof(uint32_t) * kChunk);  // [kChunk][kFwd]
-  float* sb = sf + kChunk * kFwd;                                          // [kChunk][kBwd]
-  float* ckpt = sb + kChunk * kBwd;                                        // [kChunk][kThreads]
-  float* sA = ckpt + kChunk * kThreads;                                    // [kChunk][kThreads]
-  float* sT = sA + kChunk * kThreads;                                      // [kChunk][kThreads]
-  int32_t* gacc = reinterpret_cast<int32_t*>(sT + kChunk * kThreads);      // [kChunk][16]
-  __shared__ float vpm[16];
+// The part of one (pixel, splat) backward term (splat_backward.wgsl:259-330)
+// that every valid pair evaluates: the carried dL/dT sums (updated in place),
+// dL/dalpha, dL/dpower and the shape gradients with their regularisers.
+struct PairCommon {
+  float da, d_power, d_shape_a, d_shape_b;
+};
+__device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval& e, float T_prev, float dCr,
+                                                  float dCg, float dCb, float dD, float& dT_C, float& dT_D) {
+  const float cr = f[8], cg = f[9], cb = f[10], opacity = f[7], depth = f[11];
+  const float shape_a = f[5], shape_b = f[6], al = e.al;
+  const float tcr = T_prev * cr, tcg = T_prev * cg, tcb = T_prev * cb;
+  const float da_C = dT_C * (-T_prev) + (dCr * tcr + dCg * tcg + dCb * tcb);
+  const float da_D = dT_D * (-T_prev) + dD * T_prev * depth;
+  PairCommon p;
+  p.da = da_C + da_D;
+  const float acr = al * cr, acg = al * cg, acb = al * cb;
+  dT_C = dT_C * (1.0f - al) + (dCr * acr + dCg * acg + dCb * acb);
+  dT_D = dT_D * (1.0f - al) + dD * al * depth;
+  p.d_power = e.above ? p.da * opacity * e.a_un : 0.0f;
+  const float logr = e.lg * kHalfLn2;
+  p.d_shape_a = e.above ? p.d_power * (-shape_b * e.rpa * logr) : 0.0f;
+  p.d_shape_b = e.above ? p.d_power * (-e.rpa) : 0.0f;
+  p.d_shape_a += 0.005f * 2.0f * (shape_a - 6.0f);
+  p.d_shape_b += 0.005f * 2.0f * (shape_b - 0.3f);
+  return p;
+}
+
+// One CTA per (tile, view), one pixel per thread, each warp an 8 x 4 strip.
+// Records are staged 32 at a time by warp 0 with bulk copies completing on
+// an mbarrier, double-buffered (the next chunk lands while this one is
+// composited); the forward stores T at every chunk start, and the backward
+// walks the chunks in reverse, replaying each from its checkpoint.
+//
+// Exact skips (results identical to evaluating every pair):
+//  * a warp whose 32 pixels all reached T == 0 stops compositing: a pair
+//    then adds T * alpha * c = 0 and leaves T at 0;
+//  * a chunk that starts at T == 0 for the whole warp is not replayed;
+//  * a pair whose valid pixels (alpha >= 0.001) all have T_prev == 0 adds
+//    only its shape regularisers: with T_prev == 0 every other term is a
+//    product with a zero factor, which is 0 or NaN, and i32() maps both to 0;
+//    so only dL/dT, d_shape_a and d_shape_b are evaluated and summed.
+__global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RasterSmem& S = *reinterpret_cast<RasterSmem*>(smem_raw);
+  constexpr unsigned kFull = 0xffffffffu;
 
   const uint32_t tx = blockIdx.x, ty = blockIdx.y, v = blockIdx.z;
-  const uint32_t tid = threadIdx.x, lane = tid & 31;
-  const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t px = tx * 16 + 8 * (warp & 1u) + (lane & 7u), py = ty * 16 + 4 * (warp >> 1) + (lane >> 3);
   const bool inside = px < a.w && py < a.h;
   const float aspect = (float)a.w / (float)a.h;
   const float ppx = pixel_px(px, a.w, aspect), ppy = pixel_py(py, a.h);
-  if (tid < 16) vpm[tid] = a.views[32 * (size_t)v + tid];
+  if (tid < 16) S.vpm[tid] = a.views[32 * (size_t)v + tid];
   const uint32_t key = v * a.num_tiles + ty * a.tiles_x + tx;
   const uint32_t start = a.rstart[key];
   const uint32_t len = min(a.rend[key] - start, kCap);
   const uint32_t nch = (len + kChunk - 1) / kChunk;
   const float* fwd_v = a.fwd + (size_t)v * a.n * kFwd;
   const float* bwd_v = a.bwd + (size_t)v * a.n * kBwd;
+  for (uint32_t e = tid; e < 2 * kChunk * 16; e += kThreads) (&S.gacc[0][0][0])[e] = 0;
+  if (tid == 0) {
+    bulk::mbar_init(&S.bar[0], 1);
+    bulk::mbar_init(&S.bar[1], 1);
+    S.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
 
-  float T = 1.0f, Cr = 0.0f, Cg = 0.0f, Cb = 0.0f, D = 0.0f;
-  for (uint32_t c = 0; c < nch; ++c) {
+  // Batch q (warp 0 stages it into record buffer q & 1, ids q % 3): for
+  // q < nch the forward records of chunk q, else both records of chunk
+  // 2 nch - 1 - q (the backward's order).
+  auto stage = [&](uint32_t q) {
+    const bool both = q >= nch;
+    const uint32_t c = both ? 2 * nch - 1 - q : q;
     const uint32_t cnt = min((uint32_t)kChunk, len - c * kChunk);
-    __syncthreads();
-    if (tid < cnt) ids[tid] = a.vals[start + c * kChunk + tid];
-    __syncthreads();
-    if (tid < cnt * 4) {
-      const uint32_t k = tid >> 2, q = tid & 3;
-      reinterpret_cast<float4*>(sf)[k * 4 + q] =
-          reinterpret_cast<const float4*>(fwd_v + (size_t)ids[k] * kFwd)[q];
+    const uint32_t b = q & 1u;
+    if (lane == 0) bulk::mbar_expect_tx(&S.bar[b], cnt * (both ? kFwdBytes + kBwdBytes : kFwdBytes));
+    if (lane < cnt) {
+      bulk::fence_proxy_async();  // the buffer was last read through the generic proxy
+      const uint32_t id = a.vals[start + c * kChunk + lane];
+      S.ids[q % 3][lane] = id;
+      bulk::bulk_g2s(&S.fwd[b][lane][0], fwd_v + (size_t)id * kFwd, kFwdBytes, &S.bar[b]);
+      if (both) bulk::bulk_g2s(&S.bwd[b][lane][0], bwd_v + (size_t)id * kBwd, kBwdBytes, &S.bar[b]);
     }
-    ckpt[c * kThreads + tid] = T;
-    __syncthreads();
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const float* f = sf + k * kFwd;
-      const float al = splat_alpha(f, ppx, ppy);
-      Cr += T * al * f[8];
-      Cg += T * al * f[9];
-      Cb += T * al * f[10];
-      D += T * al * f[11];
-      T = T * (1.0f - al);
+  };
+  auto wait_batch = [&](uint32_t q) {
+    if (!bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u) && lane == 0) {
+      atomicAdd(a.err, 1u);
+      S.abort = 1;
+    }
+  };
+  uint32_t issued = 0;  // batches staged so far (CTA-uniform)
+  if (nch > 0) {
+    if (warp == 0) stage(0);
+    issued = 1;
+  }
+
+  // ---- forward: front-to-back composite (splat_backward.wgsl:216-248)
+  float T = 1.0f, Cr = 0.0f, Cg = 0.0f, Cb = 0.0f, D = 0.0f;
+  bool wdone = false;
+  uint32_t c = 0;
+  for (; c < nch; ++c) {
+    __syncthreads();  // every warp is done with batch c - 1: its buffers may be refilled
+    if (S.abort) break;
+    if (issued < 2 * nch) {
+      if (warp == 0) stage(issued);
+      ++issued;
+    }
+    wait_batch(c);
+    S.ckpt[c][tid] = T;
+    if (!wdone) {
+      const uint32_t cnt = min((uint32_t)kChunk, len - c * kChunk);
+      const uint32_t b = c & 1u;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const float* f = S.fwd[b][k];
+        const float al = eval_px(f, ppx, ppy).al;
+        Cr += T * al * f[8];
+        Cg += T * al * f[9];
+        Cb += T * al * f[10];
+        D += T * al * f[11];
+        T = T * (1.0f - al);
+      }
+      wdone = __all_sync(kFull, T == 0.0f);
     }
   }
   const float bg = 0.05f;
   Cr += T * bg; Cg += T * bg; Cb += T * bg;
   D += T * 1.0f;
   const size_t pix = ((size_t)v * a.h + (inside ? py : 0)) * a.w + (inside ? px : 0);
-  if (inside && a.out_rgbd) reinterpret_cast<float4*>(a.out_rgbd)[pix] = make_float4(Cr, Cg, Cb, D);
+  if (inside && a.out_rgbd && !S.abort) reinterpret_cast<float4*>(a.out_rgbd)[pix] = make_float4(Cr, Cg, Cb, D);
   // loss, splat_backward.wgsl:250-257
-  float4 tc = inside ? reinterpret_cast<const float4*>(a.tgt_rgba)[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 tc = inside ? reinterpret_cast<const float4*>(a.tgt_rgba)[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
   const float td = inside ? a.tgt_depth[pix] : 1.0f;
   const float dCr = 2.0f * (Cr - tc.x), dCg = 2.0f * (Cg - tc.y), dCb = 2.0f * (Cb - tc.z);
   const bool fg = td < 0.99f;
@@ -359,80 +589,87 @@ __global__ void __launch_bounds__(kThreads) k_raster(RasterArgs a) {
   }
   const float DEPTH_NEAR = 0.1f;
 
-  for (int c = (int)nch - 1; c >= 0; --c) {
-    const uint32_t cnt = min((uint32_t)kChunk, len - (uint32_t)c * kChunk);
-    __syncthreads();
-    if (tid < cnt) ids[tid] = a.vals[start + c * kChunk + tid];
-    gacc[tid] = 0;
-    gacc[tid + kThreads] = 0;
-    __syncthreads();
-    if (tid < cnt * 4) {
-      const uint32_t k = tid >> 2, q = tid & 3;
-      reinterpret_cast<float4*>(sf)[k * 4 + q] =
-          reinterpret_cast<const float4*>(fwd_v + (size_t)ids[k] * kFwd)[q];
+  // ---- backward: reverse order (splat_backward.wgsl:259-456)
+  auto flush = [&](uint32_t q) {  // batch q's CTA sums -> one global atomic per (splat, value)
+    const uint32_t cc = 2 * nch - 1 - q;
+    const uint32_t cnt = min((uint32_t)kChunk, len - cc * kChunk);
+    int32_t* g = &S.gacc[q & 1u][0][0];
+    for (uint32_t e = tid; e < cnt * 16; e += kThreads) {
+      const int32_t val = g[e];
+      if (val != 0) {
+        atomicAdd(&a.grads[16 * (size_t)S.ids[q % 3][e >> 4] + (e & 15)], val);
+        g[e] = 0;
+      }
     }
-    for (uint32_t e = tid; e < cnt * 8; e += kThreads) {
-      const uint32_t k = e >> 3, q = e & 7;
-      reinterpret_cast<float4*>(sb)[k * 8 + q] = reinterpret_cast<const float4*>(bwd_v + (size_t)ids[k] * kBwd)[q];
+  };
+  uint32_t j = 0;
+  for (; c == nch && j < nch; ++j) {
+    const uint32_t q = nch + j, cc = nch - 1 - j, b = q & 1u;
+    __syncthreads();  // batch q - 1 is done: its sums are complete and its buffers free
+    if (S.abort) break;
+    if (j > 0) flush(q - 1);
+    if (issued < 2 * nch) {
+      if (warp == 0) stage(issued);
+      ++issued;
     }
-    __syncthreads();
-    // replay the chunk forward from its checkpoint: bit-identical alphas / Ts
-    float Tc = ckpt[c * kThreads + tid];
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const float al = splat_alpha(sf + k * kFwd, ppx, ppy);
-      sA[k * kThreads + tid] = al;
-      sT[k * kThreads + tid] = Tc;
-      Tc = Tc * (1.0f - al);
+    wait_batch(q);
+    const uint32_t cnt = min((uint32_t)kChunk, len - cc * kChunk);
+    // replay the chunk forward from its checkpoint: bit-identical Ts
+    const float T0 = S.ckpt[cc][tid];
+    const bool zero_chunk = __all_sync(kFull, T0 == 0.0f);
+    if (!zero_chunk) {
+      float Tc = T0;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        S.tprev[k][tid] = Tc;
+        Tc = Tc * (1.0f - eval_px(S.fwd[b][k], ppx, ppy).al);
+      }
     }
+    int32_t* gacc = &S.gacc[b][0][0];
     for (int k = (int)cnt - 1; k >= 0; --k) {
-      const float al = sA[k * kThreads + tid];
-      const bool valid = inside && !(al < 0.001f);
-      if (!__any_sync(0xffffffffu, valid)) continue;
-      int32_t q[16];
+      const float* f = S.fwd[b][k];
+      const PixEval e = eval_px(f, ppx, ppy);
+      const bool valid = inside && !(e.al < 0.001f);
+      if (!__any_sync(kFull, valid)) continue;
+      const float T_prev = zero_chunk ? 0.0f : S.tprev[k][tid];
+      if (!__any_sync(kFull, valid && T_prev != 0.0f)) {
+        // only the shape regularisers and the carried dL/dT sums (see above)
+        int32_t q13 = 0, q14 = 0;
+        if (valid) {
+          const PairCommon p = pair_common(f, e, T_prev, dCr, dCg, dCb, dD, dT_C, dT_D);
+          q13 = to_i32(p.d_shape_a * kFpPos);
+          q14 = to_i32(p.d_shape_b * kFpPos);
+        }
+        const int32_t r13 = __reduce_add_sync(kFull, q13), r14 = __reduce_add_sync(kFull, q14);
+        if (lane == 0) {
+          if (r13 != 0) atomicAdd(&gacc[k * 16 + 13], r13);
+          if (r14 != 0) atomicAdd(&gacc[k * 16 + 14], r14);
+        }
+        continue;
+      }
+      int32_t qv[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) q[j] = 0;
+      for (int jj = 0; jj < 16; ++jj) qv[jj] = 0;
       if (valid) {
-        const float* f = sf + k * kFwd;
-        const float* b = sb + k * kBwd;
-        const float T_prev = sT[k * kThreads + tid];
-        const float cr = f[8], cg = f[9], cb = f[10], opacity = f[7], depth = f[11];
+        const float* bw = S.bwd[b][k];
+        const float al = e.al;
         const float shape_a = f[5], shape_b = f[6];
-        const float Wc = b[0], clip_x = b[1], clip_y = b[2], sx = b[3], sy = b[4], sz = b[5];
-        const float m0x = b[6], m0y = b[7], m1x = b[8], m1y = b[9], m2x = b[10], m2y = b[11];
-        const float axx = b[12], axy = b[13], ayx = b[14], ayy = b[15], azx = b[16], azy = b[17];
-        const float pos0 = b[18], pos1 = b[19], pos2 = b[20];
-        const float qw = b[21], qx = b[22], qy = b[23], qz = b[24];
-        // eval_splat per-pixel part
-        const float ddx0 = ppx - f[0], ddy0 = ppy - f[1];
-        const float spx = f[2] * ddx0 + f[3] * ddy0;
-        const float spy = f[3] * ddx0 + f[4] * ddy0;
-        const float r2 = ddx0 * spx + ddy0 * spy;
-        const float r = sqrtf(fmaxf(r2, 0.0001f));
+        const float Wc = bw[0], clip_x = bw[1], clip_y = bw[2], sx = bw[3], sy = bw[4], sz = bw[5];
+        const float m0x = bw[6], m0y = bw[7], m1x = bw[8], m1y = bw[9], m2x = bw[10], m2y = bw[11];
+        const float axx = bw[12], axy = bw[13], ayx = bw[14], ayy = bw[15], azx = bw[16], azy = bw[17];
+        const float pos0 = bw[18], pos1 = bw[19], pos2 = bw[20];
+        const float qw = bw[21], qx = bw[22], qy = bw[23], qz = bw[24];
         const float TA = T_prev * al;
         const float dColr = dCr * TA, dColg = dCg * TA, dColb = dCb * TA;
-        const float tcr = T_prev * cr, tcg = T_prev * cg, tcb = T_prev * cb;
-        const float da_C = dT_C * (-T_prev) + (dCr * tcr + dCg * tcg + dCb * tcb);
-        const float da_D = dT_D * (-T_prev) + dD * T_prev * depth;
-        const float da = da_C + da_D;
-        const float acr = al * cr, acg = al * cg, acb = al * cb;
-        dT_C = dT_C * (1.0f - al) + (dCr * acr + dCg * acg + dCb * acb);
-        dT_D = dT_D * (1.0f - al) + dD * al * depth;
         const float d_depth = dD * T_prev * al;
-        const float power = -shape_b * powf(r, shape_a);
-        const bool above = power > -15.0f;
-        const float a_un = above ? expf(power) : 0.0f;
-        const float d_opacity = above ? da * a_un : 0.0f;
-        const float d_power = above ? da * opacity * a_un : 0.0f;
-        const float r_pow_a = powf(r, shape_a);
-        const float r_pow_a_m2 = powf(r, shape_a - 2.0f);
-        float d_shape_a = above ? d_power * (-shape_b * r_pow_a * logf(r)) : 0.0f;
-        float d_shape_b = above ? d_power * (-r_pow_a) : 0.0f;
-        const float kk = d_power * (-shape_b * shape_a * r_pow_a_m2);
-        const float ddx = above ? kk * spx : 0.0f, ddy = above ? kk * spy : 0.0f;
+        const PairCommon p = pair_common(f, e, T_prev, dCr, dCg, dCb, dD, dT_C, dT_D);
+        const float d_opacity = e.above ? p.da * e.a_un : 0.0f;
+        const float r_pow_a_m2 = __fdividef(e.rpa, e.r2c);  // r^(a - 2) = r^a / r^2
+        const float kk = p.d_power * (-shape_b * shape_a * r_pow_a_m2);
+        const float ddx = e.above ? kk * e.spx : 0.0f, ddy = e.above ? kk * e.spy : 0.0f;
         const float dsx_ = -ddx, dsy_ = -ddy;
-        const float sp0 = spx * m0x + spy * m0y;
-        const float sp1 = spx * m1x + spy * m1y;
-        const float sp2 = spx * m2x + spy * m2y;
+        const float sp0 = e.spx * m0x + e.spy * m0y;
+        const float sp1 = e.spx * m1x + e.spy * m1y;
+        const float sp2 = e.spx * m2x + e.spy * m2y;
         const float dm0x = -sp0 * ddx, dm0y = -sp0 * ddy;
         const float dm1x = -sp1 * ddx, dm1y = -sp1 * ddy;
         const float dm2x = -sp2 * ddx, dm2y = -sp2 * ddy;
@@ -445,7 +682,7 @@ __global__ void __launch_bounds__(kThreads) k_raster(RasterArgs a) {
         float dpos[3], daw[3], dbw[3], dcw[3];
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-          const float vp0 = vpm[ax * 4 + 0], vp1 = vpm[ax * 4 + 1], vp3 = vpm[ax * 4 + 3];
+          const float vp0 = S.vpm[ax * 4 + 0], vp1 = S.vpm[ax * 4 + 1], vp3 = S.vpm[ax * 4 + 3];
           const float ds_dx = aspect * (vp0 * Wc - clip_x * vp3) / w2;
           const float ds_dy = (vp1 * Wc - clip_y * vp3) / w2;
           dpos[ax] = dsx_ * ds_dx + dsy_ * ds_dy;
@@ -472,37 +709,40 @@ __global__ void __launch_bounds__(kThreads) k_raster(RasterArgs a) {
         const float d_qz = (-daw[0] * 4.0f * qz + daw[1] * 2.0f * qw + daw[2] * 2.0f * qx) +
                            (-dbw[0] * 2.0f * qw - dbw[1] * 4.0f * qz + dbw[2] * 2.0f * qy) +
                            (dcw[0] * 2.0f * qx + dcw[1] * 2.0f * qy);
-        d_shape_a += 0.005f * 2.0f * (shape_a - 6.0f);
-        d_shape_b += 0.005f * 2.0f * (shape_b - 0.3f);
-        q[0] = to_i32(dpos[0] * kFpPos);
-        q[1] = to_i32(dpos[1] * kFpPos);
-        q[2] = to_i32(dpos[2] * kFpPos);
-        q[3] = to_i32(d_sx * kFpPos);
-        q[4] = to_i32(dColr * kFpCol);
-        q[5] = to_i32(dColg * kFpCol);
-        q[6] = to_i32(dColb * kFpCol);
-        q[7] = to_i32(d_opacity * kFpCol);
-        q[8] = to_i32(d_qw * kFpPos);
-        q[9] = to_i32(d_qx * kFpPos);
-        q[10] = to_i32(d_qy * kFpPos);
-        q[11] = to_i32(d_qz * kFpPos);
-        q[12] = to_i32(d_sy * kFpPos);
-        q[13] = to_i32(d_shape_a * kFpPos);
-        q[14] = to_i32(d_shape_b * kFpPos);
-        q[15] = to_i32(d_sz * kFpPos);
+        qv[0] = to_i32(dpos[0] * kFpPos);
+        qv[1] = to_i32(dpos[1] * kFpPos);
+        qv[2] = to_i32(dpos[2] * kFpPos);
+        qv[3] = to_i32(d_sx * kFpPos);
+        qv[4] = to_i32(dColr * kFpCol);
+        qv[5] = to_i32(dColg * kFpCol);
+        qv[6] = to_i32(dColb * kFpCol);
+        qv[7] = to_i32(d_opacity * kFpCol);
+        qv[8] = to_i32(d_qw * kFpPos);
+        qv[9] = to_i32(d_qx * kFpPos);
+        qv[10] = to_i32(d_qy * kFpPos);
+        qv[11] = to_i32(d_qz * kFpPos);
+        qv[12] = to_i32(d_sy * kFpPos);
+        qv[13] = to_i32(p.d_shape_a * kFpPos);
+        qv[14] = to_i32(p.d_shape_b * kFpPos);
+        qv[15] = to_i32(d_sz * kFpPos);
       }
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int32_t r = __reduce_add_sync(0xffffffffu, q[j]);
-        if (lane == 0 && r != 0) atomicAdd(&gacc[k * 16 + j], r);
+      for (int jj = 0; jj < 16; ++jj) {
+        const int32_t r = __reduce_add_sync(kFull, qv[jj]);
+        if (lane == 0 && r != 0) atomicAdd(&gacc[k * 16 + jj], r);
       }
     }
-    __syncthreads();
-    for (uint32_t e = tid; e < cnt * 16; e += kThreads) {
-      const int32_t val = gacc[e];
-      if (val != 0) atomicAdd(&a.grads[16 * (size_t)ids[e >> 4] + (e & 15)], val);
-    }
   }
+  __syncthreads();
+  if (!S.abort) {
+    if (nch > 0) flush(2 * nch - 1);
+    return;
+  }
+  // a bounded wait gave up: wait (bounded) for the batches still in flight
+  // (at most the last two staged) before the CTA's shared memory is released
+  if (tid == 0)
+    for (uint32_t q = issued >= 2 ? issued - 2 : 0; q < issued; ++q)
+      (void)bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u);
 }
 
 // splat_step.wgsl:32-106, one thread per splat.
@@ -837,10 +1077,13 @@ struct nps_splat_opt {
   const float* tgt_rgba = nullptr;
   const float* tgt_depth = nullptr;
   // work
-  DevBuf fwd, bwd, counts, offsets, rects, total, keys, vals, ranges, tabs, dead, stat, tstat;
+  DevBuf fwd, bwd, counts, kept, offsets, rects, total, keys, vals, ranges, tabs, dead, stat, tstat;
+  DevBuf grid, cutoff, tile_len;  // cap-aware binning
   SortWork sw;
   uint32_t pair_cap = 0;
   uint32_t last_ranges = 0;  // (view, tile) entries of the last backward's ranges
+  bool pairs_from_ranges = true;  // the last backward kept every overlapped pair
+  uint32_t kept_pairs = 0;
   nps_stats stats{};
 };
 
@@ -899,6 +1142,7 @@ int nps_splat_opt_create(nps_ctx* ctx, uint32_t num_splats, nps_splat_opt** out)
   cudaMemsetAsync(o->av.p, 0, p16, s);
   cudaMemsetAsync(o->gacc.p, 0, sizeof(float) * num_splats, s);
   cudaMemsetAsync(o->stat.p, 0, 64, s);
+  cudaMemsetAsync(o->total.p, 0, sizeof(uint32_t) * 4, s);
   NPS_CUDA(cudaGetLastError());
   *out = o;
   return NPS_OK;
@@ -909,7 +1153,8 @@ int nps_splat_opt_destroy(nps_splat_opt* o) {
   cudaSetDevice(o->ctx->device);
   cudaStreamSynchronize(o->ctx->stream);
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->views, &o->tgt_rgba_own,
-                    &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->offsets, &o->rects, &o->total,
+                    &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->kept, &o->offsets, &o->rects, &o->total,
+                    &o->grid, &o->cutoff, &o->tile_len,
                     &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->tstat, &o->sw.hist,
                     &o->sw.partial, &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt})
     b->release();
@@ -1029,19 +1274,61 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
   NPS_TRY(o->fwd.ensure(sizeof(float) * compat::kFwd * g));
   NPS_TRY(o->bwd.ensure(sizeof(float) * compat::kBwd * g));
   NPS_TRY(o->counts.ensure(sizeof(uint32_t) * g));
+  NPS_TRY(o->kept.ensure(sizeof(uint32_t) * g));
   NPS_TRY(o->offsets.ensure(sizeof(uint32_t) * g));
   NPS_TRY(o->rects.ensure(sizeof(uint2) * g));
   NPS_TRY(o->ranges.ensure(sizeof(uint32_t) * 2 * (size_t)num_tiles * nv));
+  NPS_TRY(o->tile_len.ensure(sizeof(uint32_t) * (size_t)num_tiles * nv));
+  uint32_t* total = o->total.as<uint32_t>();  // [0] pairs kept, [1] bounded waits that gave up, [2..3] u64 pairs
+  unsigned long long* overlapped = reinterpret_cast<unsigned long long*>(total + 2);
+  o->sw.err = total + 1;
   compat::k_project<<<div_up(g, 256), 256, 0, s>>>(o->params.as<float>(), n, o->views.as<float>(), nv, o->w, o->h,
                                                     o->tabs.as<float>(), tiles_x, tiles_y, o->fwd.as<float>(),
                                                     o->bwd.as<float>(), o->counts.as<uint32_t>(),
                                                     o->rects.as<uint2>());
   NPS_CHECK_LAUNCH();
-  uint32_t* total = o->total.as<uint32_t>();
-  NPS_TRY(exclusive_scan_u32(o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)g, total, o->sw, s));
-  uint32_t K = 0;
-  NPS_CUDA(cudaMemcpyAsync(&K, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  // splat blocks of the cap-aware binning: about 1024 splats each, at most
+  // 256, and the (view, block) difference grids within 2^26 cells
+  const uint32_t gx = tiles_x + 1, gy = tiles_y + 1;
+  const uint64_t cells = (uint64_t)nv * gx * gy;
+  uint32_t nb = std::min<uint32_t>(div_up(n, 1024), 256u);
+  nb = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nb, (1ull << 26) / cells));
+  const uint32_t bs = div_up(n, nb);
+  nb = div_up(n, bs);
+  const uint32_t* cutoff = nullptr;
+  NPS_CUDA(cudaMemsetAsync(overlapped, 0, sizeof(unsigned long long), s));
+  if (nb > 1) {
+    NPS_TRY(o->grid.ensure(sizeof(int32_t) * cells * nb));
+    NPS_TRY(o->cutoff.ensure(sizeof(uint32_t) * (size_t)num_tiles * nv));
+    int32_t* grid = o->grid.as<int32_t>();
+    NPS_CUDA(cudaMemsetAsync(grid, 0, sizeof(int32_t) * cells * nb, s));
+    compat::k_bin_diff<<<div_up(g, 256), 256, 0, s>>>(o->rects.as<uint2>(), o->counts.as<uint32_t>(), n, nv, bs, nb,
+                                                       gx, gy, grid);
+    const uint32_t grids = nv * nb;
+    compat::k_bin_rows<<<div_up((size_t)grids * gy, 128), 128, 0, s>>>(grid, grids * gy, gx);
+    compat::k_bin_cols<<<div_up((size_t)grids * gx, 128), 128, 0, s>>>(grid, grids, gx, gy);
+    compat::k_bin_cutoff<<<div_up((size_t)num_tiles * nv, 128), 128, 0, s>>>(
+        grid, nv, nb, tiles_x, num_tiles, gx, gy, o->cutoff.as<uint32_t>(), o->tile_len.as<uint32_t>(), overlapped);
+    NPS_CHECK_LAUNCH();
+    cutoff = o->cutoff.as<uint32_t>();
+  }
+  const uint32_t pair_grid = 8 * kNumSMs;  // 256-thread blocks of warps over the (view, splat) items
+  compat::k_bin_pairs<false><<<pair_grid, 256, 0, s>>>(o->rects.as<uint2>(), o->counts.as<uint32_t>(), cutoff, n,
+                                                       nv, bs, tiles_x, num_tiles, o->kept.as<uint32_t>(), nullptr, 0,
+                                                       nullptr, nullptr);
+  NPS_CHECK_LAUNCH();
+  NPS_TRY(exclusive_scan_u32(o->kept.as<uint32_t>(), o->offsets.as<uint32_t>(), (uint32_t)g, total, o->sw, s));
+  uint32_t hk[2] = {0, 0};  // pairs kept, bounded waits of the previous backward that gave up
+  NPS_CUDA(cudaMemcpyAsync(hk, total, sizeof(hk), cudaMemcpyDeviceToHost, s));
   NPS_CUDA(cudaStreamSynchronize(s));
+  const uint32_t K = hk[0];
+  if (hk[1] != 0) {
+    NPS_CUDA(cudaMemsetAsync(total + 1, 0, sizeof(uint32_t), s));
+    o->stats.reserved[2] += hk[1];
+    set_error("backward: %u bounded device waits of the previous backward gave up (its gradients are not valid)",
+              hk[1]);
+    return NPS_ERR_TIMEOUT;
+  }
   if (K > o->pair_cap) {
     uint32_t cap = K + K / 4 + 4096;
     NPS_TRY(o->keys.ensure(sizeof(uint32_t) * (size_t)cap));
@@ -1051,10 +1338,27 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
   NPS_CUDA(cudaMemsetAsync(o->ranges.p, 0, sizeof(uint32_t) * 2 * (size_t)num_tiles * nv, s));
   uint32_t* rstart = o->ranges.as<uint32_t>();
   uint32_t* rend = rstart + (size_t)num_tiles * nv;
+  compat::RasterArgs ra{};
+  ra.fwd = o->fwd.as<float>();
+  ra.bwd = o->bwd.as<float>();
+  ra.vals = o->counts.as<uint32_t>();  // no pairs: never read
+  ra.rstart = rstart;
+  ra.rend = rend;
+  ra.views = o->views.as<float>();
+  ra.tgt_rgba = o->tgt_rgba;
+  ra.tgt_depth = o->tgt_depth;
+  ra.grads = o->grads.as<int32_t>();
+  ra.out_rgbd = out_rgbd;
+  ra.err = total + 1;
+  ra.n = n;
+  ra.w = o->w;
+  ra.h = o->h;
+  ra.tiles_x = tiles_x;
+  ra.num_tiles = num_tiles;
   if (K > 0) {
-    compat::k_emit<<<div_up(g, 256), 256, 0, s>>>(o->counts.as<uint32_t>(), o->offsets.as<uint32_t>(),
-                                                   o->rects.as<uint2>(), n, nv, tiles_x, num_tiles, o->pair_cap,
-                                                   o->keys.as<uint32_t>(), o->vals.as<uint32_t>());
+    compat::k_bin_pairs<true><<<pair_grid, 256, 0, s>>>(o->rects.as<uint2>(), o->counts.as<uint32_t>(), cutoff, n, nv,
+                                                        bs, tiles_x, num_tiles, nullptr, o->offsets.as<uint32_t>(),
+                                                        o->pair_cap, o->keys.as<uint32_t>(), o->vals.as<uint32_t>());
     NPS_CHECK_LAUNCH();
     int bits = 1;
     while ((1ull << bits) < (uint64_t)num_tiles * nv) ++bits;
@@ -1063,54 +1367,19 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
                            &vs));
     compat::k_ranges<<<4 * kNumSMs, 256, 0, s>>>(ks, total, o->pair_cap, rstart, rend);
     NPS_CHECK_LAUNCH();
-    compat::RasterArgs ra;
-    ra.fwd = o->fwd.as<float>();
-    ra.bwd = o->bwd.as<float>();
     ra.vals = vs;
-    ra.rstart = rstart;
-    ra.rend = rend;
-    ra.views = o->views.as<float>();
-    ra.tgt_rgba = o->tgt_rgba;
-    ra.tgt_depth = o->tgt_depth;
-    ra.grads = o->grads.as<int32_t>();
-    ra.out_rgbd = out_rgbd;
-    ra.n = n;
-    ra.w = o->w;
-    ra.h = o->h;
-    ra.tiles_x = tiles_x;
-    ra.num_tiles = num_tiles;
-    static bool attr_set = false;
-    if (!attr_set) {
-      NPS_CUDA(cudaFuncSetAttribute(compat::k_raster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)compat::kRasterSmem));
-      attr_set = true;
-    }
-    compat::k_raster<<<dim3(tiles_x, tiles_y, nv), compat::kThreads, compat::kRasterSmem, s>>>(ra);
-    NPS_CHECK_LAUNCH();
-  } else {
-    // no pairs: every pixel is background; the backward still writes the image
-    compat::RasterArgs ra{};
-    ra.fwd = o->fwd.as<float>();
-    ra.bwd = o->bwd.as<float>();
-    ra.vals = o->counts.as<uint32_t>();
-    ra.rstart = rstart;
-    ra.rend = rend;
-    ra.views = o->views.as<float>();
-    ra.tgt_rgba = o->tgt_rgba;
-    ra.tgt_depth = o->tgt_depth;
-    ra.grads = o->grads.as<int32_t>();
-    ra.out_rgbd = out_rgbd;
-    ra.n = n;
-    ra.w = o->w;
-    ra.h = o->h;
-    ra.tiles_x = tiles_x;
-    ra.num_tiles = num_tiles;
-    NPS_CUDA(cudaFuncSetAttribute(compat::k_raster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)compat::kRasterSmem));
-    compat::k_raster<<<dim3(tiles_x, tiles_y, nv), compat::kThreads, compat::kRasterSmem, s>>>(ra);
+  }
+  if (!cutoff) {
+    // every overlapped pair was kept: the lists are complete
+    compat::k_range_len<<<4 * kNumSMs, 256, 0, s>>>(rstart, rend, num_tiles * nv, o->tile_len.as<uint32_t>());
     NPS_CHECK_LAUNCH();
   }
-  o->stats.pairs = K;
+  NPS_CUDA(cudaFuncSetAttribute(compat::k_raster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(compat::RasterSmem)));
+  compat::k_raster<<<dim3(tiles_x, tiles_y, nv), compat::kThreads, sizeof(compat::RasterSmem), s>>>(ra);
+  NPS_CHECK_LAUNCH();
+  o->pairs_from_ranges = cutoff == nullptr;
+  o->kept_pairs = K;
   o->last_ranges = num_tiles * nv;
   return NPS_OK;
 }
@@ -1170,17 +1439,20 @@ int nps_splat_opt_stats(nps_splat_opt* o, nps_stats* out) {
   cudaStream_t s = o->ctx->stream;
   uint32_t clones = 0;
   uint64_t ts[2] = {0, 0};  // pairs composited (each tile list capped), longest list
+  unsigned long long overlapped = 0;
   NPS_CUDA(cudaMemcpyAsync(&clones, o->stat.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   if (o->last_ranges > 0) {
     NPS_TRY(o->tstat.ensure(2 * sizeof(uint64_t)));
     NPS_CUDA(cudaMemsetAsync(o->tstat.p, 0, 2 * sizeof(uint64_t), s));
-    const uint32_t* rstart = o->ranges.as<uint32_t>();
     compat::k_tile_stats<<<std::min(div_up(o->last_ranges, 256), 4u * kNumSMs), 256, 0, s>>>(
-        rstart, rstart + o->last_ranges, o->last_ranges, o->tstat.as<unsigned long long>());
+        o->tile_len.as<uint32_t>(), o->last_ranges, o->tstat.as<unsigned long long>());
     NPS_CHECK_LAUNCH();
     NPS_CUDA(cudaMemcpyAsync(ts, o->tstat.p, sizeof(ts), cudaMemcpyDeviceToHost, s));
+    NPS_CUDA(cudaMemcpyAsync(&overlapped, o->total.as<uint32_t>() + 2, sizeof(overlapped), cudaMemcpyDeviceToHost, s));
   }
   NPS_CUDA(cudaStreamSynchronize(s));
+  o->stats.reserved[1] = o->kept_pairs;  // pairs kept by the cap-aware binning and sorted
+  o->stats.pairs = o->pairs_from_ranges ? o->kept_pairs : overlapped;
   o->stats.pairs_capped = ts[0];
   o->stats.max_tile_len = (uint32_t)ts[1];
   o->stats.adc_clones = clones;

@@ -36,6 +36,7 @@
 #include <cstring>
 #include <vector>
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "context.h"
 #include "gs_math.cuh"
@@ -397,35 +398,7 @@ __global__ void k_ranges(const uint32_t* __restrict__ keys, const uint32_t* __re
 // cp.async.bulk global -> shared completing on the buffer's mbarrier; thread 0
 // posts the batch's byte count.  Waits are bounded: on a timeout the kernel
 // records it in *err and carries on (the batch is then undefined).
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
-                   smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_addr(bar);
-  for (uint32_t it = 0; it < (1u << 22); ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
+using namespace nps::bulk;
 // stage records vals[b0 .. b0 + nb) into buf (thread t copies records t,
 // t + blockDim.x, ...)
 __device__ __forceinline__ void stage_batch(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,

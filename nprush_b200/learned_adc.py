@@ -214,7 +214,8 @@ def main(argv=None):
             for es in a.eval_seeds:
                 r, p = run(scene, a.steps, es, adc, fn, mode=mode, views=a.views)
                 runs.append(dict(seed=es, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
-                                 skipped=r.skipped_steps, adc_events=r.adc_events[-3:]))
+                                 adc_s=r.adc_s, after_adc_s=r.after_adc_s, skipped=r.skipped_steps,
+                                 adc_events=r.adc_events[-3:]))
             out[name] = dict(mode=mode, runs=runs, psnr=float(np.mean([x["psnr"] for x in runs])),
                              count=float(np.mean([x["count"] for x in runs])),
                              wall_s=float(np.mean([x["wall_s"] for x in runs])))

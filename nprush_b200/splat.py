@@ -216,7 +216,8 @@ class GpuSplatOptimizerManager:
         st = _lib.nps_stats()
         call("nps_splat_opt_stats", self._h, ctypes.byref(st))
         return dict(pairs=st.pairs, pairs_capped=st.pairs_capped, max_tile_len=st.max_tile_len,
-                    adc_clones=st.adc_clones, step_count=st.step_count)
+                    adc_clones=st.adc_clones, step_count=st.step_count, pairs_kept=st.reserved[1],
+                    timeouts=st.reserved[2])
 
     def set_step_count(self, count: int):
         """stepCount (dispatch() calls so far; ADC every 25th)."""

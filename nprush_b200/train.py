@@ -47,6 +47,8 @@ class FitResult:
     losses: list = field(default_factory=list)
     psnr: list = field(default_factory=list)
     skipped_steps: int = 0
+    adc_s: float = 0.0        # host time in the ADC calls (they end with the new count on the host)
+    after_adc_s: float = 0.0  # host time of the first step after each ADC event (batched: the re-capture)
 
 
 @functools.lru_cache(maxsize=4)
@@ -91,21 +93,29 @@ def fit(trainer, vp, vpi, steps: int, views: int = 8, seed: int = 0, adc: AdcSch
     res = FitResult(steps=steps, wall_s=0.0, count=trainer.count)
     trainer.sync()
     t0 = time.perf_counter()
+    after_adc = False
     for s in range(steps):
         sel = view_schedule(s, n_cams, views, seed)
         want_loss = log_every > 0 and (s % log_every == 0 or s == steps - 1)
+        ts = time.perf_counter()
         if mode == "batched":
             trainer.set_views(vp[sel], vpi[sel], sel)
             l3 = trainer.train_step(read_loss=want_loss)
         else:
             l3 = trainer.train_step_per_view(vp[sel], vpi[sel], sel, read_loss=want_loss)
+        if after_adc:
+            res.after_adc_s += time.perf_counter() - ts
+            after_adc = False
         if l3 is not None:
             res.losses.append((s + 1, l3[0]))
         if adc.due(s + 1):
+            ta = time.perf_counter()
             if adc_fn is not None:
                 ev = adc_fn(trainer, s + 1)
             else:
                 ev = trainer.adc(adc.grad_thresh, adc.split_scale, adc.prune_opacity)
+            res.adc_s += time.perf_counter() - ta
+            after_adc = True
             res.adc_events.append((s + 1, ev["after"], ev["densified"], ev["pruned"]))
     trainer.sync()
     res.wall_s = time.perf_counter() - t0
@@ -168,11 +178,11 @@ def main(argv=None):
         r.psnr = evaluate_psnr(st, vp, vpi).tolist()
     out = dict(mode=a.mode, steps=a.steps, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s, count=r.count,
                psnr_mean=float(np.mean(r.psnr)), psnr_initial=float(np.mean(psnr0)), psnr=r.psnr,
-               adc_events=r.adc_events, losses=r.losses, skipped_steps=r.skipped_steps,
-               adc=asdict(adc), gaussians=a.gaussians, res=a.res)
+               adc_events=r.adc_events, losses=r.losses, skipped_steps=r.skipped_steps, adc_s=r.adc_s,
+               after_adc_s=r.after_adc_s, adc=asdict(adc), gaussians=a.gaussians, res=a.res)
     line = json.dumps(out)
     print(json.dumps({k: out[k] for k in ("mode", "steps", "wall_s", "steps_per_s", "count", "psnr_mean",
-                                          "psnr_initial", "skipped_steps")}))
+                                          "psnr_initial", "skipped_steps", "adc_s", "after_adc_s")}))
     if a.out:
         with open(a.out, "w") as f:
             f.write(line + "\n")

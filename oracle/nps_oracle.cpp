@@ -213,9 +213,14 @@ extern "C" {
 //   grads_f     N x 16 f32 unquantised sums (may be null)
 //   out_rgbd    H x W x 4: composited colour + reciprocal depth (may be null)
 //   tile_count  tiles_y x tiles_x list lengths after the cap (may be null)
+//   terms       N: ADDED the number of (pixel, splat) backward terms with
+//               alpha >= 0.001 each splat's gradient sums (may be null; the
+//               bound for the device's i32 sums, whose terms are truncated
+//               one by one)
 int orc_splat_backward(const float* splats, uint32_t n, const float* vp, const float* vpinv,
                        const float* tgt_rgba, const float* tgt_depth, uint32_t w, uint32_t h,
-                       int32_t* grads_q, float* grads_f, float* out_rgbd, uint32_t* tile_count) {
+                       int32_t* grads_q, float* grads_f, float* out_rgbd, uint32_t* tile_count,
+                       uint32_t* terms) {
   const float aspect = (float)w / (float)h;
   const uint32_t tiles_x = (w + 15) / 16, tiles_y = (h + 15) / 16;
   std::vector<SplatProj> proj(n);
@@ -282,6 +287,7 @@ int orc_splat_backward(const float* splats, uint32_t n, const float* vp, const f
             uint32_t i = list[idx];
             float a = alphas[idx];
             if (a < 0.001f) continue;
+            if (terms) ++terms[i];
             const float* s = splats + 16 * (size_t)i;
             const SplatProj& P = proj[i];
             PixEval e = splat_pix(P, p);

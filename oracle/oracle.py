@@ -59,8 +59,11 @@ def _f32(a):
 
 
 # ------------------------------------------------------------- compat splats
-def splat_backward(splats, vp, vpinv, tgt_rgba, tgt_depth, grads_q=None, want_float=True, want_image=True):
-    """One view of splat_backward.wgsl. Returns dict(grads_q, grads_f, image, tile_count)."""
+def splat_backward(splats, vp, vpinv, tgt_rgba, tgt_depth, grads_q=None, want_float=True, want_image=True,
+                   terms=None):
+    """One view of splat_backward.wgsl. Returns dict(grads_q, grads_f, image, tile_count, terms): terms[i]
+    counts the (pixel, splat) backward terms (alpha >= 0.001) splat i's gradient sums (added to `terms`
+    when given)."""
     splats = _f32(splats)
     n = splats.shape[0]
     h, w = tgt_depth.shape
@@ -68,9 +71,10 @@ def splat_backward(splats, vp, vpinv, tgt_rgba, tgt_depth, grads_q=None, want_fl
     gf = np.zeros((n, 16), np.float32) if want_float else None
     img = np.zeros((h, w, 4), np.float32) if want_image else None
     tc = np.zeros(((h + 15) // 16, (w + 15) // 16), np.uint32)
+    tm = np.zeros(n, np.uint32) if terms is None else terms
     lib().orc_splat_backward(_p(splats, F), n, _p(_f32(vp), F), _p(_f32(vpinv), F), _p(_f32(tgt_rgba), F),
-                             _p(_f32(tgt_depth), F), w, h, _p(gq, I), _p(gf, F), _p(img, F), _p(tc, U))
-    return dict(grads_q=gq, grads_f=gf, image=img, tile_count=tc)
+                             _p(_f32(tgt_depth), F), w, h, _p(gq, I), _p(gf, F), _p(img, F), _p(tc, U), _p(tm, U))
+    return dict(grads_q=gq, grads_f=gf, image=img, tile_count=tc, terms=tm)
 
 
 def splat_step(splats, grads, m, v, adam_t, grad_accum):
