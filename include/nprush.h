@@ -104,7 +104,10 @@ int nps_splat_opt_set_target(nps_splat_opt* opt, const float* rgba, const float*
 int nps_splat_opt_dispatch(nps_splat_opt* opt);
 /* The three stages of dispatch, separately (splat_backward / splat_step /
  * splat_adc).  backward optionally writes the fp32 composite the backward
- * computes (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device). */
+ * computes (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device).
+ * A backward whose raster's bounded record-staging wait or sort look-back
+ * gave up leaves invalid gradients; the next backward reports it with
+ * NPS_ERR_TIMEOUT (and runs nothing further). */
 int nps_splat_opt_backward(nps_splat_opt* opt, float* out_rgbd_device);
 int nps_splat_opt_step(nps_splat_opt* opt);
 int nps_splat_opt_adc(nps_splat_opt* opt);
@@ -153,12 +156,16 @@ int nps_splat_adc_noalloc(float* splats, float* adam_m, float* adam_v, float* gr
                           float adam_t, void* cuda_stream, uint32_t* clones_host);
 
 typedef struct nps_stats {
-  uint64_t pairs;          /* (tile, primitive) pairs emitted by the last backward, all views */
+  uint64_t pairs;          /* (tile, primitive) pairs overlapped in the last backward, all views (splats:
+                              the binning sorts only those that can fall among a tile's first 1024,
+                              reserved[1]) */
   uint64_t pairs_capped;   /* pairs composited after the per-tile cap */
   uint32_t max_tile_len;   /* longest tile list before the cap */
   uint32_t adc_clones;     /* clones + splits performed by the last ADC */
   uint32_t step_count;     /* dispatch() calls so far */
-  uint32_t reserved[3];    /* Bezier: [0] spawns.  Gaussians: [0] kernel launches per replay of the
+  uint32_t reserved[3];    /* Splats: [1] pairs kept by the cap-aware binning, [2] bounded device waits
+                              that gave up (a backward after one returns NPS_ERR_TIMEOUT).
+                              Bezier: [0] spawns.  Gaussians: [0] kernel launches per replay of the
                               captured train step (its graph's kernel nodes), [1] graph replays that
                               skipped their update (pair overflow), [2] bounded device waits
                               that gave up (raster record staging, sort look-back) */

@@ -115,14 +115,20 @@ def policy_adc_fn(policy, adc: AdcSchedule, margin: float = 0.0):
     return fn
 
 
-def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: str = "batched", views: int = 8):
+def run(scene_fn, steps: int, seed: int, adc: AdcSchedule, adc_fn=None, mode: str = "batched", views: int = 8,
+        autotune: bool = False):
     """One training run on a fresh scene; returns (FitResult, mean PSNR)."""
     vp, vpi, tg, st = scene_fn(seed)
     st.assign_ids(0)
-    r = fit(st, vp, vpi, steps, views=views, seed=seed, adc=adc, mode=mode, adc_fn=adc_fn)
+    r = fit(st, vp, vpi, steps, views=views, seed=seed, adc=adc, mode=mode, adc_fn=adc_fn, autotune=autotune)
     psnr = float(np.mean(evaluate_psnr(st, vp, vpi, views=views)))
     st.close()
     return r, psnr
+
+
+def _tile_choice(tuned):
+    """The autotuner's choice without its timing table."""
+    return None if tuned is None else {k: v for k, v in tuned.items() if k != "per_tile"}
 
 
 def main(argv=None):
@@ -137,7 +143,13 @@ def main(argv=None):
                     help="keep-logit margins of the learned arms (one evaluation run each)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain batched arm")
     ap.add_argument("--with-per-view", action="store_true",
-                    help="also run the plain per-view trainer (eager, one view per launch) on the eval seed")
+                    help="also run the plain per-view trainer (eager, one view per launch, default raster "
+                         "variants) on the eval seed")
+    ap.add_argument("--with-per-view-tuned", action="store_true",
+                    help="also run the per-view trainer with the autotuned raster variants (context)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batched arms keep the default raster variants (the autotuner is part of the batched "
+                         "trainer and its time counts in their wall time)")
     ap.add_argument("--adc-stop", type=int, default=None)
     ap.add_argument("--adc-start", type=int, default=500)
     ap.add_argument("--adc-every", type=int, default=100)
@@ -201,21 +213,26 @@ def main(argv=None):
         out["training"] = dict(samples=int(len(y)), class_counts=np.bincount(y, minlength=4).tolist(),
                                class_w=cw.tolist(), loss=lc.tolist(), acc=ac.tolist(),
                                heldout_confusion=conf.tolist(), heldout_recall=per_class_recall(conf))
-        arms = [] if a.no_plain else [("plain", None, "batched")]
+        tune = not a.no_autotune
+        arms = [] if a.no_plain else [("plain", None, "batched", tune)]
         for thr in a.plain_thresholds:
             arms.append((f"plain_t{thr:g}", plain_adc_fn(AdcSchedule(every=adc.every, start=adc.start,
-                                                                     stop=adc.stop, grad_thresh=thr)), "batched"))
+                                                                     stop=adc.stop, grad_thresh=thr)), "batched",
+                         tune))
         for mg in a.margins:
-            arms.append(("learned" if mg == 0.0 else f"learned_m{mg:g}", policy_adc_fn(pol, adc, mg), "batched"))
+            arms.append(("learned" if mg == 0.0 else f"learned_m{mg:g}", policy_adc_fn(pol, adc, mg), "batched",
+                         tune))
         if a.with_per_view:
-            arms.append(("plain_per_view", None, "per_view"))
-        for name, fn, mode in arms:
+            arms.append(("plain_per_view", None, "per_view", False))
+        if a.with_per_view_tuned:
+            arms.append(("plain_per_view_tuned", None, "per_view", True))
+        for name, fn, mode, at in arms:
             runs = []
             for es in a.eval_seeds:
-                r, p = run(scene, a.steps, es, adc, fn, mode=mode, views=a.views)
+                r, p = run(scene, a.steps, es, adc, fn, mode=mode, views=a.views, autotune=at)
                 runs.append(dict(seed=es, psnr=p, count=r.count, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s,
-                                 adc_s=r.adc_s, after_adc_s=r.after_adc_s, skipped=r.skipped_steps,
-                                 adc_events=r.adc_events[-3:]))
+                                 adc_s=r.adc_s, after_adc_s=r.after_adc_s, tune_s=r.tune_s, tuned=_tile_choice(r.tuned),
+                                 skipped=r.skipped_steps, adc_events=r.adc_events[-3:]))
             out[name] = dict(mode=mode, runs=runs, psnr=float(np.mean([x["psnr"] for x in runs])),
                              count=float(np.mean([x["count"] for x in runs])),
                              wall_s=float(np.mean([x["wall_s"] for x in runs])))
@@ -224,6 +241,12 @@ def main(argv=None):
                 d_psnr = [x["psnr"] - y["psnr"] for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
                 d_cnt = [x["count"] / y["count"] - 1.0 for x, y in zip(out[name]["runs"], out["plain"]["runs"])]
                 out[name]["vs_plain"] = dict(psnr_db=d_psnr, count_frac=d_cnt)
+        if "plain_per_view" in out:
+            # the target's comparison: batched arms against the plain per-view trainer
+            base = out["plain_per_view"]
+            for name in [k for k in out if k in ("plain", "plain_per_view_tuned") or k.startswith("learned")]:
+                out[name]["vs_per_view"] = dict(wall_frac=out[name]["wall_s"] / base["wall_s"],
+                                                psnr_db=out[name]["psnr"] - base["psnr"])
     out["config"] = vars(a)
     print(json.dumps({k: v for k, v in out.items() if k not in ("training", "log_runs", "config")}))
     print(json.dumps(dict(class_counts=out["training"]["class_counts"], acc=out["training"]["acc"][-1],

@@ -48,6 +48,8 @@ class FitResult:
     psnr: list = field(default_factory=list)
     skipped_steps: int = 0
     adc_s: float = 0.0        # host time in the ADC calls (they end with the new count on the host)
+    tune_s: float = 0.0       # host time of the raster autotuner
+    tuned: dict | None = None
     after_adc_s: float = 0.0  # host time of the first step after each ADC event (batched: the re-capture)
 
 
@@ -78,10 +80,12 @@ def evaluate_psnr(trainer, vp, vpi, views: int = 8) -> np.ndarray:
 
 
 def fit(trainer, vp, vpi, steps: int, views: int = 8, seed: int = 0, adc: AdcSchedule | None = None,
-        mode: str = "batched", log_every: int = 0, adc_fn=None) -> FitResult:
-    """Train for `steps` steps; wall time covers training and ADC, not the
-    final evaluation.  adc_fn(trainer, step) replaces the plain ADC call when
-    given (learned policies plug in here)."""
+        mode: str = "batched", log_every: int = 0, adc_fn=None, autotune: bool = False) -> FitResult:
+    """Train for `steps` steps; wall time covers training and ADC (and the
+    autotuner when asked for), not the final evaluation.  adc_fn(trainer,
+    step) replaces the plain ADC call when given (learned policies plug in
+    here).  autotune: the raster autotuner chooses the tile size and raster
+    variants on the first step's views before training."""
     n_cams = vp.shape[0]
     adc = adc or AdcSchedule()
     if mode == "batched":
@@ -93,6 +97,11 @@ def fit(trainer, vp, vpi, steps: int, views: int = 8, seed: int = 0, adc: AdcSch
     res = FitResult(steps=steps, wall_s=0.0, count=trainer.count)
     trainer.sync()
     t0 = time.perf_counter()
+    if autotune and steps > 0:
+        sel = view_schedule(0, n_cams, views, seed)
+        trainer.set_views(vp[sel], vpi[sel], sel)
+        res.tuned = trainer.autotune()
+        res.tune_s = time.perf_counter() - t0
     after_adc = False
     for s in range(steps):
         sel = view_schedule(s, n_cams, views, seed)
