@@ -460,7 +460,9 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     d = true;                                \
     _Pragma("unroll") for (int k_ = 0; k_ < PPT; ++k_) d = d && dn[k_]; \
   } while (0)
+  __shared__ uint32_t s_abort;
   if (tid == 0) {
+    s_abort = 0u;
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     if (pending_next)
       stage_batch(recs, vals, base + SB, min((uint32_t)SB, end - base - SB), s_rec[buf ^ 1u], &s_bar[buf ^ 1u],
                   nullptr);
-    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u)) s_abort = 1u;  // the batch is undefined: end the tile below
     const Rec* sr = s_rec[buf];
     // staged pairs whose alpha >= 1/255 box meets the warp's strip (one lane
     // tests SB / 32 pairs; the warp then walks the set bits in order)
@@ -526,10 +528,16 @@ __global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs,
     }
     // every pixel of the tile done: stop (after the prefetch in flight lands)
     NPS_ALL_DONE(done);
-    if (__syncthreads_count(done) == NT) {
-      if (pending_next && !mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+    if (__syncthreads_count(done) == NT || s_abort) {
+      if (pending_next && !mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u)) s_abort = 1u;
       break;
     }
+  }
+  __syncthreads();
+  if (s_abort) {
+    // a bounded wait gave up: the tile's outputs are not written (the step reports NPS_ERR_TIMEOUT)
+    if (tid == 0) atomicAdd(err, 1u);
+    return;
   }
   uint32_t wmax = 0;
 #pragma unroll
@@ -1175,8 +1183,10 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
     pix_bwd_init(p[k], px, py + k, v, W, H, bg, img, ncontrib, dimg);
     mylast = max(mylast, p[k].last);
   }
+  __shared__ uint32_t s_abort;
   if (tid == 0) {
     s_max = 0;
+    s_abort = 0u;
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1215,7 +1225,7 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       const uint32_t nbs = bstart_of(bi + 1);
       stage_batch(recs, vals, nbs, bstart - nbs, s_rec[buf ^ 1u], &s_bar[buf ^ 1u], s_g[gnext]);
     }
-    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u) && tid == 0) atomicAdd(err, 1u);
+    if (!mbar_wait(&s_bar[buf], (bi >> 1) & 1u)) s_abort = 1u;  // the batch is undefined: end the tile below
     const Rec* sr = s_rec[buf];
     float(*acc)[9] = s_acc[buf];
     uint32_t hit[SB / 32];
@@ -1260,6 +1270,15 @@ __global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs
       }
     }
     __syncthreads();
+    if (s_abort) {
+      // a bounded wait gave up: no further sums leave the tile (the step reports NPS_ERR_TIMEOUT); the
+      // batch staged for bi + 1 is waited for (bounded) before the CTA's shared memory is released
+      if (tid == 0) {
+        atomicAdd(err, 1u);
+        if (bi + 1 < nbatch) (void)mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u);
+      }
+      return;
+    }
     for (uint32_t r = tid; r < nb; r += NT) {
       float* dst = g2 + (size_t)s_g[gb][r] * kG2;
 #pragma unroll

@@ -165,6 +165,10 @@ def main(argv=None):
     ap.add_argument("--gaussians", type=int, default=200_000)
     ap.add_argument("--teacher", type=int, default=250_000)
     ap.add_argument("--res", type=int, default=800)
+    ap.add_argument("--width", type=int, default=None, help="image width (default: --res)")
+    ap.add_argument("--height", type=int, default=None, help="image height (default: --res)")
+    ap.add_argument("--cams", type=int, default=32, help="cameras on the sphere")
+    ap.add_argument("--autotune", action="store_true", help="raster autotuner before training (batched)")
     ap.add_argument("--capacity", type=int, default=3_000_000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-adc", action="store_true")
@@ -180,18 +184,21 @@ def main(argv=None):
     ctx = _lib.context(0)
     _lib.call("nps_set_stream", ctx, stream.cuda_stream)
     with torch.cuda.stream(stream):
-        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.res, a.res, capacity=a.capacity)
+        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.width or a.res, a.height or a.res,
+                                        n_cams=a.cams, capacity=a.capacity)
         adc = AdcSchedule(every=0 if a.no_adc else 100, start=a.adc_start, stop=a.adc_stop)
         psnr0 = evaluate_psnr(st, vp, vpi)
-        r = fit(st, vp, vpi, a.steps, seed=a.seed, adc=adc, mode=a.mode, log_every=a.log_every)
+        r = fit(st, vp, vpi, a.steps, seed=a.seed, adc=adc, mode=a.mode, log_every=a.log_every,
+                autotune=a.autotune)
         r.psnr = evaluate_psnr(st, vp, vpi).tolist()
     out = dict(mode=a.mode, steps=a.steps, wall_s=r.wall_s, steps_per_s=a.steps / r.wall_s, count=r.count,
                psnr_mean=float(np.mean(r.psnr)), psnr_initial=float(np.mean(psnr0)), psnr=r.psnr,
                adc_events=r.adc_events, losses=r.losses, skipped_steps=r.skipped_steps, adc_s=r.adc_s,
-               after_adc_s=r.after_adc_s, adc=asdict(adc), gaussians=a.gaussians, res=a.res)
+               after_adc_s=r.after_adc_s, tune_s=r.tune_s, adc=asdict(adc), gaussians=a.gaussians,
+               res=[a.width or a.res, a.height or a.res], cams=a.cams)
     line = json.dumps(out)
     print(json.dumps({k: out[k] for k in ("mode", "steps", "wall_s", "steps_per_s", "count", "psnr_mean",
-                                          "psnr_initial", "skipped_steps", "adc_s", "after_adc_s")}))
+                                          "psnr_initial", "skipped_steps", "adc_s", "after_adc_s", "tune_s")}))
     if a.out:
         with open(a.out, "w") as f:
             f.write(line + "\n")
