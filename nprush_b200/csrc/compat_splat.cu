@@ -113,29 +113,6 @@ __global__ void k_tile_tables(float* tabs, uint32_t tiles_x, uint32_t tiles_y, u
   }
 }
 
-// Squared screen distance from a splat's centre beyond which its alpha is
-// exactly 0 at every pixel, or +inf when that cannot be guaranteed.  alpha is
-// 0 when power = -b r^a <= -15, with r^2 = d^T Q d >= lambda_min(Q) |d|^2 for
-// the conic Q = (A, B; B, C): so |d|^2 >= (15 / b)^(2 / a) / lambda_min
-// suffices.  Margins, in double: 1% on the power threshold (the kernel's pow
-// and exp run on the special-function unit), lambda_min reduced by 1e-6 of
-// |A| + 2|B| + |C| (the fp32 evaluation of d^T Q d) and the radius widened
-// by 1% plus 1e-5 (1 + |centre|) (the fp32 offset from the pixel).  A
-// colour, depth or opacity that is not finite never skips: 0 * NaN is not 0.
-__device__ __forceinline__ float zero_alpha_dist2(float A, float B, float C, float a, float b, float cx, float cy,
-                                                  const float* s, float depth) {
-  if (!(a > 0.0f) || !(b > 0.0f) || !isfinite(cx) || !isfinite(cy)) return INFINITY;
-  if (!isfinite(s[4]) || !isfinite(s[5]) || !isfinite(s[6]) || !isfinite(s[7]) || !isfinite(depth)) return INFINITY;
-  const double dA = A, dB = B, dC = C;
-  const double half_tr = 0.5 * (dA + dC), half_df = 0.5 * (dA - dC);
-  const double lam = half_tr - sqrt(half_df * half_df + dB * dB) - 1e-6 * (fabs(dA) + 2.0 * fabs(dB) + fabs(dC));
-  if (!(lam > 0.0)) return INFINITY;
-  const double R2 = pow(15.0 * 1.01 / (double)b, 2.0 / (double)a);
-  const double rad = sqrt(R2 / lam) * 1.01 + 1e-5 * (1.0 + fabs((double)cx) + fabs((double)cy));
-  const double d2 = rad * rad;
-  return d2 < 1e30 ? __double2float_ru(d2) : INFINITY;
-}
-
 __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splats, uint32_t n,
                                                  const float* __restrict__ views, uint32_t nv, uint32_t w, uint32_t h,
                                                  const float* __restrict__ tabs, uint32_t tiles_x, uint32_t tiles_y,
@@ -182,8 +159,7 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splat
   f4[0] = make_float4(scx, scy, A, B);
   f4[1] = make_float4(C, s[13], s[14], s[7]);
   f4[2] = make_float4(s[4], s[5], s[6], depth);
-  // a / 2 for pow(r, a) = 2^((a / 2) log2 r^2); the zero-alpha distance for the rasteriser's strip culling
-  f4[3] = make_float4(0.5f * s[13], zero_alpha_dist2(A, B, C, s[13], s[14], scx, scy, s, depth), 0.0f, 0.0f);
+  f4[3] = make_float4(0.5f * s[13], 0.0f, 0.0f, 0.0f);  // a / 2 for pow(r, a) = 2^((a / 2) log2 r^2)
   float4* b4 = reinterpret_cast<float4*>(bwd + (size_t)g * kBwd);
   b4[0] = make_float4(W, clip.x, clip.y, sx);
   b4[1] = make_float4(sy, sz, m0x, m0y);
@@ -498,9 +474,6 @@ __device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval&
 // walks the chunks in reverse, replaying each from its checkpoint.
 //
 // Exact skips (results identical to evaluating every pair):
-//  * a pair whose zero-alpha distance (k_project) the warp's strip lies
-//    beyond: alpha is exactly 0 at all 32 pixels, so the pair changes
-//    nothing in the forward and is invalid (alpha < 0.001) in the backward;
 //  * a warp whose 32 pixels all reached T == 0 stops compositing: a pair
 //    then adds T * alpha * c = 0 and leaves T at 0 (for finite colours and
 //    depths, which the step keeps inside their boxes);
@@ -520,17 +493,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
   const bool inside = px < a.w && py < a.h;
   const float aspect = (float)a.w / (float)a.h;
   const float ppx = pixel_px(px, a.w, aspect), ppy = pixel_py(py, a.h);
-  // the warp's 8 x 4 strip of pixel centres (warp-uniform): a pair whose
-  // zero-alpha distance (forward record [13]) the strip lies beyond is
-  // skipped by the whole warp (alpha is exactly 0 at all its pixels)
-  const uint32_t sx0 = tx * 16 + 8 * (warp & 1u), sy0 = ty * 16 + 4 * (warp >> 1);
-  const float strip_x0 = pixel_px(sx0, a.w, aspect), strip_x1 = pixel_px(sx0 + 7, a.w, aspect);
-  const float strip_y0 = pixel_py(sy0 + 3, a.h), strip_y1 = pixel_py(sy0, a.h);
-  auto strip_misses = [&](const float* f) {
-    const float ex = fmaxf(fmaxf(strip_x0 - f[0], f[0] - strip_x1), 0.0f);
-    const float ey = fmaxf(fmaxf(strip_y0 - f[1], f[1] - strip_y1), 0.0f);
-    return ex * ex + ey * ey > f[13];
-  };
   if (tid < 16) S.vpm[tid] = a.views[32 * (size_t)v + tid];
   const uint32_t key = v * a.num_tiles + ty * a.tiles_x + tx;
   const uint32_t start = a.rstart[key];
@@ -594,7 +556,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
       const uint32_t b = c & 1u;
       for (uint32_t k = 0; k < cnt; ++k) {
         const float* f = S.fwd[b][k];
-        if (strip_misses(f)) continue;
         const float al = eval_px(f, ppx, ppy).al;
         Cr += T * al * f[8];
         Cg += T * al * f[9];
@@ -661,13 +622,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
       float Tc = T0;
       for (uint32_t k = 0; k < cnt; ++k) {
         S.tprev[k][tid] = Tc;
-        if (!strip_misses(S.fwd[b][k])) Tc = Tc * (1.0f - eval_px(S.fwd[b][k], ppx, ppy).al);
+        Tc = Tc * (1.0f - eval_px(S.fwd[b][k], ppx, ppy).al);
       }
     }
     int32_t* gacc = &S.gacc[b][0][0];
     for (int k = (int)cnt - 1; k >= 0; --k) {
       const float* f = S.fwd[b][k];
-      if (strip_misses(f)) continue;
       const PixEval e = eval_px(f, ppx, ppy);
       const bool valid = inside && !(e.al < 0.001f);
       if (!__any_sync(kFull, valid)) continue;
