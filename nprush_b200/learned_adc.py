@@ -169,6 +169,12 @@ def main(argv=None):
                     help="leave out the keep -> densify relabelling (densified at the next event anyway)")
     ap.add_argument("--views", type=int, default=8, help="views per step")
     ap.add_argument("--cams", type=int, default=32, help="cameras on the sphere")
+    ap.add_argument("--log-gaussians", type=int, default=None,
+                    help="scene of the logging runs (default: the evaluation scene's); e.g. the 200k / 800x800 / "
+                         "32-camera scene for a policy evaluated at 1M / 1920x1080 / 64 cameras")
+    ap.add_argument("--log-teacher", type=int, default=None)
+    ap.add_argument("--log-res", type=int, default=None)
+    ap.add_argument("--log-cams", type=int, default=None)
     ap.add_argument("--class-weights", action="store_true",
                     help="weight classes by inverse frequency (default: uniform; a false prune costs more "
                          "than a missed one)")
@@ -184,21 +190,30 @@ def main(argv=None):
     _lib.call("nps_set_stream", ctx, stream.cuda_stream)
     adc = AdcSchedule(every=a.adc_every, start=a.adc_start, stop=a.adc_stop or min(15000, a.steps))
 
-    def scene(seed):
-        # student and teacher seeds derived from the run seed
-        vp, vpi, tg, st = teacher_scene(0, a.gaussians, a.teacher, a.width or a.res, a.height or a.res, n_cams=a.cams,
-                                        sh_degree=a.sh_degree, capacity=4 * a.gaussians, student_seed=seed,
-                                        teacher_seed=seed + 1000)
-        if a.deterministic:
-            st.set_deterministic(True)
-        return vp, vpi, tg, st
+    def make_scene(gaussians, teacher, width, height, cams):
+        def scene(seed):
+            # student and teacher seeds derived from the run seed
+            vp, vpi, tg, st = teacher_scene(0, gaussians, teacher, width, height, n_cams=cams,
+                                            sh_degree=a.sh_degree, capacity=4 * gaussians, student_seed=seed,
+                                            teacher_seed=seed + 1000)
+            if a.deterministic:
+                st.set_deterministic(True)
+            return vp, vpi, tg, st
+        return scene
+
+    scene = make_scene(a.gaussians, a.teacher, a.width or a.res, a.height or a.res, a.cams)
+    log_scene = scene
+    if a.log_gaussians or a.log_res or a.log_cams or a.log_teacher:
+        lg = a.log_gaussians or a.gaussians
+        log_scene = make_scene(lg, a.log_teacher or a.teacher, a.log_res or a.width or a.res,
+                               a.log_res or a.height or a.res, a.log_cams or a.cams)
 
     out = {}
     with torch.cuda.stream(stream):
         log = AdcLog(seed=1)
         log_steps = a.log_steps or min(a.steps, adc.stop)
         for s in a.log_seeds:
-            r, p = run(scene, log_steps, s, adc, logging_adc_fn(log, adc))
+            r, p = run(log_scene, log_steps, s, adc, logging_adc_fn(log, adc))
             out.setdefault("log_runs", []).append(dict(seed=s, psnr=p, count=r.count, wall_s=r.wall_s))
         X, y = hindsight_labels(log, a.horizon, densify_early=not a.no_densify_early)
         cw = class_weights(y) if a.class_weights else np.ones(4, np.float32)
