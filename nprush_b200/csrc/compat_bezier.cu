@@ -34,7 +34,7 @@ namespace bz {
 constexpr int kRecF = 20;      // forward record floats
 constexpr int kRecB = 24;      // backward record floats (per control point: d screen / d world, 2 x 3)
 constexpr uint32_t kCap = 1024;  // BEZIER_MAX_TILE_BEZIERS, constants.ts:20
-constexpr int kChunk = 28;       // 2 CTAs per SM fit in shared memory
+constexpr int kChunk = 28;       // with the checkpoints in global memory, 3 CTAs per SM fit
 constexpr int kMaxChunks = (kCap + kChunk - 1) / kChunk;  // transmittance checkpoints per pixel
 constexpr int kThreads = 256;
 constexpr uint32_t kNSeg = 16;   // bezier_backward.wgsl:52
@@ -155,10 +155,11 @@ struct RasterArgs {
   float* out_rgbd;
   uint32_t n, w, h, tiles_x, num_tiles;
   Uni u;
+  float* ckpt;  // per (view, tile): T of every pixel at the start of each chunk, [kMaxChunks][kThreads]
 };
 
 constexpr size_t kRasterSmem = sizeof(uint32_t) * kChunk + sizeof(float) * kChunk * (kRecF + kRecB) +
-                               sizeof(float) * kMaxChunks * kThreads + sizeof(float) * 2 * kChunk * kThreads +
+                               sizeof(float) * 2 * kChunk * kThreads +
                                kChunk * kThreads + sizeof(int32_t) * kChunk * 18 + sizeof(float) * kChunk;
 
 // 16-segment closest-point walk (bezier_backward.wgsl:213-230)
@@ -218,13 +219,12 @@ __device__ __forceinline__ float tex_dot(const float* rgba, int32_t x, int32_t y
   return t.x * kx + t.y * ky + t.z * kz;
 }
 
-__global__ void __launch_bounds__(kThreads) k_bz_raster(RasterArgs A) {
+__global__ void __launch_bounds__(kThreads, 3) k_bz_raster(RasterArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* ids = reinterpret_cast<uint32_t*>(smem);
   float* sf = reinterpret_cast<float*>(smem + sizeof(uint32_t) * kChunk);  // [kChunk][kRecF]
   float* sb = sf + kChunk * kRecF;                                          // [kChunk][kRecB]
-  float* ckpt = sb + kChunk * kRecB;                                        // [kMaxChunks][kThreads]
-  float* sA = ckpt + kMaxChunks * kThreads;                                 // [kChunk][kThreads]
+  float* sA = sb + kChunk * kRecB;                                          // [kChunk][kThreads]
   float* sT = sA + kChunk * kThreads;
   uint8_t* sK = reinterpret_cast<uint8_t*>(sT + kChunk * kThreads);         // [kChunk][kThreads]
   int32_t* gacc = reinterpret_cast<int32_t*>(sK + kChunk * kThreads);       // [kChunk][18]
@@ -237,6 +237,10 @@ __global__ void __launch_bounds__(kThreads) k_bz_raster(RasterArgs A) {
   const float aspect = (float)A.w / (float)A.h;
   const float ppx = bin::pixel_px(px, A.w, aspect), ppy = bin::pixel_py(py, A.h);
   const uint32_t key = v * A.num_tiles + ty * A.tiles_x + tx;
+  // the checkpoints are this CTA's own (32 KB-scale, global memory kept in L2
+  // between the forward's write and the backward's read; in shared memory they
+  // held residency at two CTAs per SM, here three fit)
+  float* ckpt = A.ckpt + (size_t)key * kMaxChunks * kThreads;
   const uint32_t start = A.rstart[key];
   const uint32_t len = min(A.rend[key] - start, kCap);
   const uint32_t nch = (len + kChunk - 1) / kChunk;
@@ -1003,6 +1007,7 @@ struct nps_bezier_opt {
   DevBuf own[5];
   const float* tex[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // target, target depth, bg, bg depth, normal
   DevBuf fwd, bwd, counts, offsets, rects, total, keys, vals, ranges, tabs;
+  DevBuf ckbuf;  // raster checkpoints per (view, tile)
   SortWork sw;
   uint32_t pair_cap = 0;
   nps_stats stats{};
@@ -1077,7 +1082,7 @@ int nps_bezier_opt_destroy(nps_bezier_opt* o) {
   cudaSetDevice(o->ctx->device);
   cudaStreamSynchronize(o->ctx->stream);
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->lacc, &o->pixel_loss, &o->dead, &o->stat,
-                    &o->views, &o->own[0], &o->own[1], &o->own[2], &o->own[3], &o->own[4], &o->fwd, &o->bwd,
+                    &o->views, &o->own[0], &o->own[1], &o->own[2], &o->own[3], &o->own[4], &o->fwd, &o->bwd, &o->ckbuf,
                     &o->counts, &o->offsets, &o->rects, &o->total, &o->keys, &o->vals, &o->ranges, &o->tabs,
                     &o->sw.hist, &o->sw.partial, &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt, &o->r_rec, &o->r_counts,
                     &o->r_offsets, &o->r_rects, &o->r_total, &o->r_cam, &o->r_keys, &o->r_vals, &o->r_ranges,
@@ -1302,6 +1307,8 @@ int nps_bezier_opt_backward(nps_bezier_opt* o, float* out_rgbd) {
   ra.tiles_x = tiles_x;
   ra.num_tiles = num_tiles;
   ra.u = o->uni;
+  NPS_TRY(o->ckbuf.ensure(sizeof(float) * (size_t)tiles_x * tiles_y * nv * bz::kMaxChunks * bz::kThreads));
+  ra.ckpt = o->ckbuf.as<float>();
   NPS_CUDA(cudaFuncSetAttribute(bz::k_bz_raster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bz::kRasterSmem));
   bz::k_bz_raster<<<dim3(tiles_x, tiles_y, nv), bz::kThreads, bz::kRasterSmem, s>>>(ra);
   NPS_CHECK_LAUNCH();

@@ -381,17 +381,17 @@ struct RasterArgs {
   int32_t* grads;
   float* out_rgbd;
   uint32_t* err;  // bounded waits that gave up (the output of such a tile is not written)
+  float* ckpt;    // per (view, tile): T of every pixel at the start of each chunk, [kNumChunks][kThreads]
   uint32_t n, w, h, tiles_x, num_tiles;
 };
 
 constexpr uint32_t kNumChunks = kCap / kChunk;
 constexpr uint32_t kFwdBytes = sizeof(float) * kFwd, kBwdBytes = sizeof(float) * kBwd;
 
-// Shared memory of one k_raster CTA (dynamic, ~82 KB: two CTAs per SM).
+// Shared memory of one k_raster CTA (dynamic, ~50 KB: four CTAs per SM).
 struct __align__(16) RasterSmem {
   float fwd[2][kChunk][kFwd];          // staged forward records (double-buffered)
   float bwd[2][kChunk][kBwd];          // staged backward records
-  float ckpt[kNumChunks][kThreads];    // T of every pixel at the start of each chunk
   float tprev[kChunk][kThreads];       // T before each pair of the chunk being differentiated
   int32_t gacc[2][kChunk][16];         // per-chunk CTA sums of the i32 gradient terms
   uint32_t ids[3][kChunk];             // splat index of each staged record
@@ -471,7 +471,10 @@ __device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval&
 // Records are staged 32 at a time by warp 0 with bulk copies completing on
 // an mbarrier, double-buffered (the next chunk lands while this one is
 // composited); the forward stores T at every chunk start, and the backward
-// walks the chunks in reverse, replaying each from its checkpoint.
+// walks the chunks in reverse, replaying each from its checkpoint.  The
+// checkpoints (32 KB per CTA) live in global memory, where they stay in L2
+// between the forward's write and the backward's read: kept in shared memory
+// they held residency at two CTAs per SM, here four fit (64 registers).
 //
 // Exact skips (results identical to evaluating every pair):
 //  * a warp whose 32 pixels all reached T == 0 stops compositing: a pair
@@ -482,7 +485,7 @@ __device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval&
 //    only its shape regularisers: with T_prev == 0 every other term is a
 //    product with a zero factor, which is 0 or NaN, and i32() maps both to 0;
 //    so only dL/dT, d_shape_a and d_shape_b are evaluated and summed.
-__global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RasterSmem& S = *reinterpret_cast<RasterSmem*>(smem_raw);
   constexpr unsigned kFull = 0xffffffffu;
@@ -500,6 +503,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
   const uint32_t nch = (len + kChunk - 1) / kChunk;
   const float* fwd_v = a.fwd + (size_t)v * a.n * kFwd;
   const float* bwd_v = a.bwd + (size_t)v * a.n * kBwd;
+  float* ckpt = a.ckpt + (size_t)key * kNumChunks * kThreads;  // this CTA's own: written, then read back
   for (uint32_t e = tid; e < 2 * kChunk * 16; e += kThreads) (&S.gacc[0][0][0])[e] = 0;
   if (tid == 0) {
     bulk::mbar_init(&S.bar[0], 1);
@@ -550,7 +554,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
       ++issued;
     }
     wait_batch(c);
-    S.ckpt[c][tid] = T;
+    ckpt[c * kThreads + tid] = T;
     if (!wdone) {
       const uint32_t cnt = min((uint32_t)kChunk, len - c * kChunk);
       const uint32_t b = c & 1u;
@@ -616,7 +620,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_raster(RasterArgs a) {
     wait_batch(q);
     const uint32_t cnt = min((uint32_t)kChunk, len - cc * kChunk);
     // replay the chunk forward from its checkpoint: bit-identical Ts
-    const float T0 = S.ckpt[cc][tid];
+    const float T0 = ckpt[cc * kThreads + tid];
     const bool zero_chunk = __all_sync(kFull, T0 == 0.0f);
     if (!zero_chunk) {
       float Tc = T0;
@@ -1080,6 +1084,7 @@ struct nps_splat_opt {
   // work
   DevBuf fwd, bwd, counts, kept, offsets, rects, total, keys, vals, ranges, tabs, dead, stat, tstat;
   DevBuf grid, cutoff, tile_len;  // cap-aware binning
+  DevBuf ckbuf;                   // raster checkpoints: 32 KB per (view, tile)
   SortWork sw;
   uint32_t pair_cap = 0;
   uint32_t last_ranges = 0;  // (view, tile) entries of the last backward's ranges
@@ -1155,7 +1160,7 @@ int nps_splat_opt_destroy(nps_splat_opt* o) {
   cudaStreamSynchronize(o->ctx->stream);
   for (DevBuf* b : {&o->params, &o->grads, &o->am, &o->av, &o->gacc, &o->views, &o->tgt_rgba_own,
                     &o->tgt_depth_own, &o->fwd, &o->bwd, &o->counts, &o->kept, &o->offsets, &o->rects, &o->total,
-                    &o->grid, &o->cutoff, &o->tile_len,
+                    &o->grid, &o->cutoff, &o->tile_len, &o->ckbuf,
                     &o->keys, &o->vals, &o->ranges, &o->tabs, &o->dead, &o->stat, &o->tstat, &o->sw.hist,
                     &o->sw.partial, &o->sw.lookback, &o->sw.keys_alt, &o->sw.vals_alt})
     b->release();
@@ -1351,6 +1356,8 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
   ra.grads = o->grads.as<int32_t>();
   ra.out_rgbd = out_rgbd;
   ra.err = total + 1;
+  NPS_TRY(o->ckbuf.ensure(sizeof(float) * (size_t)num_tiles * nv * compat::kNumChunks * compat::kThreads));
+  ra.ckpt = o->ckbuf.as<float>();
   ra.n = n;
   ra.w = o->w;
   ra.h = o->h;
