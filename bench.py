@@ -185,12 +185,13 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         st.set_targets(tg, borrow=True)
         sched = view_schedule(args.warmup + args.steps + 4)
-        tuned = None
+        tuned = fixed = None
         if args.raster:
             # a fixed tile and raster variants: tile,fwd form,ppt,stage,bwd form,ppt,stage
             r7 = [int(x) for x in args.raster.split(",")]
             st.set_tile(r7[0])
             st.set_raster(r7[1:4], r7[4:7])
+            fixed = dict(zip(("tile", "fwd_form", "fwd_ppt", "fwd_stage", "bwd_form", "bwd_ppt", "bwd_stage"), r7))
         elif not args.no_autotune:
             # tile size and raster variants timed on this workload
             st.set_views(vp[sched[0]], vpi[sched[0]], sched[0])
@@ -260,7 +261,8 @@ def run_ours(args, rank, world):
         h2d = VIEWS * HEIGHT * WIDTH * 4 * 4 + VIEWS * (32 * 4 + 4)
         d2h = 3 * 4
         st.close()
-        trained = trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush) if args.trained_steps > 0 else None
+        trained = (trained_state_leg(args, dev, stream, vp, vpi, tg, tuned if tuned is not None else fixed, flush,
+                                     retune=tuned is not None) if args.trained_steps > 0 else None)
     return dict(tuned=tuned, ms_total=float(np.sum(times)), times=times, stages=stages, pairs=int(np.mean(pairs)),
                 trained=trained,
                 graph_kernels=graph_kernels,
@@ -357,7 +359,7 @@ def run_sharded(args, rank, world):
                 d2h=4 * world, loss=[loss_last])
 
 
-def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush):
+def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush, retune=True):
     """The same step timed at a trained state: a fresh student of the same
     seed fitted for args.trained_steps steps with the plain ADC schedule
     (every 100 steps from 500 to 15k; the Gaussian count then differs from
@@ -377,7 +379,7 @@ def trained_state_leg(args, dev, stream, vp, vpi, tg, tuned, flush):
             adc=AdcSchedule(stop=min(15000, args.trained_steps)))
     sched = view_schedule(args.warmup + args.steps)
     retuned = None
-    if tuned is not None:
+    if tuned is not None and retune:
         # the autotuner again, on the trained state (larger, more opaque Gaussians)
         tr.set_views(vp[sched[0]], vpi[sched[0]], sched[0])
         retuned = tr.autotune()

@@ -1142,8 +1142,11 @@ __device__ __forceinline__ bool pix_bwd_pair(PixBwd& s, const float4& a, const f
 // that meet its strip and that some of its pixels reached, then walks them in
 // reverse order.  Per-pair sums go to shared memory and then to the (view,
 // Gaussian) records with global atomics.  PPT is the autotuned variant.
+// With 1 or 2 pixels per thread at most 64 registers (1024 / (256 / PPT) blocks of 256 / PPT threads,
+// 32 warps per SM): eight 128-thread blocks per SM instead of six cut the backward by 8% at the
+// benchmark workload.  4 pixels per thread would spill under that bound and keep their registers.
 template <int PPT, int SPS, bool kOrd>
-__global__ void __launch_bounds__(256 / PPT) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+__global__ void __launch_bounds__(256 / PPT, PPT <= 2 ? 1024 / (256 / PPT) : 1) k_bwd2(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                     const uint32_t* __restrict__ rstart,
                                                     const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                     uint32_t tiles_x, uint32_t num_tiles, float3 bg,
