@@ -418,9 +418,11 @@ __device__ __forceinline__ void stage_batch(const Rec* __restrict__ recs, const 
 // threads per 16 x 16 tile, a warp covers a 16 x 2·PPT strip, records staged
 // SB = SPS · 256 / PPT at a time.  (PPT, SB) is the autotuned variant.
 // kOrd: a 1D grid whose block b takes work item order[b] (longest tile
-// lists first), else the grid is (tiles x, tiles y, views).
+// lists first), else the grid is (tiles x, tiles y, views).  With 1 or 2
+// pixels per thread at most 51 registers: ten 128-thread blocks per SM (the
+// shared-memory limit) instead of nine.
 template <int PPT, int SPS, bool kOrd>
-__global__ void __launch_bounds__(256 / PPT) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
+__global__ void __launch_bounds__(256 / PPT, PPT <= 2 ? 1280 / (256 / PPT) : 1) k_fwd(const Rec* __restrict__ recs, const uint32_t* __restrict__ vals,
                                                    const uint32_t* __restrict__ rstart,
                                                    const uint32_t* __restrict__ rend, uint32_t W, uint32_t H,
                                                    uint32_t tiles_x, uint32_t num_tiles, float3 bg,
@@ -700,7 +702,8 @@ __global__ void __launch_bounds__(256) k_ssim_fwd2(const float4* __restrict__ im
   }
 }
 
-__global__ void __launch_bounds__(256, 3) k_ssim_bwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
+// four blocks per SM (at most 64 registers; five fit in shared memory)
+__global__ void __launch_bounds__(256, 4) k_ssim_bwd2(const float4* __restrict__ img, const float4* __restrict__ tgt,
                                                    const uint32_t* __restrict__ tgt_ids,
                                                    const float* __restrict__ maps, uint32_t W, uint32_t H,
                                                    float lambda, float inv_norm, float4* __restrict__ dimg) {
