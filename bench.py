@@ -41,8 +41,8 @@ S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, o
 # Warp instructions issued by one launch of each raster kernel (smsp__inst_executed.sum) in a 1-pass
 # ncu capture of this workload with the variant named, and that launch's pair count: scaled to a
 # launch by its pair count.  Key: (stage, form, pixels per thread, records per stage) at 16 x 16 tiles.
-RASTER_INST = {("raster_fwd", 2, 2, 128): (543_132_676, 11_433_806),
-               ("raster_bwd", 2, 2, 128): (1_137_379_653, 11_433_806)}
+RASTER_INST = {("raster_fwd", 2, 2, 128): (548_836_695, 11_433_806),
+               ("raster_bwd", 2, 2, 128): (1_183_662_764, 11_433_806)}
 SMS, ISSUE_PER_SM_CLK = 148, 4  # B200: 148 SMs, four warp schedulers each issuing one instruction per clock
 
 
