@@ -107,7 +107,10 @@ int nps_splat_opt_dispatch(nps_splat_opt* opt);
  * computes (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device).
  * A backward whose raster's bounded record-staging wait or sort look-back
  * gave up leaves invalid gradients; the next backward reports it with
- * NPS_ERR_TIMEOUT (and runs nothing further). */
+ * NPS_ERR_TIMEOUT (and runs nothing further).  Work memory grows with the
+ * views and tiles: besides the pair lists, 32 KB of transmittance
+ * checkpoints per (view, 16 x 16 tile) (655 MB for 8 views at 800 x 800);
+ * an allocation that fails returns NPS_ERR_NOMEM. */
 int nps_splat_opt_backward(nps_splat_opt* opt, float* out_rgbd_device);
 int nps_splat_opt_step(nps_splat_opt* opt);
 int nps_splat_opt_adc(nps_splat_opt* opt);
@@ -213,7 +216,9 @@ int nps_bezier_opt_set_target(nps_bezier_opt* opt, const float* target_rgba, con
  * views, Adam step (gradients / (w*h)), ADC every adc_period calls. */
 int nps_bezier_opt_dispatch(nps_bezier_opt* opt);
 /* The stages of dispatch separately; backward optionally writes the composite
- * (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device). */
+ * (num_views*h*w*4: r, g, b, reciprocal depth) to out_rgbd (device).  Its
+ * work memory includes 37 KB of transmittance checkpoints per (view, 16 x 16
+ * tile). */
 int nps_bezier_opt_backward(nps_bezier_opt* opt, float* out_rgbd_device);
 int nps_bezier_opt_step(nps_bezier_opt* opt);
 int nps_bezier_opt_adc(nps_bezier_opt* opt);
