@@ -174,6 +174,12 @@ typedef struct nps_stats {
                               that gave up (raster record staging, sort look-back) */
 } nps_stats;
 int nps_splat_opt_stats(nps_splat_opt* opt, nps_stats* out);
+/* Bound of the backward raster's waits for its staged records (polls of the
+ * mbarrier; 0 = the default, 2^22) and, for tests, one batch of tile 0 (view
+ * 0) whose copies are never issued (0xffffffff = none), so that its wait runs
+ * out on a normal input: the raster's CTA for that tile stops, and the next
+ * backward returns NPS_ERR_TIMEOUT.  No counterpart in the reference. */
+int nps_splat_opt_set_wait_guard(nps_splat_opt* opt, uint32_t spin_limit, uint32_t stall_batch);
 /* Sets the manager's stepCount (GpuSplatOptimizerManager.ts:380, dispatch()
  * calls so far; ADC runs when it reaches a multiple of 25): a restored
  * checkpoint continues the ADC schedule. */

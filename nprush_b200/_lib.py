@@ -122,6 +122,7 @@ SIGNATURES = {
     "nps_gs_set_tile": [P, U32],
     "nps_gs_get_raster": [P, P],
     "nps_gs_autotune_raster": [P, ctypes.c_char_p, P, P],
+    "nps_splat_opt_set_wait_guard": [P, U32, U32],
     "nps_gs_set_sort_guard": [P, U32, U32],
     "nps_gs_autotune": [P, ctypes.c_char_p, P, P],
     "nps_gs_adc_features": [P, F32, F32, F32, F32, P, P, P],

@@ -382,6 +382,8 @@ struct RasterArgs {
   float* out_rgbd;
   uint32_t* err;  // bounded waits that gave up (the output of such a tile is not written)
   float* ckpt;    // per (view, tile): T of every pixel at the start of each chunk, [kNumChunks][kThreads]
+  uint32_t spin_limit;   // polls of a staging mbarrier before the wait gives up
+  uint32_t stall_batch;  // tests: the batch of tile 0 whose copies are never issued (0xffffffff = none)
   uint32_t n, w, h, tiles_x, num_tiles;
 };
 
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
     const uint32_t cnt = min((uint32_t)kChunk, len - c * kChunk);
     const uint32_t b = q & 1u;
     if (lane == 0) bulk::mbar_expect_tx(&S.bar[b], cnt * (both ? kFwdBytes + kBwdBytes : kFwdBytes));
-    if (lane < cnt) {
+    if (lane < cnt && !(key == 0 && q == a.stall_batch)) {
       bulk::fence_proxy_async();  // the buffer was last read through the generic proxy
       const uint32_t id = a.vals[start + c * kChunk + lane];
       S.ids[q % 3][lane] = id;
@@ -531,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
     }
   };
   auto wait_batch = [&](uint32_t q) {
-    if (!bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u) && lane == 0) {
+    if (!bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u, a.spin_limit) && lane == 0) {
       atomicAdd(a.err, 1u);
       S.abort = 1;
     }
@@ -747,7 +749,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
   // (at most the last two staged) before the CTA's shared memory is released
   if (tid == 0)
     for (uint32_t q = issued >= 2 ? issued - 2 : 0; q < issued; ++q)
-      (void)bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u);
+      (void)bulk::mbar_wait(&S.bar[q & 1u], (q >> 1) & 1u, a.spin_limit);
 }
 
 // splat_step.wgsl:32-106, one thread per splat.
@@ -1088,6 +1090,7 @@ struct nps_splat_opt {
   SortWork sw;
   uint32_t pair_cap = 0;
   uint32_t last_ranges = 0;  // (view, tile) entries of the last backward's ranges
+  uint32_t spin_limit = 1u << 22, stall_batch = 0xffffffffu;  // raster staging waits (nps_splat_opt_set_wait_guard)
   bool pairs_from_ranges = true;  // the last backward kept every overlapped pair
   uint32_t kept_pairs = 0;
   nps_stats stats{};
@@ -1358,6 +1361,8 @@ int nps_splat_opt_backward(nps_splat_opt* o, float* out_rgbd) {
   ra.err = total + 1;
   NPS_TRY(o->ckbuf.ensure(sizeof(float) * (size_t)num_tiles * nv * compat::kNumChunks * compat::kThreads));
   ra.ckpt = o->ckbuf.as<float>();
+  ra.spin_limit = o->spin_limit;
+  ra.stall_batch = o->stall_batch;
   ra.n = n;
   ra.w = o->w;
   ra.h = o->h;
@@ -1438,6 +1443,13 @@ int nps_splat_opt_buffers(nps_splat_opt* o, float** splats, int32_t** grads, flo
 int nps_splat_opt_set_step_count(nps_splat_opt* o, uint32_t count) {
   NPS_TRY(check_opt(o));
   o->step_count = count;
+  return NPS_OK;
+}
+
+int nps_splat_opt_set_wait_guard(nps_splat_opt* o, uint32_t spin_limit, uint32_t stall_batch) {
+  NPS_TRY(check_opt(o));
+  o->spin_limit = spin_limit ? spin_limit : 1u << 22;
+  o->stall_batch = stall_batch;
   return NPS_OK;
 }
 

@@ -219,6 +219,12 @@ class GpuSplatOptimizerManager:
                     adc_clones=st.adc_clones, step_count=st.step_count, pairs_kept=st.reserved[1],
                     timeouts=st.reserved[2])
 
+    def set_wait_guard(self, spin_limit: int = 0, stall_batch: int = 0xFFFFFFFF):
+        """Polls before a raster staging wait gives up (0: the default);
+        stall_batch (tests) is a batch of tile 0 whose copies are never
+        issued, so its wait runs out."""
+        call("nps_splat_opt_set_wait_guard", self._h, int(spin_limit), int(stall_batch))
+
     def set_step_count(self, count: int):
         """stepCount (dispatch() calls so far; ADC every 25th)."""
         call("nps_splat_opt_set_step_count", self._h, int(count))

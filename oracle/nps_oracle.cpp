@@ -532,11 +532,13 @@ extern "C" {
 //   textures H x W x 4 (target, background, normal); depths H x W (.r)
 //   grads_q  N x 18 i32 (+=); grads_f N x 18 unquantised (+=, may be null)
 //   loss_accum N (+=, the shader's non-atomic RMW), pixel_loss (+=, indexed y*W+x)
+//   terms    N (+=, may be null): (pixel, curve) backward terms (alpha >= 0.001)
+//            each curve's gradient sums
 int orc_bezier_backward(const float* beziers, uint32_t n, const float* vp, const float* uni,
                         const float* tgt_rgba, const float* tgt_depth, const float* bg_rgba,
                         const float* bg_depth, const float* normal_rgba, uint32_t w, uint32_t h,
                         int32_t* grads_q, float* grads_f, float* loss_accum, int32_t* pixel_loss,
-                        float* out_rgbd, uint32_t* tile_count) {
+                        float* out_rgbd, uint32_t* tile_count, uint32_t* terms) {
   const float aspect = (float)w / (float)h;
   const uint32_t tiles_x = (w + 15) / 16, tiles_y = (h + 15) / 16;
   const float mode = uni[0], max_width = uni[1], bg_penalty = uni[4];
@@ -661,6 +663,7 @@ int orc_bezier_backward(const float* beziers, uint32_t n, const float* vp, const
             float a = alphas[idx];
             if (a < 0.001f) continue;
             uint32_t i = list[idx];
+            if (terms) ++terms[i];
             const float* b = beziers + 20 * (size_t)i;
             const PC* q = &pcs[4 * i];
             float width = std::fmax(b[3], 0.001f), soft = std::fmax(b[7], 0.001f), opacity = b[19];

@@ -92,7 +92,7 @@ def splat_adc(splats, m, v, adam_t, grad_accum):
 
 # ------------------------------------------------------------ compat beziers
 def bezier_backward(beziers, vp, uni, tgt_rgba, tgt_depth, bg_rgba, bg_depth, normal_rgba,
-                    grads_q=None, loss_accum=None, pixel_loss=None, want_float=True, want_image=True):
+                    grads_q=None, loss_accum=None, pixel_loss=None, want_float=True, want_image=True, terms=None):
     beziers = _f32(beziers)
     n = beziers.shape[0]
     h, w = tgt_depth.shape
@@ -102,11 +102,12 @@ def bezier_backward(beziers, vp, uni, tgt_rgba, tgt_depth, bg_rgba, bg_depth, no
     pl = np.zeros(512 * 512, np.int32) if pixel_loss is None else pixel_loss
     img = np.zeros((h, w, 4), np.float32) if want_image else None
     tc = np.zeros(((h + 15) // 16, (w + 15) // 16), np.uint32)
+    tm = np.zeros(n, np.uint32) if terms is None else terms
     lib().orc_bezier_backward(_p(beziers, F), n, _p(_f32(vp), F), _p(_f32(uni), F), _p(_f32(tgt_rgba), F),
                               _p(_f32(tgt_depth), F), _p(_f32(bg_rgba), F), _p(_f32(bg_depth), F),
                               _p(_f32(normal_rgba), F), w, h, _p(gq, I), _p(gf, F), _p(la, F), _p(pl, I),
-                              _p(img, F), _p(tc, U))
-    return dict(grads_q=gq, grads_f=gf, loss_accum=la, pixel_loss=pl, image=img, tile_count=tc)
+                              _p(img, F), _p(tc, U), _p(tm, U))
+    return dict(grads_q=gq, grads_f=gf, loss_accum=la, pixel_loss=pl, image=img, tile_count=tc, terms=tm)
 
 
 def bezier_step(beziers, grads, m, v, adam_t, pixel_count, no_kill, grad_accum, vp, uni):

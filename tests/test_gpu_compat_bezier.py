@@ -2,8 +2,10 @@
 (oracle/nps_oracle.cpp, pinned bit-exact to the reference's own
 bezier_{backward,step,adc}.wgsl by test_oracle_pin.py).
 
-Tolerances: composite 1e-5 absolute; i32 gradient sums relative L2 <= 1e-4
-(per-pair truncation, as for splats); pixel_loss (per-pixel i32, one term per
+Tolerances: composite 1e-5 absolute; i32 gradient sums (per-pair truncation,
+as for splats) bit-exact: the curve kernels use only +, -, *, / and sqrt,
+each correctly rounded and unfused (--fmad=false), as the oracle does, and
+integer sums do not depend on their order; pixel_loss (per-pixel i32, one term per
 pixel) within 1 unit or 1e-4 relative; loss_accum 1e-4 relative (the reference
 adds it with a non-atomic read-modify-write, a race; here it is an atomic
 float sum); Adam step bit-exact; ADC bit-exact except the clone jitter (sinf).
@@ -51,10 +53,14 @@ def test_backward_matches_oracle(cls, n, w, h, mode, max_width, bgp, seed):
     ref = orc.bezier_backward(b, vp, uni6(mode, max_width, 0, 0, bgp), tgt, depth, bg, bgd, nrm,
                               loss_accum=la0.copy())
     np.testing.assert_allclose(img.cpu().numpy()[0], ref["image"], atol=1e-5, rtol=0)
+    assert ref["terms"].sum() > 0
     g, r = st["grads"].astype(np.float64), ref["grads_q"].astype(np.float64)
     assert np.abs(r).sum() > 0
     rel = np.linalg.norm(g - r) / np.linalg.norm(r)
     assert rel <= 1e-4, rel
+    diff = np.abs(g - r)
+    t = ref["terms"].astype(np.float64)[:, None]
+    assert (diff == 0).all(), ((diff != 0).mean(), (diff / (t + 1)).max())
     pl, rpl = st["pixel_loss"].astype(np.int64), ref["pixel_loss"].astype(np.int64)
     assert (np.abs(pl - rpl) <= np.maximum(1, 1e-4 * np.abs(rpl))).all()
     np.testing.assert_allclose(st["loss_accum"], ref["loss_accum"], rtol=1e-4, atol=1e-6)

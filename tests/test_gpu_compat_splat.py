@@ -151,6 +151,39 @@ def test_dense_scene_cap_aware_binning(mgr_cls):
     m.close()
 
 
+def test_raster_staging_timeout_is_reported(mgr_cls):
+    """A staging wait that runs out (tile 0's first batch never issued, 1000
+    polls): the raster's CTA for that tile stops and releases nothing in
+    flight, the next backward reports NPS_ERR_TIMEOUT, and with the default
+    bound the optimiser then matches the oracle again."""
+    from nprush_b200._lib import NpsError
+    n, w, h = 600, 48, 32
+    s = splat_scene(n, 31)
+    vp, vpi = camera(w, h)
+    tgt, depth = targets(w, h, 32)
+    ref = orc.splat_backward(s, vp, vpi, tgt, depth)
+    assert ref["tile_count"][0, 0] > 32  # tile 0 stages more than one batch
+    m = mgr_cls(n, init=s)
+    m.write_splat_vp_matrix(vp, vpi)
+    m.set_backward_target(tgt, depth, w, h)
+    m.set_wait_guard(1000, 0)
+    m.backward()
+    m.sync()
+    with pytest.raises(NpsError) as e:
+        m.backward()
+    assert e.value.code == -5  # NPS_ERR_TIMEOUT
+    assert m.stats()["timeouts"] > 0
+    m.set_wait_guard()
+    m.write_state(grads=np.zeros((n, 16), np.int32))
+    img = torch.zeros((1, h, w, 4), device="cuda")
+    m.backward(out_rgbd=img)
+    st = m.read_state()
+    np.testing.assert_allclose(img.cpu().numpy()[0], ref["image"], atol=1e-5, rtol=0)
+    rel, ok, worst, exact = grad_close(st["grads"], ref["grads_q"], ref["terms"])
+    assert rel <= 1e-4 and ok, (rel, worst, exact)
+    m.close()
+
+
 def test_step_bit_exact(mgr_cls):
     n = 3000
     rng = np.random.default_rng(3)
