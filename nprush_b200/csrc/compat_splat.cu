@@ -159,16 +159,31 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splat
   f4[0] = make_float4(scx, scy, A, B);
   f4[1] = make_float4(C, s[13], s[14], s[7]);
   f4[2] = make_float4(s[4], s[5], s[6], depth);
-  f4[3] = make_float4(0.5f * s[13], 0.0f, 0.0f, 0.0f);  // a / 2 for pow(r, a) = 2^((a / 2) log2 r^2)
+  // a / 2 for pow(r, a) = 2^((a / 2) log2 r^2); the shape regularisers' gradients (splat_backward.wgsl:427-428)
+  f4[3] = make_float4(0.5f * s[13], 0.005f * 2.0f * (s[13] - 6.0f), 0.005f * 2.0f * (s[14] - 0.3f), 0.0f);
   float4* b4 = reinterpret_cast<float4*>(bwd + (size_t)g * kBwd);
-  b4[0] = make_float4(W, clip.x, clip.y, sx);
-  b4[1] = make_float4(sy, sz, m0x, m0y);
-  b4[2] = make_float4(m1x, m1y, m2x, m2y);
-  b4[3] = make_float4(ax.x, ax.y, ay.x, ay.y);
-  b4[4] = make_float4(az.x, az.y, s[0], s[1]);
-  b4[5] = make_float4(s[2], s[8], s[9], s[10]);
-  b4[6] = make_float4(s[11], 0.0f, 0.0f, 0.0f);
-  b4[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // pixel-independent factors of the backward's screen-space chain rule
+  // (splat_backward.wgsl:380-398), per world axis: d screen / d pos, and the
+  // depth term's vp[ax][3] * DEPTH_NEAR / w^2 — the same expressions, in the
+  // same order, as a per-pixel evaluation would give
+  const float w2 = W * W;
+  const float d_depth_d_w = 0.1f / (W * W);
+  float dsx[3], dsy[3], kdep[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float vp0 = vp[k * 4 + 0], vp1 = vp[k * 4 + 1], vp3 = vp[k * 4 + 3];
+    dsx[k] = aspect * (vp0 * W - clip.x * vp3) / w2;
+    dsy[k] = (vp1 * W - clip.y * vp3) / w2;
+    kdep[k] = vp3 * d_depth_d_w;
+  }
+  b4[0] = make_float4(W, sx, sy, sz);
+  b4[1] = make_float4(m0x, m0y, m1x, m1y);
+  b4[2] = make_float4(m2x, m2y, ax.x, ax.y);
+  b4[3] = make_float4(ay.x, ay.y, az.x, az.y);
+  b4[4] = make_float4(s[0], s[1], s[2], s[8]);
+  b4[5] = make_float4(s[9], s[10], s[11], dsx[0]);
+  b4[6] = make_float4(dsx[1], dsx[2], dsy[0], dsy[1]);
+  b4[7] = make_float4(dsy[2], kdep[0], kdep[1], kdep[2]);
 
   // binning AABB, splat_backward.wgsl:157-190 (same arithmetic, cov00/cov11
   // recomputed there without cov01: identical values)
@@ -398,7 +413,6 @@ struct __align__(16) RasterSmem {
   int32_t gacc[2][kChunk][16];         // per-chunk CTA sums of the i32 gradient terms
   uint32_t ids[3][kChunk];             // splat index of each staged record
   uint64_t bar[2];                     // one mbarrier per record buffer
-  float vpm[16];
   int abort;
 };
 
@@ -451,7 +465,7 @@ struct PairCommon {
 __device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval& e, float T_prev, float dCr,
                                                   float dCg, float dCb, float dD, float& dT_C, float& dT_D) {
   const float cr = f[8], cg = f[9], cb = f[10], opacity = f[7], depth = f[11];
-  const float shape_a = f[5], shape_b = f[6], al = e.al;
+  const float shape_b = f[6], al = e.al;
   const float tcr = T_prev * cr, tcg = T_prev * cg, tcb = T_prev * cb;
   const float da_C = dT_C * (-T_prev) + (dCr * tcr + dCg * tcg + dCb * tcb);
   const float da_D = dT_D * (-T_prev) + dD * T_prev * depth;
@@ -464,8 +478,8 @@ __device__ __forceinline__ PairCommon pair_common(const float* f, const PixEval&
   const float logr = e.lg * kHalfLn2;
   p.d_shape_a = e.above ? p.d_power * (-shape_b * e.rpa * logr) : 0.0f;
   p.d_shape_b = e.above ? p.d_power * (-e.rpa) : 0.0f;
-  p.d_shape_a += 0.005f * 2.0f * (shape_a - 6.0f);
-  p.d_shape_b += 0.005f * 2.0f * (shape_b - 0.3f);
+  p.d_shape_a += f[13];  // 0.005 * 2 * (shape_a - 6), per splat (k_project)
+  p.d_shape_b += f[14];  // 0.005 * 2 * (shape_b - 0.3)
   return p;
 }
 
@@ -498,7 +512,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
   const bool inside = px < a.w && py < a.h;
   const float aspect = (float)a.w / (float)a.h;
   const float ppx = pixel_px(px, a.w, aspect), ppy = pixel_py(py, a.h);
-  if (tid < 16) S.vpm[tid] = a.views[32 * (size_t)v + tid];
   const uint32_t key = v * a.num_tiles + ty * a.tiles_x + tx;
   const uint32_t start = a.rstart[key];
   const uint32_t len = min(a.rend[key] - start, kCap);
@@ -660,11 +673,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
         const float* bw = S.bwd[b][k];
         const float al = e.al;
         const float shape_a = f[5], shape_b = f[6];
-        const float Wc = bw[0], clip_x = bw[1], clip_y = bw[2], sx = bw[3], sy = bw[4], sz = bw[5];
-        const float m0x = bw[6], m0y = bw[7], m1x = bw[8], m1y = bw[9], m2x = bw[10], m2y = bw[11];
-        const float axx = bw[12], axy = bw[13], ayx = bw[14], ayy = bw[15], azx = bw[16], azy = bw[17];
-        const float pos0 = bw[18], pos1 = bw[19], pos2 = bw[20];
-        const float qw = bw[21], qx = bw[22], qy = bw[23], qz = bw[24];
+        const float Wc = bw[0], sx = bw[1], sy = bw[2], sz = bw[3];
+        const float m0x = bw[4], m0y = bw[5], m1x = bw[6], m1y = bw[7], m2x = bw[8], m2y = bw[9];
+        const float axx = bw[10], axy = bw[11], ayx = bw[12], ayy = bw[13], azx = bw[14], azy = bw[15];
+        const float pos0 = bw[16], pos1 = bw[17], pos2 = bw[18];
+        const float qw = bw[19], qx = bw[20], qy = bw[21], qz = bw[22];
         const float TA = T_prev * al;
         const float dColr = dCr * TA, dColg = dCg * TA, dColb = dCb * TA;
         const float d_depth = dD * T_prev * al;
@@ -685,16 +698,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
         const float d_sx = dm0x * axx + dm0y * axy;
         const float d_sy = dm1x * ayx + dm1y * ayy;
         const float d_sz = dm2x * azx + dm2y * azy;
-        const float w2 = Wc * Wc;
         float dpos[3], daw[3], dbw[3], dcw[3];
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-          const float vp0 = S.vpm[ax * 4 + 0], vp1 = S.vpm[ax * 4 + 1], vp3 = S.vpm[ax * 4 + 3];
-          const float ds_dx = aspect * (vp0 * Wc - clip_x * vp3) / w2;
-          const float ds_dy = (vp1 * Wc - clip_y * vp3) / w2;
+          // d screen / d pos and vp[ax][3] DEPTH_NEAR / w^2 from the record (k_project)
+          const float ds_dx = bw[23 + ax], ds_dy = bw[26 + ax];
           dpos[ax] = dsx_ * ds_dx + dsy_ * ds_dy;
-          const float d_depth_d_w = DEPTH_NEAR / (Wc * Wc);
-          dpos[ax] += (Wc > DEPTH_NEAR) ? vp3 * d_depth_d_w * d_depth : 0.0f;
+          dpos[ax] += (Wc > DEPTH_NEAR) ? bw[29 + ax] * d_depth : 0.0f;
           daw[ax] = daxx * ds_dx + daxy * ds_dy;
           dbw[ax] = dayx * ds_dx + dayy * ds_dy;
           dcw[ax] = dazx * ds_dx + dazy * ds_dy;
