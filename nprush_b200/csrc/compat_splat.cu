@@ -39,7 +39,7 @@ namespace nps {
 namespace compat {
 
 constexpr int kFwd = 16;        // floats per forward record
-constexpr int kBwd = 32;        // floats per backward record
+constexpr int kBwd = 36;        // floats per backward record (144 B)
 constexpr uint32_t kCap = 1024; // SPLAT_MAX_TILE_SPLATS, constants.ts:35
 constexpr int kChunk = 32;
 constexpr int kThreads = 256;
@@ -176,14 +176,17 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ splat
     dsy[k] = (vp1 * W - clip.y * vp3) / w2;
     kdep[k] = vp3 * d_depth_d_w;
   }
+  // the quaternion's doubles and quadruples (exact scalings) that the
+  // rotation's gradient (splat_backward.wgsl:410-426) multiplies with
   b4[0] = make_float4(W, sx, sy, sz);
   b4[1] = make_float4(m0x, m0y, m1x, m1y);
   b4[2] = make_float4(m2x, m2y, ax.x, ax.y);
   b4[3] = make_float4(ay.x, ay.y, az.x, az.y);
-  b4[4] = make_float4(s[0], s[1], s[2], s[8]);
-  b4[5] = make_float4(s[9], s[10], s[11], dsx[0]);
-  b4[6] = make_float4(dsx[1], dsx[2], dsy[0], dsy[1]);
-  b4[7] = make_float4(dsy[2], kdep[0], kdep[1], kdep[2]);
+  b4[4] = make_float4(s[0], s[1], s[2], 2.0f * s[8]);
+  b4[5] = make_float4(2.0f * s[9], 2.0f * s[10], 2.0f * s[11], 4.0f * s[9]);
+  b4[6] = make_float4(4.0f * s[10], 4.0f * s[11], dsx[0], dsx[1]);
+  b4[7] = make_float4(dsx[2], dsy[0], dsy[1], dsy[2]);
+  b4[8] = make_float4(kdep[0], kdep[1], kdep[2], 0.0f);
 
   // binning AABB, splat_backward.wgsl:157-190 (same arithmetic, cov00/cov11
   // recomputed there without cov01: identical values)
@@ -677,7 +680,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
         const float m0x = bw[4], m0y = bw[5], m1x = bw[6], m1y = bw[7], m2x = bw[8], m2y = bw[9];
         const float axx = bw[10], axy = bw[11], ayx = bw[12], ayy = bw[13], azx = bw[14], azy = bw[15];
         const float pos0 = bw[16], pos1 = bw[17], pos2 = bw[18];
-        const float qw = bw[19], qx = bw[20], qy = bw[21], qz = bw[22];
+        // 2 q and 4 q: x * 2 * q == x * (2 q) exactly, the scaling by 2 or 4 being exact
+        const float q2w = bw[19], q2x = bw[20], q2y = bw[21], q2z = bw[22];
+        const float q4x = bw[23], q4y = bw[24], q4z = bw[25];
         const float TA = T_prev * al;
         const float dColr = dCr * TA, dColg = dCg * TA, dColb = dCb * TA;
         const float d_depth = dD * T_prev * al;
@@ -702,9 +707,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
           // d screen / d pos and vp[ax][3] DEPTH_NEAR / w^2 from the record (k_project)
-          const float ds_dx = bw[23 + ax], ds_dy = bw[26 + ax];
+          const float ds_dx = bw[26 + ax], ds_dy = bw[29 + ax];
           dpos[ax] = dsx_ * ds_dx + dsy_ * ds_dy;
-          dpos[ax] += (Wc > DEPTH_NEAR) ? bw[29 + ax] * d_depth : 0.0f;
+          dpos[ax] += (Wc > DEPTH_NEAR) ? bw[32 + ax] * d_depth : 0.0f;
           daw[ax] = daxx * ds_dx + daxy * ds_dy;
           dbw[ax] = dayx * ds_dx + dayy * ds_dy;
           dcw[ax] = dazx * ds_dx + dazy * ds_dy;
@@ -715,17 +720,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_raster(RasterArgs a) {
           dpos[2] += 0.3f * 2.0f * (pos2 - surf_z) * (T_prev * al);
         }
         // splat_backward.wgsl:410-426
-        const float d_qw = (daw[1] * 2.0f * qz - daw[2] * 2.0f * qy) + (-dbw[0] * 2.0f * qz + dbw[2] * 2.0f * qx) +
-                           (dcw[0] * 2.0f * qy - dcw[1] * 2.0f * qx);
-        const float d_qx = (daw[1] * 2.0f * qy + daw[2] * 2.0f * qz) +
-                           (dbw[0] * 2.0f * qy - dbw[1] * 4.0f * qx + dbw[2] * 2.0f * qw) +
-                           (dcw[0] * 2.0f * qz - dcw[1] * 2.0f * qw - dcw[2] * 4.0f * qx);
-        const float d_qy = (-daw[0] * 4.0f * qy + daw[1] * 2.0f * qx + daw[2] * (-2.0f * qw)) +
-                           (dbw[0] * 2.0f * qx + dbw[2] * 2.0f * qz) +
-                           (dcw[0] * 2.0f * qw + dcw[1] * 2.0f * qz - dcw[2] * 4.0f * qy);
-        const float d_qz = (-daw[0] * 4.0f * qz + daw[1] * 2.0f * qw + daw[2] * 2.0f * qx) +
-                           (-dbw[0] * 2.0f * qw - dbw[1] * 4.0f * qz + dbw[2] * 2.0f * qy) +
-                           (dcw[0] * 2.0f * qx + dcw[1] * 2.0f * qy);
+        const float d_qw = (daw[1] * q2z - daw[2] * q2y) + (-dbw[0] * q2z + dbw[2] * q2x) +
+                           (dcw[0] * q2y - dcw[1] * q2x);
+        const float d_qx = (daw[1] * q2y + daw[2] * q2z) + (dbw[0] * q2y - dbw[1] * q4x + dbw[2] * q2w) +
+                           (dcw[0] * q2z - dcw[1] * q2w - dcw[2] * q4x);
+        const float d_qy = (-daw[0] * q4y + daw[1] * q2x + daw[2] * (-q2w)) + (dbw[0] * q2x + dbw[2] * q2z) +
+                           (dcw[0] * q2w + dcw[1] * q2z - dcw[2] * q4y);
+        const float d_qz = (-daw[0] * q4z + daw[1] * q2w + daw[2] * q2x) +
+                           (-dbw[0] * q2w - dbw[1] * q4z + dbw[2] * q2y) + (dcw[0] * q2x + dcw[1] * q2y);
         qv[0] = to_i32(dpos[0] * kFpPos);
         qv[1] = to_i32(dpos[1] * kFpPos);
         qv[2] = to_i32(dpos[2] * kFpPos);
