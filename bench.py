@@ -35,8 +35,8 @@ sys.path.insert(0, str(ROOT))
 N_GAUSS, N_TEACHER, WIDTH, HEIGHT, VIEWS, CAMS, SH_DEG = 200_000, 250_000, 800, 800, 8, 32, 3  # 200k Gaussians SH3, 800x800, 8 of 32 views
 P_USED = 59          # floats per Gaussian used by the model
 # DRAM traffic of one backward-raster launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# 1-pass ncu capture of this workload (13,727,114 pairs): scaled to a launch by its pair count.
-BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 270_533_120 + 15_059_968, 13_727_114
+# 1-pass ncu capture of this workload (11,433,806 pairs): scaled to a launch by its pair count.
+BWD_TRAFFIC_BYTES, BWD_TRAFFIC_PAIRS = 239_281_152 + 18_662_144, 11_433_806
 S_REC = 36           # algorithmic projected-record bytes (mean2d, conic, rgb, opacity)
 # Warp instructions issued by one launch of each raster kernel (smsp__inst_executed.sum) in a 1-pass
 # ncu capture of this workload with the variant named, and that launch's pair count: scaled to a
