@@ -48,10 +48,11 @@ __device__ __forceinline__ float smoothstepf(float lo, float hi, float x) {
   return t * t * (3.0f - 2.0f * t);
 }
 __device__ __forceinline__ int32_t to_i32(float a) {
+  // the conversion instruction truncates and clamps below at INT32_MIN by
+  // itself (float-to-integer conversions saturate); WGSL's upper bound is the
+  // largest float below 2^31
   if (a != a) return 0;
-  if (a >= 2147483520.0f) return 2147483520;
-  if (a <= -2147483648.0f) return INT32_MIN;
-  return (int32_t)a;
+  return a >= 2147483520.0f ? 2147483520 : (int32_t)a;
 }
 __device__ __forceinline__ float4 mulv(const float* m, float x, float y, float z, float w) {
   float4 o;
