@@ -532,6 +532,8 @@ __global__ void __launch_bounds__(256 / PPT, PPT <= 2 ? 1280 / (256 / PPT) : 1) 
     NPS_ALL_DONE(done);
     if (__syncthreads_count(done) == NT || s_abort) {
       if (pending_next && !mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u)) s_abort = 1u;
+      // a batch whose wait gave up may still have copies in flight: wait again (bounded)
+      if (s_abort) (void)mbar_wait(&s_bar[buf], (bi >> 1) & 1u);
       break;
     }
   }
@@ -1281,6 +1283,7 @@ __global__ void __launch_bounds__(256 / PPT, PPT <= 2 ? 1024 / (256 / PPT) : 1) 
       // batch staged for bi + 1 is waited for (bounded) before the CTA's shared memory is released
       if (tid == 0) {
         atomicAdd(err, 1u);
+        (void)mbar_wait(&s_bar[buf], (bi >> 1) & 1u);  // the batch whose wait gave up, again (bounded)
         if (bi + 1 < nbatch) (void)mbar_wait(&s_bar[buf ^ 1u], ((bi + 1) >> 1) & 1u);
       }
       return;
