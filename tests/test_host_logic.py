@@ -1,6 +1,7 @@
 """CPU tests of the host-side logic around the kernels: the training view
 schedule, the ADC schedule, hindsight relabelling of logged ADC decisions,
-class weights and the Bezier-fit curve generator."""
+class weights, the Bezier-fit curve generator and the fit loop (against a
+fake trainer)."""
 import math
 
 import numpy as np
@@ -57,3 +58,65 @@ def test_random_walk_curves():
     px = b[:, 3] * 512 / 2
     assert px.min() >= 1.0 - 1e-5 and px.max() <= 3.0 + 1e-5
     assert np.all((b[:, 19] >= 0.3) & (b[:, 19] <= 1.0))
+
+
+class _FakeTrainer:
+    """Records the calls fit() makes (the kernels are not involved)."""
+
+    def __init__(self):
+        self.count = 100
+        self.calls = []
+
+    def set_graph(self, on):
+        self.calls.append(("graph", bool(on)))
+
+    def sync(self):
+        pass
+
+    def set_views(self, vp, vpi, sel):
+        self.calls.append(("views", tuple(int(x) for x in sel)))
+
+    def autotune(self):
+        self.calls.append(("autotune",))
+        return {"tile": 16, "fwd_form": 2, "per_tile": {}}
+
+    def train_step(self, read_loss=False):
+        self.calls.append(("step",))
+        return (1.0, 0.0, 0.0) if read_loss else None
+
+    def train_step_per_view(self, vp, vpi, sel, read_loss=False):
+        self.calls.append(("step_per_view", tuple(int(x) for x in sel)))
+        return None
+
+    def adc(self, grad_thresh, split_scale, prune_opacity):
+        self.calls.append(("adc",))
+        self.count += 1
+        return dict(before=self.count - 1, after=self.count, densified=1, pruned=0)
+
+    def stats(self):
+        return {"skipped_steps": 0}
+
+
+def test_fit_autotunes_once_on_the_first_steps_views_and_times_adc():
+    from nprush_b200.train import AdcSchedule, fit, view_schedule
+    vp = np.zeros((32, 16), np.float32)
+    t = _FakeTrainer()
+    r = fit(t, vp, vp, 300, views=8, seed=3, adc=AdcSchedule(every=100, start=100, stop=200), mode="batched",
+            autotune=True)
+    names = [c[0] for c in t.calls]
+    assert names.count("autotune") == 1 and r.tuned["tile"] == 16 and r.tune_s >= 0.0
+    i = names.index("autotune")
+    assert t.calls[i - 1] == ("views", tuple(int(x) for x in view_schedule(0, 32, 8, 3)))
+    assert names.count("step") == 300 and names.count("adc") == 2
+    assert [e[0] for e in r.adc_events] == [100, 200] and r.count == 102
+    assert r.adc_s >= 0.0 and r.after_adc_s >= 0.0
+
+
+def test_fit_per_view_mode_runs_eagerly_without_autotune():
+    from nprush_b200.train import AdcSchedule, fit
+    vp = np.zeros((16, 16), np.float32)
+    t = _FakeTrainer()
+    r = fit(t, vp, vp, 5, views=4, seed=0, adc=AdcSchedule(every=0), mode="per_view")
+    names = [c[0] for c in t.calls]
+    assert ("graph", False) in t.calls and "autotune" not in names and r.tuned is None
+    assert names.count("step_per_view") == 5 and all(len(c[1]) == 4 for c in t.calls if c[0] == "step_per_view")
