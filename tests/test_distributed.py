@@ -2,7 +2,9 @@
 ranks with a stand-in trainer (a least-squares 'renderer' whose views are
 independent until their gradients are summed, like the Gaussian trainer's)
 must follow the single-process trajectory, and stay identical to each other,
-including steps with fewer views than ranks and the ADC statistic sum."""
+including steps with fewer views than ranks and the ADC statistic sum; and a
+rank that fails between steps ends the survivor's next collective with an
+error (short process-group timeout) instead of leaving it waiting."""
 import os
 
 import numpy as np
@@ -130,3 +132,54 @@ def test_shard_views_partition():
             parts = [shard_views(n, r, world) for r in range(world)]
             allv = np.sort(np.concatenate(parts)) if parts else np.array([])
             np.testing.assert_array_equal(allv, np.arange(n))
+
+
+def _failing_worker(rank, world, port, out_dir):
+    """Rank 1 raises between steps (after step 1, before the all-reduce of
+    step 2) and leaves; rank 0 must see its next collective end with an
+    error within the process group's timeout instead of waiting forever."""
+    import datetime
+    import time
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    from nprush_b200.distributed import ShardedTrainer
+    t = FakeTrainer()
+    st = ShardedTrainer(t)
+    outcome = "finished"
+    t0 = time.perf_counter()
+    try:
+        for k, views in enumerate(SCHEDULE):
+            if rank == 1 and k == 2:
+                raise RuntimeError("rank 1 failed between steps")
+            ids = np.array(views, np.uint32)
+            vp = np.zeros((len(ids), 16), np.float32)
+            st.train_step(vp, vp, ids)
+    except RuntimeError as e:
+        outcome = "raised: " + str(e).splitlines()[0][:200]
+    elapsed = time.perf_counter() - t0
+    with open(os.path.join(out_dir, f"outcome{rank}.txt"), "w") as f:
+        f.write(f"{outcome}\n{elapsed:.3f}\n")
+    if rank == 1:
+        os._exit(0)  # leaves without joining the group's teardown
+    try:
+        dist.destroy_process_group()
+    except Exception:  # noqa: BLE001 - the peer is gone
+        pass
+
+
+def test_a_failed_rank_ends_the_survivors_next_collective_with_an_error(tmp_path):
+    port = 30500 + os.getpid() % 1000
+    ctx = mp.start_processes(_failing_worker, args=(2, port, str(tmp_path)), nprocs=2, join=False,
+                             start_method="spawn")
+    for p in ctx.processes:
+        p.join(120)
+    alive = [p for p in ctx.processes if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a rank was still waiting after 120 s"
+    o0 = (tmp_path / "outcome0.txt").read_text().splitlines()
+    o1 = (tmp_path / "outcome1.txt").read_text().splitlines()
+    assert o1[0].startswith("raised: rank 1 failed")
+    assert o0[0].startswith("raised:"), o0  # the survivor's all-reduce of step 2 failed
+    assert float(o0[1]) < 60.0
